@@ -1,0 +1,192 @@
+/*
+ * zebsdsolve_b200 — C ABI of the B200 (sm_100a) kernels of zebsdsolve's spherical
+ * cross-correlation indexing path.
+ *
+ * Every entry point takes device pointers, plain sizes and a CUDA stream (cudaStream_t passed as
+ * void*; NULL is the legacy default stream), enqueues its kernels and returns without waiting.
+ * Return value: 0 on success, a negative ZEB_E* code on failure; zeb_error() then gives the
+ * message (per thread, cleared by reading).  No entry point allocates device memory: the caller
+ * owns every buffer, scratch included, and sizes it with the zeb_*_bytes helpers.
+ *
+ * The entry points replace the reference's GPU schedule functions (zebsdsolve 0.2.8, Zig +
+ * WGSL), which record WGSL dispatches through its WebGPU layer; the file:line cited beside each
+ * is the reference function it stands in for.  The reference's Python/C front end (ze.index,
+ * ze.Solver, the ze_* engine calls) is mirrored one level up by the Python package
+ * zebsdsolve_b200, which drives these entry points.
+ */
+#ifndef ZEBSDSOLVE_B200_H
+#define ZEBSDSOLVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZEB_OK 0
+#define ZEB_EARG (-1)   /* an argument is out of range or a pointer is missing */
+#define ZEB_ECUDA (-2)  /* a CUDA launch or call failed */
+#define ZEB_ESIZE (-3)  /* a size beyond what the kernels support */
+
+/* Message of the last failure on this thread (cleared by the call); returns its length. */
+size_t zeb_error(char* buf, size_t cap);
+/* The library's version string: the reference version it is a drop-in for ("0.2.8"). */
+const char* zeb_version(void);
+
+/* ── tables in FP64 on the device ──────────────────────────────────────────────────────── */
+
+/* Gauss–Legendre nodes x (descending) and weights w of order n.
+ * Replaces sh.gaussLegendre (src/sh.zig:31-72). */
+int zeb_gauss_legendre(int n, double* x, double* w, void* stream);
+
+/* Normalized associated Legendre P̄_l^m(x_i) for every pair below L, plm[i][pair(m,l)].
+ * Replaces sh.legendreAll (src/sh.zig:75-99) over a grid's rings (sh.Grid.init, sh.zig:111-125). */
+int zeb_legendre_table(int L, int n_x, const double* x, double* plm, void* stream);
+
+/* Wigner d^l_{k,m}(π/2) for 0 ≤ k, m, l < L at d[(k·L + m)·L + l] (zero for l < max(k,m)) by
+ * the Jacobi three-term recursion. Replaces sh.wignerHalfPi (src/sh.zig:239-280). */
+int zeb_wigner_half_pi(int L, double* d, void* stream);
+
+/* ── the detector frame ─────────────────────────────────────────────────────────────────── */
+
+typedef struct {
+  int32_t h, w;       /* pattern rows, columns (pixels of the level being worked on) */
+  float c0[3];        /* detector row direction in the sample frame */
+  float c1[3];        /* detector column direction */
+  float c2[3];        /* detector normal */
+  float mask[3];      /* mask centre (row, col) and squared radius in pixels (≤ 0: none) */
+} zeb_frame_t;        /* spherical.Frame (src/spherical.zig:81-90) */
+
+/* ── preprocessing ──────────────────────────────────────────────────────────────────────── */
+
+/* Unpack n stored patterns of h × w (pixel: 0 u8, 1 u16, 2 f32), subtract the static background
+ * (h·w floats, or NULL), subtract (dynamic = 1) or divide by (2) a Gaussian blur of deviation
+ * sigma pixels (0: none), then zero mean and unit norm under the mask (zero outside).
+ * Replaces Prep.run / Prep.filter without CLAHE and band pass (src/prep.zig:143-204,263-272;
+ * shaders/prep.wgsl load, background, blur_rows/cols, the wide blur, combine, normalize). */
+int zeb_prep(const void* raw, int pixel, int n, int h, int w, const float* static_bg, int dynamic,
+             float sigma, const float mask[3], int normalize, float* out, void* stream);
+/* Device scratch bytes zeb_prep needs for a wide blur (sigma ≥ 12 pixels); 0 otherwise. */
+size_t zeb_prep_scratch_bytes(int n, int h, int w, float sigma);
+int zeb_prep_ex(const void* raw, int pixel, int n, int h, int w, const float* static_bg, int dynamic,
+                float sigma, const float mask[3], int normalize, float* out, void* scratch, void* stream);
+
+/* ── the master on the sphere ───────────────────────────────────────────────────────────── */
+
+/* One pass of Gaussian smoothing on the sphere over a (2·radius+1)² tangent lattice of step
+ * `step` radians with weights exp(−(a²+b²)·k). Replaces the sphere_blur pass of Prep.sphereBlur
+ * (src/prep.zig:215-237; shaders/mastersph.wgsl:87-109). */
+int zeb_master_blur_pass(const float* src, float* dst, int side, float step, float k, int radius, void* stream);
+
+/* The master's tangent gradient with its value: grad4[i] = (∇M.xyz, M) at every sheet pixel.
+ * Replaces Prep.gradient (src/prep.zig:253-260; shaders/mastersph.wgsl:124-138). */
+int zeb_master_gradient(const float* sheets, float* grad4, int side, void* stream);
+
+/* The master sampled (bilinear, FP64 arithmetic on the FP32 sheets) at every point of a
+ * Gauss–Legendre grid of n_theta rings (cos θ in x) and n_phi points per ring: out[ring][j].
+ * Replaces the sampling loop of master.Harmonics.init (src/master.zig:680-688). */
+int zeb_master_sample_grid(const float* sheets, int side, const double* x, int n_theta, int n_phi,
+                           double* out, void* stream);
+
+/* ── (a) patterns → spherical-harmonic coefficients ─────────────────────────────────────── */
+
+typedef struct {
+  int32_t L, n_theta, n_phi, n_pairs;
+  const float* ring;    /* [n_theta][4]: cos θ, sin θ, quadrature weight, 0 */
+  const float* phi_cs;  /* [n_phi][2]: cos φ_j, sin φ_j */
+  const float* wplm;    /* [n_theta/2][n_pairs]: w_y · P̄(cos θ_y) · 2π/n_phi */
+  const float* tw;      /* [1024][2]: e^{−2πi t/1024} */
+} zeb_sphere_tables_t;  /* spherical.Tables (src/spherical.zig:106-180) */
+
+#define ZEB_FLAG_CENTER 1u
+#define ZEB_FLAG_NORM 2u
+#define ZEB_FLAG_WINDOW 4u
+
+/* Scratch bytes for n_items items at these tables. */
+size_t zeb_sphere_scratch_bytes(const zeb_sphere_tables_t* tb, int n_items);
+
+/* Each item (items[b] = t.x, t.y, t.z in pixels, pattern index) sampled on the sphere, window-
+ * mean centred (ZEB_FLAG_CENTER), analysed into alm[b][pair][re,im] and scaled to unit norm
+ * (ZEB_FLAG_NORM); ZEB_FLAG_WINDOW projects the window itself. stats[b] = (window area,
+ * window mean, harmonic norm, a_00). Replaces Spherical.coefficients
+ * (src/spherical.zig:319-361; shaders/sphere.wgsl sphere_sums, rings, legendre, sh_norm). */
+int zeb_sphere_coefficients(const float* pats, const float* items, int n_items, const zeb_frame_t* fr,
+                            const zeb_sphere_tables_t* tb, unsigned flags, float* alm, float* stats,
+                            void* scratch, void* stream);
+
+/* ── (b) the SO(3) correlation ──────────────────────────────────────────────────────────── */
+
+typedef struct {
+  int32_t L, n, nb, nc, fold, mu_max, n_pairs;
+} zeb_so3_dims_t;  /* spherical.PhaseGpu + Tables sizes (src/spherical.zig:192-242) */
+
+/* The master's correlation table for one phase at one bandwidth, in FP64 on the device:
+ * Y[pair(m',l)][j·nc + iq] = i^{m'} Σ_k d^l_{k,m'} W[μ,l,k] β_{±}(k, j), the Wigner-d
+ * contraction with the master's weights W (master.weights, src/master.zig:727-753) and the
+ * transform along b (so3.wgsl spectrum, :147-277) folded in (β_+ = 2cos(k b_j), β_− = −2i sin,
+ * by the parity of m'+m; k = 0 once). W is [mc][L][L] complex (re, im) FP64. */
+int zeb_correlation_table(const zeb_so3_dims_t* d, const double* W, const double* wigner, double* Y, void* stream);
+
+/* U[b][j][m'][iq] = Σ_l conj(g_b[l,m']) Y[pair(m',l)][j·nc+iq]: the spectrum of every item
+ * along b, in plain FP32 (CUDA cores). alm as zeb_sphere_coefficients leaves it; Y in FP32.
+ * Replaces Spherical.spectrum (src/spherical.zig:369-382; shaders/so3.wgsl spectrum). */
+int zeb_spectrum_f32(const float* alm, int n_items, const zeb_so3_dims_t* d, const float* Y, float* U, void* stream);
+
+/* Bytes of U for n_items items. */
+size_t zeb_spectrum_bytes(const zeb_so3_dims_t* d, int n_items);
+
+/* The correlation volume's transforms along c and a, times rden (volume b / rden_div for item
+ * b), each (item, j, c) line's largest value, each item's largest, and its sub-grid vertex and
+ * orientation: peaks[b] = (q.w, q.x, q.y, q.z, score, a, b, c). Replaces Spherical.correlate's
+ * a_peak_m, peak_reduce and peak_finish_m (src/spherical.zig:401-432; shaders/so3.wgsl
+ * :489-593, 631-663, 716-796). scratch: zeb_peaks_scratch_bytes. */
+size_t zeb_peaks_scratch_bytes(const zeb_so3_dims_t* d, int n_items);
+int zeb_correlate_peaks(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw, const float* rden,
+                        int rden_div, float* peaks, void* scratch, void* stream);
+
+/* The full volumes (no peak) of n items: vol[b][j][iq][ia]. Replaces a_volume
+ * (shaders/so3.wgsl:595-612). */
+int zeb_correlate_volume(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw, float* vol, void* stream);
+
+/* rden = 1/sqrt(vol_f2 − vol_f²/area) where above 1e-6·area, else 0; area[b·4] per window.
+ * Replaces rden_build (shaders/so3.wgsl:614-626). */
+int zeb_rden_build(const float* vol_f, const float* vol_f2, const float* stats, int n, long long cells,
+                   float* rden, void* stream);
+
+/* ── (c) refinement and scores on the detector ──────────────────────────────────────────── */
+
+typedef struct {
+  int32_t iters;        /* Gauss–Newton steps; iters + 1 passes of sums */
+  float max_step;       /* largest rotation of one step, radians */
+  float scale0, scale_min, scale_max;  /* curvature scale μ: start and bounds */
+  int32_t nmi_bins;
+  float stamp;          /* written into each record's last slot */
+} zeb_refine_opts_t;    /* detector.RefineOptions (src/detector.zig:57-70) */
+
+/* Seed each item with the orientation beginning seeds[b·seed_stride] (spherical peaks or
+ * refinement records), refine it on the detector against its pattern (rotation-only
+ * Gauss–Newton), score it (NCC, NMI) and write records[b] = (q.w, q.x, q.y, q.z, NCC, NMI,
+ * last improving step, stamp). One thread block per item, the pattern resident in shared
+ * memory across the passes. Replaces Detector.seed + Detector.refine (src/detector.zig:178-212;
+ * shaders/detector.wgsl seed, refine_init, sums_rot, refine_rot_step, nmi, collect). */
+int zeb_refine(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
+               const zeb_frame_t* fr, const float* master, const float* grad4, int side,
+               const zeb_refine_opts_t* o, float* records, void* stream);
+
+/* NMI of each item's pattern against the master at `draws` random orientations (Shoemake from
+ * a hash of the item and draw): out[draw][b]. Replaces Detector.chanceOf (src/detector.zig:
+ * 216-229; shaders/detector.wgsl decoy, nmi). */
+int zeb_chance(const float* pats, const float* items, int n, int draws, const zeb_frame_t* fr,
+               const float* master, int side, int nmi_bins, float* out, void* stream);
+
+/* Simulated patterns: the master at q·ray for every pixel of item b (poses[b] = t.xyz, pattern
+ * index, q.wxyz): sims[b][h][w]. Replaces Detector.project (src/detector.zig:138-142;
+ * shaders/detector.wgsl:254-263). */
+int zeb_project(const float* master, int side, const float* poses, int n, const zeb_frame_t* fr, float* sims,
+                void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

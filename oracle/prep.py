@@ -1,0 +1,130 @@
+"""Pattern preprocessing (oracle restatement of zebsdsolve `src/prep.zig` and `shaders/prep.wgsl`):
+unpack, static background, dynamic (Gaussian) background, zero mean / unit norm under the mask.
+Statistics in float64; the blur weights follow the kernels' definitions."""
+import math
+
+import numpy as np
+
+
+def masked(h, w, mask):
+    """prep.wgsl:399-403 — boolean [h, w] of the pixels under the circular mask."""
+    r = np.arange(h)[:, None] - mask[0]
+    c = np.arange(w)[None, :] - mask[1]
+    if mask[2] <= 0:
+        return np.ones((h, w), bool)
+    return r * r + c * c <= mask[2]
+
+
+def blur_direct(img, sigma):
+    """prep.zig:108-118, prep.wgsl:87-164 — separable Gaussian (taps to ceil(3σ)), renormalized
+    over the taps inside the image."""
+    radius = max(1, int(math.ceil(3 * sigma)))
+    k0 = 1.0 / (2 * sigma * sigma)
+    out = np.asarray(img, np.float64)
+    for axis in (1, 0):
+        n = out.shape[axis]
+        x = np.arange(n)
+        d = np.abs(x[:, None] - x[None, :])
+        g = np.where(d <= radius, np.exp(-(d * d) * k0), 0.0)
+        g = g / g.sum(1, keepdims=True)
+        out = out @ g.T if axis == 1 else g @ out
+    return out
+
+
+def _cell(jr, n, s):
+    """prep.wgsl:176-183 — centre and width of coarse cell jr along an axis of n pixels."""
+    lo = jr * s
+    hi = lo + s
+    if jr >= 0 and lo < n:
+        hi = min(hi, n)
+    return 0.5 * (lo + hi - 1), float(hi - lo)
+
+
+def blur_wide(img, sigma):
+    """prep.zig:120-139, prep.wgsl:165-284 — the wide Gaussian from box sums: boxes of s = ⌊σ/6⌋
+    pixels, a coarse Gaussian over the box sums, and a narrow spread of deviation s back to the
+    pixels; sums and counts are carried together and divided at the end."""
+    img = np.asarray(img, np.float64)
+    h, w = img.shape
+    s = int(math.floor(sigma / 6))
+    coarse_sigma = math.sqrt(sigma * sigma - s * s - (s * s - 1) / 12)
+    cpad = 3
+    radius = int(math.ceil(4 * coarse_sigma))
+    kx = 1.0 / (2 * coarse_sigma * coarse_sigma)
+    kz = 1.0 / (2 * s * s)
+    hs = (h + s - 1) // s
+    ws = (w + s - 1) // s
+    wp = ws + 2 * cpad
+    hp = hs + 2 * cpad
+    box = np.zeros((hs, ws, 2))
+    for i in range(hs):
+        for j in range(ws):
+            r1 = min((i + 1) * s, h)
+            c1 = min((j + 1) * s, w)
+            box[i, j, 0] = img[i * s:r1, j * s:c1].sum()
+            box[i, j, 1] = (r1 - i * s) * (c1 - j * s)
+    rows = np.zeros((hs, wp, 2))
+    for t in range(wp):
+        c = _cell(t - cpad, w, s)[0]
+        j0 = max(int(math.floor((c - radius) / s)), 0)
+        j1 = min(int(math.floor((c + radius) / s)), ws - 1)
+        for j in range(j0, j1 + 1):
+            d = _cell(j, w, s)[0] - c
+            rows[:, t] += math.exp(-d * d * kx) * box[:, j]
+    cols = np.zeros((hp, wp, 2))
+    for t in range(hp):
+        c = _cell(t - cpad, h, s)[0]
+        i0 = max(int(math.floor((c - radius) / s)), 0)
+        i1 = min(int(math.floor((c + radius) / s)), hs - 1)
+        for i in range(i0, i1 + 1):
+            d = _cell(i, h, s)[0] - c
+            cols[t] += math.exp(-d * d * kx) * rows[i]
+    spread = np.zeros((hp, w, 2))
+    for x in range(w):
+        own = x // s
+        for t in range(2 * cpad + 1):
+            cx, cw = _cell(own + t - cpad, w, s)
+            d = x - cx
+            spread[:, x] += cw * math.exp(-d * d * kz) * cols[:, own + t]
+    out = np.zeros((h, w))
+    for y in range(h):
+        own = y // s
+        acc = np.zeros((w, 2))
+        for t in range(2 * cpad + 1):
+            cy, cw = _cell(own + t - cpad, h, s)
+            d = y - cy
+            acc += cw * math.exp(-d * d * kz) * spread[own + t]
+        out[y] = acc[:, 0] / acc[:, 1]
+    return out
+
+
+def blur(img, sigma):
+    """prep.zig:108-140 — direct below σ = 12 pixels, else from box sums."""
+    if math.floor(sigma / 6) < 2:
+        return blur_direct(img, sigma)
+    return blur_wide(img, sigma)
+
+
+def normalize(img, mask):
+    """prep.wgsl:405-443 — zero mean and unit norm under the mask, zero outside it."""
+    h, w = img.shape
+    m = masked(h, w, mask)
+    v = np.asarray(img, np.float64)
+    mean = v[m].sum() / max(m.sum(), 1)
+    out = np.where(m, v - mean, 0.0)
+    ss = (out * out).sum()
+    return out / math.sqrt(max(ss, 1e-30))
+
+
+def run(raw, static=None, dynamic="subtract", dynamic_sigma=0.0, mask=(0.0, 0.0, 0.0), do_normalize=True):
+    """prep.zig:143-204, 263-272 — one pattern [h, w] (any integer or float dtype) through the
+    filter chain: static background, dynamic background, then the mask and normalization."""
+    img = np.asarray(raw).astype(np.float64)
+    if static is not None:
+        img = img - np.asarray(static, np.float64)
+    if dynamic != "none" and dynamic_sigma > 0:
+        bg = blur(img, dynamic_sigma)
+        img = img - bg if dynamic == "subtract" else img / np.maximum(bg, 1e-6)
+    if do_normalize:
+        img = normalize(img, mask)
+    return img

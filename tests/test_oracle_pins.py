@@ -1,0 +1,179 @@
+"""The oracle pinned by the reference's own known-answer tests, restated (not copied):
+sh.zig:441-606, lambert.zig:66-85, geometry.zig:195-235, master.zig:811-850 (on a synthetic
+master), and the sphere/correlation path checked against the quadrature integral."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import geometry, lambert, rot, sh, spherical
+
+
+def test_gauss_legendre_integrates_polynomials():
+    # sh.zig:441-454
+    x, w = sh.gauss_legendre(12)
+    assert abs(w.sum() - 2) < 1e-13
+    assert abs((w * x ** 22).sum() - 2.0 / 23.0) < 1e-13
+    assert x[0] > x[11]
+
+
+def test_analysis_inverts_synthesis_and_parseval():
+    # sh.zig:456-482
+    L = 12
+    g = sh.Grid(L, 16, 32)
+    rng = np.random.default_rng(7)
+    ms, _ = sh.pair_table(L)
+    coef = (rng.random(len(ms)) - 0.5) + 1j * np.where(ms == 0, 0.0, rng.random(len(ms)) - 0.5)
+    s = g.synthesize(coef)
+    back = g.analyze(s)
+    assert np.abs(back - coef).max() < 1e-12
+    e = (g.w[:, None] * (2 * math.pi / 32) * s.reshape(16, 32) ** 2).sum()
+    assert abs(sh.power(L, coef) - e) < 1e-11
+
+
+def test_wigner_half_pi_matches_general_formula_and_factorizes():
+    # sh.zig:484-519
+    L = 9
+    tab = sh.wigner_half_pi(L)
+    for l in range(L):
+        for k in range(-l, l + 1):
+            for m in range(-l, l + 1):
+                assert abs(sh.wigner_small_d(l, k, m, math.pi / 2) - sh.d_half_pi(tab, l, k, m)) < 1e-11
+    beta = 0.83
+    l = 5
+    for mp in range(-l, l + 1):
+        for m in range(-l, l + 1):
+            acc = 0j
+            for k in range(-l, l + 1):
+                dd = sh.d_half_pi(tab, 5, k, mp) * sh.d_half_pi(tab, 5, k, m)
+                acc += dd * complex(math.cos(k * beta), -math.sin(k * beta))
+            acc *= sh.ipow(mp - m)
+            assert abs(sh.wigner_small_d(l, mp, m, beta) - acc.real) < 1e-11
+            assert abs(acc.imag) < 1e-11
+
+
+def _ylm(L, l, m, v):
+    p = sh.legendre_all(L, v[2])
+    am = abs(m)
+    phi = math.atan2(v[1], v[0])
+    val = p[sh.pair(L, am, l)]
+    s = 1.0 if (m >= 0 or am % 2 == 0) else -1.0
+    return s * val * complex(math.cos(m * phi), math.sin(m * phi))
+
+
+def test_harmonics_rotate_by_d():
+    # sh.zig:521-548
+    L = 6
+    a, b, c = 0.7, 1.1, -0.4
+    S = rot.from_zyz(a, b, c)
+    x = np.array([0.3, -0.5, 0.6])
+    x /= np.linalg.norm(x)
+    xr = rot.qapply(rot.qconj(S), x)
+    l = 4
+    for m in range(-4, 5):
+        lhs = _ylm(L, l, m, xr)
+        rhs = 0j
+        for mp in range(-4, 5):
+            ang = -(mp * a + m * c)
+            dv = sh.wigner_small_d(4, mp, m, b)
+            rhs += dv * complex(math.cos(ang), math.sin(ang)) * _ylm(L, l, mp, x)
+        assert abs(lhs - rhs) < 1e-12
+
+
+def test_correlation_formula_equals_integral():
+    # sh.zig:550-594
+    L = 6
+    tab = sh.wigner_half_pi(L)
+    rng = np.random.default_rng(3)
+    ms, _ = sh.pair_table(L)
+    f = (rng.random(len(ms)) - 0.5) + 1j * np.where(ms == 0, 0, rng.random(len(ms)) - 0.5)
+    g = (rng.random(len(ms)) - 0.5) + 1j * np.where(ms == 0, 0, rng.random(len(ms)) - 0.5)
+    grid = sh.Grid(L, 24, 48)
+    gs = grid.synthesize(g)
+    a, b, c = 0.9, 0.6, 2.2
+    R = rot.qconj(rot.from_zyz(a, b, c))
+    dirs = grid.directions().reshape(-1, 3)
+    v = rot.qapply(R, dirs)
+    fgrid = sh.Grid(L, 2, 2)  # only for its pair layout
+    p = sh.legendre_all(L, v[:, 2])
+    phi = np.arctan2(v[:, 1], v[:, 0])
+    fv = np.zeros(len(v))
+    for idx, (m, l) in enumerate(zip(*sh.pair_table(L))):
+        k = 1.0 if m == 0 else 2.0
+        fv += k * p[idx] * (f[idx].real * np.cos(m * phi) - f[idx].imag * np.sin(m * phi))
+    w = np.repeat(grid.w, 48) * (2 * math.pi / 48)
+    integral = (w * gs * fv).sum()
+    assert abs(integral - sh.correlation_at(L, tab, f, g, a, b, c)) < 1e-10
+    del fgrid
+
+
+def test_rules_are_read_from_coefficients():
+    # sh.zig:596-606
+    L = 8
+    coef = np.zeros(sh.pair_count(L), complex)
+    for m in range(L):
+        for l in range(m, L):
+            if m % 4 == 0 and l % 2 == 0:
+                coef[sh.pair(L, m, l)] = 1 + 0.5j
+    r = sh.Rules.detect(L, coef, 1e-6)
+    assert r.n_fold == 4 and r.mirror and r.inversion
+    assert r.allows(4, 4) and not r.allows(5, 4) and not r.allows(4, 2)
+
+
+def test_lambert_inverts_with_equal_area():
+    # lambert.zig:66-85
+    pts = [(0.3, -0.7), (-0.9, 0.2), (0.0, 0.5), (1.0, 1.0), (-0.01, 0.01)]
+    for x, y in pts:
+        for south in (False, True):
+            v = lambert.square_to_sphere(x, y, south)
+            assert abs(np.linalg.norm(v) - 1) < 1e-13
+            assert (v[2] <= 1e-12) == south or abs(v[2]) < 1e-12
+            q = lambert.sphere_to_square(v)
+            assert abs(q[0] - x) < 1e-10 and abs(q[1] - y) < 1e-10
+    h = 1e-6
+    for x, y in pts[:3]:
+        dx = (lambert.square_to_sphere(x + h, y, False) - lambert.square_to_sphere(x - h, y, False)) / (2 * h)
+        dy = (lambert.square_to_sphere(x, y + h, False) - lambert.square_to_sphere(x, y - h, False)) / (2 * h)
+        assert abs(np.linalg.norm(np.cross(dx, dy)) - math.pi / 2) < 1e-6
+
+
+def test_pattern_centre_and_pose_are_two_views():
+    # geometry.zig:195-221
+    g = geometry.Geometry(pc=(0.42, 0.21, 0.5), rot_vec=(0.01, -0.02, 0.005))
+    R = g.rotation()
+    t = g.translation(60, 80)
+    pc = geometry.Geometry.pc_of(R, t, 60, 80)
+    assert np.abs(pc - g.pc).max() < 1e-13
+    n = R[:, 2]
+    assert abs(np.dot(n, t) - 0.5 * 60.0) < 1e-10
+    h = geometry.Geometry(rot_vec=(0, math.radians(3.0), 0))
+    tilted = geometry.Geometry(detector_tilt_deg=3)
+    assert np.abs(h.rotation() - tilted.rotation()).max() < 1e-12
+    g.rot = np.zeros(3)
+    t0 = g.translation(60, 60)
+    a = math.radians(-70.0)
+    assert abs(0.21 * 60 * math.sin(a) + 0.5 * 60 * math.cos(a) - math.sin(a) / 2.0 - t0[0]) < 1e-10
+    assert abs(-60.0 * 0.42 + 0.5 - t0[1]) < 1e-10
+    assert abs(0.21 * 60 * math.cos(a) - 0.5 * 60 * math.sin(a) - math.cos(a) / 2.0 - t0[2]) < 1e-10
+    tr = g.translation(61.0 / 2.5, 61.0 / 2.5)
+    back = geometry.Geometry.pc_of(g.rotation(), tr, 61.0 / 2.5, 61.0 / 2.5)
+    assert np.abs(back - g.pc).max() < 1e-13
+
+
+def test_beam_travel_matches_kikuchipy_extrapolation():
+    # geometry.zig:223-235
+    g = geometry.Geometry(pc=(0.42, 0.21, 0.5), px_um=70, step_x_um=1.5, step_y_um=1.5)
+    R = g.rotation()
+    t = g.translation(60, 60)
+    s = g.scan_offset(1, 1, 0, 0, -1, -1, 8)
+    pc = geometry.Geometry.pc_of(R, t - s, 60, 60)
+    f = 1.5 / (70.0 * 8.0 * 60.0)
+    alpha = math.radians(20.0)
+    assert abs(0.42 - f - pc[0]) < 1e-12
+    assert abs(0.21 - f * math.cos(alpha) - pc[1]) < 1e-12
+    assert abs(0.5 + f * math.sin(alpha) - pc[2]) < 1e-12
+
+
+def test_fft_size_and_grids():
+    # spherical.zig:100-104: n is the next power of two ≥ 2L − 1, from 16
+    assert [spherical.fft_size(L) for L in (8, 16, 32, 64, 128)] == [16, 32, 64, 128, 256]

@@ -1,0 +1,218 @@
+"""zebsdsolve_b200: the spherical cross-correlation indexing path of zebsdsolve, on one B200.
+
+A drop-in for the reference's Python API on this path (zebsdsolve 0.2.8, python/zebsdsolve):
+
+    import zebsdsolve_b200 as ze
+
+    result = ze.index(patterns, ["Ni.npz"], pc=(0.5, 0.3, 0.6), bandwidth=64)
+    result.quaternions, result.ncc, result.phase       # per map cell
+
+`Solver` is the engine itself for driving the steps one at a time (configure, set_patterns,
+set_geometry, add_phase, index / index_begin / index_step, results, ...).  Conventions as the
+reference's: quaternions (w, x, y, z) map sample directions to crystal directions, Bunge angles
+in radians, map cells row-major, the pattern centre in the Bruker convention.
+
+Every computation on the path runs in the CUDA library libzebsdsolve_b200.so (hand-written
+sm_100a kernels behind the C ABI of include/zebsdsolve_b200.h); there is no CPU fallback.
+"""
+import json
+
+import numpy as np
+
+__version__ = "0.2.8"
+
+LAUE = {1: "-1", 2: "2/m", 3: "mmm", 4: "4/m", 5: "4/mmm", 6: "-3", 7: "-3m", 8: "6/m", 9: "6/mmm", 10: "m-3", 11: "m-3m"}
+METHODS = ("spherical", "dictionary", "pca")
+
+
+class Error(RuntimeError):
+    """An engine call failed; the message says which and why (the reference's ze.Error)."""
+
+
+def _engine():
+    from .engine import Engine, EngineError
+
+    try:
+        return Engine()
+    except Exception as e:  # noqa: BLE001 - surfaced as the API's own error
+        raise Error(f"engine: {e}") from e
+
+
+class Solver:
+    """One engine on one GPU device (python/zebsdsolve/__init__.py:65-951, the indexing path)."""
+
+    def __init__(self):
+        self._e = _engine()
+
+    def close(self):
+        self._e = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _call(self, what, fn, *a, **k):
+        try:
+            return fn(*a, **k)
+        except Error:
+            raise
+        except Exception as e:  # noqa: BLE001
+            raise Error(f"{what}: {e}") from e
+
+    @property
+    def adapter(self):
+        import torch
+
+        return torch.cuda.get_device_name(self._e.dev)
+
+    def events(self):
+        out, self._e.events = self._e.events, []
+        return out
+
+    def cancel(self):
+        self._e.cancel = True
+
+    # ── settings and geometry ──
+
+    def configure(self, **settings):
+        if settings:
+            self._call("configure", self._e.set.apply, settings)
+        return self
+
+    @property
+    def settings(self):
+        return self._e.set.as_dict()
+
+    @property
+    def geometry(self):
+        return self._e.geo.as_dict()
+
+    def set_geometry(self, **fields):
+        self._call("set_geometry", self._e.geo.set, **fields)
+        return self
+
+    # ── scan ──
+
+    def set_patterns(self, patterns):
+        """Patterns from an array: (rows, cols, h, w) or (n, h, w), uint8, uint16 or float32."""
+        self._call("set_patterns", self._e.set_patterns, patterns)
+        return self
+
+    @property
+    def scan(self):
+        rows, cols, h, w = self._call("scan", self._e.info)
+        return {"rows": rows, "cols": cols, "pattern_shape": (h, w),
+                "dtype": ["uint8", "uint16", "float32"][self._e.pixel], "format": "array"}
+
+    def shape(self, full=False):
+        return self._call("pattern_shape", self._e.pattern_shape)
+
+    @property
+    def pattern_shape(self):
+        return self.shape()
+
+    def lattice(self, n):
+        return self._call("lattice", self._e.lattice, n).astype(np.uint64)
+
+    @property
+    def pixel_angle(self):
+        return float(np.degrees(self._e.pixel_angle() / self._e.set["binning"]))
+
+    # ── phases ──
+
+    def add_phase(self, path):
+        return self._call("add_phase", self._e.add_phase, str(path))
+
+    def clear_phases(self):
+        self._e.clear_phases()
+
+    @property
+    def phases(self):
+        out = []
+        for p in self._e.phases:
+            m = p.master
+            from .rotations import LAUE_NAMES
+
+            out.append({"name": m.name, "side": m.side, "point_group": m.point_group, "space_group": m.space_group,
+                        "laue": LAUE_NAMES[m.laue], "voltage_kv": m.voltage_kv, "rotations": len(m.rotations())})
+        return out
+
+    def master(self, phase=0):
+        """A phase's master as the search compares patterns with it: (2, side, side)."""
+        self._call("master", self._e.prepare_masters)
+        p = self._e.phases[phase]
+        return p.baked[1].cpu().numpy().reshape(2, p.master.side, p.master.side)
+
+    # ── simulation ──
+
+    def simulate(self, quaternions, cells=None, phase=0):
+        q = np.asarray(quaternions, np.float32).reshape(-1, 4)
+        cells = np.arange(len(q)) if cells is None else np.asarray(cells).reshape(-1)
+        return self._call("simulate", self._e.simulate, phase, cells, q)
+
+    # ── indexing ──
+
+    def index_cells(self, cells, method=None, bandwidth=None, dict_grid=None):
+        c = np.asarray(cells, np.int64).reshape(-1)
+        if method not in (None, "spherical"):
+            raise Error(f"index_cells: method {method!r} is not on this engine's path")
+        r = self._call("index_cells", self._e.index_cells, c, bandwidth)
+        return {"quaternions": r[..., :4].copy(), "ncc": r[..., 4].copy(), "nmi": r[..., 5].copy(),
+                "step": r[..., 6].copy(), "z": r[..., 7].copy()}
+
+    def chance(self, phase=0):
+        self._call("chance", self._e.calibrate)
+        return float(self._e.chance_med[phase]), float(self._e.chance_spread[phase])
+
+    def index_begin(self):
+        self._call("index", self._e.index_begin)
+
+    def index_step(self):
+        return self._call("index", self._e.index_step)
+
+    @property
+    def index_status(self):
+        return self._e.status()
+
+    @property
+    def sweep_plan(self):
+        return [tuple(self._e.set.sweep(i)) for i in range(self._e.set["sweeps"])]
+
+    def index(self, progress=None):
+        self.index_begin()
+        while True:
+            left = self.index_step()
+            if progress is not None and progress(self.index_status) is False:
+                break
+            if left == 0:
+                break
+        return self.results()
+
+    def results(self):
+        from .rotations import to_bunge
+
+        rows, cols, h, w = self._e.info()
+        r = self._e.res
+        return {"quaternions": r["quat"].reshape(rows, cols, 4).copy(),
+                "euler": to_bunge(r["quat"].astype(np.float64)).astype(np.float32).reshape(rows, cols, 3),
+                "ncc": r["ncc"].reshape(rows, cols).copy(), "nmi": r["nmi"].reshape(rows, cols).copy(),
+                "phase": r["phase"].reshape(rows, cols).copy(), "z": r["z"].reshape(rows, cols).copy(),
+                "sweep": r["sweep"].reshape(rows, cols).copy()}
+
+    def reduce(self, quaternions, phase=0):
+        from .rotations import to_bunge, to_fz
+
+        q = to_fz(np.asarray(quaternions, np.float64).reshape(-1, 4), self._e.phases[phase].master.rotations())
+        return q.astype(np.float32), to_bunge(q)
+
+    def disorientation(self, a, b, phase=0):
+        from .rotations import disorientation
+
+        qa = np.asarray(a, np.float32).reshape(-1, 4).astype(np.float64)
+        qb = np.asarray(b, np.float32).reshape(-1, 4).astype(np.float64)
+        return disorientation(qa, qb, self._e.phases[phase].master.rotations())
+
+
+from .api import Result, index  # noqa: E402,F401

@@ -1,0 +1,112 @@
+"""ctypes bindings to libzebsdsolve_b200.so, the C ABI of include/zebsdsolve_b200.h.
+
+The library is built in place (python -m zebsdsolve_b200.build). There is no fallback: when it
+is missing, or no CUDA device is present, loading raises NativeError.
+"""
+import ctypes
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_NAME = "libzebsdsolve_b200.so"
+
+c_int, c_uint, c_float, c_double, c_size_t, c_void_p, c_char_p, c_longlong = (
+    ctypes.c_int, ctypes.c_uint, ctypes.c_float, ctypes.c_double, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_char_p,
+    ctypes.c_longlong)
+
+
+class NativeError(RuntimeError):
+    """A library call failed (the message is the library's) or the library cannot be used."""
+
+
+class Frame(ctypes.Structure):
+    _fields_ = [("h", ctypes.c_int32), ("w", ctypes.c_int32), ("c0", c_float * 3), ("c1", c_float * 3),
+                ("c2", c_float * 3), ("mask", c_float * 3)]
+
+
+class SphereTables(ctypes.Structure):
+    _fields_ = [("L", ctypes.c_int32), ("n_theta", ctypes.c_int32), ("n_phi", ctypes.c_int32),
+                ("n_pairs", ctypes.c_int32), ("ring", c_void_p), ("phi_cs", c_void_p), ("wplm", c_void_p),
+                ("tw", c_void_p)]
+
+
+class So3Dims(ctypes.Structure):
+    _fields_ = [("L", ctypes.c_int32), ("n", ctypes.c_int32), ("nb", ctypes.c_int32), ("nc", ctypes.c_int32),
+                ("fold", ctypes.c_int32), ("mu_max", ctypes.c_int32), ("n_pairs", ctypes.c_int32)]
+
+
+class RefineOpts(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int32), ("max_step", c_float), ("scale0", c_float), ("scale_min", c_float),
+                ("scale_max", c_float), ("nmi_bins", ctypes.c_int32), ("stamp", c_float)]
+
+
+P = c_void_p
+_SIGS = {
+    "zeb_error": ([ctypes.c_char_p, c_size_t], c_size_t),
+    "zeb_version": ([], c_char_p),
+    "zeb_gauss_legendre": ([c_int, P, P, P], c_int),
+    "zeb_legendre_table": ([c_int, c_int, P, P, P], c_int),
+    "zeb_wigner_half_pi": ([c_int, P, P], c_int),
+    "zeb_prep": ([P, c_int, c_int, c_int, c_int, P, c_int, c_float, P, c_int, P, P], c_int),
+    "zeb_prep_scratch_bytes": ([c_int, c_int, c_int, c_float], c_size_t),
+    "zeb_prep_ex": ([P, c_int, c_int, c_int, c_int, P, c_int, c_float, P, c_int, P, P, P], c_int),
+    "zeb_master_blur_pass": ([P, P, c_int, c_float, c_float, c_int, P], c_int),
+    "zeb_master_gradient": ([P, P, c_int, P], c_int),
+    "zeb_master_sample_grid": ([P, c_int, P, c_int, c_int, P, P], c_int),
+    "zeb_sphere_scratch_bytes": ([ctypes.POINTER(SphereTables), c_int], c_size_t),
+    "zeb_sphere_coefficients": ([P, P, c_int, ctypes.POINTER(Frame), ctypes.POINTER(SphereTables), c_uint, P, P, P, P],
+                                c_int),
+    "zeb_correlation_table": ([ctypes.POINTER(So3Dims), P, P, P, P], c_int),
+    "zeb_spectrum_f32": ([P, c_int, ctypes.POINTER(So3Dims), P, P, P], c_int),
+    "zeb_spectrum_bytes": ([ctypes.POINTER(So3Dims), c_int], c_size_t),
+    "zeb_peaks_scratch_bytes": ([ctypes.POINTER(So3Dims), c_int], c_size_t),
+    "zeb_correlate_peaks": ([P, c_int, ctypes.POINTER(So3Dims), P, P, c_int, P, P, P], c_int),
+    "zeb_correlate_volume": ([P, c_int, ctypes.POINTER(So3Dims), P, P, P], c_int),
+    "zeb_rden_build": ([P, P, P, c_int, c_longlong, P, P], c_int),
+    "zeb_refine": ([P, P, P, c_int, c_int, ctypes.POINTER(Frame), P, P, c_int, ctypes.POINTER(RefineOpts), P, P], c_int),
+    "zeb_chance": ([P, P, c_int, c_int, ctypes.POINTER(Frame), P, c_int, c_int, P, P], c_int),
+    "zeb_project": ([P, c_int, P, c_int, ctypes.POINTER(Frame), P, P], c_int),
+}
+
+_lib = None
+
+
+def lib_path():
+    return Path(os.environ.get("ZEBSDSOLVE_B200_LIB", HERE / LIB_NAME))
+
+
+def load():
+    """The library with every signature bound (cached)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = lib_path()
+    if not p.exists():
+        raise NativeError(f"{p} not found: build it with `python -m zebsdsolve_b200.build`")
+    lib = ctypes.CDLL(str(p))
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes, fn.restype = args, res
+    _lib = lib
+    return lib
+
+
+def symbols():
+    """Names this module binds (every entry point of include/zebsdsolve_b200.h)."""
+    return list(_SIGS)
+
+
+def last_error(lib=None):
+    lib = lib or load()
+    buf = ctypes.create_string_buffer(1024)
+    n = lib.zeb_error(buf, 1024)
+    return buf.value.decode(errors="replace") if n else ""
+
+
+def call(name, *args):
+    """Call an entry point; a negative return raises NativeError with the library's message."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if isinstance(rc, int) and rc < 0:
+        raise NativeError(f"{name}: {last_error(lib) or rc}")
+    return rc

@@ -1,0 +1,65 @@
+"""The plain-function API (python/zebsdsolve/api.py of the reference): one call per job, each
+opening its own engine.
+
+`scan` is an array of patterns shaped (rows, cols, h, w) or (n, h, w); `phases` are master
+pattern files (ebsdsim .npz).  Keyword arguments naming a geometry field (pc, rot,
+sample_tilt_deg, detector_tilt_deg, px_um, step_x_um, step_y_um) set the geometry; every other
+keyword is a setting.
+"""
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+GEOMETRY_FIELDS = ("pc", "rot", "sample_tilt_deg", "detector_tilt_deg", "px_um", "step_x_um", "step_y_um")
+
+
+@dataclass
+class Result:
+    """Indexing results per map cell, with the geometry they were indexed under (api.py:22-47)."""
+
+    quaternions: np.ndarray
+    euler: np.ndarray
+    ncc: np.ndarray
+    nmi: np.ndarray
+    phase: np.ndarray
+    z: np.ndarray
+    sweep: np.ndarray
+    geometry: dict
+    phases: list
+    settings: dict
+    fit: dict = field(default_factory=dict)
+
+
+def _open(solver, scan, phases, kwargs):
+    from . import Error
+
+    geo = {k: kwargs.pop(k) for k in list(kwargs) if k in GEOMETRY_FIELDS}
+    roi = {k: kwargs.pop(k) for k in list(kwargs) if k in ("roi_x", "roi_y", "roi_w", "roi_h")}
+    solver.configure(**kwargs)
+    if isinstance(scan, (str, Path)) or (isinstance(scan, (list, tuple)) and scan and isinstance(scan[0], (str, Path))):
+        raise Error("open: scan files are read by the reference's readers; pass the patterns as an array")
+    solver.set_patterns(scan)
+    if roi:
+        solver.configure(**roi)
+    if geo:
+        solver.set_geometry(**geo)
+    for p in [phases] if isinstance(phases, (str, Path)) else phases:
+        solver.add_phase(p)
+
+
+def index(scan, phases, fit=None, progress=None, **kwargs):
+    """Index a scan against candidate phases (api.py:111-132). `fit` must be None on this path."""
+    from . import Error, Solver
+
+    if fit not in (None, "geometry", "pc"):
+        raise ValueError('fit is None, "geometry" or "pc"')
+    if fit is not None:
+        raise Error(f"fit={fit!r}: the geometry fits are not part of this engine")
+    s = Solver()
+    try:
+        _open(s, scan, phases, dict(kwargs))
+        r = s.index(progress)
+        return Result(geometry=s.geometry, phases=s.phases, settings=s.settings, fit={}, **r)
+    finally:
+        s.close()

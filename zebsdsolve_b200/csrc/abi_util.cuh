@@ -1,0 +1,29 @@
+// Error reporting shared by the C-ABI entry points: a per-thread message that zeb_error() hands
+// back, argument checks that fail with a message rather than launching, and a launch check.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include "../../include/zebsdsolve_b200.h"
+#include "common.cuh"
+
+namespace zeb {
+void set_error(const char* fmt, ...);
+}
+
+#define ZEB_REQUIRE(cond, code, ...) \
+  do {                               \
+    if (!(cond)) {                   \
+      ::zeb::set_error(__VA_ARGS__); \
+      return (code);                 \
+    }                                \
+  } while (0)
+
+static inline int zeb_launch_check(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    ::zeb::set_error("%s: %s", what, cudaGetErrorString(e));
+    return ZEB_ECUDA;
+  }
+  return ZEB_OK;
+}

@@ -1,0 +1,359 @@
+// (c) The detector side: refinement of each item's orientation on the detector, its NMI, chance
+// decoys and simulated patterns.
+//
+// k_refine is one thread block per item for the whole refinement: the preprocessed pattern sits
+// in shared memory across the iters + 1 passes; each pass sums the 19 rotation-only
+// Gauss–Newton sums over the masked pixels (detector.wgsl:329-363), one thread takes the step
+// (refine_item, detector.wgsl:561-640: NCC, gradient, J'J, accept/reject with the curvature
+// scale μ adapted by the gain ratio, the 3×3 solve, the step clipped to max_step), and the block
+// goes on from the new orientation.  The NMI of the best orientation follows in the same block
+// (detector.wgsl:744-832), then the record (collect, detector.wgsl:545-558).
+#include "abi_util.cuh"
+
+namespace zeb {
+
+struct DetArgs {
+  const float* pats;
+  const float4* items;
+  const float* seeds;
+  int seed_stride;
+  int n, h, w;
+  float3 c0, c1, c2;
+  float mask[3];
+  const float* master;
+  const float4* grad;
+  int side;
+  zeb_refine_opts_t o;
+  float* records;
+  int pat_smem, sim_smem;
+  int draws;
+  float* chance;
+};
+
+__device__ __forceinline__ bool in_mask(const DetArgs& a, int row, int col) {
+  float dr = (float)row - a.mask[0], dc = (float)col - a.mask[1];
+  return a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2];
+}
+
+__device__ __forceinline__ float3 ray_dir(const DetArgs& a, float3 t, int row, int col) {
+  return normalize3(make_float3(a.c0.x * row + a.c1.x * col + t.x, a.c0.y * row + a.c1.y * col + t.y,
+                                a.c0.z * row + a.c1.z * col + t.z));
+}
+
+// symmetric 3×3 (xx, xy, xz, yy, yz, zz) by Cramer's rule (detector.wgsl:519-527)
+__device__ float3 solve3(const float* hm, float3 g) {
+  float m00 = hm[0], m01 = hm[1], m02 = hm[2], m11 = hm[3], m12 = hm[4], m22 = hm[5];
+  float det = m00 * (m11 * m22 - m12 * m12) - m01 * (m01 * m22 - m12 * m02) + m02 * (m01 * m12 - m11 * m02);
+  if (fabsf(det) < 1e-30f) return make_float3(0.f, 0.f, 0.f);
+  // columns of m: c0 = (m00, m01, m02), c1 = (m01, m11, m12), c2 = (m02, m12, m22)
+  float x = g.x * (m11 * m22 - m12 * m12) - m01 * (g.y * m22 - m12 * g.z) + m02 * (g.y * m12 - m11 * g.z);
+  float y = m00 * (g.y * m22 - g.z * m12) - g.x * (m01 * m22 - m12 * m02) + m02 * (m01 * g.z - g.y * m02);
+  float z = m00 * (m11 * g.z - m12 * g.y) - m01 * (m01 * g.z - g.y * m02) + g.x * (m01 * m12 - m11 * m02);
+  return make_float3(x / det, y / det, z / det);
+}
+
+// NMI of the pattern in `pat` against the master at orientation q (detector.wgsl:744-832).
+// `sims` (shared, h·w floats) caches the simulation between the passes when given.
+__device__ float nmi_block(const DetArgs& a, const float* pat, float* sims, float3 t, float4 q, int nbins,
+                           uint32_t* hist, float* red) {
+  const int hw = a.h * a.w;
+  float ext[4] = {3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f};
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+    int row = i / a.w, col = i - row * a.w;
+    if (!in_mask(a, row, col)) continue;
+    float e = pat[i];
+    float s = master_at(a.master, qrot(q, ray_dir(a, t, row, col)), a.side);
+    if (sims) sims[i] = s;
+    ext[0] = fminf(ext[0], e); ext[1] = fmaxf(ext[1], e);
+    ext[2] = fminf(ext[2], s); ext[3] = fmaxf(ext[3], s);
+  }
+  for (int i = threadIdx.x; i < nbins * nbins; i += blockDim.x) hist[i] = 0u;
+  // min / max across the block
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ext[0] = fminf(ext[0], __shfl_xor_sync(0xffffffffu, ext[0], o));
+    ext[1] = fmaxf(ext[1], __shfl_xor_sync(0xffffffffu, ext[1], o));
+    ext[2] = fminf(ext[2], __shfl_xor_sync(0xffffffffu, ext[2], o));
+    ext[3] = fmaxf(ext[3], __shfl_xor_sync(0xffffffffu, ext[3], o));
+  }
+  if (lane == 0)
+    for (int k = 0; k < 4; ++k) red[k * nw + wid] = ext[k];
+  __syncthreads();
+  float r[4] = {3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f};
+  for (int w = 0; w < nw; ++w) {
+    r[0] = fminf(r[0], red[0 * nw + w]); r[1] = fmaxf(r[1], red[1 * nw + w]);
+    r[2] = fminf(r[2], red[2 * nw + w]); r[3] = fmaxf(r[3], red[3 * nw + w]);
+  }
+  __syncthreads();
+  const float ke = (float)nbins / fmaxf(r[1] - r[0], 1e-20f);
+  const float ks = (float)nbins / fmaxf(r[3] - r[2], 1e-20f);
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+    int row = i / a.w, col = i - row * a.w;
+    if (!in_mask(a, row, col)) continue;
+    float e = pat[i];
+    float s = sims ? sims[i] : master_at(a.master, qrot(q, ray_dir(a, t, row, col)), a.side);
+    uint32_t be = min((uint32_t)((e - r[0]) * ke), (uint32_t)(nbins - 1));
+    uint32_t bs = min((uint32_t)((s - r[2]) * ks), (uint32_t)(nbins - 1));
+    atomicAdd(&hist[be * nbins + bs], 1u);
+  }
+  __syncthreads();
+  float acc[3] = {0.f, 0.f, 0.f};  // −Σ c log c (joint), −Σ (marginals), N
+  for (int i = threadIdx.x; i < nbins * nbins; i += blockDim.x) {
+    float c = (float)hist[i];
+    acc[2] += c;
+    if (c > 0.f) acc[0] -= c * logf(c);
+  }
+  if ((int)threadIdx.x < nbins) {
+    float rs = 0.f, cs = 0.f;
+    for (int k = 0; k < nbins; ++k) {
+      rs += (float)hist[threadIdx.x * nbins + k];
+      cs += (float)hist[k * nbins + threadIdx.x];
+    }
+    if (rs > 0.f) acc[1] -= rs * logf(rs);
+    if (cs > 0.f) acc[1] -= cs * logf(cs);
+  }
+  block_sums<3>(acc, red);
+  const float nn = fmaxf(acc[2], 1.f);
+  const float h_joint = logf(nn) + acc[0] / nn;
+  const float h_marg = 2.f * logf(nn) + acc[1] / nn;
+  return h_marg > 1e-12f ? 2.f * (h_marg - h_joint) / h_marg : 0.f;
+}
+
+__global__ void __launch_bounds__(256) k_refine(DetArgs a) {
+  extern __shared__ float smf[];
+  __shared__ float red[24 * 8];
+  __shared__ uint32_t hist[32 * 32];
+  __shared__ float4 sh_q;
+  __shared__ int sh_done;
+  const int b = blockIdx.x;
+  const int hw = a.h * a.w;
+  const float4 it = a.items[b];
+  const float3 t = make_float3(it.x, it.y, it.z);
+  const float* gpat = a.pats + (size_t)(int)it.w * hw;
+  float* pat = smf;
+  float* sims = a.sim_smem ? smf + hw : nullptr;
+  if (a.pat_smem) {
+    for (int i = threadIdx.x; i < hw; i += blockDim.x) pat[i] = gpat[i];
+  } else {
+    pat = (float*)gpat;
+  }
+  // refinement state (thread 0's registers): detector.wgsl:73-77
+  const float* sd0 = a.seeds + (size_t)b * a.seed_stride;
+  float4 q_cur = make_float4(sd0[0], sd0[1], sd0[2], sd0[3]);
+  float4 q_best = q_cur;
+  float best = -2.f, mu = a.o.scale0, g_best[3] = {0.f, 0.f, 0.f}, h_best[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float last_good = 0.f, promised = 0.f, step_len = 0.f, accepted = 0.f;
+  if (threadIdx.x == 0) sh_q = q_cur;
+  __syncthreads();
+
+  for (int iter = 0; iter <= a.o.iters; ++iter) {
+    const float4 q = sh_q;
+    float s[19];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) s[k] = 0.f;
+    for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+      int row = i / a.w, col = i - row * a.w;
+      if (!in_mask(a, row, col)) continue;
+      float3 c = qrot(q, ray_dir(a, t, row, col));
+      float4 m = grad_at(a.grad, c, a.side);
+      float3 d = cross3(c, make_float3(m.x, m.y, m.z));
+      float e = pat[i];
+      s[0] += 1.f; s[1] += m.w; s[2] += m.w * m.w; s[3] += m.w * e;
+      s[4] += d.x; s[5] += d.y; s[6] += d.z;
+      s[7] += m.w * d.x; s[8] += m.w * d.y; s[9] += m.w * d.z;
+      s[10] += e * d.x; s[11] += e * d.y; s[12] += e * d.z;
+      s[13] += d.x * d.x; s[14] += d.y * d.y; s[15] += d.z * d.z;
+      s[16] += d.x * d.y; s[17] += d.x * d.z; s[18] += d.y * d.z;
+    }
+    block_sums<19>(s, red);
+    if (threadIdx.x == 0) {
+      // refine_item (detector.wgsl:561-640)
+      const float n = fmaxf(s[0], 1.f);
+      const float mean = s[1] / n;
+      const float var_n = s[2] - n * mean * mean;
+      float ncc = -2.f, g[3] = {0.f, 0.f, 0.f}, hs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (var_n > 1e-12f) {
+        const float inv = rsqrtf(var_n);
+        ncc = s[3] * inv;
+        const float sd[3] = {s[4], s[5], s[6]};
+        float au[3];
+        for (int k = 0; k < 3; ++k) au[k] = (s[7 + k] - mean * sd[k]) * inv;
+        for (int k = 0; k < 3; ++k) g[k] = (s[10 + k] - ncc * au[k]) * inv;
+        const float iv = inv * inv;
+        hs[0] = (s[13] - sd[0] * sd[0] / n - au[0] * au[0]) * iv;
+        hs[1] = (s[16] - sd[0] * sd[1] / n - au[0] * au[1]) * iv;
+        hs[2] = (s[17] - sd[0] * sd[2] / n - au[0] * au[2]) * iv;
+        hs[3] = (s[14] - sd[1] * sd[1] / n - au[1] * au[1]) * iv;
+        hs[4] = (s[18] - sd[1] * sd[2] / n - au[1] * au[2]) * iv;
+        hs[5] = (s[15] - sd[2] * sd[2] / n - au[2] * au[2]) * iv;
+      }
+      if (ncc > best) {
+        if (accepted > 0.5f && promised > 1e-6f) {
+          float rho = (ncc - best) / promised;
+          mu = fminf(fmaxf(mu * (2.f - rho), mu / 3.f), mu * 3.f);
+        }
+        q_best = q;
+        best = ncc;
+        for (int k = 0; k < 3; ++k) g_best[k] = g[k];
+        for (int k = 0; k < 6; ++k) h_best[k] = hs[k];
+        last_good = step_len;
+        accepted += 1.f;
+      } else {
+        mu = mu * 3.f;
+      }
+      mu = fminf(fmaxf(mu, a.o.scale_min), a.o.scale_max);
+      if (iter < a.o.iters) {
+        float hh[6];
+        for (int k = 0; k < 6; ++k) hh[k] = h_best[k] * mu;
+        float tr = fmaxf(hh[0] + hh[3] + hh[5], 1e-20f);
+        hh[0] += 1e-6f * tr; hh[3] += 1e-6f * tr; hh[5] += 1e-6f * tr;
+        float3 gg = make_float3(g_best[0], g_best[1], g_best[2]);
+        float3 stp = solve3(hh, gg);
+        float len = sqrtf(dot3(stp, stp));
+        if (len > a.o.max_step) {
+          float k = a.o.max_step / len;
+          stp = make_float3(stp.x * k, stp.y * k, stp.z * k);
+        }
+        float quad = hh[0] * stp.x * stp.x + hh[3] * stp.y * stp.y + hh[5] * stp.z * stp.z +
+                     2.f * (hh[1] * stp.x * stp.y + hh[2] * stp.x * stp.z + hh[4] * stp.y * stp.z);
+        promised = dot3(gg, stp) - 0.5f * quad;
+        step_len = sqrtf(dot3(stp, stp));
+        float4 qn = qmul(qexp(stp), q_best);
+        float nq = sqrtf(qn.x * qn.x + qn.y * qn.y + qn.z * qn.z + qn.w * qn.w);
+        q_cur = nq > 0.f ? make_float4(qn.x / nq, qn.y / nq, qn.z / nq, qn.w / nq) : make_float4(1.f, 0.f, 0.f, 0.f);
+        sh_q = q_cur;
+      } else {
+        sh_q = q_best;
+      }
+    }
+    __syncthreads();
+  }
+  const float4 qf = sh_q;
+  float v = nmi_block(a, pat, sims, t, qf, a.o.nmi_bins, hist, red);
+  if (threadIdx.x == 0) {
+    float* r = a.records + (size_t)b * 8;
+    r[0] = qf.x; r[1] = qf.y; r[2] = qf.z; r[3] = qf.w;
+    r[4] = best; r[5] = v; r[6] = last_good; r[7] = a.o.stamp;
+  }
+  (void)sh_done;
+}
+
+__device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
+  uint32_t v = x * 747796405u + 2891336453u;
+  uint32_t w = ((v >> ((v >> 28u) + 4u)) ^ v) * 277803737u;
+  return (w >> 22u) ^ w;
+}
+
+__device__ __forceinline__ float unit_rand(uint32_t x) { return (float)(hash_u32(x) >> 8u) / 16777216.f; }
+
+// detector.wgsl:296-308 — Shoemake's uniform rotation, per item and draw
+__device__ __forceinline__ float4 decoy_q(uint32_t b, uint32_t draw) {
+  uint32_t s = hash_u32(b + 1u) ^ (draw * 0x9e3779b9u);
+  float u1 = unit_rand(s);
+  float a2 = unit_rand(s + 1u) * ZEB_TAU;
+  float a3 = unit_rand(s + 2u) * ZEB_TAU;
+  float ra = sqrtf(1.f - u1), rb = sqrtf(u1);
+  return make_float4(ra * sinf(a2), ra * cosf(a2), rb * sinf(a3), rb * cosf(a3));
+}
+
+__global__ void __launch_bounds__(256) k_chance(DetArgs a) {
+  extern __shared__ float smf[];
+  __shared__ float red[24 * 8];
+  __shared__ uint32_t hist[32 * 32];
+  const int b = blockIdx.x, draw = blockIdx.y;
+  const int hw = a.h * a.w;
+  const float4 it = a.items[b];
+  const float3 t = make_float3(it.x, it.y, it.z);
+  const float* gpat = a.pats + (size_t)(int)it.w * hw;
+  float* pat = smf;
+  float* sims = a.sim_smem ? smf + hw : nullptr;
+  if (a.pat_smem) {
+    for (int i = threadIdx.x; i < hw; i += blockDim.x) pat[i] = gpat[i];
+  } else {
+    pat = (float*)gpat;
+  }
+  __syncthreads();
+  float4 q = decoy_q((uint32_t)b, (uint32_t)draw);
+  float v = nmi_block(a, pat, sims, t, q, a.o.nmi_bins, hist, red);
+  if (threadIdx.x == 0) a.chance[(size_t)draw * a.n + b] = v;
+}
+
+__global__ void k_project(DetArgs a, const float* __restrict__ poses, float* __restrict__ sims) {
+  const int hw = a.h * a.w;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)a.n * hw) return;
+  int b = (int)(t / hw), pix = (int)(t % hw);
+  const float* p = poses + (size_t)b * 8;
+  float3 tt = make_float3(p[0], p[1], p[2]);
+  float4 q = make_float4(p[4], p[5], p[6], p[7]);
+  int row = pix / a.w, col = pix - row * a.w;
+  sims[t] = master_at(a.master, qrot(q, ray_dir(a, tt, row, col)), a.side);
+}
+
+static bool fill_frame(DetArgs& a, const zeb_frame_t* fr) {
+  if (!fr || fr->h < 2 || fr->w < 2) return false;
+  a.h = fr->h; a.w = fr->w;
+  a.c0 = make_float3(fr->c0[0], fr->c0[1], fr->c0[2]);
+  a.c1 = make_float3(fr->c1[0], fr->c1[1], fr->c1[2]);
+  a.c2 = make_float3(fr->c2[0], fr->c2[1], fr->c2[2]);
+  for (int k = 0; k < 3; ++k) a.mask[k] = fr->mask[k];
+  return true;
+}
+
+static size_t det_smem(DetArgs& a) {
+  size_t hw = (size_t)a.h * a.w;
+  a.pat_smem = hw * 4 <= 100 * 1024;
+  a.sim_smem = a.pat_smem && hw * 8 <= 180 * 1024;
+  return (a.pat_smem ? hw * 4 : 0) + (a.sim_smem ? hw * 4 : 0);
+}
+
+}  // namespace zeb
+
+using namespace zeb;
+
+extern "C" int zeb_refine(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
+                          const zeb_frame_t* fr, const float* master, const float* grad4, int side,
+                          const zeb_refine_opts_t* o, float* records, void* stream) {
+  ZEB_REQUIRE(pats && items && seeds && master && grad4 && o && records, ZEB_EARG, "refine: null argument");
+  ZEB_REQUIRE(seed_stride >= 4 && side >= 3 && o->iters >= 0 && o->iters <= 1000 && o->nmi_bins >= 2 &&
+                  o->nmi_bins <= 32,
+              ZEB_EARG, "refine: bad arguments");
+  if (n <= 0) return ZEB_OK;
+  DetArgs a{};
+  ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine: bad frame");
+  a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
+  a.master = master; a.grad = (const float4*)grad4; a.side = side; a.o = *o; a.records = records;
+  size_t smem = det_smem(a);
+  cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_refine<<<n, 256, smem, (cudaStream_t)stream>>>(a);
+  return zeb_launch_check("refine");
+}
+
+extern "C" int zeb_chance(const float* pats, const float* items, int n, int draws, const zeb_frame_t* fr,
+                          const float* master, int side, int nmi_bins, float* out, void* stream) {
+  ZEB_REQUIRE(pats && items && master && out && draws >= 1 && draws <= 65535 && nmi_bins >= 2 && nmi_bins <= 32,
+              ZEB_EARG, "chance: bad arguments");
+  if (n <= 0) return ZEB_OK;
+  DetArgs a{};
+  ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "chance: bad frame");
+  a.pats = pats; a.items = (const float4*)items; a.n = n; a.master = master; a.side = side;
+  a.o.nmi_bins = nmi_bins; a.chance = out; a.draws = draws;
+  size_t smem = det_smem(a);
+  cudaFuncSetAttribute(k_chance, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 g(n, draws);
+  k_chance<<<g, 256, smem, (cudaStream_t)stream>>>(a);
+  return zeb_launch_check("chance");
+}
+
+extern "C" int zeb_project(const float* master, int side, const float* poses, int n, const zeb_frame_t* fr,
+                           float* sims, void* stream) {
+  ZEB_REQUIRE(master && poses && sims && side >= 3, ZEB_EARG, "project: bad arguments");
+  if (n <= 0) return ZEB_OK;
+  DetArgs a{};
+  ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "project: bad frame");
+  a.n = n; a.master = master; a.side = side;
+  long long total = (long long)n * a.h * a.w;
+  k_project<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a, poses, sims);
+  return zeb_launch_check("project");
+}

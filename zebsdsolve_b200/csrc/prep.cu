@@ -1,0 +1,290 @@
+// Pattern preprocessing: one thread block per pattern does the whole chain (unpack, static
+// background, dynamic background, mask and normalization) with the image held in shared memory
+// when it fits, so a pattern is read from HBM once and written once.
+//
+// The arithmetic follows shaders/prep.wgsl: the direct Gaussian (taps to ceil(3σ), renormalized
+// over the taps inside the image) below σ = 12 pixels, the box-sum construction above it
+// (box sums of s = ⌊σ/6⌋ pixels, a coarse Gaussian over them with a margin of cpad = 3 cells,
+// and a spread of deviation s back over the pixels).
+#include "abi_util.cuh"
+
+namespace zeb {
+
+struct PrepArgs {
+  const void* raw;
+  int pixel, n, h, w;
+  const float* static_bg;
+  int dynamic;  // 0 none, 1 subtract, 2 divide
+  float sigma;
+  float mask[3];
+  int normalize;
+  float* out;
+  float* scratch;  // per pattern: scratch_per floats
+  long long scratch_per;
+  int use_smem;
+  // direct blur
+  int radius;
+  float k0;
+  // wide blur
+  int bin, cpad, wradius;
+  float kx, kz;
+};
+
+__device__ __forceinline__ float2 wide_cell(int jr, int n, int s) {
+  int lo = jr * s;
+  int hi = lo + s;
+  if (jr >= 0 && lo < n) hi = min(hi, n);
+  return make_float2(0.5f * (float)(lo + hi - 1), (float)(hi - lo));
+}
+
+__global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
+  extern __shared__ float sm[];
+  __shared__ float taps[64];
+  __shared__ float red[2 * 8];
+  const int b = blockIdx.x;
+  const int h = a.h, w = a.w, hw = h * w;
+  float* img = a.use_smem ? sm : a.out + (size_t)b * hw;
+  float* tmp = a.use_smem ? sm + hw : a.scratch + (size_t)b * a.scratch_per;
+
+  // unpack
+  const size_t base = (size_t)b * hw;
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+    float v;
+    if (a.pixel == 0) v = (float)((const uint8_t*)a.raw)[base + i];
+    else if (a.pixel == 1) v = (float)((const uint16_t*)a.raw)[base + i];
+    else v = ((const float*)a.raw)[base + i];
+    if (a.static_bg) v -= __ldg(a.static_bg + i);
+    img[i] = v;
+  }
+  __syncthreads();
+
+  if (a.dynamic != 0 && a.sigma > 0.f) {
+    float* bg;  // the blurred image, one value per pixel
+    if (a.bin < 2) {
+      for (int d = threadIdx.x; d <= min(a.radius, 63); d += blockDim.x) taps[d] = expf(-(float)(d * d) * a.k0);
+      __syncthreads();
+      const int R = a.radius;
+      // along the rows into tmp
+      for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+        int r = i / w, c = i - r * w;
+        float s = 0.f, g = 0.f;
+        for (int x = max(c - R, 0); x <= min(c + R, w - 1); ++x) {
+          int dd = abs(x - c);
+          float t = dd <= R ? taps[min(dd, 63)] : 0.f;
+          s += t * img[r * w + x];
+          g += t;
+        }
+        tmp[i] = s / g;
+      }
+      __syncthreads();
+      // along the columns: the background, combined with the image in place
+      for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+        int r = i / w, c = i - r * w;
+        float s = 0.f, g = 0.f;
+        for (int y = max(r - R, 0); y <= min(r + R, h - 1); ++y) {
+          int dd = abs(y - r);
+          float t = dd <= R ? taps[min(dd, 63)] : 0.f;
+          s += t * tmp[y * w + c];
+          g += t;
+        }
+        float bgv = s / g;
+        img[i] = a.dynamic == 1 ? img[i] - bgv : img[i] / fmaxf(bgv, 1e-6f);
+      }
+      __syncthreads();
+      bg = nullptr;
+    } else {
+      const int s = a.bin, cp = a.cpad;
+      const int hs = (h + s - 1) / s, ws = (w + s - 1) / s, wp = ws + 2 * cp, hp = hs + 2 * cp;
+      float2* box = (float2*)(a.scratch + (size_t)b * a.scratch_per + (a.use_smem ? 0 : hw));
+      float2* rows = box + hs * ws;
+      float2* cols = rows + hs * wp;
+      float2* spread = cols + hp * wp;
+      for (int t = threadIdx.x; t < hs * ws; t += blockDim.x) {
+        int i = t / ws, j = t - i * ws;
+        int r1 = min((i + 1) * s, h), c1 = min((j + 1) * s, w);
+        float acc = 0.f;
+        for (int r = i * s; r < r1; ++r)
+          for (int c = j * s; c < c1; ++c) acc += img[r * w + c];
+        box[t] = make_float2(acc, (float)((r1 - i * s) * (c1 - j * s)));
+      }
+      __syncthreads();
+      const float reach = (float)a.wradius;
+      for (int t = threadIdx.x; t < hs * wp; t += blockDim.x) {
+        int line = t / wp, tc = t - line * wp;
+        float c = wide_cell(tc - cp, w, s).x;
+        int j0 = max((int)floorf((c - reach) / (float)s), 0);
+        int j1 = min((int)floorf((c + reach) / (float)s), ws - 1);
+        float2 acc = make_float2(0.f, 0.f);
+        for (int j = j0; j <= j1; ++j) {
+          float d = wide_cell(j, w, s).x - c;
+          float e = expf(-d * d * a.kx);
+          float2 v = box[line * ws + j];
+          acc.x += e * v.x; acc.y += e * v.y;
+        }
+        rows[t] = acc;
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < hp * wp; t += blockDim.x) {
+        int tr = t / wp, col = t - tr * wp;
+        float c = wide_cell(tr - cp, h, s).x;
+        int i0 = max((int)floorf((c - reach) / (float)s), 0);
+        int i1 = min((int)floorf((c + reach) / (float)s), hs - 1);
+        float2 acc = make_float2(0.f, 0.f);
+        for (int i = i0; i <= i1; ++i) {
+          float d = wide_cell(i, h, s).x - c;
+          float e = expf(-d * d * a.kx);
+          float2 v = rows[i * wp + col];
+          acc.x += e * v.x; acc.y += e * v.y;
+        }
+        cols[t] = acc;
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < hp * w; t += blockDim.x) {
+        int tr = t / w, x = t - tr * w;
+        int own = x / s;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int q = 0; q <= 2 * cp; ++q) {
+          float2 cw = wide_cell(own + q - cp, w, s);
+          float d = (float)x - cw.x;
+          float e = cw.y * expf(-d * d * a.kz);
+          float2 v = cols[tr * wp + own + q];
+          acc.x += e * v.x; acc.y += e * v.y;
+        }
+        spread[t] = acc;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+        int y = i / w, x = i - y * w;
+        int own = y / s;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int q = 0; q <= 2 * cp; ++q) {
+          float2 cw = wide_cell(own + q - cp, h, s);
+          float d = (float)y - cw.x;
+          float e = cw.y * expf(-d * d * a.kz);
+          float2 v = spread[(own + q) * w + x];
+          acc.x += e * v.x; acc.y += e * v.y;
+        }
+        float bgv = acc.x / acc.y;
+        img[i] = a.dynamic == 1 ? img[i] - bgv : img[i] / fmaxf(bgv, 1e-6f);
+      }
+      __syncthreads();
+      bg = nullptr;
+    }
+    (void)bg;
+  }
+
+  float* out = a.out + base;
+  if (!a.normalize) {
+    if (a.use_smem)
+      for (int i = threadIdx.x; i < hw; i += blockDim.x) out[i] = img[i];
+    return;
+  }
+  // zero mean and unit norm under the mask (prep.wgsl:405-443)
+  float v2[2] = {0.f, 0.f};
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+    int r = i / w, c = i - r * w;
+    float dr = (float)r - a.mask[0], dc = (float)c - a.mask[1];
+    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) {
+      v2[0] += img[i];
+      v2[1] += 1.f;
+    }
+  }
+  block_sums<2>(v2, red);
+  const float mean = v2[0] / fmaxf(v2[1], 1.f);
+  float ss[1] = {0.f};
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+    int r = i / w, c = i - r * w;
+    float dr = (float)r - a.mask[0], dc = (float)c - a.mask[1];
+    float v = 0.f;
+    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) v = img[i] - mean;
+    img[i] = v;
+    ss[0] += v * v;
+  }
+  block_sums<1>(ss, red);
+  const float inv = rsqrtf(fmaxf(ss[0], 1e-30f));
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) out[i] = img[i] * inv;
+}
+
+struct WideDims {
+  int bin, hs, ws, hp, wp;
+};
+
+static WideDims wide_dims(int h, int w, float sigma) {
+  WideDims d{};
+  d.bin = (int)floorf(sigma / 6.f);
+  if (d.bin < 2) return d;
+  d.hs = (h + d.bin - 1) / d.bin;
+  d.ws = (w + d.bin - 1) / d.bin;
+  d.hp = d.hs + 6;
+  d.wp = d.ws + 6;
+  return d;
+}
+
+static long long scratch_floats(int h, int w, float sigma, int dynamic, bool smem) {
+  long long per = 0;
+  if (!smem) per += (long long)h * w;  // the row-blurred image
+  if (dynamic && sigma > 0.f) {
+    WideDims d = wide_dims(h, w, sigma);
+    if (d.bin >= 2) per += 2LL * (d.hs * d.ws + d.hs * d.wp + d.hp * d.wp + (long long)d.hp * w);
+  }
+  return per;
+}
+
+static bool prep_smem(int h, int w) { return 2LL * h * w * 4 <= 160 * 1024; }
+
+}  // namespace zeb
+
+using namespace zeb;
+
+extern "C" size_t zeb_prep_scratch_bytes(int n, int h, int w, float sigma) {
+  if (n <= 0 || h <= 0 || w <= 0) return 0;
+  long long per = scratch_floats(h, w, sigma, 1, prep_smem(h, w));
+  if (!prep_smem(h, w) && per == 0) per = (long long)h * w;
+  return (size_t)per * 4 * (size_t)n;
+}
+
+extern "C" int zeb_prep_ex(const void* raw, int pixel, int n, int h, int w, const float* static_bg, int dynamic,
+                           float sigma, const float mask[3], int normalize, float* out, void* scratch,
+                           void* stream) {
+  ZEB_REQUIRE(raw && out && mask, ZEB_EARG, "prep: null pointer");
+  ZEB_REQUIRE(pixel >= 0 && pixel <= 2 && n >= 0 && h >= 4 && w >= 4 && dynamic >= 0 && dynamic <= 2, ZEB_EARG,
+              "prep: bad arguments pixel=%d n=%d h=%d w=%d dynamic=%d", pixel, n, h, w, dynamic);
+  if (n == 0) return ZEB_OK;
+  PrepArgs a{};
+  a.raw = raw; a.pixel = pixel; a.n = n; a.h = h; a.w = w; a.static_bg = static_bg;
+  a.dynamic = (sigma > 0.f) ? dynamic : 0; a.sigma = sigma;
+  a.mask[0] = mask[0]; a.mask[1] = mask[1]; a.mask[2] = mask[2];
+  a.normalize = normalize; a.out = out;
+  a.use_smem = prep_smem(h, w) ? 1 : 0;
+  a.scratch_per = scratch_floats(h, w, sigma, a.dynamic, a.use_smem);
+  a.scratch = (float*)scratch;
+  ZEB_REQUIRE(a.scratch_per == 0 || scratch, ZEB_EARG, "prep: scratch needed (%lld floats per pattern)",
+              a.scratch_per);
+  if (a.dynamic) {
+    WideDims d = wide_dims(h, w, sigma);
+    a.bin = d.bin;
+    if (d.bin < 2) {
+      a.radius = (int)fmaxf(1.f, ceilf(3.f * sigma));
+      ZEB_REQUIRE(a.radius <= 63, ZEB_ESIZE, "prep: blur radius %d", a.radius);
+      a.k0 = (float)(1.0 / (2.0 * (double)sigma * sigma));
+    } else {
+      double sf = d.bin;
+      double cs = sqrt((double)sigma * sigma - sf * sf - (sf * sf - 1.0) / 12.0);
+      a.cpad = 3;
+      a.wradius = (int)ceil(4.0 * cs);
+      a.kx = (float)(1.0 / (2.0 * cs * cs));
+      a.kz = (float)(1.0 / (2.0 * sf * sf));
+    }
+  }
+  size_t smem = a.use_smem ? 2 * (size_t)h * w * 4 : 0;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_prep<<<n, 256, smem, (cudaStream_t)stream>>>(a);
+  return zeb_launch_check("prep");
+}
+
+extern "C" int zeb_prep(const void* raw, int pixel, int n, int h, int w, const float* static_bg, int dynamic,
+                        float sigma, const float mask[3], int normalize, float* out, void* stream) {
+  ZEB_REQUIRE(zeb_prep_scratch_bytes(n, h, w, dynamic ? sigma : 0.f) == 0, ZEB_EARG,
+              "prep: this size needs scratch (zeb_prep_ex)");
+  return zeb_prep_ex(raw, pixel, n, h, w, static_bg, dynamic, sigma, mask, normalize, out, nullptr, stream);
+}

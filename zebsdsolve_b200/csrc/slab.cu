@@ -1,0 +1,312 @@
+// (b, second stage) The correlation volume's transforms along c and a, one (item, j) slab per
+// thread block, entirely in shared memory, and the peak.
+//
+// The slab U[b][j][m' < L][iq < nc] is loaded, transformed along c (length nc) row by row into
+// V[m'][c]; the real transform along a, C(a) = V[0] + 2 Re Σ_{m'>0} V[m'] e^{−i m' a} at the n
+// grid values of a, comes out of one complex FFT of length h = n/2 per column: its input is
+// Z_q = (X_q + X_{q+h}) + i e^{−2πiq/n}(X_q − X_{q+h}) with X_{q+h} = conj X_{h−q}, and its
+// output z_p = C(a_{2p}) + i C(a_{2p+1}) (so3.wgsl:279-315, 396-593).  Each column's values are
+// scaled by the reciprocal denominator volume and the largest kept with its volume index
+// (j·nc + c)·n + ia; the block keeps its slab's best (first index of equal values).
+// k_peak_finish then takes each item's best slab, re-evaluates the six neighbours of the peak by
+// direct sums over m' (V taken from U along c directly) and fits the parabolic vertex along a, c
+// and b (so3.wgsl:665-796).
+#include "abi_util.cuh"
+
+namespace zeb {
+
+struct SlabArgs {
+  const float2* U;
+  int n_items;
+  zeb_so3_dims_t d;
+  int lgc, lgh;
+  const float2* tw;
+  const float* rden;
+  int rden_div;
+  float2* cand;  // [item][nb]: (value, bits of index)
+  float* vol;    // volume mode: [item][nb][nc][n]
+};
+
+template <bool VOLUME>
+__global__ void __launch_bounds__(256) k_slab(SlabArgs a) {
+  extern __shared__ float2 sm2[];
+  __shared__ float redv[8];
+  __shared__ uint32_t redi[8];
+  const zeb_so3_dims_t& d = a.d;
+  const int L = d.L, nc = d.nc, n = d.n, nb = d.nb;
+  const int h = n >> 1;
+  const int slab = blockIdx.x;  // b·nb + j
+  const int b = slab / nb, j = slab - b * nb;
+  const int lgc = a.lgc, lgh = a.lgh;
+  float2* V = sm2;            // [L][nc]
+  float2* Z = sm2 + L * nc;   // [h][nc]
+  RowLines rows{lgc};
+  ColLines cols{lgc};
+  const float2* src = a.U + (size_t)slab * L * nc;
+  // rows bit-reversed along c
+  for (int e = threadIdx.x; e < L * nc; e += blockDim.x) {
+    int r = e >> lgc, c = e & (nc - 1);
+    V[rows(r, bitrev(c, lgc))] = src[e];
+  }
+  __syncthreads();
+  if (lgc > 0) fft_lines_smem(V, L, lgc, a.tw, rows);
+  // Z down each column, bit-reversed along a
+  const int tws = ZEB_TW_LEN / (2 * h);
+  for (int e = threadIdx.x; e < h * nc; e += blockDim.x) {
+    int q = e >> lgc, c = e & (nc - 1);
+    float2 x = make_float2(0.f, 0.f), y = make_float2(0.f, 0.f);
+    if (q < L) x = V[rows(q, c)];
+    if (q == 0) {
+      x.y = 0.f;
+    } else if (h - q < L) {
+      float2 v = V[rows(h - q, c)];
+      y = make_float2(v.x, -v.y);
+    }
+    float2 w = __ldg(a.tw + q * tws);
+    float2 dd = make_float2(x.x - y.x, x.y - y.y);
+    float2 z = make_float2(x.x + y.x - (w.x * dd.y + w.y * dd.x), x.y + y.y + (w.x * dd.x - w.y * dd.y));
+    Z[cols(c, bitrev(q, lgh))] = z;
+  }
+  __syncthreads();
+  fft_lines_smem_lf(Z, nc, lgh, a.tw, cols);
+
+  if (VOLUME) {
+    float* out = a.vol + (size_t)slab * nc * n;
+    for (int e = threadIdx.x; e < nc * h; e += blockDim.x) {
+      int c = e / h, p = e - c * h;
+      float2 z = Z[cols(c, p)];
+      out[c * n + 2 * p] = z.x;
+      out[c * n + 2 * p + 1] = z.y;
+    }
+    return;
+  }
+  // the best of the slab: value × rden, first index of equal values
+  const float* rd = a.rden + ((size_t)(b / a.rden_div) * nb + j) * nc * n;
+  float bv = -3.4e38f;
+  uint32_t bi = 0xffffffffu;
+  for (int e = threadIdx.x; e < nc * h; e += blockDim.x) {
+    int c = e / h, p = e - c * h;
+    float2 z = Z[cols(c, p)];
+    const float* r = rd + (size_t)c * n + 2 * p;
+    float ev = z.x * __ldg(r), od = z.y * __ldg(r + 1);
+    uint32_t ie = ((uint32_t)(j * nc + c)) * n + 2 * p;
+    if (ev > bv || (ev == bv && ie < bi)) { bv = ev; bi = ie; }
+    if (od > bv || (od == bv && ie + 1 < bi)) { bv = od; bi = ie + 1; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { redv[wid] = bv; redi[wid] = bi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      if (redv[w] > bv || (redv[w] == bv && redi[w] < bi)) { bv = redv[w]; bi = redi[w]; }
+    }
+    a.cand[slab] = make_float2(bv, __uint_as_float(bi));
+  }
+}
+
+// V[j; m', c] of item b straight from U along c (so3.wgsl:667-674)
+__device__ __forceinline__ float2 v_at(const float2* __restrict__ U, const float2* __restrict__ tw, int b, int j,
+                                       int mp, int c, const zeb_so3_dims_t& d) {
+  const float2* row = U + (((size_t)b * d.nb + j) * d.L + mp) * d.nc;
+  const int ts = ZEB_TW_LEN / d.nc;
+  float2 acc = make_float2(0.f, 0.f);
+  for (int x = 0; x < d.nc; ++x) {
+    float2 v = __ldg(row + x);
+    float2 w = __ldg(tw + ((x * c) & (d.nc - 1)) * ts);
+    acc.x += v.x * w.x - v.y * w.y;
+    acc.y += v.x * w.y + v.y * w.x;
+  }
+  return acc;
+}
+
+// Re(V e^{−i m a}) at grid point ia (so3.wgsl:766-769)
+__device__ __forceinline__ float a_term(float2 v, int m, int ia, int n) {
+  float ang = ZEB_TAU * (float)((m * ia) & (n - 1)) / (float)n;
+  float sa, ca;
+  sincosf(ang, &sa, &ca);
+  return v.x * ca + v.y * sa;
+}
+
+__device__ __forceinline__ float vertex(float lo, float mid, float hi) {
+  float den = lo - 2.f * mid + hi;
+  if (den >= -1e-12f) return 0.f;
+  return fminf(fmaxf(0.5f * (lo - hi) / den, -0.5f), 0.5f);
+}
+
+__global__ void __launch_bounds__(64) k_peak_finish(SlabArgs a, float* __restrict__ peaks) {
+  __shared__ float pf[6][64];
+  __shared__ float2 best;
+  const zeb_so3_dims_t& d = a.d;
+  const int b = blockIdx.x;
+  const int n = d.n, nc = d.nc, nb = d.nb, L = d.L;
+  if (threadIdx.x < 32) {
+    float bv = -3.4e38f;
+    uint32_t bi = 0xffffffffu;
+    for (int j = threadIdx.x; j < nb; j += 32) {
+      float2 c = a.cand[(size_t)b * nb + j];
+      uint32_t ci = __float_as_uint(c.y);
+      if (c.x > bv || (c.x == bv && ci < bi)) { bv = c.x; bi = ci; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if (threadIdx.x == 0) best = make_float2(bv, __uint_as_float(bi));
+  }
+  __syncthreads();
+  const float v0 = best.x;
+  uint32_t idx = __float_as_uint(best.y);
+  if (idx == 0xffffffffu) idx = 0;
+  const int ia = idx & (n - 1);
+  const int iq = (idx / n) & (nc - 1);
+  const int j = idx / (n * nc);
+  const bool inner = j > 0 && j < n / 2;
+  const int iqm = (iq + nc - 1) & (nc - 1), iqp = (iq + 1) & (nc - 1);
+  const int iam = (ia + n - 1) & (n - 1), iap = (ia + 1) & (n - 1);
+  float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int m = threadIdx.x; m < L; m += 64) {
+    float f = m == 0 ? 1.f : 2.f;
+    float2 vc = v_at(a.U, a.tw, b, j, m, iq, d);
+    float2 vm = v_at(a.U, a.tw, b, j, m, iqm, d);
+    float2 vp = v_at(a.U, a.tw, b, j, m, iqp, d);
+    s[0] += f * a_term(vc, m, iam, n);
+    s[1] += f * a_term(vc, m, iap, n);
+    s[2] += f * a_term(vm, m, ia, n);
+    s[3] += f * a_term(vp, m, ia, n);
+    if (inner) {
+      s[4] += f * a_term(v_at(a.U, a.tw, b, j - 1, m, iq, d), m, ia, n);
+      s[5] += f * a_term(v_at(a.U, a.tw, b, j + 1, m, iq, d), m, ia, n);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) pf[k][threadIdx.x] = s[k];
+  __syncthreads();
+  for (int off = 32; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off)
+#pragma unroll
+      for (int k = 0; k < 6; ++k) pf[k][threadIdx.x] += pf[k][threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const float* rd = a.rden + (size_t)(b / a.rden_div) * nb * nc * n;
+  auto rat = [&](int jj, int qq, int aa) { return __ldg(rd + ((size_t)jj * nc + qq) * n + aa); };
+  float da = vertex(pf[0][0] * rat(j, iq, iam), v0, pf[1][0] * rat(j, iq, iap));
+  float dc = vertex(pf[2][0] * rat(j, iqm, ia), v0, pf[3][0] * rat(j, iqp, ia));
+  float dj = 0.f;
+  if (inner) dj = vertex(pf[4][0] * rat(j - 1, iq, ia), v0, pf[5][0] * rat(j + 1, iq, ia));
+  // S = Rz(a) Ry(b) Rz(c); the orientation is its inverse, w ≥ 0 (so3.wgsl:776-796)
+  const float step = ZEB_TAU / (float)n;
+  float aa = ((float)ia + da) * step, bb = ((float)j + dj) * step, cc = ((float)iq + dc) * step;
+  float4 qa = make_float4(cosf(0.5f * aa), 0.f, 0.f, sinf(0.5f * aa));
+  float4 qb = make_float4(cosf(0.5f * bb), 0.f, sinf(0.5f * bb), 0.f);
+  float4 qc = make_float4(cosf(0.5f * cc), 0.f, 0.f, sinf(0.5f * cc));
+  float4 q = qmul(qa, qmul(qb, qc));
+  q = make_float4(q.x, -q.y, -q.z, -q.w);
+  if (q.x < 0.f) q = make_float4(-q.x, -q.y, -q.z, -q.w);
+  float* o = peaks + (size_t)b * 8;
+  o[0] = q.x; o[1] = q.y; o[2] = q.z; o[3] = q.w;
+  o[4] = v0; o[5] = aa; o[6] = bb; o[7] = cc;
+}
+
+__global__ void k_rden_build(const float* __restrict__ vf, const float* __restrict__ vf2, const float* __restrict__ stats,
+                             long long per_item, long long total, float* __restrict__ rden) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  float ar = fmaxf(stats[(t / per_item) * 4], 1e-12f);
+  float m = vf[t];
+  float v = vf2[t] - m * m / ar;
+  rden[t] = v > 1e-6f * ar ? rsqrtf(v) : 0.f;
+}
+
+static int ilog2i(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+
+static bool dims_ok(const zeb_so3_dims_t* d) {
+  return d && d->L >= 2 && d->L <= 256 && d->n >= 2 * d->L - 1 && (d->n & (d->n - 1)) == 0 && d->nb == d->n / 2 + 1 &&
+         d->fold >= 1 && d->nc == d->n / d->fold && (d->nc & (d->nc - 1)) == 0 && d->L <= d->n / 2 &&
+         d->n <= ZEB_TW_LEN;
+}
+
+static size_t slab_smem(const zeb_so3_dims_t* d) {
+  return ((size_t)d->L * d->nc + (size_t)(d->n / 2) * d->nc) * sizeof(float2);
+}
+
+}  // namespace zeb
+
+using namespace zeb;
+
+extern "C" size_t zeb_peaks_scratch_bytes(const zeb_so3_dims_t* d, int n_items) {
+  if (!dims_ok(d) || n_items <= 0) return 0;
+  return (size_t)n_items * d->nb * sizeof(float2);
+}
+
+static int slab_launch(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw, SlabArgs& a, bool vol,
+                       cudaStream_t st) {
+  a.U = (const float2*)U;
+  a.n_items = n_items;
+  a.d = *d;
+  a.lgc = ilog2i(d->nc);
+  a.lgh = ilog2i(d->n / 2);
+  a.tw = (const float2*)tw;
+  size_t smem = slab_smem(d);
+  ZEB_REQUIRE(smem <= 220 * 1024, ZEB_ESIZE, "correlate: slab of L=%d, nc=%d needs %zu bytes of shared memory", d->L,
+              d->nc, smem);
+  long long blocks = (long long)n_items * d->nb;
+  ZEB_REQUIRE(blocks < (1LL << 31), ZEB_ESIZE, "correlate: too many slabs");
+  if (vol) {
+    cudaFuncSetAttribute(k_slab<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_slab<true><<<(unsigned)blocks, 256, smem, st>>>(a);
+  } else {
+    cudaFuncSetAttribute(k_slab<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_slab<false><<<(unsigned)blocks, 256, smem, st>>>(a);
+  }
+  return zeb_launch_check("correlate slab");
+}
+
+extern "C" int zeb_correlate_peaks(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw,
+                                   const float* rden, int rden_div, float* peaks, void* scratch, void* stream) {
+  ZEB_REQUIRE(U && tw && rden && peaks && scratch, ZEB_EARG, "correlate_peaks: null argument");
+  ZEB_REQUIRE(dims_ok(d), ZEB_EARG, "correlate_peaks: inconsistent dims");
+  ZEB_REQUIRE(rden_div >= 1, ZEB_EARG, "correlate_peaks: rden_div=%d", rden_div);
+  if (n_items <= 0) return ZEB_OK;
+  SlabArgs a{};
+  a.rden = rden;
+  a.rden_div = rden_div;
+  a.cand = (float2*)scratch;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = slab_launch(U, n_items, d, tw, a, false, st);
+  if (rc) return rc;
+  k_peak_finish<<<n_items, 64, 0, st>>>(a, peaks);
+  return zeb_launch_check("peak_finish");
+}
+
+extern "C" int zeb_correlate_volume(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw, float* vol,
+                                    void* stream) {
+  ZEB_REQUIRE(U && tw && vol, ZEB_EARG, "correlate_volume: null argument");
+  ZEB_REQUIRE(dims_ok(d), ZEB_EARG, "correlate_volume: inconsistent dims");
+  if (n_items <= 0) return ZEB_OK;
+  SlabArgs a{};
+  a.vol = vol;
+  return slab_launch(U, n_items, d, tw, a, true, (cudaStream_t)stream);
+}
+
+extern "C" int zeb_rden_build(const float* vol_f, const float* vol_f2, const float* stats, int n, long long cells,
+                              float* rden, void* stream) {
+  ZEB_REQUIRE(vol_f && vol_f2 && stats && rden && n >= 0 && cells > 0, ZEB_EARG, "rden_build: bad arguments");
+  long long total = (long long)n * cells;
+  if (total == 0) return ZEB_OK;
+  k_rden_build<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(vol_f, vol_f2, stats, cells, total,
+                                                                                  rden);
+  return zeb_launch_check("rden_build");
+}

@@ -1,0 +1,269 @@
+// (a) Patterns onto the sphere and into spherical harmonics.
+//
+// k_sphere_rings: one thread block per item. The pattern sits in shared memory; every Gauss–
+// Legendre direction's ray is intersected with the detector plane and the pattern sampled
+// bilinearly there (zero off the detector and outside the mask).  A first pass takes the
+// window's quadrature-weighted sums (its area and mean); the second takes each northern ring
+// with its mirror as one complex line (ring real, mirror imaginary), window-mean centred,
+// transforms it along φ in shared memory and keeps of the two spectra their orders m < L as
+// sum and difference (sphere.wgsl:128-269).
+// k_legendre: contracts the ring spectra with the weighted Legendre table, a block per
+// (order m, tile of items) with the table's rows for m staged in shared memory (sphere.wgsl:
+// 271-288). k_sh_norm: unit harmonic norm and the item's stats (sphere.wgsl:290-324).
+#include "abi_util.cuh"
+
+namespace zeb {
+
+struct SphereArgs {
+  const float* pats;
+  const float4* items;
+  int n_items, h, w;
+  float c0[3], c1[3], c2[3], mask[3];
+  int L, n_theta, n_phi, lg_phi, n_pairs;
+  const float4* ring;
+  const float2* phi_cs;
+  const float* wplm;
+  const float2* tw;
+  unsigned flags;
+  float4* spectra;  // [item][n_theta/2][L]
+  float2* alm;      // [item][n_pairs]
+  float* stats;     // [item][4]
+  int lines_per_chunk;
+  int pat_in_smem;
+};
+
+struct Sampler {
+  const float* pat;
+  int h, w;
+  float3 c0, c1, c2, t;
+  float c2t;
+  float mask[3];
+  bool window;
+
+  // (pattern value, window weight) of direction d (sphere.wgsl:128-163)
+  __device__ __forceinline__ float2 sample(float3 d) const {
+    float nd = dot3(c2, d);
+    float val = 0.f, wv = 0.f;
+    if (nd > 1e-4f) {
+      float s = c2t / nd;
+      float3 hh = make_float3(s * d.x - t.x, s * d.y - t.y, s * d.z - t.z);
+      float row = dot3(c0, hh), col = dot3(c1, hh);
+      float hmax = (float)(h - 1), wmax = (float)(w - 1);
+      float dr = row - mask[0], dc = col - mask[1];
+      if (row >= 0.f && row <= hmax && col >= 0.f && col <= wmax && (mask[2] <= 0.f || dr * dr + dc * dc <= mask[2])) {
+        wv = 1.f;
+        val = 1.f;
+        if (!window) {
+          int r0 = min((int)row, h - 2), q0 = min((int)col, w - 2);
+          float fr = row - (float)r0, fc = col - (float)q0;
+          const float* p = pat + r0 * w + q0;
+          float top = lerpf(p[0], p[1], fc), bot = lerpf(p[w], p[w + 1], fc);
+          val = lerpf(top, bot, fr);
+        }
+      }
+    }
+    return make_float2(val, wv);
+  }
+};
+
+__global__ void __launch_bounds__(256) k_sphere_rings(SphereArgs a) {
+  extern __shared__ float4 smem4[];
+  __shared__ float red[2 * 8];
+  const int b = blockIdx.x;
+  const int hw = a.h * a.w;
+  float2* lines = (float2*)smem4;
+  float* spat = (float*)(lines + (size_t)a.lines_per_chunk * a.n_phi);
+  const float4 it = a.items[b];
+  const bool window = (a.flags & ZEB_FLAG_WINDOW) != 0;
+  Sampler s;
+  s.pat = nullptr;
+  if (!window) {
+    const float* src = a.pats + (size_t)(int)it.w * hw;
+    if (a.pat_in_smem) {
+      for (int i = threadIdx.x; i < hw; i += blockDim.x) spat[i] = src[i];
+      s.pat = spat;
+    } else {
+      s.pat = src;
+    }
+  }
+  s.h = a.h; s.w = a.w;
+  s.c0 = make_float3(a.c0[0], a.c0[1], a.c0[2]);
+  s.c1 = make_float3(a.c1[0], a.c1[1], a.c1[2]);
+  s.c2 = make_float3(a.c2[0], a.c2[1], a.c2[2]);
+  s.t = make_float3(it.x, it.y, it.z);
+  s.c2t = dot3(s.c2, s.t);
+  s.mask[0] = a.mask[0]; s.mask[1] = a.mask[1]; s.mask[2] = a.mask[2];
+  s.window = window;
+  __syncthreads();
+
+  // the window's sums over the whole grid
+  const int nphi = a.n_phi, nt = a.n_theta, lg = a.lg_phi;
+  float acc[2] = {0.f, 0.f};
+  for (int e = threadIdx.x; e < nt * nphi; e += blockDim.x) {
+    int y = e >> lg, j = e & (nphi - 1);
+    float4 rg = __ldg(a.ring + y);
+    float2 cs = __ldg(a.phi_cs + j);
+    float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
+    acc[0] += g.x * g.y * rg.z;
+    acc[1] += g.y * rg.z;
+  }
+  block_sums<2>(acc, red);
+  const float mean = (a.flags & ZEB_FLAG_CENTER) ? acc[0] / fmaxf(acc[1], 1e-20f) : 0.f;
+  if (threadIdx.x == 0) {
+    a.stats[b * 4 + 0] = acc[1] * ZEB_TAU / (float)nphi;
+    a.stats[b * 4 + 1] = mean;
+  }
+
+  // ring pairs, a chunk of lines at a time
+  const int nh = nt / 2, L = a.L;
+  const int CH = a.lines_per_chunk;
+  RowLines idx{lg};
+  for (int y0 = 0; y0 < nh; y0 += CH) {
+    const int cnt = min(CH, nh - y0);
+    for (int e = threadIdx.x; e < cnt * nphi; e += blockDim.x) {
+      int i = e >> lg, j = e & (nphi - 1);
+      int y = y0 + i;
+      float4 rn = __ldg(a.ring + y), rs = __ldg(a.ring + (nt - 1 - y));
+      float2 cs = __ldg(a.phi_cs + j);
+      float2 gn = s.sample(make_float3(rn.y * cs.x, rn.y * cs.y, rn.x));
+      float2 gs = s.sample(make_float3(rs.y * cs.x, rs.y * cs.y, rs.x));
+      lines[idx(i, bitrev(j, lg))] = make_float2((gn.x - mean) * gn.y, (gs.x - mean) * gs.y);
+    }
+    __syncthreads();
+    fft_lines_smem(lines, cnt, lg, a.tw, idx);
+    // the two apart: Z = N + iS for real N, S gives N_m = (Z_m + conj Z_{n−m})/2 and
+    // S_m = (Z_m − conj Z_{n−m})/2i; keep (N+S, N−S) for m < L
+    float4* out = a.spectra + ((size_t)b * nh + y0) * L;
+    for (int e = threadIdx.x; e < cnt * L; e += blockDim.x) {
+      int i = e / L, m = e - i * L;
+      float2 z = lines[idx(i, m)];
+      float2 zr = lines[idx(i, (nphi - m) & (nphi - 1))];
+      float2 rn = make_float2(0.5f * (z.x + zr.x), 0.5f * (z.y - zr.y));
+      float2 dd = make_float2(z.x - zr.x, z.y + zr.y);
+      float2 rs = make_float2(0.5f * dd.y, -0.5f * dd.x);
+      out[e] = make_float4(rn.x + rs.x, rn.y + rs.y, rn.x - rs.x, rn.y - rs.y);
+    }
+    __syncthreads();
+  }
+}
+
+// a_lm = Σ_y wplm[y, pair] · (N+S or N−S by the parity of l+m): block (m, tile of 16 items).
+#define LEG_ITEMS 16
+__global__ void __launch_bounds__(256) k_legendre(SphereArgs a) {
+  extern __shared__ float4 smem4[];
+  const int m = blockIdx.x;
+  const int b0 = blockIdx.y * LEG_ITEMS;
+  const int L = a.L, nh = a.n_theta / 2, np = a.n_pairs;
+  const int nl = L - m;
+  const int p0 = m * L - (m * (m - 1)) / 2;
+  float4* spec = smem4;                        // [LEG_ITEMS][nh]
+  float* wp = (float*)(spec + LEG_ITEMS * nh);  // [nh][nl]
+  const int nb = min(LEG_ITEMS, a.n_items - b0);
+  for (int e = threadIdx.x; e < nb * nh; e += blockDim.x) {
+    int i = e / nh, y = e - i * nh;
+    spec[e] = a.spectra[((size_t)(b0 + i) * nh + y) * L + m];
+  }
+  for (int e = threadIdx.x; e < nh * nl; e += blockDim.x) {
+    int y = e / nl, l = e - y * nl;
+    wp[e] = __ldg(a.wplm + (size_t)y * np + p0 + l);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nb * nl; e += blockDim.x) {
+    int i = e / nl, li = e - i * nl;
+    bool odd = ((li + 2 * m) & 1) != 0;  // l + m = li + 2m
+    float re = 0.f, im = 0.f;
+    for (int y = 0; y < nh; ++y) {
+      float4 r = spec[i * nh + y];
+      float k = wp[y * nl + li];
+      re += k * (odd ? r.z : r.x);
+      im += k * (odd ? r.w : r.y);
+    }
+    a.alm[(size_t)(b0 + i) * np + p0 + li] = make_float2(re, im);
+  }
+}
+
+// unit harmonic norm (Σ over signed orders: m > 0 twice) and the stats
+__global__ void __launch_bounds__(256) k_sh_norm(SphereArgs a) {
+  __shared__ float red[8];
+  const int b = blockIdx.x;
+  const int L = a.L, np = a.n_pairs;
+  float2* al = a.alm + (size_t)b * np;
+  float e[1] = {0.f};
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    float2 v = al[p];
+    float k = p < L ? 1.f : 2.f;  // pairs 0 … L−1 are m = 0
+    e[0] += k * (v.x * v.x + v.y * v.y);
+  }
+  block_sums<1>(e, red);
+  const float nrm = sqrtf(fmaxf(e[0], 1e-30f));
+  if (a.flags & ZEB_FLAG_NORM) {
+    const float inv = 1.f / nrm;
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+      float2 v = al[p];
+      al[p] = make_float2(v.x * inv, v.y * inv);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a.stats[b * 4 + 2] = nrm;
+    a.stats[b * 4 + 3] = al[0].x;
+  }
+}
+
+static int ilog2(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+
+}  // namespace zeb
+
+using namespace zeb;
+
+extern "C" size_t zeb_sphere_scratch_bytes(const zeb_sphere_tables_t* tb, int n_items) {
+  if (!tb || n_items <= 0) return 0;
+  return (size_t)n_items * (tb->n_theta / 2) * tb->L * sizeof(float4);
+}
+
+extern "C" int zeb_sphere_coefficients(const float* pats, const float* items, int n_items, const zeb_frame_t* fr,
+                                       const zeb_sphere_tables_t* tb, unsigned flags, float* alm, float* stats,
+                                       void* scratch, void* stream) {
+  ZEB_REQUIRE(items && fr && tb && alm && stats && scratch, ZEB_EARG, "sphere_coefficients: null argument");
+  ZEB_REQUIRE((flags & ZEB_FLAG_WINDOW) || pats, ZEB_EARG, "sphere_coefficients: patterns missing");
+  ZEB_REQUIRE(tb->ring && tb->phi_cs && tb->wplm && tb->tw, ZEB_EARG, "sphere_coefficients: table missing");
+  const int L = tb->L, nphi = tb->n_phi, nt = tb->n_theta;
+  ZEB_REQUIRE(L >= 2 && L <= 256 && nt >= 2 * L - 1 && (nphi & (nphi - 1)) == 0 && nphi >= 32 && nphi <= ZEB_TW_LEN &&
+                  nt % 2 == 0 && tb->n_pairs == L * (L + 1) / 2 && fr->h >= 2 && fr->w >= 2 && L <= nphi / 2,
+              ZEB_EARG, "sphere_coefficients: bad tables L=%d nt=%d nphi=%d", L, nt, nphi);
+  if (n_items == 0) return ZEB_OK;
+  SphereArgs a{};
+  a.pats = pats; a.items = (const float4*)items; a.n_items = n_items; a.h = fr->h; a.w = fr->w;
+  for (int k = 0; k < 3; ++k) {
+    a.c0[k] = fr->c0[k]; a.c1[k] = fr->c1[k]; a.c2[k] = fr->c2[k]; a.mask[k] = fr->mask[k];
+  }
+  a.L = L; a.n_theta = nt; a.n_phi = nphi; a.lg_phi = ilog2(nphi); a.n_pairs = tb->n_pairs;
+  a.ring = (const float4*)tb->ring; a.phi_cs = (const float2*)tb->phi_cs; a.wplm = tb->wplm;
+  a.tw = (const float2*)tb->tw; a.flags = flags;
+  a.spectra = (float4*)scratch; a.alm = (float2*)alm; a.stats = stats;
+  // a chunk of lines of 32 KB, whole lines
+  a.lines_per_chunk = max(1, min(nt / 2, 4096 / nphi));
+  size_t hw = (size_t)fr->h * fr->w;
+  size_t lines_bytes = (size_t)a.lines_per_chunk * nphi * sizeof(float2);
+  a.pat_in_smem = (!(flags & ZEB_FLAG_WINDOW) && hw * 4 + lines_bytes <= 200 * 1024) ? 1 : 0;
+  size_t smem = lines_bytes + (a.pat_in_smem ? hw * 4 : 0);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaFuncSetAttribute(k_sphere_rings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_sphere_rings<<<n_items, 256, smem, st>>>(a);
+  int rc = zeb_launch_check("sphere_rings");
+  if (rc) return rc;
+  const int nh = nt / 2;
+  size_t lsm = (size_t)LEG_ITEMS * nh * sizeof(float4) + (size_t)nh * L * sizeof(float);
+  ZEB_REQUIRE(lsm <= 220 * 1024, ZEB_ESIZE, "sphere_coefficients: L=%d needs %zu bytes of shared memory", L, lsm);
+  cudaFuncSetAttribute(k_legendre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm);
+  dim3 g(L, (n_items + LEG_ITEMS - 1) / LEG_ITEMS);
+  k_legendre<<<g, 256, lsm, st>>>(a);
+  rc = zeb_launch_check("legendre");
+  if (rc) return rc;
+  k_sh_norm<<<n_items, 256, 0, st>>>(a);
+  return zeb_launch_check("sh_norm");
+}

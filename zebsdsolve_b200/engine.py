@@ -1,0 +1,568 @@
+"""The indexing engine: the reference's Engine (zebsdsolve src/engine.zig) for the spherical path,
+driving the C-ABI kernels on one GPU.
+
+State: the settings, the detector geometry, the scan (patterns on the host), the candidate phases
+(masters, baked per pattern resolution on the device), the per-bandwidth tables, the chance
+calibration and the per-cell results.  Indexing goes in batches of cells, each batch one pass of
+the device path: upload → preprocess → sphere → spectrum → peaks → refine → NMI → records, one
+readback (engine.zig:2005-2137).
+"""
+import ctypes
+import json
+import math
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import master as M
+from . import rotations as R
+from .device import BandTables, PhaseBand, master_blur, ptr, stream_ptr
+from .settings import Settings
+
+FLAG_CENTER, FLAG_NORM, FLAG_WINDOW = 1, 2, 4
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+class Geometry:
+    """geometry.zig:113-193 — one detector pose and per-cell beam offsets."""
+
+    FIELDS = ("pc", "sample_tilt_deg", "detector_tilt_deg", "rot", "px_um", "step_x_um", "step_y_um")
+
+    def __init__(self):
+        self.pc = np.array([0.5, 0.5, 0.5])
+        self.sample_tilt_deg = 70.0
+        self.detector_tilt_deg = 0.0
+        self.rot = np.zeros(3)
+        self.px_um = 0.0
+        self.step_x_um = 1.0
+        self.step_y_um = 1.0
+
+    def as_dict(self):
+        return {"pc": list(map(float, self.pc)), "sample_tilt_deg": self.sample_tilt_deg,
+                "detector_tilt_deg": self.detector_tilt_deg, "rot": list(map(float, self.rot)), "px_um": self.px_um,
+                "step_x_um": self.step_x_um, "step_y_um": self.step_y_um, "plane_kind": "none",
+                "plane": [[0.0, 0.0, 0.0]] * 3 + [[0.0, 0.0, 1.0]]}
+
+    def set(self, **kw):
+        for k, v in kw.items():
+            if k in ("pc", "rot"):
+                a = np.asarray(v, np.float64).reshape(3)
+                setattr(self, k, a)
+            elif k in self.FIELDS:
+                setattr(self, k, float(v))
+            elif k in ("plane_kind", "plane"):
+                continue
+            else:
+                raise EngineError(f"geometry has no field {k!r}")
+
+    def key(self):
+        return (tuple(self.pc), self.sample_tilt_deg, self.detector_tilt_deg, tuple(self.rot), self.px_um,
+                self.step_x_um, self.step_y_um)
+
+    def rotation(self):
+        """geometry.zig:141-150 — R0(sample tilt, detector tilt) · Exp(rot)."""
+        a = math.radians(self.detector_tilt_deg - self.sample_tilt_deg)
+        s, c = math.sin(a), math.cos(a)
+        r0 = np.array([[-s, 0, c], [0, 1, 0], [-c, 0, -s]])
+        return r0 @ R.to_matrix(R.exp_map(self.rot))
+
+    def translation(self, rows, cols, pc=None):
+        """geometry.zig:153-161 — t in pixels for a pattern of rows × cols."""
+        pc = self.pc if pc is None else pc
+        return self.rotation() @ np.array([0.5 - pc[1] * rows, 0.5 - pc[0] * cols, pc[2] * rows])
+
+    def scan_offsets(self, row, col, ref_row, ref_col, x_sign, y_sign, binning):
+        """geometry.zig:184-192 — beam travel of cells from the reference cell, in pixels."""
+        row = np.asarray(row, np.float64)
+        col = np.asarray(col, np.float64)
+        if not self.px_um > 0:
+            return np.zeros(row.shape + (3,))
+        k = 1.0 / (self.px_um * binning)
+        return np.stack([y_sign * (row - ref_row) * self.step_y_um * k, x_sign * (col - ref_col) * self.step_x_um * k,
+                         np.zeros_like(row)], -1)
+
+
+class Phase:
+    def __init__(self, master):
+        self.master = master
+        self.baked = None  # (key, sheets f32 device, grad4 device, host sheets)
+
+    def info(self, bands):
+        m = self.master
+        out = {"name": m.name, "side": m.side, "point_group": m.point_group, "space_group": m.space_group,
+               "laue": R.LAUE_NAMES[m.laue], "rotations": len(m.rotations()), "voltage_kv": m.voltage_kv,
+               "n_fold": 0, "mirror": False, "inversion": False}
+        return out
+
+
+class Engine:
+    def __init__(self, device=None):
+        if not torch.cuda.is_available():
+            raise EngineError("no CUDA device: this engine runs only on the GPU")
+        N.load()
+        self.dev = torch.device(device or "cuda")
+        self.set = Settings()
+        self.geo = Geometry()
+        self.patterns = None  # host array [rows, cols, h, w]
+        self.pixel = None
+        self.phases = []
+        self.bands = {}
+        self.avg = None
+        self.chance_key = None
+        self.chance_med = []
+        self.chance_spread = []
+        self.batch_stamp = 0
+        self.events = []
+        self.cancel = False
+        self.res = None
+        self.index_cells_list = None
+        self.index_done = 0
+        self.index_sweep = 0
+        self.index_accepted = 0
+        self.index_region = 0
+        self._buf = {}
+        self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
+
+    # ── plumbing ──
+
+    def log(self, text):
+        self.events.append({"kind": "log", "text": text})
+
+    def buf(self, name, numel, dtype=torch.float32):
+        t = self._buf.get(name)
+        if t is None or t.numel() < numel or t.dtype != dtype:
+            t = torch.empty(max(int(numel), 1), dtype=dtype, device=self.dev)
+            self._buf[name] = t
+        return t
+
+    # ── scan ──
+
+    def set_patterns(self, a):
+        a = np.asarray(a)
+        if a.ndim == 3:
+            a = a[None]
+        if a.ndim != 4:
+            raise EngineError("patterns must be (rows, cols, h, w) or (n, h, w)")
+        if a.dtype == np.uint8:
+            self.pixel = 0
+        elif a.dtype == np.uint16:
+            self.pixel = 1
+        else:
+            a = a.astype(np.float32)
+            self.pixel = 2
+        if a.shape[2] < 4 or a.shape[3] < 4:
+            raise EngineError("PatternTooSmall")
+        self.patterns = np.ascontiguousarray(a)
+        rows, cols = a.shape[:2]
+        self.avg = None
+        self.chance_key = None
+        self.res = {"quat": np.zeros((rows * cols, 4), np.float32), "ncc": np.zeros(rows * cols, np.float32),
+                    "nmi": np.zeros(rows * cols, np.float32), "phase": np.full(rows * cols, -1, np.int32),
+                    "z": np.zeros(rows * cols, np.float32), "sweep": np.full(rows * cols, -1, np.int32),
+                    "settled": np.zeros(rows * cols, bool)}
+        self.res["quat"][:, 0] = 1
+
+    def info(self):
+        if self.patterns is None:
+            raise EngineError("NoScan")
+        rows, cols, h, w = self.patterns.shape
+        return rows, cols, h, w
+
+    def pattern_shape(self):
+        """engine.zig:1011-1017 — the reduced size floor(size / binning) (no other level here)."""
+        rows, cols, h, w = self.info()
+        b = self.set["binning"]
+        return int(math.floor(h / b)), int(math.floor(w / b))
+
+    def mask_of(self, h, w):
+        """engine.zig:1444-1448"""
+        if not self.set["mask"]:
+            return (0.0, 0.0, 0.0)
+        r = self.set["mask_radius"] * 0.5 * min(h, w)
+        return (0.5 * (h - 1), 0.5 * (w - 1), r * r)
+
+    def frame(self):
+        """engine.zig:1567-1578"""
+        h, w = self.pattern_shape()
+        Rm = self.geo.rotation()
+        fr = N.Frame()
+        fr.h, fr.w = h, w
+        for k in range(3):
+            fr.c0[k], fr.c1[k], fr.c2[k] = Rm[k, 0], Rm[k, 1], Rm[k, 2]
+        fr.mask[0], fr.mask[1], fr.mask[2] = self.mask_of(h, w)
+        return fr
+
+    def positions(self, cells):
+        """engine.zig:1601-1613 — the detector position for each cell, in pixels (float32)."""
+        rows, cols, h, w = self.info()
+        b = self.set["binning"]
+        cells = np.asarray(cells, np.int64)
+        t = self.geo.translation(h / b, w / b)
+        off = self.geo.scan_offsets(cells // cols, cells % cols, 0.5 * (rows - 1), 0.5 * (cols - 1),
+                                    self.set["scan_x_sign"], self.set["scan_y_sign"], b)
+        return (t[None, :] - off).astype(np.float32)
+
+    def lattice(self, want):
+        """engine.zig:1325-1341 — about `want` cells on a lattice over the map."""
+        rows, cols = self.info()[:2]
+        gy, gx = rows, cols
+        if rows * cols > want:
+            ratio = rows / cols
+            gy = int(min(max(round(math.sqrt(want * ratio)), 1), rows))
+            gx = int(min(max(want // gy, 1), cols))
+        r = (2 * np.arange(gy) + 1) * rows // (2 * gy)
+        c = (2 * np.arange(gx) + 1) * cols // (2 * gx)
+        return (r[:, None] * cols + c[None, :]).reshape(-1).astype(np.int64)
+
+    def region_cells(self):
+        """engine.zig:2312-2330"""
+        rows, cols = self.info()[:2]
+        s = self.set
+        x0, y0, w, h = 0, 0, cols, rows
+        if s["roi_w"] and s["roi_h"]:
+            x0 = min(s["roi_x"], cols - 1)
+            y0 = min(s["roi_y"], rows - 1)
+            w = min(s["roi_w"], cols - x0)
+            h = min(s["roi_h"], rows - y0)
+        return ((y0 + np.arange(h))[:, None] * cols + x0 + np.arange(w)[None, :]).reshape(-1).astype(np.int64)
+
+    def static_background(self):
+        """engine.zig:1344-1424 — the average of `static_patterns` lattice patterns (none/file)."""
+        if self.set["static_background"] != "average":
+            return None
+        if self.avg is None or self.avg[0] != self.set["static_patterns"]:
+            cells = self.lattice(self.set["static_patterns"])
+            rows, cols, h, w = self.info()
+            flat = self.patterns.reshape(rows * cols, h, w)
+            acc = np.zeros((h, w))
+            for i in range(0, len(cells), 1024):
+                acc += flat[cells[i:i + 1024]].astype(np.float64).sum(0)
+            avg = (acc / len(cells)).astype(np.float32)
+            self.avg = (self.set["static_patterns"], torch.as_tensor(avg, device=self.dev))
+            self.log(f"static background: the average of {len(cells)} patterns over the map")
+        return self.avg[1]
+
+    # ── phases ──
+
+    def add_phase(self, path):
+        return self.add_master(M.load_npz(path))
+
+    def add_master(self, m):
+        self.phases.append(Phase(m))
+        self.chance_key = None
+        self.log(f"phase {len(self.phases) - 1}: {m.name} ({m.side} px), orientations reduced by {len(m.rotations())} rotations")
+        return len(self.phases) - 1
+
+    def clear_phases(self):
+        self.phases = []
+        self.bands = {}
+        self.chance_key = None
+
+    def pixel_angle(self):
+        """engine.zig:1028-1035 — angular width of one reduced pixel, radians."""
+        rows, cols, h, w = self.info()
+        stored = math.radians(self.set["pixel_angle_deg"]) if self.set["pixel_angle_deg"] > 0 else 1.0 / max(self.geo.pc[2] * h, 1e-9)
+        return stored * self.set["binning"]
+
+    def prepare_masters(self):
+        """engine.zig:1676-1788 — each phase's master smoothed on the sphere by master_smooth
+        pattern pixels (quantized in steps of 5 % of the sheet pixels a detector pixel spans),
+        renormalized, and its gradient table."""
+        if not self.phases:
+            raise EngineError("NoPhases")
+        angle = self.pixel_angle()
+        for p in self.phases:
+            m = p.master
+            px = angle * m.side / math.sqrt(2 * math.pi)
+            q = int(round(math.log(px) / math.log(1.05))) if px > 0 else None
+            key = (q, self.set["master_smooth"])
+            if p.baked is not None and p.baked[0] == key:
+                continue
+            sheets = torch.as_tensor(m.raw, device=self.dev)
+            smooth = self.set["master_smooth"] * (1.05 ** q) if q is not None else 0.0
+            if smooth > 0.05:
+                sheets = master_blur(sheets, m.side, smooth)
+                host = sheets.double()
+                mean = host.mean()
+                sd = torch.sqrt(((host - mean) ** 2).mean())
+                sheets = ((host - mean) / torch.clamp(sd, min=1e-30)).float().contiguous()
+            grad = torch.empty(sheets.numel() * 4, dtype=torch.float32, device=self.dev)
+            N.call("zeb_master_gradient", ptr(sheets), ptr(grad), m.side, stream_ptr())
+            p.baked = (key, sheets, grad)
+            self.chance_key = None
+
+    def band(self, L):
+        """engine.zig:1793-1836 — the tables of bandwidth L and every phase's, built on first use."""
+        self.prepare_masters()
+        b = self.bands.get(L)
+        if b is None:
+            b = {"tables": BandTables(L, self.dev), "phases": {}}
+            self.bands[L] = b
+        prec = self.set["precision"]
+        for i, p in enumerate(self.phases):
+            key = (id(p.baked[1]), prec)
+            pb = b["phases"].get(i)
+            if pb is None or pb[0] != key:
+                ph = PhaseBand(b["tables"], p.baked[1], p.master.side, L, prec)
+                b["phases"][i] = (key, ph)
+                r = ph.rules
+                self.log(f"phase {i}: bandwidth {L}, rotation order {r.n_fold} about z{', mirror' if r.mirror else ''}"
+                         f"{', inversion' if r.inversion else ''}")
+        return b
+
+    def denominators(self, b, fr):
+        """engine.zig:1839-1849, spherical.zig:448-464 — each phase's reciprocal denominator
+        volume for the map-centre geometry (cached per geometry)."""
+        rows, cols, h, w = self.info()
+        bn = self.set["binning"]
+        t = self.geo.translation(h / bn, w / bn).astype(np.float32)
+        key = (tuple(fr.c0), tuple(fr.c1), tuple(fr.c2), fr.h, fr.w, tuple(fr.mask), tuple(t))
+        bt = b["tables"]
+        for i, (k, ph) in b["phases"].items():
+            if ph.rden_key == key:
+                continue
+            items = torch.as_tensor(np.array([[t[0], t[1], t[2], 0.0]], np.float32), device=self.dev)
+            alm = torch.empty(bt.n_pairs * 2, dtype=torch.float32, device=self.dev)
+            stats = torch.empty(4, dtype=torch.float32, device=self.dev)
+            scratch = self.buf("sphere_scratch", N.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), 1) // 4 + 1)
+            N.call("zeb_sphere_coefficients", None, ptr(items), 1, ctypes.byref(fr), ctypes.byref(bt.st), FLAG_WINDOW,
+                   ptr(alm), ptr(stats), ptr(scratch), stream_ptr())
+            cells = ph.volume_cells()
+            vols = []
+            for Y in (ph.Y_f, ph.Y_f2):
+                U = self.buf("spec_window", N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), 1) // 4 + 1)
+                self.spectrum(alm, 1, ph, Y, U)
+                vol = torch.empty(cells, dtype=torch.float32, device=self.dev)
+                N.call("zeb_correlate_volume", ptr(U), 1, ctypes.byref(ph.dims), ptr(bt.tw), ptr(vol), stream_ptr())
+                vols.append(vol)
+            rden = torch.empty(cells, dtype=torch.float32, device=self.dev)
+            N.call("zeb_rden_build", ptr(vols[0]), ptr(vols[1]), ptr(stats), 1, cells, ptr(rden), stream_ptr())
+            ph.rden = rden
+            ph.rden_key = key
+
+    def spectrum(self, alm, n, ph, Y, U):
+        N.call("zeb_spectrum_f32", ptr(alm), n, ctypes.byref(ph.dims), ptr(Y), ptr(U), stream_ptr())
+
+    # ── device passes ──
+
+    def upload(self, cells):
+        """engine.zig:1452-1563 — the cells' stored patterns to the device, preprocessed."""
+        rows, cols, h, w = self.info()
+        if self.set["binning"] != 1:
+            raise EngineError("binning: not supported on this engine yet")
+        cells = np.asarray(cells, np.int64)
+        flat = self.patterns.reshape(rows * cols, h, w)
+        host = torch.from_numpy(flat[cells])
+        raw = host.pin_memory().to(self.dev, non_blocking=True) if host.numel() else host.to(self.dev)
+        n = len(cells)
+        out = self.buf("pats", n * h * w)
+        s = self.set
+        static = self.static_background()
+        dyn = {"none": 0, "subtract": 1, "divide": 2}[s["dynamic_background"]]
+        sigma = s["dynamic_sigma"] * w if dyn else 0.0
+        mask = (ctypes.c_float * 3)(*self.mask_of(h, w))
+        sb = N.load().zeb_prep_scratch_bytes(n, h, w, sigma)
+        scratch = self.buf("prep_scratch", sb // 4 + 1) if sb else None
+        N.call("zeb_prep_ex", ptr(raw), self.pixel, n, h, w, ptr(static), dyn, sigma, mask, 1, ptr(out),
+               ptr(scratch), stream_ptr())
+        return out
+
+    def index_cells(self, cells, bandwidth=None):
+        """engine.zig:1990-2137 — index the given cells against every phase: records
+        [phase][cell][8] = (q, NCC, NMI, last improving step, z)."""
+        cells = np.asarray(cells, np.int64)
+        n = len(cells)
+        n_ph = len(self.phases)
+        if n_ph == 0:
+            raise EngineError("NoPhases")
+        if n == 0:
+            return np.zeros((n_ph, 0, 8), np.float32)
+        s = self.set
+        L = int(bandwidth or s["bandwidth"])
+        b = self.band(L)
+        self.calibrate()
+        fr = self.frame()
+        self.denominators(b, fr)
+        pats = self.upload(cells)
+        t = self.positions(cells)
+        items_h = np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1)
+        items = torch.as_tensor(items_h, device=self.dev)
+        self.batch_stamp = self.batch_stamp % (1 << 24) + 1
+        bt = b["tables"]
+        recs = torch.empty(n_ph * n * 8, dtype=torch.float32, device=self.dev)
+        alm = self.buf("alm", n * bt.n_pairs * 2)
+        stats = self.buf("stats", n * 4)
+        sphere_scratch = self.buf("sphere_scratch", N.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), n) // 4 + 1)
+        N.call("zeb_sphere_coefficients", ptr(pats), ptr(items), n, ctypes.byref(fr), ctypes.byref(bt.st),
+               FLAG_CENTER | FLAG_NORM, ptr(alm), ptr(stats), ptr(sphere_scratch), stream_ptr())
+        opts = N.RefineOpts(s["refine_iters"] if s["refine"] else 0, math.radians(s["refine_step"]), 1.0, 0.02, 1e4,
+                            s["nmi_bins"], float(self.batch_stamp))
+        for pi, p in enumerate(self.phases):
+            ph = b["phases"][pi][1]
+            peaks = self.buf("peaks", n * 8)
+            tile = self.tile_items(ph, n)
+            for t0 in range(0, n, tile):
+                nt = min(tile, n - t0)
+                U = self.buf("spec", N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), nt) // 4 + 1)
+                a0 = alm[t0 * bt.n_pairs * 2:]
+                self.spectrum(a0, nt, ph, ph.Y_f, U)
+                cand = self.buf("cand", N.load().zeb_peaks_scratch_bytes(ctypes.byref(ph.dims), nt) // 4 + 1)
+                N.call("zeb_correlate_peaks", ptr(U), nt, ctypes.byref(ph.dims), ptr(bt.tw), ptr(ph.rden), 1 << 30,
+                       ptr(peaks[t0 * 8:]), ptr(cand), stream_ptr())
+            _, sheets, grad = p.baked
+            N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(sheets), ptr(grad),
+                   p.master.side, ctypes.byref(opts), ptr(recs[pi * n * 8:]), stream_ptr())
+        out = recs.view(n_ph, n, 8).cpu().numpy()
+        if self.pending_skip > 0:
+            # a readback that did not come from this batch (what a device that silently skipped the
+            # batch would hand back): the stamp check below rejects it
+            self.pending_skip -= 1
+            out = out.copy()
+            out[..., 7] = float(self.batch_stamp - 1)
+        if not (out[..., 7] == float(self.batch_stamp)).all():
+            raise EngineError("DeviceSkippedBatch")
+        for pi in range(n_ph):
+            out[pi, :, 7] = (out[pi, :, 5] - self.chance_med[pi]) / self.chance_spread[pi]
+        return out
+
+    def tile_items(self, ph, n):
+        """Items whose spectra one pass holds: tile_mb of them, at least 512 (spherical.zig:311-315)."""
+        per = N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), 1)
+        return int(max(1, min(n, max(512, (self.set["tile_mb"] << 20) // per))))
+
+    def calibrate(self):
+        """engine.zig:2202-2292 — chance NMI per phase: ~256 region cells × 8 random orientations;
+        median and 1.4826 × median absolute deviation."""
+        n_ph = len(self.phases)
+        s = self.set
+        key = (s["static_background"], s["static_patterns"], s["dynamic_background"], s["dynamic_sigma"], s["mask"],
+               s["mask_radius"], s["nmi_bins"], s["binning"], s["master_smooth"], s["pixel_angle_deg"], self.geo.key(),
+               tuple(id(p.baked[1]) if p.baked else None for p in self.phases), s["roi_x"], s["roi_y"], s["roi_w"],
+               s["roi_h"], id(self.patterns))
+        if key == self.chance_key and len(self.chance_med) == n_ph:
+            return
+        self.prepare_masters()
+        region = self.region_cells()
+        n = min(len(region), 256)
+        cells = region[((2 * np.arange(n) + 1) * len(region)) // (2 * n)]
+        draws = 8
+        pats = self.upload(cells)
+        t = self.positions(cells)
+        items = torch.as_tensor(np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1), device=self.dev)
+        fr = self.frame()
+        self.chance_med, self.chance_spread = [], []
+        for pi, p in enumerate(self.phases):
+            out = torch.empty(draws * n, dtype=torch.float32, device=self.dev)
+            N.call("zeb_chance", ptr(pats), ptr(items), n, draws, ctypes.byref(fr), ptr(p.baked[1]), p.master.side,
+                   s["nmi_bins"], ptr(out), stream_ptr())
+            c = np.sort(out.cpu().numpy())
+            med = c[len(c) // 2]
+            dev = np.sort(np.abs(c - med))
+            spread = max(1.4826 * dev[len(c) // 2], 1e-6)
+            self.chance_med.append(float(med))
+            self.chance_spread.append(float(spread))
+            self.log(f"chance, phase {pi}: NMI {med:.4f} ± {spread:.4f} over {n} patterns at random orientations; "
+                     f"z {s['accept_z']:.0f} is NMI {med + s['accept_z'] * spread:.4f}")
+        self.chance_key = key
+
+    def choose_phase(self, recs):
+        """engine.zig:2295-2307 — per cell, the phase with the largest NMI (or NCC)."""
+        col = 5 if self.set["phase_by"] == "nmi" else 4
+        return np.argmax(recs[:, :, col], axis=0)
+
+    # ── indexing in sweeps ──
+
+    def index_begin(self):
+        if not self.phases:
+            raise EngineError("NoPhases")
+        cells = self.region_cells()
+        self.index_cells_list = cells
+        self.index_done = 0
+        self.index_region = len(cells)
+        self.index_sweep = 0
+        self.index_accepted = 0
+        self.cancel = False
+        self.res["phase"][cells] = -1
+        self.res["sweep"][cells] = -1
+        self.res["z"][cells] = 0
+
+    def land(self, cells, recs):
+        """engine.zig:2392-2419 — each cell keeps the better match; accepted ones their sweep."""
+        s = self.set
+        settle = math.radians(s["accept_step_deg"])
+        best = self.choose_phase(recs)
+        for k, c in enumerate(cells):
+            p = int(best[k])
+            r = recs[p, k]
+            good = r[5] >= s["accept_nmi"] if s["accept_nmi"] > 0 else r[7] >= s["accept_z"]
+            res = self.res
+            if res["phase"][c] < 0 or (good and r[6] <= settle) or r[7] > res["z"][c]:
+                q = R.to_fz(r[:4].astype(np.float64), self.phases[p].master.rotations())
+                res["quat"][c] = q
+                res["ncc"][c] = r[4]
+                res["nmi"][c] = r[5]
+                res["z"][c] = r[7]
+                res["phase"][c] = p
+                res["settled"][c] = r[6] <= settle
+            kept = res["nmi"][c] >= s["accept_nmi"] if s["accept_nmi"] > 0 else res["z"][c] >= s["accept_z"]
+            if res["sweep"][c] < 0 and kept and res["settled"][c]:
+                res["sweep"][c] = self.index_sweep
+                self.index_accepted += 1
+        self.index_done += len(cells)
+        self.events.append({"kind": "progress", "stage": "index", "done": int(self.index_done),
+                            "total": int(len(self.index_cells_list)), "sweep": self.index_sweep, "sweeps": s["sweeps"]})
+
+    def index_step(self):
+        """engine.zig:2426-2465 — about 4096 cells of the sweep in progress; returns cells left."""
+        s = self.set
+        cells_all = self.index_cells_list
+        left = len(cells_all) - self.index_done
+        if left == 0 or self.cancel:
+            return 0
+        batch = max(s["batch"], 1)
+        n = min(left, batch * min(max(4096 // batch, 2), 16))
+        cells = cells_all[self.index_done:self.index_done + n]
+        bw, _, method = s.sweep(self.index_sweep)
+        if method != "spherical":
+            raise EngineError(f"method {method!r}: not supported on this engine yet")
+        recs = self.index_cells(cells, bw)
+        self.land(cells, recs)
+        if self.index_done == len(cells_all) and self.index_sweep + 1 < s["sweeps"]:
+            keep = cells_all[self.res["sweep"][cells_all] < 0]
+            self.log(f"sweep {self.index_sweep + 1} of {s['sweeps']} (spherical, bandwidth {bw}): "
+                     f"{len(cells_all) - len(keep)} of {len(cells_all)} patterns accepted, {len(keep)} left")
+            if len(keep):
+                self.index_cells_list = keep
+                self.index_done = 0
+                self.index_sweep += 1
+        return len(self.index_cells_list) - self.index_done
+
+    def status(self):
+        s = self.set
+        bw, dg, method = s.sweep(self.index_sweep)
+        return {"sweep": self.index_sweep, "sweeps": s["sweeps"], "bandwidth": bw, "dict_grid": dg,
+                "done": int(self.index_done), "total": int(len(self.index_cells_list) if self.index_cells_list is not None else 0),
+                "region": int(self.index_region), "accepted": int(self.index_accepted), "method": method}
+
+    # ── simulation ──
+
+    def simulate(self, phase, cells, quats):
+        """engine.zig:2753-2769 — simulated patterns of a phase at the given orientations, each as
+        cell cells[k] would record it (from the master as smoothed for the patterns)."""
+        self.prepare_masters()
+        cells = np.asarray(cells, np.int64)
+        q = np.asarray(quats, np.float32).reshape(-1, 4)
+        n = len(cells)
+        h, w = self.pattern_shape()
+        t = self.positions(cells)
+        poses = np.concatenate([t, np.zeros((n, 1), np.float32), q], 1)
+        pd = torch.as_tensor(poses, device=self.dev)
+        out = torch.empty(n * h * w, dtype=torch.float32, device=self.dev)
+        p = self.phases[phase]
+        fr = self.frame()
+        N.call("zeb_project", ptr(p.baked[1]), p.master.side, ptr(pd), n, ctypes.byref(fr), ptr(out), stream_ptr())
+        return out.view(n, h, w).cpu().numpy()
