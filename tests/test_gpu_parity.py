@@ -1,0 +1,288 @@
+"""Parity of the CUDA path with the FP64 oracle, stage by stage, through the C ABI (GPU only).
+
+Tolerances are float32 ones: the kernels compute in FP32 (tables in FP64) and the oracle in
+FP64 throughout; each assertion states its bound.
+"""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import oracle.detector as od  # noqa: E402
+import oracle.geometry as og  # noqa: E402
+import oracle.master as om  # noqa: E402
+import oracle.prep as op  # noqa: E402
+import oracle.sh as osh  # noqa: E402
+import oracle.spherical as osp  # noqa: E402
+import oracle.sym as osym  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from zebsdsolve_b200 import _native
+
+    return _native
+
+
+def sp():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def P(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+@pytest.fixture(scope="module")
+def world(lib):
+    """A small synthetic master (432), an engine with it, and a few simulated noisy patterns."""
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import synthetic as syn
+
+    sheets = syn.master_sheets(11, side=151, lmax=28, group="432")
+    import tempfile
+    from zebsdsolve_b200.master import write_npz
+
+    d = tempfile.mkdtemp()
+    path = f"{d}/m432.npz"
+    write_npz(path, sheets, 151, syn.group_matrices("432"), 30)
+    s = ze.Solver()
+    s.configure(static_background="none", dynamic_background="none", bandwidth=16)
+    s.add_phase(path)
+    rng = np.random.default_rng(5)
+    n = 6
+    s.set_patterns(np.zeros((1, n, 60, 60), np.float32))
+    s.set_geometry(pc=(0.5, 0.3, 0.6), sample_tilt_deg=70, detector_tilt_deg=0)
+    q = syn.uniform_quaternions(rng, n)
+    sims = s.simulate(q, cells=np.arange(n))
+    pats = sims + 0.3 * sims.std() * rng.normal(size=sims.shape)
+    s.set_patterns(pats.astype(np.float32).reshape(1, n, 60, 60))
+    baked = s.master(0).reshape(-1)
+    m_or = om.Master(151, baked, syn.group_matrices("432"), 30)
+    m_or.measure_symmetry()
+    return {"s": s, "q": q, "pats": pats, "baked": baked, "m_or": m_or, "path": path}
+
+
+def test_fp64_tables_match_oracle(lib):
+    from zebsdsolve_b200 import device
+
+    x, w = device.gauss_legendre(64, torch.device("cuda"))
+    xo, wo = osh.gauss_legendre(64)
+    assert np.abs(x.cpu().numpy() - xo).max() < 1e-14 and np.abs(w.cpu().numpy() - wo).max() < 1e-14
+    plm = device.legendre_table(24, x).cpu().numpy()  # [x][pair]
+    assert np.abs(plm - osh.legendre_all(24, xo).T).max() < 1e-12
+    L = 20
+    d = torch.empty(L ** 3, dtype=torch.float64, device="cuda")
+    lib.call("zeb_wigner_half_pi", L, P(d), sp())
+    assert np.abs(d.cpu().numpy().reshape(L, L, L) - osh.wigner_half_pi(L)).max() < 1e-12
+
+
+@pytest.mark.parametrize("h,w,sigma,pixel", [(60, 60, 9.0, 1), (96, 96, 14.4, 1), (50, 70, 0.0, 0), (160, 160, 24.0, 2)])
+def test_prep_matches_oracle(lib, h, w, sigma, pixel):
+    rng = np.random.default_rng(h + w)
+    n = 3
+    dt = {0: np.uint8, 1: np.uint16, 2: np.float32}[pixel]
+    raw = (rng.random((n, h, w)) * (200 if pixel == 0 else 3000)).astype(dt)
+    bg = (rng.random((h, w)) * 30).astype(np.float32)
+    r = min(h, w) * 0.5
+    mask = (0.5 * (h - 1), 0.5 * (w - 1), r * r)
+    out = torch.empty(n * h * w, dtype=torch.float32, device="cuda")
+    rawd = torch.as_tensor(raw, device="cuda")
+    bgd = torch.as_tensor(bg, device="cuda")
+    sb = lib.load().zeb_prep_scratch_bytes(n, h, w, sigma)
+    scratch = torch.empty(max(sb // 4, 1), dtype=torch.float32, device="cuda")
+    m3 = (ctypes.c_float * 3)(*mask)
+    lib.call("zeb_prep_ex", P(rawd), pixel, n, h, w, P(bgd), 1 if sigma > 0 else 0, sigma, m3, 1, P(out), P(scratch), sp())
+    got = out.cpu().numpy().reshape(n, h, w)
+    for i in range(n):
+        ref = op.run(raw[i], static=bg, dynamic="subtract" if sigma > 0 else "none", dynamic_sigma=sigma, mask=mask)
+        # unit-norm images: values ~ 1/sqrt(h·w); FP32 agreement to 2e-6 absolute
+        assert np.abs(got[i] - ref).max() < 2e-6, (h, w, sigma, np.abs(got[i] - ref).max())
+
+
+def _frame(s):
+    e = s._e
+    return e.frame()
+
+
+def test_sphere_coefficients_match_oracle(world, lib):
+    from zebsdsolve_b200.device import BandTables
+
+    s = world["s"]
+    e = s._e
+    L = 16
+    bt = BandTables(L, e.dev)
+    fr = _frame(s)
+    n = world["pats"].shape[0]
+    pats = torch.as_tensor(world["pats"].astype(np.float32), device="cuda").reshape(-1)
+    t = e.positions(np.arange(n))
+    items = torch.as_tensor(np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1), device="cuda")
+    alm = torch.empty(n * bt.n_pairs * 2, dtype=torch.float32, device="cuda")
+    stats = torch.empty(n * 4, dtype=torch.float32, device="cuda")
+    scr = torch.empty(lib.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), n) // 4 + 1, device="cuda")
+    lib.call("zeb_sphere_coefficients", P(pats), P(items), n, ctypes.byref(fr), ctypes.byref(bt.st), 3, P(alm), P(stats),
+             P(scr), sp())
+    got = alm.cpu().numpy().reshape(n, -1, 2)
+    got = got[..., 0] + 1j * got[..., 1]
+    tb = osp.Tables(L)
+    frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
+    for i in range(n):
+        ref, st = osp.coefficients(tb, world["pats"][i].astype(np.float64), t[i].astype(np.float64), frame,
+                                   np.array(fr.mask))
+        # unit-norm coefficients: FP32 sampling and transforms agree to 2e-5
+        assert np.abs(got[i] - ref).max() < 2e-5, np.abs(got[i] - ref).max()
+        gs = stats.cpu().numpy().reshape(n, 4)[i]
+        assert abs(gs[0] - st[0]) < 1e-4 * st[0] and abs(gs[1] - st[1]) < 1e-5 and abs(gs[2] - st[2]) < 1e-4 * st[2]
+
+
+def test_master_harmonics_match_oracle(world):
+    s = world["s"]
+    e = s._e
+    L = 16
+    b = e.band(L)
+    ph = b["phases"][0][1]
+    hm = om.Harmonics(world["m_or"], world["baked"], L)
+    f = ph.f.cpu().numpy()
+    f2 = ph.f2.cpu().numpy()
+    assert np.abs(f - hm.f).max() < 1e-9 * max(1.0, np.abs(hm.f).max())
+    assert np.abs(f2 - hm.f2).max() < 1e-9 * max(1.0, np.abs(hm.f2).max())
+    assert ph.rules.n_fold == hm.rules.n_fold == 4
+
+
+def test_correlation_peaks_match_oracle(world, lib):
+    s = world["s"]
+    e = s._e
+    L = 16
+    b = e.band(L)
+    fr = _frame(s)
+    e.denominators(b, fr)
+    bt = b["tables"]
+    ph = b["phases"][0][1]
+    n = world["pats"].shape[0]
+    pats = torch.as_tensor(world["pats"].astype(np.float32), device="cuda").reshape(-1)
+    t = e.positions(np.arange(n))
+    items = torch.as_tensor(np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1), device="cuda")
+    alm = torch.empty(n * bt.n_pairs * 2, dtype=torch.float32, device="cuda")
+    stats = torch.empty(n * 4, dtype=torch.float32, device="cuda")
+    scr = torch.empty(lib.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), n) // 4 + 1, device="cuda")
+    lib.call("zeb_sphere_coefficients", P(pats), P(items), n, ctypes.byref(fr), ctypes.byref(bt.st), 3, P(alm), P(stats),
+             P(scr), sp())
+    U = torch.empty(lib.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), n) // 4 + 1, device="cuda")
+    lib.call("zeb_spectrum_f32", P(alm), n, ctypes.byref(ph.dims), P(ph.Y_f), P(U), sp())
+    peaks = torch.empty(n * 8, device="cuda")
+    cand = torch.empty(lib.load().zeb_peaks_scratch_bytes(ctypes.byref(ph.dims), n) // 4 + 1, device="cuda")
+    lib.call("zeb_correlate_peaks", P(U), n, ctypes.byref(ph.dims), P(bt.tw), P(ph.rden), 1 << 30, P(peaks), P(cand), sp())
+    got = peaks.cpu().numpy().reshape(n, 8)
+    # the oracle: harmonics of the same baked master, its window denominators, the volume, the peak
+    tb = osp.Tables(L)
+    hm = om.Harmonics(world["m_or"], world["baked"], L)
+    pt = osp.PhaseTables(tb, hm, om.fold_of(hm.rules))
+    frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
+    t0 = e.geo.translation(60, 60)
+    walm, wst = osp.coefficients(tb, None, t0, frame, np.array(fr.mask), flags=osp.FLAG_WINDOW, shape=(60, 60))
+    rden = osp.window_denominators(tb, pt, walm, wst[0])
+    assert np.abs(ph.rden.cpu().numpy().reshape(rden.shape) - rden).max() < 1e-4 * np.abs(rden).max()
+    ops = world["m_or"].rotations()
+    for i in range(n):
+        g, _ = osp.coefficients(tb, world["pats"][i].astype(np.float64), t[i].astype(np.float64), frame, np.array(fr.mask))
+        vol = osp.correlation_volume(tb, pt, hm.f, g) * rden
+        q, v0, abc, idx = osp.peak(tb, pt, vol)
+        assert abs(got[i, 4] - v0) < 2e-4, (got[i, 4], v0)
+        dis = math.degrees(float(osym.disorientation(got[i, :4].astype(np.float64), q, ops)))
+        assert dis < 0.05, dis
+
+
+def test_refine_and_nmi_match_oracle(world, lib):
+    s = world["s"]
+    e = s._e
+    e.prepare_masters()
+    fr = _frame(s)
+    n = world["pats"].shape[0]
+    pats = world["pats"].astype(np.float32)
+    # normalized patterns as the engine's preprocessing leaves them
+    mask = np.array(fr.mask)
+    normed = np.stack([op.normalize(p.astype(np.float64), mask) for p in pats]).astype(np.float32)
+    t = e.positions(np.arange(n))
+    items = torch.as_tensor(np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1), device="cuda")
+    rng = np.random.default_rng(9)
+    from zebsdsolve_b200 import rotations as R
+
+    start = R.qstd(R.qmul(R.exp_map(rng.normal(0, math.radians(0.8), (n, 3))), world["q"]))
+    seeds = torch.as_tensor(np.concatenate([start, np.zeros((n, 4))], 1).astype(np.float32), device="cuda")
+    recs = torch.empty(n * 8, device="cuda")
+    p = e.phases[0]
+    opts = lib.RefineOpts(8, math.radians(2.0), 1.0, 0.02, 1e4, 16, 7.0)
+    pd = torch.as_tensor(normed, device="cuda").reshape(-1)
+    lib.call("zeb_refine", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(p.baked[1]), P(p.baked[2]), p.master.side,
+             ctypes.byref(opts), P(recs), sp())
+    got = recs.cpu().numpy().reshape(n, 8)
+    grad = od.gradient_table(world["baked"], 151)
+    frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
+    ops = world["m_or"].rotations()
+    for i in range(n):
+        qb, best, step = od.refine(grad, 151, frame, t[i], start[i], normed[i].astype(np.float64), mask)
+        assert abs(got[i, 4] - best) < 2e-4, (got[i, 4], best)
+        dis = math.degrees(float(osym.disorientation(got[i, :4].astype(np.float64), qb, ops)))
+        assert dis < 0.02, dis
+        v = od.nmi(world["baked"], 151, frame, t[i], got[i, :4].astype(np.float64), normed[i].astype(np.float64), mask)
+        assert abs(got[i, 5] - v) < 2e-3, (got[i, 5], v)
+        assert got[i, 7] == 7.0
+        # and the refinement found the truth
+        assert math.degrees(float(osym.disorientation(got[i, :4].astype(np.float64), world["q"][i], ops))) < 0.3
+
+
+def test_chance_decoys_match_oracle(world, lib):
+    s = world["s"]
+    e = s._e
+    e.prepare_masters()
+    fr = _frame(s)
+    n = world["pats"].shape[0]
+    mask = np.array(fr.mask)
+    normed = np.stack([op.normalize(p.astype(np.float64), mask) for p in world["pats"]]).astype(np.float32)
+    t = e.positions(np.arange(n))
+    items = torch.as_tensor(np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1), device="cuda")
+    out = torch.empty(3 * n, device="cuda")
+    pd = torch.as_tensor(normed, device="cuda").reshape(-1)
+    p = e.phases[0]
+    lib.call("zeb_chance", P(pd), P(items), n, 3, ctypes.byref(fr), P(p.baked[1]), p.master.side, 16, P(out), sp())
+    got = out.cpu().numpy().reshape(3, n)
+    frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
+    for d in range(3):
+        qd = od.decoy(np.arange(n), d)
+        for i in range(n):
+            v = od.nmi(world["baked"], 151, frame, t[i], qd[i], normed[i].astype(np.float64), mask)
+            assert abs(got[d, i] - v) < 2e-3
+
+
+def test_index_end_to_end_recovers_orientations(lib):
+    """The reference's own bar (tests/test_api.py:206-214): 8 × 12 simulated patterns with noise of
+    1.0 × their deviation, indexed: median disorientation < 0.15°, max < 1°."""
+    import tempfile
+
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import synthetic as syn
+    from zebsdsolve_b200.master import write_npz
+
+    sheets = syn.master_sheets(2, side=201, lmax=48, group="432")
+    d = tempfile.mkdtemp()
+    write_npz(f"{d}/m.npz", sheets, 201, syn.group_matrices("432"), 30)
+    rng = np.random.default_rng(7)
+    s = ze.Solver()
+    s.configure(static_background="none", dynamic_background="none")
+    s.add_phase(f"{d}/m.npz")
+    rows, cols = 8, 12
+    s.set_patterns(np.zeros((rows, cols, 60, 60), np.float32))
+    s.set_geometry(pc=(0.44, 0.24, 0.53), sample_tilt_deg=70, detector_tilt_deg=0, px_um=70 * 8, step_x_um=20, step_y_um=20)
+    q = syn.uniform_quaternions(rng, rows * cols)
+    sims = s.simulate(q, cells=np.arange(rows * cols))
+    sims = sims + 1.0 * sims.std() * rng.normal(size=sims.shape)
+    s.set_patterns(sims.astype(np.float32).reshape(rows, cols, 60, 60))
+    r = s.index()
+    dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), q))
+    assert np.median(dis) < 0.15 and dis.max() < 1.0, (np.median(dis), dis.max())
+    assert (r["phase"] == 0).all()

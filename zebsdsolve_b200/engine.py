@@ -278,7 +278,7 @@ class Engine:
         for p in self.phases:
             m = p.master
             px = angle * m.side / math.sqrt(2 * math.pi)
-            q = int(round(math.log(px) / math.log(1.05))) if px > 0 else None
+            q = int(math.floor(math.log(px) / math.log(1.05) + 0.5)) if px > 0 else None
             key = (q, self.set["master_smooth"])
             if p.baked is not None and p.baked[0] == key:
                 continue
