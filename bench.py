@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Throughput of the spherical indexing path (patterns/s indexed + refined) on B200.
+
+    python bench.py [--gpus N --steps K --warmup W --precision bf16|f32 --patterns P]
+    python bench.py --impl reference ...   # the reference's algorithm on the host cores
+
+Workload (the precision-form configuration at scale): a 316 × 316 scan (99,856 patterns) of
+60 × 60 uint16 patterns whose orientations are 200 Voronoi grains with a 0.5° Gaussian spread,
+simulated from a seeded 432-symmetrised master (SH degree ≤ 96, 401² Lambert sheets) at pattern
+centre (0.5, 0.3, 0.6), sample tilt 70°, with a Gaussian background and Poisson counts; indexed
+at L = 64 on the 128³ Euler grid (the reference's defaults: static and dynamic background,
+circular mask, 8 refinement iterations).  A step is one pass of the whole path over the whole
+scan.  Inputs (720 MB) exceed L2 (126 MB), so no flush is needed between steps.
+
+`value` times the device path with the stored patterns already resident in HBM; `e2e` times the
+public API (Solver.index) from host memory: uploads, device path, the records' readback and the
+host's landing of results.  Under torchrun each rank indexes its own scan (weak scaling, no
+collective on the data path; the max of the ranks' times is reported).
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+ROWS = COLS = 316
+H = W = 60
+L = 64
+GRAINS = 200
+SPREAD_DEG = 0.5
+PC = (0.5, 0.3, 0.6)
+WORKLOAD = ("316x316 scan of 60x60 uint16 patterns, 200 Voronoi grains (0.5 deg spread), 432 master 401^2 "
+            "(SH <= 96), bandwidth 64 (128^3 Euler grid), 8 refinement iterations")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--precision", default="f32", choices=("f32", "bf16"))
+    ap.add_argument("--patterns", type=int, default=ROWS * COLS, help="scan size (cells), default 316x316")
+    ap.add_argument("--batch", type=int, default=16384, help="patterns per device pass in the value measurement")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def scan_shape(n):
+    if n == ROWS * COLS:
+        return ROWS, COLS
+    cols = int(math.ceil(math.sqrt(n)))
+    return int(math.ceil(n / cols)), cols
+
+
+# ── the reference's algorithm on the host (the oracle restatement) ──
+
+def _oracle_world(seed=2):
+    """Inputs of the CPU legs: the master and a handful of patterns, made on the host."""
+    import oracle.detector as od
+    import oracle.geometry as og
+    import oracle.master as om
+    import oracle.prep as op
+    import oracle.spherical as osp
+    from zebsdsolve_b200 import synthetic as syn
+
+    sheets = syn.master_sheets(seed, side=401, lmax=96, group="432").reshape(-1)
+    m = om.Master(401, sheets, syn.group_matrices("432"), 30)
+    geo = og.Geometry(pc=PC, sample_tilt_deg=70.0)
+    frame = geo.frame()
+    mask = og.mask_of(H, W)
+    return {"sheets": sheets, "m": m, "geo": geo, "frame": frame, "mask": mask}
+
+
+def _oracle_setup(L_):
+    import oracle.master as om
+    import oracle.detector as od
+    import oracle.spherical as osp
+
+    w = _oracle_world()
+    tb = osp.Tables(L_)
+    hm = om.Harmonics(w["m"], w["sheets"], L_)
+    pt = osp.PhaseTables(tb, hm, om.fold_of(hm.rules))
+    t0 = w["geo"].translation(H, W)
+    walm, wst = osp.coefficients(tb, None, t0, w["frame"], w["mask"], flags=osp.FLAG_WINDOW, shape=(H, W))
+    rden = osp.window_denominators(tb, pt, walm, wst[0])
+    grad = od.gradient_table(w["sheets"], 401)
+    return w, tb, hm, pt, rden, grad
+
+
+_ORACLE = {}
+
+
+def _oracle_pattern(args):
+    """One pattern through the oracle's path: filters, sphere, correlation, peak, refinement, NMI."""
+    import oracle.detector as od
+    import oracle.prep as op
+    import oracle.spherical as osp
+
+    raw, q0 = args
+    if "state" not in _ORACLE:
+        _ORACLE["state"] = _oracle_setup(L)
+    w, tb, hm, pt, rden, grad = _ORACLE["state"]
+    t = w["geo"].translation(H, W)
+    pat = op.run(raw, static=None, dynamic="subtract", dynamic_sigma=0.15 * W, mask=w["mask"])
+    g, _ = osp.coefficients(tb, pat, t, w["frame"], w["mask"])
+    vol = osp.correlation_volume(tb, pt, hm.f, g) * rden
+    q, v0, _, _ = osp.peak(tb, pt, vol)
+    qb, best, step = od.refine(grad, 401, w["frame"], t, q, pat, w["mask"])
+    v = od.nmi(w["sheets"], 401, w["frame"], t, qb, pat, w["mask"])
+    return float(best), float(v)
+
+
+def cpu_leg(seconds, seed=4):
+    """The oracle over a bounded sample of the workload, in a spawn pool over every host core.
+    Returns (patterns/s, cores, sample description)."""
+    import multiprocessing as mp
+
+    import oracle.detector as od
+
+    w = _oracle_world()
+    rng = np.random.default_rng(seed)
+    cores = min(len(os.sched_getaffinity(0)), 64)
+    n = 2 * cores
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    t = w["geo"].translation(H, W)
+    yy, xx = np.meshgrid(np.arange(H) + 0.5 - H / 2, np.arange(W) + 0.5 - W / 2, indexing="ij")
+    B = np.exp(-(xx ** 2 + yy ** 2) / (2 * (0.4 * W) ** 2))
+    B *= B.size / B.sum()
+    pats = []
+    for i in range(n):
+        sim = od.project(w["sheets"], 401, w["frame"], t, q[i], H, W)
+        pats.append(np.clip(rng.poisson(np.maximum(1000 * (0.6 + 0.4 * sim) * B, 0)), 0, 65535).astype(np.uint16))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_oracle_pattern, [(pats[i], q[i]) for i in range(cores)])  # set-up in every worker
+        done = 0
+        t0 = time.perf_counter()
+        while True:
+            pool.map(_oracle_pattern, [(pats[i % n], q[i % n]) for i in range(cores)])
+            done += cores
+            if time.perf_counter() - t0 > seconds:
+                break
+        dt = time.perf_counter() - t0
+    return done / dt, cores, f"{done} patterns of the workload (60x60, L=64, refined) through the FP64 NumPy oracle in {dt:.1f} s"
+
+
+# ── the device ──
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        self.path = tempfile.mktemp(suffix=".csv")
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 3 + k and "Active" in r[3 + k] and "Not" not in r[3 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+class StageTimer:
+    """CUDA events at the stage boundaries of one pass (on the launching stream)."""
+
+    def __init__(self, torch):
+        self.torch = torch
+        self.events = []
+
+    def mark(self, name):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.events.append((name, e))
+
+    def totals(self):
+        self.torch.cuda.synchronize()
+        out = {}
+        for (name, e0), (_, e1) in zip(self.events, self.events[1:]):
+            out[name] = out.get(name, 0.0) + e0.elapsed_time(e1)
+        return out
+
+
+def device_main(a):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import _native
+    from zebsdsolve_b200 import synthetic as syn
+    from zebsdsolve_b200.master import write_npz
+
+    rows, cols = scan_shape(a.patterns)
+    n = rows * cols
+    sheets = syn.master_sheets(2, side=401, lmax=96, group="432", device="cuda")
+    tmp = tempfile.mkdtemp()
+    write_npz(f"{tmp}/m432.npz", sheets, 401, syn.group_matrices("432"), 30)
+    s = ze.Solver()
+    s.configure(bandwidth=L, precision=a.precision)
+    s.add_phase(f"{tmp}/m432.npz")
+    s.set_patterns(np.zeros((rows, cols, H, W), np.uint16))
+    s.set_geometry(pc=PC, sample_tilt_deg=70.0, detector_tilt_deg=0.0)
+    e = s._e
+    rng = np.random.default_rng(100 + rank)
+    q, grain = syn.grain_map(rng, rows, cols, GRAINS, SPREAD_DEG)
+    pats = np.empty((n, H, W), np.uint16)
+    for i in range(0, n, 16384):
+        sims = e.simulate_device(0, np.arange(i, min(n, i + 16384)), q[i:i + 16384])
+        pats[i:i + len(sims)] = syn.counted_patterns(sims, seed=1000 * rank + i // 16384).cpu().numpy()
+    s.set_patterns(pats.reshape(rows, cols, H, W))
+    e.prepare(L)
+    torch.cuda.synchronize()
+
+    # value: stored patterns resident in HBM
+    raw = torch.as_tensor(pats, device="cuda")
+    cells = np.arange(n)
+    batch = min(a.batch, n)
+
+    def device_pass(timer=None):
+        for b0 in range(0, n, batch):
+            c = cells[b0:b0 + batch]
+            e.run_device(raw[b0:b0 + len(c)], c, L, timer)
+
+    for _ in range(a.warmup):
+        device_pass()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    _native.launches["count"] = 0
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        t0.record()
+        for _ in range(a.steps):
+            device_pass()
+        t1.record()
+        torch.cuda.synchronize()
+    launches = _native.launches["count"]
+    ms = t0.elapsed_time(t1) / a.steps
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    value = n * world / (ms / 1e3)
+
+    # stage times of one more pass, for the roofline of the dominant kernel
+    timer = StageTimer(torch)
+    device_pass(timer)
+    stages = timer.totals()
+
+    # e2e: the public API from host memory, every step
+    for _ in range(max(1, a.warmup - 2)):
+        s.index()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(a.steps):
+        r = s.index()
+    e1.record()
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1) / a.steps
+    if dist:
+        tt = torch.tensor([ems], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ems = float(tt.item())
+    e2e = n * world / (ems / 1e3)
+    dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), q))
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    ph = e.bands[L]["phases"][0][1]
+    d = ph.dims
+    per_pass = math.ceil(n / batch)
+    dom = max(stages, key=stages.get)
+    # algorithmic work of each stage per pattern
+    u_bytes = d.nb * d.L * d.nc * 8
+    work = {"peaks": ("hbm", u_bytes, "GB/s"),  # the spectrum U read once
+            "spectrum": ("hbm", u_bytes + d.n_pairs * 8, "GB/s"),  # U written once, coefficients read
+            "prep": ("hbm", H * W * (2 + 4), "GB/s"),
+            "sphere": ("hbm", H * W * 4 + d.n_pairs * 8, "GB/s"),
+            "refine": ("hbm", H * W * 4 + 32, "GB/s")}
+    bound, per_unit, unit = work.get(dom, ("hbm", 0, "GB/s"))
+    achieved = per_unit * n / (stages[dom] / 1e3) / 1e9
+    line = {
+        "metric": "patterns/s indexed+refined on 1 B200, BF16 form vs plain FP32 at <=0.1 deg error",
+        "value": round(value, 1), "unit": "patterns/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if a.precision == "f32" else "bf16+f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "patterns_per_gpu": n, "bandwidth": L, "precision": a.precision,
+                   "device_batch": batch, "l2": "inputs (720 MB) larger than L2, no flush"},
+        "e2e": {"value": round(e2e, 1), "unit": "patterns/s", "h2d_bytes_per_step": int(n * H * W * 2),
+                "d2h_bytes_per_step": int(n * 8 * 4 * len(e.phases))},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": bound, "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": unit,
+                     "frac": round(achieved / hbm, 4), "traffic": None,
+                     "stage_ms_per_step": {k: round(v, 3) for k, v in stages.items()}},
+        "accuracy": {"median_deg": round(float(np.median(dis)), 4), "p99_deg": round(float(np.percentile(dis, 99)), 4),
+                     "within_0.1deg": round(float((dis < 0.1).mean()), 4)},
+        "clocks": clk.summary(),
+    }
+    if not a.no_cpu:
+        v, cores, sample = cpu_leg(a.cpu_seconds)
+        line["cpu_baseline"] = {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port", "sample": sample}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def reference_main(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    v, cores, sample = cpu_leg(max(5.0, a.cpu_seconds))
+    line = {"impl": "reference", "metric": "patterns/s indexed+refined on 1 B200, BF16 form vs plain FP32 at <=0.1 deg error",
+            "value": round(v, 3), "unit": "patterns/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "bandwidth": L},
+            "cpu_baseline": {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": round(v, 3), "unit": "patterns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference engine (Zig + WGSL on wgpu-native) cannot be built or run here; its algorithm is timed "
+                    "as the FP64 NumPy restatement on the host cores"}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    args = parse()
+    if args.impl == "reference":
+        reference_main(args)
+    else:
+        device_main(args)

@@ -268,9 +268,9 @@ def test_index_end_to_end_recovers_orientations(lib):
     from zebsdsolve_b200 import synthetic as syn
     from zebsdsolve_b200.master import write_npz
 
-    sheets = syn.master_sheets(2, side=201, lmax=48, group="432")
+    sheets = syn.master_sheets(2, side=401, lmax=96, group="432", device="cuda")
     d = tempfile.mkdtemp()
-    write_npz(f"{d}/m.npz", sheets, 201, syn.group_matrices("432"), 30)
+    write_npz(f"{d}/m.npz", sheets, 401, syn.group_matrices("432"), 30)
     rng = np.random.default_rng(7)
     s = ze.Solver()
     s.configure(static_background="none", dynamic_background="none")

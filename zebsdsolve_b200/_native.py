@@ -70,6 +70,14 @@ _SIGS = {
 
 _lib = None
 
+# kernels each entry point launches (for the launch counts the benchmark reports)
+KERNELS = {"zeb_prep": 1, "zeb_prep_ex": 1, "zeb_sphere_coefficients": 3, "zeb_spectrum_f32": 1,
+           "zeb_spectrum_bf16": 1, "zeb_correlate_peaks": 2, "zeb_correlate_volume": 1, "zeb_rden_build": 1,
+           "zeb_refine": 1, "zeb_chance": 1, "zeb_project": 1, "zeb_master_blur_pass": 1, "zeb_master_gradient": 1,
+           "zeb_master_sample_grid": 1, "zeb_gauss_legendre": 1, "zeb_legendre_table": 1, "zeb_wigner_half_pi": 1,
+           "zeb_correlation_table": 1}
+launches = {"count": 0}
+
 
 def lib_path():
     return Path(os.environ.get("ZEBSDSOLVE_B200_LIB", HERE / LIB_NAME))
@@ -107,6 +115,7 @@ def call(name, *args):
     """Call an entry point; a negative return raises NativeError with the library's message."""
     lib = load()
     rc = getattr(lib, name)(*args)
+    launches["count"] += KERNELS.get(name, 0)
     if isinstance(rc, int) and rc < 0:
         raise NativeError(f"{name}: {last_error(lib) or rc}")
     return rc

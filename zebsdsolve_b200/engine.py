@@ -349,21 +349,22 @@ class Engine:
 
     # ── device passes ──
 
-    def upload(self, cells):
-        """engine.zig:1452-1563 — the cells' stored patterns to the device, preprocessed."""
+    def prep_options(self):
+        rows, cols, h, w = self.info()
+        s = self.set
+        dyn = {"none": 0, "subtract": 1, "divide": 2}[s["dynamic_background"]]
+        sigma = s["dynamic_sigma"] * w if dyn else 0.0
+        return dyn, sigma
+
+    def preprocess(self, raw, n):
+        """engine.zig:1452-1563 — n stored patterns on the device (raw, the scan's pixel type)
+        through the filter chain into the float32 pattern buffer."""
         rows, cols, h, w = self.info()
         if self.set["binning"] != 1:
             raise EngineError("binning: not supported on this engine yet")
-        cells = np.asarray(cells, np.int64)
-        flat = self.patterns.reshape(rows * cols, h, w)
-        host = torch.from_numpy(flat[cells])
-        raw = host.pin_memory().to(self.dev, non_blocking=True) if host.numel() else host.to(self.dev)
-        n = len(cells)
         out = self.buf("pats", n * h * w)
-        s = self.set
         static = self.static_background()
-        dyn = {"none": 0, "subtract": 1, "divide": 2}[s["dynamic_background"]]
-        sigma = s["dynamic_sigma"] * w if dyn else 0.0
+        dyn, sigma = self.prep_options()
         mask = (ctypes.c_float * 3)(*self.mask_of(h, w))
         sb = N.load().zeb_prep_scratch_bytes(n, h, w, sigma)
         scratch = self.buf("prep_scratch", sb // 4 + 1) if sb else None
@@ -371,32 +372,47 @@ class Engine:
                ptr(scratch), stream_ptr())
         return out
 
-    def index_cells(self, cells, bandwidth=None):
-        """engine.zig:1990-2137 — index the given cells against every phase: records
-        [phase][cell][8] = (q, NCC, NMI, last improving step, z)."""
+    def upload(self, cells):
+        """The cells' stored patterns to the device (pinned host → device), preprocessed."""
+        rows, cols, h, w = self.info()
         cells = np.asarray(cells, np.int64)
-        n = len(cells)
-        n_ph = len(self.phases)
-        if n_ph == 0:
-            raise EngineError("NoPhases")
-        if n == 0:
-            return np.zeros((n_ph, 0, 8), np.float32)
-        s = self.set
-        L = int(bandwidth or s["bandwidth"])
+        flat = self.patterns.reshape(rows * cols, h, w)
+        host = torch.from_numpy(flat[cells])
+        raw = host.pin_memory().to(self.dev, non_blocking=True) if host.numel() else host.to(self.dev)
+        return self.preprocess(raw, len(cells))
+
+    def prepare(self, bandwidth=None):
+        """Everything a batch needs besides its patterns: tables, chance calibration, denominators."""
+        L = int(bandwidth or self.set["bandwidth"])
         b = self.band(L)
         self.calibrate()
-        fr = self.frame()
-        self.denominators(b, fr)
-        pats = self.upload(cells)
+        self.denominators(b, self.frame())
+        return b
+
+    def items_of(self, cells):
+        cells = np.asarray(cells, np.int64)
         t = self.positions(cells)
-        items_h = np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1)
-        items = torch.as_tensor(items_h, device=self.dev)
+        return torch.as_tensor(np.concatenate([t, np.arange(len(cells), dtype=np.float32)[:, None]], 1), device=self.dev)
+
+    def run_device(self, raw, cells, bandwidth=None, timer=None):
+        """One pass of the device path over n = len(cells) stored patterns already on the device:
+        records [phase][cell][8] as a device tensor (engine.zig:2005-2122, no readback)."""
+        n = len(cells)
+        n_ph = len(self.phases)
+        s = self.set
+        b = self.prepare(bandwidth)
+        fr = self.frame()
+        mark = timer.mark if timer is not None else (lambda name: None)
+        mark("prep")
+        pats = self.preprocess(raw, n)
+        items = self.items_of(cells)
         self.batch_stamp = self.batch_stamp % (1 << 24) + 1
         bt = b["tables"]
-        recs = torch.empty(n_ph * n * 8, dtype=torch.float32, device=self.dev)
+        recs = self.buf("recs", n_ph * n * 8)
         alm = self.buf("alm", n * bt.n_pairs * 2)
         stats = self.buf("stats", n * 4)
         sphere_scratch = self.buf("sphere_scratch", N.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), n) // 4 + 1)
+        mark("sphere")
         N.call("zeb_sphere_coefficients", ptr(pats), ptr(items), n, ctypes.byref(fr), ctypes.byref(bt.st),
                FLAG_CENTER | FLAG_NORM, ptr(alm), ptr(stats), ptr(sphere_scratch), stream_ptr())
         opts = N.RefineOpts(s["refine_iters"] if s["refine"] else 0, math.radians(s["refine_step"]), 1.0, 0.02, 1e4,
@@ -409,14 +425,39 @@ class Engine:
                 nt = min(tile, n - t0)
                 U = self.buf("spec", N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), nt) // 4 + 1)
                 a0 = alm[t0 * bt.n_pairs * 2:]
+                mark("spectrum")
                 self.spectrum(a0, nt, ph, ph.Y_f, U)
                 cand = self.buf("cand", N.load().zeb_peaks_scratch_bytes(ctypes.byref(ph.dims), nt) // 4 + 1)
+                mark("peaks")
                 N.call("zeb_correlate_peaks", ptr(U), nt, ctypes.byref(ph.dims), ptr(bt.tw), ptr(ph.rden), 1 << 30,
                        ptr(peaks[t0 * 8:]), ptr(cand), stream_ptr())
             _, sheets, grad = p.baked
+            mark("refine")
             N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(sheets), ptr(grad),
                    p.master.side, ctypes.byref(opts), ptr(recs[pi * n * 8:]), stream_ptr())
-        out = recs.view(n_ph, n, 8).cpu().numpy()
+        mark("end")
+        return recs[: n_ph * n * 8].view(n_ph, n, 8)
+
+    def index_cells(self, cells, bandwidth=None):
+        """engine.zig:1990-2137 — index the given cells against every phase: records
+        [phase][cell][8] = (q, NCC, NMI, last improving step, z)."""
+        cells = np.asarray(cells, np.int64)
+        n = len(cells)
+        n_ph = len(self.phases)
+        if n_ph == 0:
+            raise EngineError("NoPhases")
+        if n == 0:
+            return np.zeros((n_ph, 0, 8), np.float32)
+        self.prepare(bandwidth)
+        rows, cols, h, w = self.info()
+        flat = self.patterns.reshape(rows * cols, h, w)
+        host = torch.from_numpy(flat[cells])
+        raw = host.pin_memory().to(self.dev, non_blocking=True)
+        out = self.run_device(raw, cells, bandwidth).cpu().numpy()
+        return self.finish(out)
+
+    def finish(self, out):
+        """engine.zig:2127-2137 — the batch stamp checked, and each NMI on the scan's chance scale."""
         if self.pending_skip > 0:
             # a readback that did not come from this batch (what a device that silently skipped the
             # batch would hand back): the stamp check below rejects it
@@ -425,7 +466,7 @@ class Engine:
             out[..., 7] = float(self.batch_stamp - 1)
         if not (out[..., 7] == float(self.batch_stamp)).all():
             raise EngineError("DeviceSkippedBatch")
-        for pi in range(n_ph):
+        for pi in range(out.shape[0]):
             out[pi, :, 7] = (out[pi, :, 5] - self.chance_med[pi]) / self.chance_spread[pi]
         return out
 
@@ -493,25 +534,28 @@ class Engine:
     def land(self, cells, recs):
         """engine.zig:2392-2419 — each cell keeps the better match; accepted ones their sweep."""
         s = self.set
+        res = self.res
+        cells = np.asarray(cells, np.int64)
         settle = math.radians(s["accept_step_deg"])
         best = self.choose_phase(recs)
-        for k, c in enumerate(cells):
-            p = int(best[k])
-            r = recs[p, k]
-            good = r[5] >= s["accept_nmi"] if s["accept_nmi"] > 0 else r[7] >= s["accept_z"]
-            res = self.res
-            if res["phase"][c] < 0 or (good and r[6] <= settle) or r[7] > res["z"][c]:
-                q = R.to_fz(r[:4].astype(np.float64), self.phases[p].master.rotations())
-                res["quat"][c] = q
-                res["ncc"][c] = r[4]
-                res["nmi"][c] = r[5]
-                res["z"][c] = r[7]
-                res["phase"][c] = p
-                res["settled"][c] = r[6] <= settle
-            kept = res["nmi"][c] >= s["accept_nmi"] if s["accept_nmi"] > 0 else res["z"][c] >= s["accept_z"]
-            if res["sweep"][c] < 0 and kept and res["settled"][c]:
-                res["sweep"][c] = self.index_sweep
-                self.index_accepted += 1
+        r = recs[best, np.arange(len(cells))]
+        good = r[:, 5] >= s["accept_nmi"] if s["accept_nmi"] > 0 else r[:, 7] >= s["accept_z"]
+        replace = (res["phase"][cells] < 0) | (good & (r[:, 6] <= settle)) | (r[:, 7] > res["z"][cells])
+        q = np.empty((len(cells), 4))
+        for p in np.unique(best):
+            sel = best == p
+            q[sel] = R.to_fz(r[sel, :4].astype(np.float64), self.phases[int(p)].master.rotations())
+        idx = cells[replace]
+        res["quat"][idx] = q[replace]
+        res["ncc"][idx] = r[replace, 4]
+        res["nmi"][idx] = r[replace, 5]
+        res["z"][idx] = r[replace, 7]
+        res["phase"][idx] = best[replace]
+        res["settled"][idx] = r[replace, 6] <= settle
+        kept = res["nmi"][cells] >= s["accept_nmi"] if s["accept_nmi"] > 0 else res["z"][cells] >= s["accept_z"]
+        newly = (res["sweep"][cells] < 0) & kept & res["settled"][cells]
+        res["sweep"][cells[newly]] = self.index_sweep
+        self.index_accepted += int(newly.sum())
         self.index_done += len(cells)
         self.events.append({"kind": "progress", "stage": "index", "done": int(self.index_done),
                             "total": int(len(self.index_cells_list)), "sweep": self.index_sweep, "sweeps": s["sweeps"]})
@@ -549,6 +593,21 @@ class Engine:
                 "region": int(self.index_region), "accepted": int(self.index_accepted), "method": method}
 
     # ── simulation ──
+
+    def simulate_device(self, phase, cells, quats):
+        """The simulated patterns as a device tensor [n, h, w] (see simulate)."""
+        self.prepare_masters()
+        cells = np.asarray(cells, np.int64)
+        q = np.asarray(quats, np.float32).reshape(-1, 4)
+        n = len(cells)
+        h, w = self.pattern_shape()
+        t = self.positions(cells)
+        pd = torch.as_tensor(np.concatenate([t, np.zeros((n, 1), np.float32), q], 1), device=self.dev)
+        out = torch.empty(n * h * w, dtype=torch.float32, device=self.dev)
+        p = self.phases[phase]
+        fr = self.frame()
+        N.call("zeb_project", ptr(p.baked[1]), p.master.side, ptr(pd), n, ctypes.byref(fr), ptr(out), stream_ptr())
+        return out.view(n, h, w)
 
     def simulate(self, phase, cells, quats):
         """engine.zig:2753-2769 — simulated patterns of a phase at the given orientations, each as
