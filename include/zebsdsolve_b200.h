@@ -145,6 +145,23 @@ size_t zeb_peaks_scratch_bytes(const zeb_so3_dims_t* d, int n_items);
 int zeb_correlate_peaks(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw, const float* rden,
                         int rden_div, float* peaks, void* scratch, void* stream);
 
+/* zeb_correlate_peaks without caller scratch — this entry point has no counterpart in the
+ * reference. It is for callers that cannot call cudaMalloc: hosts that reserve their device
+ * memory once at start-up and forbid allocation afterwards (an allocator owns the rest of the
+ * GPU), and latency-bound loops that must not let an allocation call synchronize the device.
+ * The candidates' scratch is a file-scope __device__ array of ZEB_PEAKS_STATIC_SLABS (item, j)
+ * slabs (4 MiB; every GPU that loads the library holds it until the process exits), so one call
+ * takes at most ZEB_PEAKS_STATIC_SLABS / nb items (8065 at L = 64); larger calls fail with
+ * ZEB_ESIZE and a message. The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress, once per device, with that device current); make that first call
+ * before any stream capture. Every call shares the one array and leaves its candidates in it:
+ * calls that overlap on the GPU (other streams, other threads) race and must be serialized by
+ * the caller. Nothing in it needs to start at zero: each call writes every candidate it reads.
+ * Allocates nothing (no cudaMalloc, cudaFree or allocating library routine). */
+#define ZEB_PEAKS_STATIC_SLABS (1 << 19)
+int zeb_correlate_peaks_static(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw,
+                               const float* rden, int rden_div, float* peaks, void* stream);
+
 /* The full volumes (no peak) of n items: vol[b][j][iq][ia]. Replaces a_volume
  * (shaders/so3.wgsl:595-612). */
 int zeb_correlate_volume(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw, float* vol, void* stream);

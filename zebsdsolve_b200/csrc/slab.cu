@@ -11,6 +11,8 @@
 // k_peak_finish then takes each item's best slab, re-evaluates the six neighbours of the peak by
 // direct sums over m' (V taken from U along c directly) and fits the parabolic vertex along a, c
 // and b (so3.wgsl:665-796).
+#include <mutex>
+
 #include "abi_util.cuh"
 
 namespace zeb {
@@ -309,4 +311,56 @@ extern "C" int zeb_rden_build(const float* vol_f, const float* vol_f2, const flo
   k_rden_build<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(vol_f, vol_f2, stats, cells, total,
                                                                                   rden);
   return zeb_launch_check("rden_build");
+}
+
+// ── the same peaks with their scratch in a static device array (no allocation anywhere) ──
+//
+// The candidates of zeb_correlate_peaks (one (value, index) per (item, j) slab) live here instead
+// of in caller memory: ZEB_PEAKS_STATIC_SLABS of them, 4 MiB, held by every device that loads the
+// library until the process exits. Host code may not hand g_peaks_scratch to a kernel (in host
+// code the name stands for a host-side shadow, not a device address): each device's address is
+// looked up once with cudaGetSymbolAddress, with that device current, and passed to the kernels.
+static __device__ __align__(256) float2 g_peaks_scratch[ZEB_PEAKS_STATIC_SLABS];
+
+namespace {
+std::mutex g_static_mu;
+float2* g_static_addr[256];
+}
+
+extern "C" int zeb_correlate_peaks_static(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw,
+                                          const float* rden, int rden_div, float* peaks, void* stream) {
+  ZEB_REQUIRE(U && tw && rden && peaks, ZEB_EARG, "correlate_peaks_static: null argument");
+  ZEB_REQUIRE(dims_ok(d), ZEB_EARG, "correlate_peaks_static: inconsistent dims");
+  ZEB_REQUIRE(rden_div >= 1, ZEB_EARG, "correlate_peaks_static: rden_div=%d", rden_div);
+  if (n_items <= 0) return ZEB_OK;
+  ZEB_REQUIRE((long long)n_items * d->nb <= (long long)ZEB_PEAKS_STATIC_SLABS, ZEB_ESIZE,
+              "correlate_peaks_static: %d items need %lld slabs of scratch; the static scratch holds %d "
+              "(at most %d items at this bandwidth)",
+              n_items, (long long)n_items * d->nb, ZEB_PEAKS_STATIC_SLABS, ZEB_PEAKS_STATIC_SLABS / d->nb);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  ZEB_REQUIRE(e == cudaSuccess && dev >= 0 && dev < 256, ZEB_ECUDA, "correlate_peaks_static: cudaGetDevice: %s",
+              cudaGetErrorString(e));
+  float2* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_peaks_scratch);
+      ZEB_REQUIRE(e == cudaSuccess && p, ZEB_ECUDA, "correlate_peaks_static: cudaGetSymbolAddress: %s",
+                  cudaGetErrorString(e));
+      g_static_addr[dev] = (float2*)p;
+    }
+    scratch = g_static_addr[dev];
+  }
+  // every slab writes its candidate before k_peak_finish reads it: nothing needs clearing
+  SlabArgs a{};
+  a.rden = rden;
+  a.rden_div = rden_div;
+  a.cand = scratch;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = slab_launch(U, n_items, d, tw, a, false, st);
+  if (rc) return rc;
+  k_peak_finish<<<n_items, 64, 0, st>>>(a, peaks);
+  return zeb_launch_check("peak_finish");
 }
