@@ -154,10 +154,10 @@ def test_master_harmonics_match_oracle(world):
     assert ph.rules.n_fold == hm.rules.n_fold == 4
 
 
-def test_correlation_peaks_match_oracle(world, lib):
+@pytest.mark.parametrize("L", [16, 32])
+def test_correlation_peaks_match_oracle(world, lib, L):
     s = world["s"]
     e = s._e
-    L = 16
     b = e.band(L)
     fr = _frame(s)
     e.denominators(b, fr)

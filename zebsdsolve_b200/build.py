@@ -36,8 +36,28 @@ def _compile(src, obj, verbose):
     return src.name, r.stderr if verbose else ""
 
 
+def write_twiddles():
+    """csrc/twiddles.cuh: e^{-2πi t/N} for the register FFTs, from float64 rounded to float."""
+    import math
+
+    lines = ["// Twiddles e^{-2πi t/N} as float literals (written by build.py from the float64 values",
+             "// rounded to the nearest float), for the register FFTs of the slab kernel.",
+             "#pragma once", "", "namespace zeb {", ""]
+    for n in (16, 32, 64, 128, 256):
+        re = ", ".join(f"{math.cos(-2 * math.pi * t / n):.9e}f" for t in range(n))
+        im = ", ".join(f"{math.sin(-2 * math.pi * t / n):.9e}f" for t in range(n))
+        lines.append(f"__device__ constexpr float kTwRe{n}[{n}] = {{{re}}};")
+        lines.append(f"__device__ constexpr float kTwIm{n}[{n}] = {{{im}}};")
+    lines += ["", "}  // namespace zeb", ""]
+    text = "\n".join(lines)
+    path = CSRC / "twiddles.cuh"
+    if not path.exists() or path.read_text() != text:
+        path.write_text(text)
+
+
 def build(force=False, verbose=False):
     BUILD.mkdir(exist_ok=True)
+    write_twiddles()
     sources = sorted(CSRC.glob("*.cu"))
     headers = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
     newest_header = max((h.stat().st_mtime for h in headers), default=0)

@@ -14,6 +14,7 @@
 #include <mutex>
 
 #include "abi_util.cuh"
+#include "twiddles.cuh"
 
 namespace zeb {
 
@@ -109,6 +110,149 @@ __global__ void __launch_bounds__(256) k_slab(SlabArgs a) {
       if (redv[w] > bv || (redv[w] == bv && redi[w] < bi)) { bv = redv[w]; bi = redi[w]; }
     }
     a.cand[slab] = make_float2(bv, __uint_as_float(bi));
+  }
+}
+
+// ── the slab a warp at a time, its transforms in registers ──
+//
+// One warp per (item, j) slab: the slab comes in with coalesced 16-byte loads into the warp's
+// padded shared-memory tile; each lane transforms whole rows along c in registers (radix-2 with
+// compile-time twiddles), the tile goes back once, and each lane then holds one column: it forms
+// the half-length real-transform input Z_q from V[q] and V[h−q] in place, transforms it along a
+// in registers, scales by rden and keeps its column's best. The warp's best goes to `cand`.
+// No block-wide barrier: the warps of a block work on different slabs.
+
+template <int N>
+__device__ __forceinline__ float2 tw_of(int t);
+template <> __device__ __forceinline__ float2 tw_of<16>(int t) { return make_float2(kTwRe16[t], kTwIm16[t]); }
+template <> __device__ __forceinline__ float2 tw_of<32>(int t) { return make_float2(kTwRe32[t], kTwIm32[t]); }
+template <> __device__ __forceinline__ float2 tw_of<64>(int t) { return make_float2(kTwRe64[t], kTwIm64[t]); }
+template <> __device__ __forceinline__ float2 tw_of<128>(int t) { return make_float2(kTwRe128[t], kTwIm128[t]); }
+
+__host__ __device__ constexpr int brev_bits(int i, int bits) {
+  int r = 0;
+  for (int k = 0; k < bits; ++k) r |= ((i >> k) & 1) << (bits - 1 - k);
+  return r;
+}
+
+__host__ __device__ constexpr int log2_const(int n) { return n <= 1 ? 0 : 1 + log2_const(n >> 1); }
+
+// forward DFT of N points in registers (radix-2, decimation in time, natural order in and out)
+template <int N>
+__device__ __forceinline__ void fft_reg(float2 (&x)[N]) {
+  constexpr int LG = log2_const(N);
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const int j = brev_bits(i, LG);
+    if (j > i) {
+      float2 t = x[i];
+      x[i] = x[j];
+      x[j] = t;
+    }
+  }
+#pragma unroll
+  for (int s = 1; s <= LG; ++s) {
+    // every butterfly of the stage, by a flat index: constant trip counts unroll fully
+#pragma unroll
+    for (int e = 0; e < N / 2; ++e) {
+      const int h = 1 << (s - 1);
+      const int j = e & (h - 1);
+      const int i0 = ((e >> (s - 1)) << s) + j;
+      float2 b = x[i0 + h];
+      float2 t;
+      if (j == 0) {
+        t = b;
+      } else if (2 * j == h) {
+        t = make_float2(b.y, -b.x);  // × e^{−iπ/2}
+      } else {
+        t = cmulf(b, tw_of<N>(j * (N >> s)));
+      }
+      float2 a = x[i0];
+      x[i0] = make_float2(a.x + t.x, a.y + t.y);
+      x[i0 + h] = make_float2(a.x - t.x, a.y - t.y);
+    }
+  }
+}
+
+template <int NC, int H, int WARPS, int PER_SM>
+__global__ void __launch_bounds__(WARPS * 32, PER_SM) k_slab_warp(SlabArgs a) {
+  constexpr int LD = NC + 1;  // padded row (float2): rows and columns both read without conflicts
+  extern __shared__ float2 smw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* buf = smw + (size_t)warp * H * LD;
+  const int L = a.d.L, nb = a.d.nb, n = 2 * H;
+  const long long total = (long long)a.n_items * nb;
+  for (long long slab = (long long)blockIdx.x * WARPS + warp; slab < total; slab += (long long)gridDim.x * WARPS) {
+    const int b = (int)(slab / nb), j = (int)(slab - (long long)b * nb);
+    const float4* src = (const float4*)(a.U + slab * L * NC);
+    for (int e = lane; e < L * NC / 2; e += 32) {
+      float4 v = __ldcs(src + e);
+      const int f = 2 * e, r = f / NC, c = f - r * NC;
+      buf[r * LD + c] = make_float2(v.x, v.y);
+      buf[r * LD + c + 1] = make_float2(v.z, v.w);
+    }
+    __syncwarp();
+    for (int r = lane; r < L; r += 32) {
+      float2 x[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) x[c] = buf[r * LD + c];
+      fft_reg<NC>(x);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) buf[r * LD + c] = x[c];
+    }
+    __syncwarp();
+    float bv = -3.4e38f;
+    uint32_t bi = 0xffffffffu;
+    for (int c = lane; c < NC; c += 32) {
+      float2 z[H];
+#pragma unroll
+      for (int q = 0; q < H; ++q) z[q] = q < L ? buf[q * LD + c] : make_float2(0.f, 0.f);
+      // Z_q = (X_q + X_{q+h}) + i w_q (X_q − X_{q+h}), X_{q+h} = conj X_{h−q}, w_q = e^{−2πi q/n},
+      // computed for q and h − q together from the same two points (in place)
+#pragma unroll
+      for (int q = 0; q <= H / 2; ++q) {
+        const int qm = (H - q) & (H - 1);
+        float2 xq = z[q], xm = z[qm];
+        float2 zq, zm;
+        {
+          float2 x = xq, y = make_float2(0.f, 0.f);
+          if (q == 0) x.y = 0.f;
+          else y = make_float2(xm.x, -xm.y);
+          const float2 w = tw_of<2 * H>(q);
+          const float2 dd = make_float2(x.x - y.x, x.y - y.y);
+          zq = make_float2(x.x + y.x - (w.x * dd.y + w.y * dd.x), x.y + y.y + (w.x * dd.x - w.y * dd.y));
+        }
+        if (q != 0 && qm != q) {
+          float2 x = xm, y = make_float2(xq.x, -xq.y);
+          const float2 w = tw_of<2 * H>(qm);
+          const float2 dd = make_float2(x.x - y.x, x.y - y.y);
+          zm = make_float2(x.x + y.x - (w.x * dd.y + w.y * dd.x), x.y + y.y + (w.x * dd.x - w.y * dd.y));
+          z[qm] = zm;
+        }
+        z[q] = zq;
+      }
+      fft_reg<H>(z);
+      const float4* rd = (const float4*)(a.rden + (((size_t)(b / a.rden_div) * nb + j) * NC + c) * n);
+      const uint32_t base = ((uint32_t)(j * NC + c)) * n;
+#pragma unroll
+      for (int p = 0; p < H; p += 2) {
+        const float4 r = __ldg(rd + p / 2);
+        const float v0 = z[p].x * r.x, v1 = z[p].y * r.y, v2 = z[p + 1].x * r.z, v3 = z[p + 1].y * r.w;
+        const uint32_t i0 = base + 2 * p;
+        if (v0 > bv || (v0 == bv && i0 < bi)) { bv = v0; bi = i0; }
+        if (v1 > bv || (v1 == bv && i0 + 1 < bi)) { bv = v1; bi = i0 + 1; }
+        if (v2 > bv || (v2 == bv && i0 + 2 < bi)) { bv = v2; bi = i0 + 2; }
+        if (v3 > bv || (v3 == bv && i0 + 3 < bi)) { bv = v3; bi = i0 + 3; }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) a.cand[slab] = make_float2(bv, __uint_as_float(bi));
+    __syncwarp();
   }
 }
 
@@ -266,6 +410,28 @@ static int slab_launch(const float* U, int n_items, const zeb_so3_dims_t* d, con
               d->nc, smem);
   long long blocks = (long long)n_items * d->nb;
   ZEB_REQUIRE(blocks < (1LL << 31), ZEB_ESIZE, "correlate: too many slabs");
+  if (!vol && d->L <= d->n / 2) {
+    // the warp-per-slab kernels, where a lane's row and column fit in registers
+    const int H = d->n / 2, NC = d->nc;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+#define ZEB_SLAB_WARP(nc_, h_, w_, per_sm_)                                                                     \
+  if (NC == nc_ && H == h_) {                                                                                 \
+    size_t sm = (size_t)(w_) * (h_) * ((nc_) + 1) * sizeof(float2);                                          \
+    cudaFuncSetAttribute(k_slab_warp<nc_, h_, w_, per_sm_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);      \
+    long long want = (blocks + (w_)-1) / (w_);                                                                \
+    long long grid = want < (long long)sms * (per_sm_)*8 ? want : (long long)sms * (per_sm_)*8;              \
+    k_slab_warp<nc_, h_, w_, per_sm_><<<(unsigned)grid, (w_)*32, sm, st>>>(a);                                        \
+    return zeb_launch_check("correlate slab (warp)");                                                         \
+  }
+    ZEB_SLAB_WARP(16, 32, 4, 4)
+    ZEB_SLAB_WARP(32, 32, 4, 4)
+    ZEB_SLAB_WARP(64, 32, 2, 6)
+    ZEB_SLAB_WARP(32, 64, 4, 3)
+    ZEB_SLAB_WARP(64, 64, 2, 6)
+#undef ZEB_SLAB_WARP
+  }
   if (vol) {
     cudaFuncSetAttribute(k_slab<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_slab<true><<<(unsigned)blocks, 256, smem, st>>>(a);
