@@ -136,6 +136,24 @@ int zeb_spectrum_f32(const float* alm, int n_items, const zeb_so3_dims_t* d, con
 /* Bytes of U for n_items items. */
 size_t zeb_spectrum_bytes(const zeb_so3_dims_t* d, int n_items);
 
+/* The same U on the tcgen05 tensor cores (the BF16 form): BF16 operands, FP32 accumulation in
+ * tensor memory.  Every operand is split x = hi + lo into two BF16 values; for l <= split the
+ * product keeps hi*hi + hi*lo + lo*hi (near FP32), above it hi*hi (2^-9 relative per operand);
+ * split = -1: hi*hi everywhere, split >= L-1: the split product everywhere.
+ * A is the master's table packed once per phase and split by zeb_tc_pack_master from the FP64 Y
+ * of zeb_correlation_table (zeb_tc_master_bytes bytes); B is scratch of
+ * zeb_tc_patterns_bytes(d, split, n_items) bytes that this call packs from alm.  status (one
+ * int, zeroed by the caller) is left nonzero if a wait inside the kernel timed out (the kernel
+ * then returns early and U is incomplete).  Supported while K of order 0,
+ * 2L + 4(min(split, L-1) + 1), is at most 384 (L <= 64 with every order split; L <= 160 with none).
+ * Replaces Spherical.spectrum (src/spherical.zig:369-382; shaders/so3.wgsl spectrum). */
+int zeb_spectrum_bf16(const float* alm, int n_items, const zeb_so3_dims_t* d, int split, const void* A, void* B,
+                      float* U, int* status, void* stream);
+int zeb_tc_pack_master(const zeb_so3_dims_t* d, int split, const double* Y, void* A, void* stream);
+/* Bytes of A, and of B for n_items items (0 for unsupported dims). */
+size_t zeb_tc_master_bytes(const zeb_so3_dims_t* d, int split);
+size_t zeb_tc_patterns_bytes(const zeb_so3_dims_t* d, int split, int n_items);
+
 /* The correlation volume's transforms along c and a, times rden (volume b / rden_div for item
  * b), each (item, j, c) line's largest value, each item's largest, and its sub-grid vertex and
  * orientation: peaks[b] = (q.w, q.x, q.y, q.z, score, a, b, c). Replaces Spherical.correlate's

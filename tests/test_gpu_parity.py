@@ -197,6 +197,125 @@ def test_correlation_peaks_match_oracle(world, lib, L):
         assert dis < 0.05, dis
 
 
+def _spectra(lib, bt, ph, alm, n, status):
+    """U of n items in both forms (plain FP32, tensor-core BF16 at the phase's split) through the C ABI."""
+    nbytes = lib.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), n)
+    U32 = torch.empty(nbytes // 4, device="cuda")
+    lib.call("zeb_spectrum_f32", P(alm), n, ctypes.byref(ph.dims), P(ph.Y_f), P(U32), sp())
+    U16 = torch.full((nbytes // 4,), float("nan"), device="cuda")
+    B = torch.empty(lib.load().zeb_tc_patterns_bytes(ctypes.byref(ph.dims), ph.split, n), dtype=torch.uint8,
+                    device="cuda")
+    lib.call("zeb_spectrum_bf16", P(alm), n, ctypes.byref(ph.dims), ph.split, P(ph.A), P(B), P(U16), P(status), sp())
+    return U32, U16
+
+
+def _peaks(lib, bt, ph, rden, U, n):
+    peaks = torch.empty(n * 8, device="cuda")
+    cand = torch.empty(lib.load().zeb_peaks_scratch_bytes(ctypes.byref(ph.dims), n) // 4 + 1, device="cuda")
+    lib.call("zeb_correlate_peaks", P(U), n, ctypes.byref(ph.dims), P(bt.tw), P(rden), 1 << 30, P(peaks), P(cand), sp())
+    return peaks.cpu().numpy().reshape(n, 8)
+
+
+def _refined(lib, e, fr, pd, items, seeds, n):
+    """Records after 8 refinement iterations from the given peaks (the engine's own settings)."""
+    p = e.phases[0]
+    recs = torch.empty(n * 8, device="cuda")
+    opts = lib.RefineOpts(8, math.radians(2.0), 1.0, 0.02, 1e4, 16, 7.0)
+    sd = torch.as_tensor(seeds.astype(np.float32), device="cuda").reshape(-1)
+    lib.call("zeb_refine", P(pd), P(items), P(sd), 8, n, ctypes.byref(fr), P(p.baked[1]), P(p.baked[2]), p.master.side,
+             ctypes.byref(opts), P(recs), sp())
+    return recs.cpu().numpy().reshape(n, 8)
+
+
+@pytest.mark.parametrize("L,precision", [(32, "bf16x3"), (64, "bf16x3"), (32, "bf16"), (64, "bf16")])
+def test_bf16_spectrum_matches_fp32_and_oracle(world, lib, L, precision):
+    """The tensor-core spectrum (BF16 operands, FP32 accumulation) against the plain FP32 one and,
+    at L = 32, the FP64 oracle.  bf16x3 (every order split hi/lo): U within 5e-5 of its largest
+    magnitude, the peak score within 1e-4 and its orientation within 0.05 deg, as the FP32 form.
+    bf16 (split for l <= 16, hi*hi above): U within 4e-3, the peak score within 1e-3; a peak may
+    land in the other cell of a near tie, so orientations are compared after refinement
+    (within 0.1 deg, NCC within 1e-3)."""
+    from zebsdsolve_b200 import device
+
+    s = world["s"]
+    e = s._e
+    b = e.band(L)
+    fr = _frame(s)
+    e.denominators(b, fr)
+    bt = b["tables"]
+    ph32 = b["phases"][0][1]
+    p = e.phases[0]
+    ph = device.PhaseBand(bt, p.baked[1], p.master.side, L, precision)
+    assert ph.A is not None and torch.equal(ph.Y_f, ph32.Y_f)
+    full = precision == "bf16x3"
+    n = world["pats"].shape[0]
+    pats = torch.as_tensor(world["pats"].astype(np.float32), device="cuda").reshape(-1)
+    t = e.positions(np.arange(n))
+    items = torch.as_tensor(np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1), device="cuda")
+    alm = torch.empty(n * bt.n_pairs * 2, dtype=torch.float32, device="cuda")
+    stats = torch.empty(n * 4, dtype=torch.float32, device="cuda")
+    scr = torch.empty(lib.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), n) // 4 + 1, device="cuda")
+    lib.call("zeb_sphere_coefficients", P(pats), P(items), n, ctypes.byref(fr), ctypes.byref(bt.st), 3, P(alm), P(stats),
+             P(scr), sp())
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    U32, U16 = _spectra(lib, bt, ph, alm, n, status)
+    assert int(status.item()) == 0
+    a32, a16 = U32.cpu().numpy(), U16.cpu().numpy()
+    assert np.isfinite(a16).all()
+    scale = np.abs(a32).max()
+    err = np.abs(a16 - a32).max() / scale
+    rms = np.sqrt(np.mean((a16 - a32) ** 2)) / np.sqrt(np.mean(a32 ** 2))
+    print(f"L={L} {precision}: U max error {err:.2e} of max, rms {rms:.2e}")
+    assert err < (5e-5 if full else 4e-3), err
+    assert rms < (5e-5 if full else 3e-3), rms
+
+    g32 = _peaks(lib, bt, ph, ph32.rden, U32, n)
+    g16 = _peaks(lib, bt, ph, ph32.rden, U16, n)
+    ops = world["m_or"].rotations()
+
+    def dis(q1, q2):
+        return math.degrees(float(osym.disorientation(q1.astype(np.float64), q2.astype(np.float64), ops)))
+
+    for i in range(n):
+        print(f"  item {i}: score {g16[i, 4]:.6f} vs {g32[i, 4]:.6f}, {dis(g16[i, :4], g32[i, :4]):.4f} deg")
+        assert abs(g16[i, 4] - g32[i, 4]) < (1e-4 if full else 1e-3), (g16[i, 4], g32[i, 4])
+        if full:
+            assert dis(g16[i, :4], g32[i, :4]) < 0.05
+    if not full:
+        pd = e.preprocess(torch.as_tensor(world["pats"].astype(np.float32), device="cuda"), n)
+        r32 = _refined(lib, e, fr, pd, items, g32, n)
+        r16 = _refined(lib, e, fr, pd, items, g16, n)
+        for i in range(n):
+            assert abs(r16[i, 4] - r32[i, 4]) < 1e-3, (r16[i, 4], r32[i, 4])
+            assert dis(r16[i, :4], r32[i, :4]) < 0.1, dis(r16[i, :4], r32[i, :4])
+    if L == 32:
+        tb = osp.Tables(L)
+        hm = om.Harmonics(world["m_or"], world["baked"], L)
+        pt = osp.PhaseTables(tb, hm, om.fold_of(hm.rules))
+        frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
+        walm, wst = osp.coefficients(tb, None, e.geo.translation(60, 60), frame, np.array(fr.mask),
+                                     flags=osp.FLAG_WINDOW, shape=(60, 60))
+        rden = osp.window_denominators(tb, pt, walm, wst[0])
+        for i in range(n):
+            g, _ = osp.coefficients(tb, world["pats"][i].astype(np.float64), t[i].astype(np.float64), frame,
+                                    np.array(fr.mask))
+            vol = osp.correlation_volume(tb, pt, hm.f, g) * rden
+            q, v0, abc, idx = osp.peak(tb, pt, vol)
+            assert abs(g16[i, 4] - v0) < (2e-4 if full else 1e-3), (g16[i, 4], v0)
+            if full:
+                assert dis(g16[i, :4], q) < 0.05
+
+    # several pattern tiles, the last one ragged: 300 items = the 6 coefficient sets repeated
+    m = 300
+    big = alm[: n * bt.n_pairs * 2].view(n, -1).repeat(m // n, 1).reshape(-1).contiguous()
+    V32, V16 = _spectra(lib, bt, ph, big, m, status)
+    assert int(status.item()) == 0
+    v32 = V32.view(m, -1)
+    v16 = V16.view(m, -1)
+    assert torch.equal(v16[:n].repeat(m // n, 1), v16), "tiles disagree on equal inputs"
+    assert float((v16 - v32).abs().max()) < (5e-5 if full else 4e-3) * float(v32.abs().max())
+
+
 def test_refine_and_nmi_match_oracle(world, lib):
     s = world["s"]
     e = s._e

@@ -59,6 +59,10 @@ _SIGS = {
     "zeb_correlation_table": ([ctypes.POINTER(So3Dims), P, P, P, P], c_int),
     "zeb_spectrum_f32": ([P, c_int, ctypes.POINTER(So3Dims), P, P, P], c_int),
     "zeb_spectrum_bytes": ([ctypes.POINTER(So3Dims), c_int], c_size_t),
+    "zeb_spectrum_bf16": ([P, c_int, ctypes.POINTER(So3Dims), c_int, P, P, P, P, P], c_int),
+    "zeb_tc_pack_master": ([ctypes.POINTER(So3Dims), c_int, P, P, P], c_int),
+    "zeb_tc_master_bytes": ([ctypes.POINTER(So3Dims), c_int], c_size_t),
+    "zeb_tc_patterns_bytes": ([ctypes.POINTER(So3Dims), c_int, c_int], c_size_t),
     "zeb_peaks_scratch_bytes": ([ctypes.POINTER(So3Dims), c_int], c_size_t),
     "zeb_correlate_peaks": ([P, c_int, ctypes.POINTER(So3Dims), P, P, c_int, P, P, P], c_int),
     "zeb_correlate_peaks_static": ([P, c_int, ctypes.POINTER(So3Dims), P, P, c_int, P, P], c_int),
@@ -74,7 +78,7 @@ ZEB_PEAKS_STATIC_SLABS = 1 << 19  # include/zebsdsolve_b200.h
 
 # kernels each entry point launches (for the launch counts the benchmark reports)
 KERNELS = {"zeb_prep": 1, "zeb_prep_ex": 1, "zeb_sphere_coefficients": 3, "zeb_spectrum_f32": 1,
-           "zeb_spectrum_bf16": 1, "zeb_correlate_peaks": 2, "zeb_correlate_peaks_static": 2, "zeb_correlate_volume": 1, "zeb_rden_build": 1,
+           "zeb_spectrum_bf16": 2, "zeb_tc_pack_master": 0, "zeb_correlate_peaks": 2, "zeb_correlate_peaks_static": 2, "zeb_correlate_volume": 1, "zeb_rden_build": 1,
            "zeb_refine": 1, "zeb_chance": 1, "zeb_project": 1, "zeb_master_blur_pass": 1, "zeb_master_gradient": 1,
            "zeb_master_sample_grid": 1, "zeb_gauss_legendre": 1, "zeb_legendre_table": 1, "zeb_wigner_half_pi": 1,
            "zeb_correlation_table": 1}

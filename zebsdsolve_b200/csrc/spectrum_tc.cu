@@ -1,0 +1,567 @@
+// (b, first stage) The spectrum GEMM on the tcgen05 tensor cores: BF16 operands, FP32
+// accumulation in tensor memory (TMEM).
+//
+//   U[b][j][m'][iq] = Σ_l conj(g_b[l,m']) · Y[pair(m',l)][j·nc + iq]
+//
+// as one real GEMM per order m':  D[ν][b] = Σ_κ A_m'[ν][κ] · B_m'[b][κ], with ν = 2(j·nc+iq) + (re|im)
+// (the rows, M) and κ = 2(l−m') + (re|im) (the reduction, K):
+//   A[2n][2l'] = Re Y,  A[2n][2l'+1] = Im Y,  A[2n+1][2l'] = Im Y,  A[2n+1][2l'+1] = −Re Y
+//   B[b][2l'] = Re g,   B[b][2l'+1] = Im g
+// (conj(g)·Y = (gr·Yr + gi·Yi) + i(gr·Yi − gi·Yr)).
+//
+// Accuracy: every operand is split x = hi + lo into two BF16 values; for the orders l ≤ split
+// (the low orders, which carry most of the energy of a pattern and of a master) the product takes
+// hi·hi + hi·lo + lo·hi, as two more K segments of the same GEMM (K' = K + 2·K_split); above,
+// hi·hi alone (2^-9 relative per operand).  split = 16 keeps the low orders near FP32; split =
+// L − 1 makes the whole product so (relative error ~2^-16).  A per-order scale would only shift
+// exponents, of which BF16 has as many as FP32, so none is applied.
+//
+// Operands live in HBM already in the shared-memory layout the MMA reads (K-major, 128-byte
+// rows, the 16-byte chunks of row r XOR-swizzled by r mod 8, 8-row groups 1024 B apart), in
+// blocks of 64 K-elements: a block is one bulk async copy. The master's A is built once per phase
+// (k_pack_master, FP64 → BF16 hi/lo); the patterns' B per batch (k_pack_patterns).
+//
+// k_spectrum_tc: one CTA per (pattern tile of 128, order m'), 6 warps: warp 0 issues the bulk
+// copies (B once, then A block by block through a ring of TC_STAGES), warp 1 allocates TMEM and one of
+// its threads issues the MMAs (M = 128 rows of ν, N = 128 patterns, K = 16 a step) into two
+// accumulators of 128 columns, warps 2-5 drain an accumulator (tcgen05.ld) while the next one
+// fills, staging 32 patterns at a time in shared memory for a tensor store into U (scattered
+// 128-byte stores from four warps cap an SM near 13 GB/s; the tensor store does not). Every wait is bounded: on a timeout the CTA records the failure, drains what it
+// issued, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
+#include "abi_util.cuh"
+
+namespace zeb {
+
+constexpr int TC_BN = 128;            // patterns per tile (MMA N)
+constexpr int TC_BM = 128;            // rows ν per tile (MMA M)
+constexpr int TC_KB = 64;             // K-elements per block (one 128-byte swizzled row)
+constexpr int TC_A_BLOCK = TC_BM * 128;  // bytes of one A block (16 KB)
+constexpr int TC_B_BLOCK = TC_BN * 128;  // bytes of one B block (16 KB)
+constexpr int TC_MAX_KB = 6;          // K' ≤ 384: B stays resident (96 KB)
+constexpr int TC_STAGES = 5;          // A ring: 5 blocks of 16 KB
+constexpr int TC_THREADS = 192;
+
+// K' of order m': 2(L − m') + 4·(number of l in [m', split])
+__host__ __device__ inline int tc_k0(int L, int mp) { return 2 * (L - mp); }
+__host__ __device__ inline int tc_k1(int L, int mp, int split) {
+  int hi = split < L - 1 ? split : L - 1;
+  return mp <= hi ? 2 * (hi - mp + 1) : 0;
+}
+__host__ __device__ inline int tc_kblocks(int L, int mp, int split) {
+  int k = tc_k0(L, mp) + 2 * tc_k1(L, mp, split);
+  return (k + TC_KB - 1) / TC_KB;
+}
+
+// byte offset of element (row, k) inside a swizzled block of 128-byte rows
+__device__ __forceinline__ uint32_t sw128(int row, int k) {
+  const int chunk = (k >> 3) ^ (row & 7);
+  return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + chunk * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+__device__ __forceinline__ float bf16_value(uint16_t b) { return __bfloat162float(__ushort_as_bfloat16(b)); }
+
+// (segment, l, re|im) of K-element κ of order m' (segment 0: hi·hi over all l; 1: hi(A)·lo(B) for
+// l ≤ split; 2: lo(A)·hi(B) for l ≤ split; 3: padding)
+struct KSlot {
+  int seg, l, part;
+};
+__device__ __forceinline__ KSlot k_slot(int L, int mp, int split, int k) {
+  const int k0 = tc_k0(L, mp), k1 = tc_k1(L, mp, split);
+  KSlot s;
+  if (k < k0) {
+    s.seg = 0; s.l = mp + (k >> 1); s.part = k & 1;
+  } else if (k < k0 + k1) {
+    s.seg = 1; s.l = mp + ((k - k0) >> 1); s.part = (k - k0) & 1;
+  } else if (k < k0 + 2 * k1) {
+    s.seg = 2; s.l = mp + ((k - k0 - k1) >> 1); s.part = (k - k0 - k1) & 1;
+  } else {
+    s.seg = 3; s.l = 0; s.part = 0;
+  }
+  return s;
+}
+
+struct TcLayout {
+  int L, nb, nc, rows, mtiles, ptiles, split;
+};
+
+// byte offset of order m''s blocks: Σ over the lower orders of tiles · K-blocks · block bytes
+__host__ __device__ inline long long tc_offset(int L, int split, int mp, int tiles, int block_bytes) {
+  long long o = 0;
+  for (int q = 0; q < mp; ++q) o += (long long)tiles * tc_kblocks(L, q, split) * block_bytes;
+  return o;
+}
+
+// A_m'[ν][κ] from Y (FP64 complex [pair][nb·nc]), one thread per 16-byte chunk of a block row.
+__global__ void k_pack_master(const double2* __restrict__ Y, TcLayout t, int mp, long long a_off,
+                              uint8_t* __restrict__ A) {
+  const int kb = tc_kblocks(t.L, mp, t.split);
+  const long long chunks = (long long)t.mtiles * kb * TC_BM * 8;
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= chunks) return;
+  const int c16 = (int)(e & 7);
+  const int row = (int)((e >> 3) % TC_BM);
+  const long long blk = (e >> 3) / TC_BM;  // mtile·kb + kblock
+  const int kblock = (int)(blk % kb), mtile = (int)(blk / kb);
+  const int nu = mtile * TC_BM + row;
+  const int ncols = t.nb * t.nc;
+  const int p0 = mp * t.L - (mp * (mp - 1)) / 2;
+  uint16_t v[8];
+  for (int i = 0; i < 8; ++i) {
+    const int k = kblock * TC_KB + c16 * 8 + i;
+    KSlot s = k_slot(t.L, mp, t.split, k);
+    float out = 0.f;
+    if (s.seg < 3 && nu < 2 * ncols) {
+      const double2 y = Y[(size_t)(p0 + s.l - mp) * ncols + (nu >> 1)];
+      // rows re: (Yr, Yi); rows im: (Yi, −Yr)
+      double val = (nu & 1) == 0 ? (s.part == 0 ? y.x : y.y) : (s.part == 0 ? y.y : -y.x);
+      float hi = bf16_value(bf16_bits((float)val));
+      out = s.seg == 2 ? (float)(val - (double)hi) : (float)val;
+    }
+    v[i] = bf16_bits(out);
+  }
+  uint8_t* blkp = A + a_off + (size_t)blk * TC_A_BLOCK;
+  uint4 w;
+  w.x = v[0] | ((uint32_t)v[1] << 16);
+  w.y = v[2] | ((uint32_t)v[3] << 16);
+  w.z = v[4] | ((uint32_t)v[5] << 16);
+  w.w = v[6] | ((uint32_t)v[7] << 16);
+  *(uint4*)(blkp + sw128(row, c16 * 8)) = w;
+}
+
+// B_m'[b][κ] from the coefficients (complex f32 [b][pair]), every order, one thread per chunk.
+__global__ void k_pack_patterns(const float2* __restrict__ alm, int n_items, int n_pairs, TcLayout t,
+                                uint8_t* __restrict__ B) {
+  const int mp = blockIdx.y;
+  __shared__ long long b_off;
+  if (threadIdx.x == 0) b_off = tc_offset(t.L, t.split, mp, t.ptiles, TC_B_BLOCK);
+  __syncthreads();
+  const int kb = tc_kblocks(t.L, mp, t.split);
+  const long long chunks = (long long)t.ptiles * kb * TC_BN * 8;
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= chunks) return;
+  const int c16 = (int)(e & 7);
+  const int row = (int)((e >> 3) % TC_BN);
+  const long long blk = (e >> 3) / TC_BN;  // ptile·kb + kblock
+  const int kblock = (int)(blk % kb), ptile = (int)(blk / kb);
+  const int b = ptile * TC_BN + row;
+  const int p0 = mp * t.L - (mp * (mp - 1)) / 2;
+  uint16_t v[8];
+  for (int i = 0; i < 8; ++i) {
+    const int k = kblock * TC_KB + c16 * 8 + i;
+    KSlot s = k_slot(t.L, mp, t.split, k);
+    float out = 0.f;
+    if (s.seg < 3 && b < n_items) {
+      const float2 g = alm[(size_t)b * n_pairs + p0 + s.l - mp];
+      const float x = s.part == 0 ? g.x : g.y;
+      const float hi = bf16_value(bf16_bits(x));
+      out = s.seg == 1 ? x - hi : x;  // the lo part pairs with A's hi in segment 1
+    }
+    v[i] = bf16_bits(out);
+  }
+  uint8_t* blkp = B + b_off + (size_t)blk * TC_B_BLOCK;
+  uint4 w;
+  w.x = v[0] | ((uint32_t)v[1] << 16);
+  w.y = v[2] | ((uint32_t)v[3] << 16);
+  w.z = v[4] | ((uint32_t)v[5] << 16);
+  w.w = v[6] | ((uint32_t)v[7] << 16);
+  *(uint4*)(blkp + sw128(row, c16 * 8)) = w;
+}
+
+// ── PTX helpers ──
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  // the hint lets the thread sleep until the phase completes (or ~20 µs pass) instead of spinning
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(20000u)
+      : "memory");
+  return done != 0;
+}
+
+// wait for the phase of parity `parity` to complete; false once `limit_ns` nanoseconds have passed
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit_ns) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 63) == 0 && (long long)(global_ns() - t0) > limit_ns) return false;
+  }
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+// K-major, 128-byte swizzle, 8-row groups 1024 B apart (the canonical layout the blocks are in)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);        // start address
+  d |= (uint64_t)1 << 16;                         // leading byte offset (unused for this layout)
+  d |= (uint64_t)(1024 >> 4) << 32;               // stride byte offset: 8 rows
+  d |= (uint64_t)1 << 46;                         // descriptor version (sm100)
+  d |= (uint64_t)2 << 61;                         // 128-byte swizzle
+  return d;
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accum));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
+#define TMEM_LD32(taddr, r)                                                                                       \
+  asm volatile(                                                                                                   \
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18," \
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                             \
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), \
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),      \
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),     \
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                   \
+      : "r"(taddr))
+
+// a barrier over `count` threads that also ANDs a predicate across them
+__device__ __forceinline__ bool bar_and(int id, int count, bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, %2, %3, q;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)v), "r"(id), "r"(count)
+      : "memory");
+  return out != 0;
+}
+__device__ __forceinline__ void bar_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+// 4-D tensor store of a staging buffer (bulk async group) and its group bookkeeping
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, const void* src, int c0, int c1, int c2, int c3) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(
+                   (uint64_t)map),
+               "r"(smem_addr(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+struct TcArgs {
+  TcLayout t;
+  const uint8_t* A;
+  const uint8_t* B;
+  int n_items;
+  float2* U;
+  int* status;      // nonzero after a timed-out wait (what the CTA was waiting on)
+  long long limit;  // nanoseconds before a wait gives up
+  int per;          // row tiles per CTA (blockIdx.z picks the group)
+};
+
+struct TcShared {
+  uint8_t b[TC_MAX_KB][TC_B_BLOCK];   // 96 KB, 1024-aligned
+  uint8_t a[TC_STAGES][TC_A_BLOCK];   // 80 KB
+  float stage[2][32 * TC_BM];          // 2 × 16 KB: a 32-pattern chunk of the tile, [pattern][row]
+  uint64_t b_full, a_full[TC_STAGES], a_empty[TC_STAGES], acc_full[2], acc_empty[2], mma_done;
+  long long a_off, b_off;
+  uint32_t tmem;
+  int failed;
+};
+
+__global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const __grid_constant__ CUtensorMap umap) {
+  extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
+  TcShared& s = *reinterpret_cast<TcShared*>((void*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ptile = blockIdx.x, mp = blockIdx.y;
+  const TcLayout& t = a.t;
+  const int kb = tc_kblocks(t.L, mp, t.split);
+  // this CTA's row tiles: [mt0, mt0 + mtiles) of the order's t.mtiles
+  const int mt0 = blockIdx.z * a.per;
+  const int mtiles = max(0, min(t.mtiles - mt0, a.per));
+  if (threadIdx.x == 0) {
+    mbar_init(&s.b_full, 1);
+    mbar_init(&s.mma_done, 1);
+    s.a_off = tc_offset(t.L, t.split, mp, t.mtiles, TC_A_BLOCK);
+    s.b_off = tc_offset(t.L, t.split, mp, t.ptiles, TC_B_BLOCK);
+    for (int i = 0; i < TC_STAGES; ++i) {
+      mbar_init(&s.a_full[i], 1);
+      mbar_init(&s.a_empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&s.acc_full[i], 1);
+      mbar_init(&s.acc_empty[i], 4);
+    }
+    s.failed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s.tmem)),
+                 "r"(2 * TC_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s.tmem;
+  const long long lim = a.limit;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // B once; then A block by block through the ring (block it of the CTA goes to stage it mod S)
+      const uint8_t* bsrc = a.B + s.b_off + (size_t)ptile * kb * TC_B_BLOCK;
+      mbar_expect_tx(&s.b_full, kb * TC_B_BLOCK);
+      for (int k = 0; k < kb; ++k) bulk_g2s(s.b[k], bsrc + (size_t)k * TC_B_BLOCK, TC_B_BLOCK, &s.b_full);
+      const uint8_t* asrc = a.A + s.a_off + (size_t)mt0 * kb * TC_A_BLOCK;
+      const int total = mtiles * kb;  // this CTA's blocks of the order's A, [mtile][kblock]
+      int it = 0;
+      for (; it < total; ++it) {
+        const int st = it % TC_STAGES;
+        if (!mbar_wait(&s.a_empty[st], ((it / TC_STAGES) & 1) ^ 1, lim)) break;
+        mbar_expect_tx(&s.a_full[st], TC_A_BLOCK);
+        bulk_g2s(s.a[st], asrc + (size_t)it * TC_A_BLOCK, TC_A_BLOCK, &s.a_full[st]);
+      }
+      if (it < total) {
+        atomicOr(a.status, 1);
+        s.failed = 1;
+        // the copies still in flight land before the CTA may leave (bounded waits on their phases)
+        mbar_wait(&s.b_full, 0, lim);
+        for (int i = (it > TC_STAGES ? it - TC_STAGES : 0); i < it; ++i)
+          mbar_wait(&s.a_full[i % TC_STAGES], (i / TC_STAGES) & 1, lim);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // kind::f16: F32 accumulate, BF16 A and B, both K-major, N = 128, M = 128
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+      bool ok = mbar_wait(&s.b_full, 0, lim);
+      int it = 0;
+      for (int mt = 0; mt < mtiles && ok; ++mt) {
+        const int acc = mt & 1;
+        ok = mbar_wait(&s.acc_empty[acc], ((mt >> 1) & 1) ^ 1, lim);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + (uint32_t)(acc * TC_BN);
+        for (int k = 0; k < kb; ++k, ++it) {
+          const int st = it % TC_STAGES;
+          ok = mbar_wait(&s.a_full[st], (it / TC_STAGES) & 1, lim);
+          if (!ok) break;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t abase = smem_addr(s.a[st]), bbase = smem_addr(s.b[k]);
+#pragma unroll
+          for (int ks = 0; ks < TC_KB / 16; ++ks)
+            umma_f16(d, umma_desc(abase + ks * 32), umma_desc(bbase + ks * 32), idesc, (k | ks) != 0);
+          umma_commit(&s.a_empty[st]);  // the stage is free once these MMAs have read it
+        }
+        if (!ok) break;
+        umma_commit(&s.acc_full[acc]);
+      }
+      if (!ok) {
+        atomicOr(a.status, 2);
+        s.failed = 1;
+      }
+      // every MMA issued has finished before TMEM may be freed
+      umma_commit(&s.mma_done);
+      if (!mbar_wait(&s.mma_done, 0, lim)) atomicOr(a.status, 8);
+    }
+  } else {
+    // epilogue (warps 2-5): a warp may reach only its TMEM lane quadrant, so warp w drains tile
+    // rows 32·(w mod 4) …  Each 32-pattern chunk goes TMEM → registers → a staging buffer laid
+    // out [pattern][row] (the tensor-store box: rows ν of a tile are whole (j, m') lines of U)
+    // → one 16 KB tensor store; rows and patterns past the ends are clipped by the store.
+    const int ew = warp & 3;
+    const int row = ew * 32 + lane;
+    const bool leader = warp == 2 && lane == 0;
+    const int two_nc = 2 * t.nc;
+    int chunk = 0;
+    for (int mt = 0; mt < mtiles; ++mt) {
+      const int acc = mt & 1;
+      // the four warps agree on the outcome (a barrier that ANDs their results)
+      if (!bar_and(1, 128, mbar_wait(&s.acc_full[acc], (mt >> 1) & 1, lim))) {
+        if (leader) {
+          atomicOr(a.status, 4);
+          s.failed = 1;
+        }
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int r0 = (mt0 + mt) * TC_BM;  // first row ν of the tile
+      const int j0 = r0 / two_nc, x0 = two_nc <= TC_BM ? 0 : r0 % two_nc;
+#pragma unroll 1
+      for (int c0 = 0; c0 < TC_BN; c0 += 32, ++chunk) {
+        uint32_t v[32];
+        TMEM_LD32(tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(acc * TC_BN + c0), v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (c0 + 32 == TC_BN) {  // the accumulator is read out: the next tile's MMAs may start
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&s.acc_empty[acc]);
+        }
+        float* stg = s.stage[chunk & 1];
+        if (leader) bulk_wait_read1();  // the store that last used this buffer has read it
+        bar_sync(1, 128);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) stg[c * TC_BM + row] = __uint_as_float(v[c]);
+        fence_proxy_async();
+        bar_sync(1, 128);
+        if (leader) {
+          if (ptile * TC_BN + c0 < a.n_items) tma_store_4d(&umap, stg, x0, mp, j0, ptile * TC_BN + c0);
+          bulk_commit();
+        }
+      }
+    }
+    if (leader) bulk_wait_all();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_BN));
+}
+
+}  // namespace zeb
+
+using namespace zeb;
+
+static bool tc_dims_ok(const zeb_so3_dims_t* d, int split) {
+  return d && d->L >= 2 && d->L <= 256 && d->n >= 2 * d->L - 1 && d->nb == d->n / 2 + 1 && d->fold >= 1 &&
+         d->nc == d->n / d->fold && d->mu_max == (d->L - 1) / d->fold && d->n_pairs == d->L * (d->L + 1) / 2 &&
+         split >= -1 && tc_kblocks(d->L, 0, split) <= TC_MAX_KB;
+}
+
+static TcLayout tc_layout(const zeb_so3_dims_t* d, int split, int n_items) {
+  TcLayout t{};
+  t.L = d->L; t.nb = d->nb; t.nc = d->nc; t.rows = 2 * d->nb * d->nc;
+  t.mtiles = (t.rows + TC_BM - 1) / TC_BM;
+  t.ptiles = (n_items + TC_BN - 1) / TC_BN;
+  t.split = split;
+  return t;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tc_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// U as a 4-D tensor [item][j][m'][2·nc floats]; the box is one tile's rows for 32 items
+static bool tc_u_map(CUtensorMap* m, float* U, const zeb_so3_dims_t* d, int n_items) {
+  auto fn = tc_encode_fn();
+  if (!fn) return false;
+  const cuuint64_t two_nc = 2 * (cuuint64_t)d->nc;
+  cuuint64_t dims[4] = {two_nc, (cuuint64_t)d->L, (cuuint64_t)d->nb, (cuuint64_t)n_items};
+  cuuint64_t strides[3] = {two_nc * 4, two_nc * 4 * d->L, two_nc * 4 * d->L * d->nb};
+  cuuint32_t box[4] = {(cuuint32_t)(two_nc <= TC_BM ? two_nc : TC_BM), 1,
+                       (cuuint32_t)(two_nc <= TC_BM ? TC_BM / two_nc : 1), 32};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, U, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+extern "C" size_t zeb_tc_master_bytes(const zeb_so3_dims_t* d, int split) {
+  if (!tc_dims_ok(d, split)) return 0;
+  TcLayout t = tc_layout(d, split, 1);
+  return (size_t)tc_offset(d->L, split, d->L, t.mtiles, TC_A_BLOCK);
+}
+
+extern "C" size_t zeb_tc_patterns_bytes(const zeb_so3_dims_t* d, int split, int n_items) {
+  if (!tc_dims_ok(d, split) || n_items <= 0) return 0;
+  TcLayout t = tc_layout(d, split, n_items);
+  return (size_t)tc_offset(d->L, split, d->L, t.ptiles, TC_B_BLOCK);
+}
+
+extern "C" int zeb_tc_pack_master(const zeb_so3_dims_t* d, int split, const double* Y, void* A, void* stream) {
+  ZEB_REQUIRE(Y && A, ZEB_EARG, "tc_pack_master: null argument");
+  ZEB_REQUIRE(tc_dims_ok(d, split), ZEB_EARG, "tc_pack_master: unsupported dims (L=%d, split=%d)", d ? d->L : -1,
+              split);
+  TcLayout t = tc_layout(d, split, 1);
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int mp = 0; mp < d->L; ++mp) {
+    long long chunks = (long long)t.mtiles * tc_kblocks(d->L, mp, split) * TC_BM * 8;
+    k_pack_master<<<(unsigned)((chunks + 255) / 256), 256, 0, st>>>(
+        (const double2*)Y, t, mp, tc_offset(d->L, split, mp, t.mtiles, TC_A_BLOCK), (uint8_t*)A);
+  }
+  return zeb_launch_check("tc_pack_master");
+}
+
+extern "C" int zeb_spectrum_bf16(const float* alm, int n_items, const zeb_so3_dims_t* d, int split, const void* A,
+                                 void* B, float* U, int* status, void* stream) {
+  ZEB_REQUIRE(alm && A && B && U && status, ZEB_EARG, "spectrum_bf16: null argument");
+  ZEB_REQUIRE(tc_dims_ok(d, split), ZEB_EARG, "spectrum_bf16: unsupported dims (L=%d, split=%d)", d ? d->L : -1,
+              split);
+  if (n_items <= 0) return ZEB_OK;
+  TcLayout t = tc_layout(d, split, n_items);
+  cudaStream_t st = (cudaStream_t)stream;
+  long long chunks = (long long)t.ptiles * tc_kblocks(d->L, 0, split) * TC_BN * 8;
+  dim3 gp((unsigned)((chunks + 255) / 256), d->L);
+  k_pack_patterns<<<gp, 256, 0, st>>>((const float2*)alm, n_items, d->n_pairs, t, (uint8_t*)B);
+  int rc = zeb_launch_check("pack_patterns");
+  if (rc) return rc;
+  CUtensorMap umap;
+  ZEB_REQUIRE(((uintptr_t)U & 15) == 0, ZEB_EARG, "spectrum_bf16: U must be 16-byte aligned");
+  ZEB_REQUIRE(tc_u_map(&umap, U, d, n_items), ZEB_ECUDA, "spectrum_bf16: tensor map for U refused");
+  TcArgs a{};
+  a.t = t; a.A = (const uint8_t*)A; a.B = (const uint8_t*)B; a.n_items = n_items; a.U = (float2*)U;
+  a.status = status;
+  a.limit = 1000000000LL;  // 1 s: far above any legitimate wait inside one CTA
+  size_t smem = sizeof(TcShared) + 1024;
+  cudaFuncSetAttribute(k_spectrum_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // enough CTAs for several waves: row tiles split into groups when the pattern tiles are few
+  int sms = 148;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const long long base = (long long)t.ptiles * d->L;
+  int groups = (int)std::min<long long>(t.mtiles, (8LL * sms + base - 1) / base);
+  groups = std::max(1, std::min(groups, 65535));
+  a.per = (t.mtiles + groups - 1) / groups;
+  groups = (t.mtiles + a.per - 1) / a.per;  // no empty group: every CTA has at least one row tile
+  dim3 g(t.ptiles, d->L, groups);
+  k_spectrum_tc<<<g, TC_THREADS, smem, st>>>(a, umap);
+  return zeb_launch_check("spectrum_bf16");
+}

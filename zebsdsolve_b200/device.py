@@ -150,8 +150,23 @@ class PhaseBand:
         self.fold = {4: 4, 2: 2, 6: 2}.get(self.rules.n_fold, 1)
         n = bt.n
         self.dims = N.So3Dims(L, n, n // 2 + 1, n // self.fold, self.fold, (L - 1) // self.fold, bt.n_pairs)
-        self.Y_f = self._table(bt, f)
+        self.Y_f, Y64 = self._table(bt, f, keep=True)
         self.Y_f2 = self._table(bt, f2)
+        # the BF16 forms: the master's table split and packed once for the tensor-core spectrum
+        # (hi/lo BF16 pairs from the FP64 table, in the shared-memory layout the MMA reads)
+        from .settings import SPLIT_L
+
+        self.A = None
+        self.split = None
+        if SPLIT_L.get(precision) is not None:
+            self.split = min(SPLIT_L[precision], L - 1)
+            nbytes = N.load().zeb_tc_master_bytes(ctypes.byref(self.dims), self.split)
+            if nbytes == 0:
+                raise N.NativeError(f"precision {precision}: bandwidth {L} is beyond the tensor-core spectrum")
+            self.A = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            N.call("zeb_tc_pack_master", ctypes.byref(self.dims), self.split, ptr(torch.view_as_real(Y64)),
+                   ptr(self.A), stream_ptr())
+        del Y64
         self.rden = None
         self.rden_key = None
 
@@ -182,13 +197,15 @@ class PhaseBand:
         W = ph[:, None, None] * F[:, :, None] * D.permute(0, 2, 1).to(torch.complex128)  # [mi][l][k]
         return W.contiguous()
 
-    def _table(self, bt, coef):
+    def _table(self, bt, coef, keep=False):
+        """The FP32 table (and with keep, the FP64 one it was rounded from)."""
         W = self.weights(bt, coef)
         d = self.dims
         Y = torch.empty(bt.n_pairs, d.nb * d.nc, dtype=torch.complex128, device=coef.device)
         N.call("zeb_correlation_table", ctypes.byref(d), ptr(torch.view_as_real(W)), ptr(bt.wigner),
                ptr(torch.view_as_real(Y)), stream_ptr())
-        return torch.view_as_real(Y.to(torch.complex64)).contiguous()
+        Yf = torch.view_as_real(Y.to(torch.complex64)).contiguous()
+        return (Yf, Y) if keep else Yf
 
     def volume_cells(self):
         d = self.dims

@@ -335,7 +335,7 @@ class Engine:
             vols = []
             for Y in (ph.Y_f, ph.Y_f2):
                 U = self.buf("spec_window", N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), 1) // 4 + 1)
-                self.spectrum(alm, 1, ph, Y, U)
+                self.spectrum(alm, 1, ph, Y, U, tensor_cores=False)
                 vol = torch.empty(cells, dtype=torch.float32, device=self.dev)
                 N.call("zeb_correlate_volume", ptr(U), 1, ctypes.byref(ph.dims), ptr(bt.tw), ptr(vol), stream_ptr())
                 vols.append(vol)
@@ -344,8 +344,32 @@ class Engine:
             ph.rden = rden
             ph.rden_key = key
 
-    def spectrum(self, alm, n, ph, Y, U):
-        N.call("zeb_spectrum_f32", ptr(alm), n, ctypes.byref(ph.dims), ptr(Y), ptr(U), stream_ptr())
+    def spectrum(self, alm, n, ph, Y, U, tensor_cores=True):
+        """spherical.zig:369-382 — U of n items: on the tensor cores (BF16 form) when the phase
+        has its packed table, else in plain FP32."""
+        if tensor_cores and ph.A is not None and Y is ph.Y_f:
+            B = self.buf("tc_b", N.load().zeb_tc_patterns_bytes(ctypes.byref(ph.dims), ph.split, n), torch.uint8)
+            N.call("zeb_spectrum_bf16", ptr(alm), n, ctypes.byref(ph.dims), ph.split, ptr(ph.A), ptr(B), ptr(U),
+                   ptr(self.tc_status()), stream_ptr())
+        else:
+            N.call("zeb_spectrum_f32", ptr(alm), n, ctypes.byref(ph.dims), ptr(Y), ptr(U), stream_ptr())
+
+    def tc_status(self):
+        """One int on the device that a timed-out wait in the tensor-core spectrum sets."""
+        t = self._buf.get("tc_status")
+        if t is None:
+            t = torch.zeros(1, dtype=torch.int32, device=self.dev)
+            self._buf["tc_status"] = t
+        return t
+
+    def check_device(self):
+        """After a readback: raise if a tensor-core spectrum gave up on a wait (its U incomplete)."""
+        t = self._buf.get("tc_status")
+        if t is not None:
+            v = int(t.item())
+            if v:
+                t.zero_()
+                raise EngineError(f"DeviceTimeout: tensor-core spectrum wait gave up (status {v})")
 
     # ── device passes ──
 
@@ -454,6 +478,7 @@ class Engine:
         host = torch.from_numpy(flat[cells])
         raw = host.pin_memory().to(self.dev, non_blocking=True)
         out = self.run_device(raw, cells, bandwidth).cpu().numpy()
+        self.check_device()
         return self.finish(out)
 
     def finish(self, out):

@@ -60,10 +60,14 @@ DEFAULTS = dict([
     ("pca_components", 256), ("pca_epochs", 2),
     ("accept_nmi", 0.0), ("accept_z", 15.0), ("accept_step_deg", 0.2),
     # this engine's own: which arithmetic the Wigner-d contraction runs in ("f32": the plain FP32
-    # form on the CUDA cores, "bf16": BF16 tensor cores with FP32 accumulation)
+    # form on the CUDA cores; "bf16": BF16 tensor cores with FP32 accumulation, operands split
+    # hi + lo for the orders l <= 16; "bf16x3": split for every order, near FP32 throughout)
     ("precision", "f32"),
 ])
-ENUMS["precision"] = ("f32", "bf16")
+ENUMS["precision"] = ("f32", "bf16", "bf16x3")
+
+# the largest order l whose products keep the lo parts, per precision (None: plain FP32)
+SPLIT_L = {"f32": None, "bf16": 16, "bf16x3": 1 << 20}
 
 
 class SettingsError(ValueError):
