@@ -122,14 +122,16 @@ typedef struct {
 } zeb_so3_dims_t;  /* spherical.PhaseGpu + Tables sizes (src/spherical.zig:192-242) */
 
 /* The master's correlation table for one phase at one bandwidth, in FP64 on the device:
- * Y[pair(m',l)][j·nc + iq] = i^{m'} Σ_k d^l_{k,m'} W[μ,l,k] β_{±}(k, j), the Wigner-d
- * contraction with the master's weights W (master.weights, src/master.zig:727-753) and the
- * transform along b (so3.wgsl spectrum, :147-277) folded in (β_+ = 2cos(k b_j), β_− = −2i sin,
- * by the parity of m'+m; k = 0 once). W is [mc][L][L] complex (re, im) FP64. */
+ * Y[pair(m',l)][j·nc + c] = Σ_μ e^{−2πi μ c/nc} i^{m'} Σ_k d^l_{k,m'} W[μ,l,k] β_{±}(k, j), the
+ * Wigner-d contraction with the master's weights W (master.weights, src/master.zig:727-753) and
+ * the transforms along b (so3.wgsl spectrum, :147-277; β_+ = 2cos(k b_j), β_− = −2i sin, by the
+ * parity of m'+m; k = 0 once) and along c (so3.wgsl:396-430, m = fold·μ at the nc grid points
+ * c) folded in, so that the spectrum U of an item is already transformed along b and c.
+ * W is [mc][L][L] complex (re, im) FP64. */
 int zeb_correlation_table(const zeb_so3_dims_t* d, const double* W, const double* wigner, double* Y, void* stream);
 
-/* U[b][j][m'][iq] = Σ_l conj(g_b[l,m']) Y[pair(m',l)][j·nc+iq]: the spectrum of every item
- * along b, in plain FP32 (CUDA cores). alm as zeb_sphere_coefficients leaves it; Y in FP32.
+/* U[b][j][m'][c] = Σ_l conj(g_b[l,m']) Y[pair(m',l)][j·nc+c]: the spectrum of every item,
+ * transformed along b and c, in plain FP32 (CUDA cores). alm as zeb_sphere_coefficients leaves it; Y in FP32.
  * Replaces Spherical.spectrum (src/spherical.zig:369-382; shaders/so3.wgsl spectrum). */
 int zeb_spectrum_f32(const float* alm, int n_items, const zeb_so3_dims_t* d, const float* Y, float* U, void* stream);
 
@@ -154,8 +156,8 @@ int zeb_tc_pack_master(const zeb_so3_dims_t* d, int split, const double* Y, void
 size_t zeb_tc_master_bytes(const zeb_so3_dims_t* d, int split);
 size_t zeb_tc_patterns_bytes(const zeb_so3_dims_t* d, int split, int n_items);
 
-/* The correlation volume's transforms along c and a, times rden (volume b / rden_div for item
- * b), each (item, j, c) line's largest value, each item's largest, and its sub-grid vertex and
+/* The correlation volume's transform along a (U comes transformed along b and c), times rden
+ * (volume b / rden_div for item b), each (item, j, c) line's largest value, each item's largest, and its sub-grid vertex and
  * orientation: peaks[b] = (q.w, q.x, q.y, q.z, score, a, b, c). Replaces Spherical.correlate's
  * a_peak_m, peak_reduce and peak_finish_m (src/spherical.zig:401-432; shaders/so3.wgsl
  * :489-593, 631-663, 716-796). scratch: zeb_peaks_scratch_bytes. */
@@ -180,7 +182,7 @@ int zeb_correlate_peaks(const float* U, int n_items, const zeb_so3_dims_t* d, co
 int zeb_correlate_peaks_static(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw,
                                const float* rden, int rden_div, float* peaks, void* stream);
 
-/* The full volumes (no peak) of n items: vol[b][j][iq][ia]. Replaces a_volume
+/* The full volumes (no peak) of n items: vol[b][j][c][ia]. Replaces a_volume
  * (shaders/so3.wgsl:595-612). */
 int zeb_correlate_volume(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw, float* vol, void* stream);
 

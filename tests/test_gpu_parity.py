@@ -154,7 +154,7 @@ def test_master_harmonics_match_oracle(world):
     assert ph.rules.n_fold == hm.rules.n_fold == 4
 
 
-@pytest.mark.parametrize("L", [16, 32])
+@pytest.mark.parametrize("L", [16, 32, 64])
 def test_correlation_peaks_match_oracle(world, lib, L):
     s = world["s"]
     e = s._e
@@ -178,6 +178,11 @@ def test_correlation_peaks_match_oracle(world, lib, L):
     cand = torch.empty(lib.load().zeb_peaks_scratch_bytes(ctypes.byref(ph.dims), n) // 4 + 1, device="cuda")
     lib.call("zeb_correlate_peaks", P(U), n, ctypes.byref(ph.dims), P(bt.tw), P(ph.rden), 1 << 30, P(peaks), P(cand), sp())
     got = peaks.cpu().numpy().reshape(n, 8)
+    # one rden per item (rden_div = 1) takes the other slab kernel: the same arithmetic, the same bits
+    rep = ph.rden.repeat(n)
+    peaks1 = torch.empty(n * 8, device="cuda")
+    lib.call("zeb_correlate_peaks", P(U), n, ctypes.byref(ph.dims), P(bt.tw), P(rep), 1, P(peaks1), P(cand), sp())
+    assert np.array_equal(peaks1.cpu().numpy().reshape(n, 8), got)
     # the oracle: harmonics of the same baked master, its window denominators, the volume, the peak
     tb = osp.Tables(L)
     hm = om.Harmonics(world["m_or"], world["baked"], L)
@@ -378,9 +383,10 @@ def test_chance_decoys_match_oracle(world, lib):
             assert abs(got[d, i] - v) < 2e-3
 
 
-def test_index_end_to_end_recovers_orientations(lib):
+@pytest.mark.parametrize("precision", ["f32", "bf16", "bf16x3"])
+def test_index_end_to_end_recovers_orientations(lib, precision):
     """The reference's own bar (tests/test_api.py:206-214): 8 × 12 simulated patterns with noise of
-    1.0 × their deviation, indexed: median disorientation < 0.15°, max < 1°."""
+    1.0 × their deviation, indexed: median disorientation < 0.15°, max < 1°, in each precision."""
     import tempfile
 
     import zebsdsolve_b200 as ze
@@ -392,7 +398,7 @@ def test_index_end_to_end_recovers_orientations(lib):
     write_npz(f"{d}/m.npz", sheets, 401, syn.group_matrices("432"), 30)
     rng = np.random.default_rng(7)
     s = ze.Solver()
-    s.configure(static_background="none", dynamic_background="none")
+    s.configure(static_background="none", dynamic_background="none", precision=precision)
     s.add_phase(f"{d}/m.npz")
     rows, cols = 8, 12
     s.set_patterns(np.zeros((rows, cols, 60, 60), np.float32))

@@ -1,16 +1,14 @@
-// (b, second stage) The correlation volume's transforms along c and a, one (item, j) slab per
-// thread block, entirely in shared memory, and the peak.
+// (b, second stage) The correlation volume's transform along a, and the peak.
 //
-// The slab U[b][j][m' < L][iq < nc] is loaded, transformed along c (length nc) row by row into
-// V[m'][c]; the real transform along a, C(a) = V[0] + 2 Re Σ_{m'>0} V[m'] e^{−i m' a} at the n
-// grid values of a, comes out of one complex FFT of length h = n/2 per column: its input is
-// Z_q = (X_q + X_{q+h}) + i e^{−2πiq/n}(X_q − X_{q+h}) with X_{q+h} = conj X_{h−q}, and its
-// output z_p = C(a_{2p}) + i C(a_{2p+1}) (so3.wgsl:279-315, 396-593).  Each column's values are
-// scaled by the reciprocal denominator volume and the largest kept with its volume index
-// (j·nc + c)·n + ia; the block keeps its slab's best (first index of equal values).
+// The slab U[b][j][m' < L][c < nc] arrives already transformed along b and c (both folded into
+// the master's table); the real transform along a, C(a) = V[0] + 2 Re Σ_{m'>0} V[m'] e^{−i m' a}
+// at the n grid values of a, comes out of one complex FFT of length h = n/2 per column c: its
+// input is Z_q = (X_q + X_{q+h}) + i e^{−2πiq/n}(X_q − X_{q+h}) with X_{q+h} = conj X_{h−q}, and
+// its output z_p = C(a_{2p}) + i C(a_{2p+1}) (so3.wgsl:279-315, 396-593).  Each column's values
+// are scaled by the reciprocal denominator volume and the largest kept with its volume index
+// (j·nc + c)·n + ia; each slab keeps its best (first index of equal values).
 // k_peak_finish then takes each item's best slab, re-evaluates the six neighbours of the peak by
-// direct sums over m' (V taken from U along c directly) and fits the parabolic vertex along a, c
-// and b (so3.wgsl:665-796).
+// direct sums over m' and fits the parabolic vertex along a, c and b (so3.wgsl:665-796).
 #include <mutex>
 
 #include "abi_util.cuh"
@@ -46,13 +44,11 @@ __global__ void __launch_bounds__(256) k_slab(SlabArgs a) {
   RowLines rows{lgc};
   ColLines cols{lgc};
   const float2* src = a.U + (size_t)slab * L * nc;
-  // rows bit-reversed along c
   for (int e = threadIdx.x; e < L * nc; e += blockDim.x) {
     int r = e >> lgc, c = e & (nc - 1);
-    V[rows(r, bitrev(c, lgc))] = src[e];
+    V[rows(r, c)] = src[e];
   }
   __syncthreads();
-  if (lgc > 0) fft_lines_smem(V, L, lgc, a.tw, rows);
   // Z down each column, bit-reversed along a
   const int tws = ZEB_TW_LEN / (2 * h);
   for (int e = threadIdx.x; e < h * nc; e += blockDim.x) {
@@ -113,15 +109,15 @@ __global__ void __launch_bounds__(256) k_slab(SlabArgs a) {
   }
 }
 
-// ── the slab a warp at a time, its transforms in registers ──
+// ── the slab a warp at a time, its transform in registers ──
 //
-// One warp per (item, j) slab: the slab comes in with coalesced 16-byte loads into the warp's
-// padded shared-memory tile; each lane transforms whole rows along c in registers (radix-2 with
-// compile-time twiddles), the tile goes back once, and each lane then holds one column: it forms
-// the half-length real-transform input Z_q from V[q] and V[h−q] in place, transforms it along a
-// in registers, scales by rden and keeps its column's best. The warp's best goes to `cand`.
-// No block-wide barrier: the warps of a block work on different slabs.
-
+// A warp takes NC/32 columns per lane (or, for nc < 32, 32/nc slabs at once, one column per
+// lane): the lane loads its column of the slab straight into registers (the lanes of a row read
+// consecutive addresses; every load of the column is independent, so they are all in flight at
+// once), forms the half-length real-transform input Z_q from V[q] and V[h−q] in place,
+// transforms it along a in registers (radix-2, compile-time twiddles), scales by its rden row and
+// keeps the largest value.  Within a lane the indices only grow, so the first of equal values is
+// kept by a strict comparison; lanes then reduce by (value, lowest index).
 template <int N>
 __device__ __forceinline__ float2 tw_of(int t);
 template <> __device__ __forceinline__ float2 tw_of<16>(int t) { return make_float2(kTwRe16[t], kTwIm16[t]); }
@@ -175,45 +171,36 @@ __device__ __forceinline__ void fft_reg(float2 (&x)[N]) {
 }
 
 template <int NC, int H, int WARPS, int PER_SM>
-__global__ void __launch_bounds__(WARPS * 32, PER_SM) k_slab_warp(SlabArgs a) {
-  constexpr int LD = NC + 1;  // padded row (float2): rows and columns both read without conflicts
-  extern __shared__ float2 smw[];
+__global__ void __launch_bounds__(WARPS * 32, PER_SM) k_slab_cols(SlabArgs a) {
+  constexpr int n = 2 * H;
+  constexpr int SEG = NC < 32 ? NC : 32;  // lanes per slab
+  constexpr int SPW = 32 / SEG;           // slabs per warp
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* buf = smw + (size_t)warp * H * LD;
-  const int L = a.d.L, nb = a.d.nb, n = 2 * H;
+  const int sub = lane / SEG, cl = lane - sub * SEG;
+  const int L = a.d.L, nb = a.d.nb;
   const long long total = (long long)a.n_items * nb;
-  for (long long slab = (long long)blockIdx.x * WARPS + warp; slab < total; slab += (long long)gridDim.x * WARPS) {
-    const int b = (int)(slab / nb), j = (int)(slab - (long long)b * nb);
-    const float4* src = (const float4*)(a.U + slab * L * NC);
-    for (int e = lane; e < L * NC / 2; e += 32) {
-      float4 v = __ldcs(src + e);
-      const int f = 2 * e, r = f / NC, c = f - r * NC;
-      buf[r * LD + c] = make_float2(v.x, v.y);
-      buf[r * LD + c + 1] = make_float2(v.z, v.w);
-    }
-    __syncwarp();
-    for (int r = lane; r < L; r += 32) {
-      float2 x[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) x[c] = buf[r * LD + c];
-      fft_reg<NC>(x);
-#pragma unroll
-      for (int c = 0; c < NC; ++c) buf[r * LD + c] = x[c];
-    }
-    __syncwarp();
+  for (long long s0 = ((long long)blockIdx.x * WARPS + warp) * SPW; s0 < total;
+       s0 += (long long)gridDim.x * WARPS * SPW) {
+    const long long slab = s0 + sub;
+    const bool live = slab < total;
+    const long long sl = live ? slab : s0;
+    const int b = (int)(sl / nb), j = (int)(sl - (long long)b * nb);
+    const float2* src = a.U + sl * L * NC;
+    const float* rslab = a.rden + ((size_t)(b / a.rden_div) * nb + j) * NC * n;
     float bv = -3.4e38f;
     uint32_t bi = 0xffffffffu;
-    for (int c = lane; c < NC; c += 32) {
+#pragma unroll 1
+    for (int c = cl; c < NC; c += SEG) {
       float2 z[H];
 #pragma unroll
-      for (int q = 0; q < H; ++q) z[q] = q < L ? buf[q * LD + c] : make_float2(0.f, 0.f);
+      for (int q = 0; q < H; ++q) z[q] = q < L ? __ldcs(src + q * NC + c) : make_float2(0.f, 0.f);
       // Z_q = (X_q + X_{q+h}) + i w_q (X_q − X_{q+h}), X_{q+h} = conj X_{h−q}, w_q = e^{−2πi q/n},
       // computed for q and h − q together from the same two points (in place)
 #pragma unroll
       for (int q = 0; q <= H / 2; ++q) {
         const int qm = (H - q) & (H - 1);
         float2 xq = z[q], xm = z[qm];
-        float2 zq, zm;
+        float2 zq;
         {
           float2 x = xq, y = make_float2(0.f, 0.f);
           if (q == 0) x.y = 0.f;
@@ -226,49 +213,39 @@ __global__ void __launch_bounds__(WARPS * 32, PER_SM) k_slab_warp(SlabArgs a) {
           float2 x = xm, y = make_float2(xq.x, -xq.y);
           const float2 w = tw_of<2 * H>(qm);
           const float2 dd = make_float2(x.x - y.x, x.y - y.y);
-          zm = make_float2(x.x + y.x - (w.x * dd.y + w.y * dd.x), x.y + y.y + (w.x * dd.x - w.y * dd.y));
-          z[qm] = zm;
+          z[qm] = make_float2(x.x + y.x - (w.x * dd.y + w.y * dd.x), x.y + y.y + (w.x * dd.x - w.y * dd.y));
         }
         z[q] = zq;
       }
       fft_reg<H>(z);
-      const float4* rd = (const float4*)(a.rden + (((size_t)(b / a.rden_div) * nb + j) * NC + c) * n);
+      const float4* rd = (const float4*)(rslab + (size_t)c * n);
       const uint32_t base = ((uint32_t)(j * NC + c)) * n;
 #pragma unroll
       for (int p = 0; p < H; p += 2) {
         const float4 r = __ldg(rd + p / 2);
         const float v0 = z[p].x * r.x, v1 = z[p].y * r.y, v2 = z[p + 1].x * r.z, v3 = z[p + 1].y * r.w;
         const uint32_t i0 = base + 2 * p;
-        if (v0 > bv || (v0 == bv && i0 < bi)) { bv = v0; bi = i0; }
-        if (v1 > bv || (v1 == bv && i0 + 1 < bi)) { bv = v1; bi = i0 + 1; }
-        if (v2 > bv || (v2 == bv && i0 + 2 < bi)) { bv = v2; bi = i0 + 2; }
-        if (v3 > bv || (v3 == bv && i0 + 3 < bi)) { bv = v3; bi = i0 + 3; }
+        if (v0 > bv) { bv = v0; bi = i0; }
+        if (v1 > bv) { bv = v1; bi = i0 + 1; }
+        if (v2 > bv) { bv = v2; bi = i0 + 2; }
+        if (v3 > bv) { bv = v3; bi = i0 + 3; }
       }
     }
+    // the slab's best over its SEG lanes (xor offsets below SEG stay inside the segment)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = SEG / 2; o > 0; o >>= 1) {
       float ov = __shfl_xor_sync(0xffffffffu, bv, o);
       uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
       if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
-    if (lane == 0) a.cand[slab] = make_float2(bv, __uint_as_float(bi));
-    __syncwarp();
+    if (cl == 0 && live) a.cand[slab] = make_float2(bv, __uint_as_float(bi));
   }
 }
 
-// V[j; m', c] of item b straight from U along c (so3.wgsl:667-674)
-__device__ __forceinline__ float2 v_at(const float2* __restrict__ U, const float2* __restrict__ tw, int b, int j,
-                                       int mp, int c, const zeb_so3_dims_t& d) {
-  const float2* row = U + (((size_t)b * d.nb + j) * d.L + mp) * d.nc;
-  const int ts = ZEB_TW_LEN / d.nc;
-  float2 acc = make_float2(0.f, 0.f);
-  for (int x = 0; x < d.nc; ++x) {
-    float2 v = __ldg(row + x);
-    float2 w = __ldg(tw + ((x * c) & (d.nc - 1)) * ts);
-    acc.x += v.x * w.x - v.y * w.y;
-    acc.y += v.x * w.y + v.y * w.x;
-  }
-  return acc;
+// V[j; m', c] of item b: U is already transformed along c (so3.wgsl:667-674)
+__device__ __forceinline__ float2 v_at(const float2* __restrict__ U, int b, int j, int mp, int c,
+                                       const zeb_so3_dims_t& d) {
+  return __ldg(U + (((size_t)b * d.nb + j) * d.L + mp) * d.nc + c);
 }
 
 // Re(V e^{−i m a}) at grid point ia (so3.wgsl:766-769)
@@ -320,16 +297,16 @@ __global__ void __launch_bounds__(64) k_peak_finish(SlabArgs a, float* __restric
   float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   for (int m = threadIdx.x; m < L; m += 64) {
     float f = m == 0 ? 1.f : 2.f;
-    float2 vc = v_at(a.U, a.tw, b, j, m, iq, d);
-    float2 vm = v_at(a.U, a.tw, b, j, m, iqm, d);
-    float2 vp = v_at(a.U, a.tw, b, j, m, iqp, d);
+    float2 vc = v_at(a.U, b, j, m, iq, d);
+    float2 vm = v_at(a.U, b, j, m, iqm, d);
+    float2 vp = v_at(a.U, b, j, m, iqp, d);
     s[0] += f * a_term(vc, m, iam, n);
     s[1] += f * a_term(vc, m, iap, n);
     s[2] += f * a_term(vm, m, ia, n);
     s[3] += f * a_term(vp, m, ia, n);
     if (inner) {
-      s[4] += f * a_term(v_at(a.U, a.tw, b, j - 1, m, iq, d), m, ia, n);
-      s[5] += f * a_term(v_at(a.U, a.tw, b, j + 1, m, iq, d), m, ia, n);
+      s[4] += f * a_term(v_at(a.U, b, j - 1, m, iq, d), m, ia, n);
+      s[5] += f * a_term(v_at(a.U, b, j + 1, m, iq, d), m, ia, n);
     }
   }
 #pragma unroll
@@ -411,26 +388,27 @@ static int slab_launch(const float* U, int n_items, const zeb_so3_dims_t* d, con
   long long blocks = (long long)n_items * d->nb;
   ZEB_REQUIRE(blocks < (1LL << 31), ZEB_ESIZE, "correlate: too many slabs");
   if (!vol && d->L <= d->n / 2) {
-    // the warp-per-slab kernels, where a lane's row and column fit in registers
+    // the warp-per-slab kernels, where a lane's column fits in registers
     const int H = d->n / 2, NC = d->nc;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-#define ZEB_SLAB_WARP(nc_, h_, w_, per_sm_)                                                                     \
-  if (NC == nc_ && H == h_) {                                                                                 \
-    size_t sm = (size_t)(w_) * (h_) * ((nc_) + 1) * sizeof(float2);                                          \
-    cudaFuncSetAttribute(k_slab_warp<nc_, h_, w_, per_sm_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);      \
-    long long want = (blocks + (w_)-1) / (w_);                                                                \
-    long long grid = want < (long long)sms * (per_sm_)*8 ? want : (long long)sms * (per_sm_)*8;              \
-    k_slab_warp<nc_, h_, w_, per_sm_><<<(unsigned)grid, (w_)*32, sm, st>>>(a);                                        \
-    return zeb_launch_check("correlate slab (warp)");                                                         \
+#define ZEB_SLAB_COLS(nc_, h_, w_, per_sm_)                                                                    \
+  if (NC == nc_ && H == h_) {                                                                                \
+    constexpr int spw = (nc_) < 32 ? 32 / (nc_) : 1;                                                        \
+    long long want = (blocks + (long long)(w_)*spw - 1) / ((long long)(w_)*spw);                             \
+    long long grid = want < (long long)sms * (per_sm_)*8 ? want : (long long)sms * (per_sm_)*8;             \
+    k_slab_cols<nc_, h_, w_, per_sm_><<<(unsigned)grid, (w_)*32, 0, st>>>(a);                               \
+    return zeb_launch_check("correlate slab (columns)");                                                    \
   }
-    ZEB_SLAB_WARP(16, 32, 4, 4)
-    ZEB_SLAB_WARP(32, 32, 4, 4)
-    ZEB_SLAB_WARP(64, 32, 2, 6)
-    ZEB_SLAB_WARP(32, 64, 4, 3)
-    ZEB_SLAB_WARP(64, 64, 2, 6)
-#undef ZEB_SLAB_WARP
+    ZEB_SLAB_COLS(8, 16, 4, 6)
+    ZEB_SLAB_COLS(16, 16, 4, 6)
+    ZEB_SLAB_COLS(16, 32, 4, 4)
+    ZEB_SLAB_COLS(32, 32, 4, 4)
+    ZEB_SLAB_COLS(64, 32, 4, 4)
+    ZEB_SLAB_COLS(32, 64, 4, 3)
+    ZEB_SLAB_COLS(64, 64, 4, 3)
+#undef ZEB_SLAB_COLS
   }
   if (vol) {
     cudaFuncSetAttribute(k_slab<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -147,6 +147,37 @@ __global__ void k_correlation_table(zeb_so3_dims_t dm, const double2* __restrict
   Y[t] = out;
 }
 
+// The transform along c folded into the table: each (pair, j) row of nc slots (the master's
+// order μ ≡ slot mod nc) becomes its DFT at the nc grid points of c,
+//   Y'[pair][j·nc + c] = Σ_s Y[pair][j·nc + s] e^{−2πi s c / nc}
+// (e^{−i m c} with m = fold·μ and c = 2π q/n, so3.wgsl:396-430), in place, FP64.  A block holds
+// 256/nc whole rows (or one row of nc > 256) and the nc twiddles, from sincospi of exact fractions.
+__global__ void k_table_cdft(double2* __restrict__ Y, long long rows, int nc) {
+  extern __shared__ double2 cd_sm[];
+  double2* tw = cd_sm;       // [nc]
+  double2* row = cd_sm + nc;  // [rows per block][nc]
+  const int per = blockDim.x / nc;
+  const long long r0 = (long long)blockIdx.x * per;
+  for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+    double sn, cs;
+    sincospi(-2.0 * (double)t / (double)nc, &sn, &cs);
+    tw[t] = make_double2(cs, sn);
+  }
+  const int rl = threadIdx.x / nc, c = threadIdx.x - rl * nc;
+  const bool live = rl < per && r0 + rl < rows;
+  if (live) row[rl * nc + c] = Y[(r0 + rl) * nc + c];
+  __syncthreads();
+  if (!live) return;
+  double re = 0.0, im = 0.0;
+  const double2* in = row + rl * nc;
+  for (int s = 0; s < nc; ++s) {
+    const double2 v = in[s], w = tw[(s * c) & (nc - 1)];
+    re += v.x * w.x - v.y * w.y;
+    im += v.x * w.y + v.y * w.x;
+  }
+  Y[(r0 + rl) * nc + c] = make_double2(re, im);
+}
+
 }  // namespace zeb
 
 using namespace zeb;
@@ -183,6 +214,14 @@ extern "C" int zeb_correlation_table(const zeb_so3_dims_t* d, const double* W, c
   long long total = (long long)d->n_pairs * d->nb * d->nc;
   int th = 256;
   long long bl = (total + th - 1) / th;
+  ZEB_REQUIRE((d->nc & (d->nc - 1)) == 0 && d->nc <= 1024, ZEB_EARG, "correlation_table: nc=%d", d->nc);
   k_correlation_table<<<(unsigned)bl, th, 0, (cudaStream_t)stream>>>(*d, (const double2*)W, wigner, (double2*)Y);
-  return zeb_launch_check("correlation_table");
+  int rc = zeb_launch_check("correlation_table");
+  if (rc) return rc;
+  const long long rows = (long long)d->n_pairs * d->nb;
+  const int per = d->nc >= 256 ? 1 : 256 / d->nc;
+  const int threads = per * d->nc;
+  const size_t sm = (size_t)(d->nc + threads) * sizeof(double2);
+  k_table_cdft<<<(unsigned)((rows + per - 1) / per), threads, sm, (cudaStream_t)stream>>>((double2*)Y, rows, d->nc);
+  return zeb_launch_check("correlation_table (transform along c)");
 }
