@@ -383,6 +383,58 @@ def test_chance_decoys_match_oracle(world, lib):
             assert abs(got[d, i] - v) < 2e-3
 
 
+def test_refine_and_chance_on_a_large_detector_match_oracle(world, lib):
+    """A 120 × 120 detector (its masked-pixel list exceeds the shared-memory budget, so the kernels
+    that evaluate each pixel's ray in place run): refinement, NMI and decoys against the oracle."""
+    import zebsdsolve_b200 as ze
+
+    s = ze.Solver()
+    s.configure(static_background="none", dynamic_background="none", bandwidth=16)
+    s.add_phase(world["path"])
+    n = 3
+    s.set_patterns(np.zeros((1, n, 120, 120), np.float32))
+    s.set_geometry(pc=(0.5, 0.3, 0.6), sample_tilt_deg=70, detector_tilt_deg=0)
+    q = world["q"][:n]
+    rng = np.random.default_rng(15)
+    sims = s.simulate(q, cells=np.arange(n))
+    pats = sims + 0.3 * sims.std() * rng.normal(size=sims.shape)
+    s.set_patterns(pats.astype(np.float32).reshape(1, n, 120, 120))
+    e = s._e
+    e.prepare_masters()
+    fr = _frame(s)
+    assert 120 * 120 * 16 > 200 * 1024
+    mask = np.array(fr.mask)
+    normed = np.stack([op.normalize(p.astype(np.float64), mask) for p in pats]).astype(np.float32)
+    t = e.positions(np.arange(n))
+    items = torch.as_tensor(np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1), device="cuda")
+    from zebsdsolve_b200 import rotations as R
+
+    start = R.qstd(R.qmul(R.exp_map(rng.normal(0, math.radians(0.8), (n, 3))), q))
+    seeds = torch.as_tensor(np.concatenate([start, np.zeros((n, 4))], 1).astype(np.float32), device="cuda")
+    recs = torch.empty(n * 8, device="cuda")
+    p = e.phases[0]
+    opts = lib.RefineOpts(8, math.radians(2.0), 1.0, 0.02, 1e4, 16, 3.0)
+    pd = torch.as_tensor(normed, device="cuda").reshape(-1)
+    lib.call("zeb_refine", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(p.baked[1]), P(p.baked[2]), p.master.side,
+             ctypes.byref(opts), P(recs), sp())
+    got = recs.cpu().numpy().reshape(n, 8)
+    out = torch.empty(2 * n, device="cuda")
+    lib.call("zeb_chance", P(pd), P(items), n, 2, ctypes.byref(fr), P(p.baked[1]), p.master.side, 16, P(out), sp())
+    dec = out.cpu().numpy().reshape(2, n)
+    grad = od.gradient_table(world["baked"], 151)
+    frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
+    ops = world["m_or"].rotations()
+    for i in range(n):
+        qb, best, step = od.refine(grad, 151, frame, t[i], start[i], normed[i].astype(np.float64), mask)
+        assert abs(got[i, 4] - best) < 2e-4, (got[i, 4], best)
+        assert math.degrees(float(osym.disorientation(got[i, :4].astype(np.float64), qb, ops))) < 0.02
+        v = od.nmi(world["baked"], 151, frame, t[i], got[i, :4].astype(np.float64), normed[i].astype(np.float64), mask)
+        assert abs(got[i, 5] - v) < 2e-3, (got[i, 5], v)
+        for d in range(2):
+            vd = od.nmi(world["baked"], 151, frame, t[i], od.decoy(np.arange(n), d)[i], normed[i].astype(np.float64), mask)
+            assert abs(dec[d, i] - vd) < 2e-3
+
+
 @pytest.mark.parametrize("precision", ["f32", "bf16", "bf16x3"])
 def test_index_end_to_end_recovers_orientations(lib, precision):
     """The reference's own bar (tests/test_api.py:206-214): 8 × 12 simulated patterns with noise of

@@ -150,3 +150,22 @@ def test_reference_masters_load_when_present():
     gan = Path("/root/reference/testdata/gan/GaN_master_20kV.npz")
     g = M.load_npz(gan)
     assert g.setting.rotation == "c6" and g.setting.laue == "d6" and len(g.rotations()) == 6 and len(g.ops) == 12
+
+
+def test_atan01_polynomial_error_bound():
+    """The detector kernels' atan on [0, 1] (an 8-term odd polynomial in csrc/common.cuh), evaluated
+    by Horner in float32 as the kernels do: within 1.5e-7 of atan everywhere on the interval."""
+    import re
+    from pathlib import Path
+
+    src = (Path(__file__).resolve().parents[1] / "zebsdsolve_b200" / "csrc" / "common.cuh").read_text()
+    body = src[src.index("float atan01(float t)"):src.index("return t * p;")]
+    cs = [float(x.rstrip("f")) for x in re.findall(r"(-?\d\.\d+e[-+]\d+)f", body)]
+    assert len(cs) == 8
+    x = np.linspace(0, 1, 1_000_001).astype(np.float32)
+    t2 = x * x
+    p = np.float32(cs[0])
+    for c in cs[1:]:
+        p = (p * t2 + np.float32(c)).astype(np.float32)
+    err = np.abs((x * p).astype(np.float64) - np.arctan(x.astype(np.float64)))
+    assert err.max() < 1.5e-7, err.max()

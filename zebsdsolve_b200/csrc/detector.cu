@@ -120,7 +120,72 @@ __device__ float nmi_block(const DetArgs& a, const float* pat, float* sims, floa
   return h_marg > 1e-12f ? 2.f * (h_marg - h_joint) / h_marg : 0.f;
 }
 
-__global__ void __launch_bounds__(256) k_refine(DetArgs a) {
+// One step of refine_item (detector.wgsl:561-640) from the 19 sums s of the orientation q just
+// evaluated: NCC, gradient and J'J; accept (tracking the best) or reject, the curvature scale μ
+// adapted by the gain ratio; then the damped 3×3 solve, clipped to max_step, from the best
+// orientation.  q_next: the next orientation to evaluate (the best after the last pass).
+__device__ void refine_step(const zeb_refine_opts_t& o, int iter, float4 q, const float* s, float& best, float& mu,
+                            float* g_best, float* h_best, float& last_good, float& promised, float& step_len,
+                            float& accepted, float4& q_best, float4& q_next) {
+  const float n = fmaxf(s[0], 1.f);
+  const float mean = s[1] / n;
+  const float var_n = s[2] - n * mean * mean;
+  float ncc = -2.f, g[3] = {0.f, 0.f, 0.f}, hs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (var_n > 1e-12f) {
+    const float inv = rsqrtf(var_n);
+    ncc = s[3] * inv;
+    const float sd[3] = {s[4], s[5], s[6]};
+    float au[3];
+    for (int k = 0; k < 3; ++k) au[k] = (s[7 + k] - mean * sd[k]) * inv;
+    for (int k = 0; k < 3; ++k) g[k] = (s[10 + k] - ncc * au[k]) * inv;
+    const float iv = inv * inv;
+    hs[0] = (s[13] - sd[0] * sd[0] / n - au[0] * au[0]) * iv;
+    hs[1] = (s[16] - sd[0] * sd[1] / n - au[0] * au[1]) * iv;
+    hs[2] = (s[17] - sd[0] * sd[2] / n - au[0] * au[2]) * iv;
+    hs[3] = (s[14] - sd[1] * sd[1] / n - au[1] * au[1]) * iv;
+    hs[4] = (s[18] - sd[1] * sd[2] / n - au[1] * au[2]) * iv;
+    hs[5] = (s[15] - sd[2] * sd[2] / n - au[2] * au[2]) * iv;
+  }
+  if (ncc > best) {
+    if (accepted > 0.5f && promised > 1e-6f) {
+      float rho = (ncc - best) / promised;
+      mu = fminf(fmaxf(mu * (2.f - rho), mu / 3.f), mu * 3.f);
+    }
+    q_best = q;
+    best = ncc;
+    for (int k = 0; k < 3; ++k) g_best[k] = g[k];
+    for (int k = 0; k < 6; ++k) h_best[k] = hs[k];
+    last_good = step_len;
+    accepted += 1.f;
+  } else {
+    mu = mu * 3.f;
+  }
+  mu = fminf(fmaxf(mu, o.scale_min), o.scale_max);
+  if (iter < o.iters) {
+    float hh[6];
+    for (int k = 0; k < 6; ++k) hh[k] = h_best[k] * mu;
+    float tr = fmaxf(hh[0] + hh[3] + hh[5], 1e-20f);
+    hh[0] += 1e-6f * tr; hh[3] += 1e-6f * tr; hh[5] += 1e-6f * tr;
+    float3 gg = make_float3(g_best[0], g_best[1], g_best[2]);
+    float3 stp = solve3(hh, gg);
+    float len = sqrtf(dot3(stp, stp));
+    if (len > o.max_step) {
+      float k = o.max_step / len;
+      stp = make_float3(stp.x * k, stp.y * k, stp.z * k);
+    }
+    float quad = hh[0] * stp.x * stp.x + hh[3] * stp.y * stp.y + hh[5] * stp.z * stp.z +
+                 2.f * (hh[1] * stp.x * stp.y + hh[2] * stp.x * stp.z + hh[4] * stp.y * stp.z);
+    promised = dot3(gg, stp) - 0.5f * quad;
+    step_len = sqrtf(dot3(stp, stp));
+    float4 qn = qmul(qexp(stp), q_best);
+    float nq = sqrtf(qn.x * qn.x + qn.y * qn.y + qn.z * qn.z + qn.w * qn.w);
+    q_next = nq > 0.f ? make_float4(qn.x / nq, qn.y / nq, qn.z / nq, qn.w / nq) : make_float4(1.f, 0.f, 0.f, 0.f);
+  } else {
+    q_next = q_best;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_refine_direct(DetArgs a) {
   extern __shared__ float smf[];
   __shared__ float red[24 * 8];
   __shared__ uint32_t hist[32 * 32];
@@ -140,11 +205,10 @@ __global__ void __launch_bounds__(256) k_refine(DetArgs a) {
   }
   // refinement state (thread 0's registers): detector.wgsl:73-77
   const float* sd0 = a.seeds + (size_t)b * a.seed_stride;
-  float4 q_cur = make_float4(sd0[0], sd0[1], sd0[2], sd0[3]);
-  float4 q_best = q_cur;
+  float4 q_best = make_float4(sd0[0], sd0[1], sd0[2], sd0[3]);
   float best = -2.f, mu = a.o.scale0, g_best[3] = {0.f, 0.f, 0.f}, h_best[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float last_good = 0.f, promised = 0.f, step_len = 0.f, accepted = 0.f;
-  if (threadIdx.x == 0) sh_q = q_cur;
+  if (threadIdx.x == 0) sh_q = q_best;
   __syncthreads();
 
   for (int iter = 0; iter <= a.o.iters; ++iter) {
@@ -168,64 +232,9 @@ __global__ void __launch_bounds__(256) k_refine(DetArgs a) {
     }
     block_sums<19>(s, red);
     if (threadIdx.x == 0) {
-      // refine_item (detector.wgsl:561-640)
-      const float n = fmaxf(s[0], 1.f);
-      const float mean = s[1] / n;
-      const float var_n = s[2] - n * mean * mean;
-      float ncc = -2.f, g[3] = {0.f, 0.f, 0.f}, hs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      if (var_n > 1e-12f) {
-        const float inv = rsqrtf(var_n);
-        ncc = s[3] * inv;
-        const float sd[3] = {s[4], s[5], s[6]};
-        float au[3];
-        for (int k = 0; k < 3; ++k) au[k] = (s[7 + k] - mean * sd[k]) * inv;
-        for (int k = 0; k < 3; ++k) g[k] = (s[10 + k] - ncc * au[k]) * inv;
-        const float iv = inv * inv;
-        hs[0] = (s[13] - sd[0] * sd[0] / n - au[0] * au[0]) * iv;
-        hs[1] = (s[16] - sd[0] * sd[1] / n - au[0] * au[1]) * iv;
-        hs[2] = (s[17] - sd[0] * sd[2] / n - au[0] * au[2]) * iv;
-        hs[3] = (s[14] - sd[1] * sd[1] / n - au[1] * au[1]) * iv;
-        hs[4] = (s[18] - sd[1] * sd[2] / n - au[1] * au[2]) * iv;
-        hs[5] = (s[15] - sd[2] * sd[2] / n - au[2] * au[2]) * iv;
-      }
-      if (ncc > best) {
-        if (accepted > 0.5f && promised > 1e-6f) {
-          float rho = (ncc - best) / promised;
-          mu = fminf(fmaxf(mu * (2.f - rho), mu / 3.f), mu * 3.f);
-        }
-        q_best = q;
-        best = ncc;
-        for (int k = 0; k < 3; ++k) g_best[k] = g[k];
-        for (int k = 0; k < 6; ++k) h_best[k] = hs[k];
-        last_good = step_len;
-        accepted += 1.f;
-      } else {
-        mu = mu * 3.f;
-      }
-      mu = fminf(fmaxf(mu, a.o.scale_min), a.o.scale_max);
-      if (iter < a.o.iters) {
-        float hh[6];
-        for (int k = 0; k < 6; ++k) hh[k] = h_best[k] * mu;
-        float tr = fmaxf(hh[0] + hh[3] + hh[5], 1e-20f);
-        hh[0] += 1e-6f * tr; hh[3] += 1e-6f * tr; hh[5] += 1e-6f * tr;
-        float3 gg = make_float3(g_best[0], g_best[1], g_best[2]);
-        float3 stp = solve3(hh, gg);
-        float len = sqrtf(dot3(stp, stp));
-        if (len > a.o.max_step) {
-          float k = a.o.max_step / len;
-          stp = make_float3(stp.x * k, stp.y * k, stp.z * k);
-        }
-        float quad = hh[0] * stp.x * stp.x + hh[3] * stp.y * stp.y + hh[5] * stp.z * stp.z +
-                     2.f * (hh[1] * stp.x * stp.y + hh[2] * stp.x * stp.z + hh[4] * stp.y * stp.z);
-        promised = dot3(gg, stp) - 0.5f * quad;
-        step_len = sqrtf(dot3(stp, stp));
-        float4 qn = qmul(qexp(stp), q_best);
-        float nq = sqrtf(qn.x * qn.x + qn.y * qn.y + qn.z * qn.z + qn.w * qn.w);
-        q_cur = nq > 0.f ? make_float4(qn.x / nq, qn.y / nq, qn.z / nq, qn.w / nq) : make_float4(1.f, 0.f, 0.f, 0.f);
-        sh_q = q_cur;
-      } else {
-        sh_q = q_best;
-      }
+      float4 qn = q_best;
+      refine_step(a.o, iter, q, s, best, mu, g_best, h_best, last_good, promised, step_len, accepted, q_best, qn);
+      sh_q = qn;
     }
     __syncthreads();
   }
@@ -257,7 +266,7 @@ __device__ __forceinline__ float4 decoy_q(uint32_t b, uint32_t draw) {
   return make_float4(ra * sinf(a2), ra * cosf(a2), rb * sinf(a3), rb * cosf(a3));
 }
 
-__global__ void __launch_bounds__(256) k_chance(DetArgs a) {
+__global__ void __launch_bounds__(256) k_chance_direct(DetArgs a) {
   extern __shared__ float smf[];
   __shared__ float red[24 * 8];
   __shared__ uint32_t hist[32 * 32];
@@ -291,6 +300,169 @@ __global__ void k_project(DetArgs a, const float* __restrict__ poses, float* __r
   sims[t] = master_at(a.master, qrot(q, ray_dir(a, tt, row, col)), a.side);
 }
 
+// ── the same with the masked pixels compacted once per block ──
+//
+// The block first lists its item's masked pixels in raster order, each as (detector ray in the
+// sample frame, pattern value) in shared memory; every pass then runs over that list alone: no
+// mask test, no index arithmetic and no ray normalization per pixel and pass, and the sphere →
+// square map with fast arithmetic.  For detectors whose list fits in shared memory.
+
+// px[0..npix) ← (ray, value) of the masked pixels of the pattern at gpat; returns npix
+__device__ int compact_pixels(const DetArgs& a, const float* gpat, float3 t, float4* px, int* wcnt) {
+  const int hw = a.h * a.w;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int out = 0;
+  for (int base = 0; base < hw; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int row = i / a.w, col = i - row * a.w;
+    const bool m = i < hw && in_mask(a, row, col);
+    const unsigned bal = __ballot_sync(0xffffffffu, m);
+    if (lane == 0) wcnt[wid] = __popc(bal);
+    __syncthreads();
+    int off = out, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < wid) off += wcnt[w];
+      tot += wcnt[w];
+    }
+    if (m) {
+      const float3 d = ray_dir(a, t, row, col);
+      px[off + __popc(bal & ((1u << lane) - 1u))] = make_float4(d.x, d.y, d.z, __ldg(gpat + i));
+    }
+    out += tot;
+    __syncthreads();
+  }
+  return out;
+}
+
+// NMI over the compacted pixels (detector.wgsl:744-832)
+__device__ float nmi_compact(const DetArgs& a, const float4* px, int npix, float4 q, int nbins, uint32_t* hist,
+                             float* red) {
+  float ext[4] = {3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f};
+  for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    const float4 p = px[k];
+    const float sv = master_at(a.master, qrot(q, make_float3(p.x, p.y, p.z)), a.side);
+    ext[0] = fminf(ext[0], p.w); ext[1] = fmaxf(ext[1], p.w);
+    ext[2] = fminf(ext[2], sv); ext[3] = fmaxf(ext[3], sv);
+  }
+  for (int i = threadIdx.x; i < nbins * nbins; i += blockDim.x) hist[i] = 0u;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ext[0] = fminf(ext[0], __shfl_xor_sync(0xffffffffu, ext[0], o));
+    ext[1] = fmaxf(ext[1], __shfl_xor_sync(0xffffffffu, ext[1], o));
+    ext[2] = fminf(ext[2], __shfl_xor_sync(0xffffffffu, ext[2], o));
+    ext[3] = fmaxf(ext[3], __shfl_xor_sync(0xffffffffu, ext[3], o));
+  }
+  if (lane == 0)
+    for (int k = 0; k < 4; ++k) red[k * nw + wid] = ext[k];
+  __syncthreads();
+  float r[4] = {3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f};
+  for (int w = 0; w < nw; ++w) {
+    r[0] = fminf(r[0], red[0 * nw + w]); r[1] = fmaxf(r[1], red[1 * nw + w]);
+    r[2] = fminf(r[2], red[2 * nw + w]); r[3] = fmaxf(r[3], red[3 * nw + w]);
+  }
+  __syncthreads();
+  const float ke = (float)nbins / fmaxf(r[1] - r[0], 1e-20f);
+  const float ks = (float)nbins / fmaxf(r[3] - r[2], 1e-20f);
+  for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    const float4 p = px[k];
+    const float sv = master_at(a.master, qrot(q, make_float3(p.x, p.y, p.z)), a.side);
+    const uint32_t be = min((uint32_t)((p.w - r[0]) * ke), (uint32_t)(nbins - 1));
+    const uint32_t bs = min((uint32_t)((sv - r[2]) * ks), (uint32_t)(nbins - 1));
+    atomicAdd(&hist[be * nbins + bs], 1u);
+  }
+  __syncthreads();
+  float acc[3] = {0.f, 0.f, 0.f};  // −Σ c log c (joint), −Σ (marginals), N
+  for (int i = threadIdx.x; i < nbins * nbins; i += blockDim.x) {
+    float c = (float)hist[i];
+    acc[2] += c;
+    if (c > 0.f) acc[0] -= c * logf(c);
+  }
+  if ((int)threadIdx.x < nbins) {
+    float rs = 0.f, cs = 0.f;
+    for (int k = 0; k < nbins; ++k) {
+      rs += (float)hist[threadIdx.x * nbins + k];
+      cs += (float)hist[k * nbins + threadIdx.x];
+    }
+    if (rs > 0.f) acc[1] -= rs * logf(rs);
+    if (cs > 0.f) acc[1] -= cs * logf(cs);
+  }
+  block_sums<3>(acc, red);
+  const float nn = fmaxf(acc[2], 1.f);
+  const float h_joint = logf(nn) + acc[0] / nn;
+  const float h_marg = 2.f * logf(nn) + acc[1] / nn;
+  return h_marg > 1e-12f ? 2.f * (h_marg - h_joint) / h_marg : 0.f;
+}
+
+__global__ void __launch_bounds__(256, 3) k_refine(DetArgs a) {
+  extern __shared__ float4 px[];
+  __shared__ float red[24 * 8];
+  __shared__ uint32_t hist[32 * 32];
+  __shared__ int wcnt[8];
+  __shared__ float4 sh_q;
+  const int b = blockIdx.x;
+  const int hw = a.h * a.w;
+  const float4 it = a.items[b];
+  const float3 t = make_float3(it.x, it.y, it.z);
+  const int npix = compact_pixels(a, a.pats + (size_t)(int)it.w * hw, t, px, wcnt);
+  // refinement state (thread 0's registers): detector.wgsl:73-77
+  const float* sd0 = a.seeds + (size_t)b * a.seed_stride;
+  float4 q_best = make_float4(sd0[0], sd0[1], sd0[2], sd0[3]);
+  float best = -2.f, mu = a.o.scale0, g_best[3] = {0.f, 0.f, 0.f}, h_best[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float last_good = 0.f, promised = 0.f, step_len = 0.f, accepted = 0.f;
+  if (threadIdx.x == 0) sh_q = q_best;
+  __syncthreads();
+
+  for (int iter = 0; iter <= a.o.iters; ++iter) {
+    const float4 q = sh_q;
+    float s[19];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) s[k] = 0.f;
+    for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+      const float4 p = px[k];
+      const float3 c = qrot(q, make_float3(p.x, p.y, p.z));
+      const float4 m = grad_at(a.grad, c, a.side);
+      const float3 d = cross3(c, make_float3(m.x, m.y, m.z));
+      const float e = p.w;
+      s[1] += m.w; s[2] += m.w * m.w; s[3] += m.w * e;
+      s[4] += d.x; s[5] += d.y; s[6] += d.z;
+      s[7] += m.w * d.x; s[8] += m.w * d.y; s[9] += m.w * d.z;
+      s[10] += e * d.x; s[11] += e * d.y; s[12] += e * d.z;
+      s[13] += d.x * d.x; s[14] += d.y * d.y; s[15] += d.z * d.z;
+      s[16] += d.x * d.y; s[17] += d.x * d.z; s[18] += d.y * d.z;
+    }
+    block_sums<19>(s, red);
+    s[0] = (float)npix;
+    if (threadIdx.x == 0) {
+      float4 qn = q_best;
+      refine_step(a.o, iter, q, s, best, mu, g_best, h_best, last_good, promised, step_len, accepted, q_best, qn);
+      sh_q = qn;
+    }
+    __syncthreads();
+  }
+  const float4 qf = sh_q;
+  float v = nmi_compact(a, px, npix, qf, a.o.nmi_bins, hist, red);
+  if (threadIdx.x == 0) {
+    float* r = a.records + (size_t)b * 8;
+    r[0] = qf.x; r[1] = qf.y; r[2] = qf.z; r[3] = qf.w;
+    r[4] = best; r[5] = v; r[6] = last_good; r[7] = a.o.stamp;
+  }
+}
+
+__global__ void __launch_bounds__(256, 3) k_chance(DetArgs a) {
+  extern __shared__ float4 px[];
+  __shared__ float red[24 * 8];
+  __shared__ uint32_t hist[32 * 32];
+  __shared__ int wcnt[8];
+  const int b = blockIdx.x, draw = blockIdx.y;
+  const int hw = a.h * a.w;
+  const float4 it = a.items[b];
+  const int npix = compact_pixels(a, a.pats + (size_t)(int)it.w * hw, make_float3(it.x, it.y, it.z), px, wcnt);
+  const float4 q = decoy_q((uint32_t)b, (uint32_t)draw);
+  const float v = nmi_compact(a, px, npix, q, a.o.nmi_bins, hist, red);
+  if (threadIdx.x == 0) a.chance[(size_t)draw * a.n + b] = v;
+}
+
 static bool fill_frame(DetArgs& a, const zeb_frame_t* fr) {
   if (!fr || fr->h < 2 || fr->w < 2) return false;
   a.h = fr->h; a.w = fr->w;
@@ -300,6 +472,9 @@ static bool fill_frame(DetArgs& a, const zeb_frame_t* fr) {
   for (int k = 0; k < 3; ++k) a.mask[k] = fr->mask[k];
   return true;
 }
+
+// the compacted-pixel kernels while their list fits (up to 12 800 pixels: 113 × 113)
+constexpr size_t DET_LIST_SMEM = 200 * 1024;
 
 static size_t det_smem(DetArgs& a) {
   size_t hw = (size_t)a.h * a.w;
@@ -324,9 +499,15 @@ extern "C" int zeb_refine(const float* pats, const float* items, const float* se
   ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine: bad frame");
   a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
   a.master = master; a.grad = (const float4*)grad4; a.side = side; a.o = *o; a.records = records;
-  size_t smem = det_smem(a);
-  cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_refine<<<n, 256, smem, (cudaStream_t)stream>>>(a);
+  const size_t list = (size_t)a.h * a.w * sizeof(float4);
+  if (list <= DET_LIST_SMEM) {
+    cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
+    k_refine<<<n, 256, list, (cudaStream_t)stream>>>(a);
+  } else {
+    size_t smem = det_smem(a);
+    cudaFuncSetAttribute(k_refine_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_refine_direct<<<n, 256, smem, (cudaStream_t)stream>>>(a);
+  }
   return zeb_launch_check("refine");
 }
 
@@ -339,10 +520,16 @@ extern "C" int zeb_chance(const float* pats, const float* items, int n, int draw
   ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "chance: bad frame");
   a.pats = pats; a.items = (const float4*)items; a.n = n; a.master = master; a.side = side;
   a.o.nmi_bins = nmi_bins; a.chance = out; a.draws = draws;
-  size_t smem = det_smem(a);
-  cudaFuncSetAttribute(k_chance, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g(n, draws);
-  k_chance<<<g, 256, smem, (cudaStream_t)stream>>>(a);
+  const size_t list = (size_t)a.h * a.w * sizeof(float4);
+  if (list <= DET_LIST_SMEM) {
+    cudaFuncSetAttribute(k_chance, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
+    k_chance<<<g, 256, list, (cudaStream_t)stream>>>(a);
+  } else {
+    size_t smem = det_smem(a);
+    cudaFuncSetAttribute(k_chance_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_chance_direct<<<g, 256, smem, (cudaStream_t)stream>>>(a);
+  }
   return zeb_launch_check("chance");
 }
 

@@ -31,7 +31,7 @@ __global__ void k_master_blur(const float* __restrict__ src, float* __restrict__
       float a = (float)i * step, b = (float)j * step;
       float wgt = expf(-(a * a + b * b) * k);
       float3 v = normalize3(make_float3(d.x + a * e1.x + b * e2.x, d.y + a * e1.y + b * e2.y, d.z + a * e1.z + b * e2.z));
-      acc += wgt * master_at(src, v, side);
+      acc += wgt * master_at<false>(src, v, side);
       wsum += wgt;
     }
   }
@@ -49,8 +49,8 @@ __global__ void k_master_gradient(const float* __restrict__ src, float4* __restr
   float3 m1 = normalize3(make_float3(c.x - h * e1.x, c.y - h * e1.y, c.z - h * e1.z));
   float3 p2 = normalize3(make_float3(c.x + h * e2.x, c.y + h * e2.y, c.z + h * e2.z));
   float3 m2 = normalize3(make_float3(c.x - h * e2.x, c.y - h * e2.y, c.z - h * e2.z));
-  float g1 = (master_at(src, p1, side) - master_at(src, m1, side)) / (2.f * h);
-  float g2 = (master_at(src, p2, side) - master_at(src, m2, side)) / (2.f * h);
+  float g1 = (master_at<false>(src, p1, side) - master_at<false>(src, m1, side)) / (2.f * h);
+  float g2 = (master_at<false>(src, p2, side) - master_at<false>(src, m2, side)) / (2.f * h);
   grad[tid] = make_float4(g1 * e1.x + g2 * e2.x, g1 * e1.y + g2 * e2.y, g1 * e1.z + g2 * e2.z, src[tid]);
 }
 
