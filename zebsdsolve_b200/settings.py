@@ -5,7 +5,10 @@ Front ends set options with a JSON object or keyword arguments; keys are these n
 names as strings, absent keys keep their value.  An unknown key is an error, and a value the
 pipeline cannot run with is rejected with the settings left as they were (settings.zig:403-461).
 The speed-only options (`batch`, `tile_mb`, `refine_pixels`, `wg_fft`, `wg_refine`) are accepted
-and validated as the reference does; on this engine they size device batches and tiles.
+and validated as the reference does; on this engine they size device batches and tiles.  Results
+do not depend on them.  `tile_mb` (the spectra one pass may hold) defaults to the reference's
+largest valid value, 8192, rather than its 256: a B200 holds 180 GB, and tiles of a few thousand
+patterns keep the tensor-core and slab kernels' grids full.
 """
 import json
 import math
@@ -55,7 +58,7 @@ DEFAULTS = dict([
     ("phase_by", "nmi"), ("nmi_bins", 16),
     ("ipf_colors", "perfect"),
     ("method", "spherical"), ("dict_grid", 30), ("batch", 256),
-    ("tile_mb", 256), ("refine_pixels", 64), ("wg_fft", 64), ("wg_refine", 64),
+    ("tile_mb", 8192), ("refine_pixels", 64), ("wg_fft", 64), ("wg_refine", 64),
     ("sweeps", 1), ("sweep_bandwidth", 32), ("sweep_dict_grid", 20), ("sweep_method", "same"),
     ("pca_components", 256), ("pca_epochs", 2),
     ("accept_nmi", 0.0), ("accept_z", 15.0), ("accept_step_deg", 0.2),
