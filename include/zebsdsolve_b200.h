@@ -115,6 +115,22 @@ int zeb_sphere_coefficients(const float* pats, const float* items, int n_items, 
                             const zeb_sphere_tables_t* tb, unsigned flags, float* alm, float* stats,
                             void* scratch, void* stream);
 
+/* The same, sampling each ring only over its span (zeb_sphere_spans): spans[2y], spans[2y+1] =
+ * first φ sample and count (cyclic) of ring y. A ring whose span's end samples meet the detector
+ * for an item is sampled whole for that item, so the result is that of full sampling whatever
+ * the spans; spans NULL samples everything. Replaces Spherical.coefficients as above. */
+int zeb_sphere_coefficients_spans(const float* pats, const float* items, int n_items, const zeb_frame_t* fr,
+                                  const zeb_sphere_tables_t* tb, const int* spans, unsigned flags, float* alm,
+                                  float* stats, void* scratch, void* stream);
+
+/* Ring spans for the detector positions ts[k] (float4 t.x, t.y, t.z, unused; n_t <= 64): per ring
+ * the shortest cyclic run of φ samples holding every sample on the masked detector for any of
+ * them, widened by `margin` samples each side. spans: device int[n_theta][2]. No counterpart in
+ * the reference (which samples every direction): the sampling work of the rings drops to the
+ * detector's footprint. */
+int zeb_sphere_spans(const zeb_frame_t* fr, const zeb_sphere_tables_t* tb, const float* ts, int n_t, int margin,
+                     int* spans, void* stream);
+
 /* ── (b) the SO(3) correlation ──────────────────────────────────────────────────────────── */
 
 typedef struct {

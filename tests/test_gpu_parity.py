@@ -140,6 +140,42 @@ def test_sphere_coefficients_match_oracle(world, lib):
         assert abs(gs[0] - st[0]) < 1e-4 * st[0] and abs(gs[1] - st[1]) < 1e-5 and abs(gs[2] - st[2]) < 1e-4 * st[2]
 
 
+def test_sphere_spans_give_the_full_sampling(world, lib):
+    """Ring spans (zeb_sphere_spans) only drop samples off the detector: coefficients over the spans
+    equal the full sampling's (to float rounding of the window sums' order), also for items far
+    outside the positions the spans were made for (their rings fall back to whole)."""
+    from zebsdsolve_b200.device import BandTables
+
+    s = world["s"]
+    e = s._e
+    L = 32
+    bt = BandTables(L, e.dev)
+    fr = _frame(s)
+    n = world["pats"].shape[0]
+    pats = torch.as_tensor(world["pats"].astype(np.float32), device="cuda").reshape(-1)
+    t = e.positions(np.arange(n)).astype(np.float32)
+    # the spans are made for the first item's position; items 3.. move by up to 6 pixels
+    shift = np.zeros_like(t)
+    shift[3:] = np.random.default_rng(4).uniform(-6, 6, size=(n - 3, 3))
+    tt = t + shift
+    items = torch.as_tensor(np.concatenate([tt, np.arange(n, dtype=np.float32)[:, None]], 1), device="cuda")
+    ts = torch.as_tensor(np.array([[*t[0], 0.0]], np.float32), device="cuda")
+    spans = torch.empty(bt.n_theta * 2, dtype=torch.int32, device="cuda")
+    lib.call("zeb_sphere_spans", ctypes.byref(fr), ctypes.byref(bt.st), P(ts), 1, 2, P(spans), sp())
+    sv = spans.cpu().numpy().reshape(-1, 2)
+    assert (sv[:, 1] < bt.n_phi).any() and (sv[:, 1] == 0).any()  # the spans do cut work
+    out = []
+    for sp_arg in (None, P(spans)):
+        alm = torch.empty(n * bt.n_pairs * 2, device="cuda")
+        stats = torch.empty(n * 4, device="cuda")
+        scr = torch.empty(lib.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), n) // 4 + 1, device="cuda")
+        lib.call("zeb_sphere_coefficients_spans", P(pats), P(items), n, ctypes.byref(fr), ctypes.byref(bt.st), sp_arg, 3,
+                 P(alm), P(stats), P(scr), sp())
+        out.append((alm.cpu().numpy(), stats.cpu().numpy()))
+    assert np.abs(out[0][0] - out[1][0]).max() < 2e-6
+    assert np.allclose(out[0][1], out[1][1], rtol=1e-5, atol=1e-6)
+
+
 def test_master_harmonics_match_oracle(world):
     s = world["s"]
     e = s._e

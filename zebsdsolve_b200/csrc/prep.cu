@@ -37,6 +37,49 @@ __device__ __forceinline__ float2 wide_cell(int jr, int n, int s) {
   return make_float2(0.5f * (float)(lo + hi - 1), (float)(hi - lo));
 }
 
+// zero mean and unit norm under the mask (prep.wgsl:405-443), or the plain copy out
+__device__ void prep_finish(const PrepArgs& a, float* img, float* out, float* red) {
+  const int h = a.h, w = a.w, hw = h * w;
+  if (!a.normalize) {
+    if (a.use_smem)
+      for (int i = threadIdx.x; i < hw; i += blockDim.x) out[i] = img[i];
+    return;
+  }
+  float v2[2] = {0.f, 0.f};
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+    int r = i / w, c = i - r * w;
+    float dr = (float)r - a.mask[0], dc = (float)c - a.mask[1];
+    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) {
+      v2[0] += img[i];
+      v2[1] += 1.f;
+    }
+  }
+  block_sums<2>(v2, red);
+  const float mean = v2[0] / fmaxf(v2[1], 1.f);
+  float ss[1] = {0.f};
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+    int r = i / w, c = i - r * w;
+    float dr = (float)r - a.mask[0], dc = (float)c - a.mask[1];
+    float v = 0.f;
+    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) v = img[i] - mean;
+    img[i] = v;
+    ss[0] += v * v;
+  }
+  block_sums<1>(ss, red);
+  const float inv = rsqrtf(fmaxf(ss[0], 1e-30f));
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) out[i] = img[i] * inv;
+}
+
+// unpack one stored pixel (u8, u16 or f32) and take the static background off
+__device__ __forceinline__ float prep_pixel(const PrepArgs& a, size_t base, int i) {
+  float v;
+  if (a.pixel == 0) v = (float)((const uint8_t*)a.raw)[base + i];
+  else if (a.pixel == 1) v = (float)((const uint16_t*)a.raw)[base + i];
+  else v = ((const float*)a.raw)[base + i];
+  if (a.static_bg) v -= __ldg(a.static_bg + i);
+  return v;
+}
+
 __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
   extern __shared__ float sm[];
   __shared__ float taps[64];
@@ -173,36 +216,91 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
     (void)bg;
   }
 
-  float* out = a.out + base;
-  if (!a.normalize) {
-    if (a.use_smem)
-      for (int i = threadIdx.x; i < hw; i += blockDim.x) out[i] = img[i];
-    return;
+  prep_finish(a, img, a.out + base, red);
+}
+
+
+// The direct blur with the image, its zero-padded rows P[h][w + 2R] and the zero-padded row-blurred
+// image Q[h + 2R][w] all in shared memory: each thread takes four rows of one column, so every tap
+// is one broadcast tap load, four conflict-free loads and four FMAs, with no bounds tests; the
+// taps inside the image are summed once per column (rows), the sums in the order of k_prep, so
+// the results are the same bits.
+__global__ void __launch_bounds__(256) k_prep_direct(PrepArgs a) {
+  extern __shared__ float sm[];
+  __shared__ float taps[127];
+  __shared__ float gsum[2][512];  // Σ taps inside the image, per column and per row
+  __shared__ float red[2 * 8];
+  const int b = blockIdx.x;
+  const int h = a.h, w = a.w, hw = h * w, R = a.radius;
+  const int pw = w + 2 * R, ph = h + 2 * R;
+  float* img = sm;
+  float* P = img + hw;
+  float* Q = P + h * pw;
+  const size_t base = (size_t)b * hw;
+  for (int d = threadIdx.x; d <= 2 * R; d += blockDim.x) {
+    const int dd = abs(d - R);
+    taps[d] = expf(-(float)(dd * dd) * a.k0);
   }
-  // zero mean and unit norm under the mask (prep.wgsl:405-443)
-  float v2[2] = {0.f, 0.f};
+  for (int i = threadIdx.x; i < h * pw; i += blockDim.x) P[i] = 0.f;
+  for (int i = threadIdx.x; i < R * w; i += blockDim.x) {
+    Q[i] = 0.f;
+    Q[(R + h) * w + i] = 0.f;
+  }
+  __syncthreads();
   for (int i = threadIdx.x; i < hw; i += blockDim.x) {
-    int r = i / w, c = i - r * w;
-    float dr = (float)r - a.mask[0], dc = (float)c - a.mask[1];
-    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) {
-      v2[0] += img[i];
-      v2[1] += 1.f;
+    const int r = i / w, c = i - r * w;
+    const float v = prep_pixel(a, base, i);
+    img[i] = v;
+    P[r * pw + R + c] = v;
+  }
+  for (int k = threadIdx.x; k < w + h; k += blockDim.x) {
+    const int n = k < w ? w : h, c = k < w ? k : k - w;
+    float g = 0.f;
+    for (int x = max(c - R, 0); x <= min(c + R, n - 1); ++x) g += taps[x - c + R];
+    gsum[k < w ? 0 : 1][c] = g;
+  }
+  __syncthreads();
+  // along the rows: Q[R + r][c] = Σ_d taps[d] P[r][c + d] / gsum_col[c]
+  const int rb = (h + 3) / 4;
+  for (int t = threadIdx.x; t < rb * w; t += blockDim.x) {
+    const int r0 = (t / w) * 4, c = t - (t / w) * w;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    const int nk = min(4, h - r0);
+    for (int d = 0; d <= 2 * R; ++d) {
+      const float tv = taps[d];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k < nk) acc[k] = fmaf(tv, P[(r0 + k) * pw + c + d], acc[k]);
+    }
+    const float g = gsum[0][c];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < nk) Q[(R + r0 + k) * w + c] = acc[k] / g;
+  }
+  __syncthreads();
+  // along the columns: the background, combined with the image in place
+  for (int t = threadIdx.x; t < rb * w; t += blockDim.x) {
+    const int r0 = (t / w) * 4, c = t - (t / w) * w;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    const int nk = min(4, h - r0);
+    for (int d = 0; d <= 2 * R; ++d) {
+      const float tv = taps[d];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (k < nk) acc[k] = fmaf(tv, Q[(r0 + k + d) * w + c], acc[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k < nk) {
+        const int i = (r0 + k) * w + c;
+        const float bgv = acc[k] / gsum[1][r0 + k];
+        img[i] = a.dynamic == 1 ? img[i] - bgv : img[i] / fmaxf(bgv, 1e-6f);
+      }
     }
   }
-  block_sums<2>(v2, red);
-  const float mean = v2[0] / fmaxf(v2[1], 1.f);
-  float ss[1] = {0.f};
-  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
-    int r = i / w, c = i - r * w;
-    float dr = (float)r - a.mask[0], dc = (float)c - a.mask[1];
-    float v = 0.f;
-    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) v = img[i] - mean;
-    img[i] = v;
-    ss[0] += v * v;
-  }
-  block_sums<1>(ss, red);
-  const float inv = rsqrtf(fmaxf(ss[0], 1e-30f));
-  for (int i = threadIdx.x; i < hw; i += blockDim.x) out[i] = img[i] * inv;
+  __syncthreads();
+  (void)ph;
+  prep_finish(a, img, a.out + base, red);
 }
 
 struct WideDims {
@@ -274,6 +372,14 @@ extern "C" int zeb_prep_ex(const void* raw, int pixel, int n, int h, int w, cons
       a.wradius = (int)ceil(4.0 * cs);
       a.kx = (float)(1.0 / (2.0 * cs * cs));
       a.kz = (float)(1.0 / (2.0 * sf * sf));
+    }
+  }
+  if (a.dynamic && a.bin < 2 && a.use_smem && h <= 512 && w <= 512) {
+    const size_t dsm = 4 * ((size_t)h * w + (size_t)h * (w + 2 * a.radius) + (size_t)(h + 2 * a.radius) * w);
+    if (dsm <= 200 * 1024) {
+      cudaFuncSetAttribute(k_prep_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+      k_prep_direct<<<n, 256, dsm, (cudaStream_t)stream>>>(a);
+      return zeb_launch_check("prep (direct blur)");
     }
   }
   size_t smem = a.use_smem ? 2 * (size_t)h * w * 4 : 0;

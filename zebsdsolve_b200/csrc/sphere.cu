@@ -7,6 +7,10 @@
 // with its mirror as one complex line (ring real, mirror imaginary), window-mean centred,
 // transforms it along φ in shared memory and keeps of the two spectra their orders m < L as
 // sum and difference (sphere.wgsl:128-269).
+// With ring spans (zeb_sphere_spans: per ring the cyclic run of φ samples that can meet the
+// detector, with a margin), only those samples are taken; a ring whose span's end samples are
+// themselves on the detector (the span did not cover this item) is taken whole, so the result
+// equals the full sampling.  Ring pairs with no samples get zero spectra without a transform.
 // k_legendre: contracts the ring spectra with the weighted Legendre table, a block per
 // (order m, tile of items) with the table's rows for m staged in shared memory (sphere.wgsl:
 // 271-288). k_sh_norm: unit harmonic norm and the item's stats (sphere.wgsl:290-324).
@@ -30,6 +34,7 @@ struct SphereArgs {
   float* stats;     // [item][4]
   int lines_per_chunk;
   int pat_in_smem;
+  const int2* spans;  // [n_theta] (first φ sample, count), cyclic; null: every sample
 };
 
 struct Sampler {
@@ -66,9 +71,26 @@ struct Sampler {
   }
 };
 
+// index of the last prefix entry <= e (prefix[0] = 0, non-decreasing, n + 1 entries)
+__device__ __forceinline__ int span_of(const int* prefix, int n, int e) {
+  int lo = 0, hi = n;  // prefix[lo] <= e < prefix[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (prefix[mid] <= e) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+constexpr int SPH_MAX_THETA = 512;
+
 __global__ void __launch_bounds__(256) k_sphere_rings(SphereArgs a) {
   extern __shared__ float4 smem4[];
   __shared__ float red[2 * 8];
+  __shared__ int2 sp[SPH_MAX_THETA];        // this item's spans (whole rings where a span fell short)
+  __shared__ int pre[SPH_MAX_THETA + 1];    // prefix sums of span counts
+  __shared__ int act[SPH_MAX_THETA / 2];    // ring pairs with samples
+  __shared__ int n_act;
   const int b = blockIdx.x;
   const int hw = a.h * a.w;
   float2* lines = (float2*)smem4;
@@ -94,13 +116,41 @@ __global__ void __launch_bounds__(256) k_sphere_rings(SphereArgs a) {
   s.c2t = dot3(s.c2, s.t);
   s.mask[0] = a.mask[0]; s.mask[1] = a.mask[1]; s.mask[2] = a.mask[2];
   s.window = window;
+  const int nphi = a.n_phi, nt = a.n_theta, lg = a.lg_phi, nh = nt / 2, L = a.L;
+  const int pmask = nphi - 1;
+
+  // spans: the table's, widened to the whole ring where an end sample is on the detector
+  for (int y = threadIdx.x; y < nt; y += blockDim.x) {
+    int2 v = a.spans ? a.spans[y] : make_int2(0, nphi);
+    if (v.y > 0 && v.y < nphi) {
+      const float4 rg = __ldg(a.ring + y);
+      const float2 c0 = __ldg(a.phi_cs + (v.x & pmask)), c1 = __ldg(a.phi_cs + ((v.x + v.y - 1) & pmask));
+      const float w0 = s.sample(make_float3(rg.y * c0.x, rg.y * c0.y, rg.x)).y;
+      const float w1 = s.sample(make_float3(rg.y * c1.x, rg.y * c1.y, rg.x)).y;
+      if (w0 > 0.f || w1 > 0.f) v = make_int2(0, nphi);
+    }
+    sp[y] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0, na = 0;
+    for (int y = 0; y < nt; ++y) {
+      pre[y] = acc;
+      acc += sp[y].y;
+    }
+    pre[nt] = acc;
+    for (int y = 0; y < nh; ++y)
+      if (sp[y].y > 0 || sp[nt - 1 - y].y > 0) act[na++] = y;
+    n_act = na;
+  }
   __syncthreads();
 
-  // the window's sums over the whole grid
-  const int nphi = a.n_phi, nt = a.n_theta, lg = a.lg_phi;
+  // the window's sums over the spans
   float acc[2] = {0.f, 0.f};
-  for (int e = threadIdx.x; e < nt * nphi; e += blockDim.x) {
-    int y = e >> lg, j = e & (nphi - 1);
+  const int total = pre[nt];
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int y = span_of(pre, nt, e);
+    const int j = (sp[y].x + (e - pre[y])) & pmask;
     float4 rg = __ldg(a.ring + y);
     float2 cs = __ldg(a.phi_cs + j);
     float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
@@ -114,26 +164,47 @@ __global__ void __launch_bounds__(256) k_sphere_rings(SphereArgs a) {
     a.stats[b * 4 + 1] = mean;
   }
 
-  // ring pairs, a chunk of lines at a time
-  const int nh = nt / 2, L = a.L;
+  // ring pairs without samples: zero spectra
+  float4* outb = a.spectra + (size_t)b * nh * L;
+  for (int e = threadIdx.x; e < nh * L; e += blockDim.x) {
+    const int y = e / L;
+    if (sp[y].y == 0 && sp[nt - 1 - y].y == 0) outb[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+
+  // the others, a chunk of lines at a time: slot i holds pair act[c0 + i] (ring real, mirror
+  // imaginary), zero where not sampled
+  const int na = n_act;
   const int CH = a.lines_per_chunk;
   RowLines idx{lg};
-  for (int y0 = 0; y0 < nh; y0 += CH) {
-    const int cnt = min(CH, nh - y0);
-    for (int e = threadIdx.x; e < cnt * nphi; e += blockDim.x) {
-      int i = e >> lg, j = e & (nphi - 1);
-      int y = y0 + i;
-      float4 rn = __ldg(a.ring + y), rs = __ldg(a.ring + (nt - 1 - y));
-      float2 cs = __ldg(a.phi_cs + j);
-      float2 gn = s.sample(make_float3(rn.y * cs.x, rn.y * cs.y, rn.x));
-      float2 gs = s.sample(make_float3(rs.y * cs.x, rs.y * cs.y, rs.x));
-      lines[idx(i, bitrev(j, lg))] = make_float2((gn.x - mean) * gn.y, (gs.x - mean) * gs.y);
+  __shared__ int cpre[2 * 64 + 1];  // (slot, side) prefix of the chunk; lines_per_chunk <= 64
+  for (int c0 = 0; c0 < na; c0 += CH) {
+    const int cnt = min(CH, na - c0);
+    for (int e = threadIdx.x; e < cnt * nphi; e += blockDim.x) lines[e] = make_float2(0.f, 0.f);
+    if (threadIdx.x == 0) {
+      int q = 0;
+      for (int k = 0; k < 2 * cnt; ++k) {
+        cpre[k] = q;
+        const int y = act[c0 + (k >> 1)];
+        q += sp[(k & 1) ? nt - 1 - y : y].y;
+      }
+      cpre[2 * cnt] = q;
+    }
+    __syncthreads();
+    const int ctot = cpre[2 * cnt];
+    for (int e = threadIdx.x; e < ctot; e += blockDim.x) {
+      const int k = span_of(cpre, 2 * cnt, e);
+      const int i = k >> 1, side = k & 1;
+      const int y = side ? nt - 1 - act[c0 + i] : act[c0 + i];
+      const int j = (sp[y].x + (e - cpre[k])) & pmask;
+      const float4 rg = __ldg(a.ring + y);
+      const float2 cs = __ldg(a.phi_cs + j);
+      const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
+      ((float*)&lines[idx(i, bitrev(j, lg))])[side] = (g.x - mean) * g.y;
     }
     __syncthreads();
     fft_lines_smem(lines, cnt, lg, a.tw, idx);
     // the two apart: Z = N + iS for real N, S gives N_m = (Z_m + conj Z_{n−m})/2 and
     // S_m = (Z_m − conj Z_{n−m})/2i; keep (N+S, N−S) for m < L
-    float4* out = a.spectra + ((size_t)b * nh + y0) * L;
     for (int e = threadIdx.x; e < cnt * L; e += blockDim.x) {
       int i = e / L, m = e - i * L;
       float2 z = lines[idx(i, m)];
@@ -141,9 +212,64 @@ __global__ void __launch_bounds__(256) k_sphere_rings(SphereArgs a) {
       float2 rn = make_float2(0.5f * (z.x + zr.x), 0.5f * (z.y - zr.y));
       float2 dd = make_float2(z.x - zr.x, z.y + zr.y);
       float2 rs = make_float2(0.5f * dd.y, -0.5f * dd.x);
-      out[e] = make_float4(rn.x + rs.x, rn.y + rs.y, rn.x - rs.x, rn.y - rs.y);
+      outb[(size_t)act[c0 + i] * L + m] = make_float4(rn.x + rs.x, rn.y + rs.y, rn.x - rs.x, rn.y - rs.y);
     }
     __syncthreads();
+  }
+}
+
+// Spans of the sphere's rings for a set of detector positions: per ring, the shortest cyclic run
+// of φ samples holding every sample that meets the masked detector for any of the n_t positions,
+// widened by `margin` samples on each side ((0, 0): none; (0, n_φ): the whole ring).
+__global__ void k_sphere_spans(SphereArgs a, const float4* __restrict__ ts, int n_t, int margin, int2* spans) {
+  __shared__ unsigned char hit[ZEB_TW_LEN];
+  const int y = blockIdx.x, nphi = a.n_phi;
+  const float4 rg = __ldg(a.ring + y);
+  Sampler s;
+  s.pat = nullptr;
+  s.h = a.h; s.w = a.w;
+  s.c0 = make_float3(a.c0[0], a.c0[1], a.c0[2]);
+  s.c1 = make_float3(a.c1[0], a.c1[1], a.c1[2]);
+  s.c2 = make_float3(a.c2[0], a.c2[1], a.c2[2]);
+  s.mask[0] = a.mask[0]; s.mask[1] = a.mask[1]; s.mask[2] = a.mask[2];
+  s.window = true;
+  for (int j = threadIdx.x; j < nphi; j += blockDim.x) {
+    const float2 cs = __ldg(a.phi_cs + j);
+    const float3 d = make_float3(rg.y * cs.x, rg.y * cs.y, rg.x);
+    unsigned char h = 0;
+    for (int k = 0; k < n_t; ++k) {
+      s.t = make_float3(ts[k].x, ts[k].y, ts[k].z);
+      s.c2t = dot3(s.c2, s.t);
+      if (s.sample(d).y > 0.f) h = 1;
+    }
+    hit[j] = h;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // the longest cyclic run of misses; the span is its complement
+    int first = -1;
+    for (int j = 0; j < nphi; ++j)
+      if (hit[j]) { first = j; break; }
+    int2 out = make_int2(0, 0);
+    if (first >= 0) {
+      int best = 0, best_end = first, run = 0;
+      for (int k = 1; k <= nphi; ++k) {
+        const int j = (first + k) % nphi;
+        if (hit[j]) {
+          if (run > best) { best = run; best_end = j; }
+          run = 0;
+        } else {
+          ++run;
+        }
+      }
+      // hits lie in [best_end, best_end + nphi − best): start after the longest gap
+      int start = best_end, count = nphi - best;
+      start -= margin;
+      count += 2 * margin;
+      if (count >= nphi) out = make_int2(0, nphi);
+      else out = make_int2(((start % nphi) + nphi) % nphi, count);
+    }
+    spans[y] = out;
   }
 }
 
@@ -225,28 +351,54 @@ extern "C" size_t zeb_sphere_scratch_bytes(const zeb_sphere_tables_t* tb, int n_
   return (size_t)n_items * (tb->n_theta / 2) * tb->L * sizeof(float4);
 }
 
-extern "C" int zeb_sphere_coefficients(const float* pats, const float* items, int n_items, const zeb_frame_t* fr,
-                                       const zeb_sphere_tables_t* tb, unsigned flags, float* alm, float* stats,
-                                       void* scratch, void* stream) {
-  ZEB_REQUIRE(items && fr && tb && alm && stats && scratch, ZEB_EARG, "sphere_coefficients: null argument");
-  ZEB_REQUIRE((flags & ZEB_FLAG_WINDOW) || pats, ZEB_EARG, "sphere_coefficients: patterns missing");
-  ZEB_REQUIRE(tb->ring && tb->phi_cs && tb->wplm && tb->tw, ZEB_EARG, "sphere_coefficients: table missing");
+static bool sphere_fill(SphereArgs& a, const zeb_frame_t* fr, const zeb_sphere_tables_t* tb) {
   const int L = tb->L, nphi = tb->n_phi, nt = tb->n_theta;
-  ZEB_REQUIRE(L >= 2 && L <= 256 && nt >= 2 * L - 1 && (nphi & (nphi - 1)) == 0 && nphi >= 32 && nphi <= ZEB_TW_LEN &&
-                  nt % 2 == 0 && tb->n_pairs == L * (L + 1) / 2 && fr->h >= 2 && fr->w >= 2 && L <= nphi / 2,
-              ZEB_EARG, "sphere_coefficients: bad tables L=%d nt=%d nphi=%d", L, nt, nphi);
-  if (n_items == 0) return ZEB_OK;
-  SphereArgs a{};
-  a.pats = pats; a.items = (const float4*)items; a.n_items = n_items; a.h = fr->h; a.w = fr->w;
+  if (!(L >= 2 && L <= 256 && nt >= 2 * L - 1 && nt <= SPH_MAX_THETA && (nphi & (nphi - 1)) == 0 && nphi >= 32 &&
+        nphi <= ZEB_TW_LEN && nt % 2 == 0 && tb->n_pairs == L * (L + 1) / 2 && fr->h >= 2 && fr->w >= 2 &&
+        L <= nphi / 2))
+    return false;
+  a.h = fr->h; a.w = fr->w;
   for (int k = 0; k < 3; ++k) {
     a.c0[k] = fr->c0[k]; a.c1[k] = fr->c1[k]; a.c2[k] = fr->c2[k]; a.mask[k] = fr->mask[k];
   }
   a.L = L; a.n_theta = nt; a.n_phi = nphi; a.lg_phi = ilog2(nphi); a.n_pairs = tb->n_pairs;
   a.ring = (const float4*)tb->ring; a.phi_cs = (const float2*)tb->phi_cs; a.wplm = tb->wplm;
-  a.tw = (const float2*)tb->tw; a.flags = flags;
+  a.tw = (const float2*)tb->tw;
+  return true;
+}
+
+extern "C" int zeb_sphere_spans(const zeb_frame_t* fr, const zeb_sphere_tables_t* tb, const float* ts, int n_t,
+                                int margin, int* spans, void* stream) {
+  ZEB_REQUIRE(fr && tb && ts && spans && n_t >= 1 && n_t <= 64 && margin >= 0, ZEB_EARG, "sphere_spans: bad arguments");
+  ZEB_REQUIRE(tb->ring && tb->phi_cs, ZEB_EARG, "sphere_spans: table missing");
+  SphereArgs a{};
+  ZEB_REQUIRE(sphere_fill(a, fr, tb), ZEB_EARG, "sphere_spans: bad tables");
+  k_sphere_spans<<<tb->n_theta, 256, 0, (cudaStream_t)stream>>>(a, (const float4*)ts, n_t, margin, (int2*)spans);
+  return zeb_launch_check("sphere_spans");
+}
+
+extern "C" int zeb_sphere_coefficients(const float* pats, const float* items, int n_items, const zeb_frame_t* fr,
+                                       const zeb_sphere_tables_t* tb, unsigned flags, float* alm, float* stats,
+                                       void* scratch, void* stream) {
+  return zeb_sphere_coefficients_spans(pats, items, n_items, fr, tb, nullptr, flags, alm, stats, scratch, stream);
+}
+
+extern "C" int zeb_sphere_coefficients_spans(const float* pats, const float* items, int n_items, const zeb_frame_t* fr,
+                                             const zeb_sphere_tables_t* tb, const int* spans, unsigned flags,
+                                             float* alm, float* stats, void* scratch, void* stream) {
+  ZEB_REQUIRE(items && fr && tb && alm && stats && scratch, ZEB_EARG, "sphere_coefficients: null argument");
+  ZEB_REQUIRE((flags & ZEB_FLAG_WINDOW) || pats, ZEB_EARG, "sphere_coefficients: patterns missing");
+  ZEB_REQUIRE(tb->ring && tb->phi_cs && tb->wplm && tb->tw, ZEB_EARG, "sphere_coefficients: table missing");
+  const int L = tb->L, nphi = tb->n_phi, nt = tb->n_theta;
+  SphereArgs a{};
+  ZEB_REQUIRE(sphere_fill(a, fr, tb), ZEB_EARG, "sphere_coefficients: bad tables L=%d nt=%d nphi=%d", L, nt, nphi);
+  if (n_items == 0) return ZEB_OK;
+  a.pats = pats; a.items = (const float4*)items; a.n_items = n_items;
+  a.flags = flags;
+  a.spans = (const int2*)spans;
   a.spectra = (float4*)scratch; a.alm = (float2*)alm; a.stats = stats;
   // a chunk of lines of 32 KB, whole lines
-  a.lines_per_chunk = max(1, min(nt / 2, 4096 / nphi));
+  a.lines_per_chunk = max(1, min(min(nt / 2, 64), 4096 / nphi));
   size_t hw = (size_t)fr->h * fr->w;
   size_t lines_bytes = (size_t)a.lines_per_chunk * nphi * sizeof(float2);
   a.pat_in_smem = (!(flags & ZEB_FLAG_WINDOW) && hw * 4 + lines_bytes <= 200 * 1024) ? 1 : 0;

@@ -125,6 +125,9 @@ class Engine:
         self.index_accepted = 0
         self.index_region = 0
         self._buf = {}
+        self._batch_t = None  # bounding box of the last batch's detector positions
+        self._spans = {}
+        self._pinned = None
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
 
     # ── plumbing ──
@@ -416,7 +419,30 @@ class Engine:
     def items_of(self, cells):
         cells = np.asarray(cells, np.int64)
         t = self.positions(cells)
+        self._batch_t = (t.min(0), t.max(0)) if len(t) else None
         return torch.as_tensor(np.concatenate([t, np.arange(len(cells), dtype=np.float32)[:, None]], 1), device=self.dev)
+
+    def spans(self, bt, fr):
+        """The sphere's ring spans for the detector positions of the last items_of batch: the
+        corners of their bounding box, two samples of margin (cached per geometry and box)."""
+        if self._batch_t is None:
+            return None
+        lo, hi = self._batch_t
+        key = (bt.L, tuple(fr.c0), tuple(fr.c1), tuple(fr.c2), fr.h, fr.w, tuple(fr.mask),
+               tuple(np.round(lo, 3)), tuple(np.round(hi, 3)))
+        hit = self._spans.get(key)
+        if hit is not None:
+            return hit
+        if len(self._spans) > 64:
+            self._spans = {}
+        corners = np.array([[x, y, z, 0.0] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])],
+                           np.float32)
+        ts = torch.as_tensor(corners, device=self.dev)
+        sp = torch.empty(bt.n_theta * 2, dtype=torch.int32, device=self.dev)
+        N.call("zeb_sphere_spans", ctypes.byref(fr), ctypes.byref(bt.st), ptr(ts), len(corners), 2, ptr(sp),
+               stream_ptr())
+        self._spans[key] = sp
+        return sp
 
     def run_device(self, raw, cells, bandwidth=None, timer=None):
         """One pass of the device path over n = len(cells) stored patterns already on the device:
@@ -437,8 +463,9 @@ class Engine:
         stats = self.buf("stats", n * 4)
         sphere_scratch = self.buf("sphere_scratch", N.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), n) // 4 + 1)
         mark("sphere")
-        N.call("zeb_sphere_coefficients", ptr(pats), ptr(items), n, ctypes.byref(fr), ctypes.byref(bt.st),
-               FLAG_CENTER | FLAG_NORM, ptr(alm), ptr(stats), ptr(sphere_scratch), stream_ptr())
+        spans = self.spans(bt, fr)
+        N.call("zeb_sphere_coefficients_spans", ptr(pats), ptr(items), n, ctypes.byref(fr), ctypes.byref(bt.st),
+               ptr(spans), FLAG_CENTER | FLAG_NORM, ptr(alm), ptr(stats), ptr(sphere_scratch), stream_ptr())
         opts = N.RefineOpts(s["refine_iters"] if s["refine"] else 0, math.radians(s["refine_step"]), 1.0, 0.02, 1e4,
                             s["nmi_bins"], float(self.batch_stamp))
         for pi, p in enumerate(self.phases):
