@@ -110,12 +110,12 @@ def _frame(s):
     return e.frame()
 
 
-def test_sphere_coefficients_match_oracle(world, lib):
+@pytest.mark.parametrize("L", [16, 64])  # n_phi 64 (the block kernel) and 256 (a warp per ring pair)
+def test_sphere_coefficients_match_oracle(world, lib, L):
     from zebsdsolve_b200.device import BandTables
 
     s = world["s"]
     e = s._e
-    L = 16
     bt = BandTables(L, e.dev)
     fr = _frame(s)
     n = world["pats"].shape[0]
@@ -140,7 +140,8 @@ def test_sphere_coefficients_match_oracle(world, lib):
         assert abs(gs[0] - st[0]) < 1e-4 * st[0] and abs(gs[1] - st[1]) < 1e-5 and abs(gs[2] - st[2]) < 1e-4 * st[2]
 
 
-def test_sphere_spans_give_the_full_sampling(world, lib):
+@pytest.mark.parametrize("L", [32, 64])
+def test_sphere_spans_give_the_full_sampling(world, lib, L):
     """Ring spans (zeb_sphere_spans) only drop samples off the detector: coefficients over the spans
     equal the full sampling's (to float rounding of the window sums' order), also for items far
     outside the positions the spans were made for (their rings fall back to whole)."""
@@ -148,7 +149,6 @@ def test_sphere_spans_give_the_full_sampling(world, lib):
 
     s = world["s"]
     e = s._e
-    L = 32
     bt = BandTables(L, e.dev)
     fr = _frame(s)
     n = world["pats"].shape[0]

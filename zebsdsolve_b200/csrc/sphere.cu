@@ -35,6 +35,7 @@ struct SphereArgs {
   int lines_per_chunk;
   int pat_in_smem;
   const int2* spans;  // [n_theta] (first φ sample, count), cyclic; null: every sample
+  int ring_major;     // spectra laid out [item][m][ring pair] (else [item][ring pair][m])
 };
 
 struct Sampler {
@@ -218,6 +219,226 @@ __global__ void __launch_bounds__(256) k_sphere_rings(SphereArgs a) {
   }
 }
 
+// forward 8-point DFT in registers (radix-2, decimation in time, natural order in and out)
+__device__ __forceinline__ void fft_reg8(float2 (&x)[8]) {
+  const float r = 0.70710678118654752f;
+  float2 t;
+  t = x[1]; x[1] = x[4]; x[4] = t;
+  t = x[3]; x[3] = x[6]; x[6] = t;
+#pragma unroll
+  for (int i = 0; i < 8; i += 2) {
+    const float2 p = x[i], q = x[i + 1];
+    x[i] = make_float2(p.x + q.x, p.y + q.y);
+    x[i + 1] = make_float2(p.x - q.x, p.y - q.y);
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i += 4) {
+    float2 p = x[i], q = x[i + 2];
+    x[i] = make_float2(p.x + q.x, p.y + q.y);
+    x[i + 2] = make_float2(p.x - q.x, p.y - q.y);
+    p = x[i + 1];
+    q = make_float2(x[i + 3].y, -x[i + 3].x);  // × e^{−iπ/2}
+    x[i + 1] = make_float2(p.x + q.x, p.y + q.y);
+    x[i + 3] = make_float2(p.x - q.x, p.y - q.y);
+  }
+  {
+    float2 p = x[0], q = x[4];
+    x[0] = make_float2(p.x + q.x, p.y + q.y);
+    x[4] = make_float2(p.x - q.x, p.y - q.y);
+    p = x[1];
+    q = make_float2(r * (x[5].x + x[5].y), r * (x[5].y - x[5].x));  // × e^{−iπ/4}
+    x[1] = make_float2(p.x + q.x, p.y + q.y);
+    x[5] = make_float2(p.x - q.x, p.y - q.y);
+    p = x[2];
+    q = make_float2(x[6].y, -x[6].x);  // × e^{−iπ/2}
+    x[2] = make_float2(p.x + q.x, p.y + q.y);
+    x[6] = make_float2(p.x - q.x, p.y - q.y);
+    p = x[3];
+    q = make_float2(r * (x[7].y - x[7].x), -r * (x[7].x + x[7].y));  // × e^{−3iπ/4}
+    x[3] = make_float2(p.x + q.x, p.y + q.y);
+    x[7] = make_float2(p.x - q.x, p.y - q.y);
+  }
+}
+
+// ── the rings of one item, a warp per ring pair, for n_φ = 256 ──
+//
+// The block holds the item's pattern and the φ cosines; after the window sums (over the spans),
+// each warp takes one ring pair with samples at a time: it zeroes its 256-point line, samples the
+// northern ring (real part) and its mirror (imaginary part) over their spans, and transforms the
+// line with no block barrier: lane l holds points l + 32k (k < 8), takes the 8-point DFT over k in
+// registers, multiplies by e^{−2πi l k₁/256}, then the 32-point DFT over the lanes by five radix-2
+// stages of shuffles (decimation in frequency, so lane l ends with output bit-reverse(l)); the
+// outputs go back to the line (a padded order without bank conflicts) and the lanes split N and S
+// for m < L.  Spectra are written [item][m][ring pair].
+constexpr int RW_WARPS = 8;
+constexpr int RW_PAD = 256 + 32;  // line slots per warp: F + F/8
+
+__device__ __forceinline__ int rw_slot(int f) { return f + (f >> 3); }
+
+__global__ void __launch_bounds__(RW_WARPS * 32) k_sphere_rings_w(SphereArgs a) {
+  extern __shared__ float4 smem4[];
+  __shared__ float red[2 * 8];
+  __shared__ int2 sp[SPH_MAX_THETA];
+  __shared__ int pre[SPH_MAX_THETA + 1];
+  __shared__ int act[SPH_MAX_THETA / 2];
+  __shared__ int n_act;
+  __shared__ float2 pcs[256];
+  const int b = blockIdx.x;
+  const int hw = a.h * a.w;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* lines = (float2*)smem4;                 // [RW_WARPS][RW_PAD]
+  float* spat = (float*)(lines + RW_WARPS * RW_PAD);
+  const float4 it = a.items[b];
+  const bool window = (a.flags & ZEB_FLAG_WINDOW) != 0;
+  Sampler s;
+  s.pat = nullptr;
+  if (!window) {
+    const float* src = a.pats + (size_t)(int)it.w * hw;
+    if (a.pat_in_smem) {
+      for (int i = threadIdx.x; i < hw; i += blockDim.x) spat[i] = src[i];
+      s.pat = spat;
+    } else {
+      s.pat = src;
+    }
+  }
+  s.h = a.h; s.w = a.w;
+  s.c0 = make_float3(a.c0[0], a.c0[1], a.c0[2]);
+  s.c1 = make_float3(a.c1[0], a.c1[1], a.c1[2]);
+  s.c2 = make_float3(a.c2[0], a.c2[1], a.c2[2]);
+  s.t = make_float3(it.x, it.y, it.z);
+  s.c2t = dot3(s.c2, s.t);
+  s.mask[0] = a.mask[0]; s.mask[1] = a.mask[1]; s.mask[2] = a.mask[2];
+  s.window = window;
+  constexpr int nphi = 256, pmask = 255;
+  const int nt = a.n_theta, nh = nt / 2, L = a.L;
+  for (int j = threadIdx.x; j < nphi; j += blockDim.x) pcs[j] = __ldg(a.phi_cs + j);
+  __syncthreads();
+
+  for (int y = threadIdx.x; y < nt; y += blockDim.x) {
+    int2 v = a.spans ? a.spans[y] : make_int2(0, nphi);
+    if (v.y > 0 && v.y < nphi) {
+      const float4 rg = __ldg(a.ring + y);
+      const float2 c0 = pcs[v.x & pmask], c1 = pcs[(v.x + v.y - 1) & pmask];
+      const float w0 = s.sample(make_float3(rg.y * c0.x, rg.y * c0.y, rg.x)).y;
+      const float w1 = s.sample(make_float3(rg.y * c1.x, rg.y * c1.y, rg.x)).y;
+      if (w0 > 0.f || w1 > 0.f) v = make_int2(0, nphi);
+    }
+    sp[y] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0, na = 0;
+    for (int y = 0; y < nt; ++y) {
+      pre[y] = acc;
+      acc += sp[y].y;
+    }
+    pre[nt] = acc;
+    for (int y = 0; y < nh; ++y)
+      if (sp[y].y > 0 || sp[nt - 1 - y].y > 0) act[na++] = y;
+    n_act = na;
+  }
+  __syncthreads();
+
+  // the window's sums over the spans
+  float acc[2] = {0.f, 0.f};
+  const int total = pre[nt];
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int y = span_of(pre, nt, e);
+    const int j = (sp[y].x + (e - pre[y])) & pmask;
+    const float4 rg = __ldg(a.ring + y);
+    const float2 cs = pcs[j];
+    const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
+    acc[0] += g.x * g.y * rg.z;
+    acc[1] += g.y * rg.z;
+  }
+  block_sums<2>(acc, red);
+  const float mean = (a.flags & ZEB_FLAG_CENTER) ? acc[0] / fmaxf(acc[1], 1e-20f) : 0.f;
+  if (threadIdx.x == 0) {
+    a.stats[b * 4 + 0] = acc[1] * ZEB_TAU / (float)nphi;
+    a.stats[b * 4 + 1] = mean;
+  }
+
+  float4* outb = a.spectra + (size_t)b * L * nh;  // [m][ring pair]
+  for (int e = threadIdx.x; e < nh * L; e += blockDim.x) {
+    const int m = e / nh, y = e - m * nh;
+    if (sp[y].y == 0 && sp[nt - 1 - y].y == 0) outb[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+
+  // this lane's twiddles: e^{−2πi l k₁/256} (k₁ < 8) and, per shuffle stage h, e^{−2πi (l mod h)/(2h)}
+  float2 tw8[8], tws[5];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) tw8[k] = __ldg(a.tw + ((lane * k * 4) & (ZEB_TW_LEN - 1)));
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const int h = 16 >> q;
+    tws[q] = __ldg(a.tw + (lane & (h - 1)) * (ZEB_TW_LEN / (2 * h)));
+  }
+  float2* buf = lines + warp * RW_PAD;
+  const int na = n_act;
+  for (int ai = warp; ai < na; ai += RW_WARPS) {
+    const int y = act[ai], ys = nt - 1 - y;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) buf[lane + 32 * k] = make_float2(0.f, 0.f);
+    __syncwarp();
+    {
+      const float4 rg = __ldg(a.ring + y);
+      const int2 v = sp[y];
+      for (int e = lane; e < v.y; e += 32) {
+        const int j = (v.x + e) & pmask;
+        const float2 cs = pcs[j];
+        const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
+        buf[j].x = (g.x - mean) * g.y;
+      }
+    }
+    {
+      const float4 rg = __ldg(a.ring + ys);
+      const int2 v = sp[ys];
+      for (int e = lane; e < v.y; e += 32) {
+        const int j = (v.x + e) & pmask;
+        const float2 cs = pcs[j];
+        const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
+        buf[j].y = (g.x - mean) * g.y;
+      }
+    }
+    __syncwarp();
+    float2 x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = buf[lane + 32 * k];
+    fft_reg8(x);
+#pragma unroll
+    for (int k = 1; k < 8; ++k) x[k] = cmulf(x[k], tw8[k]);
+    // the 32-point transforms over the lanes, decimation in frequency
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const int h = 16 >> q;
+      const bool upper = (lane & h) != 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const float2 u = make_float2(__shfl_xor_sync(0xffffffffu, x[k].x, h), __shfl_xor_sync(0xffffffffu, x[k].y, h));
+        const float2 sum = make_float2(x[k].x + u.x, x[k].y + u.y);
+        const float2 dif = cmulf(make_float2(u.x - x[k].x, u.y - x[k].y), tws[q]);
+        x[k] = upper ? dif : sum;
+      }
+    }
+    __syncwarp();
+    const int r = (int)(__brev((unsigned)lane) >> 27);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) buf[rw_slot(k + 8 * r)] = x[k];
+    __syncwarp();
+    // the two apart: Z = N + iS for real N, S gives N_m = (Z_m + conj Z_{n−m})/2 and
+    // S_m = (Z_m − conj Z_{n−m})/2i; keep (N+S, N−S) for m < L
+    for (int m = lane; m < L; m += 32) {
+      const float2 z = buf[rw_slot(m)];
+      const float2 zr = buf[rw_slot((nphi - m) & pmask)];
+      const float2 rn = make_float2(0.5f * (z.x + zr.x), 0.5f * (z.y - zr.y));
+      const float2 dd = make_float2(z.x - zr.x, z.y + zr.y);
+      const float2 rs = make_float2(0.5f * dd.y, -0.5f * dd.x);
+      outb[(size_t)m * nh + y] = make_float4(rn.x + rs.x, rn.y + rs.y, rn.x - rs.x, rn.y - rs.y);
+    }
+    __syncwarp();
+  }
+}
+
 // Spans of the sphere's rings for a set of detector positions: per ring, the shortest cyclic run
 // of φ samples holding every sample that meets the masked detector for any of the n_t positions,
 // widened by `margin` samples on each side ((0, 0): none; (0, n_φ): the whole ring).
@@ -287,7 +508,7 @@ __global__ void __launch_bounds__(256) k_legendre(SphereArgs a) {
   const int nb = min(LEG_ITEMS, a.n_items - b0);
   for (int e = threadIdx.x; e < nb * nh; e += blockDim.x) {
     int i = e / nh, y = e - i * nh;
-    spec[e] = a.spectra[((size_t)(b0 + i) * nh + y) * L + m];
+    spec[e] = a.ring_major ? a.spectra[((size_t)(b0 + i) * L + m) * nh + y] : a.spectra[((size_t)(b0 + i) * nh + y) * L + m];
   }
   for (int e = threadIdx.x; e < nh * nl; e += blockDim.x) {
     int y = e / nl, l = e - y * nl;
@@ -404,9 +625,19 @@ extern "C" int zeb_sphere_coefficients_spans(const float* pats, const float* ite
   a.pat_in_smem = (!(flags & ZEB_FLAG_WINDOW) && hw * 4 + lines_bytes <= 200 * 1024) ? 1 : 0;
   size_t smem = lines_bytes + (a.pat_in_smem ? hw * 4 : 0);
   cudaStream_t st = (cudaStream_t)stream;
-  cudaFuncSetAttribute(k_sphere_rings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_sphere_rings<<<n_items, 256, smem, st>>>(a);
-  int rc = zeb_launch_check("sphere_rings");
+  int rc;
+  if (nphi == 256) {
+    // the warp-per-ring-pair kernel
+    a.ring_major = 1;
+    const size_t wsm = (size_t)RW_WARPS * RW_PAD * sizeof(float2) + (a.pat_in_smem ? hw * 4 : 0);
+    cudaFuncSetAttribute(k_sphere_rings_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+    k_sphere_rings_w<<<n_items, RW_WARPS * 32, wsm, st>>>(a);
+    rc = zeb_launch_check("sphere_rings (warps)");
+  } else {
+    cudaFuncSetAttribute(k_sphere_rings, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sphere_rings<<<n_items, 256, smem, st>>>(a);
+    rc = zeb_launch_check("sphere_rings");
+  }
   if (rc) return rc;
   const int nh = nt / 2;
   size_t lsm = (size_t)LEG_ITEMS * nh * sizeof(float4) + (size_t)nh * L * sizeof(float);
