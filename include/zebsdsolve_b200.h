@@ -83,6 +83,12 @@ int zeb_master_blur_pass(const float* src, float* dst, int side, float step, flo
  * Replaces Prep.gradient (src/prep.zig:253-260; shaders/mastersph.wgsl:124-138). */
 int zeb_master_gradient(const float* sheets, float* grad4, int side, void* stream);
 
+/* The sheets and the gradient table with each pixel's right-hand neighbour beside it:
+ * vpair[i] = (M[i], M[i+1]) (2 floats), gpair[i] = (grad4[i], grad4[i+1]) (8 floats, 32-byte
+ * records), [2][side][side] each. The detector kernels read these so that a bilinear lookup takes
+ * one record per row. No counterpart in the reference (its lookups read the four texels). */
+int zeb_master_pairs(const float* sheets, const float* grad4, int side, float* vpair, float* gpair, void* stream);
+
 /* The master sampled (bilinear, FP64 arithmetic on the FP32 sheets) at every point of a
  * Gauss–Legendre grid of n_theta rings (cos θ in x) and n_phi points per ring: out[ring][j].
  * Replaces the sampling loop of master.Harmonics.init (src/master.zig:680-688). */
@@ -224,14 +230,14 @@ typedef struct {
  * memory across the passes. Replaces Detector.seed + Detector.refine (src/detector.zig:178-212;
  * shaders/detector.wgsl seed, refine_init, sums_rot, refine_rot_step, nmi, collect). */
 int zeb_refine(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
-               const zeb_frame_t* fr, const float* master, const float* grad4, int side,
-               const zeb_refine_opts_t* o, float* records, void* stream);
+               const zeb_frame_t* fr, const float* vpair, const float* gpair, int side,
+               const zeb_refine_opts_t* o, float* records, void* stream);  /* tables: zeb_master_pairs */
 
 /* NMI of each item's pattern against the master at `draws` random orientations (Shoemake from
  * a hash of the item and draw): out[draw][b]. Replaces Detector.chanceOf (src/detector.zig:
  * 216-229; shaders/detector.wgsl decoy, nmi). */
 int zeb_chance(const float* pats, const float* items, int n, int draws, const zeb_frame_t* fr,
-               const float* master, int side, int nmi_bins, float* out, void* stream);
+               const float* vpair, int side, int nmi_bins, float* out, void* stream);  /* vpair: zeb_master_pairs */
 
 /* Simulated patterns: the master at q·ray for every pixel of item b (poses[b] = t.xyz, pattern
  * index, q.wxyz): sims[b][h][w]. Replaces Detector.project (src/detector.zig:138-142;

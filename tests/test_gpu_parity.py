@@ -263,7 +263,7 @@ def _refined(lib, e, fr, pd, items, seeds, n):
     recs = torch.empty(n * 8, device="cuda")
     opts = lib.RefineOpts(8, math.radians(2.0), 1.0, 0.02, 1e4, 16, 7.0)
     sd = torch.as_tensor(seeds.astype(np.float32), device="cuda").reshape(-1)
-    lib.call("zeb_refine", P(pd), P(items), P(sd), 8, n, ctypes.byref(fr), P(p.baked[1]), P(p.baked[2]), p.master.side,
+    lib.call("zeb_refine", P(pd), P(items), P(sd), 8, n, ctypes.byref(fr), P(p.baked[3]), P(p.baked[4]), p.master.side,
              ctypes.byref(opts), P(recs), sp())
     return recs.cpu().numpy().reshape(n, 8)
 
@@ -378,7 +378,7 @@ def test_refine_and_nmi_match_oracle(world, lib):
     p = e.phases[0]
     opts = lib.RefineOpts(8, math.radians(2.0), 1.0, 0.02, 1e4, 16, 7.0)
     pd = torch.as_tensor(normed, device="cuda").reshape(-1)
-    lib.call("zeb_refine", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(p.baked[1]), P(p.baked[2]), p.master.side,
+    lib.call("zeb_refine", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(p.baked[3]), P(p.baked[4]), p.master.side,
              ctypes.byref(opts), P(recs), sp())
     got = recs.cpu().numpy().reshape(n, 8)
     grad = od.gradient_table(world["baked"], 151)
@@ -409,7 +409,7 @@ def test_chance_decoys_match_oracle(world, lib):
     out = torch.empty(3 * n, device="cuda")
     pd = torch.as_tensor(normed, device="cuda").reshape(-1)
     p = e.phases[0]
-    lib.call("zeb_chance", P(pd), P(items), n, 3, ctypes.byref(fr), P(p.baked[1]), p.master.side, 16, P(out), sp())
+    lib.call("zeb_chance", P(pd), P(items), n, 3, ctypes.byref(fr), P(p.baked[3]), p.master.side, 16, P(out), sp())
     got = out.cpu().numpy().reshape(3, n)
     frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
     for d in range(3):
@@ -451,11 +451,11 @@ def test_refine_and_chance_on_a_large_detector_match_oracle(world, lib):
     p = e.phases[0]
     opts = lib.RefineOpts(8, math.radians(2.0), 1.0, 0.02, 1e4, 16, 3.0)
     pd = torch.as_tensor(normed, device="cuda").reshape(-1)
-    lib.call("zeb_refine", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(p.baked[1]), P(p.baked[2]), p.master.side,
+    lib.call("zeb_refine", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(p.baked[3]), P(p.baked[4]), p.master.side,
              ctypes.byref(opts), P(recs), sp())
     got = recs.cpu().numpy().reshape(n, 8)
     out = torch.empty(2 * n, device="cuda")
-    lib.call("zeb_chance", P(pd), P(items), n, 2, ctypes.byref(fr), P(p.baked[1]), p.master.side, 16, P(out), sp())
+    lib.call("zeb_chance", P(pd), P(items), n, 2, ctypes.byref(fr), P(p.baked[3]), p.master.side, 16, P(out), sp())
     dec = out.cpu().numpy().reshape(2, n)
     grad = od.gradient_table(world["baked"], 151)
     frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
@@ -497,5 +497,6 @@ def test_index_end_to_end_recovers_orientations(lib, precision):
     s.set_patterns(sims.astype(np.float32).reshape(rows, cols, 60, 60))
     r = s.index()
     dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), q))
-    assert np.median(dis) < 0.15 and dis.max() < 1.0, (np.median(dis), dis.max())
+    bad = np.flatnonzero(dis > 1.0)
+    assert np.median(dis) < 0.15 and dis.max() < 1.0, (np.median(dis), dis.max(), bad.tolist())
     assert (r["phase"] == 0).all()

@@ -158,6 +158,28 @@ __device__ __forceinline__ float4 grad_at(const float4* __restrict__ g, float3 v
   return lerp4(lerp4(a, b, p.tj), lerp4(c, d, p.tj), p.ti);
 }
 
+// The same lookups from the pair tables (zeb_master_pairs): one 32-byte (gradient) or 8-byte
+// (value) record per row of the 2 × 2 neighbourhood, the same arithmetic.
+__device__ __forceinline__ void ldg_v8(const float* p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+
+__device__ __forceinline__ float4 grad_at_pair(const float* __restrict__ gp, float3 v, int side) {
+  SheetPos p = sheet_pos(v, side);
+  float4 a, b, c, d;
+  ldg_v8(gp + 8 * (size_t)p.o, a, b);
+  ldg_v8(gp + 8 * ((size_t)p.o + side), c, d);
+  return lerp4(lerp4(a, b, p.tj), lerp4(c, d, p.tj), p.ti);
+}
+
+__device__ __forceinline__ float master_at_pair(const float2* __restrict__ vp, float3 v, int side) {
+  SheetPos p = sheet_pos(v, side);
+  const float2 t = __ldg(vp + p.o), u = __ldg(vp + p.o + side);
+  return lerpf(lerpf(t.x, t.y, p.tj), lerpf(u.x, u.y, p.tj), p.ti);
+}
+
 // ── block reductions ──
 
 __device__ __forceinline__ float warp_sum(float v) {

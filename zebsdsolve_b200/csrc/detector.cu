@@ -20,8 +20,9 @@ struct DetArgs {
   int n, h, w;
   float3 c0, c1, c2;
   float mask[3];
-  const float* master;
-  const float4* grad;
+  const float* master;   // plain sheets (zeb_project)
+  const float2* vpair;   // value pairs (zeb_master_pairs)
+  const float* gpair;    // gradient pairs (zeb_master_pairs)
   int side;
   zeb_refine_opts_t o;
   float* records;
@@ -62,7 +63,7 @@ __device__ float nmi_block(const DetArgs& a, const float* pat, float* sims, floa
     int row = i / a.w, col = i - row * a.w;
     if (!in_mask(a, row, col)) continue;
     float e = pat[i];
-    float s = master_at(a.master, qrot(q, ray_dir(a, t, row, col)), a.side);
+    float s = master_at_pair(a.vpair, qrot(q, ray_dir(a, t, row, col)), a.side);
     if (sims) sims[i] = s;
     ext[0] = fminf(ext[0], e); ext[1] = fmaxf(ext[1], e);
     ext[2] = fminf(ext[2], s); ext[3] = fmaxf(ext[3], s);
@@ -92,7 +93,7 @@ __device__ float nmi_block(const DetArgs& a, const float* pat, float* sims, floa
     int row = i / a.w, col = i - row * a.w;
     if (!in_mask(a, row, col)) continue;
     float e = pat[i];
-    float s = sims ? sims[i] : master_at(a.master, qrot(q, ray_dir(a, t, row, col)), a.side);
+    float s = sims ? sims[i] : master_at_pair(a.vpair, qrot(q, ray_dir(a, t, row, col)), a.side);
     uint32_t be = min((uint32_t)((e - r[0]) * ke), (uint32_t)(nbins - 1));
     uint32_t bs = min((uint32_t)((s - r[2]) * ks), (uint32_t)(nbins - 1));
     atomicAdd(&hist[be * nbins + bs], 1u);
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(256) k_refine_direct(DetArgs a) {
       int row = i / a.w, col = i - row * a.w;
       if (!in_mask(a, row, col)) continue;
       float3 c = qrot(q, ray_dir(a, t, row, col));
-      float4 m = grad_at(a.grad, c, a.side);
+      float4 m = grad_at_pair(a.gpair, c, a.side);
       float3 d = cross3(c, make_float3(m.x, m.y, m.z));
       float e = pat[i];
       s[0] += 1.f; s[1] += m.w; s[2] += m.w * m.w; s[3] += m.w * e;
@@ -340,7 +341,7 @@ __device__ float nmi_compact(const DetArgs& a, const float4* px, int npix, float
   float ext[4] = {3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f};
   for (int k = threadIdx.x; k < npix; k += blockDim.x) {
     const float4 p = px[k];
-    const float sv = master_at(a.master, qrot(q, make_float3(p.x, p.y, p.z)), a.side);
+    const float sv = master_at_pair(a.vpair, qrot(q, make_float3(p.x, p.y, p.z)), a.side);
     ext[0] = fminf(ext[0], p.w); ext[1] = fmaxf(ext[1], p.w);
     ext[2] = fminf(ext[2], sv); ext[3] = fmaxf(ext[3], sv);
   }
@@ -366,7 +367,7 @@ __device__ float nmi_compact(const DetArgs& a, const float4* px, int npix, float
   const float ks = (float)nbins / fmaxf(r[3] - r[2], 1e-20f);
   for (int k = threadIdx.x; k < npix; k += blockDim.x) {
     const float4 p = px[k];
-    const float sv = master_at(a.master, qrot(q, make_float3(p.x, p.y, p.z)), a.side);
+    const float sv = master_at_pair(a.vpair, qrot(q, make_float3(p.x, p.y, p.z)), a.side);
     const uint32_t be = min((uint32_t)((p.w - r[0]) * ke), (uint32_t)(nbins - 1));
     const uint32_t bs = min((uint32_t)((sv - r[2]) * ks), (uint32_t)(nbins - 1));
     atomicAdd(&hist[be * nbins + bs], 1u);
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(256, 3) k_refine(DetArgs a) {
     for (int k = threadIdx.x; k < npix; k += blockDim.x) {
       const float4 p = px[k];
       const float3 c = qrot(q, make_float3(p.x, p.y, p.z));
-      const float4 m = grad_at(a.grad, c, a.side);
+      const float4 m = grad_at_pair(a.gpair, c, a.side);
       const float3 d = cross3(c, make_float3(m.x, m.y, m.z));
       const float e = p.w;
       s[1] += m.w; s[2] += m.w * m.w; s[3] += m.w * e;
@@ -488,9 +489,10 @@ static size_t det_smem(DetArgs& a) {
 using namespace zeb;
 
 extern "C" int zeb_refine(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
-                          const zeb_frame_t* fr, const float* master, const float* grad4, int side,
+                          const zeb_frame_t* fr, const float* vpair, const float* gpair, int side,
                           const zeb_refine_opts_t* o, float* records, void* stream) {
-  ZEB_REQUIRE(pats && items && seeds && master && grad4 && o && records, ZEB_EARG, "refine: null argument");
+  ZEB_REQUIRE(pats && items && seeds && vpair && gpair && o && records, ZEB_EARG, "refine: null argument");
+  ZEB_REQUIRE(((uintptr_t)gpair & 31) == 0 && ((uintptr_t)vpair & 7) == 0, ZEB_EARG, "refine: pair tables misaligned");
   ZEB_REQUIRE(seed_stride >= 4 && side >= 3 && o->iters >= 0 && o->iters <= 1000 && o->nmi_bins >= 2 &&
                   o->nmi_bins <= 32,
               ZEB_EARG, "refine: bad arguments");
@@ -498,7 +500,7 @@ extern "C" int zeb_refine(const float* pats, const float* items, const float* se
   DetArgs a{};
   ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine: bad frame");
   a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
-  a.master = master; a.grad = (const float4*)grad4; a.side = side; a.o = *o; a.records = records;
+  a.vpair = (const float2*)vpair; a.gpair = gpair; a.side = side; a.o = *o; a.records = records;
   const size_t list = (size_t)a.h * a.w * sizeof(float4);
   if (list <= DET_LIST_SMEM) {
     cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
@@ -512,13 +514,14 @@ extern "C" int zeb_refine(const float* pats, const float* items, const float* se
 }
 
 extern "C" int zeb_chance(const float* pats, const float* items, int n, int draws, const zeb_frame_t* fr,
-                          const float* master, int side, int nmi_bins, float* out, void* stream) {
-  ZEB_REQUIRE(pats && items && master && out && draws >= 1 && draws <= 65535 && nmi_bins >= 2 && nmi_bins <= 32,
+                          const float* vpair, int side, int nmi_bins, float* out, void* stream) {
+  ZEB_REQUIRE(pats && items && vpair && out && draws >= 1 && draws <= 65535 && nmi_bins >= 2 && nmi_bins <= 32,
               ZEB_EARG, "chance: bad arguments");
+  ZEB_REQUIRE(((uintptr_t)vpair & 7) == 0, ZEB_EARG, "chance: value pairs misaligned");
   if (n <= 0) return ZEB_OK;
   DetArgs a{};
   ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "chance: bad frame");
-  a.pats = pats; a.items = (const float4*)items; a.n = n; a.master = master; a.side = side;
+  a.pats = pats; a.items = (const float4*)items; a.n = n; a.vpair = (const float2*)vpair; a.side = side;
   a.o.nmi_bins = nmi_bins; a.chance = out; a.draws = draws;
   dim3 g(n, draws);
   const size_t list = (size_t)a.h * a.w * sizeof(float4);

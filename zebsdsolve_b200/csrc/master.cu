@@ -116,6 +116,30 @@ extern "C" int zeb_master_gradient(const float* sheets, float* grad4, int side, 
   return zeb_launch_check("master_gradient");
 }
 
+// Each sheet pixel with its right-hand neighbour side by side: vpair[i] = (M[i], M[i+1]),
+// gpair[i] = (grad4[i], grad4[i+1]) (the last column repeats itself; bilinear lookups never read
+// it), so a lookup reads one 8- or 32-byte record per row instead of two scattered texels.
+__global__ void k_master_pairs(const float* __restrict__ sheets, const float4* __restrict__ grad4, int side,
+                               float2* __restrict__ vpair, float4* __restrict__ gpair) {
+  const long long total = 2LL * side * side;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int c = (int)(i % side);
+  const long long k = c + 1 < side ? i + 1 : i;
+  vpair[i] = make_float2(sheets[i], sheets[k]);
+  gpair[2 * i] = grad4[i];
+  gpair[2 * i + 1] = grad4[k];
+}
+
+extern "C" int zeb_master_pairs(const float* sheets, const float* grad4, int side, float* vpair, float* gpair,
+                                void* stream) {
+  ZEB_REQUIRE(sheets && grad4 && vpair && gpair && side >= 3, ZEB_EARG, "master_pairs: bad arguments side=%d", side);
+  const long long total = 2LL * side * side;
+  k_master_pairs<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(sheets, (const float4*)grad4, side,
+                                                                                  (float2*)vpair, (float4*)gpair);
+  return zeb_launch_check("master_pairs");
+}
+
 extern "C" int zeb_master_sample_grid(const float* sheets, int side, const double* x, int n_theta, int n_phi,
                                       double* out, void* stream) {
   ZEB_REQUIRE(sheets && x && out && side >= 2 && n_theta >= 1 && n_phi >= 1, ZEB_EARG,

@@ -89,7 +89,7 @@ class Geometry:
 class Phase:
     def __init__(self, master):
         self.master = master
-        self.baked = None  # (key, sheets f32 device, grad4 device, host sheets)
+        self.baked = None  # (key, sheets, grad4, value pairs, gradient pairs), all on the device
 
     def info(self, bands):
         m = self.master
@@ -296,7 +296,10 @@ class Engine:
                 sheets = ((host - mean) / torch.clamp(sd, min=1e-30)).float().contiguous()
             grad = torch.empty(sheets.numel() * 4, dtype=torch.float32, device=self.dev)
             N.call("zeb_master_gradient", ptr(sheets), ptr(grad), m.side, stream_ptr())
-            p.baked = (key, sheets, grad)
+            vpair = torch.empty(sheets.numel() * 2, dtype=torch.float32, device=self.dev)
+            gpair = torch.empty(sheets.numel() * 8, dtype=torch.float32, device=self.dev)
+            N.call("zeb_master_pairs", ptr(sheets), ptr(grad), m.side, ptr(vpair), ptr(gpair), stream_ptr())
+            p.baked = (key, sheets, grad, vpair, gpair)
             self.chance_key = None
 
     def band(self, L):
@@ -482,9 +485,9 @@ class Engine:
                 mark("peaks")
                 N.call("zeb_correlate_peaks", ptr(U), nt, ctypes.byref(ph.dims), ptr(bt.tw), ptr(ph.rden), 1 << 30,
                        ptr(peaks[t0 * 8:]), ptr(cand), stream_ptr())
-            _, sheets, grad = p.baked
+            _, sheets, grad, vpair, gpair = p.baked
             mark("refine")
-            N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(sheets), ptr(grad),
+            N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(vpair), ptr(gpair),
                    p.master.side, ctypes.byref(opts), ptr(recs[pi * n * 8:]), stream_ptr())
         mark("end")
         return recs[: n_ph * n * 8].view(n_ph, n, 8)
@@ -556,6 +559,9 @@ class Engine:
             self._copy_stream = torch.cuda.Stream(device=self.dev)
         cps = self._copy_stream
         raw = [self.buf(f"raw_pipe{k}", B * h * w, pin.dtype)[: B * h * w].view(B, h, w) for k in range(2)]
+        # the copy stream starts after everything already queued on the compute stream: memory the
+        # caching allocator hands out here may have been freed by work still pending there
+        cps.wait_stream(comp)
         host = [torch.empty((n_ph, B, 8), dtype=torch.float32, pin_memory=True) for _ in range(2)]
         parts = [cells[i:i + B] for i in range(0, len(cells), B)]
         up_done = [None, None]
@@ -648,7 +654,7 @@ class Engine:
         self.chance_med, self.chance_spread = [], []
         for pi, p in enumerate(self.phases):
             out = torch.empty(draws * n, dtype=torch.float32, device=self.dev)
-            N.call("zeb_chance", ptr(pats), ptr(items), n, draws, ctypes.byref(fr), ptr(p.baked[1]), p.master.side,
+            N.call("zeb_chance", ptr(pats), ptr(items), n, draws, ctypes.byref(fr), ptr(p.baked[3]), p.master.side,
                    s["nmi_bins"], ptr(out), stream_ptr())
             c = np.sort(out.cpu().numpy())
             med = c[len(c) // 2]
