@@ -170,23 +170,87 @@ __device__ __forceinline__ void fft_reg(float2 (&x)[N]) {
   }
 }
 
-template <int NC, int H, int WARPS, int PER_SM>
+// rden rows of one j staged per warp (rows padded by 4 floats: the lanes' 16-byte reads of
+// their own rows fall in distinct banks)
+template <int NC, int H>
+struct ColsRden {
+  static constexpr int RLD = 2 * H + 4;
+  static constexpr int ROWS = NC < 32 ? 32 : NC;  // every slab of a warp: 32 rows, or NC
+  static constexpr size_t BYTES = (size_t)ROWS * RLD * sizeof(float);
+};
+
+// SHARED: every item shares one rden volume; the warps then walk the slabs j-major in contiguous
+// chunks, so a warp's j changes rarely, and keep the rows of their j in shared memory (the global
+// rows of each lane otherwise come one dependent 16-byte load after another).
+template <int NC, int H, int WARPS, int PER_SM, bool SHARED>
 __global__ void __launch_bounds__(WARPS * 32, PER_SM) k_slab_cols(SlabArgs a) {
   constexpr int n = 2 * H;
   constexpr int SEG = NC < 32 ? NC : 32;  // lanes per slab
   constexpr int SPW = 32 / SEG;           // slabs per warp
+  extern __shared__ __align__(16) float rtile_all[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / SEG, cl = lane - sub * SEG;
-  const int L = a.d.L, nb = a.d.nb;
-  const long long total = (long long)a.n_items * nb;
-  for (long long s0 = ((long long)blockIdx.x * WARPS + warp) * SPW; s0 < total;
-       s0 += (long long)gridDim.x * WARPS * SPW) {
+  const int L = a.d.L, nb = a.d.nb, ni = a.n_items;
+  const long long total = (long long)ni * nb;
+  const long long steps = (total + SPW - 1) / SPW;
+  float* rtile = rtile_all + (size_t)warp * ColsRden<NC, H>::ROWS * ColsRden<NC, H>::RLD;
+  int tile_j[SPW];
+#pragma unroll
+  for (int k = 0; k < SPW; ++k) tile_j[k] = -1;
+  long long t0, t1, tstep;
+  if (SHARED) {
+    const long long wid = (long long)blockIdx.x * WARPS + warp, nw = (long long)gridDim.x * WARPS;
+    const long long chunk = (steps + nw - 1) / nw;
+    t0 = wid * chunk;
+    t1 = t0 + chunk < steps ? t0 + chunk : steps;
+    tstep = 1;
+  } else {
+    t0 = (long long)blockIdx.x * WARPS + warp;
+    t1 = steps;
+    tstep = (long long)gridDim.x * WARPS;
+  }
+  for (long long t = t0; t < t1; t += tstep) {
+    const long long s0 = t * SPW;
     const long long slab = s0 + sub;
     const bool live = slab < total;
     const long long sl = live ? slab : s0;
-    const int b = (int)(sl / nb), j = (int)(sl - (long long)b * nb);
-    const float2* src = a.U + sl * L * NC;
-    const float* rslab = a.rden + ((size_t)(b / a.rden_div) * nb + j) * NC * n;
+    int b, j;
+    if (SHARED) {  // work order j-major: (j, b) ↔ U slab b·nb + j
+      j = (int)(sl / ni);
+      b = (int)(sl - (long long)j * ni);
+    } else {
+      b = (int)(sl / nb);
+      j = (int)(sl - (long long)b * nb);
+    }
+    const long long uslab = (long long)b * nb + j;
+    const float2* src = a.U + uslab * L * NC;
+    const float* rslab;
+    int rstride;
+    if (SHARED) {
+      // (re)stage the rows of each sub-slab's j when it changed (warp-uniform: every lane sees all)
+#pragma unroll
+      for (int k = 0; k < SPW; ++k) {
+        long long sk = s0 + k;
+        if (sk >= total) sk = s0;
+        const int jk = (int)(sk / ni);
+        if (jk != tile_j[k]) {
+          __syncwarp();
+          const float4* g = (const float4*)(a.rden + (size_t)jk * NC * n);
+          float* dst = rtile + (size_t)k * NC * ColsRden<NC, H>::RLD;
+          for (int e = lane; e < NC * n / 4; e += 32) {
+            const int c = e / (n / 4), p4 = e - c * (n / 4);
+            *(float4*)(dst + c * ColsRden<NC, H>::RLD + 4 * p4) = __ldg(g + e);
+          }
+          tile_j[k] = jk;
+          __syncwarp();
+        }
+      }
+      rslab = rtile + (size_t)sub * NC * ColsRden<NC, H>::RLD;
+      rstride = ColsRden<NC, H>::RLD;
+    } else {
+      rslab = a.rden + ((size_t)(b / a.rden_div) * nb + j) * NC * n;
+      rstride = n;
+    }
     float bv = -3.4e38f;
     uint32_t bi = 0xffffffffu;
 #pragma unroll 1
@@ -218,11 +282,11 @@ __global__ void __launch_bounds__(WARPS * 32, PER_SM) k_slab_cols(SlabArgs a) {
         z[q] = zq;
       }
       fft_reg<H>(z);
-      const float4* rd = (const float4*)(rslab + (size_t)c * n);
+      const float4* rd = (const float4*)(rslab + (size_t)c * rstride);
       const uint32_t base = ((uint32_t)(j * NC + c)) * n;
 #pragma unroll
       for (int p = 0; p < H; p += 2) {
-        const float4 r = __ldg(rd + p / 2);
+        const float4 r = rd[p / 2];
         const float v0 = z[p].x * r.x, v1 = z[p].y * r.y, v2 = z[p + 1].x * r.z, v3 = z[p + 1].y * r.w;
         const uint32_t i0 = base + 2 * p;
         if (v0 > bv) { bv = v0; bi = i0; }
@@ -238,7 +302,7 @@ __global__ void __launch_bounds__(WARPS * 32, PER_SM) k_slab_cols(SlabArgs a) {
       uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
       if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
-    if (cl == 0 && live) a.cand[slab] = make_float2(bv, __uint_as_float(bi));
+    if (cl == 0 && live) a.cand[uslab] = make_float2(bv, __uint_as_float(bi));
   }
 }
 
@@ -397,8 +461,18 @@ static int slab_launch(const float* U, int n_items, const zeb_so3_dims_t* d, con
   if (NC == nc_ && H == h_) {                                                                                \
     constexpr int spw = (nc_) < 32 ? 32 / (nc_) : 1;                                                        \
     long long want = (blocks + (long long)(w_)*spw - 1) / ((long long)(w_)*spw);                             \
-    long long grid = want < (long long)sms * (per_sm_)*8 ? want : (long long)sms * (per_sm_)*8;             \
-    k_slab_cols<nc_, h_, w_, per_sm_><<<(unsigned)grid, (w_)*32, 0, st>>>(a);                               \
+    if (a.rden_div >= n_items) {                                                                              \
+      const size_t sm = (size_t)(w_) * ColsRden<nc_, h_>::BYTES;                                             \
+      cudaFuncSetAttribute(k_slab_cols<nc_, h_, w_, per_sm_, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                           (int)sm);                                                                          \
+      const long long fit = (long long)((220u * 1024u) / sm) < (per_sm_) ? (long long)((220u * 1024u) / sm)     \
+                                                                           : (long long)(per_sm_);           \
+      long long grid = want < (long long)sms * fit ? want : (long long)sms * fit;                              \
+      k_slab_cols<nc_, h_, w_, per_sm_, true><<<(unsigned)grid, (w_)*32, sm, st>>>(a);                        \
+    } else {                                                                                                  \
+      long long grid = want < (long long)sms * (per_sm_)*8 ? want : (long long)sms * (per_sm_)*8;             \
+      k_slab_cols<nc_, h_, w_, per_sm_, false><<<(unsigned)grid, (w_)*32, 0, st>>>(a);                        \
+    }                                                                                                         \
     return zeb_launch_check("correlate slab (columns)");                                                    \
   }
     ZEB_SLAB_COLS(8, 16, 4, 6)
