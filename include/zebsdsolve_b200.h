@@ -239,6 +239,12 @@ int zeb_refine(const float* pats, const float* items, const float* seeds, int se
 int zeb_chance(const float* pats, const float* items, int n, int draws, const zeb_frame_t* fr,
                const float* vpair, int side, int nmi_bins, float* out, void* stream);  /* vpair: zeb_master_pairs */
 
+/* The records' orientations (records[b][0..3]) in the fundamental zone of a group of n_ops
+ * rotations (ops[k] = w, x, y, z, FP64, identity first): fz[b] = the g·q of largest w, unit norm,
+ * w >= 0, ties within 1e-12 keeping the first, in FP64 rounded once to FP32. The landing's
+ * reduction (engine.zig:2392-2419 with sym.zig:120-131), moved from the host to the device. */
+int zeb_records_fz(const float* records, int n, const double* ops, int n_ops, float* fz, void* stream);
+
 /* Simulated patterns: the master at q·ray for every pixel of item b (poses[b] = t.xyz, pattern
  * index, q.wxyz): sims[b][h][w]. Replaces Detector.project (src/detector.zig:138-142;
  * shaders/detector.wgsl:254-263). */

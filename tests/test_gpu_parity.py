@@ -357,6 +357,27 @@ def test_bf16_spectrum_matches_fp32_and_oracle(world, lib, L, precision):
     assert float((v16 - v32).abs().max()) < (5e-5 if full else 4e-3) * float(v32.abs().max())
 
 
+@pytest.mark.parametrize("kind", ["o", "d6", "c2", "c1"])
+def test_records_fz_equals_the_host_reduction(lib, kind):
+    """zeb_records_fz against the host's to_fz (FP64, ties within 1e-12 keeping the first): the
+    same FP32 values, bit for bit, also for orientations on the zone's boundary."""
+    from zebsdsolve_b200 import rotations as R
+
+    rng = np.random.default_rng(12)
+    ops = R.group(kind)
+    q = rng.normal(size=(4000, 4))
+    q[:200] = ops[rng.integers(0, len(ops), 200)]  # symmetry operators themselves: ties
+    q[200:400] *= 1.0 + rng.uniform(-1e-3, 1e-3, (200, 1))  # off unit norm
+    recs = np.zeros((len(q), 8), np.float32)
+    recs[:, :4] = q.astype(np.float32)
+    rd = torch.as_tensor(recs, device="cuda")
+    od_ = torch.as_tensor(ops, device="cuda")
+    fz = torch.empty(len(q) * 4, device="cuda")
+    lib.call("zeb_records_fz", P(rd), len(q), P(od_), len(ops), P(fz), sp())
+    want = R.to_fz(recs[:, :4].astype(np.float64), ops).astype(np.float32)
+    assert np.array_equal(fz.cpu().numpy().reshape(-1, 4), want)
+
+
 def test_refine_and_nmi_match_oracle(world, lib):
     s = world["s"]
     e = s._e

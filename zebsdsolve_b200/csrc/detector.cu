@@ -464,6 +464,53 @@ __global__ void __launch_bounds__(256, 3) k_chance(DetArgs a) {
   if (threadIdx.x == 0) a.chance[(size_t)draw * a.n + b] = v;
 }
 
+// The records' orientations reduced to the fundamental zone of a group (the landing's
+// reduction, sym.zig:120-131): the symmetry-equivalent g·q of largest w (unit norm, w >= 0), ties
+// within 1e-12 keeping the first; FP64 with every product and sum rounded on its own (no fused
+// multiply-add), in the order of the host's reduction.
+__device__ __forceinline__ double4 qstd_d(double4 q) {
+  double s = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(q.x, q.x), __dmul_rn(q.y, q.y)), __dmul_rn(q.z, q.z)),
+                       __dmul_rn(q.w, q.w));
+  double nrm = sqrt(s);
+  if (nrm == 0.0) nrm = 1.0;
+  const double sg = q.x < 0.0 ? -1.0 : 1.0;
+  return make_double4(__dmul_rn(__ddiv_rn(q.x, nrm), sg), __dmul_rn(__ddiv_rn(q.y, nrm), sg),
+                      __dmul_rn(__ddiv_rn(q.z, nrm), sg), __dmul_rn(__ddiv_rn(q.w, nrm), sg));
+}
+
+__device__ __forceinline__ double4 qmul_d(double4 a, double4 b) {
+  // (w, x, y, z) in (.x, .y, .z, .w)
+  const double w = __dsub_rn(__dsub_rn(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dmul_rn(a.z, b.z)),
+                             __dmul_rn(a.w, b.w));
+  const double x = __dsub_rn(__dadd_rn(__dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)), __dmul_rn(a.z, b.w)),
+                             __dmul_rn(a.w, b.z));
+  const double y = __dadd_rn(__dadd_rn(__dsub_rn(__dmul_rn(a.x, b.z), __dmul_rn(a.y, b.w)), __dmul_rn(a.z, b.x)),
+                             __dmul_rn(a.w, b.y));
+  const double z = __dadd_rn(__dsub_rn(__dadd_rn(__dmul_rn(a.x, b.w), __dmul_rn(a.y, b.z)), __dmul_rn(a.z, b.y)),
+                             __dmul_rn(a.w, b.x));
+  return make_double4(w, x, y, z);
+}
+
+__global__ void k_records_fz(const float* __restrict__ recs, int n, const double4* __restrict__ ops, int n_ops,
+                             float* __restrict__ fz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* r = recs + (size_t)i * 8;
+  const double4 q = make_double4((double)r[0], (double)r[1], (double)r[2], (double)r[3]);
+  double4 best = qstd_d(q);
+  double bw = best.x;
+  for (int k = 0; k < n_ops; ++k) {
+    const double4 c = qstd_d(qmul_d(ops[k], q));
+    if (c.x > bw + 1e-12) {
+      best = c;
+      bw = c.x;
+    }
+  }
+  float* o = fz + (size_t)i * 4;
+  o[0] = __double2float_rn(best.x); o[1] = __double2float_rn(best.y);
+  o[2] = __double2float_rn(best.z); o[3] = __double2float_rn(best.w);
+}
+
 static bool fill_frame(DetArgs& a, const zeb_frame_t* fr) {
   if (!fr || fr->h < 2 || fr->w < 2) return false;
   a.h = fr->h; a.w = fr->w;
@@ -546,4 +593,11 @@ extern "C" int zeb_project(const float* master, int side, const float* poses, in
   long long total = (long long)n * a.h * a.w;
   k_project<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a, poses, sims);
   return zeb_launch_check("project");
+}
+
+extern "C" int zeb_records_fz(const float* records, int n, const double* ops, int n_ops, float* fz, void* stream) {
+  ZEB_REQUIRE(records && ops && fz && n_ops >= 1 && n_ops <= 48, ZEB_EARG, "records_fz: bad arguments");
+  if (n <= 0) return ZEB_OK;
+  k_records_fz<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(records, n, (const double4*)ops, n_ops, fz);
+  return zeb_launch_check("records_fz");
 }

@@ -128,6 +128,7 @@ class Engine:
         self._batch_t = None  # bounding box of the last batch's detector positions
         self._spans = {}
         self._pinned = None
+        self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
 
     # ── plumbing ──
@@ -517,6 +518,18 @@ class Engine:
                 c0 = int(cells[a0])
                 dst[a0:a1].copy_(src[c0:c0 + (a1 - a0)], non_blocking=True)
 
+    def fz_of(self, recs):
+        """Each phase's records reduced to its fundamental zone on the device: [phase][n][4]."""
+        n_ph, n = recs.shape[0], recs.shape[1]
+        fz = self.buf("fz", max(n_ph * n * 4, 1))[: n_ph * n * 4].view(n_ph, n, 4)
+        for pi, p in enumerate(self.phases):
+            ops = getattr(p, "ops_dev", None)
+            if ops is None:
+                ops = torch.as_tensor(np.ascontiguousarray(p.master.rotations(), np.float64), device=self.dev)
+                p.ops_dev = ops
+            N.call("zeb_records_fz", ptr(recs[pi]), n, ptr(ops), ops.shape[0], ptr(fz[pi]), stream_ptr())
+        return fz
+
     def index_cells(self, cells, bandwidth=None):
         """engine.zig:1990-2137 — index the given cells against every phase: records
         [phase][cell][8] = (q, NCC, NMI, last improving step, z)."""
@@ -531,7 +544,9 @@ class Engine:
         rows, cols, h, w = self.info()
         raw = self.buf("raw_up", n * h * w, self.pinned().dtype).view(-1)[: n * h * w].view(n, h, w)
         self.upload_raw(cells, raw, torch.cuda.current_stream())
-        out = self.run_device(raw, cells, bandwidth).cpu().numpy()
+        recs = self.run_device(raw, cells, bandwidth)
+        self._last_fz = self.fz_of(recs).cpu().numpy()
+        out = recs.cpu().numpy()
         self.check_device()
         return self.finish(out)
 
@@ -542,7 +557,7 @@ class Engine:
     def index_pipelined(self, cells, bandwidth, on_batch, keep_going=lambda: True):
         """engine.zig:1990-2137 over many cells at once: device passes of device_batch() cells,
         each pass's upload (a copy stream, from the pinned scan) overlapping the previous pass's
-        kernels, its records read back asynchronously and handed to on_batch(cells, records) on
+        kernels, its records read back asynchronously and handed to on_batch(cells, records, fz) on
         the host while the next pass runs.  keep_going() is asked before each new pass."""
         cells = np.asarray(cells, np.int64)
         n_ph = len(self.phases)
@@ -563,6 +578,7 @@ class Engine:
         # caching allocator hands out here may have been freed by work still pending there
         cps.wait_stream(comp)
         host = [torch.empty((n_ph, B, 8), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+        hfz = [torch.empty((n_ph, B, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
         parts = [cells[i:i + B] for i in range(0, len(cells), B)]
         up_done = [None, None]
         comp_done = [None, None]
@@ -582,7 +598,8 @@ class Engine:
             ev.synchronize()
             back[k] = None
             out = host[k][:, : len(cb)].numpy().copy()
-            on_batch(cb, self.finish(out, stamp))
+            fz = hfz[k][:, : len(cb)].numpy().copy()
+            on_batch(cb, self.finish(out, stamp), fz)
 
         issue_upload(0)
         for i in range(len(parts)):
@@ -597,7 +614,9 @@ class Engine:
             comp_done[k] = ev
             if back[k] is not None:
                 drain(k)
+            fzd = self.fz_of(recs)
             host[k][:, : len(cb)].copy_(recs, non_blocking=True)
+            hfz[k][:, : len(cb)].copy_(fzd, non_blocking=True)
             evb = torch.cuda.Event()
             evb.record(comp)
             back[k] = (evb, cb, self.batch_stamp)
@@ -687,8 +706,10 @@ class Engine:
         self.res["sweep"][cells] = -1
         self.res["z"][cells] = 0
 
-    def land(self, cells, recs):
-        """engine.zig:2392-2419 — each cell keeps the better match; accepted ones their sweep."""
+    def land(self, cells, recs, fz=None):
+        """engine.zig:2392-2419 — each cell keeps the better match; accepted ones their sweep.
+        fz: the records' orientations already in each phase's fundamental zone ([phase][cell][4],
+        zeb_records_fz); computed here on the host when absent."""
         s = self.set
         res = self.res
         cells = np.asarray(cells, np.int64)
@@ -697,10 +718,13 @@ class Engine:
         r = recs[best, np.arange(len(cells))]
         good = r[:, 5] >= s["accept_nmi"] if s["accept_nmi"] > 0 else r[:, 7] >= s["accept_z"]
         replace = (res["phase"][cells] < 0) | (good & (r[:, 6] <= settle)) | (r[:, 7] > res["z"][cells])
-        q = np.empty((len(cells), 4))
-        for p in np.unique(best):
-            sel = best == p
-            q[sel] = R.to_fz(r[sel, :4].astype(np.float64), self.phases[int(p)].master.rotations())
+        if fz is not None:
+            q = fz[best, np.arange(len(cells))]
+        else:
+            q = np.empty((len(cells), 4))
+            for p in np.unique(best):
+                sel = best == p
+                q[sel] = R.to_fz(r[sel, :4].astype(np.float64), self.phases[int(p)].master.rotations())
         idx = cells[replace]
         res["quat"][idx] = q[replace]
         res["ncc"][idx] = r[replace, 4]
@@ -730,7 +754,7 @@ class Engine:
         if method != "spherical":
             raise EngineError(f"method {method!r}: not supported on this engine yet")
         recs = self.index_cells(cells, bw)
-        self.land(cells, recs)
+        self.land(cells, recs, self._last_fz)
         self.next_sweep(bw)
         return len(self.index_cells_list) - self.index_done
 
@@ -758,8 +782,8 @@ class Engine:
                 raise EngineError(f"method {method!r}: not supported on this engine yet")
             stop = [False]
 
-            def on_batch(cb, recs):
-                self.land(cb, recs)  # a pass already in flight when the stop came still lands
+            def on_batch(cb, recs, fz):
+                self.land(cb, recs, fz)  # a pass already in flight when the stop came still lands
                 if progress is not None and not stop[0] and progress(self.status()) is False:
                     stop[0] = True
 
