@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Throughput of the spherical indexing path (patterns/s indexed + refined) on B200.
 
-    python bench.py [--gpus N --steps K --warmup W --precision bf16|f32 --patterns P]
+    python bench.py [--gpus N --steps K --warmup W --precision bf16|bf16x3|f32 --patterns P]
     python bench.py --impl reference ...   # the reference's algorithm on the host cores
 
 Workload (the precision-form configuration at scale): a 316 × 316 scan (99,856 patterns) of
@@ -49,7 +49,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--precision", default="f32", choices=("f32", "bf16", "bf16x3"))
+    ap.add_argument("--precision", default="bf16", choices=("f32", "bf16", "bf16x3"),
+                    help="the form timed as `value` and `e2e` (the plain FP32 form is timed beside it)")
+    ap.add_argument("--no-fp32-form", action="store_true", help="skip the plain FP32 form's timing")
     ap.add_argument("--patterns", type=int, default=ROWS * COLS, help="scan size (cells), default 316x316")
     ap.add_argument("--batch", type=int, default=16384, help="patterns per device pass in the value measurement")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -122,9 +124,10 @@ def _oracle_pattern(args):
     return float(best), float(v)
 
 
-def cpu_leg(seconds, seed=4):
-    """The oracle over a bounded sample of the workload, in a spawn pool over every host core.
-    Returns (patterns/s, cores, sample description)."""
+def cpu_leg(seconds, seed=4, warmup=1, steps=0):
+    """The oracle over bounded samples of the workload in a spawn pool over the host cores: after
+    one set-up round and `warmup` rounds, timed rounds of one pattern per core until at least
+    `steps` rounds and `seconds` have passed. Returns (patterns/s, cores, sample description)."""
     import multiprocessing as mp
 
     import oracle.detector as od
@@ -143,18 +146,28 @@ def cpu_leg(seconds, seed=4):
     for i in range(n):
         sim = od.project(w["sheets"], 401, w["frame"], t, q[i], H, W)
         pats.append(np.clip(rng.poisson(np.maximum(1000 * (0.6 + 0.4 * sim) * B, 0)), 0, 65535).astype(np.uint16))
+    # one thread per worker: the workers' BLAS and FFT pools would otherwise each take every core
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS"):
+        os.environ[k] = "1"
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        pool.map(_oracle_pattern, [(pats[i], q[i]) for i in range(cores)])  # set-up in every worker
-        done = 0
+        # every round is bounded: a round that does not finish in `limit` seconds raises
+        limit = 600.0
+        pool.map_async(_oracle_pattern, [(pats[i], q[i]) for i in range(cores)]).get(limit)  # set-up in every worker
+        for _ in range(warmup):
+            pool.map_async(_oracle_pattern, [(pats[i % n], q[i % n]) for i in range(cores)]).get(limit)
+        done = rounds = 0
         t0 = time.perf_counter()
         while True:
-            pool.map(_oracle_pattern, [(pats[i % n], q[i % n]) for i in range(cores)])
+            pool.map_async(_oracle_pattern, [(pats[(i + rounds) % n], q[(i + rounds) % n])
+                                             for i in range(cores)]).get(limit)
             done += cores
-            if time.perf_counter() - t0 > seconds:
+            rounds += 1
+            if rounds >= steps and time.perf_counter() - t0 > seconds:
                 break
         dt = time.perf_counter() - t0
-    return done / dt, cores, f"{done} patterns of the workload (60x60, L=64, refined) through the FP64 NumPy oracle in {dt:.1f} s"
+    return done / dt, cores, (f"{done} patterns of the workload (60x60 u16, L=64, filtered, correlated, refined, NMI) "
+                              f"through the FP64 NumPy restatement, {rounds} rounds of {cores} in {dt:.1f} s")
 
 
 # ── the device ──
@@ -162,12 +175,15 @@ def cpu_leg(seconds, seed=4):
 class Clocks:
     """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
 
-    def __init__(self, index):
+    def __init__(self, index, off=False):
         self.index = index
+        self.off = off
         self.proc = None
         self.path = None
 
     def __enter__(self):
+        if self.off:
+            return self
         self.path = tempfile.mktemp(suffix=".csv")
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -268,57 +284,74 @@ def device_main(a):
             c = cells[b0:b0 + batch]
             e.run_device(raw[b0:b0 + len(c)], c, L, timer)
 
-    for _ in range(a.warmup):
-        device_pass()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    _native.launches["count"] = 0
-    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        torch.cuda.synchronize()
-        torch.cuda.nvtx.range_push("timed")  # the range a profiler's launch list is filtered to
-        t0.record()
-        for _ in range(a.steps):
+    def max_over_ranks(v):
+        if dist:
+            tt = torch.tensor([v], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            return float(tt.item())
+        return v
+
+    def time_form(precision, clocks=None, nvtx=False):
+        """(device-resident ms per step, e2e ms per step, launches, stage ms, results) of one form."""
+        s.configure(precision=precision)
+        e.prepare(L)
+        for _ in range(a.warmup):
             device_pass()
-        t1.record()
         torch.cuda.synchronize()
-        torch.cuda.nvtx.range_pop()
-    launches = _native.launches["count"]
-    e.check_device()  # a tensor-core wait that gave up would have left U incomplete
-    ms = t0.elapsed_time(t1) / a.steps
-    if dist:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-        dist.barrier()
+        if dist:
+            dist.barrier()
+        _native.launches["count"] = 0
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with (clocks if clocks is not None else Clocks(None, off=True)):
+            torch.cuda.synchronize()
+            if nvtx:
+                torch.cuda.nvtx.range_push("timed")  # the range a profiler's launch list is filtered to
+            t0.record()
+            for _ in range(a.steps):
+                device_pass()
+            t1.record()
+            torch.cuda.synchronize()
+            if nvtx:
+                torch.cuda.nvtx.range_pop()
+        launches = _native.launches["count"]
+        e.check_device()  # a tensor-core wait that gave up would have left U incomplete
+        ms = max_over_ranks(t0.elapsed_time(t1) / a.steps)
+        if dist:
+            dist.barrier()
+        # stage times of one more pass (CUDA events on the launching stream between the stages)
+        timer = StageTimer(torch)
+        device_pass(timer)
+        stages = timer.totals()
+        # e2e: the public API from pinned host memory, every step (uploads, passes, readbacks, landing)
+        for _ in range(max(1, a.warmup - 2)):
+            s.index()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.steps):
+            r = s.index()
+        e1.record()
+        torch.cuda.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1) / a.steps)
+        return ms, ems, launches, stages, r
+
+    clk = Clocks(local)
+    ms, ems, launches, stages, r = time_form(a.precision, clk, nvtx=True)
     value = n * world / (ms / 1e3)
-
-    # stage times of one more pass, for the roofline of the dominant kernel
-    timer = StageTimer(torch)
-    device_pass(timer)
-    stages = timer.totals()
-
-    # e2e: the public API from host memory, every step
-    for _ in range(max(1, a.warmup - 2)):
-        s.index()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(a.steps):
-        r = s.index()
-    e1.record()
-    torch.cuda.synchronize()
-    ems = e0.elapsed_time(e1) / a.steps
-    if dist:
-        tt = torch.tensor([ems], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ems = float(tt.item())
     e2e = n * world / (ems / 1e3)
     dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), q))
+    fp32 = None
+    if not a.no_fp32_form and a.precision != "f32":
+        ms32, ems32, _, stages32, r32 = time_form("f32")
+        dis32 = np.degrees(s.disorientation(r32["quaternions"].reshape(-1, 4), q))
+        agree = np.degrees(s.disorientation(r32["quaternions"].reshape(-1, 4), r["quaternions"].reshape(-1, 4)))
+        fp32 = {"value": round(n * world / (ms32 / 1e3), 1), "e2e": round(n * world / (ems32 / 1e3), 1),
+                "ms_per_step": round(ms32, 3), "stage_ms_per_step": {k: round(v, 3) for k, v in stages32.items()},
+                "median_deg": round(float(np.median(dis32)), 4),
+                "forms_within_0.1deg": round(float((agree < 0.1).mean()), 5)}
 
     if rank != 0:
         if dist:
@@ -328,17 +361,26 @@ def device_main(a):
     hbm = peaks.get("hbm_gbs", 6650.0)
     ph = e.bands[L]["phases"][0][1]
     d = ph.dims
-    per_pass = math.ceil(n / batch)
-    dom = max(stages, key=stages.get)
-    # algorithmic work of each stage per pattern
+    # algorithmic HBM bytes of each stage per pattern (its kernels' compulsory reads and writes)
     u_bytes = d.nb * d.L * d.nc * 8
-    work = {"peaks": ("hbm", u_bytes, "GB/s"),  # the spectrum U read once
-            "spectrum": ("hbm", u_bytes + d.n_pairs * 8, "GB/s"),  # U written once, coefficients read
-            "prep": ("hbm", H * W * (2 + 4), "GB/s"),
-            "sphere": ("hbm", H * W * 4 + d.n_pairs * 8, "GB/s"),
-            "refine": ("hbm", H * W * 4 + 32, "GB/s")}
-    bound, per_unit, unit = work.get(dom, ("hbm", 0, "GB/s"))
-    achieved = per_unit * n / (stages[dom] / 1e3) / 1e9
+    algo = {"prep": H * W * (2 + 4),                       # u16 in, f32 out
+            "sphere": H * W * 4 + d.n_pairs * 8,           # pattern in, coefficients out
+            "spectrum": d.n_pairs * 8 + u_bytes,           # coefficients in, U out
+            "peaks": u_bytes + 8 * 4,                      # U in, peak out
+            "refine": H * W * 4 + 8 * 4}                   # pattern in, record out
+    traffic = {}
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")  # ncu DRAM bytes per pattern of each stage
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(a.precision, {})
+    roof = {}
+    for k, ms_k in stages.items():
+        if k not in algo or ms_k <= 0:
+            continue
+        ach = algo[k] * n / (ms_k / 1e3) / 1e9
+        t = traffic.get(k)
+        roof[k] = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
+                   "traffic": int(t * batch) if t else None, "ms_per_step": round(ms_k, 3)}
+    dom = max((k for k in roof), key=lambda k: stages[k])
     line = {
         "metric": "patterns/s indexed+refined on 1 B200, BF16 form vs plain FP32 at <=0.1 deg error",
         "value": round(value, 1), "unit": "patterns/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -347,15 +389,17 @@ def device_main(a):
         "config": {"workload": WORKLOAD, "patterns_per_gpu": n, "bandwidth": L, "precision": a.precision,
                    "device_batch": batch, "l2": "inputs (720 MB) larger than L2, no flush"},
         "e2e": {"value": round(e2e, 1), "unit": "patterns/s", "h2d_bytes_per_step": int(n * H * W * 2),
-                "d2h_bytes_per_step": int(n * 8 * 4 * len(e.phases))},
+                "d2h_bytes_per_step": int(n * (8 + 4) * 4 * len(e.phases))},
         "gpu_launches": int(launches),
-        "roofline": {"bound": bound, "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": unit,
-                     "frac": round(achieved / hbm, 4), "traffic": None,
-                     "stage_ms_per_step": {k: round(v, 3) for k, v in stages.items()}},
+        "roofline": dict(roof[dom], kernel=dom, per_launch_patterns=batch),
+        "rooflines": roof,
         "accuracy": {"median_deg": round(float(np.median(dis)), 4), "p99_deg": round(float(np.percentile(dis, 99)), 4),
                      "within_0.1deg": round(float((dis < 0.1).mean()), 4)},
         "clocks": clk.summary(),
     }
+    if fp32 is not None:
+        line["fp32_form"] = fp32
+        line["vs_fp32_form"] = {"value": round(value / fp32["value"], 3), "e2e": round(e2e / fp32["e2e"], 3)}
     if not a.no_cpu:
         v, cores, sample = cpu_leg(a.cpu_seconds)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port", "sample": sample}
@@ -368,7 +412,7 @@ def reference_main(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    v, cores, sample = cpu_leg(max(5.0, a.cpu_seconds))
+    v, cores, sample = cpu_leg(0.0, warmup=a.warmup, steps=a.steps)
     line = {"impl": "reference", "metric": "patterns/s indexed+refined on 1 B200, BF16 form vs plain FP32 at <=0.1 deg error",
             "value": round(v, 3), "unit": "patterns/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",

@@ -646,9 +646,12 @@ class Engine:
         return out
 
     def tile_items(self, ph, n):
-        """Items whose spectra one pass holds: tile_mb of them, at least 512 (spherical.zig:311-315)."""
+        """Items whose spectra one pass holds: tile_mb of them, at least 512 (spherical.zig:311-315),
+        spread evenly over the passes a batch needs (no short last tile)."""
         per = N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), 1)
-        return int(max(1, min(n, max(512, (self.set["tile_mb"] << 20) // per))))
+        most = int(max(1, min(n, max(512, (self.set["tile_mb"] << 20) // per))))
+        tiles = -(-n // most)
+        return -(-n // tiles)
 
     def calibrate(self):
         """engine.zig:2202-2292 — chance NMI per phase: ~256 region cells × 8 random orientations;
