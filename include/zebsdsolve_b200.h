@@ -245,6 +245,25 @@ int zeb_chance(const float* pats, const float* items, int n, int draws, const ze
  * reduction (engine.zig:2392-2419 with sym.zig:120-131), moved from the host to the device. */
 int zeb_records_fz(const float* records, int n, const double* ops, int n_ops, float* fz, void* stream);
 
+/* Six unknowns per item: x[b] = (δt: the rays' origin moved, 3 floats in pixels, sample axes;
+ * φ: a rotation vector applied on the left of q0[b], radians), the detector projection
+ * v = c0·row + c1·col + t + δt, c = (exp(φ)·q0)·v/|v| and the normalized cross-correlation of
+ * the pattern with the master there. One block per item, the masked pixels listed in shared
+ * memory. mode 0: out[b] = NCC (the forward). mode 1: out[b][0..5] = ∂NCC/∂x by the exact
+ * derivatives of the forward (the bilinear lookup's slopes through the square-Lambert map, the
+ * rotation and the ray's normalization), out[b][6] = NCC: the adjoint, which recomputes the
+ * projection. mode 2: out[b][0..42] = the 43 sums of detector.wgsl:435-499 (sums), with the
+ * directions from the gradient table gpair (the reference's Gauss–Newton Jacobian), from which
+ * planefit.zig:176-200 (localOf) forms NCC, gradient and GN matrix. vpair/gpair:
+ * zeb_master_pairs. Replaces Detector's `sums` schedule (src/planefit.zig:523-558 eval). */
+int zeb_det6(int mode, const float* pats, const float* items, int n, const zeb_frame_t* fr, const float* vpair,
+             const float* gpair, int side, const float* x, const float* q0, float* out, void* stream);
+
+/* x[b] = A[b]⁻¹ b[b] for n systems of 6 (A: [n][6][6], b: [n][6], FP64) by elimination with
+ * partial pivoting; ok[b] = 0 where a pivot falls below 1e-300 (x[b] = 0). Replaces the host
+ * solve of planefit.zig:203-233 (the damped Levenberg–Marquardt step of settle). */
+int zeb_solve6(const double* A, const double* b, int n, double* x, int* ok, void* stream);
+
 /* Simulated patterns: the master at q·ray for every pixel of item b (poses[b] = t.xyz, pattern
  * index, q.wxyz): sims[b][h][w]. Replaces Detector.project (src/detector.zig:138-142;
  * shaders/detector.wgsl:254-263). */

@@ -1,5 +1,6 @@
 """The detector side in float64 (oracle restatement of zebsdsolve `src/detector.zig`,
-`shaders/detector.wgsl`, `shaders/mastersph.wgsl` and `shaders/common.wgsl`): master lookups,
+`shaders/detector.wgsl`, `shaders/mastersph.wgsl`, `shaders/common.wgsl` and the per-pattern steps
+of `src/planefit.zig`): master lookups,
 simulated patterns, rotation-only Gauss–Newton refinement, NMI, chance decoys."""
 import math
 
@@ -309,3 +310,134 @@ def decoy(b, draw):
     ra = np.sqrt(1.0 - u1)
     rb = np.sqrt(u1)
     return np.stack([ra * np.sin(a2), ra * np.cos(a2), rb * np.sin(a3), rb * np.cos(a3)], -1)
+
+
+# ── six unknowns per pattern: the source's shift and the crystal's rotation ──
+
+def sums6(grad, side, frame, t, q, shift, pattern, mask):
+    """detector.wgsl:435-499 (sums) — the 43 sums over the masked pixels at orientation q with the
+    rays' origin moved by `shift` (pixels, sample axes): with u = c0·row + c1·col + t + shift,
+    c = q·u/|u| and (∇M, M) = grad(c), the directions d = (q⁻¹·∇M/|u|, c × ∇M); sums
+    n, ΣM, ΣM², ΣM·e, Σd (6), ΣM·d (6), Σe·d (6), Σd_i d_j (i ≤ j, 21)."""
+    h, w = pattern.shape
+    m_ = in_mask(h, w, mask)
+    u = (rays(h, w, frame, np.asarray(t, np.float64) + np.asarray(shift, np.float64)))[m_]
+    dist = np.linalg.norm(u, axis=-1, keepdims=True)
+    q = np.asarray(q, np.float64)
+    c = rot.qapply(q, u / dist)
+    g = sheet_lookup(grad, side, c)
+    val = g[:, 3]
+    a = np.cross(c, g[:, :3])
+    wv = rot.qapply(rot.qconj(q), g[:, :3]) / dist
+    d = np.concatenate([wv, a], 1)
+    e = np.asarray(pattern, np.float64)[m_]
+    s = np.zeros(43)
+    s[0] = float(m_.sum())
+    s[1] = val.sum()
+    s[2] = (val * val).sum()
+    s[3] = (val * e).sum()
+    s[4:10] = d.sum(0)
+    s[10:16] = (val[:, None] * d).sum(0)
+    s[16:22] = (e[:, None] * d).sum(0)
+    o = 22
+    for i in range(6):
+        for j in range(i, 6):
+            s[o] = (d[:, i] * d[:, j]).sum()
+            o += 1
+    return s
+
+
+def local_of(s):
+    """planefit.zig:176-200 (localOf) — NCC, its gradient g (6) and Gauss–Newton matrix H (6×6)
+    from the 43 sums; None where the simulation has no variance."""
+    n = max(s[0], 1.0)
+    mean = s[1] / n
+    var_n = s[2] - n * mean * mean
+    if not var_n > 1e-12:
+        return None
+    inv = 1.0 / math.sqrt(var_n)
+    ncc = s[3] * inv
+    sd = s[4:10]
+    au = (s[10:16] - mean * sd) * inv
+    g = (s[16:22] - ncc * au) * inv
+    H = np.zeros((6, 6))
+    o = 22
+    for i in range(6):
+        for j in range(i, 6):
+            v = (s[o] - sd[i] * sd[j] / n - au[i] * au[j]) * inv * inv
+            H[i, j] = H[j, i] = v
+            o += 1
+    return ncc, g, H
+
+
+def solve_pivot(A, b):
+    """planefit.zig:203-233 (solve) — elimination with partial pivoting; None when singular."""
+    A = np.array(A, np.float64, copy=True)
+    b = np.array(b, np.float64, copy=True)
+    N = len(b)
+    for c in range(N):
+        piv = c
+        for r in range(c + 1, N):
+            if abs(A[r, c]) > abs(A[piv, c]):
+                piv = r
+        if abs(A[piv, c]) < 1e-300:
+            return None
+        if piv != c:
+            A[[c, piv]] = A[[piv, c]]
+            b[[c, piv]] = b[[piv, c]]
+        for r in range(c + 1, N):
+            f = A[r, c] / A[c, c]
+            if f == 0:
+                continue
+            A[r, c:] -= f * A[c, c:]
+            b[r] -= f * b[c]
+    x = np.zeros(N)
+    for r in range(N - 1, -1, -1):
+        x[r] = (b[r] - A[r, r + 1:] @ x[r + 1:]) / A[r, r]
+    return x
+
+
+def damped(H, g, lam):
+    """planefit.zig:237-248 (damped, k = 6) — A = H with its diagonal × (1 + λ) + 1e-9·tr + 1e-30."""
+    A = np.array(H, np.float64, copy=True)
+    tr = np.trace(A)
+    A[np.diag_indices(6)] = A[np.diag_indices(6)] * (1 + lam) + 1e-9 * tr + 1e-30
+    return A, np.array(g, np.float64)
+
+
+def settle6(grad, side, frame, t, q0, pattern, mask, trust, most):
+    """planefit.zig:570-622 (settle, k = 6) for one pattern: Levenberg–Marquardt on its own score
+    over the source's shift and its rotation: λ from 1e-3, a step kept where the score rose
+    (λ ← max(λ/3, 1e-4)), else λ ← min(5λ, 1e8); the shift clamped to ±trust pixels; stops when
+    a round gains less than 1e-7 (a round whose step overshot goes again while λ < 1e8) or after
+    `most` rounds. Returns (q, shift, ncc, rounds)."""
+    q = rot.qstd(np.asarray(q0, np.float64))
+    shift = np.zeros(3)
+    keep = local_of(sums6(grad, side, frame, t, q, shift, pattern, mask))
+    lam = 1e-3
+    it = 0
+    while it < most:
+        A, b = damped(keep[2], keep[1], lam)
+        d = solve_pivot(A, b)
+        qt, st = q, shift
+        if d is not None:
+            st = np.clip(shift + d[:3], -trust, trust)
+            qt = rot.qstd(rot.qmul(rot.so3_exp(d[3:]), q))
+        now = local_of(sums6(grad, side, frame, t, qt, st, pattern, mask))
+        gain = 0.0
+        kept = damp = 0
+        if now is not None and now[0] > keep[0]:
+            gain = now[0] - keep[0]
+            kept = 1
+            q, shift, keep = qt, st, now
+            lam = max(lam / 3, 1e-4)
+        else:
+            if lam < 1e8:
+                damp = 1
+            lam = min(lam * 5, 1e8)
+        it += 1
+        if kept == 0 and damp > 0:
+            continue
+        if gain < 1e-7:
+            break
+    return q, shift, keep[0], it

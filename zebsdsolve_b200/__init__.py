@@ -152,6 +152,24 @@ class Solver:
         cells = np.arange(len(q)) if cells is None else np.asarray(cells).reshape(-1)
         return self._call("simulate", self._e.simulate, phase, cells, q)
 
+    # ── six unknowns per pattern (source and orientation) ──
+
+    def refine_patterns(self, cells, quaternions=None, phase=0, trust=None, rounds=None, gradient="reference"):
+        """Each given pattern refined by itself over its orientation and its source's place (its
+        pattern centre): the per-pattern Levenberg–Marquardt of the reference's plane fit
+        (planefit.zig:570-622 with six unknowns; Winkelmann et al., kikuchipy's
+        refine_orientation_projection_center). quaternions: the starting orientations (default:
+        the cells' current results). trust: how far a source may move, in pattern heights
+        (default plane_trust); rounds: at most this many (default plane_iters). gradient:
+        "reference" (the master's gradient table, as the reference) or "adjoint" (the exact
+        derivative of the projection, through the torch.autograd.Function of `adjoint.py`).
+        Returns a dict: quaternions (n, 4), shift (n, 3, pixels in the sample's axes), pc (n, 3),
+        ncc (n), rounds."""
+        c = np.asarray(cells, np.int64).reshape(-1)
+        if gradient not in ("reference", "adjoint"):
+            raise Error(f"refine_patterns: gradient {gradient!r}")
+        return self._call("refine_patterns", self._e.refine_patterns, c, quaternions, phase, trust, rounds, gradient)
+
     # ── indexing ──
 
     def index_cells(self, cells, method=None, bandwidth=None, dict_grid=None):

@@ -27,3 +27,14 @@ static inline int zeb_launch_check(const char* what) {
   }
   return ZEB_OK;
 }
+
+// pixels of an h × w pattern inside the frame's circular mask (all of them without one), on the host
+static inline int zeb_mask_count(const zeb_frame_t* fr) {
+  int cnt = 0;
+  for (int r = 0; r < fr->h; ++r)
+    for (int c = 0; c < fr->w; ++c) {
+      const float dr = (float)r - fr->mask[0], dc = (float)c - fr->mask[1];
+      if (fr->mask[2] <= 0.f || dr * dr + dc * dc <= fr->mask[2]) ++cnt;
+    }
+  return cnt;
+}

@@ -521,7 +521,8 @@ static bool fill_frame(DetArgs& a, const zeb_frame_t* fr) {
   return true;
 }
 
-// the compacted-pixel kernels while their list fits (up to 12 800 pixels: 113 × 113)
+// the compacted-pixel kernels while their list of masked pixels fits (12 800 of them: a 127 × 127
+// pattern under the circular mask)
 constexpr size_t DET_LIST_SMEM = 200 * 1024;
 
 static size_t det_smem(DetArgs& a) {
@@ -548,7 +549,7 @@ extern "C" int zeb_refine(const float* pats, const float* items, const float* se
   ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine: bad frame");
   a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
   a.vpair = (const float2*)vpair; a.gpair = gpair; a.side = side; a.o = *o; a.records = records;
-  const size_t list = (size_t)a.h * a.w * sizeof(float4);
+  const size_t list = (size_t)zeb_mask_count(fr) * sizeof(float4);
   if (list <= DET_LIST_SMEM) {
     cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
     k_refine<<<n, 256, list, (cudaStream_t)stream>>>(a);
@@ -571,7 +572,7 @@ extern "C" int zeb_chance(const float* pats, const float* items, int n, int draw
   a.pats = pats; a.items = (const float4*)items; a.n = n; a.vpair = (const float2*)vpair; a.side = side;
   a.o.nmi_bins = nmi_bins; a.chance = out; a.draws = draws;
   dim3 g(n, draws);
-  const size_t list = (size_t)a.h * a.w * sizeof(float4);
+  const size_t list = (size_t)zeb_mask_count(fr) * sizeof(float4);
   if (list <= DET_LIST_SMEM) {
     cudaFuncSetAttribute(k_chance, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
     k_chance<<<g, 256, list, (cudaStream_t)stream>>>(a);

@@ -1,0 +1,311 @@
+// (c, config 3) Six unknowns per pattern: the source's shift (the rays' origin, pixels in the
+// sample's axes) and the crystal's rotation, and the score they give: the normalized cross-
+// correlation of the pattern with the master projected through them.
+//
+// k_det6<MODE>: one block per pattern. The masked pixels are listed once per block as (c0·row +
+// c1·col + t, pattern value) in shared memory; with the pattern's parameters x = (δt, φ) the block
+// projects every listed pixel, v = u + δt, c = (exp(φ)·q0)·v/|v|, and sums over the pixels:
+//   MODE 0 (forward): n, ΣM, ΣM², ΣM·e → the NCC;
+//   MODE 1 (adjoint): with the exact derivatives D = ∂M/∂x of the forward — the bilinear
+//     lookup's slopes in the sheet, through the square-Lambert map's Jacobian, the rotation and
+//     the normalization of the ray — also ΣD, ΣM·D, Σe·D → ∂NCC/∂x (the projection is recomputed,
+//     nothing of the forward is stored);
+//   MODE 2 (the reference's Gauss–Newton sums, detector.wgsl:435-499): with D from the master's
+//     gradient table instead (q⁻¹·∇M/|v|, c × ∇M), all 43 sums (n, ΣM, ΣM², ΣM·e, ΣD, ΣM·D, Σe·D,
+//     ΣDᵢDⱼ) from which planefit.zig:176-200 forms the NCC, its gradient and its GN matrix.
+// k_solve6: a damped 6 × 6 system per pattern in FP64 by elimination with partial pivoting
+// (planefit.zig:203-248).
+#include "abi_util.cuh"
+
+namespace zeb {
+
+struct Det6Args {
+  const float* pats;
+  const float4* items;
+  int n, h, w;
+  float3 c0, c1, c2;
+  float mask[3];
+  const float2* vpair;
+  const float* gpair;
+  int side;
+  const float* x;   // [n][6]: δt (3, pixels), φ (3, radians)
+  const float* q0;  // [n][4] (w, x, y, z)
+  float* out;       // MODE 0: [n]; MODE 1: [n][7] (∂NCC/∂x, NCC); MODE 2: [n][43]
+};
+
+// ∂(fj, fi)/∂c of the sheet coordinates fj = (U + 1)/2·last, fi = (W + 1)/2·last of direction c
+// (sphere_to_square, common.wgsl:44-57), from the map's own formula; zero where clamped or at
+// the poles of the map (x = y = 0).
+__device__ __forceinline__ void sheet_jacobian(float3 c, int side, float3& dfj, float3& dfi) {
+  const float ax = fabsf(c.x), ay = fabsf(c.y), az = fabsf(c.z);
+  const float sx = c.x < 0.f ? -1.f : 1.f, sy = c.y < 0.f ? -1.f : 1.f, sz = c.z < 0.f ? -1.f : 1.f;
+  const float rho2 = ax * ax + ay * ay;
+  dfj = make_float3(0.f, 0.f, 0.f);
+  dfi = make_float3(0.f, 0.f, 0.f);
+  if (rho2 < 1e-20f) return;
+  const float den = 1.f + az;
+  const float qv = 0.5f * ZEB_PI * rho2 / den;
+  const float xn = sqrtf(qv);
+  // ∂xn = ∂q / (2 xn); ∂q = (π x/den, π y/den, −(π/2) ρ² sgn(z)/den²)
+  const float k = 0.5f / xn;
+  const float3 dxn = make_float3(k * ZEB_PI * c.x / den, k * ZEB_PI * c.y / den, -k * 0.5f * ZEB_PI * rho2 * sz / (den * den));
+  const float four_pi = 4.f / ZEB_PI;
+  float3 du, dw;
+  if (ax >= ay) {
+    const float al = atan2f(ay, ax);
+    const float3 dal = make_float3(-ay * sx / rho2, ax * sy / rho2, 0.f);
+    du = dxn;
+    dw = make_float3(four_pi * (dxn.x * al + xn * dal.x), four_pi * (dxn.y * al + xn * dal.y), four_pi * dxn.z * al);
+  } else {
+    const float be = atan2f(ax, ay);
+    const float3 dbe = make_float3(ay * sx / rho2, -ax * sy / rho2, 0.f);
+    du = make_float3(four_pi * (dxn.x * be + xn * dbe.x), four_pi * (dxn.y * be + xn * dbe.y), four_pi * dxn.z * be);
+    dw = dxn;
+  }
+  const float sc = 0.79788456080286536f;  // 1 / sqrt(π / 2)
+  const float last = (float)(side - 1);
+  const float kj = 0.5f * last * sc * sx, ki = 0.5f * last * sc * sy;
+  dfj = make_float3(kj * du.x, kj * du.y, kj * du.z);
+  dfi = make_float3(ki * dw.x, ki * dw.y, ki * dw.z);
+}
+
+// The bilinear master value at c and its gradient along the sphere (the exact derivative of the
+// lookup, projected on the tangent plane at c).
+__device__ __forceinline__ float master_and_slope(const float2* __restrict__ vp, float3 c, int side, float3& grad) {
+  const float2 uv = sphere_to_square_fast(c);
+  const float last = (float)(side - 1);
+  const float fj0 = (uv.x + 1.f) * 0.5f * last, fi0 = (uv.y + 1.f) * 0.5f * last;
+  const float fj = fminf(fmaxf(fj0, 0.f), last), fi = fminf(fmaxf(fi0, 0.f), last);
+  const uint32_t cj = min((uint32_t)fj, (uint32_t)(side - 2)), ri = min((uint32_t)fi, (uint32_t)(side - 2));
+  uint32_t o = ri * side + cj;
+  if (c.z < 0.f) o += side * side;
+  const float tj = fj - (float)cj, ti = fi - (float)ri;
+  const float2 t = __ldg(vp + o), u = __ldg(vp + o + side);
+  const float top = lerpf(t.x, t.y, tj), bot = lerpf(u.x, u.y, tj);
+  const float m = lerpf(top, bot, ti);
+  const float dmj = (fj0 > 0.f && fj0 < last) ? (1.f - ti) * (t.y - t.x) + ti * (u.y - u.x) : 0.f;
+  const float dmi = (fi0 > 0.f && fi0 < last) ? bot - top : 0.f;
+  float3 dfj, dfi;
+  sheet_jacobian(c, side, dfj, dfi);
+  float3 g = make_float3(dmj * dfj.x + dmi * dfi.x, dmj * dfj.y + dmi * dfi.y, dmj * dfj.z + dmi * dfi.z);
+  const float r = dot3(g, c);
+  grad = make_float3(g.x - r * c.x, g.y - r * c.y, g.z - r * c.z);
+  return m;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_det6(Det6Args a) {
+  constexpr int NS = MODE == 0 ? 4 : (MODE == 1 ? 22 : 43);
+  extern __shared__ float4 px6[];
+  __shared__ float red[NS * 8];
+  __shared__ int wcnt[8];
+  __shared__ float4 sh_q;
+  __shared__ float3 sh_t;
+  const int b = blockIdx.x;
+  const int hw = a.h * a.w;
+  const float4 it = a.items[b];
+  const float* gpat = a.pats + (size_t)(int)it.w * hw;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // the masked pixels in raster order: (c0·row + c1·col + t, value)
+  int npix = 0;
+  for (int base = 0; base < hw; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int row = i / a.w, col = i - row * a.w;
+    float dr = (float)row - a.mask[0], dc = (float)col - a.mask[1];
+    const bool m = i < hw && (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]);
+    const unsigned bal = __ballot_sync(0xffffffffu, m);
+    if (lane == 0) wcnt[wid] = __popc(bal);
+    __syncthreads();
+    int off = npix, tot = 0;
+    for (int w2 = 0; w2 < nw; ++w2) {
+      if (w2 < wid) off += wcnt[w2];
+      tot += wcnt[w2];
+    }
+    if (m) {
+      const float3 u = make_float3(a.c0.x * row + a.c1.x * col + it.x, a.c0.y * row + a.c1.y * col + it.y,
+                                   a.c0.z * row + a.c1.z * col + it.z);
+      px6[off + __popc(bal & ((1u << lane) - 1u))] = make_float4(u.x, u.y, u.z, __ldg(gpat + i));
+    }
+    npix += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const float* x = a.x + (size_t)b * 6;
+    const float* q0 = a.q0 + (size_t)b * 4;
+    float4 q = qmul(qexp(make_float3(x[3], x[4], x[5])), make_float4(q0[0], q0[1], q0[2], q0[3]));
+    const float nq = rsqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    sh_q = make_float4(q.x * nq, q.y * nq, q.z * nq, q.w * nq);
+    sh_t = make_float3(x[0], x[1], x[2]);
+  }
+  __syncthreads();
+  const float4 q = sh_q;
+  const float4 qi = make_float4(q.x, -q.y, -q.z, -q.w);
+  const float3 dt = sh_t;
+  float s[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) s[k] = 0.f;
+  for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    const float4 p = px6[k];
+    const float3 v = make_float3(p.x + dt.x, p.y + dt.y, p.z + dt.z);
+    const float dist = sqrtf(dot3(v, v));
+    const float inv = 1.f / dist;
+    const float3 c = qrot(q, make_float3(v.x * inv, v.y * inv, v.z * inv));
+    const float e = p.w;
+    float m;
+    float d[6];
+    if (MODE == 0) {
+      m = master_at_pair(a.vpair, c, a.side);
+    } else {
+      float3 g;
+      if (MODE == 1) {
+        m = master_and_slope(a.vpair, c, a.side, g);
+      } else {
+        const float4 gm = grad_at_pair(a.gpair, c, a.side);
+        m = gm.w;
+        g = make_float3(gm.x, gm.y, gm.z);
+      }
+      const float3 w = qrot(qi, g);
+      const float3 r = cross3(c, g);
+      d[0] = w.x * inv; d[1] = w.y * inv; d[2] = w.z * inv;
+      d[3] = r.x; d[4] = r.y; d[5] = r.z;
+    }
+    s[0] += 1.f;
+    s[1] += m;
+    s[2] += m * m;
+    s[3] += m * e;
+    if (MODE >= 1) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        s[4 + i] += d[i];
+        s[10 + i] += m * d[i];
+        s[16 + i] += e * d[i];
+      }
+    }
+    if (MODE == 2) {
+      int o = 22;
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = i; j < 6; ++j) s[o++] += d[i] * d[j];
+    }
+  }
+  block_sums<NS>(s, red);
+  if (threadIdx.x != 0) return;
+  if (MODE == 2) {
+    for (int k = 0; k < 43; ++k) a.out[(size_t)b * 43 + k] = s[k];
+    return;
+  }
+  // planefit.zig:176-200: NCC and (MODE 1) its gradient
+  const float n = fmaxf(s[0], 1.f);
+  const float mean = s[1] / n;
+  const float var_n = s[2] - n * mean * mean;
+  float ncc = -2.f, g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (var_n > 1e-12f) {
+    const float inv = rsqrtf(var_n);
+    ncc = s[3] * inv;
+    if (MODE == 1)
+      for (int i = 0; i < 6; ++i) {
+        const float au = (s[10 + i] - mean * s[4 + i]) * inv;
+        g[i] = (s[16 + i] - ncc * au) * inv;
+      }
+  }
+  if (MODE == 0) {
+    a.out[b] = ncc;
+  } else {
+    float* o = a.out + (size_t)b * 7;
+    for (int i = 0; i < 6; ++i) o[i] = g[i];
+    o[6] = ncc;
+  }
+}
+
+// x = A⁻¹ b for a (6 × 6, 6) system per item in FP64 (planefit.zig:203-233); ok[b] = 0 where a
+// pivot is below 1e-300 (x left 0).
+__global__ void k_solve6(const double* __restrict__ A, const double* __restrict__ bvec, int n, double* __restrict__ x,
+                         int* __restrict__ ok) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  double M[36], r[6];
+  for (int i = 0; i < 36; ++i) M[i] = A[(size_t)b * 36 + i];
+  for (int i = 0; i < 6; ++i) r[i] = bvec[(size_t)b * 6 + i];
+  bool good = true;
+  for (int c = 0; c < 6 && good; ++c) {
+    int piv = c;
+    for (int rr = c + 1; rr < 6; ++rr)
+      if (fabs(M[rr * 6 + c]) > fabs(M[piv * 6 + c])) piv = rr;
+    if (fabs(M[piv * 6 + c]) < 1e-300) {
+      good = false;
+      break;
+    }
+    if (piv != c) {
+      for (int k = 0; k < 6; ++k) {
+        const double t = M[c * 6 + k];
+        M[c * 6 + k] = M[piv * 6 + k];
+        M[piv * 6 + k] = t;
+      }
+      const double t = r[c];
+      r[c] = r[piv];
+      r[piv] = t;
+    }
+    for (int rr = c + 1; rr < 6; ++rr) {
+      const double f = M[rr * 6 + c] / M[c * 6 + c];
+      if (f == 0.0) continue;
+      for (int k = c; k < 6; ++k) M[rr * 6 + k] -= f * M[c * 6 + k];
+      r[rr] -= f * r[c];
+    }
+  }
+  double y[6] = {0, 0, 0, 0, 0, 0};
+  if (good) {
+    for (int rr = 5; rr >= 0; --rr) {
+      double acc = r[rr];
+      for (int k = rr + 1; k < 6; ++k) acc -= M[rr * 6 + k] * y[k];
+      y[rr] = acc / M[rr * 6 + rr];
+    }
+  }
+  for (int i = 0; i < 6; ++i) x[(size_t)b * 6 + i] = y[i];
+  ok[b] = good ? 1 : 0;
+}
+
+}  // namespace zeb
+
+using namespace zeb;
+
+extern "C" int zeb_det6(int mode, const float* pats, const float* items, int n, const zeb_frame_t* fr,
+                        const float* vpair, const float* gpair, int side, const float* x, const float* q0, float* out,
+                        void* stream) {
+  ZEB_REQUIRE(mode >= 0 && mode <= 2, ZEB_EARG, "det6: mode %d", mode);
+  ZEB_REQUIRE(pats && items && vpair && x && q0 && out && fr && side >= 3 && (mode != 2 || gpair), ZEB_EARG,
+              "det6: bad arguments");
+  ZEB_REQUIRE(((uintptr_t)gpair & 31) == 0 && ((uintptr_t)vpair & 7) == 0, ZEB_EARG, "det6: pair tables misaligned");
+  if (n <= 0) return ZEB_OK;
+  Det6Args a{};
+  ZEB_REQUIRE(fr->h >= 2 && fr->w >= 2, ZEB_EARG, "det6: bad frame");
+  a.h = fr->h; a.w = fr->w;
+  a.c0 = make_float3(fr->c0[0], fr->c0[1], fr->c0[2]);
+  a.c1 = make_float3(fr->c1[0], fr->c1[1], fr->c1[2]);
+  a.c2 = make_float3(fr->c2[0], fr->c2[1], fr->c2[2]);
+  for (int k = 0; k < 3; ++k) a.mask[k] = fr->mask[k];
+  a.pats = pats; a.items = (const float4*)items; a.n = n; a.vpair = (const float2*)vpair; a.gpair = gpair;
+  a.side = side; a.x = x; a.q0 = q0; a.out = out;
+  const size_t list = (size_t)zeb_mask_count(fr) * sizeof(float4);
+  ZEB_REQUIRE(list <= 200 * 1024, ZEB_ESIZE, "det6: the %d x %d pattern's masked pixels exceed the shared-memory list",
+              a.h, a.w);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (mode == 0) {
+    cudaFuncSetAttribute(k_det6<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
+    k_det6<0><<<n, 256, list, st>>>(a);
+  } else if (mode == 1) {
+    cudaFuncSetAttribute(k_det6<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
+    k_det6<1><<<n, 256, list, st>>>(a);
+  } else {
+    cudaFuncSetAttribute(k_det6<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
+    k_det6<2><<<n, 256, list, st>>>(a);
+  }
+  return zeb_launch_check("det6");
+}
+
+extern "C" int zeb_solve6(const double* A, const double* b, int n, double* x, int* ok, void* stream) {
+  ZEB_REQUIRE(A && b && x && ok, ZEB_EARG, "solve6: null argument");
+  if (n <= 0) return ZEB_OK;
+  k_solve6<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(A, b, n, x, ok);
+  return zeb_launch_check("solve6");
+}

@@ -518,6 +518,36 @@ class Engine:
                 c0 = int(cells[a0])
                 dst[a0:a1].copy_(src[c0:c0 + (a1 - a0)], non_blocking=True)
 
+    def refine_patterns(self, cells, quaternions, phase, trust, rounds, gradient):
+        """planefit.zig:570-622 (settle, k = 6) for the given cells against one phase."""
+        from . import adjoint
+
+        if not self.phases:
+            raise EngineError("NoPhases")
+        if not 0 <= phase < len(self.phases):
+            raise EngineError(f"phase {phase} of {len(self.phases)}")
+        self.prepare_masters()
+        rows, cols, h, w = self.info()
+        n = len(cells)
+        if quaternions is None:
+            q0 = self.res["quat"][cells].astype(np.float64)
+        else:
+            q0 = np.asarray(quaternions, np.float64).reshape(n, 4)
+        pats = self.upload(cells)
+        items = self.items_of(cells)
+        fr = self.frame()
+        _, sheets, grad, vpair, gpair = self.phases[phase].baked
+        plan = adjoint.Plan(pats, items, fr, vpair, gpair, self.phases[phase].master.side)
+        s = self.set
+        trust_px = (s["plane_trust"] if trust is None else float(trust)) * h
+        most = int(s["plane_iters"] if rounds is None else rounds)
+        q, shift, ncc, it = adjoint.refine6(plan, torch.as_tensor(q0, device=self.dev), trust_px, most, gradient)
+        J = adjoint.pc_jacobian(self.geo, h, w)
+        sh = shift.cpu().numpy()
+        dpc = np.linalg.solve(J, sh.T).T
+        return {"quaternions": q.cpu().numpy(), "shift": sh, "pc": self.geo.pc[None, :] + dpc,
+                "ncc": ncc.cpu().numpy(), "rounds": int(it)}
+
     def fz_of(self, recs):
         """Each phase's records reduced to its fundamental zone on the device: [phase][n][4]."""
         n_ph, n = recs.shape[0], recs.shape[1]
