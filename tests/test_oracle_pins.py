@@ -177,3 +177,49 @@ def test_beam_travel_matches_kikuchipy_extrapolation():
 def test_fft_size_and_grids():
     # spherical.zig:100-104: n is the next power of two ≥ 2L − 1, from 16
     assert [spherical.fft_size(L) for L in (8, 16, 32, 64, 128)] == [16, 32, 64, 128, 256]
+
+
+def test_six_unknown_system_is_consistent():
+    """The oracle's restatement of the six-unknown sums (detector.wgsl `sums`) and localOf
+    (planefit.zig:176-200): its gradient is that of the NCC it reports up to the gradient table's
+    discretization (a central difference a master pixel wide) — the same direction, a few percent
+    apart — and its pivoted solve (planefit.zig:203-233) inverts a damped system; settle raises
+    the NCC from a start 1° off."""
+    import math
+
+    import oracle.detector as od
+    import oracle.geometry as og
+    import oracle.rot as rot
+
+    rng = np.random.default_rng(4)
+    side = 101
+    # a smooth master: a few low-order terms on the sheets' directions
+    d = od.pixel_dirs(side)
+    sheets = np.sin(3 * d[:, 0]) * np.cos(2 * d[:, 1]) + 0.5 * d[:, 2] ** 2 + 0.3 * np.sin(4 * d[:, 1] + d[:, 2])
+    sheets = (sheets - sheets.mean()) / sheets.std()
+    grad = od.gradient_table(sheets, side)
+    geo = og.Geometry(pc=(0.5, 0.3, 0.6), sample_tilt_deg=70.0)
+    fr, mask, t = geo.frame(), og.mask_of(40, 40), geo.translation(40, 40)
+    q = rot.qstd(rng.normal(size=4))
+    pat = od.project(sheets, side, fr, t, q, 40, 40)
+    m_ = od.in_mask(40, 40, mask)
+    pat = np.where(m_, pat - pat[m_].mean(), 0.0)
+    pat /= np.linalg.norm(pat)
+    q1 = rot.qmul(rot.so3_exp([0.004, -0.006, 0.005]), q)
+    sh = np.array([0.2, -0.1, 0.3])
+    ncc, g, H = od.local_of(od.sums6(grad, side, fr, t, q1, sh, pat, mask))
+
+    def f(x):
+        return od.local_of(od.sums6(grad, side, fr, t, rot.qmul(rot.so3_exp(x[3:]), q1), sh + x[:3], pat, mask))[0]
+
+    fd = np.array([(f(np.eye(6)[i] * 1e-5) - f(-np.eye(6)[i] * 1e-5)) / 2e-5 for i in range(6)])
+    cos = g @ fd / (np.linalg.norm(g) * np.linalg.norm(fd))
+    assert cos > 0.99 and np.linalg.norm(g - fd) < 0.1 * np.linalg.norm(fd), (g, fd)
+    A, b = od.damped(H, g, 1e-3)
+    x = od.solve_pivot(A, b)
+    assert np.allclose(A @ x, b, rtol=1e-10, atol=1e-12)
+    q0 = rot.qmul(rot.so3_exp(np.radians([0.6, -0.5, 0.4])), q)
+    start = od.local_of(od.sums6(grad, side, fr, t, q0, np.zeros(3), pat, mask))[0]
+    qe, she, ncce, it = od.settle6(grad, side, fr, t, q0, pat, mask, trust=2.0, most=40)
+    assert ncce > start and ncce > 0.99 and it >= 1
+    assert math.degrees(2 * math.acos(min(1.0, abs(float(np.dot(rot.qstd(qe), rot.qstd(q))))))) < 0.2
