@@ -71,6 +71,14 @@ int zeb_prep(const void* raw, int pixel, int n, int h, int w, const float* stati
 size_t zeb_prep_scratch_bytes(int n, int h, int w, float sigma);
 int zeb_prep_ex(const void* raw, int pixel, int n, int h, int w, const float* static_bg, int dynamic,
                 float sigma, const float mask[3], int normalize, float* out, void* scratch, void* stream);
+/* zeb_prep_ex on patterns stored at src_h × src_w and reduced by `factor` (settings.binning, 1 to
+ * 64) as they are unpacked: a whole factor is the k × k blocks' means, any other the source area
+ * each output pixel covers (area resampling); the output is floor(size / factor) each way, the
+ * remainder dropped. static_bg, mask, sigma and out are at the reduced size. Replaces the host
+ * reduction of reduce.zig:44-131 (which the reference runs on the CPU before the upload). */
+int zeb_prep_reduced(const void* raw, int pixel, int n, int src_h, int src_w, double factor, const float* static_bg,
+                     int dynamic, float sigma, const float mask[3], int normalize, float* out, void* scratch,
+                     void* stream);
 
 /* ── the master on the sphere ───────────────────────────────────────────────────────────── */
 

@@ -128,3 +128,34 @@ def run(raw, static=None, dynamic="subtract", dynamic_sigma=0.0, mask=(0.0, 0.0,
     if do_normalize:
         img = normalize(img, mask)
     return img
+
+
+def reduced_shape(h, w, factor):
+    """reduce.zig:12-19 — floor(size / factor) each way."""
+    return int(math.floor(h / factor + 1e-9)), int(math.floor(w / factor + 1e-9))
+
+
+def reduce(pixels, factor):
+    """reduce.zig:44-131 — one pattern reduced by `factor`: for a whole factor the mean of each
+    k × k block; otherwise area resampling (each output pixel the average of the source area it
+    covers, partly covered pixels weighted by the part). From the top-left corner; the remainder
+    of the last row and column is dropped. FP64."""
+    p = np.asarray(pixels, np.float64)
+    H, W = p.shape
+    h, w = reduced_shape(H, W, factor)
+    if abs(factor - round(factor)) < 1e-9:
+        k = int(round(factor))
+        return p[: h * k, : w * k].reshape(h, k, w, k).sum((1, 3)) / (k * k)
+
+    def weights(n_out, n_src):
+        # M[o, s]: the part of source pixel s inside output pixel o's span [o·f, (o+1)·f)
+        M = np.zeros((n_out, n_src))
+        for o in range(n_out):
+            x0, x1 = o * factor, (o + 1) * factor
+            j = int(math.floor(x0))
+            while j < x1 - 1e-12 and j < n_src:
+                M[o, j] = min(x1, j + 1) - max(x0, j)
+                j += 1
+        return M
+
+    return weights(h, H) @ p @ weights(w, W).T / (factor * factor)

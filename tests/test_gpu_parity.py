@@ -105,6 +105,54 @@ def test_prep_matches_oracle(lib, h, w, sigma, pixel):
         assert np.abs(got[i] - ref).max() < 2e-6, (h, w, sigma, np.abs(got[i] - ref).max())
 
 
+@pytest.mark.parametrize("sh,sw,factor,pixel,sigma", [(160, 160, 2.0, 1, 12.0), (90, 96, 3.0, 0, 0.0),
+                                                      (150, 150, 2.5, 1, 9.0), (121, 100, 2.0, 2, 7.0)])
+def test_prep_reduced_matches_oracle(lib, sh, sw, factor, pixel, sigma):
+    """Binning on the device as the patterns are unpacked (reduce.zig) and then the same filters."""
+    rng = np.random.default_rng(sh + sw)
+    n = 3
+    dt = {0: np.uint8, 1: np.uint16, 2: np.float32}[pixel]
+    raw = (rng.random((n, sh, sw)) * (200 if pixel == 0 else 3000)).astype(dt)
+    h, w = op.reduced_shape(sh, sw, factor)
+    bg = (rng.random((h, w)) * 30).astype(np.float32)
+    r = min(h, w) * 0.5
+    mask = (0.5 * (h - 1), 0.5 * (w - 1), r * r)
+    out = torch.empty(n * h * w, dtype=torch.float32, device="cuda")
+    rawd = torch.as_tensor(raw, device="cuda")
+    bgd = torch.as_tensor(bg, device="cuda")
+    sb = lib.load().zeb_prep_scratch_bytes(n, h, w, sigma)
+    scratch = torch.empty(max(sb // 4, 1), dtype=torch.float32, device="cuda")
+    m3 = (ctypes.c_float * 3)(*mask)
+    lib.call("zeb_prep_reduced", P(rawd), pixel, n, sh, sw, ctypes.c_double(factor), P(bgd), 1 if sigma > 0 else 0,
+             sigma, m3, 1, P(out), P(scratch), sp())
+    got = out.cpu().numpy().reshape(n, h, w)
+    for i in range(n):
+        red = op.reduce(raw[i], factor)
+        assert red.shape == (h, w)
+        ref = op.run(red, static=bg, dynamic="subtract" if sigma > 0 else "none", dynamic_sigma=sigma, mask=mask)
+        # unit-norm images: FP32 reduction and filters against FP64, to 2e-6 absolute
+        assert np.abs(got[i] - ref).max() < 2e-6, (sh, sw, factor, np.abs(got[i] - ref).max())
+
+
+def test_binned_scan_indexes(world):
+    """A 120 × 120 scan binned by 2 indexes like its 60 × 60 patterns: the area means of the
+    simulated patterns upsampled by pixel replication are the patterns themselves."""
+    import zebsdsolve_b200 as ze
+
+    pats = world["pats"].reshape(-1, 60, 60)
+    big = np.repeat(np.repeat(pats, 2, 1), 2, 2).astype(np.float32).reshape(1, -1, 120, 120)
+    s = ze.Solver()
+    s.configure(static_background="none", dynamic_background="none", bandwidth=16, binning=2)
+    s.add_phase(world["path"])
+    s.set_patterns(big)
+    s.set_geometry(pc=(0.5, 0.3, 0.6), sample_tilt_deg=70, detector_tilt_deg=0)
+    assert tuple(s.pattern_shape) == (60, 60)
+    r = s.index()
+    ref = world["s"].index()
+    dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), ref["quaternions"].reshape(-1, 4)))
+    assert dis.max() < 1e-3, dis
+
+
 def _frame(s):
     e = s._e
     return e.frame()

@@ -171,3 +171,14 @@ def test_atan01_polynomial_error_bound():
         p = (p * t2 + np.float32(c)).astype(np.float32)
     err = np.abs((x * p).astype(np.float64) - np.arctan(x.astype(np.float64)))
     assert err.max() < 1.5e-7, err.max()
+
+
+@pytest.mark.parametrize("factor", [2.0, 3.0, 2.5, 1.75])
+def test_host_reduction_matches_oracle(factor):
+    """The static background's host reduction equals the oracle's restatement of reduce.zig."""
+    import oracle.prep as op
+    from zebsdsolve_b200.reduce import reduce_image, reduced_shape
+
+    img = np.random.default_rng(3).random((61, 47)) * 100
+    assert reduced_shape(61, 47, factor) == op.reduced_shape(61, 47, factor)
+    assert np.abs(reduce_image(img, factor) - op.reduce(img, factor)).max() < 1e-12

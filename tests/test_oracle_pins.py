@@ -223,3 +223,27 @@ def test_six_unknown_system_is_consistent():
     qe, she, ncce, it = od.settle6(grad, side, fr, t, q0, pat, mask, trust=2.0, most=40)
     assert ncce > start and ncce > 0.99 and it >= 1
     assert math.degrees(2 * math.acos(min(1.0, abs(float(np.dot(rot.qstd(qe), rot.qstd(q))))))) < 0.2
+
+
+def test_reduction_matches_reduce_zig_tests():
+    """reduce.zig:151-215's assertions on the oracle's reduction: a whole factor is block
+    binning (u8 6 × 8 by 2; 7 × 9 by 3 with the remainder dropped, u16 and f32 alike); any
+    factor conserves the total (10 × 10 by 2.5), the first pixel by hand, a flat pattern stays flat."""
+    import oracle.prep as op
+
+    src = np.array([(i * 7 + 3) % 251 for i in range(48)], np.float64).reshape(6, 8)
+    got = op.reduce(src, 2)
+    want = src.reshape(3, 2, 4, 2).mean((1, 3))
+    assert np.allclose(got, want, atol=1e-5)
+    assert op.reduced_shape(7, 9, 2) == (3, 4)
+    v = np.array([(i * 977 + 31) % 60000 for i in range(63)], np.float64).reshape(7, 9)
+    a = op.reduce(v.astype(np.uint16), 3)
+    b = op.reduce(v.astype(np.float32), 3)
+    assert a.shape == (2, 3) and np.allclose(a, b, rtol=1e-6)
+    s10 = np.array([(i * 37 + 11) % 1000 for i in range(100)], np.float64).reshape(10, 10)
+    d = op.reduce(s10, 2.5)
+    assert d.shape == (4, 4) and abs(d.sum() * 6.25 - s10.sum()) < 1e-5 * s10.sum()
+    wr = np.array([1, 1, 0.5])
+    assert abs(d[0, 0] - (wr[:, None] * wr[None, :] * s10[:3, :3]).sum() / 6.25) < 1e-5 * d[0, 0]
+    flat = op.reduce(np.full((10, 10), 7.0), 3)
+    assert flat.shape == (3, 3) and np.allclose(flat, 7.0)

@@ -13,6 +13,9 @@ namespace zeb {
 struct PrepArgs {
   const void* raw;
   int pixel, n, h, w;
+  int sh, sw;      // the stored pattern's size (h, w when nothing is reduced)
+  double factor;   // reduction factor (1: none)
+  int kwhole;      // the factor as a whole number, 0 when it is not one
   const float* static_bg;
   int dynamic;  // 0 none, 1 subtract, 2 divide
   float sigma;
@@ -70,12 +73,70 @@ __device__ void prep_finish(const PrepArgs& a, float* img, float* out, float* re
   for (int i = threadIdx.x; i < hw; i += blockDim.x) out[i] = img[i] * inv;
 }
 
-// unpack one stored pixel (u8, u16 or f32) and take the static background off
-__device__ __forceinline__ float prep_pixel(const PrepArgs& a, size_t base, int i) {
+__device__ __forceinline__ float stored_px(const PrepArgs& a, size_t i) {
+  if (a.pixel == 0) return (float)((const uint8_t*)a.raw)[i];
+  if (a.pixel == 1) return (float)((const uint16_t*)a.raw)[i];
+  return ((const float*)a.raw)[i];
+}
+
+// Output pixel (r, c) of stored pattern b reduced by a.factor (reduce.zig:44-131): for a whole
+// factor k the k × k block's mean (integer pixels summed exactly, f32 ones row by row); otherwise
+// the source area the output pixel covers, each source row's part summed in FP64 then shared
+// between the one or two output rows it lies in, in the order of the source rows (products and
+// sums rounded one at a time, as the host reduction does).
+__device__ float reduced_px(const PrepArgs& a, int b, int r, int c) {
+  const size_t base = (size_t)b * a.sh * a.sw;
+  if (a.kwhole > 0) {
+    const int k = a.kwhole;
+    const float inv = 1.f / (float)(k * k);
+    if (a.pixel != 2) {
+      uint32_t acc = 0;
+      for (int i = 0; i < k; ++i)
+        for (int j = 0; j < k; ++j) acc += (uint32_t)stored_px(a, base + (size_t)(r * k + i) * a.sw + c * k + j);
+      return __fmul_rn((float)acc, inv);
+    }
+    float out = 0.f;
+    for (int i = 0; i < k; ++i) {
+      float acc = 0.f;
+      for (int j = 0; j < k; ++j) acc = __fadd_rn(acc, stored_px(a, base + (size_t)(r * k + i) * a.sw + c * k + j));
+      out = __fadd_rn(out, acc);
+    }
+    return __fmul_rn(out, inv);
+  }
+  const double f = a.factor;
+  const int rows = (int)ceil((double)a.h * f - 1e-9);
+  const double x0 = (double)c * f, x1 = x0 + f;
+  const int j0 = (int)floor(x0);
+  float out = 0.f;
+  const int lo = max(0, (int)floor(((double)r - 1.0) * f) - 1), hi = min(rows - 1, (int)ceil(((double)r + 1.0) * f) + 1);
+  for (int rs = lo; rs <= hi; ++rs) {
+    const double y0 = (double)rs;
+    const int top = (int)floor(y0 / f + 1e-12);
+    const double edge = (double)(top + 1) * f;
+    const float w0 = (float)(fmin(y0 + 1.0, edge) - y0);
+    float wt;
+    if (top == r) wt = w0;
+    else if (top + 1 == r && w0 < 1.f) wt = __fsub_rn(1.f, w0);
+    else continue;
+    double acc = 0.0;
+    for (int j = j0; (double)j < x1 - 1e-12; ++j) {
+      const double aa = fmax(x0, (double)j), bb = fmin(x1, (double)(j + 1));
+      acc = __dadd_rn(acc, __dmul_rn(bb - aa, (double)stored_px(a, base + (size_t)rs * a.sw + j)));
+    }
+    out = __fadd_rn(out, __fmul_rn(wt, (float)acc));
+  }
+  return __fmul_rn(out, (float)(1.0 / (f * f)));
+}
+
+// one pixel of pattern b as the chain starts from it: stored (or reduced), static background off
+__device__ __forceinline__ float prep_pixel(const PrepArgs& a, int b, int i) {
   float v;
-  if (a.pixel == 0) v = (float)((const uint8_t*)a.raw)[base + i];
-  else if (a.pixel == 1) v = (float)((const uint16_t*)a.raw)[base + i];
-  else v = ((const float*)a.raw)[base + i];
+  if (a.factor == 1.0) {
+    v = stored_px(a, (size_t)b * a.h * a.w + i);
+  } else {
+    const int r = i / a.w;
+    v = reduced_px(a, b, r, i - r * a.w);
+  }
   if (a.static_bg) v -= __ldg(a.static_bg + i);
   return v;
 }
@@ -91,14 +152,7 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
 
   // unpack
   const size_t base = (size_t)b * hw;
-  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
-    float v;
-    if (a.pixel == 0) v = (float)((const uint8_t*)a.raw)[base + i];
-    else if (a.pixel == 1) v = (float)((const uint16_t*)a.raw)[base + i];
-    else v = ((const float*)a.raw)[base + i];
-    if (a.static_bg) v -= __ldg(a.static_bg + i);
-    img[i] = v;
-  }
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) img[i] = prep_pixel(a, b, i);
   __syncthreads();
 
   if (a.dynamic != 0 && a.sigma > 0.f) {
@@ -249,7 +303,7 @@ __global__ void __launch_bounds__(256) k_prep_direct(PrepArgs a) {
   __syncthreads();
   for (int i = threadIdx.x; i < hw; i += blockDim.x) {
     const int r = i / w, c = i - r * w;
-    const float v = prep_pixel(a, base, i);
+    const float v = prep_pixel(a, b, i);
     img[i] = v;
     P[r * pw + R + c] = v;
   }
@@ -341,15 +395,20 @@ extern "C" size_t zeb_prep_scratch_bytes(int n, int h, int w, float sigma) {
   return (size_t)per * 4 * (size_t)n;
 }
 
-extern "C" int zeb_prep_ex(const void* raw, int pixel, int n, int h, int w, const float* static_bg, int dynamic,
-                           float sigma, const float mask[3], int normalize, float* out, void* scratch,
-                           void* stream) {
+static int prep_launch(const void* raw, int pixel, int n, int src_h, int src_w, double factor, const float* static_bg,
+                       int dynamic, float sigma, const float mask[3], int normalize, float* out, void* scratch,
+                       void* stream) {
   ZEB_REQUIRE(raw && out && mask, ZEB_EARG, "prep: null pointer");
+  ZEB_REQUIRE(factor >= 1.0 && factor <= 64.0, ZEB_EARG, "prep: reduction factor %g", factor);
+  const int h = (int)floor((double)src_h / factor + 1e-9), w = (int)floor((double)src_w / factor + 1e-9);
   ZEB_REQUIRE(pixel >= 0 && pixel <= 2 && n >= 0 && h >= 4 && w >= 4 && dynamic >= 0 && dynamic <= 2, ZEB_EARG,
               "prep: bad arguments pixel=%d n=%d h=%d w=%d dynamic=%d", pixel, n, h, w, dynamic);
   if (n == 0) return ZEB_OK;
   PrepArgs a{};
   a.raw = raw; a.pixel = pixel; a.n = n; a.h = h; a.w = w; a.static_bg = static_bg;
+  a.sh = src_h; a.sw = src_w; a.factor = factor;
+  a.kwhole = fabs(factor - round(factor)) < 1e-9 && factor > 1.0 ? (int)round(factor) : 0;
+  if (a.kwhole == 1) { a.kwhole = 0; a.factor = 1.0; }
   a.dynamic = (sigma > 0.f) ? dynamic : 0; a.sigma = sigma;
   a.mask[0] = mask[0]; a.mask[1] = mask[1]; a.mask[2] = mask[2];
   a.normalize = normalize; a.out = out;
@@ -386,6 +445,19 @@ extern "C" int zeb_prep_ex(const void* raw, int pixel, int n, int h, int w, cons
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_prep<<<n, 256, smem, (cudaStream_t)stream>>>(a);
   return zeb_launch_check("prep");
+}
+
+extern "C" int zeb_prep_ex(const void* raw, int pixel, int n, int h, int w, const float* static_bg, int dynamic,
+                           float sigma, const float mask[3], int normalize, float* out, void* scratch,
+                           void* stream) {
+  return prep_launch(raw, pixel, n, h, w, 1.0, static_bg, dynamic, sigma, mask, normalize, out, scratch, stream);
+}
+
+extern "C" int zeb_prep_reduced(const void* raw, int pixel, int n, int src_h, int src_w, double factor,
+                                const float* static_bg, int dynamic, float sigma, const float mask[3], int normalize,
+                                float* out, void* scratch, void* stream) {
+  return prep_launch(raw, pixel, n, src_h, src_w, factor, static_bg, dynamic, sigma, mask, normalize, out, scratch,
+                     stream);
 }
 
 extern "C" int zeb_prep(const void* raw, int pixel, int n, int h, int w, const float* static_bg, int dynamic,

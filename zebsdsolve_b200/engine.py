@@ -15,6 +15,7 @@ import numpy as np
 import torch
 
 from . import _native as N
+from .reduce import reduce_image
 from . import master as M
 from . import rotations as R
 from .device import BandTables, PhaseBand, master_blur, ptr, stream_ptr
@@ -246,7 +247,7 @@ class Engine:
             acc = np.zeros((h, w))
             for i in range(0, len(cells), 1024):
                 acc += flat[cells[i:i + 1024]].astype(np.float64).sum(0)
-            avg = (acc / len(cells)).astype(np.float32)
+            avg = reduce_image(acc / len(cells), self.set["binning"]).astype(np.float32)
             self.avg = (self.set["static_patterns"], torch.as_tensor(avg, device=self.dev))
             self.log(f"static background: the average of {len(cells)} patterns over the map")
         return self.avg[1]
@@ -382,7 +383,7 @@ class Engine:
     # ── device passes ──
 
     def prep_options(self):
-        rows, cols, h, w = self.info()
+        h, w = self.pattern_shape()
         s = self.set
         dyn = {"none": 0, "subtract": 1, "divide": 2}[s["dynamic_background"]]
         sigma = s["dynamic_sigma"] * w if dyn else 0.0
@@ -391,17 +392,16 @@ class Engine:
     def preprocess(self, raw, n):
         """engine.zig:1452-1563 — n stored patterns on the device (raw, the scan's pixel type)
         through the filter chain into the float32 pattern buffer."""
-        rows, cols, h, w = self.info()
-        if self.set["binning"] != 1:
-            raise EngineError("binning: not supported on this engine yet")
+        rows, cols, sh, sw = self.info()
+        h, w = self.pattern_shape()  # reduced by binning as the patterns are unpacked
         out = self.buf("pats", n * h * w)
         static = self.static_background()
         dyn, sigma = self.prep_options()
         mask = (ctypes.c_float * 3)(*self.mask_of(h, w))
         sb = N.load().zeb_prep_scratch_bytes(n, h, w, sigma)
         scratch = self.buf("prep_scratch", sb // 4 + 1) if sb else None
-        N.call("zeb_prep_ex", ptr(raw), self.pixel, n, h, w, ptr(static), dyn, sigma, mask, 1, ptr(out),
-               ptr(scratch), stream_ptr())
+        N.call("zeb_prep_reduced", ptr(raw), self.pixel, n, sh, sw, float(self.set["binning"]), ptr(static), dyn,
+               sigma, mask, 1, ptr(out), ptr(scratch), stream_ptr())
         return out
 
     def upload(self, cells):
