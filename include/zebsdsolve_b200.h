@@ -272,6 +272,47 @@ int zeb_det6(int mode, const float* pats, const float* items, int n, const zeb_f
  * solve of planefit.zig:203-233 (the damped Levenberg–Marquardt step of settle). */
 int zeb_solve6(const double* A, const double* b, int n, double* x, int* ok, void* stream);
 
+/* ── dictionary indexing ────────────────────────────────────────────────────────────────── */
+
+/* The dictionary's entries simulated at detector position t0 (pixels): out[e][h·w] = the master
+ * (value pairs of zeb_master_pairs) at dict_q[e]·(c0·row + c1·col + t0)/|…|, then zero mean and
+ * unit norm under the mask (zero outside). h·w ≤ 51200. Replaces Detector.dictSims
+ * (src/detector.zig:250-260; shaders/detector.wgsl project_dict 266-273, sim_norm 662-699). */
+int zeb_dict_sims(const zeb_frame_t* fr, const float* vpair, int side, const float t0[3], const float* dict_q,
+                  int n, float* out, void* stream);
+
+/* Bytes of the BF16 operand panel of `rows` rows of `cols` values: ⌈cols/64⌉ blocks of
+ * [rows rounded up to 256][128 B], the 16-byte chunks of row r XOR-swizzled by r mod 8. */
+size_t zeb_panel_bytes(int rows, int cols);
+
+/* FP32 rows (src[r·ld + k]) rounded to BF16 into a panel; padding rows and columns are zero. */
+int zeb_pack_panel(const float* src, int rows, int cols, int ld, void* panel, void* stream);
+
+/* How many dictionary slices the match kernels split the entries into for n_exp patterns (form 0:
+ * FP32, 1: BF16 tensor cores): the candidate buffers hold n_exp × slices (FP32) or
+ * n_exp × slices × 8 (BF16) entries. */
+int zeb_match_slices(int n_exp, int n_dict, int form);
+
+/* Per pattern and dictionary slice the eight largest inner products of the pattern's panel row
+ * with the dictionary's panel rows (BF16 operands, FP32 accumulation on the tensor cores),
+ * descending, equal scores in index order: cand_v/cand_i[p][slice][8] (index −1 where a slice has
+ * fewer than eight entries). status gets a nonzero bit when a wait inside the kernel timed out.
+ * Replaces the scoring of Detector.dictChunk and Pca.match (src/detector.zig:262-271,
+ * src/pca.zig:166-171; shaders/detector.wgsl dict_score 705-740, pca.wgsl nearest 114-168). */
+int zeb_match_bf16(const void* x_panel, int n_exp, const void* d_panel, int n_dict, int cols, int slices,
+                   float* cand_v, int* cand_i, int* status, void* stream);
+
+/* The same in plain FP32 (CUDA cores) from row-major x[n_exp][cols] and d[n_dict][cols]: per
+ * pattern and slice the best entry, ties to the lower index: cand_v/cand_i[p][slice]. */
+int zeb_match_f32(const float* x, int n_exp, const float* d, int n_dict, int cols, int slices, float* cand_v,
+                  int* cand_i, void* stream);
+
+/* Each pattern's n_cand candidate entries scored again in FP32 (x·d over cols; indices outside
+ * [0, n_dict) skipped), the best (ties to the lower index) written as a seed: seeds[p] = (dict_q[best] (w, x, y, z), score, best, 0, 0).
+ * Replaces Detector.seedDict (src/detector.zig:231-235; shaders/detector.wgsl seed_dict 311-317). */
+int zeb_match_best(const float* x, int n_exp, const float* d, int n_dict, int cols, const int* cand, int n_cand,
+                   const float* dict_q, float* seeds, void* stream);
+
 /* Simulated patterns: the master at q·ray for every pixel of item b (poses[b] = t.xyz, pattern
  * index, q.wxyz): sims[b][h][w]. Replaces Detector.project (src/detector.zig:138-142;
  * shaders/detector.wgsl:254-263). */

@@ -247,3 +247,50 @@ def test_reduction_matches_reduce_zig_tests():
     assert abs(d[0, 0] - (wr[:, None] * wr[None, :] * s10[:3, :3]).sum() / 6.25) < 1e-5 * d[0, 0]
     flat = op.reduce(np.full((10, 10), 7.0), 3)
     assert flat.shape == (3, 3) and np.allclose(flat, 7.0)
+
+
+def test_cubochoric_map_matches_rot_zig_tests():
+    """rot.zig:330-355's assertions on the oracle's cubochoric and homochoric maps: a face centre
+    lands on the ball's surface (radius (3π/4)^(1/3)); unit Jacobian determinant inside each
+    pyramid; |h|³ = (3/4)(θ − sin θ)."""
+    import oracle.dictionary as odict
+
+    top = odict.cu_to_ho((0.0, 0.0, odict.CUBOCHORIC_HALF_EDGE))
+    assert abs(top[2] - (0.75 * math.pi) ** (1 / 3)) < 1e-12
+    for c in [(0.21, -0.33, 0.87), (-0.9, 0.2, 0.4), (0.1, 0.8, -0.35), (0.05, 0.02, 0.01)]:
+        J = np.zeros((3, 3))
+        for j in range(3):
+            cp, cm = list(c), list(c)
+            cp[j] += 1e-6
+            cm[j] -= 1e-6
+            J[:, j] = (np.array(odict.cu_to_ho(cp)) - np.array(odict.cu_to_ho(cm))) / 2e-6
+        assert abs(np.linalg.det(J) - 1) < 1e-6
+    q = odict.from_homochoric((0.3, 0.4, 0.5))
+    th = 2 * math.acos(q[0])
+    assert abs(0.75 * (th - math.sin(th)) - math.sqrt(0.5) ** 3) < 1e-12
+
+
+def test_generators_match_published_vectors():
+    """SplitMix64 from seed 0 and xoshiro256++ from the state (1, 2, 3, 4): the published first
+    outputs of Vigna's reference implementations."""
+    import oracle.dictionary as odict
+
+    g = odict.SplitMix64(0)
+    assert [g.next() for _ in range(3)] == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F]
+    x = odict.Xoshiro256(0)
+    x.s = [1, 2, 3, 4]
+    assert [x.next() for _ in range(4)] == [41943041, 58720359, 3588806011781223, 3591011842654386]
+
+
+def test_dictionary_grid_equals_its_restatement():
+    """The package's vectorized dictionary (grid, zone, shuffle) is the oracle's entry for entry."""
+    import oracle.dictionary as odict
+    from zebsdsolve_b200 import dictionary as DI
+    from zebsdsolve_b200 import rotations as R
+
+    for g in ("o", "d6"):
+        rots = R.group(g)
+        for N in (3, 7):
+            a = odict.dictionary(N, rots)
+            b = DI.cubochoric_grid(N, rots)
+            assert a.shape == b.shape and np.array_equal(a, b), (g, N)

@@ -174,9 +174,11 @@ class Solver:
 
     def index_cells(self, cells, method=None, bandwidth=None, dict_grid=None):
         c = np.asarray(cells, np.int64).reshape(-1)
-        if method not in (None, "spherical"):
-            raise Error(f"index_cells: method {method!r} is not on this engine's path")
-        r = self._call("index_cells", self._e.index_cells, c, bandwidth)
+        st = self._e.set
+        method = method if method is not None else st["method"]
+        if method not in ("spherical", "dictionary", "pca"):
+            raise Error(f"index_cells: unknown method {method!r}")
+        r = self._call("index_cells", self._e.index_cells, c, bandwidth, method, dict_grid)
         return {"quaternions": r[..., :4].copy(), "ncc": r[..., 4].copy(), "nmi": r[..., 5].copy(),
                 "step": r[..., 6].copy(), "z": r[..., 7].copy()}
 

@@ -15,6 +15,7 @@ import numpy as np
 import torch
 
 from . import _native as N
+from . import dictionary as DI
 from .reduce import reduce_image
 from . import master as M
 from . import rotations as R
@@ -128,6 +129,7 @@ class Engine:
         self._buf = {}
         self._batch_t = None  # bounding box of the last batch's detector positions
         self._spans = {}
+        self.dicts = {}  # (phase, grid) → dictionary.Dictionary
         self._pinned = None
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
@@ -266,6 +268,7 @@ class Engine:
     def clear_phases(self):
         self.phases = []
         self.bands = {}
+        self.dicts = {}
         self.chance_key = None
 
     def pixel_angle(self):
@@ -412,13 +415,48 @@ class Engine:
         self.upload_raw(cells, raw, torch.cuda.current_stream())
         return self.preprocess(raw, n)
 
-    def prepare(self, bandwidth=None):
-        """Everything a batch needs besides its patterns: tables, chance calibration, denominators."""
+    def prepare(self, bandwidth=None, method="spherical", grid=None):
+        """Everything a batch needs besides its patterns: tables, chance calibration, denominators
+        (spherical), or each phase's dictionary (its simulated entries or components)."""
+        if method != "spherical":
+            self.prepare_masters()
+            for pi in range(len(self.phases)):
+                self.dictionary(pi, int(grid or self.set["dict_grid"]), method)
+            self.calibrate()
+            return None
         L = int(bandwidth or self.set["bandwidth"])
         b = self.band(L)
         self.calibrate()
         self.denominators(b, self.frame())
         return b
+
+    def dictionary(self, pi, grid, method):
+        """engine.zig:1851-1955 — phase pi's dictionary of this grid, simulated at the map's
+        reference position (method "dictionary") or learned as components ("pca"); kept until the
+        master, the geometry, the grid or the settings change."""
+        p = self.phases[pi]
+        d = self.dicts.get((pi, grid))
+        if d is None:
+            q = DI.cubochoric_grid(grid, p.master.rotations())
+            d = DI.Dictionary(q, self.dev)
+            self.dicts[(pi, grid)] = d
+            self.log(f"dictionary: {d.n} orientations for the rotations {p.master.setting.rotation} (grid {grid})")
+        rows, cols, h, w = self.info()
+        bn = self.set["binning"]
+        t = self.geo.translation(h / bn, w / bn).astype(np.float32)
+        fr = self.frame()
+        s = self.set
+        key = (method, id(p.baked[1]), tuple(fr.c0), tuple(fr.c1), tuple(fr.c2), fr.h, fr.w, tuple(fr.mask),
+               tuple(t), s["pca_components"] if method == "pca" else 0, s["pca_epochs"] if method == "pca" else 0)
+        if d.key != key:
+            _, sheets, grad, vpair, gpair = p.baked
+            d.key, d.panel = None, None
+            if method == "pca":
+                d.prepare_pca(fr, vpair, p.master.side, t, s["pca_components"], s["pca_epochs"], self.log)
+            else:
+                d.prepare_sims(fr, vpair, p.master.side, t)
+            d.key = key
+        return d
 
     def items_of(self, cells):
         cells = np.asarray(cells, np.int64)
@@ -448,9 +486,11 @@ class Engine:
         self._spans[key] = sp
         return sp
 
-    def run_device(self, raw, cells, bandwidth=None, timer=None):
+    def run_device(self, raw, cells, bandwidth=None, timer=None, method="spherical", grid=None):
         """One pass of the device path over n = len(cells) stored patterns already on the device:
         records [phase][cell][8] as a device tensor (engine.zig:2005-2122, no readback)."""
+        if method != "spherical":
+            return self.run_device_dictionary(raw, cells, method, int(grid or self.set["dict_grid"]), timer)
         n = len(cells)
         n_ph = len(self.phases)
         s = self.set
@@ -486,6 +526,36 @@ class Engine:
                 mark("peaks")
                 N.call("zeb_correlate_peaks", ptr(U), nt, ctypes.byref(ph.dims), ptr(bt.tw), ptr(ph.rden), 1 << 30,
                        ptr(peaks[t0 * 8:]), ptr(cand), stream_ptr())
+            _, sheets, grad, vpair, gpair = p.baked
+            mark("refine")
+            N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(vpair), ptr(gpair),
+                   p.master.side, ctypes.byref(opts), ptr(recs[pi * n * 8:]), stream_ptr())
+        mark("end")
+        return recs[: n_ph * n * 8].view(n_ph, n, 8)
+
+    def run_device_dictionary(self, raw, cells, method, grid, timer=None):
+        """run_device with a dictionary search (engine.zig:2094-2112): each pattern's best entry
+        (by its pixels, or by its coefficients on the components) seeds the refinement."""
+        n = len(cells)
+        n_ph = len(self.phases)
+        s = self.set
+        self.prepare(None, method, grid)
+        fr = self.frame()
+        mark = timer.mark if timer is not None else (lambda name: None)
+        mark("prep")
+        pats = self.preprocess(raw, n)
+        items = self.items_of(cells)
+        self.batch_stamp = self.batch_stamp % (1 << 24) + 1
+        recs = self.buf("recs", n_ph * n * 8)
+        opts = N.RefineOpts(s["refine_iters"] if s["refine"] else 0, math.radians(s["refine_step"]), 1.0, 0.02, 1e4,
+                            s["nmi_bins"], float(self.batch_stamp))
+        x = pats[: n * fr.h * fr.w].view(n, fr.h * fr.w)
+        tc = s["precision"] != "f32"
+        for pi, p in enumerate(self.phases):
+            d = self.dictionary(pi, grid, method)
+            mark("match")
+            xs = x @ d.W.T if method == "pca" else x  # the patterns' coefficients (pca.zig:159-162)
+            peaks = d.seeds(xs.contiguous(), tc, self.tc_status(), self.buf("peaks", n * 8))
             _, sheets, grad, vpair, gpair = p.baked
             mark("refine")
             N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(vpair), ptr(gpair),
@@ -560,7 +630,7 @@ class Engine:
             N.call("zeb_records_fz", ptr(recs[pi]), n, ptr(ops), ops.shape[0], ptr(fz[pi]), stream_ptr())
         return fz
 
-    def index_cells(self, cells, bandwidth=None):
+    def index_cells(self, cells, bandwidth=None, method="spherical", grid=None):
         """engine.zig:1990-2137 — index the given cells against every phase: records
         [phase][cell][8] = (q, NCC, NMI, last improving step, z)."""
         cells = np.asarray(cells, np.int64)
@@ -570,11 +640,11 @@ class Engine:
             raise EngineError("NoPhases")
         if n == 0:
             return np.zeros((n_ph, 0, 8), np.float32)
-        self.prepare(bandwidth)
+        self.prepare(bandwidth, method, grid)
         rows, cols, h, w = self.info()
         raw = self.buf("raw_up", n * h * w, self.pinned().dtype).view(-1)[: n * h * w].view(n, h, w)
         self.upload_raw(cells, raw, torch.cuda.current_stream())
-        recs = self.run_device(raw, cells, bandwidth)
+        recs = self.run_device(raw, cells, bandwidth, method=method, grid=grid)
         self._last_fz = self.fz_of(recs).cpu().numpy()
         out = recs.cpu().numpy()
         self.check_device()
@@ -584,7 +654,7 @@ class Engine:
         """Patterns per device pass of a pipelined run."""
         return 16384
 
-    def index_pipelined(self, cells, bandwidth, on_batch, keep_going=lambda: True):
+    def index_pipelined(self, cells, bandwidth, on_batch, keep_going=lambda: True, method="spherical", grid=None):
         """engine.zig:1990-2137 over many cells at once: device passes of device_batch() cells,
         each pass's upload (a copy stream, from the pinned scan) overlapping the previous pass's
         kernels, its records read back asynchronously and handed to on_batch(cells, records, fz) on
@@ -595,7 +665,7 @@ class Engine:
             raise EngineError("NoPhases")
         if len(cells) == 0:
             return
-        self.prepare(bandwidth)
+        self.prepare(bandwidth, method, grid)
         rows, cols, h, w = self.info()
         B = min(self.device_batch(), len(cells))
         pin = self.pinned()
@@ -638,7 +708,7 @@ class Engine:
                 issue_upload(i + 1)
             comp.wait_event(up_done[k])
             cb = parts[i]
-            recs = self.run_device(raw[k][: len(cb)], cb, bandwidth)
+            recs = self.run_device(raw[k][: len(cb)], cb, bandwidth, method=method, grid=grid)
             ev = torch.cuda.Event()
             ev.record(comp)
             comp_done[k] = ev
@@ -783,10 +853,8 @@ class Engine:
         batch = max(s["batch"], 1)
         n = min(left, batch * min(max(4096 // batch, 2), 16))
         cells = cells_all[self.index_done:self.index_done + n]
-        bw, _, method = s.sweep(self.index_sweep)
-        if method != "spherical":
-            raise EngineError(f"method {method!r}: not supported on this engine yet")
-        recs = self.index_cells(cells, bw)
+        bw, dg, method = s.sweep(self.index_sweep)
+        recs = self.index_cells(cells, bw, method, dg)
         self.land(cells, recs, self._last_fz)
         self.next_sweep(bw)
         return len(self.index_cells_list) - self.index_done
@@ -797,7 +865,10 @@ class Engine:
         cells_all = self.index_cells_list
         if self.index_done == len(cells_all) and self.index_sweep + 1 < s["sweeps"]:
             keep = cells_all[self.res["sweep"][cells_all] < 0]
-            self.log(f"sweep {self.index_sweep + 1} of {s['sweeps']} (spherical, bandwidth {bw}): "
+            _, dg, method = s.sweep(self.index_sweep)
+            what = {"spherical": f"spherical, bandwidth {bw}", "dictionary": f"dictionary, grid {dg}",
+                    "pca": f"dictionary components, grid {dg}"}[method]
+            self.log(f"sweep {self.index_sweep + 1} of {s['sweeps']} ({what}): "
                      f"{len(cells_all) - len(keep)} of {len(cells_all)} patterns accepted, {len(keep)} left")
             if len(keep):
                 self.index_cells_list = keep
@@ -810,9 +881,7 @@ class Engine:
         index_step calls, with uploads, kernels, readbacks and landing overlapped."""
         s = self.set
         while len(self.index_cells_list) - self.index_done > 0 and not self.cancel:
-            bw, _, method = s.sweep(self.index_sweep)
-            if method != "spherical":
-                raise EngineError(f"method {method!r}: not supported on this engine yet")
+            bw, dg, method = s.sweep(self.index_sweep)
             stop = [False]
 
             def on_batch(cb, recs, fz):
@@ -821,7 +890,7 @@ class Engine:
                     stop[0] = True
 
             self.index_pipelined(self.index_cells_list[self.index_done:], bw, on_batch,
-                                 keep_going=lambda: not (stop[0] or self.cancel))
+                                 keep_going=lambda: not (stop[0] or self.cancel), method=method, grid=dg)
             if stop[0]:
                 return
             self.next_sweep(bw)
