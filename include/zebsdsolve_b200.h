@@ -288,10 +288,11 @@ size_t zeb_panel_bytes(int rows, int cols);
 /* FP32 rows (src[r·ld + k]) rounded to BF16 into a panel; padding rows and columns are zero. */
 int zeb_pack_panel(const float* src, int rows, int cols, int ld, void* panel, void* stream);
 
-/* How many dictionary slices the match kernels split the entries into for n_exp patterns (form 0:
- * FP32, 1: BF16 tensor cores): the candidate buffers hold n_exp × slices (FP32) or
- * n_exp × slices × 8 (BF16) entries. */
-int zeb_match_slices(int n_exp, int n_dict, int form);
+/* How many dictionary slices the match kernels split the entries into for n_exp patterns of cols
+ * values (form 0: FP32, 1: BF16 tensor cores): enough CTAs to fill the GPU, and bands of the
+ * dictionary small enough to stay in L2 while the pattern tiles stream them. The candidate
+ * buffers hold n_exp × slices (FP32) or n_exp × slices × 8 (BF16) entries. */
+int zeb_match_slices(int n_exp, int n_dict, int cols, int form);
 
 /* Per pattern and dictionary slice the eight largest inner products of the pattern's panel row
  * with the dictionary's panel rows (BF16 operands, FP32 accumulation on the tensor cores),

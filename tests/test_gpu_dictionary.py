@@ -115,7 +115,7 @@ def test_tensor_core_top8_matches_a_bf16_reference(world):
     nd = d.shape[0]
     assert nd % 256 and K % 64  # ragged in both
     xp, dp = DI.panel(x), DI.panel(d)
-    sl = Nn.load().zeb_match_slices(n, nd, 1)
+    sl = Nn.load().zeb_match_slices(n, nd, K, 1)
     cv = torch.empty(n * sl * 8, device="cuda")
     ci = torch.empty(n * sl * 8, dtype=torch.int32, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -154,7 +154,7 @@ def test_fp32_match_picks_the_oracles_best(world):
     x, d, qd = _dictionary_rows(world, 9, 3.0)
     n, K = x.shape
     nd = d.shape[0]
-    sl = Nn.load().zeb_match_slices(n, nd, 0)
+    sl = Nn.load().zeb_match_slices(n, nd, K, 0)
     cv = torch.empty(n * sl, device="cuda")
     ci = torch.empty(n * sl, dtype=torch.int32, device="cuda")
     Nn.call("zeb_match_f32", P(x), n, P(d), nd, K, sl, P(cv), P(ci), sp())

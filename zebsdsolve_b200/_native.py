@@ -81,7 +81,7 @@ _SIGS = {
     "zeb_panel_bytes": ([c_int, c_int], c_size_t),
     "zeb_pack_panel": ([P, c_int, c_int, c_int, P, P], c_int),
     "zeb_dict_sims": ([ctypes.POINTER(Frame), P, c_int, P, P, c_int, P, P], c_int),
-    "zeb_match_slices": ([c_int, c_int, c_int], c_int),
+    "zeb_match_slices": ([c_int, c_int, c_int, c_int], c_int),
     "zeb_match_bf16": ([P, c_int, P, c_int, c_int, c_int, P, P, P, P], c_int),
     "zeb_match_f32": ([P, c_int, P, c_int, c_int, c_int, P, P, P], c_int),
     "zeb_match_best": ([P, c_int, P, c_int, c_int, P, c_int, P, P, P], c_int),

@@ -29,7 +29,8 @@ constexpr int MT_BN = 256;               // dictionary entries per tile (MMA N)
 constexpr int MT_A_BLOCK = MT_BM * 128;  // 16 KB
 constexpr int MT_B_BLOCK = MT_BN * 128;  // 32 KB
 constexpr int MT_STAGES = 4;
-constexpr int MT_THREADS = 192;
+constexpr int MT_EPI = 8;                          // epilogue warps: two per TMEM lane quadrant
+constexpr int MT_THREADS = 64 + 32 * MT_EPI;       // + the copy warp and the MMA warp
 constexpr int MT_TOP = 8;
 
 __host__ __device__ inline int panel_rows(int rows) { return (rows + 255) / 256 * 256; }
@@ -137,22 +138,42 @@ struct MatchArgs {
 struct MatchShared {
   uint8_t a[MT_STAGES][MT_A_BLOCK];
   uint8_t b[MT_STAGES][MT_B_BLOCK];
+  float stash[32][32 * MT_EPI];  // a chunk of each epilogue thread's scores, [column][thread]
   uint64_t full[MT_STAGES], empty[MT_STAGES], acc_full[2], acc_empty[2], mma_done;
   uint32_t tmem;
 };
 
-// insert (x, i) into the descending list (v, id) of eight; equal scores keep the earlier entry first
+// (x, i) before (y, j): the larger score first, equal scores in index order
+__device__ __forceinline__ bool top8_before(float x, int i, float y, int j) { return x > y || (x == y && i < j); }
+
+// insert (x, i) into the list (v, id) of eight kept in that order
 __device__ __forceinline__ void top8_insert(float (&v)[MT_TOP], int (&id)[MT_TOP], float x, int i) {
-  if (!(x > v[MT_TOP - 1])) return;
+  if (!top8_before(x, i, v[MT_TOP - 1], id[MT_TOP - 1])) return;
   v[MT_TOP - 1] = x;
   id[MT_TOP - 1] = i;
 #pragma unroll
   for (int k = MT_TOP - 1; k > 0; --k) {
-    if (v[k] > v[k - 1]) {
+    if (top8_before(v[k], id[k], v[k - 1], id[k - 1])) {
       const float tv = v[k]; v[k] = v[k - 1]; v[k - 1] = tv;
       const int ti = id[k]; id[k] = id[k - 1]; id[k - 1] = ti;
     }
   }
+}
+
+// push (x, i) into the descending list when it beats the last entry (equal scores keep the
+// entry already there, which came first): every slot's new content from the comparisons with
+// the old list at once, no chain of dependent swaps
+__device__ __forceinline__ void top8_push(float (&v)[MT_TOP], int (&id)[MT_TOP], float x, int i) {
+  bool gt[MT_TOP];
+#pragma unroll
+  for (int k = 0; k < MT_TOP; ++k) gt[k] = x > v[k];
+#pragma unroll
+  for (int k = MT_TOP - 1; k > 0; --k) {
+    v[k] = gt[k - 1] ? v[k - 1] : (gt[k] ? x : v[k]);
+    id[k] = gt[k - 1] ? id[k - 1] : (gt[k] ? i : id[k]);
+  }
+  v[0] = gt[0] ? x : v[0];
+  id[0] = gt[0] ? i : id[0];
 }
 
 __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
@@ -170,7 +191,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&s.acc_full[i], 1);
-      mbar_init(&s.acc_empty[i], 4);
+      mbar_init(&s.acc_empty[i], MT_EPI);
     }
     mbar_init(&s.mma_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -237,44 +258,92 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
       if (!mbar_wait(&s.mma_done, 0, lim)) atomicOr(a.status, 8);
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32·(w mod 4) …; thread = one pattern (row of the tile)
+    // epilogue: warp w may read only TMEM lanes 32·(w mod 4) …, so warps w and w + 4 share a
+    // quadrant and split the 256 columns: thread = one pattern (row of the tile) × one half of
+    // the entries of each tile.  The two halves' lists merge at the end.
     const int ew = warp & 3;
     const int row = ew * 32 + lane;
+    const int half = (warp - 2) >> 2;
+    const int me = half * MT_BM + row;  // this thread's column of the stash
+    const uint32_t lanes = (uint32_t)(ew * 32) << 16;
     float tv[MT_TOP];
     int ti[MT_TOP];
 #pragma unroll
     for (int k = 0; k < MT_TOP; ++k) { tv[k] = -3.4e38f; ti[k] = -1; }
+    // the scores v of entries e0 + j (j < 32; none past the dictionary's end) into the list: a
+    // mask of the scores above the list's last entry first; only those (after the first tiles,
+    // rarely any) go in, one at a time from the thread's own column of the stash (registers
+    // cannot be indexed by a variable)
+    auto take = [&](const uint32_t (&v)[32], int e0) {
+      const int lim_c = min(32, a.n_dict - e0);
+      const float th = tv[MT_TOP - 1];
+      uint32_t mask = 0;
+#pragma unroll
+      for (int c = 0; c < 32; ++c) mask |= (c < lim_c && __uint_as_float(v[c]) > th) ? (1u << c) : 0u;
+      if (mask) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) s.stash[c][me] = __uint_as_float(v[c]);
+        while (mask) {
+          const int c = __ffs(mask) - 1;
+          mask &= mask - 1;
+          top8_push(tv, ti, s.stash[c][me], e0 + c);
+        }
+      }
+    };
     bool ok = true;
     for (int t = 0; t < my_tiles; ++t) {
       const int acc = t & 1;
-      if (!bar_and(1, 128, mbar_wait(&s.acc_full[acc], (t >> 1) & 1, lim))) {
+      // one thread waits for the accumulator (sleeping between polls); the barrier hands the
+      // outcome to the others, which wait there without taking issue slots
+      const bool lead = warp == 2 && lane == 0;
+      if (!bar_and(1, 32 * MT_EPI, lead ? mbar_wait_sleep(&s.acc_full[acc], (t >> 1) & 1, lim) : true)) {
         if (warp == 2 && lane == 0) atomicOr(a.status, 4);
         ok = false;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int e0 = (nt0 + t) * MT_BN;
-#pragma unroll 1
-      for (int c0 = 0; c0 < MT_BN; c0 += 32) {
-        uint32_t v[32];
-        TMEM_LD32(tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(acc * MT_BN + c0), v);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        const int lim_c = min(32, a.n_dict - (e0 + c0));
-#pragma unroll
-        for (int c = 0; c < 32; ++c)
-          if (c < lim_c) top8_insert(tv, ti, __uint_as_float(v[c]), e0 + c0 + c);
-      }
+      const int e0 = (nt0 + t) * MT_BN + half * 128;
+      const uint32_t c0 = tmem + lanes + (uint32_t)(acc * MT_BN + half * 128);
+      // four chunks of 32 columns, the next one's load in flight while one is taken
+      uint32_t va[32], vb[32];
+      TMEM_LD32(c0, va);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      TMEM_LD32(c0 + 32, vb);
+      take(va, e0);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      TMEM_LD32(c0 + 64, va);
+      take(vb, e0 + 32);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      TMEM_LD32(c0 + 96, vb);
+      take(va, e0 + 64);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      // the accumulator is read out: the MMAs of tile t + 2 may start
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&s.acc_empty[acc]);
+      take(vb, e0 + 96);
     }
-    const int p = mt * MT_BM + row;
-    if (ok && p < a.n_exp) {
-      const size_t o = ((size_t)p * a.slices + slice) * MT_TOP;
+    // the second half's list joins the first's (through the stash, once every thread is done)
+    bar_sync(1, 32 * MT_EPI);
+    if (half == 1) {
 #pragma unroll
       for (int k = 0; k < MT_TOP; ++k) {
-        a.cand_v[o + k] = tv[k];
-        a.cand_i[o + k] = ti[k];
+        s.stash[k][row] = tv[k];
+        s.stash[MT_TOP + k][row] = __int_as_float(ti[k]);
+      }
+    }
+    bar_sync(1, 32 * MT_EPI);
+    const int p = mt * MT_BM + row;
+    if (half == 0) {
+#pragma unroll 1
+      for (int k = 0; k < MT_TOP; ++k) top8_insert(tv, ti, s.stash[k][row], __float_as_int(s.stash[MT_TOP + k][row]));
+      if (ok && p < a.n_exp) {
+        const size_t o = ((size_t)p * a.slices + slice) * MT_TOP;
+#pragma unroll
+        for (int k = 0; k < MT_TOP; ++k) {
+          a.cand_v[o + k] = tv[k];
+          a.cand_i[o + k] = ti[k];
+        }
       }
     }
   }
@@ -451,13 +520,20 @@ extern "C" int zeb_dict_sims(const zeb_frame_t* fr, const float* vpair, int side
   return zeb_launch_check("dict_sims");
 }
 
-extern "C" int zeb_match_slices(int n_exp, int n_dict, int form) {
-  if (n_exp <= 0 || n_dict <= 0) return 1;
+extern "C" int zeb_match_slices(int n_exp, int n_dict, int cols, int form) {
+  if (n_exp <= 0 || n_dict <= 0 || cols <= 0) return 1;
   const int sms = sm_count();
   const int mtiles = form ? (n_exp + MT_BM - 1) / MT_BM : (n_exp + MF_BM - 1) / MF_BM;
   const int ntiles = form ? (n_dict + MT_BN - 1) / MT_BN : (n_dict + MF_BN - 1) / MF_BN;
   const int want = form ? sms : 4 * sms;  // resident CTAs: one per SM (tensor cores), about four (FP32)
-  int slices = std::min(ntiles, std::max(1, (want + mtiles - 1) / mtiles));
+  int slices = std::max(1, (want + mtiles - 1) / mtiles);
+  // a slice is a band of the dictionary that every pattern tile reads in turn (the pattern tiles
+  // run fastest in the grid): at most ~48 MB of it, so that the band stays in L2 while a wave of
+  // CTAs streams it
+  const long long tile_bytes = form ? (long long)panel_kblocks(cols) * MT_B_BLOCK : (long long)MF_BN * cols * 4;
+  const long long band = 48LL << 20;
+  slices = std::max<long long>(slices, ((long long)ntiles * tile_bytes + band - 1) / band);
+  slices = std::min(ntiles, slices);
   const int per = (ntiles + slices - 1) / slices;
   return (ntiles + per - 1) / per;
 }

@@ -295,7 +295,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
     for (int mt = 0; mt < mtiles; ++mt) {
       const int acc = mt & 1;
       // the four warps agree on the outcome (a barrier that ANDs their results)
-      if (!bar_and(1, 128, mbar_wait(&s.acc_full[acc], (mt >> 1) & 1, lim))) {
+      // one thread waits for the accumulator (sleeping between polls); the barrier hands the
+      // outcome to the others, which wait there without taking issue slots
+      if (!bar_and(1, 128, leader ? mbar_wait_sleep(&s.acc_full[acc], (mt >> 1) & 1, lim) : true)) {
         if (leader) {
           atomicOr(a.status, 4);
           s.failed = 1;

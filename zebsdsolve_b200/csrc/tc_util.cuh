@@ -63,6 +63,21 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
   }
 }
 
+// the same for a thread that may wait long (an epilogue waiting for its accumulator): it backs
+// off with nanosleep between polls, so that it takes no issue slots from the warps that feed the
+// tensor cores
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, long long limit_ns) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  uint32_t ns = 32;
+  for (;;) {
+    __nanosleep(ns);
+    if (mbar_try(bar, parity)) return true;
+    if (ns < 512) ns <<= 1;
+    if ((long long)(global_ns() - t0) > limit_ns) return false;
+  }
+}
+
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_addr(dst)),

@@ -270,14 +270,14 @@ class Dictionary:
             if self.panel is None:
                 self.panel = panel(self.rows)
             xp = panel(x)
-            sl = N.load().zeb_match_slices(n, self.n, 1)
+            sl = N.load().zeb_match_slices(n, self.n, K, 1)
             cv = torch.empty(n * sl * 8, dtype=torch.float32, device=dev)
             ci = torch.empty(n * sl * 8, dtype=torch.int32, device=dev)
             N.call("zeb_match_bf16", ptr(xp), n, ptr(self.panel), self.n, K, sl, ptr(cv), ptr(ci), ptr(status),
                    stream_ptr())
             nc = sl * 8
         else:
-            sl = N.load().zeb_match_slices(n, self.n, 0)
+            sl = N.load().zeb_match_slices(n, self.n, K, 0)
             cv = torch.empty(n * sl, dtype=torch.float32, device=dev)
             ci = torch.empty(n * sl, dtype=torch.int32, device=dev)
             N.call("zeb_match_f32", ptr(x), n, ptr(self.rows), self.n, K, sl, ptr(cv), ptr(ci), stream_ptr())
