@@ -274,38 +274,45 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
 }
 
 
-// The direct blur with the image, its zero-padded rows P[h][w + 2R] and the zero-padded row-blurred
-// image Q[h + 2R][w] all in shared memory: each thread takes four rows of one column, so every tap
-// is one broadcast tap load, four conflict-free loads and four FMAs, with no bounds tests; the
-// taps inside the image are summed once per column (rows), the sums in the order of k_prep, so
-// the results are the same bits.
+// The direct blur in shared memory: the image inside its zero-padded rows P[h][pw] (R zeros on
+// the left, at least R + 14 on the right, pw odd so that rows at stride pw fall in different
+// banks) and the zero-padded row-blurred image Q[R + h + R + 16][w].  A thread takes eight
+// consecutive outputs along the blur's direction and walks the taps eight at a time: eight taps
+// and the fifteen inputs they reach go into registers, then 64 FMAs, so a shared load serves
+// several FMAs (the taps beyond 2R are zeros, adding exact zeros).  Each output sums its taps in
+// increasing order with fmaf, the order of k_prep, so the results are the same bits; the taps
+// inside the image are summed once per column and per row for the edge renormalization.
+constexpr int PD_OUT = 8;
+
+__host__ __device__ inline int pd_pw(int w, int R) { return ((w + 2 * R + 2 * PD_OUT) | 1); }
+__host__ __device__ inline int pd_qrows(int h, int R) { return h + 2 * R + 2 * PD_OUT; }
+__host__ __device__ inline size_t pd_smem(int h, int w, int R) {
+  return 4 * ((size_t)h * pd_pw(w, R) + (size_t)pd_qrows(h, R) * w);
+}
+
 __global__ void __launch_bounds__(256) k_prep_direct(PrepArgs a) {
   extern __shared__ float sm[];
-  __shared__ float taps[127];
+  __shared__ float taps[128 + PD_OUT];
   __shared__ float gsum[2][512];  // Σ taps inside the image, per column and per row
   __shared__ float red[2 * 8];
   const int b = blockIdx.x;
   const int h = a.h, w = a.w, hw = h * w, R = a.radius;
-  const int pw = w + 2 * R, ph = h + 2 * R;
-  float* img = sm;
-  float* P = img + hw;
-  float* Q = P + h * pw;
+  const int pw = pd_pw(w, R), qr = pd_qrows(h, R);
+  const int ntap = 2 * R + 1, nblk = (ntap + PD_OUT - 1) / PD_OUT;
+  float* P = sm;           // [h][pw], the image at columns R … R + w − 1
+  float* Q = P + h * pw;   // [qr][w], the row-blurred image at rows R … R + h − 1
   const size_t base = (size_t)b * hw;
-  for (int d = threadIdx.x; d <= 2 * R; d += blockDim.x) {
+  for (int d = threadIdx.x; d < nblk * PD_OUT; d += blockDim.x) {
     const int dd = abs(d - R);
-    taps[d] = expf(-(float)(dd * dd) * a.k0);
+    taps[d] = d < ntap ? expf(-(float)(dd * dd) * a.k0) : 0.f;
   }
   for (int i = threadIdx.x; i < h * pw; i += blockDim.x) P[i] = 0.f;
-  for (int i = threadIdx.x; i < R * w; i += blockDim.x) {
-    Q[i] = 0.f;
-    Q[(R + h) * w + i] = 0.f;
-  }
+  for (int i = threadIdx.x; i < R * w; i += blockDim.x) Q[i] = 0.f;
+  for (int i = threadIdx.x; i < (qr - R - h) * w; i += blockDim.x) Q[(R + h) * w + i] = 0.f;
   __syncthreads();
   for (int i = threadIdx.x; i < hw; i += blockDim.x) {
     const int r = i / w, c = i - r * w;
-    const float v = prep_pixel(a, b, i);
-    img[i] = v;
-    P[r * pw + R + c] = v;
+    P[r * pw + R + c] = prep_pixel(a, b, i);
   }
   for (int k = threadIdx.x; k < w + h; k += blockDim.x) {
     const int n = k < w ? w : h, c = k < w ? k : k - w;
@@ -314,47 +321,68 @@ __global__ void __launch_bounds__(256) k_prep_direct(PrepArgs a) {
     gsum[k < w ? 0 : 1][c] = g;
   }
   __syncthreads();
-  // along the rows: Q[R + r][c] = Σ_d taps[d] P[r][c + d] / gsum_col[c]
-  const int rb = (h + 3) / 4;
-  for (int t = threadIdx.x; t < rb * w; t += blockDim.x) {
-    const int r0 = (t / w) * 4, c = t - (t / w) * w;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    const int nk = min(4, h - r0);
-    for (int d = 0; d <= 2 * R; ++d) {
-      const float tv = taps[d];
+  // along the rows: Q[R + r][c] = Σ_d taps[d] P[r][c + d] / gsum_col[c]; a thread takes row r,
+  // columns c0 … c0 + 7 (threads of a warp: consecutive rows)
+  const int cg = (w + PD_OUT - 1) / PD_OUT;
+  for (int t = threadIdx.x; t < cg * h; t += blockDim.x) {
+    const int r = t % h, c0 = (t / h) * PD_OUT;
+    const float* src = P + r * pw + c0;
+    float acc[PD_OUT];
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (k < nk) acc[k] = fmaf(tv, P[(r0 + k) * pw + c + d], acc[k]);
+    for (int k = 0; k < PD_OUT; ++k) acc[k] = 0.f;
+    for (int d0 = 0; d0 < nblk * PD_OUT; d0 += PD_OUT) {
+      float tv[PD_OUT], x[2 * PD_OUT - 1];
+#pragma unroll
+      for (int k = 0; k < PD_OUT; ++k) tv[k] = taps[d0 + k];
+#pragma unroll
+      for (int k = 0; k < 2 * PD_OUT - 1; ++k) x[k] = src[d0 + k];
+#pragma unroll
+      for (int dd = 0; dd < PD_OUT; ++dd)
+#pragma unroll
+        for (int k = 0; k < PD_OUT; ++k) acc[k] = fmaf(tv[dd], x[k + dd], acc[k]);
     }
-    const float g = gsum[0][c];
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (k < nk) Q[(R + r0 + k) * w + c] = acc[k] / g;
+    for (int k = 0; k < PD_OUT; ++k)
+      if (c0 + k < w) Q[(R + r) * w + c0 + k] = acc[k] / gsum[0][c0 + k];
   }
   __syncthreads();
-  // along the columns: the background, combined with the image in place
-  for (int t = threadIdx.x; t < rb * w; t += blockDim.x) {
-    const int r0 = (t / w) * 4, c = t - (t / w) * w;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    const int nk = min(4, h - r0);
-    for (int d = 0; d <= 2 * R; ++d) {
-      const float tv = taps[d];
+  // along the columns: the background, combined with the image in place (P's interior); a thread
+  // takes column c, rows r0 … r0 + 7 (threads of a warp: consecutive columns)
+  const int rg = (h + PD_OUT - 1) / PD_OUT;
+  for (int t = threadIdx.x; t < rg * w; t += blockDim.x) {
+    const int c = t % w, r0 = (t / w) * PD_OUT;
+    const float* src = Q + r0 * w + c;
+    float acc[PD_OUT];
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (k < nk) acc[k] = fmaf(tv, Q[(r0 + k + d) * w + c], acc[k]);
+    for (int k = 0; k < PD_OUT; ++k) acc[k] = 0.f;
+    for (int d0 = 0; d0 < nblk * PD_OUT; d0 += PD_OUT) {
+      float tv[PD_OUT], x[2 * PD_OUT - 1];
+#pragma unroll
+      for (int k = 0; k < PD_OUT; ++k) tv[k] = taps[d0 + k];
+#pragma unroll
+      for (int k = 0; k < 2 * PD_OUT - 1; ++k) x[k] = src[(d0 + k) * w];
+#pragma unroll
+      for (int dd = 0; dd < PD_OUT; ++dd)
+#pragma unroll
+        for (int k = 0; k < PD_OUT; ++k) acc[k] = fmaf(tv[dd], x[k + dd], acc[k]);
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (k < nk) {
-        const int i = (r0 + k) * w + c;
+    for (int k = 0; k < PD_OUT; ++k) {
+      if (r0 + k < h) {
+        float* px = P + (r0 + k) * pw + R + c;
         const float bgv = acc[k] / gsum[1][r0 + k];
-        img[i] = a.dynamic == 1 ? img[i] - bgv : img[i] / fmaxf(bgv, 1e-6f);
+        *px = a.dynamic == 1 ? *px - bgv : *px / fmaxf(bgv, 1e-6f);
       }
     }
   }
   __syncthreads();
-  (void)ph;
-  prep_finish(a, img, a.out + base, red);
+  // the combined image, contiguous, where Q was
+  for (int i = threadIdx.x; i < hw; i += blockDim.x) {
+    const int r = i / w, c = i - r * w;
+    Q[i] = P[r * pw + R + c];
+  }
+  __syncthreads();
+  prep_finish(a, Q, a.out + base, red);
 }
 
 struct WideDims {
@@ -433,8 +461,8 @@ static int prep_launch(const void* raw, int pixel, int n, int src_h, int src_w, 
       a.kz = (float)(1.0 / (2.0 * sf * sf));
     }
   }
-  if (a.dynamic && a.bin < 2 && a.use_smem && h <= 512 && w <= 512) {
-    const size_t dsm = 4 * ((size_t)h * w + (size_t)h * (w + 2 * a.radius) + (size_t)(h + 2 * a.radius) * w);
+  if (a.dynamic && a.bin < 2 && a.use_smem && h <= 512 && w <= 512 && 2 * a.radius + 1 <= 128) {
+    const size_t dsm = pd_smem(h, w, a.radius);
     if (dsm <= 200 * 1024) {
       cudaFuncSetAttribute(k_prep_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
       k_prep_direct<<<n, 256, dsm, (cudaStream_t)stream>>>(a);

@@ -36,6 +36,7 @@ struct SphereArgs {
   int pat_in_smem;
   const int2* spans;  // [n_theta] (first φ sample, count), cyclic; null: every sample
   int ring_major;     // spectra laid out [item][m][ring pair] (else [item][ring pair][m])
+  int leg_items;      // items per k_legendre block (a multiple of 4)
 };
 
 struct Sampler {
@@ -495,37 +496,92 @@ __global__ void k_sphere_spans(SphereArgs a, const float4* __restrict__ ts, int 
 }
 
 // a_lm = Σ_y wplm[y, pair] · (N+S or N−S by the parity of l+m): block (m, tile of 16 items).
-#define LEG_ITEMS 16
-__global__ void __launch_bounds__(256) k_legendre(SphereArgs a) {
+// A block per (order m, group of leg_items items): the group's ring spectra of order m and the
+// table column wplm[y][pair(m, l)] go to shared memory; a thread then takes a tile of 4 items ×
+// 4 degrees l and walks the ring pairs y: per y, four 16-byte spectrum loads (shared by the
+// lanes of an item group) and one 16-byte load of four table entries feed 32 FMAs.  The tile's
+// first degree has l + m even, so its 2nd and 4th degrees take the odd ring combination
+// (N − S) and the others the even one (N + S).  Each coefficient sums over y in increasing order
+// (fmaf), as a thread per coefficient would.
+constexpr int LEG_THREADS = 128;
+
+// asynchronous global → shared copies of 16 or 4 bytes; `bytes` of them read, the rest zero-filled
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+__host__ __device__ inline int leg_nlp(int nl) { return (nl + 3) & ~3; }
+
+__global__ void __launch_bounds__(LEG_THREADS) k_legendre(SphereArgs a) {
   extern __shared__ float4 smem4[];
   const int m = blockIdx.x;
-  const int b0 = blockIdx.y * LEG_ITEMS;
+  const int G = a.leg_items;
+  const int b0 = blockIdx.y * G;
   const int L = a.L, nh = a.n_theta / 2, np = a.n_pairs;
-  const int nl = L - m;
+  const int nl = L - m, nlp = leg_nlp(nl);
   const int p0 = m * L - (m * (m - 1)) / 2;
-  float4* spec = smem4;                        // [LEG_ITEMS][nh]
-  float* wp = (float*)(spec + LEG_ITEMS * nh);  // [nh][nl]
-  const int nb = min(LEG_ITEMS, a.n_items - b0);
-  for (int e = threadIdx.x; e < nb * nh; e += blockDim.x) {
+  float4* spec = smem4;                   // [G][nh]
+  float* wp = (float*)(spec + G * nh);    // [nh][nlp]
+  const int nb = min(G, a.n_items - b0);
+  // both through asynchronous copies (cp.async: no round trip through registers, every copy of
+  // the thread in flight at once); entries past the items or the degrees are zero-filled
+  for (int e = threadIdx.x; e < G * nh; e += blockDim.x) {
     int i = e / nh, y = e - i * nh;
-    spec[e] = a.ring_major ? a.spectra[((size_t)(b0 + i) * L + m) * nh + y] : a.spectra[((size_t)(b0 + i) * nh + y) * L + m];
+    const float4* src = a.spectra;
+    if (i < nb)
+      src += a.ring_major ? ((size_t)(b0 + i) * L + m) * nh + y : ((size_t)(b0 + i) * nh + y) * L + m;
+    cp_async16(spec + e, src, i < nb ? 16 : 0);
   }
-  for (int e = threadIdx.x; e < nh * nl; e += blockDim.x) {
-    int y = e / nl, l = e - y * nl;
-    wp[e] = __ldg(a.wplm + (size_t)y * np + p0 + l);
+  for (int e = threadIdx.x; e < nh * nlp; e += blockDim.x) {
+    int y = e / nlp, l = e - y * nlp;
+    cp_async4(wp + e, a.wplm + (l < nl ? (size_t)y * np + p0 + l : 0), l < nl ? 4 : 0);
   }
+  cp_async_wait_all();
   __syncthreads();
-  for (int e = threadIdx.x; e < nb * nl; e += blockDim.x) {
-    int i = e / nl, li = e - i * nl;
-    bool odd = ((li + 2 * m) & 1) != 0;  // l + m = li + 2m
-    float re = 0.f, im = 0.f;
+  const int nlg = nlp / 4, tiles = (G / 4) * nlg;
+  for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
+    const int lg = t % nlg, ig = t / nlg;
+    float re[4][4], im[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) re[k][j] = im[k][j] = 0.f;
+    const float4* sp = spec + (size_t)ig * 4 * nh;
+    const float* wq = wp + lg * 4;
+#pragma unroll 2
     for (int y = 0; y < nh; ++y) {
-      float4 r = spec[i * nh + y];
-      float k = wp[y * nl + li];
-      re += k * (odd ? r.z : r.x);
-      im += k * (odd ? r.w : r.y);
+      const float4 w4 = *(const float4*)(wq + (size_t)y * nlp);
+      const float wj[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float4 r = sp[k * nh + y];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          re[k][j] = fmaf(wj[j], (j & 1) ? r.z : r.x, re[k][j]);
+          im[k][j] = fmaf(wj[j], (j & 1) ? r.w : r.y, im[k][j]);
+        }
+      }
     }
-    a.alm[(size_t)(b0 + i) * np + p0 + li] = make_float2(re, im);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = ig * 4 + k;
+      if (i >= nb) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int l = lg * 4 + j;
+        if (l < nl) a.alm[(size_t)(b0 + i) * np + p0 + l] = make_float2(re[k][j], im[k][j]);
+      }
+    }
   }
 }
 
@@ -640,11 +696,16 @@ extern "C" int zeb_sphere_coefficients_spans(const float* pats, const float* ite
   }
   if (rc) return rc;
   const int nh = nt / 2;
-  size_t lsm = (size_t)LEG_ITEMS * nh * sizeof(float4) + (size_t)nh * L * sizeof(float);
+  // items per block: 32, or fewer where the spectra and the table column would not fit
+  int G = 32;
+  auto lsm_of = [&](int g) { return (size_t)g * nh * sizeof(float4) + (size_t)nh * leg_nlp(L) * sizeof(float); };
+  while (G > 4 && lsm_of(G) > 96 * 1024) G /= 2;
+  const size_t lsm = lsm_of(G);
   ZEB_REQUIRE(lsm <= 220 * 1024, ZEB_ESIZE, "sphere_coefficients: L=%d needs %zu bytes of shared memory", L, lsm);
+  a.leg_items = G;
   cudaFuncSetAttribute(k_legendre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm);
-  dim3 g(L, (n_items + LEG_ITEMS - 1) / LEG_ITEMS);
-  k_legendre<<<g, 256, lsm, st>>>(a);
+  dim3 g(L, (n_items + G - 1) / G);
+  k_legendre<<<g, LEG_THREADS, lsm, st>>>(a);
   rc = zeb_launch_check("legendre");
   if (rc) return rc;
   k_sh_norm<<<n_items, 256, 0, st>>>(a);
