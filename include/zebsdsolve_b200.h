@@ -314,6 +314,19 @@ int zeb_match_f32(const float* x, int n_exp, const float* d, int n_dict, int col
 int zeb_match_best(const float* x, int n_exp, const float* d, int n_dict, int cols, const int* cand, int n_cand,
                    const float* dict_q, float* seeds, void* stream);
 
+/* The number of pixels of an h × w frame inside its circular mask (all of them without one), and
+ * their list in raster order, list[k] = (row << 16) | col (zeb_mask_pixels entries). Both use the
+ * same test as the kernels (dr² + dc² ≤ r², each product and the sum rounded on its own). */
+int zeb_mask_pixels(const zeb_frame_t* fr);
+int zeb_mask_list(const zeb_frame_t* fr, uint32_t* list, void* stream);
+
+/* zeb_refine over the frame's pixel list (zeb_mask_list, npix = zeb_mask_pixels entries, at most
+ * 25600): a block of 128 threads per item keeps only the pattern's values along the list in shared
+ * memory, so that six items share an SM. The same records as zeb_refine. */
+int zeb_refine_list(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
+                    const zeb_frame_t* fr, const uint32_t* list, int npix, const float* vpair, const float* gpair,
+                    int side, const zeb_refine_opts_t* o, float* records, void* stream);
+
 /* Simulated patterns: the master at q·ray for every pixel of item b (poses[b] = t.xyz, pattern
  * index, q.wxyz): sims[b][h][w]. Replaces Detector.project (src/detector.zig:138-142;
  * shaders/detector.wgsl:254-263). */

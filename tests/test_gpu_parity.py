@@ -426,7 +426,10 @@ def test_records_fz_equals_the_host_reduction(lib, kind):
     assert np.array_equal(fz.cpu().numpy().reshape(-1, 4), want)
 
 
-def test_refine_and_nmi_match_oracle(world, lib):
+@pytest.mark.parametrize("entry", ["zeb_refine", "zeb_refine_list"])
+def test_refine_and_nmi_match_oracle(world, lib, entry):
+    """Both refinement kernels (pixels compacted per block; the frame's shared pixel list, 128
+    threads an item) against the oracle's refinement and NMI."""
     s = world["s"]
     e = s._e
     e.prepare_masters()
@@ -447,8 +450,17 @@ def test_refine_and_nmi_match_oracle(world, lib):
     p = e.phases[0]
     opts = lib.RefineOpts(8, math.radians(2.0), 1.0, 0.02, 1e4, 16, 7.0)
     pd = torch.as_tensor(normed, device="cuda").reshape(-1)
-    lib.call("zeb_refine", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(p.baked[3]), P(p.baked[4]), p.master.side,
-             ctypes.byref(opts), P(recs), sp())
+    if entry == "zeb_refine":
+        lib.call("zeb_refine", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(p.baked[3]), P(p.baked[4]),
+                 p.master.side, ctypes.byref(opts), P(recs), sp())
+    else:
+        npix = lib.load().zeb_mask_pixels(ctypes.byref(fr))
+        lst = torch.empty(npix, dtype=torch.int32, device="cuda")
+        lib.call("zeb_mask_list", ctypes.byref(fr), P(lst), sp())
+        rr, cc = np.nonzero(od.in_mask(fr.h, fr.w, mask))  # raster order
+        assert np.array_equal(lst.cpu().numpy(), (rr << 16) | cc)
+        lib.call("zeb_refine_list", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(lst), npix, P(p.baked[3]),
+                 P(p.baked[4]), p.master.side, ctypes.byref(opts), P(recs), sp())
     got = recs.cpu().numpy().reshape(n, 8)
     grad = od.gradient_table(world["baked"], 151)
     frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))

@@ -34,7 +34,7 @@ static inline int zeb_mask_count(const zeb_frame_t* fr) {
   for (int r = 0; r < fr->h; ++r)
     for (int c = 0; c < fr->w; ++c) {
       const float dr = (float)r - fr->mask[0], dc = (float)c - fr->mask[1];
-      if (fr->mask[2] <= 0.f || dr * dr + dc * dc <= fr->mask[2]) ++cnt;
+      if (::zeb::zeb_in_circle(dr, dc, fr->mask[2])) ++cnt;
     }
   return cnt;
 }

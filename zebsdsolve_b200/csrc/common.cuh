@@ -28,6 +28,18 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
 
 __device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
+// The circular mask's test dr² + dc² ≤ r² (r² ≤ 0: no mask) with every product and the sum rounded
+// on its own (no fused multiply-add), on the device as on the host, so that both count the same
+// pixels (a boundary pixel must not be in one list and not the other).
+__host__ __device__ __forceinline__ bool zeb_in_circle(float dr, float dc, float r2) {
+#ifdef __CUDA_ARCH__
+  return r2 <= 0.f || __fadd_rn(__fmul_rn(dr, dr), __fmul_rn(dc, dc)) <= r2;
+#else
+  const volatile float a = dr * dr, b = dc * dc;
+  return r2 <= 0.f || (float)(a + b) <= r2;
+#endif
+}
+
 // q v q*
 __device__ __forceinline__ float3 qrot(float4 q, float3 v) {
   float3 u = make_float3(q.y, q.z, q.w);

@@ -33,7 +33,7 @@ struct DetArgs {
 
 __device__ __forceinline__ bool in_mask(const DetArgs& a, int row, int col) {
   float dr = (float)row - a.mask[0], dc = (float)col - a.mask[1];
-  return a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2];
+  return zeb_in_circle(dr, dc, a.mask[2]);
 }
 
 __device__ __forceinline__ float3 ray_dir(const DetArgs& a, float3 t, int row, int col) {
@@ -532,6 +532,179 @@ static size_t det_smem(DetArgs& a) {
   return (a.pat_smem ? hw * 4 : 0) + (a.sim_smem ? hw * 4 : 0);
 }
 
+// ── the refinement over a precomputed pixel list ──
+//
+// The frame's masked pixels, in raster order, come as one list shared by every item (packed
+// (row << 16) | col, zeb_mask_list); a block of 128 threads per item keeps only the pattern's
+// values along the list in shared memory (4 bytes a pixel, 8 with NMI's simulated values), so
+// that six items share an SM and one item's serial phase (the reduction and thread 0's step)
+// overlaps the others' pixel passes.  Each pass recomputes the detector ray of every pixel (nine
+// FMAs and a reciprocal square root) instead of keeping it; the sums per pixel are those of
+// k_refine.
+constexpr int RL_THREADS = 128;
+
+__device__ __forceinline__ float3 list_ray(const DetArgs& a, float3 t, uint32_t v) {
+  return ray_dir(a, t, (int)(v >> 16), (int)(v & 0xffffu));
+}
+
+// the NMI over the list (detector.wgsl:744-832); sims (shared, npix floats) keeps the simulated
+// values of the first pass for the histogram pass
+__device__ float nmi_list(const DetArgs& a, const uint32_t* __restrict__ list, const float* pv, float* sims,
+                          int npix, float3 t, float4 q, int nbins, uint32_t* hist, float* red) {
+  float ext[4] = {3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f};
+  for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    const float e = pv[k];
+    const float sv = master_at_pair(a.vpair, qrot(q, list_ray(a, t, __ldg(list + k))), a.side);
+    sims[k] = sv;
+    ext[0] = fminf(ext[0], e); ext[1] = fmaxf(ext[1], e);
+    ext[2] = fminf(ext[2], sv); ext[3] = fmaxf(ext[3], sv);
+  }
+  for (int i = threadIdx.x; i < nbins * nbins; i += blockDim.x) hist[i] = 0u;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ext[0] = fminf(ext[0], __shfl_xor_sync(0xffffffffu, ext[0], o));
+    ext[1] = fmaxf(ext[1], __shfl_xor_sync(0xffffffffu, ext[1], o));
+    ext[2] = fminf(ext[2], __shfl_xor_sync(0xffffffffu, ext[2], o));
+    ext[3] = fmaxf(ext[3], __shfl_xor_sync(0xffffffffu, ext[3], o));
+  }
+  if (lane == 0)
+    for (int k = 0; k < 4; ++k) red[k * nw + wid] = ext[k];
+  __syncthreads();
+  float r[4] = {3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f};
+  for (int w = 0; w < nw; ++w) {
+    r[0] = fminf(r[0], red[0 * nw + w]); r[1] = fmaxf(r[1], red[1 * nw + w]);
+    r[2] = fminf(r[2], red[2 * nw + w]); r[3] = fmaxf(r[3], red[3 * nw + w]);
+  }
+  __syncthreads();
+  const float ke = (float)nbins / fmaxf(r[1] - r[0], 1e-20f);
+  const float ks = (float)nbins / fmaxf(r[3] - r[2], 1e-20f);
+  for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    const uint32_t be = min((uint32_t)((pv[k] - r[0]) * ke), (uint32_t)(nbins - 1));
+    const uint32_t bs = min((uint32_t)((sims[k] - r[2]) * ks), (uint32_t)(nbins - 1));
+    atomicAdd(&hist[be * nbins + bs], 1u);
+  }
+  __syncthreads();
+  float acc[3] = {0.f, 0.f, 0.f};  // −Σ c log c (joint), −Σ (marginals), N
+  for (int i = threadIdx.x; i < nbins * nbins; i += blockDim.x) {
+    float c = (float)hist[i];
+    acc[2] += c;
+    if (c > 0.f) acc[0] -= c * logf(c);
+  }
+  if ((int)threadIdx.x < nbins) {
+    float rs = 0.f, cs = 0.f;
+    for (int k = 0; k < nbins; ++k) {
+      rs += (float)hist[threadIdx.x * nbins + k];
+      cs += (float)hist[k * nbins + threadIdx.x];
+    }
+    if (rs > 0.f) acc[1] -= rs * logf(rs);
+    if (cs > 0.f) acc[1] -= cs * logf(cs);
+  }
+  block_sums<3>(acc, red);
+  const float nn = fmaxf(acc[2], 1.f);
+  const float h_joint = logf(nn) + acc[0] / nn;
+  const float h_marg = 2.f * logf(nn) + acc[1] / nn;
+  return h_marg > 1e-12f ? 2.f * (h_marg - h_joint) / h_marg : 0.f;
+}
+
+__global__ void __launch_bounds__(RL_THREADS, 6) k_refine_list(DetArgs a, const uint32_t* __restrict__ list,
+                                                                 int npix) {
+  extern __shared__ float pv[];  // [npix] pattern values, then [npix] simulated values (NMI)
+  __shared__ float red[20 * (RL_THREADS / 32)];
+  __shared__ uint32_t hist[32 * 32];
+  __shared__ float4 sh_q;
+  const int b = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  constexpr int NW = RL_THREADS / 32;
+  const float4 it = a.items[b];
+  const float3 t = make_float3(it.x, it.y, it.z);
+  const float* gpat = a.pats + (size_t)(int)it.w * a.h * a.w;
+  for (int k = threadIdx.x; k < npix; k += RL_THREADS) {
+    const uint32_t v = __ldg(list + k);
+    pv[k] = __ldg(gpat + (int)(v >> 16) * a.w + (int)(v & 0xffffu));
+  }
+  // refinement state (thread 0's registers): detector.wgsl:73-77
+  const float* sd0 = a.seeds + (size_t)b * a.seed_stride;
+  float4 q_best = make_float4(sd0[0], sd0[1], sd0[2], sd0[3]);
+  float best = -2.f, mu = a.o.scale0, g_best[3] = {0.f, 0.f, 0.f}, h_best[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float last_good = 0.f, promised = 0.f, step_len = 0.f, accepted = 0.f;
+  if (threadIdx.x == 0) sh_q = q_best;
+  __syncthreads();
+
+  for (int iter = 0; iter <= a.o.iters; ++iter) {
+    const float4 q = sh_q;
+    float s[19];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) s[k] = 0.f;
+    for (int k = threadIdx.x; k < npix; k += RL_THREADS) {
+      const float3 c = qrot(q, list_ray(a, t, __ldg(list + k)));
+      const float4 m = grad_at_pair(a.gpair, c, a.side);
+      const float3 d = cross3(c, make_float3(m.x, m.y, m.z));
+      const float e = pv[k];
+      s[1] += m.w; s[2] += m.w * m.w; s[3] += m.w * e;
+      s[4] += d.x; s[5] += d.y; s[6] += d.z;
+      s[7] += m.w * d.x; s[8] += m.w * d.y; s[9] += m.w * d.z;
+      s[10] += e * d.x; s[11] += e * d.y; s[12] += e * d.z;
+      s[13] += d.x * d.x; s[14] += d.y * d.y; s[15] += d.z * d.z;
+      s[16] += d.x * d.y; s[17] += d.x * d.z; s[18] += d.y * d.z;
+    }
+    // each warp's sums, then warp 0 alone adds the warps' (lane k: sum k) and takes the step
+#pragma unroll
+    for (int k = 1; k < 19; ++k) {
+      const float w = warp_sum(s[k]);
+      if (lane == 0) red[k * NW + wid] = w;
+    }
+    __syncthreads();
+    if (wid == 0) {
+      float tot = 0.f;
+      if (lane >= 1 && lane < 19)
+#pragma unroll
+        for (int w = 0; w < NW; ++w) tot += red[lane * NW + w];
+#pragma unroll
+      for (int k = 1; k < 19; ++k) s[k] = __shfl_sync(0xffffffffu, tot, k);
+      s[0] = (float)npix;
+      if (lane == 0) {
+        float4 qn = q_best;
+        refine_step(a.o, iter, q, s, best, mu, g_best, h_best, last_good, promised, step_len, accepted, q_best, qn);
+        sh_q = qn;
+      }
+    }
+    __syncthreads();
+  }
+  const float4 qf = sh_q;
+  const float v = nmi_list(a, list, pv, pv + npix, npix, t, qf, a.o.nmi_bins, hist, red);
+  if (threadIdx.x == 0) {
+    float* r = a.records + (size_t)b * 8;
+    r[0] = qf.x; r[1] = qf.y; r[2] = qf.z; r[3] = qf.w;
+    r[4] = best; r[5] = v; r[6] = last_good; r[7] = a.o.stamp;
+  }
+}
+
+// the frame's masked pixels in raster order, (row << 16) | col: one block, a chunk of 256 pixels
+// at a time (ballots and a running count keep the order)
+__global__ void k_mask_list(DetArgs a, uint32_t* __restrict__ list) {
+  __shared__ int wcnt[8];
+  const int hw = a.h * a.w;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int out = 0;
+  for (int base = 0; base < hw; base += 256) {
+    const int i = base + threadIdx.x;
+    const int row = i / a.w, col = i - row * a.w;
+    const bool m = i < hw && in_mask(a, row, col);
+    const unsigned bal = __ballot_sync(0xffffffffu, m);
+    if (lane == 0) wcnt[wid] = __popc(bal);
+    __syncthreads();
+    int off = out, tot = 0;
+    for (int w = 0; w < 8; ++w) {
+      if (w < wid) off += wcnt[w];
+      tot += wcnt[w];
+    }
+    if (m) list[off + __popc(bal & ((1u << lane) - 1u))] = ((uint32_t)row << 16) | (uint32_t)col;
+    out += tot;
+    __syncthreads();
+  }
+}
+
 }  // namespace zeb
 
 using namespace zeb;
@@ -559,6 +732,46 @@ extern "C" int zeb_refine(const float* pats, const float* items, const float* se
     k_refine_direct<<<n, 256, smem, (cudaStream_t)stream>>>(a);
   }
   return zeb_launch_check("refine");
+}
+
+extern "C" int zeb_mask_pixels(const zeb_frame_t* fr) {
+  if (!fr || fr->h <= 0 || fr->w <= 0) return 0;
+  return zeb_mask_count(fr);
+}
+
+extern "C" int zeb_mask_list(const zeb_frame_t* fr, uint32_t* list, void* stream) {
+  ZEB_REQUIRE(fr && list, ZEB_EARG, "mask_list: null argument");
+  ZEB_REQUIRE(fr->h > 0 && fr->w > 0 && fr->h < 65536 && fr->w < 65536, ZEB_EARG, "mask_list: bad frame size");
+  DetArgs a{};
+  ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "mask_list: bad frame");
+  k_mask_list<<<1, 256, 0, (cudaStream_t)stream>>>(a, list);
+  return zeb_launch_check("mask_list");
+}
+
+extern "C" int zeb_refine_list(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
+                               const zeb_frame_t* fr, const uint32_t* list, int npix, const float* vpair,
+                               const float* gpair, int side, const zeb_refine_opts_t* o, float* records,
+                               void* stream) {
+  ZEB_REQUIRE(pats && items && seeds && list && vpair && gpair && o && records, ZEB_EARG,
+              "refine_list: null argument");
+  ZEB_REQUIRE(((uintptr_t)gpair & 31) == 0 && ((uintptr_t)vpair & 7) == 0, ZEB_EARG,
+              "refine_list: pair tables misaligned");
+  ZEB_REQUIRE(seed_stride >= 4 && side >= 3 && o->iters >= 0 && o->iters <= 1000 && o->nmi_bins >= 2 &&
+                  o->nmi_bins <= 32,
+              ZEB_EARG, "refine_list: bad arguments");
+  ZEB_REQUIRE(fr && npix == zeb_mask_count(fr), ZEB_EARG, "refine_list: %d pixels listed, the frame masks %d", npix,
+              fr ? zeb_mask_count(fr) : -1);
+  const size_t smem = (size_t)npix * 2 * sizeof(float);
+  ZEB_REQUIRE(npix >= 1 && smem <= DET_LIST_SMEM, ZEB_ESIZE, "refine_list: %d pixels (at most %zu)", npix,
+              DET_LIST_SMEM / 8);
+  if (n <= 0) return ZEB_OK;
+  DetArgs a{};
+  ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine_list: bad frame");
+  a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
+  a.vpair = (const float2*)vpair; a.gpair = gpair; a.side = side; a.o = *o; a.records = records;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_refine_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_refine_list<<<n, RL_THREADS, smem, (cudaStream_t)stream>>>(a, list, npix);
+  return zeb_launch_check("refine_list");
 }
 
 extern "C" int zeb_chance(const float* pats, const float* items, int n, int draws, const zeb_frame_t* fr,

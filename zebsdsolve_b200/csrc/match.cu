@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(256) k_dict_sims(SimArgs a) {
     const int row = i / a.w, col = i - row * a.w;
     const float dr = (float)row - a.mask[0], dc = (float)col - a.mask[1];
     float v = 0.f;
-    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) {
+    if (zeb_in_circle(dr, dc, a.mask[2])) {
       const float3 u = normalize3(make_float3(a.c0.x * row + a.c1.x * col + a.t0.x, a.c0.y * row + a.c1.y * col + a.t0.y,
                                               a.c0.z * row + a.c1.z * col + a.t0.z));
       v = master_at_pair(a.vpair, qrot(q, u), a.side);
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256) k_dict_sims(SimArgs a) {
   for (int i = threadIdx.x; i < hw; i += blockDim.x) {
     const int row = i / a.w, col = i - row * a.w;
     const float dr = (float)row - a.mask[0], dc = (float)col - a.mask[1];
-    const float d = (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) ? sim_px[i] - mean : 0.f;
+    const float d = zeb_in_circle(dr, dc, a.mask[2]) ? sim_px[i] - mean : 0.f;
     sim_px[i] = d;
     ss += d * d;
   }

@@ -52,7 +52,7 @@ __device__ void prep_finish(const PrepArgs& a, float* img, float* out, float* re
   for (int i = threadIdx.x; i < hw; i += blockDim.x) {
     int r = i / w, c = i - r * w;
     float dr = (float)r - a.mask[0], dc = (float)c - a.mask[1];
-    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) {
+    if (zeb_in_circle(dr, dc, a.mask[2])) {
       v2[0] += img[i];
       v2[1] += 1.f;
     }
@@ -64,7 +64,7 @@ __device__ void prep_finish(const PrepArgs& a, float* img, float* out, float* re
     int r = i / w, c = i - r * w;
     float dr = (float)r - a.mask[0], dc = (float)c - a.mask[1];
     float v = 0.f;
-    if (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]) v = img[i] - mean;
+    if (zeb_in_circle(dr, dc, a.mask[2])) v = img[i] - mean;
     img[i] = v;
     ss[0] += v * v;
   }

@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
     const int i = base + threadIdx.x;
     const int row = i / a.w, col = i - row * a.w;
     float dr = (float)row - a.mask[0], dc = (float)col - a.mask[1];
-    const bool m = i < hw && (a.mask[2] <= 0.f || dr * dr + dc * dc <= a.mask[2]);
+    const bool m = i < hw && zeb_in_circle(dr, dc, a.mask[2]);
     const unsigned bal = __ballot_sync(0xffffffffu, m);
     if (lane == 0) wcnt[wid] = __popc(bal);
     __syncthreads();

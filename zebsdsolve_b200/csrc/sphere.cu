@@ -57,7 +57,7 @@ struct Sampler {
       float row = dot3(c0, hh), col = dot3(c1, hh);
       float hmax = (float)(h - 1), wmax = (float)(w - 1);
       float dr = row - mask[0], dc = col - mask[1];
-      if (row >= 0.f && row <= hmax && col >= 0.f && col <= wmax && (mask[2] <= 0.f || dr * dr + dc * dc <= mask[2])) {
+      if (row >= 0.f && row <= hmax && col >= 0.f && col <= wmax && zeb_in_circle(dr, dc, mask[2])) {
         wv = 1.f;
         val = 1.f;
         if (!window) {

@@ -526,10 +526,8 @@ class Engine:
                 mark("peaks")
                 N.call("zeb_correlate_peaks", ptr(U), nt, ctypes.byref(ph.dims), ptr(bt.tw), ptr(ph.rden), 1 << 30,
                        ptr(peaks[t0 * 8:]), ptr(cand), stream_ptr())
-            _, sheets, grad, vpair, gpair = p.baked
             mark("refine")
-            N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(vpair), ptr(gpair),
-                   p.master.side, ctypes.byref(opts), ptr(recs[pi * n * 8:]), stream_ptr())
+            self.refine(pats, items, peaks, n, fr, p, opts, recs[pi * n * 8:])
         mark("end")
         return recs[: n_ph * n * 8].view(n_ph, n, 8)
 
@@ -556,12 +554,36 @@ class Engine:
             mark("match")
             xs = x @ d.W.T if method == "pca" else x  # the patterns' coefficients (pca.zig:159-162)
             peaks = d.seeds(xs.contiguous(), tc, self.tc_status(), self.buf("peaks", n * 8))
-            _, sheets, grad, vpair, gpair = p.baked
             mark("refine")
-            N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(vpair), ptr(gpair),
-                   p.master.side, ctypes.byref(opts), ptr(recs[pi * n * 8:]), stream_ptr())
+            self.refine(pats, items, peaks, n, fr, p, opts, recs[pi * n * 8:])
         mark("end")
         return recs[: n_ph * n * 8].view(n_ph, n, 8)
+
+    def mask_list(self, fr):
+        """The frame's masked pixels in raster order on the device (zeb_mask_list), cached per
+        frame; None when the list is beyond the list kernel (zeb_refine then takes the frame)."""
+        key = (fr.h, fr.w, tuple(fr.mask))
+        hit = getattr(self, "_mask_list", None)
+        if hit is not None and hit[0] == key:
+            return hit[1]
+        npix = N.load().zeb_mask_pixels(ctypes.byref(fr))
+        lst = None
+        if 1 <= npix <= 25600:
+            lst = torch.empty(npix, dtype=torch.int32, device=self.dev)
+            N.call("zeb_mask_list", ctypes.byref(fr), ptr(lst), stream_ptr())
+        self._mask_list = (key, lst)
+        return lst
+
+    def refine(self, pats, items, peaks, n, fr, p, opts, out):
+        """detector.zig:178-202 — every item refined from its seed (peaks, stride 8) and scored."""
+        _, sheets, grad, vpair, gpair = p.baked
+        lst = self.mask_list(fr)
+        if lst is not None:
+            N.call("zeb_refine_list", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(lst), lst.numel(),
+                   ptr(vpair), ptr(gpair), p.master.side, ctypes.byref(opts), ptr(out), stream_ptr())
+        else:
+            N.call("zeb_refine", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(vpair), ptr(gpair),
+                   p.master.side, ctypes.byref(opts), ptr(out), stream_ptr())
 
     def pinned(self):
         """The stored patterns in page-locked host memory ([cell][h][w], the scan's pixel type),
