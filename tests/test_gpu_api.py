@@ -65,10 +65,12 @@ def test_progress_returning_false_stops_after_a_pass(scan):
         return False
 
     r = s.index(progress)
-    assert seen == [40]
+    # one call, after the first pass (a short one: its upload is not hidden behind kernels)
+    assert len(seen) == 1 and 0 < seen[0] <= 40, seen
     # the pass in flight when the stop came (the next 40) lands too; nothing after it runs
+    k = seen[0] + 40
     ph = r["phase"].reshape(-1)
-    assert (ph[:80] >= 0).all() and (ph[80:] == -1).all()
+    assert (ph[:k] >= 0).all() and (ph[k:] == -1).all()
 
 
 def test_two_sweeps_run_to_the_end(scan):

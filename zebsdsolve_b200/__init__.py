@@ -209,12 +209,10 @@ class Solver:
         return self.results()
 
     def results(self):
-        from .rotations import to_bunge
-
         rows, cols, h, w = self._e.info()
         r = self._e.res
         return {"quaternions": r["quat"].reshape(rows, cols, 4).copy(),
-                "euler": to_bunge(r["quat"].astype(np.float64)).astype(np.float32).reshape(rows, cols, 3),
+                "euler": r["euler"].reshape(rows, cols, 3).copy(),
                 "ncc": r["ncc"].reshape(rows, cols).copy(), "nmi": r["nmi"].reshape(rows, cols).copy(),
                 "phase": r["phase"].reshape(rows, cols).copy(), "z": r["z"].reshape(rows, cols).copy(),
                 "sweep": r["sweep"].reshape(rows, cols).copy()}

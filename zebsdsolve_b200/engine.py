@@ -130,6 +130,7 @@ class Engine:
         self._batch_t = None  # bounding box of the last batch's detector positions
         self._spans = {}
         self.dicts = {}  # (phase, grid) → dictionary.Dictionary
+        self._stage, self._stage_next = {}, {}  # page-locked staging rings of to_device
         self._pinned = None
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
@@ -173,6 +174,7 @@ class Engine:
                     "z": np.zeros(rows * cols, np.float32), "sweep": np.full(rows * cols, -1, np.int32),
                     "settled": np.zeros(rows * cols, bool)}
         self.res["quat"][:, 0] = 1
+        self.res["euler"] = np.zeros((rows * cols, 3), np.float32)  # Bunge angles of quat, kept as cells land
 
     def info(self):
         if self.patterns is None:
@@ -458,11 +460,37 @@ class Engine:
             d.key = key
         return d
 
+    def to_device(self, name, arr):
+        """A small host array on the device without stalling the host: copied into one of a ring of
+        page-locked buffers and from there asynchronously on the current stream (a copy from
+        pageable memory would wait for all the work queued before it)."""
+        arr = np.ascontiguousarray(arr)
+        ring = self._stage.setdefault(name, [])
+        k = self._stage_next.get(name, 0)
+        self._stage_next[name] = (k + 1) % 4
+        while len(ring) <= k:
+            ring.append([None, None])
+        slot = ring[k]
+        nbytes = arr.nbytes
+        if slot[0] is None or slot[0].numel() < nbytes:
+            slot[0] = torch.empty(max(nbytes, 1 << 16), dtype=torch.uint8, pin_memory=True)
+            slot[1] = None
+        if slot[1] is not None:
+            slot[1].synchronize()  # the copy that last read this buffer (four uses ago) is done
+        host = slot[0][:nbytes].view(torch.from_numpy(arr).dtype).view(arr.shape)
+        host.numpy()[...] = arr
+        dev = torch.empty(arr.shape, dtype=host.dtype, device=self.dev)
+        dev.copy_(host, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream())
+        slot[1] = ev
+        return dev
+
     def items_of(self, cells):
         cells = np.asarray(cells, np.int64)
         t = self.positions(cells)
         self._batch_t = (t.min(0), t.max(0)) if len(t) else None
-        return torch.as_tensor(np.concatenate([t, np.arange(len(cells), dtype=np.float32)[:, None]], 1), device=self.dev)
+        return self.to_device("items", np.concatenate([t, np.arange(len(cells), dtype=np.float32)[:, None]], 1))
 
     def spans(self, bt, fr):
         """The sphere's ring spans for the detector positions of the last items_of batch: the
@@ -479,7 +507,7 @@ class Engine:
             self._spans = {}
         corners = np.array([[x, y, z, 0.0] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])],
                            np.float32)
-        ts = torch.as_tensor(corners, device=self.dev)
+        ts = self.to_device("corners", corners)
         sp = torch.empty(bt.n_theta * 2, dtype=torch.int32, device=self.dev)
         N.call("zeb_sphere_spans", ctypes.byref(fr), ctypes.byref(bt.st), ptr(ts), len(corners), 2, ptr(sp),
                stream_ptr())
@@ -701,7 +729,9 @@ class Engine:
         cps.wait_stream(comp)
         host = [torch.empty((n_ph, B, 8), dtype=torch.float32, pin_memory=True) for _ in range(2)]
         hfz = [torch.empty((n_ph, B, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
-        parts = [cells[i:i + B] for i in range(0, len(cells), B)]
+        # a small first pass (its upload is the one nothing hides), then passes of B
+        first = min(len(cells), max(1, B // 4))
+        parts = [cells[:first]] + [cells[i:i + B] for i in range(first, len(cells), B)]
         up_done = [None, None]
         comp_done = [None, None]
         back = [None, None]  # (event, cells, stamp)
@@ -820,6 +850,8 @@ class Engine:
     def index_begin(self):
         if not self.phases:
             raise EngineError("NoPhases")
+        if "euler" not in self.res or self.res["euler"].shape[0] != self.res["quat"].shape[0]:
+            self.res["euler"] = R.to_bunge(self.res["quat"].astype(np.float64)).astype(np.float32)
         cells = self.region_cells()
         self.index_cells_list = cells
         self.index_done = 0
@@ -852,6 +884,7 @@ class Engine:
                 q[sel] = R.to_fz(r[sel, :4].astype(np.float64), self.phases[int(p)].master.rotations())
         idx = cells[replace]
         res["quat"][idx] = q[replace]
+        res["euler"][idx] = R.to_bunge(q[replace].astype(np.float64)).astype(np.float32)
         res["ncc"][idx] = r[replace, 4]
         res["nmi"][idx] = r[replace, 5]
         res["z"][idx] = r[replace, 7]
