@@ -340,17 +340,22 @@ __global__ void __launch_bounds__(RW_WARPS * 32) k_sphere_rings_w(SphereArgs a) 
   }
   __syncthreads();
 
-  // the window's sums over the spans
+  // the window's sums over the spans, a warp per ring pair as below (no search for a flat
+  // index's ring)
   float acc[2] = {0.f, 0.f};
-  const int total = pre[nt];
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    const int y = span_of(pre, nt, e);
-    const int j = (sp[y].x + (e - pre[y])) & pmask;
-    const float4 rg = __ldg(a.ring + y);
-    const float2 cs = pcs[j];
-    const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
-    acc[0] += g.x * g.y * rg.z;
-    acc[1] += g.y * rg.z;
+  for (int ai = warp; ai < n_act; ai += RW_WARPS) {
+    const int y2[2] = {act[ai], nt - 1 - act[ai]};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float4 rg = __ldg(a.ring + y2[h]);
+      const int2 v = sp[y2[h]];
+      for (int e = lane; e < v.y; e += 32) {
+        const float2 cs = pcs[(v.x + e) & pmask];
+        const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
+        acc[0] += g.x * g.y * rg.z;
+        acc[1] += g.y * rg.z;
+      }
+    }
   }
   block_sums<2>(acc, red);
   const float mean = (a.flags & ZEB_FLAG_CENTER) ? acc[0] / fmaxf(acc[1], 1e-20f) : 0.f;
