@@ -552,6 +552,7 @@ __device__ __forceinline__ float3 list_ray(const DetArgs& a, float3 t, uint32_t 
 __device__ float nmi_list(const DetArgs& a, const uint32_t* __restrict__ list, const float* pv, float* sims,
                           int npix, float3 t, float4 q, int nbins, uint32_t* hist, float* red) {
   float ext[4] = {3.4e38f, -3.4e38f, 3.4e38f, -3.4e38f};
+#pragma unroll 4
   for (int k = threadIdx.x; k < npix; k += blockDim.x) {
     const float e = pv[k];
     const float sv = master_at_pair(a.vpair, qrot(q, list_ray(a, t, __ldg(list + k))), a.side);
@@ -636,6 +637,7 @@ __global__ void __launch_bounds__(RL_THREADS, 6) k_refine_list(DetArgs a, const 
     float s[19];
 #pragma unroll
     for (int k = 0; k < 19; ++k) s[k] = 0.f;
+#pragma unroll 4
     for (int k = threadIdx.x; k < npix; k += RL_THREADS) {
       const float3 c = qrot(q, list_ray(a, t, __ldg(list + k)));
       const float4 m = grad_at_pair(a.gpair, c, a.side);
