@@ -285,11 +285,9 @@ def device_main(a):
             e.run_device(raw[b0:b0 + len(c)], c, L, timer)
 
     def max_over_ranks(v):
-        if dist:
-            tt = torch.tensor([v], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            return float(tt.item())
-        return v
+        from zebsdsolve_b200.shard import max_over_ranks as mor
+
+        return mor(v, dist, "cuda")
 
     def time_form(precision, clocks=None, nvtx=False):
         """(device-resident ms per step, e2e ms per step, launches, stage ms, results) of one form."""
