@@ -270,6 +270,13 @@ int zeb_det6(int mode, const float* pats, const float* items, int n, const zeb_f
 /* x[b] = A[b]⁻¹ b[b] for n systems of 6 (A: [n][6][6], b: [n][6], FP64) by elimination with
  * partial pivoting; ok[b] = 0 where a pivot falls below 1e-300 (x[b] = 0). Replaces the host
  * solve of planefit.zig:203-233 (the damped Levenberg–Marquardt step of settle). */
+/* zeb_det6 over the frame's masked-pixel list (zeb_mask_list, npix = zeb_mask_pixels entries, at
+ * most 51200): 128 threads per pattern keep only the pattern's values in shared memory and
+ * recompute each pixel's ray, so that four patterns share an SM; the same outputs. */
+int zeb_det6_list(int mode, const float* pats, const float* items, int n, const zeb_frame_t* fr, const uint32_t* list,
+                  int npix, const float* vpair, const float* gpair, int side, const float* x, const float* q0,
+                  float* out, void* stream);
+
 int zeb_solve6(const double* A, const double* b, int n, double* x, int* ok, void* stream);
 
 /* ── dictionary indexing ────────────────────────────────────────────────────────────────── */

@@ -219,3 +219,25 @@ def test_refine_patterns_settles_like_the_oracle(setup, gradient):
             assert np.abs(r["shift"][i] - shift).max() < 0.05, (r["shift"][i], shift)
         else:  # the exact gradient's optimum: the same NCC to the discretization of the reference's
             assert r["ncc"][i] > ncc - 1e-4, (r["ncc"][i], ncc)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_pixel_list_kernel_equals_the_block_list_kernel(setup, mode):
+    """zeb_det6_list (the frame's shared pixel list, 128 threads a pattern) gives zeb_det6's
+    outputs in every mode, to FP32 summation-order noise (1e-5 of each output's scale)."""
+    from zebsdsolve_b200 import adjoint
+
+    st = setup
+    e = st["e"]
+    plan, pats = _plan(st)
+    lst = e.mask_list(e.frame())
+    assert lst is not None
+    plan_l = adjoint.Plan(plan.pats, plan.items, plan.frame, plan.vpair, plan.gpair, plan.side, lst)
+    rng = np.random.default_rng(mode)
+    x = torch.as_tensor(np.concatenate([rng.normal(0, 0.5, (st["n"], 3)), rng.normal(0, 0.01, (st["n"], 3))], 1),
+                        dtype=torch.float32, device="cuda").contiguous()
+    q0 = torch.as_tensor(st["q_start"], dtype=torch.float32, device="cuda").contiguous()
+    a = plan.run(mode, x, q0).cpu().numpy()
+    b = plan_l.run(mode, x, q0).cpu().numpy()
+    scale = np.maximum(np.abs(a).max(0) if a.ndim > 1 else np.abs(a).max(), 1e-6)
+    assert np.all(np.abs(a - b) <= 1e-5 * scale + 1e-7), np.abs(a - b).max()

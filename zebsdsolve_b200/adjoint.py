@@ -9,7 +9,7 @@ projection of every pixel from the parameters instead of keeping the projected p
 `refine6` runs the reference's Levenberg–Marquardt settle over all the given patterns at once,
 with the damped 6 × 6 solve in FP64 on the device (`zeb_solve6`) and the Gauss–Newton matrix
 from the reference's 43 sums (`zeb_det6` mode 2); the gradient is the reference's (the gradient
-table's) or the exact adjoint's, through autograd.
+table's) or the exact adjoint's (the kernel behind ProjectedNCC's backward).
 """
 import ctypes
 import math
@@ -25,16 +25,22 @@ class Plan:
     """What a batch of patterns needs besides its parameters: preprocessed patterns, items,
     frame, and the master's pair tables."""
 
-    def __init__(self, pats, items, frame, vpair, gpair, side):
+    def __init__(self, pats, items, frame, vpair, gpair, side, pixels=None):
         self.pats, self.items, self.frame = pats, items, frame
         self.vpair, self.gpair, self.side = vpair, gpair, side
+        self.pixels = pixels  # the frame's masked-pixel list (zeb_mask_list), or None
         self.n = items.shape[0]
 
     def run(self, mode, x, q0):
         width = (1, 7, 43)[mode]
         out = torch.empty(self.n * width, dtype=torch.float32, device=x.device)
-        N.call("zeb_det6", mode, ptr(self.pats), ptr(self.items), self.n, ctypes.byref(self.frame), ptr(self.vpair),
-               ptr(self.gpair), self.side, ptr(x), ptr(q0), ptr(out), stream_ptr())
+        if self.pixels is not None:
+            N.call("zeb_det6_list", mode, ptr(self.pats), ptr(self.items), self.n, ctypes.byref(self.frame),
+                   ptr(self.pixels), self.pixels.numel(), ptr(self.vpair), ptr(self.gpair), self.side, ptr(x), ptr(q0),
+                   ptr(out), stream_ptr())
+        else:
+            N.call("zeb_det6", mode, ptr(self.pats), ptr(self.items), self.n, ctypes.byref(self.frame),
+                   ptr(self.vpair), ptr(self.gpair), self.side, ptr(x), ptr(q0), ptr(out), stream_ptr())
         return out.view(self.n, width) if width > 1 else out
 
 
@@ -118,8 +124,9 @@ def refine6(plan, q0, trust, most=60, gradient="reference"):
     exp(d)·q) is kept where its own NCC rose (λ ← max(λ/3, 1e-4)), else λ ← min(5λ, 1e8); until
     a round gains the patterns' mean NCC less than 1e-7 (a round in which every step overshot
     goes again while some λ < 1e8) or after `most` rounds. gradient: "reference" (the gradient
-    table's, as the reference) or "adjoint" (the exact derivative of the forward, by autograd
-    through ProjectedNCC). Returns (q [n,4] f64, shift [n,3] f64 pixels, NCC [n], rounds)."""
+    table's, as the reference) or "adjoint" (the exact derivative of the forward: the adjoint
+    kernel that ProjectedNCC's backward runs, called once per round for gradient and NCC).
+    Returns (q [n,4] f64, shift [n,3] f64 pixels, NCC [n], rounds)."""
     dev = q0.device
     n = plan.n
     q = _qstd(q0.to(torch.float64))
@@ -130,11 +137,11 @@ def refine6(plan, q0, trust, most=60, gradient="reference"):
         qf = qq.to(torch.float32).contiguous()
         ok, ncc, g, H = local_of(plan.run(2, x, qf))
         if gradient == "adjoint":
-            xa = x.clone().requires_grad_(True)
-            score = projected_ncc(xa, qf, plan)
-            (ga,) = torch.autograd.grad(score.sum(), xa)
-            g = ga.to(torch.float64)
-            ncc = torch.where(ok, score.detach().to(torch.float64), ncc)
+            # the exact gradient and the NCC from one pass of the adjoint kernel (what
+            # ProjectedNCC's backward runs; its forward pass would only repeat the NCC)
+            res = plan.run(1, x, qf).to(torch.float64)
+            g = res[:, :6]
+            ncc = torch.where(ok, res[:, 6], ncc)
         return ok, ncc, g, H
 
     keep = local(q, shift)

@@ -93,6 +93,84 @@ __device__ __forceinline__ float master_and_slope(const float2* __restrict__ vp,
   return m;
 }
 
+// one pixel's share of the sums: its ray u (pixels, before the shift), pattern value e
+template <int MODE, int NS>
+__device__ __forceinline__ void det6_pixel(const Det6Args& a, float4 q, float4 qi, float3 dt, float3 u, float e,
+                                           float (&s)[NS]) {
+  const float3 v = make_float3(u.x + dt.x, u.y + dt.y, u.z + dt.z);
+  const float dist = sqrtf(dot3(v, v));
+  const float inv = 1.f / dist;
+  const float3 c = qrot(q, make_float3(v.x * inv, v.y * inv, v.z * inv));
+  float m;
+  float d[6];
+  if (MODE == 0) {
+    m = master_at_pair(a.vpair, c, a.side);
+  } else {
+    float3 g;
+    if (MODE == 1) {
+      m = master_and_slope(a.vpair, c, a.side, g);
+    } else {
+      const float4 gm = grad_at_pair(a.gpair, c, a.side);
+      m = gm.w;
+      g = make_float3(gm.x, gm.y, gm.z);
+    }
+    const float3 w = qrot(qi, g);
+    const float3 r = cross3(c, g);
+    d[0] = w.x * inv; d[1] = w.y * inv; d[2] = w.z * inv;
+    d[3] = r.x; d[4] = r.y; d[5] = r.z;
+  }
+  s[0] += 1.f;
+  s[1] += m;
+  s[2] += m * m;
+  s[3] += m * e;
+  if (MODE >= 1) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      s[4 + i] += d[i];
+      s[10 + i] += m * d[i];
+      s[16 + i] += e * d[i];
+    }
+  }
+  if (MODE == 2) {
+    int o = 22;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int j = i; j < 6; ++j) s[o++] += d[i] * d[j];
+  }
+}
+
+// the pattern's outputs from its summed sums (thread 0): MODE 2 the 43 sums; MODE 0 the NCC;
+// MODE 1 the NCC and its gradient (planefit.zig:176-200)
+template <int MODE, int NS>
+__device__ __forceinline__ void det6_finish(const Det6Args& a, int b, const float (&s)[NS]) {
+  if (MODE == 2) {
+    for (int k = 0; k < 43; ++k) a.out[(size_t)b * 43 + k] = s[k];
+    return;
+  }
+  // planefit.zig:176-200: NCC and (MODE 1) its gradient
+  const float n = fmaxf(s[0], 1.f);
+  const float mean = s[1] / n;
+  const float var_n = s[2] - n * mean * mean;
+  float ncc = -2.f, g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (var_n > 1e-12f) {
+    const float inv = rsqrtf(var_n);
+    ncc = s[3] * inv;
+    if (MODE == 1)
+      for (int i = 0; i < 6; ++i) {
+        const float au = (s[10 + i] - mean * s[4 + i]) * inv;
+        g[i] = (s[16 + i] - ncc * au) * inv;
+      }
+  }
+  if (MODE == 0) {
+    a.out[b] = ncc;
+  } else {
+    float* o = a.out + (size_t)b * 7;
+    for (int i = 0; i < 6; ++i) o[i] = g[i];
+    o[6] = ncc;
+  }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
   constexpr int NS = MODE == 0 ? 4 : (MODE == 1 ? 22 : 43);
@@ -144,78 +222,61 @@ __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
   float s[NS];
 #pragma unroll
   for (int k = 0; k < NS; ++k) s[k] = 0.f;
+  // unrolled: several master lookups of a thread in flight at once
+#pragma unroll 2
   for (int k = threadIdx.x; k < npix; k += blockDim.x) {
     const float4 p = px6[k];
-    const float3 v = make_float3(p.x + dt.x, p.y + dt.y, p.z + dt.z);
-    const float dist = sqrtf(dot3(v, v));
-    const float inv = 1.f / dist;
-    const float3 c = qrot(q, make_float3(v.x * inv, v.y * inv, v.z * inv));
-    const float e = p.w;
-    float m;
-    float d[6];
-    if (MODE == 0) {
-      m = master_at_pair(a.vpair, c, a.side);
-    } else {
-      float3 g;
-      if (MODE == 1) {
-        m = master_and_slope(a.vpair, c, a.side, g);
-      } else {
-        const float4 gm = grad_at_pair(a.gpair, c, a.side);
-        m = gm.w;
-        g = make_float3(gm.x, gm.y, gm.z);
-      }
-      const float3 w = qrot(qi, g);
-      const float3 r = cross3(c, g);
-      d[0] = w.x * inv; d[1] = w.y * inv; d[2] = w.z * inv;
-      d[3] = r.x; d[4] = r.y; d[5] = r.z;
-    }
-    s[0] += 1.f;
-    s[1] += m;
-    s[2] += m * m;
-    s[3] += m * e;
-    if (MODE >= 1) {
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        s[4 + i] += d[i];
-        s[10 + i] += m * d[i];
-        s[16 + i] += e * d[i];
-      }
-    }
-    if (MODE == 2) {
-      int o = 22;
-#pragma unroll
-      for (int i = 0; i < 6; ++i)
-#pragma unroll
-        for (int j = i; j < 6; ++j) s[o++] += d[i] * d[j];
-    }
+    det6_pixel<MODE, NS>(a, q, qi, dt, make_float3(p.x, p.y, p.z), p.w, s);
   }
   block_sums<NS>(s, red);
   if (threadIdx.x != 0) return;
-  if (MODE == 2) {
-    for (int k = 0; k < 43; ++k) a.out[(size_t)b * 43 + k] = s[k];
-    return;
+  det6_finish<MODE, NS>(a, b, s);
+}
+
+// The same over the frame's masked-pixel list (zeb_mask_list, shared by every pattern): 128
+// threads per pattern keep only the pattern's values along the list in shared memory and
+// recompute each pixel's ray, so that several patterns share an SM (a list of (ray, value) per
+// block fills an SM's shared memory for one 120 × 120 pattern).
+template <int MODE>
+__global__ void __launch_bounds__(128, 4) k_det6_list(Det6Args a, const uint32_t* __restrict__ list, int npix) {
+  constexpr int NS = MODE == 0 ? 4 : (MODE == 1 ? 22 : 43);
+  extern __shared__ float pv6[];
+  __shared__ float red[NS * 4];
+  __shared__ float4 sh_q;
+  __shared__ float3 sh_t;
+  const int b = blockIdx.x;
+  const float4 it = a.items[b];
+  const float* gpat = a.pats + (size_t)(int)it.w * a.h * a.w;
+  for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    const uint32_t v = __ldg(list + k);
+    pv6[k] = __ldg(gpat + (int)(v >> 16) * a.w + (int)(v & 0xffffu));
   }
-  // planefit.zig:176-200: NCC and (MODE 1) its gradient
-  const float n = fmaxf(s[0], 1.f);
-  const float mean = s[1] / n;
-  const float var_n = s[2] - n * mean * mean;
-  float ncc = -2.f, g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if (var_n > 1e-12f) {
-    const float inv = rsqrtf(var_n);
-    ncc = s[3] * inv;
-    if (MODE == 1)
-      for (int i = 0; i < 6; ++i) {
-        const float au = (s[10 + i] - mean * s[4 + i]) * inv;
-        g[i] = (s[16 + i] - ncc * au) * inv;
-      }
+  if (threadIdx.x == 0) {
+    const float* x = a.x + (size_t)b * 6;
+    const float* q0 = a.q0 + (size_t)b * 4;
+    float4 q = qmul(qexp(make_float3(x[3], x[4], x[5])), make_float4(q0[0], q0[1], q0[2], q0[3]));
+    const float nq = rsqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    sh_q = make_float4(q.x * nq, q.y * nq, q.z * nq, q.w * nq);
+    sh_t = make_float3(x[0], x[1], x[2]);
   }
-  if (MODE == 0) {
-    a.out[b] = ncc;
-  } else {
-    float* o = a.out + (size_t)b * 7;
-    for (int i = 0; i < 6; ++i) o[i] = g[i];
-    o[6] = ncc;
+  __syncthreads();
+  const float4 q = sh_q;
+  const float4 qi = make_float4(q.x, -q.y, -q.z, -q.w);
+  const float3 dt = sh_t;
+  float s[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) s[k] = 0.f;
+#pragma unroll 2
+  for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+    const uint32_t v = __ldg(list + k);
+    const float row = (float)(int)(v >> 16), col = (float)(int)(v & 0xffffu);
+    const float3 u = make_float3(a.c0.x * row + a.c1.x * col + it.x, a.c0.y * row + a.c1.y * col + it.y,
+                                 a.c0.z * row + a.c1.z * col + it.z);
+    det6_pixel<MODE, NS>(a, q, qi, dt, u, pv6[k], s);
   }
+  block_sums<NS>(s, red);
+  if (threadIdx.x != 0) return;
+  det6_finish<MODE, NS>(a, b, s);
 }
 
 // x = A⁻¹ b for a (6 × 6, 6) system per item in FP64 (planefit.zig:203-233); ok[b] = 0 where a
@@ -301,6 +362,42 @@ extern "C" int zeb_det6(int mode, const float* pats, const float* items, int n, 
     k_det6<2><<<n, 256, list, st>>>(a);
   }
   return zeb_launch_check("det6");
+}
+
+extern "C" int zeb_det6_list(int mode, const float* pats, const float* items, int n, const zeb_frame_t* fr,
+                             const uint32_t* list, int npix, const float* vpair, const float* gpair, int side,
+                             const float* x, const float* q0, float* out, void* stream) {
+  ZEB_REQUIRE(mode >= 0 && mode <= 2, ZEB_EARG, "det6_list: mode %d", mode);
+  ZEB_REQUIRE(pats && items && list && vpair && x && q0 && out && fr && side >= 3 && (mode != 2 || gpair), ZEB_EARG,
+              "det6_list: bad arguments");
+  ZEB_REQUIRE(((uintptr_t)gpair & 31) == 0 && ((uintptr_t)vpair & 7) == 0, ZEB_EARG,
+              "det6_list: pair tables misaligned");
+  ZEB_REQUIRE(npix == zeb_mask_count(fr), ZEB_EARG, "det6_list: %d pixels listed, the frame masks %d", npix,
+              zeb_mask_count(fr));
+  const size_t smem = (size_t)npix * sizeof(float);
+  ZEB_REQUIRE(npix >= 1 && smem <= 200 * 1024, ZEB_ESIZE, "det6_list: %d pixels (at most 51200)", npix);
+  if (n <= 0) return ZEB_OK;
+  Det6Args a{};
+  ZEB_REQUIRE(fr->h >= 2 && fr->w >= 2 && fr->h < 65536 && fr->w < 65536, ZEB_EARG, "det6_list: bad frame");
+  a.h = fr->h; a.w = fr->w;
+  a.c0 = make_float3(fr->c0[0], fr->c0[1], fr->c0[2]);
+  a.c1 = make_float3(fr->c1[0], fr->c1[1], fr->c1[2]);
+  a.c2 = make_float3(fr->c2[0], fr->c2[1], fr->c2[2]);
+  for (int k = 0; k < 3; ++k) a.mask[k] = fr->mask[k];
+  a.pats = pats; a.items = (const float4*)items; a.n = n; a.vpair = (const float2*)vpair; a.gpair = gpair;
+  a.side = side; a.x = x; a.q0 = q0; a.out = out;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (mode == 0) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_det6_list<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_det6_list<0><<<n, 128, smem, st>>>(a, list, npix);
+  } else if (mode == 1) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_det6_list<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_det6_list<1><<<n, 128, smem, st>>>(a, list, npix);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_det6_list<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_det6_list<2><<<n, 128, smem, st>>>(a, list, npix);
+  }
+  return zeb_launch_check("det6_list");
 }
 
 extern "C" int zeb_solve6(const double* A, const double* b, int n, double* x, int* ok, void* stream) {

@@ -657,7 +657,10 @@ class Engine:
         items = self.items_of(cells)
         fr = self.frame()
         _, sheets, grad, vpair, gpair = self.phases[phase].baked
-        plan = adjoint.Plan(pats, items, fr, vpair, gpair, self.phases[phase].master.side)
+        lst = self.mask_list(fr)
+        if lst is not None and lst.numel() > 51200:
+            lst = None
+        plan = adjoint.Plan(pats, items, fr, vpair, gpair, self.phases[phase].master.side, lst)
         s = self.set
         trust_px = (s["plane_trust"] if trust is None else float(trust)) * h
         most = int(s["plane_iters"] if rounds is None else rounds)
@@ -959,14 +962,18 @@ class Engine:
 
     # ── simulation ──
 
-    def simulate_device(self, phase, cells, quats):
-        """The simulated patterns as a device tensor [n, h, w] (see simulate)."""
+    def simulate_device(self, phase, cells, quats, shifts=None):
+        """The simulated patterns as a device tensor [n, h, w] (see simulate); `shifts` [n, 3]
+        (pixels, sample frame) moves each pattern's source from its cell's position, as a
+        pattern-centre offset does."""
         self.prepare_masters()
         cells = np.asarray(cells, np.int64)
         q = np.asarray(quats, np.float32).reshape(-1, 4)
         n = len(cells)
         h, w = self.pattern_shape()
         t = self.positions(cells)
+        if shifts is not None:
+            t = (t + np.asarray(shifts, np.float32).reshape(n, 3)).astype(np.float32)
         pd = torch.as_tensor(np.concatenate([t, np.zeros((n, 1), np.float32), q], 1), device=self.dev)
         out = torch.empty(n * h * w, dtype=torch.float32, device=self.dev)
         p = self.phases[phase]
