@@ -56,9 +56,12 @@ def parse():
     ap.add_argument("--batch", type=int, default=16384, help="patterns per device pass in the value measurement")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="index", choices=("index", "adjoint"),
+    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven"),
                     help="index: the scan of 60x60 patterns (the headline); adjoint: six-unknown refinement "
-                         "of 120x120 patterns with jittered pattern centres")
+                         "of 120x120 patterns with jittered pattern centres; uneven: many scans of uneven "
+                         "lengths and detector sizes, two phases")
+    ap.add_argument("--scans", type=int, default=16, help="uneven: number of scans")
+    ap.add_argument("--max-count", type=int, default=20000, help="uneven: the longest scan (log-uniform from 1000)")
     return ap.parse_args()
 
 
@@ -483,6 +486,91 @@ def adjoint_main(a):
     print(json.dumps(line), flush=True)
 
 
+def uneven_main(a):
+    """Many scans of uneven lengths (log-uniform from 1 000 to --max-count patterns) and detector
+    sizes (40², 60², 96², 160² u16), each with two phases (432 and 622 masters, grains assigned by
+    a fair coin), indexed one after another through one Solver at L = 64 in the BF16 form: the
+    whole job's patterns over its wall time, every scan's set-up (pinned copy, chance
+    calibration, denominators, masks) included."""
+    import time
+
+    import torch
+
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import synthetic as syn
+    from zebsdsolve_b200.master import write_npz
+
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp()
+    paths = []
+    for g, seed in (("432", 2), ("622", 3)):
+        sheets = syn.master_sheets(seed, side=401, lmax=96, group=g, device="cuda")
+        write_npz(f"{tmp}/m{g}.npz", sheets, 401, syn.group_matrices(g), syn.POINT_GROUP[g])
+        paths.append(f"{tmp}/m{g}.npz")
+    s = ze.Solver()
+    s.configure(bandwidth=L, precision=a.precision)
+    for p in paths:
+        s.add_phase(p)
+    e = s._e
+    rng = np.random.default_rng(400)
+    counts = np.exp(rng.uniform(np.log(1000), np.log(max(a.max_count, 1001)), a.scans)).astype(int)
+    sizes = rng.choice([40, 60, 96, 160], a.scans)
+    scans, truth = [], []
+    for k in range(a.scans):
+        n, side = int(counts[k]), int(sizes[k])
+        cols = int(np.ceil(np.sqrt(n)))
+        rows = -(-n // cols)
+        n = rows * cols
+        s.set_patterns(np.zeros((rows, cols, side, side), np.uint16))
+        s.set_geometry(pc=PC, sample_tilt_deg=70.0, detector_tilt_deg=0.0)
+        q, grain = syn.grain_map(rng, rows, cols, max(4, n // 500), SPREAD_DEG)
+        phase_of = rng.integers(0, 2, grain.max() + 1)[grain.reshape(-1)]
+        pats = np.empty((n, side, side), np.uint16)
+        for ph in (0, 1):
+            sel = np.flatnonzero(phase_of == ph)
+            for i in range(0, len(sel), 4096):
+                c = sel[i:i + 4096]
+                sims = e.simulate_device(ph, c, q[c])
+                pats[c] = syn.counted_patterns(sims, seed=k * 1000 + i).cpu().numpy()
+        scans.append(pats.reshape(rows, cols, side, side))
+        truth.append((q, phase_of))
+    # warm-up: one pass over the first two scans
+    for pats in scans[:2]:
+        s.set_patterns(pats)
+        s.index()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    results = []
+    for pats in scans:
+        s.set_patterns(pats)
+        results.append(s.index())
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    total = int(sum(x.shape[0] * x.shape[1] for x in scans))
+    right, dis_all = [], []
+    for (q, phase_of), r in zip(truth, results):
+        ph = r["phase"].reshape(-1)
+        right.append(ph == phase_of)
+        qq = r["quaternions"].reshape(-1, 4)
+        for p in (0, 1):
+            sel = (ph == p) & (phase_of == p)
+            if sel.any():
+                dis_all.append(np.degrees(s.disorientation(qq[sel], q[sel], phase=p)))
+    right = np.concatenate(right)
+    dis = np.concatenate(dis_all)
+    line = {"metric": "patterns/s over uneven scans (lengths, detector sizes, two phases), 1 B200",
+            "value": round(total / wall, 1), "unit": "patterns/s", "n_gpus": 1, "steps": 1, "warmup": 2,
+            "higher_is_better": True, "dtype": "bf16+f32", "data": "synthetic",
+            "config": {"workload": f"{a.scans} scans, 1000-{a.max_count} patterns (log-uniform), detector sizes "
+                                   "40/60/96/160 u16, masters 432 and 622 (401^2, SH <= 96), L = 64",
+                       "patterns": total, "scan_patterns": [int(x.shape[0] * x.shape[1]) for x in scans],
+                       "scan_sizes": [int(x.shape[2]) for x in scans], "precision": a.precision},
+            "wall_s": round(wall, 3),
+            "accuracy": {"phase_right": round(float(right.mean()), 4), "median_deg": round(float(np.median(dis)), 4),
+                         "within_0.1deg": round(float((dis < 0.1).mean()), 4)}}
+    print(json.dumps(line), flush=True)
+
+
 def reference_main(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -505,5 +593,7 @@ if __name__ == "__main__":
         reference_main(args)
     elif args.workload == "adjoint":
         adjoint_main(args)
+    elif args.workload == "uneven":
+        uneven_main(args)
     else:
         device_main(args)

@@ -92,6 +92,7 @@ class Phase:
     def __init__(self, master):
         self.master = master
         self.baked = None  # (key, sheets, grad4, value pairs, gradient pairs), all on the device
+        self.bakes = {}    # the last few of them by smoothing key (detector sizes met before)
 
     def info(self, bands):
         m = self.master
@@ -293,6 +294,10 @@ class Engine:
             key = (q, self.set["master_smooth"])
             if p.baked is not None and p.baked[0] == key:
                 continue
+            if key in p.bakes:  # a detector size met before (scans of several sizes): its master as baked then
+                p.baked = p.bakes[key]
+                self.chance_key = None
+                continue
             sheets = torch.as_tensor(m.raw, device=self.dev)
             smooth = self.set["master_smooth"] * (1.05 ** q) if q is not None else 0.0
             if smooth > 0.05:
@@ -307,6 +312,9 @@ class Engine:
             gpair = torch.empty(sheets.numel() * 8, dtype=torch.float32, device=self.dev)
             N.call("zeb_master_pairs", ptr(sheets), ptr(grad), m.side, ptr(vpair), ptr(gpair), stream_ptr())
             p.baked = (key, sheets, grad, vpair, gpair)
+            if len(p.bakes) >= 8:
+                p.bakes.pop(next(iter(p.bakes)))
+            p.bakes[key] = p.baked
             self.chance_key = None
 
     def band(self, L):
@@ -317,11 +325,19 @@ class Engine:
             b = {"tables": BandTables(L, self.dev), "phases": {}}
             self.bands[L] = b
         prec = self.set["precision"]
+        cache = b.setdefault("cache", {})
         for i, p in enumerate(self.phases):
             key = (id(p.baked[1]), prec)
             pb = b["phases"].get(i)
             if pb is None or pb[0] != key:
+                hit = cache.get((i, key))
+                if hit is not None:
+                    b["phases"][i] = (key, hit)
+                    continue
                 ph = PhaseBand(b["tables"], p.baked[1], p.master.side, L, prec)
+                if len(cache) >= 16:
+                    cache.pop(next(iter(cache)))
+                cache[(i, key)] = ph
                 b["phases"][i] = (key, ph)
                 r = ph.rules
                 self.log(f"phase {i}: bandwidth {L}, rotation order {r.n_fold} about z{', mirror' if r.mirror else ''}"
