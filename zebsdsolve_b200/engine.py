@@ -133,6 +133,7 @@ class Engine:
         self.dicts = {}  # (phase, grid) → dictionary.Dictionary
         self._stage, self._stage_next = {}, {}  # page-locked staging rings of to_device
         self._pinned = None
+        self._pin_buf = None  # the page-locked buffer behind _pinned, reused across scans
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
 
@@ -251,7 +252,7 @@ class Engine:
             flat = self.patterns.reshape(rows * cols, h, w)
             acc = np.zeros((h, w))
             for i in range(0, len(cells), 1024):
-                acc += flat[cells[i:i + 1024]].astype(np.float64).sum(0)
+                acc += flat[cells[i:i + 1024]].sum(0, dtype=np.float64)
             avg = reduce_image(acc / len(cells), self.set["binning"]).astype(np.float32)
             self.avg = (self.set["static_patterns"], torch.as_tensor(avg, device=self.dev))
             self.log(f"static background: the average of {len(cells)} patterns over the map")
@@ -635,7 +636,14 @@ class Engine:
         if self._pinned is None:
             rows, cols, h, w = self.info()
             src = torch.from_numpy(self.patterns.reshape(rows * cols, h, w))
-            self._pinned = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+            nbytes = src.numel() * src.element_size()
+            # one page-locked buffer kept across scans, grown when a scan needs more (allocating
+            # page-locked memory per scan costs more than many small scans' indexing)
+            if self._pin_buf is None or self._pin_buf.numel() < nbytes:
+                self._pin_buf = None
+                self._pin_buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            torch.cuda.synchronize(self.dev)  # no copy from the buffer is still pending
+            self._pinned = self._pin_buf[:nbytes].view(src.dtype).view(src.shape)
             self._pinned.copy_(src)
         return self._pinned
 
