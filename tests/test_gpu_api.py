@@ -79,3 +79,18 @@ def test_two_sweeps_run_to_the_end(scan):
     st = s.index_status
     assert st["sweep"] == 1 and st["done"] == st["total"] == 96
     assert (r["phase"] >= 0).all()
+
+
+def test_tune_changes_no_result(scan):
+    """tune() times the pipelined path on a sample and keeps the fastest way of cutting up the
+    work; the results after it are the results before it, bit for bit."""
+    s, q = _solver(scan)
+    r1 = s.index()
+    seen = []
+    out = s.tune(lambda k: seen.append(k))
+    assert set(out) == {"before", "after", "summary"} and out["summary"].startswith("tuned on")
+    assert seen == list(range(1, len(seen) + 1)) and len(seen) >= 3
+    assert 2048 <= out["after"]["device_batch"] <= 65536 and 512 <= out["after"]["tile_mb"] <= 8192
+    r2 = s.index()
+    for k in ("quaternions", "ncc", "nmi", "phase", "z", "sweep"):
+        assert np.array_equal(r1[k], r2[k]), k

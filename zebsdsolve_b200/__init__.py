@@ -182,6 +182,15 @@ class Solver:
         return {"quaternions": r[..., :4].copy(), "ncc": r[..., 4].copy(), "nmi": r[..., 5].copy(),
                 "step": r[..., 6].copy(), "z": r[..., 7].copy()}
 
+    def tune(self, progress=None):
+        """Fit how the work is cut up to this GPU and this scan (a sample of the region indexed and
+        timed, nothing stored touched): the knobs that matter here are the patterns per device pass
+        and the memory a pass's spectra may take; the reference's workgroup sizes (`batch`,
+        `refine_pixels`, `wg_refine`, `wg_fft`) have no counterpart on this engine. Returns the
+        knobs before and after and a summary; progress(trials) after each timed trial, False stops."""
+        before, after, summary = self._call("tune", self._e.tune, progress)
+        return {"before": before, "after": after, "summary": summary}
+
     def chance(self, phase=0):
         self._call("chance", self._e.calibrate)
         return float(self._e.chance_med[phase]), float(self._e.chance_spread[phase])

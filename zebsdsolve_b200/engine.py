@@ -132,6 +132,7 @@ class Engine:
         self._spans = {}
         self.dicts = {}  # (phase, grid) → dictionary.Dictionary
         self._stage, self._stage_next = {}, {}  # page-locked staging rings of to_device
+        self.tuned = {}  # what tune() chose for the way work is cut up (device_batch)
         self._pinned = None
         self._pin_buf = None  # the page-locked buffer behind _pinned, reused across scans
         self._last_fz = None  # the last index_cells' records in the fundamental zones
@@ -728,8 +729,77 @@ class Engine:
         return self.finish(out)
 
     def device_batch(self):
-        """Patterns per device pass of a pipelined run."""
-        return 16384
+        """Patterns per device pass of a pipelined run (16 384 unless tune() found better)."""
+        return int(self.tuned.get("device_batch", 16384))
+
+    def tune(self, progress=None):
+        """Fit how the work is cut up to this GPU and this scan: a sample of the region (about
+        32 768 patterns at L ≤ 64, fewer above) is indexed through the pipelined path and timed,
+        with nothing landed, and each knob in turn climbs from its value — doubled while that is
+        faster, else halved while that is (the reference's tune, engine.zig ze_tune_*):
+        `device_batch` (patterns per device pass, 2 048 … 65 536) and `tile_mb` (the memory a
+        pass's spectra may take, which sets the items per spectrum tile, 512 … 8 192). Neither
+        the orientations found nor which matches are accepted depend on them. progress(trials)
+        after each trial; False stops (the best so far stays). Returns (before, after, summary)."""
+        import time
+
+        s = self.set
+        bw, dg, method = s.sweep(self.index_sweep if self.index_cells_list is not None else 0)
+        region = self.region_cells()
+        want = 65536 if bw <= 32 else 32768 if bw <= 64 else 8192 if bw <= 128 else 2048
+        n = min(len(region), want)
+        cells = region[((2 * np.arange(n) + 1) * len(region)) // (2 * n)] if n < len(region) else region
+        before = {"device_batch": self.device_batch(), "tile_mb": int(s["tile_mb"])}
+        knobs = {"device_batch": (2048, 65536), "tile_mb": (512, 8192)}
+        trials = [0]
+        stop = [False]
+
+        def apply(k, v):
+            if k == "device_batch":
+                self.tuned["device_batch"] = v
+            else:
+                s.apply({"tile_mb": v})
+
+        def timed(k, v):
+            apply(k, v)
+            torch.cuda.synchronize(self.dev)
+            t0 = time.perf_counter()
+            try:
+                self.index_pipelined(cells, bw, lambda *x: None, method=method, grid=dg)
+                torch.cuda.synchronize(self.dev)
+                sec = time.perf_counter() - t0
+            except (RuntimeError, N.NativeError):  # a value this GPU cannot run (memory) just loses
+                sec = float("inf")
+            trials[0] += 1
+            if progress is not None and progress(trials[0]) is False:
+                stop[0] = True
+            return sec
+
+        timed("device_batch", before["device_batch"])  # warm-up: tables, buffers
+        for k, (lo, hi) in knobs.items():
+            if stop[0]:
+                break
+            cur = before[k] if k == "device_batch" else int(s["tile_mb"])
+            best = timed(k, cur)
+            for direction in (2.0, 0.5):
+                moved = False
+                while not stop[0]:
+                    v = int(cur * direction)
+                    if not lo <= v <= hi:
+                        break
+                    t = timed(k, v)
+                    if t < best:
+                        best, cur, moved = t, v, True
+                    else:
+                        break
+                if moved:
+                    break
+            apply(k, cur)
+        after = {"device_batch": self.device_batch(), "tile_mb": int(s["tile_mb"])}
+        summary = (f"tuned on {len(cells)} patterns in {trials[0]} trials: device_batch {after['device_batch']}, "
+                   f"tile_mb {after['tile_mb']}")
+        self.log(summary)
+        return before, after, summary
 
     def index_pipelined(self, cells, bandwidth, on_batch, keep_going=lambda: True, method="spherical", grid=None):
         """engine.zig:1990-2137 over many cells at once: device passes of device_batch() cells,
