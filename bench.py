@@ -56,10 +56,11 @@ def parse():
     ap.add_argument("--batch", type=int, default=16384, help="patterns per device pass in the value measurement")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven"),
+    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit"),
                     help="index: the scan of 60x60 patterns (the headline); adjoint: six-unknown refinement "
                          "of 120x120 patterns with jittered pattern centres; uneven: many scans of uneven "
-                         "lengths and detector sizes, two phases")
+                         "lengths and detector sizes, two phases; pcfit: the pattern-centre vote at its default "
+                         "settings")
     ap.add_argument("--scans", type=int, default=16, help="uneven: number of scans")
     ap.add_argument("--max-count", type=int, default=20000, help="uneven: the longest scan (log-uniform from 1000)")
     return ap.parse_args()
@@ -587,6 +588,104 @@ def reference_main(a):
     print(json.dumps(line), flush=True)
 
 
+def pcfit_cpu_sample(seconds):
+    """The oracle's score of one fit pattern under one candidate at L = 64 (its window's
+    denominators shared by the 25 fit patterns of a candidate), timed on one host core."""
+    import oracle.master as om
+    import oracle.spherical as osp
+    from zebsdsolve_b200 import synthetic as syn
+
+    side = 201
+    sheets = syn.master_sheets(3, side=side, lmax=48, group="432").reshape(-1).astype(np.float64)
+    m = om.Master(side, sheets, syn.group_matrices("432"), 30)
+    m.measure_symmetry()
+    hm = om.Harmonics(m, sheets, L)
+    tb = osp.Tables(L)
+    pt = osp.PhaseTables(tb, hm, om.fold_of(hm.rules))
+    import oracle.geometry as og
+
+    geo = og.Geometry(pc=PC, sample_tilt_deg=70.0)
+    frame = geo.frame()
+    mask = og.mask_of(H, W)
+    rng = np.random.default_rng(1)
+    t = geo.translation(H, W)
+    t0 = time.perf_counter()
+    walm, wst = osp.coefficients(tb, None, t, frame, mask, flags=osp.FLAG_WINDOW, shape=(H, W))
+    rden = osp.window_denominators(tb, pt, walm, wst[0])
+    t_win = time.perf_counter() - t0
+    done, t1 = 0, time.perf_counter()
+    while done < 2 or time.perf_counter() - t1 < max(seconds - t_win, 0):
+        g, _ = osp.coefficients(tb, rng.normal(size=(H, W)), t, frame, mask)
+        osp.peak(tb, pt, osp.correlation_volume(tb, pt, hm.f, g) * rden)
+        done += 1
+    t_pat = (time.perf_counter() - t1) / done
+    return 1.0 / (t_pat + t_win / 25), f"1 candidate window and {done} pattern scores at L=64 through the FP64 oracle"
+
+
+def pcfit_main(a):
+    """The pattern-centre vote at the reference's default settings (25 fit patterns on a 5 x 5
+    lattice, 9 x 9 x 5 candidates per grid, 3 levels narrowing by 0.35, ballots, L = 64) on a
+    40 x 40 scan of 60 x 60 u16 patterns simulated at a known centre, from a start 0.015-0.02 off:
+    (fit patterns x candidates scored) per second of the whole fit, every readback and the host
+    vote inside the time."""
+    import torch
+
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import synthetic as syn
+    from zebsdsolve_b200.master import write_npz
+
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp()
+    write_npz(f"{tmp}/m432.npz", syn.master_sheets(2, side=401, lmax=96, group="432", device="cuda"), 401,
+              syn.group_matrices("432"), 30)
+    rows = cols = 40
+    s = ze.Solver()
+    s.configure(bandwidth=L, precision=a.precision)
+    s.add_phase(f"{tmp}/m432.npz")
+    s.set_patterns(np.zeros((rows, cols, H, W), np.uint16))
+    s.set_geometry(pc=PC, sample_tilt_deg=70.0, detector_tilt_deg=0.0)
+    rng = np.random.default_rng(500)
+    q, _ = syn.grain_map(rng, rows, cols, 20, SPREAD_DEG)
+    sims = s._e.simulate_device(0, np.arange(rows * cols), q)
+    s.set_patterns(syn.counted_patterns(sims, seed=9).cpu().numpy().reshape(rows, cols, H, W))
+    start = (PC[0] + 0.015, PC[1] + 0.02, PC[2] - 0.02)
+    for _ in range(max(1, a.warmup)):
+        s.set_geometry(pc=start)
+        s.fit_pc()
+    times, fits = [], []
+    for _ in range(max(1, a.steps)):
+        s.set_geometry(pc=start)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f = s.fit_pc()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        fits.append(f)
+    f = fits[-1]
+    dt = float(np.median(times))
+    from zebsdsolve_b200 import pcfit
+
+    s.set_geometry(pc=start)
+    timer = StageTimer(torch)
+    pcfit.run(s._e, timer)  # one more fit, untimed, for where its time goes
+    stages = {k: round(v, 3) for k, v in timer.totals().items()}
+    scored = f["n_candidates"] * f["n_patterns"]
+    err = np.abs(np.array(f["pc"]) - PC)
+    line = {"metric": "candidate scores/s in the pattern-centre vote (fit patterns x candidate centres), 1 B200",
+            "value": round(scored / dt, 1), "unit": "scores/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_fit": round(1e3 * dt, 2), "higher_is_better": True, "dtype": "bf16+f32", "data": "synthetic",
+            "config": {"workload": f"{rows}x{cols} scan of 60x60 uint16 patterns simulated at pc {PC}, 432 master "
+                                   f"401^2 (SH <= 96), start {tuple(round(v, 3) for v in start)}, fit_grid 5, "
+                                   "9x9x5 candidates, 3 levels, ballots, fit_bandwidth 64", "precision": a.precision},
+            "grids": len(s.pc_levels()), "candidates": f["n_candidates"], "fit_patterns": f["n_patterns"],
+            "pc": [round(v, 5) for v in f["pc"]], "pc_error": round(float(err.max()), 5),
+            "score": round(f["score"], 4), "start_score": round(f["start_score"], 4), "stage_ms_per_fit": stages}
+    if not a.no_cpu:
+        v, sample = pcfit_cpu_sample(a.cpu_seconds)
+        line["cpu_baseline"] = {"value": round(v, 3), "unit": "scores/s", "cores": 1, "kind": "port", "sample": sample}
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     args = parse()
     if args.impl == "reference":
@@ -595,5 +694,7 @@ if __name__ == "__main__":
         adjoint_main(args)
     elif args.workload == "uneven":
         uneven_main(args)
+    elif args.workload == "pcfit":
+        pcfit_main(args)
     else:
         device_main(args)

@@ -340,6 +340,13 @@ int zeb_refine_list(const float* pats, const float* items, const float* seeds, i
 int zeb_project(const float* master, int side, const float* poses, int n, const zeb_frame_t* fr, float* sims,
                 void* stream);
 
+/* The pattern-centre vote's density (host function, no GPU): n_ballots ballots at integer
+ * candidate coordinates at[b] = (x, y, z) with weights w[b], each spread by a Gaussian of sigma[a]
+ * candidate steps along axis a out to ceil(3 sigma) (clipped to the n[0] × n[1] × n[2] grid) and
+ * added in float32, ballot by ballot: out[x + n0 (y + n1 z)]. Replaces splat
+ * (src/pcfit.zig:210-236). */
+int zeb_pc_splat(const int* at, const double* w, int n_ballots, const int* n, const double* sigma, float* out);
+
 #ifdef __cplusplus
 }
 #endif

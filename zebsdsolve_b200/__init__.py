@@ -191,6 +191,58 @@ class Solver:
         before, after, summary = self._call("tune", self._e.tune, progress)
         return {"before": before, "after": after, "summary": summary}
 
+    # ── the pattern-centre vote ──
+
+    def fit_pc(self):
+        """Fit the pattern centre by the voting search (settings fit_grid, fit_bandwidth, pc_*;
+        __init__.py:426-434): the geometry takes the result. Returns pc, start, score (the fit
+        patterns' mean best correlation at the fitted centre), start_score, n_patterns,
+        n_candidates, levels, at_border."""
+        from . import pcfit
+
+        r = self._call("fit_pc", pcfit.run, self._e)
+        return {"pc": list(r["pc"]), "start": list(r["start"]), "score": r["score"], "start_score": r["start_score"],
+                "n_patterns": r["n_patterns"], "n_candidates": r["n_candidates"], "levels": r["levels"],
+                "at_border": bool(r["at_border"])}
+
+    def pc_scores(self):
+        """The last search grid's votes: (scores[nz, ny, nx], pcx values, pcy values, pcz values)."""
+        h = self._e.pc_history
+        if not h:
+            e = np.zeros(0)
+            return np.zeros((0, 0, 0), np.float32), e, e.copy(), e.copy()
+        x, y, z = h[-1]["axes"]
+        return h[-1]["scores"].reshape(len(z), len(y), len(x)).copy(), x.copy(), y.copy(), z.copy()
+
+    def pc_levels(self):
+        """Every grid the last pattern-centre search scored, in order (__init__.py:446-477): scores,
+        x, y, z, winner (ix, iy, iz), walked, pattern_best (rows of ix, iy, iz), pattern_ncc,
+        pattern_scores[n, nz, ny, nx]; density (None when the mean decided), peak, ballots, inliers."""
+        out = []
+        for lv in self._e.pc_history:
+            x, y, z = lv["axes"]
+            nx, ny, nz = len(x), len(y), len(z)
+
+            def split(c):
+                c = np.asarray(c, np.int64)
+                return np.stack([c % nx, (c // nx) % ny, c // (nx * ny)], -1)
+
+            out.append({"scores": lv["scores"].reshape(nz, ny, nx).copy(), "x": x.copy(), "y": y.copy(), "z": z.copy(),
+                        "pattern_scores": lv["pat_scores"].reshape(-1, nz, ny, nx).copy(),
+                        "density": None if lv["density"] is None else lv["density"].reshape(nz, ny, nx).copy(),
+                        "peak": tuple(float(v) for v in lv["peak"]), "ballots": int(lv["ballots"]),
+                        "inliers": int(lv["inliers"]), "winner": tuple(int(v) for v in split(lv["best"])),
+                        "walked": bool(lv["walked"]), "pattern_best": split(lv["pat_best"]),
+                        "pattern_ncc": lv["pat_ncc"].copy()})
+        return out
+
+    def fit_patterns(self):
+        """The last fit's patterns: (cells, phases, quaternions in the fundamental zone, scores)."""
+        f = self._e.fit
+        if f is None:
+            return np.zeros(0, np.uint64), np.zeros(0, np.int32), np.zeros((0, 4), np.float32), np.zeros(0, np.float32)
+        return f["cells"].astype(np.uint64), f["phase"].copy(), f["quats"].copy(), f["ncc"].copy()
+
     def chance(self, phase=0):
         self._call("chance", self._e.calibrate)
         return float(self._e.chance_med[phase]), float(self._e.chance_spread[phase])
@@ -240,4 +292,4 @@ class Solver:
         return disorientation(qa, qb, self._e.phases[phase].master.rotations())
 
 
-from .api import Result, index  # noqa: E402,F401
+from .api import Result, fit_pattern_center, index  # noqa: E402,F401

@@ -48,18 +48,40 @@ def _open(solver, scan, phases, kwargs):
         solver.add_phase(p)
 
 
+def fit_pattern_center(scan, phases, **kwargs):
+    """Fit the pattern centre by the voting search (api.py:83-93). Returns the fit's report (pc,
+    score, start, …) with the last grid's votes under "scores", its axes under "axes" and the
+    geometry it leaves under "geometry"."""
+    from . import Solver
+
+    s = Solver()
+    try:
+        _open(s, scan, phases, dict(kwargs))
+        r = s.fit_pc()
+        scores, x, y, z = s.pc_scores()
+        r.update(scores=scores, axes=(x, y, z), geometry=s.geometry)
+        return r
+    finally:
+        s.close()
+
+
 def index(scan, phases, fit=None, progress=None, **kwargs):
-    """Index a scan against candidate phases (api.py:111-132). `fit` must be None on this path."""
+    """Index a scan against candidate phases (api.py:111-132). fit: None indexes under the
+    geometry as given; "pc" first fits the pattern centre by the vote; "geometry" (the vote,
+    then the plane of source points) is not part of this engine."""
     from . import Error, Solver
 
     if fit not in (None, "geometry", "pc"):
         raise ValueError('fit is None, "geometry" or "pc"')
-    if fit is not None:
-        raise Error(f"fit={fit!r}: the geometry fits are not part of this engine")
+    if fit == "geometry":
+        raise Error("fit='geometry': the plane fit is not part of this engine")
     s = Solver()
     try:
         _open(s, scan, phases, dict(kwargs))
+        report = {}
+        if fit == "pc":
+            report["pc"] = s.fit_pc()
         r = s.index(progress)
-        return Result(geometry=s.geometry, phases=s.phases, settings=s.settings, fit={}, **r)
+        return Result(geometry=s.geometry, phases=s.phases, settings=s.settings, fit=report, **r)
     finally:
         s.close()

@@ -137,6 +137,8 @@ class Engine:
         self._pin_buf = None  # the page-locked buffer behind _pinned, reused across scans
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
+        self.pc_history = []  # the grids of the last pattern-centre vote (pcfit.run)
+        self.fit = None  # the last fit's patterns: cells, orientations, phases, scores
 
     # ── plumbing ──
 
