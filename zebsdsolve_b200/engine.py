@@ -65,12 +65,15 @@ class Geometry:
         return (tuple(self.pc), self.sample_tilt_deg, self.detector_tilt_deg, tuple(self.rot), self.px_um,
                 self.step_x_um, self.step_y_um)
 
-    def rotation(self):
-        """geometry.zig:141-150 — R0(sample tilt, detector tilt) · Exp(rot)."""
+    def nominal(self):
+        """geometry.zig:141-146 — R0(sample tilt, detector tilt)."""
         a = math.radians(self.detector_tilt_deg - self.sample_tilt_deg)
         s, c = math.sin(a), math.cos(a)
-        r0 = np.array([[-s, 0, c], [0, 1, 0], [-c, 0, -s]])
-        return r0 @ R.to_matrix(R.exp_map(self.rot))
+        return np.array([[-s, 0, c], [0, 1, 0], [-c, 0, -s]])
+
+    def rotation(self):
+        """geometry.zig:141-150 — R0(sample tilt, detector tilt) · Exp(rot)."""
+        return self.nominal() @ R.to_matrix(R.exp_map(self.rot))
 
     def translation(self, rows, cols, pc=None):
         """geometry.zig:153-161 — t in pixels for a pattern of rows × cols."""

@@ -69,6 +69,14 @@ def exp_map(phi):
     return np.concatenate([np.cos(0.5 * th), k * phi], -1)
 
 
+def log_map(q):
+    """so(3) log: the rotation vector of quaternions [..., 4] (rot.zig:201-207)"""
+    q = qstd(q)
+    s = np.linalg.norm(q[..., 1:], axis=-1, keepdims=True)
+    k = np.where(s < 1e-9, 2.0, 2.0 * np.arctan2(s, q[..., :1]) / np.where(s < 1e-9, 1.0, s))
+    return k * q[..., 1:]
+
+
 def to_bunge(q):
     """Bunge (φ1, Φ, φ2) radians of quaternions [..., 4] (rot.zig:151-173)"""
     q = qstd(q)
