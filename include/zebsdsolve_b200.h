@@ -340,6 +340,15 @@ int zeb_refine_list(const float* pats, const float* items, const float* seeds, i
 int zeb_project(const float* master, int side, const float* poses, int n, const zeb_frame_t* fr, float* sims,
                 void* stream);
 
+/* The 43 Gauss–Newton sums of zeb_det6_list (mode 2) with the master taken by `interp`: 0 the
+ * gradient table (gpair, bilinear), 1 bicubic (Catmull–Rom) or 2 Keys' six-point cubic convolution
+ * of the sheets themselves (sheets [2][side][side]), each with its own surface's gradient on the
+ * sphere. Replaces Detector.sumsOf with settings.plane_interp (src/detector.zig:145-159;
+ * shaders/detector.wgsl sums 435-499, grad_at_cubic / grad_at_keys6 146-248). */
+int zeb_sums6_list(const float* pats, const float* items, int n, const zeb_frame_t* fr, const uint32_t* list,
+                   int npix, const float* sheets, const float* gpair, int side, int interp, const float* x,
+                   const float* q0, float* out, void* stream);
+
 /* The pattern-centre vote's density (host function, no GPU): n_ballots ballots at integer
  * candidate coordinates at[b] = (x, y, z) with weights w[b], each spread by a Gaussian of sigma[a]
  * candidate steps along axis a out to ceil(3 sigma) (clipped to the n[0] × n[1] × n[2] grid) and

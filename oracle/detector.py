@@ -314,18 +314,85 @@ def decoy(b, draw):
 
 # ── six unknowns per pattern: the source's shift and the crystal's rotation ──
 
-def sums6(grad, side, frame, t, q, shift, pattern, mask):
+def _catmull_rom(t):
+    """Catmull–Rom weights of the texels at −1, 0, 1, 2 and their slopes (detector.wgsl:161-164)."""
+    w = 0.5 * np.stack([((-t + 2) * t - 1) * t, (3 * t - 5) * t * t + 2, ((-3 * t + 4) * t + 1) * t, (t - 1) * t * t], -1)
+    d = 0.5 * np.stack([(-3 * t + 4) * t - 1, (9 * t - 10) * t, (-9 * t + 8) * t + 1, (3 * t - 2) * t], -1)
+    return w, d
+
+
+def _keys(a):
+    """Keys' six-point kernel at a ≥ 0 and its slope (detector.wgsl:193-198)."""
+    v = np.where(a < 1, ((4 / 3) * a - 7 / 3) * a * a + 1,
+                 np.where(a < 2, ((-7 / 12 * a + 3) * a - 59 / 12) * a + 2.5,
+                          np.where(a < 3, ((1 / 12 * a - 2 / 3) * a + 1.75) * a - 1.5, 0.0)))
+    d = np.where(a < 1, (4 * a - 14 / 3) * a,
+                 np.where(a < 2, (-1.75 * a + 6) * a - 59 / 12, np.where(a < 3, (0.25 * a - 4 / 3) * a + 1.75, 0.0)))
+    return v, d
+
+
+def grad_smooth(sheets, side, v, kind):
+    """detector.wgsl:141-248 (grad_at_cubic, kind 1; grad_at_keys6, kind 2) — the master at
+    directions v [n, 3] by a smooth kernel over the sheet's texels (indices held inside the sheet),
+    with that surface's gradient carried onto the sphere by central differences of the square-
+    Lambert map (1e-3 rad along two tangent directions). Returns [n, 4]: gradient, intensity."""
+    v = np.asarray(v, np.float64)
+    tab = np.asarray(sheets, np.float64).reshape(2, side, side)
+    uv = sphere_to_square(v)
+    last = float(side - 1)
+    fj = np.clip((uv[:, 0] + 1.0) * 0.5 * last, 0.0, last)
+    fi = np.clip((uv[:, 1] + 1.0) * 0.5 * last, 0.0, last)
+    c0 = np.minimum(np.floor(fj).astype(np.int64), side - 2)
+    r0 = np.minimum(np.floor(fi).astype(np.int64), side - 2)
+    sh = (v[:, 2] < 0).astype(np.int64)
+    tj, ti = fj - c0, fi - r0
+    if kind == 1:
+        wj, dj = _catmull_rom(tj)
+        wi, di = _catmull_rom(ti)
+        offs = np.arange(-1, 3)
+    else:
+        sj = tj[:, None] - (np.arange(6) - 2)[None, :]
+        si = ti[:, None] - (np.arange(6) - 2)[None, :]
+        wj, dj = _keys(np.abs(sj))
+        wi, di = _keys(np.abs(si))
+        dj, di = dj * np.sign(sj), di * np.sign(si)
+        offs = np.arange(-2, 4)
+    rr = np.clip(r0[:, None] + offs[None, :], 0, side - 1)
+    cc = np.clip(c0[:, None] + offs[None, :], 0, side - 1)
+    T = tab[sh[:, None, None], rr[:, :, None], cc[:, None, :]]  # [n][a][b]
+    val = np.einsum("na,nb,nab->n", wi, wj, T)
+    gj = np.einsum("na,nb,nab->n", wi, dj, T)
+    gi = np.einsum("na,nb,nab->n", di, wj, T)
+    e1 = np.cross(v, np.array([0.0, 0.0, 1.0]))
+    small = (e1 * e1).sum(-1) < 1e-4
+    e1[small] = np.cross(v[small], np.array([1.0, 0.0, 0.0]))
+    e1 /= np.linalg.norm(e1, axis=-1, keepdims=True)
+    e2 = np.cross(v, e1)
+    h = 1e-3
+    k = 0.5 * last / (2 * h)
+
+    def s2s(x):
+        return sphere_to_square(x / np.linalg.norm(x, axis=-1, keepdims=True))
+
+    d1 = (s2s(v + h * e1) - s2s(v - h * e1)) * k
+    d2 = (s2s(v + h * e2) - s2s(v - h * e2)) * k
+    g = e1 * (gj * d1[:, 0] + gi * d1[:, 1])[:, None] + e2 * (gj * d2[:, 0] + gi * d2[:, 1])[:, None]
+    return np.concatenate([g, val[:, None]], 1)
+
+
+def sums6(grad, side, frame, t, q, shift, pattern, mask, interp=0, sheets=None):
     """detector.wgsl:435-499 (sums) — the 43 sums over the masked pixels at orientation q with the
     rays' origin moved by `shift` (pixels, sample axes): with u = c0·row + c1·col + t + shift,
     c = q·u/|u| and (∇M, M) = grad(c), the directions d = (q⁻¹·∇M/|u|, c × ∇M); sums
-    n, ΣM, ΣM², ΣM·e, Σd (6), ΣM·d (6), Σe·d (6), Σd_i d_j (i ≤ j, 21)."""
+    n, ΣM, ΣM², ΣM·e, Σd (6), ΣM·d (6), Σe·d (6), Σd_i d_j (i ≤ j, 21). interp 1 or 2: the
+    master by grad_smooth of the raw sheets instead of the gradient table (plane_interp)."""
     h, w = pattern.shape
     m_ = in_mask(h, w, mask)
     u = (rays(h, w, frame, np.asarray(t, np.float64) + np.asarray(shift, np.float64)))[m_]
     dist = np.linalg.norm(u, axis=-1, keepdims=True)
     q = np.asarray(q, np.float64)
     c = rot.qapply(q, u / dist)
-    g = sheet_lookup(grad, side, c)
+    g = sheet_lookup(grad, side, c) if interp == 0 else grad_smooth(sheets, side, c, interp)
     val = g[:, 3]
     a = np.cross(c, g[:, :3])
     wv = rot.qapply(rot.qconj(q), g[:, :3]) / dist

@@ -223,5 +223,5 @@ def test_index_with_the_vote_first(scan):
     assert r.fit["pc"]["pc"] == r.geometry["pc"]
     f = ze.fit_pattern_center(scan["pats"], [scan["path"]], pc=START, sample_tilt_deg=70, detector_tilt_deg=0)
     assert np.abs(np.array(f["pc"]) - TRUTH).max() < 0.012 and f["scores"].ndim == 3 and len(f["axes"]) == 3
-    with pytest.raises(ze.Error, match="plane fit"):
-        ze.index(scan["pats"], [scan["path"]], fit="geometry")
+    with pytest.raises(ValueError):
+        ze.index(scan["pats"], [scan["path"]], fit="plane")

@@ -90,7 +90,10 @@ class Solver:
         return self._e.geo.as_dict()
 
     def set_geometry(self, **fields):
-        self._call("set_geometry", self._e.geo.set, **fields)
+        """Set any of the geometry's fields (pc, rot, sample_tilt_deg, detector_tilt_deg, px_um,
+        step_x_um, step_y_um, plane_kind, plane). A pattern centre set by hand is one for the whole
+        map again (the plane of source points goes unless one comes with it)."""
+        self._call("set_geometry", self._e.geo.given, fields, self._e.geo_given)
         return self
 
     # ── scan ──
@@ -236,6 +239,59 @@ class Solver:
                         "pattern_ncc": lv["pat_ncc"].copy()})
         return out
 
+    # ── the plane of source points ──
+
+    def fit_plane(self):
+        """Fit the plane of source points (planefit.zig; __init__.py:487-523): every plane_stride-th
+        cell each way (at most plane_patterns_max) fitted by itself, its orientation and the place
+        of its own source, from the geometry as it stands; then the transformation of the scan's
+        indices through those points (plane_kind affine or projective; plane_method "points"), or
+        fitted to all the patterns at once ("joint"). The geometry takes the plane. Returns the
+        reference's dict: plane (4 × 3), kind, frame, model, method, pc, pc_se, start_pc, rot,
+        n_patterns, n_used, rmsd, ncc, start_ncc, iterations, said (rot, rot_se, sample_tilt_deg,
+        sample_tilt_se_deg, step, step_se, skew, skew_se, blocks)."""
+        from . import planefit
+
+        return self._plane_result(self._call("fit_plane", planefit.fit_plane, self._e))
+
+    def fit_geometry(self):
+        """The automatic fit from the geometry as it was given (set_geometry): the vote for the
+        pattern centre, then the fit patterns' own source points from there and the simplest model
+        of how they move over the scan the map supports (one centre with the scan's steps, a tilt
+        line, or the plane); `models` gives each one's cross-validated error (cv, cv_se)."""
+        from . import planefit
+
+        return self._plane_result(self._call("fit_geometry", planefit.auto, self._e))
+
+    def _plane_result(self, r):
+        import math
+
+        models = ("centre", "line", "affine", "projective")
+        g = self.geometry
+        se = r["se"]
+        sd = r["said"]
+        return {"plane": r["plane"].copy(), "kind": ("none", "affine", "projective")[r["kind"]],
+                "frame": "follow" if r["frame"] else "nominal", "model": r["model"], "method": r["method"],
+                "models": {m: {"cv": r["cv"][i], "cv_se": r["cv_se"][i]} for i, m in enumerate(models)
+                           if r["compared"] and r["cv"][i] > 0},
+                "pc": list(r["pc"]), "pc_se": list(se[6:9]), "start_pc": r["start_pc"], "rot": r["rot"],
+                "n_patterns": r["n_patterns"], "n_used": r["n_used"], "rmsd": list(r["rmsd"]), "ncc": r["ncc"],
+                "start_ncc": r["start_ncc"], "iterations": r["iterations"],
+                "said": {"rot": list(sd["rot"]), "rot_se": list(se[0:3]),
+                         "sample_tilt_deg": g["sample_tilt_deg"] - math.degrees(sd["rot"][1]),
+                         "sample_tilt_se_deg": math.degrees(se[1]), "step": list(sd["step"]), "step_se": list(se[3:5]),
+                         "skew": sd["skew"], "skew_se": float(se[5]), "blocks": r["blocks"]}}
+
+    def plane_points(self):
+        """The source points the last plane fit measured, one a fit pattern: cells, pc (n × 3: where
+        each pattern's own fit put its source), fit (n × 3: where the plane has it), ncc, used."""
+        p = self._e.plane_points
+        if p is None:
+            z = np.zeros((0, 3))
+            return {"cells": np.zeros(0, np.uint64), "pc": z, "fit": z.copy(), "ncc": np.zeros(0),
+                    "used": np.zeros(0, bool)}
+        return {k: v.copy() for k, v in p.items()}
+
     def fit_patterns(self):
         """The last fit's patterns: (cells, phases, quaternions in the fundamental zone, scores)."""
         f = self._e.fit
@@ -292,4 +348,4 @@ class Solver:
         return disorientation(qa, qb, self._e.phases[phase].master.rotations())
 
 
-from .api import Result, fit_pattern_center, index  # noqa: E402,F401
+from .api import Result, fit_pattern_center, fit_plane, index  # noqa: E402,F401

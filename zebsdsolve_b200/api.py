@@ -65,22 +65,37 @@ def fit_pattern_center(scan, phases, **kwargs):
         s.close()
 
 
+def fit_plane(scan, phases, **kwargs):
+    """Fit the plane of source points from the pattern centre as given (api.py:96-108). Returns the
+    fit's report with the final "geometry" and the measured "points" (Solver.plane_points)."""
+    from . import Solver
+
+    s = Solver()
+    try:
+        _open(s, scan, phases, dict(kwargs))
+        r = s.fit_plane()
+        r.update(geometry=s.geometry, points=s.plane_points())
+        return r
+    finally:
+        s.close()
+
+
 def index(scan, phases, fit=None, progress=None, **kwargs):
     """Index a scan against candidate phases (api.py:111-132). fit: None indexes under the
-    geometry as given; "pc" first fits the pattern centre by the vote; "geometry" (the vote,
-    then the plane of source points) is not part of this engine."""
-    from . import Error, Solver
+    geometry as given; "geometry" first fits it by itself (Solver.fit_geometry: the vote for the
+    pattern centre, then the plane of source points); "pc" fits the pattern centre by the vote."""
+    from . import Solver
 
     if fit not in (None, "geometry", "pc"):
         raise ValueError('fit is None, "geometry" or "pc"')
-    if fit == "geometry":
-        raise Error("fit='geometry': the plane fit is not part of this engine")
     s = Solver()
     try:
         _open(s, scan, phases, dict(kwargs))
         report = {}
         if fit == "pc":
             report["pc"] = s.fit_pc()
+        if fit == "geometry":
+            report["geometry"] = s.fit_geometry()
         r = s.index(progress)
         return Result(geometry=s.geometry, phases=s.phases, settings=s.settings, fit=report, **r)
     finally:

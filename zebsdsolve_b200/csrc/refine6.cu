@@ -31,7 +31,123 @@ struct Det6Args {
   const float* x;   // [n][6]: δt (3, pixels), φ (3, radians)
   const float* q0;  // [n][4] (w, x, y, z)
   float* out;       // MODE 0: [n]; MODE 1: [n][7] (∂NCC/∂x, NCC); MODE 2: [n][43]
+  const float* sheets;  // MODE 2 with interp 1 or 2: the master's two sheets [2][side][side]
+  int interp;           // MODE 2: 0 the gradient table (bilinear), 1 bicubic, 2 Keys' six-point
 };
+
+// ── the master sampled by a smooth kernel, with that surface's own gradient on the sphere ──
+//
+// The plane fit's sums may take the master by bicubic (Catmull–Rom) or by Keys' six-point cubic
+// convolution (Keys 1981, fourth-order accurate) instead of the bilinear gradient table
+// (detector.wgsl grad_at_cubic / grad_at_keys6, 146-248): the intensity is then smooth across the
+// sheet's pixels, and the gradient is the derivative of the same surface. The sheet's
+// coordinates are carried onto the sphere by central differences of the square-Lambert map
+// along two tangent directions, 1e-3 rad either way.
+
+// one texel of the hemisphere's sheet at offset o, the indices held inside the sheet
+__device__ __forceinline__ float sheet_texel(const float* __restrict__ s, int o, int r, int c, int side) {
+  r = min(max(r, 0), side - 1);
+  c = min(max(c, 0), side - 1);
+  return __ldg(s + o + r * side + c);
+}
+
+// Catmull–Rom weights of the four texels at −1, 0, 1, 2 from the cell's corner, and their slopes
+__device__ __forceinline__ void catmull_rom(float t, float (&w)[4], float (&d)[4]) {
+  const float t2 = t * t, t3 = t2 * t;
+  w[0] = 0.5f * (-t3 + 2.f * t2 - t);
+  w[1] = 0.5f * (3.f * t3 - 5.f * t2 + 2.f);
+  w[2] = 0.5f * (-3.f * t3 + 4.f * t2 + t);
+  w[3] = 0.5f * (t3 - t2);
+  d[0] = 0.5f * (-3.f * t2 + 4.f * t - 1.f);
+  d[1] = 0.5f * (9.f * t2 - 10.f * t);
+  d[2] = 0.5f * (-9.f * t2 + 8.f * t + 1.f);
+  d[3] = 0.5f * (3.f * t2 - 2.f * t);
+}
+
+// Keys' six-point kernel at distance a ≥ 0 and its slope (cubic pieces on [0,1), [1,2), [2,3))
+__device__ __forceinline__ float2 keys_kernel(float a) {
+  if (a < 1.f) return make_float2((4.f / 3.f * a - 7.f / 3.f) * a * a + 1.f, (4.f * a - 14.f / 3.f) * a);
+  if (a < 2.f)
+    return make_float2(((-7.f / 12.f * a + 3.f) * a - 59.f / 12.f) * a + 2.5f, (-1.75f * a + 6.f) * a - 59.f / 12.f);
+  if (a < 3.f)
+    return make_float2(((1.f / 12.f * a - 2.f / 3.f) * a + 1.75f) * a - 1.5f, (0.25f * a - 4.f / 3.f) * a + 1.75f);
+  return make_float2(0.f, 0.f);
+}
+
+__device__ __forceinline__ float3 unit3(float3 v) {
+  const float r = rsqrtf(dot3(v, v));
+  return make_float3(v.x * r, v.y * r, v.z * r);
+}
+
+// (intensity, gradient on the sphere) of the master at direction v by the smooth kernel KIND
+// (1 Catmull–Rom, 2 Keys' six-point): .xyz the gradient, .w the intensity
+template <int KIND>
+__device__ float4 grad_smooth(const float* __restrict__ sheets, float3 v, int side) {
+  const float2 uv = sphere_to_square(v);
+  const float last = (float)(side - 1);
+  const float fj = fminf(fmaxf((uv.x + 1.f) * 0.5f * last, 0.f), last);
+  const float fi = fminf(fmaxf((uv.y + 1.f) * 0.5f * last, 0.f), last);
+  const int c0 = min((int)fj, side - 2), r0 = min((int)fi, side - 2);
+  const int o = v.z < 0.f ? side * side : 0;
+  const float tj = fj - (float)c0, ti = fi - (float)r0;
+  float val = 0.f, gj = 0.f, gi = 0.f;
+  if (KIND == 1) {
+    float wj[4], dj[4], wi[4], di[4];
+    catmull_rom(tj, wj, dj);
+    catmull_rom(ti, wi, di);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      float row = 0.f, drow = 0.f;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const float t = sheet_texel(sheets, o, r0 - 1 + a, c0 - 1 + b, side);
+        row += wj[b] * t;
+        drow += dj[b] * t;
+      }
+      val += wi[a] * row;
+      gj += wi[a] * drow;
+      gi += di[a] * row;
+    }
+  } else {
+    float wj[6], dj[6], wi[6], di[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      const float sj = tj - (float)(m - 2), si = ti - (float)(m - 2);
+      const float2 kj = keys_kernel(fabsf(sj)), ki = keys_kernel(fabsf(si));
+      wj[m] = kj.x;
+      dj[m] = sj < 0.f ? -kj.y : (sj > 0.f ? kj.y : 0.f);
+      wi[m] = ki.x;
+      di[m] = si < 0.f ? -ki.y : (si > 0.f ? ki.y : 0.f);
+    }
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+      float row = 0.f, drow = 0.f;
+#pragma unroll
+      for (int b = 0; b < 6; ++b) {
+        const float t = sheet_texel(sheets, o, r0 - 2 + a, c0 - 2 + b, side);
+        row += wj[b] * t;
+        drow += dj[b] * t;
+      }
+      val += wi[a] * row;
+      gj += wi[a] * drow;
+      gi += di[a] * row;
+    }
+  }
+  // two directions across v, and how the sheet's coordinates move along them
+  float3 e1 = cross3(v, make_float3(0.f, 0.f, 1.f));
+  if (dot3(e1, e1) < 1e-4f) e1 = cross3(v, make_float3(1.f, 0.f, 0.f));
+  e1 = unit3(e1);
+  const float3 e2 = cross3(v, e1);
+  const float h = 1e-3f, k = 0.5f * last / (2.f * h);
+  const float2 p1 = sphere_to_square(unit3(make_float3(v.x + h * e1.x, v.y + h * e1.y, v.z + h * e1.z)));
+  const float2 m1 = sphere_to_square(unit3(make_float3(v.x - h * e1.x, v.y - h * e1.y, v.z - h * e1.z)));
+  const float2 p2 = sphere_to_square(unit3(make_float3(v.x + h * e2.x, v.y + h * e2.y, v.z + h * e2.z)));
+  const float2 m2 = sphere_to_square(unit3(make_float3(v.x - h * e2.x, v.y - h * e2.y, v.z - h * e2.z)));
+  const float2 d1 = make_float2((p1.x - m1.x) * k, (p1.y - m1.y) * k);
+  const float2 d2 = make_float2((p2.x - m2.x) * k, (p2.y - m2.y) * k);
+  const float a1 = gj * d1.x + gi * d1.y, a2 = gj * d2.x + gi * d2.y;
+  return make_float4(e1.x * a1 + e2.x * a2, e1.y * a1 + e2.y * a2, e1.z * a1 + e2.z * a2, val);
+}
 
 // ∂(fj, fi)/∂c of the sheet coordinates fj = (U + 1)/2·last, fi = (W + 1)/2·last of direction c
 // (sphere_to_square, common.wgsl:44-57), from the map's own formula; zero where clamped or at
@@ -110,7 +226,9 @@ __device__ __forceinline__ void det6_pixel(const Det6Args& a, float4 q, float4 q
     if (MODE == 1) {
       m = master_and_slope(a.vpair, c, a.side, g);
     } else {
-      const float4 gm = grad_at_pair(a.gpair, c, a.side);
+      const float4 gm = a.interp == 0   ? grad_at_pair(a.gpair, c, a.side)
+                        : a.interp == 1 ? grad_smooth<1>(a.sheets, c, a.side)
+                                        : grad_smooth<2>(a.sheets, c, a.side);
       m = gm.w;
       g = make_float3(gm.x, gm.y, gm.z);
     }
@@ -398,6 +516,34 @@ extern "C" int zeb_det6_list(int mode, const float* pats, const float* items, in
     k_det6_list<2><<<n, 128, smem, st>>>(a, list, npix);
   }
   return zeb_launch_check("det6_list");
+}
+
+extern "C" int zeb_sums6_list(const float* pats, const float* items, int n, const zeb_frame_t* fr,
+                              const uint32_t* list, int npix, const float* sheets, const float* gpair, int side,
+                              int interp, const float* x, const float* q0, float* out, void* stream) {
+  ZEB_REQUIRE(interp >= 0 && interp <= 2, ZEB_EARG, "sums6_list: interp %d", interp);
+  ZEB_REQUIRE(pats && items && list && x && q0 && out && fr && side >= 3 && (interp != 0 || gpair) &&
+                  (interp == 0 || sheets),
+              ZEB_EARG, "sums6_list: bad arguments");
+  ZEB_REQUIRE(((uintptr_t)gpair & 31) == 0, ZEB_EARG, "sums6_list: gradient pairs misaligned");
+  ZEB_REQUIRE(npix == zeb_mask_count(fr), ZEB_EARG, "sums6_list: %d pixels listed, the frame masks %d", npix,
+              zeb_mask_count(fr));
+  const size_t smem = (size_t)npix * sizeof(float);
+  ZEB_REQUIRE(npix >= 1 && smem <= 200 * 1024, ZEB_ESIZE, "sums6_list: %d pixels (at most 51200)", npix);
+  if (n <= 0) return ZEB_OK;
+  Det6Args a{};
+  ZEB_REQUIRE(fr->h >= 2 && fr->w >= 2 && fr->h < 65536 && fr->w < 65536, ZEB_EARG, "sums6_list: bad frame");
+  a.h = fr->h; a.w = fr->w;
+  a.c0 = make_float3(fr->c0[0], fr->c0[1], fr->c0[2]);
+  a.c1 = make_float3(fr->c1[0], fr->c1[1], fr->c1[2]);
+  a.c2 = make_float3(fr->c2[0], fr->c2[1], fr->c2[2]);
+  for (int k = 0; k < 3; ++k) a.mask[k] = fr->mask[k];
+  a.pats = pats; a.items = (const float4*)items; a.n = n; a.gpair = gpair; a.sheets = sheets; a.interp = interp;
+  a.side = side; a.x = x; a.q0 = q0; a.out = out;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_det6_list<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_det6_list<2><<<n, 128, smem, st>>>(a, list, npix);
+  return zeb_launch_check("sums6_list");
 }
 
 extern "C" int zeb_solve6(const double* A, const double* b, int n, double* x, int* ok, void* stream) {

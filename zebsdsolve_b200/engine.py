@@ -30,9 +30,12 @@ class EngineError(RuntimeError):
 
 
 class Geometry:
-    """geometry.zig:113-193 — one detector pose and per-cell beam offsets."""
+    """geometry.zig:113-193 — one detector pose, per-cell beam offsets, and (after a plane fit)
+    the plane of source points that replaces them: plane_kind 0 none, 1 affine, 2 projective;
+    plane P (12, row-major 4 × 3) with P · (column, row, 1) = w · (PCx, PCy, PCz, 1)."""
 
     FIELDS = ("pc", "sample_tilt_deg", "detector_tilt_deg", "rot", "px_um", "step_x_um", "step_y_um")
+    KINDS = ("none", "affine", "projective")
 
     def __init__(self):
         self.pc = np.array([0.5, 0.5, 0.5])
@@ -42,12 +45,19 @@ class Geometry:
         self.px_um = 0.0
         self.step_x_um = 1.0
         self.step_y_um = 1.0
+        self.plane_kind = 0
+        self.plane = np.zeros(12)
+
+    def copy(self):
+        g = Geometry()
+        g.__dict__.update({k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items()})
+        return g
 
     def as_dict(self):
         return {"pc": list(map(float, self.pc)), "sample_tilt_deg": self.sample_tilt_deg,
                 "detector_tilt_deg": self.detector_tilt_deg, "rot": list(map(float, self.rot)), "px_um": self.px_um,
-                "step_x_um": self.step_x_um, "step_y_um": self.step_y_um, "plane_kind": "none",
-                "plane": [[0.0, 0.0, 0.0]] * 3 + [[0.0, 0.0, 1.0]]}
+                "step_x_um": self.step_x_um, "step_y_um": self.step_y_um, "plane_kind": self.KINDS[self.plane_kind],
+                "plane": [list(map(float, self.plane[3 * k:3 * k + 3])) for k in range(4)]}
 
     def set(self, **kw):
         for k, v in kw.items():
@@ -56,14 +66,31 @@ class Geometry:
                 setattr(self, k, a)
             elif k in self.FIELDS:
                 setattr(self, k, float(v))
-            elif k in ("plane_kind", "plane"):
-                continue
+            elif k == "plane_kind":
+                self.plane_kind = self.KINDS.index(v) if isinstance(v, str) else int(v)
+            elif k == "plane":
+                self.plane = np.asarray(v, np.float64).reshape(12).copy()
             else:
                 raise EngineError(f"geometry has no field {k!r}")
 
+    def given(self, kw, given):
+        """exports.zig:131-155 — set_geometry's fields: a pattern centre set by hand (changed,
+        with no other plane given) is one for the whole map again, the scan's steps saying how the
+        beam went from it; the fields the caller changed are recorded in `given` (the geometry an
+        automatic fit starts from)."""
+        was = self.copy()
+        self.set(**kw)
+        pc_changed = not np.array_equal(self.pc, was.pc)
+        if pc_changed and np.array_equal(self.plane, was.plane) and self.plane_kind == was.plane_kind:
+            self.plane_kind = 0
+        for k in self.FIELDS:
+            a, b = getattr(self, k), getattr(was, k)
+            if not np.array_equal(a, b):
+                setattr(given, k, a.copy() if isinstance(a, np.ndarray) else a)
+
     def key(self):
         return (tuple(self.pc), self.sample_tilt_deg, self.detector_tilt_deg, tuple(self.rot), self.px_um,
-                self.step_x_um, self.step_y_um)
+                self.step_x_um, self.step_y_um, self.plane_kind, tuple(self.plane) if self.plane_kind else ())
 
     def nominal(self):
         """geometry.zig:141-146 — R0(sample tilt, detector tilt)."""
@@ -140,7 +167,9 @@ class Engine:
         self._pin_buf = None  # the page-locked buffer behind _pinned, reused across scans
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
+        self.geo_given = Geometry()  # the geometry as given (set_geometry), where a full fit starts
         self.pc_history = []  # the grids of the last pattern-centre vote (pcfit.run)
+        self.plane_points = None  # the source points of the last plane fit
         self.fit = None  # the last fit's patterns: cells, orientations, phases, scores
 
     # ── plumbing ──
@@ -214,15 +243,28 @@ class Engine:
         fr.mask[0], fr.mask[1], fr.mask[2] = self.mask_of(h, w)
         return fr
 
-    def positions(self, cells):
+    def positions(self, cells, geo=None):
         """engine.zig:1601-1613 — the detector position for each cell, in pixels (float32)."""
+        return self.positions64(cells, geo).astype(np.float32)
+
+    def positions64(self, cells, geo=None):
+        """The detector position for each cell (FP64; geometry.zig:80-83): the plane of source
+        points' where the geometry has one, else the reference cell's less the beam's travel."""
         rows, cols, h, w = self.info()
         b = self.set["binning"]
+        g = self.geo if geo is None else geo
         cells = np.asarray(cells, np.int64)
-        t = self.geo.translation(h / b, w / b)
-        off = self.geo.scan_offsets(cells // cols, cells % cols, 0.5 * (rows - 1), 0.5 * (cols - 1),
-                                    self.set["scan_x_sign"], self.set["scan_y_sign"], b)
-        return (t[None, :] - off).astype(np.float32)
+        if g.plane_kind:
+            from .plane import at
+
+            pc = at(g.plane, cells // cols, cells % cols)  # [n][3]
+            Rm = g.rotation()
+            v = np.stack([0.5 - pc[:, 1] * (h / b), 0.5 - pc[:, 0] * (w / b), pc[:, 2] * (h / b)], 1)
+            return v @ Rm.T
+        t = g.translation(h / b, w / b)
+        off = g.scan_offsets(cells // cols, cells % cols, 0.5 * (rows - 1), 0.5 * (cols - 1),
+                             self.set["scan_x_sign"], self.set["scan_y_sign"], b)
+        return t[None, :] - off
 
     def lattice(self, want):
         """engine.zig:1325-1341 — about `want` cells on a lattice over the map."""

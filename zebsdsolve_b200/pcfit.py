@@ -442,7 +442,10 @@ def run(e, timer=None):
     mark("end")
     lo = history[-1]["scored"][0]
     q, ph, ncc = sc.poses(best - lo)
+    # (the vote moves one pattern centre, the scan's steps saying how the beam went from it: a
+    # plane fitted before goes)
     e.geo.pc = np.array(res["pc"], np.float64)
+    e.geo.plane_kind = 0
     e.pc_history = history
     e.fit = {"cells": cells, "quats": q, "phase": ph, "ncc": ncc}
     e.log(f"pattern centre {res['pc'][0]:.5f} {res['pc'][1]:.5f} {res['pc'][2]:.5f}  mean NCC {res['score']:.4f} "
