@@ -56,11 +56,11 @@ def parse():
     ap.add_argument("--batch", type=int, default=16384, help="patterns per device pass in the value measurement")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit"),
+    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit", "plane"),
                     help="index: the scan of 60x60 patterns (the headline); adjoint: six-unknown refinement "
                          "of 120x120 patterns with jittered pattern centres; uneven: many scans of uneven "
                          "lengths and detector sizes, two phases; pcfit: the pattern-centre vote at its default "
-                         "settings")
+                         "settings; plane: the plane of source points (fit_plane, fit_geometry)")
     ap.add_argument("--scans", type=int, default=16, help="uneven: number of scans")
     ap.add_argument("--max-count", type=int, default=20000, help="uneven: the longest scan (log-uniform from 1000)")
     return ap.parse_args()
@@ -686,6 +686,92 @@ def pcfit_main(a):
     print(json.dumps(line), flush=True)
 
 
+def plane_cpu_sample(seconds, grad, side, frame, t, q, pats, mask):
+    """The oracle's settle of one fit pattern over six unknowns (FP64 NumPy), on one host core."""
+    import oracle.detector as od
+
+    done, t0 = 0, time.perf_counter()
+    while done < 1 or time.perf_counter() - t0 < seconds:
+        od.settle6(grad, side, frame, t, q[done % len(q)], pats[done % len(q)], mask, 3.0, 60)
+        done += 1
+    dt = time.perf_counter() - t0
+    return done / dt, f"{done} fit patterns of 60x60 settled over six unknowns by the FP64 oracle"
+
+
+def plane_main(a):
+    """The plane of source points at the reference's default settings (every 2nd cell each way,
+    points method, information weights, bicubic master, the master's pixel chosen of five widths)
+    on a 100 x 100 map of 60 x 60 patterns simulated with the beam travelling 25 um a step on 60 um
+    detector pixels, Gaussian noise as strong as the signal, from a pattern centre 0.005 off: fit
+    patterns refined per second of the whole fit (indexing them at fit_bandwidth 64, the
+    settles, the plane, its standard errors); then the automatic fit (the vote, then the plane
+    with the model the map supports) timed the same way."""
+    import torch
+
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import synthetic as syn
+    from zebsdsolve_b200.master import write_npz
+
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp()
+    write_npz(f"{tmp}/m432.npz", syn.master_sheets(2, side=401, lmax=96, group="432", device="cuda"), 401,
+              syn.group_matrices("432"), 30)
+    rows = cols = 100
+    geo = dict(sample_tilt_deg=70.0, detector_tilt_deg=0.0, px_um=60.0, step_x_um=25.0, step_y_um=25.0)
+    s = ze.Solver()
+    s.configure(bandwidth=L, precision=a.precision)
+    s.add_phase(f"{tmp}/m432.npz")
+    s.set_patterns(np.zeros((rows, cols, H, W), np.float32))
+    s.set_geometry(pc=PC, **geo)
+    rng = np.random.default_rng(600)
+    q, _ = syn.grain_map(rng, rows, cols, 40, SPREAD_DEG)
+    sims = s._e.simulate_device(0, np.arange(rows * cols), q)
+    sims = sims + sims.std() * torch.randn(sims.shape, device=sims.device, generator=torch.Generator("cuda").manual_seed(6))
+    s.set_patterns(sims.cpu().numpy().astype(np.float32).reshape(rows, cols, H, W))
+    start = (PC[0] + 0.005, PC[1] - 0.004, PC[2] + 0.004)
+    out = {}
+    for name, call in (("fit_plane", s.fit_plane), ("fit_geometry", s.fit_geometry)):
+        times = []
+        for i in range(max(1, a.warmup) + max(1, a.steps)):
+            s.set_geometry(pc=start)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = call()
+            torch.cuda.synchronize()
+            if i >= max(1, a.warmup):
+                times.append(time.perf_counter() - t0)
+        dt = float(np.median(times))
+        out[name] = {"s_per_fit": round(dt, 4), "fit_patterns": r["n_patterns"], "used": r["n_used"],
+                     "rounds": r["iterations"], "model": r["model"], "pc_error": round(float(np.abs(np.array(r["pc"]) - PC).max()), 5),
+                     "ncc": round(r["ncc"], 4), "start_ncc": round(r["start_ncc"], 4),
+                     "value": round(r["n_patterns"] / dt, 1)}
+    line = {"metric": "fit patterns/s in the plane fit (each refined over six unknowns, then the plane), 1 B200",
+            "value": out["fit_plane"]["value"], "unit": "patterns/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{rows}x{cols} map of 60x60 patterns simulated at pc {PC} with the beam travelling "
+                                   "(25 um steps, 60 um pixels), Gaussian noise as strong as the signal, start 0.005 "
+                                   "off; plane_stride 2, points, information weights, bicubic, master pixel auto"},
+            "fit_plane": out["fit_plane"], "fit_geometry": out["fit_geometry"]}
+    if not a.no_cpu:
+        import oracle.detector as od
+        import oracle.geometry as og
+
+        e = s._e
+        e.prepare_masters()
+        baked = e.phases[0].baked[1].cpu().numpy().astype(np.float64)
+        gq = og.Geometry(pc=PC, sample_tilt_deg=70.0)
+        mask = og.mask_of(H, W)
+        pats = [np.asarray(e.patterns.reshape(-1, H, W)[k], np.float64) for k in range(4)]
+        import oracle.prep as op
+
+        pats = [op.normalize(p, mask) for p in pats]
+        v, sample = plane_cpu_sample(a.cpu_seconds, od.gradient_table(baked, 401), 401, gq.frame(),
+                                     gq.translation(H, W), q[:4], pats, mask)
+        line["cpu_baseline"] = {"value": round(v, 3), "unit": "patterns/s", "cores": 1, "kind": "port",
+                                "sample": sample}
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     args = parse()
     if args.impl == "reference":
@@ -696,5 +782,7 @@ if __name__ == "__main__":
         uneven_main(args)
     elif args.workload == "pcfit":
         pcfit_main(args)
+    elif args.workload == "plane":
+        plane_main(args)
     else:
         device_main(args)

@@ -472,15 +472,15 @@ def damped(H, g, lam):
     return A, np.array(g, np.float64)
 
 
-def settle6(grad, side, frame, t, q0, pattern, mask, trust, most):
+def settle6(grad, side, frame, t, q0, pattern, mask, trust, most, interp=0, sheets=None):
     """planefit.zig:570-622 (settle, k = 6) for one pattern: Levenberg–Marquardt on its own score
     over the source's shift and its rotation: λ from 1e-3, a step kept where the score rose
     (λ ← max(λ/3, 1e-4)), else λ ← min(5λ, 1e8); the shift clamped to ±trust pixels; stops when
     a round gains less than 1e-7 (a round whose step overshot goes again while λ < 1e8) or after
-    `most` rounds. Returns (q, shift, ncc, rounds)."""
+    `most` rounds. interp / sheets: the master as sums6 takes it. Returns (q, shift, ncc, rounds)."""
     q = rot.qstd(np.asarray(q0, np.float64))
     shift = np.zeros(3)
-    keep = local_of(sums6(grad, side, frame, t, q, shift, pattern, mask))
+    keep = local_of(sums6(grad, side, frame, t, q, shift, pattern, mask, interp, sheets))
     lam = 1e-3
     it = 0
     while it < most:
@@ -490,7 +490,7 @@ def settle6(grad, side, frame, t, q0, pattern, mask, trust, most):
         if d is not None:
             st = np.clip(shift + d[:3], -trust, trust)
             qt = rot.qstd(rot.qmul(rot.so3_exp(d[3:]), q))
-        now = local_of(sums6(grad, side, frame, t, qt, st, pattern, mask))
+        now = local_of(sums6(grad, side, frame, t, qt, st, pattern, mask, interp, sheets))
         gain = 0.0
         kept = damp = 0
         if now is not None and now[0] > keep[0]:
@@ -502,9 +502,10 @@ def settle6(grad, side, frame, t, q0, pattern, mask, trust, most):
             if lam < 1e8:
                 damp = 1
             lam = min(lam * 5, 1e8)
-        it += 1
         if kept == 0 and damp > 0:
+            it += 1
             continue
-        if gain < 1e-7:
+        if gain < 1e-7:  # (planefit.zig:570-622: the loop's continue expression counts rounds; a break does not)
             break
+        it += 1
     return q, shift, keep[0], it

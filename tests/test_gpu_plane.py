@@ -107,6 +107,48 @@ def test_plane_sums_match_oracle(small, interp):
             assert abs(g[3 + k] - fd) < 2e-2 * max(1.0, np.abs(g[3:]).max()), (k, g[3 + k], fd)
 
 
+@pytest.mark.parametrize("interp", [0, 1])
+def test_fit_settle_matches_oracle(small, interp):
+    """The plane fit's per-pattern Levenberg–Marquardt over six unknowns (Fit.settle: the device's
+    sums, the host's damped steps for all patterns at once) against the oracle's settle of each
+    pattern by itself, from orientations 1° off: NCC 2e-4, orientation 0.02°, shift 0.05 px."""
+    from zebsdsolve_b200 import _native as N
+    from zebsdsolve_b200 import planefit
+    from zebsdsolve_b200 import rotations as R
+
+    st = small
+    e, n, h, w = st["e"], st["n"], st["h"], st["w"]
+    cells = np.arange(n)
+    rng = np.random.default_rng(9)
+    ax = rng.normal(size=(n, 3))
+    ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+    q0 = np.stack([orot.qstd(orot.qmul(orot.so3_exp(math.radians(1.0) * ax[i]), st["q"][i])) for i in range(n)])
+    f = planefit.Fit.__new__(planefit.Fit)
+    f.e, f.n, f.cells = e, n, cells
+    f.use, f.n_used, f.phase = np.ones(n, bool), n, np.zeros(n, np.int32)
+    f.q, f.shift, f.base = q0.copy(), np.zeros((n, 3)), e.positions64(cells)
+    f.fr = e.frame()
+    f.pats = e.upload(cells)[: n * h * w].clone()
+    npix = N.load().zeb_mask_pixels(ctypes.byref(f.fr))
+    f.list = torch.empty(npix, dtype=torch.int32, device="cuda")
+    N.call("zeb_mask_list", ctypes.byref(f.fr), ctypes.c_void_p(f.list.data_ptr()), None)
+    f.interp, f.masters = interp, None
+    trust = 0.05 * h
+    f.settle(6, trust, 60)
+    G = e.phases[0].master.rotations()
+    mask = og.mask_of(h, w)
+    t0 = st["geo"].translation(h, w)
+    for i in range(n):
+        pat = op.normalize(st["pats"][i].astype(np.float64), mask)
+        q, shift, ncc, _ = od.settle6(st["grad"], st["side"], st["geo"].frame(), t0, q0[i], pat, mask, trust, 60,
+                                      interp=interp, sheets=st["baked"])
+        assert abs(f.keep[1][i] - ncc) < 2e-4, (i, f.keep[1][i], ncc)
+        assert np.degrees(float(R.disorientation(f.q[i:i + 1], q[None], G)[0])) < 0.02
+        assert np.abs(f.shift[i] - shift).max() < 0.05, (f.shift[i], shift)
+    dis = np.degrees(R.disorientation(f.q, st["q"], G))
+    assert (dis < 0.5).all(), dis
+
+
 TRUTH = (0.5, 0.3, 0.6)
 
 

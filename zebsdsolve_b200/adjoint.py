@@ -170,9 +170,10 @@ def refine6(plan, q0, trust, most=60, gradient="reference"):
         shift = torch.where(better[:, None], st, shift)
         keep = tuple(torch.where(better.view(-1, *([1] * (k.dim() - 1))), nw, k) for k, nw in zip(keep, now))
         lam = torch.where(better, torch.clamp(lam / 3, min=1e-4), torch.clamp(lam * 5, max=1e8))
-        rounds += 1
-        if kept == 0 and damp > 0:
+        if kept == 0 and damp > 0:  # (every step overshot: they go again, damped more)
+            rounds += 1
             continue
-        if gain / count < 1e-7:
+        if gain / count < 1e-7:  # (the round that ends the loop is not counted, as the reference's)
             break
+        rounds += 1
     return q, shift, keep[1], rounds
