@@ -417,13 +417,12 @@ class Scorer:
         of the last grid scored (pcfit.zig:540-561)."""
         pk, choice = self.last
         ph = choice[j]
+        r = pk[ph, j, np.arange(self.n_pat)]  # [pattern][8], each of its own phase
         q = np.empty((self.n_pat, 4), np.float32)
-        ncc = np.empty(self.n_pat, np.float32)
-        for b in range(self.n_pat):
-            r = pk[ph[b], j, b]
-            q[b] = R.to_fz(r[None, :4].astype(np.float64), self.e.phases[int(ph[b])].master.rotations())[0]
-            ncc[b] = r[4]
-        return q, ph.astype(np.int32), ncc
+        for p in np.unique(ph):
+            sel = ph == p
+            q[sel] = R.to_fz(r[sel, :4].astype(np.float64), self.e.phases[int(p)].master.rotations())
+        return q, ph.astype(np.int32), r[:, 4].astype(np.float32)
 
 
 def run(e, timer=None):

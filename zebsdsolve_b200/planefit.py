@@ -726,9 +726,10 @@ def _finish(e, f, res, before, P, model, kind, pts, fr, aspect, said):
     R0 = before.nominal()
     frame_rot = R.qmul(R.exp_map(R0 @ before.rot), R.qconj(R.exp_map(R0 @ g.rot)))
     quats = np.empty((f.n, 4), np.float32)
-    for b in range(f.n):
-        p = int(f.phase[b])
-        quats[b] = R.to_fz(R.qmul(f.q[b], frame_rot)[None], e.phases[p].master.rotations())[0]
+    turned = R.qmul(f.q, frame_rot[None, :])
+    for p in np.unique(f.phase):
+        sel = f.phase == p
+        quats[sel] = R.to_fz(turned[sel], e.phases[int(p)].master.rotations())
     e.fit = {"cells": f.cells, "quats": quats, "phase": f.phase.copy(),
              "ncc": np.where(f.use, f.keep[1], f.seed_ncc).astype(np.float32)}
     deg = 180.0 / math.pi
