@@ -80,7 +80,28 @@ int zeb_prep_reduced(const void* raw, int pixel, int n, int src_h, int src_w, do
                      int dynamic, float sigma, const float mask[3], int normalize, float* out, void* scratch,
                      void* stream);
 
+/* dynamic = 3 in the zeb_prep entries: the output is the Gaussian blur itself (the band pass's
+ * two Gaussians; prep.zig:190-200). */
+
+/* Contrast-limited adaptive histogram equalization of n images of h × w in place: each stretched
+ * to [0, 1], padded by reflection to tiles × tiles whole tiles, each tile's histogram of `bins`
+ * levels clipped at clip × the mean count per level and redistributed, the pixel read from the
+ * four nearest tiles' tables between its two nearest levels. scratch: zeb_clahe_scratch_bytes.
+ * Replaces Prep.filter's CLAHE (src/prep.zig:167-188; shaders/prep.wgsl stretch, clahe_hist,
+ * clahe_cdf, clahe_apply). */
+size_t zeb_clahe_scratch_bytes(int n, int tiles, int bins);
+int zeb_clahe(float* img, int n, int h, int w, int tiles, int bins, float clip, void* scratch, void* stream);
+
+/* out = a − b (op 0) or a / max(b, 1e-6) (op 1), elementwise over count floats. Replaces
+ * combine (shaders/prep.wgsl; the band pass's difference, src/prep.zig:190-200). */
+int zeb_combine(const float* a, const float* b, float* out, long long count, int op, void* stream);
+
 /* ── the master on the sphere ───────────────────────────────────────────────────────────── */
+
+/* The master's mean over its point group: dst at each sheet pixel's direction d is the mean of
+ * src (bilinear) at g·d over the n_ops operators (ops: 3 × 3 row-major each). Replaces
+ * Prep.symmetrize (src/prep.zig:240-249; shaders/mastersph.wgsl symmetrize 111-122). */
+int zeb_master_symmetrize(const float* src, float* dst, int side, const float* ops, int n_ops, void* stream);
 
 /* One pass of Gaussian smoothing on the sphere over a (2·radius+1)² tangent lattice of step
  * `step` radians with weights exp(−(a²+b²)·k). Replaces the sphere_blur pass of Prep.sphereBlur

@@ -79,6 +79,17 @@ def pixel_dirs(side):
     return np.concatenate([north, south])
 
 
+def symmetrize(sheets, side, ops):
+    """mastersph.wgsl:111-122 — the master's mean over its point group: at each sheet pixel's
+    direction d, the mean of the master (bilinear) at g·d over the operators g (3 × 3)."""
+    d = pixel_dirs(side)
+    acc = np.zeros(len(d))
+    for g in ops:
+        v = d @ np.asarray(g, np.float64).T
+        acc += sheet_lookup(sheets, side, v / np.linalg.norm(v, axis=-1, keepdims=True))
+    return acc / max(len(ops), 1)
+
+
 def _tangent_frame(c):
     ref = np.where((np.abs(c[..., 0]) > 0.8)[..., None], np.array([0.0, 1.0, 0.0]), np.array([1.0, 0.0, 0.0]))
     e1 = np.cross(c, ref)

@@ -116,15 +116,100 @@ def normalize(img, mask):
     return out / math.sqrt(max(ss, 1e-30))
 
 
-def run(raw, static=None, dynamic="subtract", dynamic_sigma=0.0, mask=(0.0, 0.0, 0.0), do_normalize=True):
+def stretch(img):
+    """prep.wgsl stretch — an image to [0, 1] between its extremes (float32)."""
+    f = np.float32
+    v = np.asarray(img, f)
+    lo, hi = v.min(), v.max()
+    k = f(1) / max(f(hi - lo), f(1e-20))
+    return ((v - lo) * k).astype(f)
+
+
+def clahe(img, tiles, bins, clip):
+    """prep.wgsl clahe_hist / clahe_cdf / clahe_apply (prep.zig:167-188) on one image, float32
+    as the kernels round: the image stretched to [0, 1]; padded by reflection at its top and left
+    to a whole number of tiles; each tile's histogram clipped at clip × the mean count per level,
+    the cut spread evenly (the remainder one count each to the first levels) and cumulated; each
+    pixel from its four nearest tiles' tables, between its two nearest levels."""
+    f = np.float32
+    v = stretch(img)
+    h, w = v.shape
+    pad_h, pad_w = (tiles - h % tiles) % tiles, (tiles - w % tiles) % tiles
+    th, tw = max(1, (h + pad_h) // tiles), max(1, (w + pad_w) // tiles)
+
+    def reflect(i, n, pad):
+        if n <= 1:
+            return np.zeros_like(i)
+        x = np.abs(i - pad)
+        x = np.where(x >= n, 2 * n - 2 - x, x)
+        return np.clip(x, 0, n - 1)
+
+    py, px = np.arange(h + pad_h), np.arange(w + pad_w)
+    padded = np.clip(v[reflect(py, h, pad_h)][:, reflect(px, w, pad_w)], f(0), f(1))
+    top = f(bins - 1)
+    level = np.clip(padded * top, f(0), top).astype(np.int64)
+    hist = np.zeros((tiles, tiles, bins), np.int64)
+    np.add.at(hist, ((py // th)[:, None].repeat(len(px), 1), (px // tw)[None, :].repeat(len(py), 0), level), 1)
+    voxels, nb = f(max(th * tw, 1)), f(bins)
+    limit = max(f(f(f(clip) * voxels) / nb), f(1))
+    cdf = np.empty((tiles, tiles, bins), f)
+    for ty in range(tiles):
+        for tx in range(tiles):
+            c = np.minimum(hist[ty, tx].astype(f), limit)
+            sumc = f(0)
+            for x in c:
+                sumc = f(sumc + x)
+            clipped = f(voxels - sumc)
+            residual = int(f(clipped - f(nb * f(np.floor(f(clipped / nb))))))
+            redist = f(f(clipped - f(residual)) / nb)
+            acc = f(0)
+            for i in range(bins):
+                ci = f(c[i] + redist)
+                if i < residual:
+                    ci = f(ci + f(1))
+                acc = f(acc + ci)
+                cdf[ty, tx, i] = min(max(f(acc / voxels), f(0)), f(1))
+
+    def mix(a, b, t):
+        return (a * (f(1) - t)).astype(f) + (b * t).astype(f)
+
+    tl = f(tiles - 1)
+    gy = ((np.arange(h, dtype=f) + f(0.5)) / f(h) * tl).astype(f)
+    gx = ((np.arange(w, dtype=f) + f(0.5)) / f(w) * tl).astype(f)
+    y0, x0 = np.floor(gy).astype(np.int64), np.floor(gx).astype(np.int64)
+    y1, x1 = np.minimum(y0 + 1, tiles - 1), np.minimum(x0 + 1, tiles - 1)
+    fy, fx = (gy - y0.astype(f))[:, None], (gx - x0.astype(f))[None, :]
+    vv = np.clip(v, f(0), f(1))
+    bf = (vv * f(bins - 1)).astype(f)
+    b0 = np.clip(np.floor(bf), 0, bins - 2).astype(np.int64)
+    fb = (bf - b0.astype(f)).astype(f)
+
+    def look(yy, xx):
+        t = cdf[yy[:, None], xx[None, :]]
+        lo = np.take_along_axis(t, b0[..., None], -1)[..., 0]
+        hi = np.take_along_axis(t, b0[..., None] + 1, -1)[..., 0]
+        return mix(lo, hi, fb)
+
+    return mix(mix(look(y0, x0), look(y0, x1), fx), mix(look(y1, x0), look(y1, x1), fx), fy).astype(f)
+
+
+def run(raw, static=None, dynamic="subtract", dynamic_sigma=0.0, mask=(0.0, 0.0, 0.0), do_normalize=True,
+        clahe_opts=None, bandpass=None):
     """prep.zig:143-204, 263-272 — one pattern [h, w] (any integer or float dtype) through the
-    filter chain: static background, dynamic background, then the mask and normalization."""
+    filter chain: static background, dynamic background, CLAHE (clahe_opts = (tiles, bins,
+    clip)), band pass (bandpass = (fine, coarse) deviations in pixels: the fine blur less the
+    coarse, the fine one skipped below 0.05), then the mask and normalization."""
     img = np.asarray(raw).astype(np.float64)
     if static is not None:
         img = img - np.asarray(static, np.float64)
     if dynamic != "none" and dynamic_sigma > 0:
         bg = blur(img, dynamic_sigma)
         img = img - bg if dynamic == "subtract" else img / np.maximum(bg, 1e-6)
+    if clahe_opts is not None:
+        img = clahe(img, *clahe_opts).astype(np.float64)
+    if bandpass is not None and bandpass[1] > 0:
+        fine = blur(img, bandpass[0]) if bandpass[0] > 0.05 else img
+        img = fine - blur(img, bandpass[1])
     if do_normalize:
         img = normalize(img, mask)
     return img

@@ -17,7 +17,7 @@ struct PrepArgs {
   double factor;   // reduction factor (1: none)
   int kwhole;      // the factor as a whole number, 0 when it is not one
   const float* static_bg;
-  int dynamic;  // 0 none, 1 subtract, 2 divide
+  int dynamic;  // 0 none, 1 subtract, 2 divide, 3 the blur itself
   float sigma;
   float mask[3];
   int normalize;
@@ -32,6 +32,12 @@ struct PrepArgs {
   int bin, cpad, wradius;
   float kx, kz;
 };
+
+// the image against its blurred self: 1 subtract, 2 divide (the dynamic background), 3 the
+// blurred image itself (a band pass's Gaussians)
+__device__ __forceinline__ float with_background(int dynamic, float v, float bg) {
+  return dynamic == 1 ? v - bg : (dynamic == 2 ? v / fmaxf(bg, 1e-6f) : bg);
+}
 
 __device__ __forceinline__ float2 wide_cell(int jr, int n, int s) {
   int lo = jr * s;
@@ -185,7 +191,7 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
           g += t;
         }
         float bgv = s / g;
-        img[i] = a.dynamic == 1 ? img[i] - bgv : img[i] / fmaxf(bgv, 1e-6f);
+        img[i] = with_background(a.dynamic, img[i], bgv);
       }
       __syncthreads();
       bg = nullptr;
@@ -262,7 +268,7 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
           acc.x += e * v.x; acc.y += e * v.y;
         }
         float bgv = acc.x / acc.y;
-        img[i] = a.dynamic == 1 ? img[i] - bgv : img[i] / fmaxf(bgv, 1e-6f);
+        img[i] = with_background(a.dynamic, img[i], bgv);
       }
       __syncthreads();
       bg = nullptr;
@@ -371,7 +377,7 @@ __global__ void __launch_bounds__(256) k_prep_direct(PrepArgs a) {
       if (r0 + k < h) {
         float* px = P + (r0 + k) * pw + R + c;
         const float bgv = acc[k] / gsum[1][r0 + k];
-        *px = a.dynamic == 1 ? *px - bgv : *px / fmaxf(bgv, 1e-6f);
+        *px = with_background(a.dynamic, *px, bgv);
       }
     }
   }
@@ -429,7 +435,7 @@ static int prep_launch(const void* raw, int pixel, int n, int src_h, int src_w, 
   ZEB_REQUIRE(raw && out && mask, ZEB_EARG, "prep: null pointer");
   ZEB_REQUIRE(factor >= 1.0 && factor <= 64.0, ZEB_EARG, "prep: reduction factor %g", factor);
   const int h = (int)floor((double)src_h / factor + 1e-9), w = (int)floor((double)src_w / factor + 1e-9);
-  ZEB_REQUIRE(pixel >= 0 && pixel <= 2 && n >= 0 && h >= 4 && w >= 4 && dynamic >= 0 && dynamic <= 2, ZEB_EARG,
+  ZEB_REQUIRE(pixel >= 0 && pixel <= 2 && n >= 0 && h >= 4 && w >= 4 && dynamic >= 0 && dynamic <= 3, ZEB_EARG,
               "prep: bad arguments pixel=%d n=%d h=%d w=%d dynamic=%d", pixel, n, h, w, dynamic);
   if (n == 0) return ZEB_OK;
   PrepArgs a{};

@@ -329,32 +329,44 @@ class Engine:
         stored = math.radians(self.set["pixel_angle_deg"]) if self.set["pixel_angle_deg"] > 0 else 1.0 / max(self.geo.pc[2] * h, 1e-9)
         return stored * self.set["binning"]
 
+    def bake_key(self, p):
+        """engine.zig:1674-1697 — what a phase's master must be filtered for: the smoothing (its
+        pixel's width quantized in steps of 5 %), and the patterns' own band pass and CLAHE at the
+        sizes they have on the sphere (CLAHE's tiles as wide as the patterns' are)."""
+        s = self.set
+        angle = self.pixel_angle()
+        m = p.master
+        px = angle * m.side / math.sqrt(2 * math.pi)
+        if not px > 0:
+            return (None, s["master_smooth"], False, 0.0, 0.0, False, 0, 0, 0.0)
+        q = int(math.floor(math.log(px) / math.log(1.05) + 0.5))
+        f = s["binning"]
+        fine, coarse = (s["bp_fine"] / f, s["bp_coarse"] / f) if s["bandpass"] else (0.0, 0.0)
+        tiles = bins = 0
+        clip = 0.0
+        if s["clahe"]:
+            tile = self.pattern_shape()[0] / s["clahe_grid"] * px
+            tiles = int(min(max(math.floor(m.side / tile + 0.5), 1), 64))
+            bins, clip = s["clahe_bins"], s["clahe_clip"]
+        return (q, s["master_smooth"], bool(s["bandpass"]), fine, coarse, bool(s["clahe"]), tiles, bins, clip)
+
     def prepare_masters(self):
-        """engine.zig:1676-1788 — each phase's master smoothed on the sphere by master_smooth
-        pattern pixels (quantized in steps of 5 % of the sheet pixels a detector pixel spans),
-        renormalized, and its gradient table."""
+        """engine.zig:1699-1788 — each phase's master filtered as the patterns are (smoothed on the
+        sphere by master_smooth pattern pixels; CLAHE on the sheets then the mean over the point
+        group; the band pass as a difference of two smoothings on the sphere), the two sheets
+        normalized together, and its gradient and pair tables."""
         if not self.phases:
             raise EngineError("NoPhases")
-        angle = self.pixel_angle()
         for p in self.phases:
             m = p.master
-            px = angle * m.side / math.sqrt(2 * math.pi)
-            q = int(math.floor(math.log(px) / math.log(1.05) + 0.5)) if px > 0 else None
-            key = (q, self.set["master_smooth"])
+            key = self.bake_key(p)
             if p.baked is not None and p.baked[0] == key:
                 continue
             if key in p.bakes:  # a detector size met before (scans of several sizes): its master as baked then
                 p.baked = p.bakes[key]
                 self.chance_key = None
                 continue
-            sheets = torch.as_tensor(m.raw, device=self.dev)
-            smooth = self.set["master_smooth"] * (1.05 ** q) if q is not None else 0.0
-            if smooth > 0.05:
-                sheets = master_blur(sheets, m.side, smooth)
-                host = sheets.double()
-                mean = host.mean()
-                sd = torch.sqrt(((host - mean) ** 2).mean())
-                sheets = ((host - mean) / torch.clamp(sd, min=1e-30)).float().contiguous()
+            sheets = self.bake(p, key)
             grad = torch.empty(sheets.numel() * 4, dtype=torch.float32, device=self.dev)
             N.call("zeb_master_gradient", ptr(sheets), ptr(grad), m.side, stream_ptr())
             vpair = torch.empty(sheets.numel() * 2, dtype=torch.float32, device=self.dev)
@@ -365,6 +377,44 @@ class Engine:
                 p.bakes.pop(next(iter(p.bakes)))
             p.bakes[key] = p.baked
             self.chance_key = None
+
+    def bake(self, p, key):
+        """engine.zig:1738-1788 — the master's sheets filtered for `key` (bake_key), on the device."""
+        m = p.master
+        side = m.side
+        q, smooth0, bandpass, fine0, coarse0, clahe, tiles, bins, clip = key
+        sheets = torch.as_tensor(m.raw, device=self.dev)
+        if q is None:
+            return sheets
+        pxq = 1.05 ** q
+        smooth = smooth0 * pxq
+        if not (smooth > 0.05 or bandpass or clahe):
+            return sheets
+        fine = fine0 * pxq
+        if clahe:
+            sheets = master_blur(sheets, side, smooth).contiguous()
+            scratch = torch.empty(N.load().zeb_clahe_scratch_bytes(2, tiles, bins) // 4 + 1, dtype=torch.float32,
+                                  device=self.dev)
+            N.call("zeb_clahe", ptr(sheets), 2, side, side, tiles, bins, float(clip), ptr(scratch), stream_ptr())
+            if len(m.ops) > 1:
+                # CLAHE on the sheets as images does not respect the crystal's symmetry: the mean over
+                # the master's own point group
+                ops = torch.as_tensor(np.asarray(m.ops, np.float32).reshape(-1), device=self.dev)
+                out = torch.empty_like(sheets)
+                N.call("zeb_master_symmetrize", ptr(sheets), ptr(out), side, ptr(ops), len(m.ops), stream_ptr())
+                sheets = out
+        else:
+            # what the pixel averages and the band pass's fine Gaussian compose into one
+            fine = math.sqrt(smooth * smooth + fine * fine)
+            if not bandpass:
+                sheets = master_blur(sheets, side, smooth)
+        if bandpass:
+            low = master_blur(sheets.clone(), side, coarse0 * pxq)
+            sheets = master_blur(sheets, side, fine) - low
+        host = sheets.double()
+        mean = host.mean()
+        sd = torch.sqrt(((host - mean) ** 2).mean())
+        return ((host - mean) / torch.clamp(sd, min=1e-30)).float().contiguous()
 
     def band(self, L):
         """engine.zig:1793-1836 — the tables of bandwidth L and every phase's, built on first use."""
@@ -460,18 +510,46 @@ class Engine:
         return dyn, sigma
 
     def preprocess(self, raw, n):
-        """engine.zig:1452-1563 — n stored patterns on the device (raw, the scan's pixel type)
-        through the filter chain into the float32 pattern buffer."""
+        """engine.zig:1452-1563, prep.zig:143-204 — n stored patterns on the device (raw, the scan's
+        pixel type) through the filter chain into the float32 pattern buffer: static background,
+        dynamic background, CLAHE, band pass, then the mask and the normalization."""
         rows, cols, sh, sw = self.info()
         h, w = self.pattern_shape()  # reduced by binning as the patterns are unpacked
+        s = self.set
         out = self.buf("pats", n * h * w)
         static = self.static_background()
         dyn, sigma = self.prep_options()
         mask = (ctypes.c_float * 3)(*self.mask_of(h, w))
-        sb = N.load().zeb_prep_scratch_bytes(n, h, w, sigma)
-        scratch = self.buf("prep_scratch", sb // 4 + 1) if sb else None
-        N.call("zeb_prep_reduced", ptr(raw), self.pixel, n, sh, sw, float(self.set["binning"]), ptr(static), dyn,
-               sigma, mask, 1, ptr(out), ptr(scratch), stream_ptr())
+        bandpass = s["bandpass"] and s["bp_coarse"] > 0
+        extra = s["clahe"] or bandpass
+
+        def run(src, pixel, sh_, sw_, factor, bg, dyn_, sigma_, normalize, dst):
+            sb = N.load().zeb_prep_scratch_bytes(n, h, w, sigma_)
+            scratch = self.buf("prep_scratch", sb // 4 + 1) if sb else None
+            N.call("zeb_prep_reduced", ptr(src), pixel, n, sh_, sw_, factor, ptr(bg), dyn_, sigma_, mask, normalize,
+                   ptr(dst), ptr(scratch), stream_ptr())
+
+        if not extra:
+            run(raw, self.pixel, sh, sw, float(s["binning"]), static, dyn, sigma, 1, out)
+            return out
+        cur = self.buf("prep_cur", n * h * w)
+        run(raw, self.pixel, sh, sw, float(s["binning"]), static, dyn, sigma, 0, cur)
+        if s["clahe"]:
+            cs = self.buf("clahe_scratch", N.load().zeb_clahe_scratch_bytes(n, s["clahe_grid"], s["clahe_bins"]) // 4 + 1)
+            N.call("zeb_clahe", ptr(cur), n, h, w, s["clahe_grid"], s["clahe_bins"], float(s["clahe_clip"]), ptr(cs),
+                   stream_ptr())
+        if bandpass:
+            f = float(s["binning"])
+            fine, coarse = s["bp_fine"] / f, s["bp_coarse"] / f
+            low = self.buf("prep_low", n * h * w)
+            run(cur, 2, h, w, 1.0, None, 3, coarse, 0, low)
+            if fine > 0.05:
+                high = self.buf("prep_high", n * h * w)
+                run(cur, 2, h, w, 1.0, None, 3, fine, 0, high)
+            else:
+                high = cur
+            N.call("zeb_combine", ptr(high), ptr(low), ptr(cur), n * h * w, 0, stream_ptr())
+        run(cur, 2, h, w, 1.0, None, 0, 0.0, 1, out)
         return out
 
     def upload(self, cells):
