@@ -96,6 +96,20 @@ int zeb_clahe(float* img, int n, int h, int w, int tiles, int bins, float clip, 
  * combine (shaders/prep.wgsl; the band pass's difference, src/prep.zig:190-200). */
 int zeb_combine(const float* a, const float* b, float* out, long long count, int op, void* stream);
 
+/* Non-local pattern averaging (NLPAR; Brewick, Wright and Rowenhorst 2019) of a window of loaded
+ * patterns (px floats each, f32, in the window's order: the wanted cells first, then ring after
+ * ring around them; counts[d] (host, radius·passes + 2 entries) cells lie within d rings): passes
+ * of weighted means over (2·radius + 1)² neighbours, each weight from the pair's mean squared
+ * difference against the noise the pair's shares of the stored patterns give. nbr (device,
+ * [n_win][(2·radius·passes + 1)²] rows first, 0xffffffff outside the map) lists each cell's
+ * neighbours. Writes the counts[0] averages to out; `patterns` is working space (clobbered when
+ * passes ≥ 3). sig_out (counts[rings − 1] floats) and shares_out (counts[0] × F) take the noise and
+ * the final shares when not NULL. Replaces Nlpar.average (src/nlpar.zig:89-138; shaders/nlpar.wgsl
+ * distance, sigma, weights, average, shares). */
+size_t zeb_nlpar_scratch_bytes(int n_win, int px, int radius, int passes);
+int zeb_nlpar(float* patterns, int px, const uint32_t* nbr, const int* counts, int radius, int passes, float lambda,
+              float* out, float* sig_out, float* shares_out, void* scratch, void* stream);
+
 /* ── the master on the sphere ───────────────────────────────────────────────────────────── */
 
 /* The master's mean over its point group: dst at each sheet pixel's direction d is the mean of

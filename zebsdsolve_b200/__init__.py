@@ -292,6 +292,27 @@ class Solver:
                     "used": np.zeros(0, bool)}
         return {k: v.copy() for k, v in p.items()}
 
+    # ── one pattern ──
+
+    def pattern(self, cell, processed=True, full=False):
+        """One pattern as float32 (h, w), at the reduced size (the `binning` setting) or (`full`) the
+        stored one (__init__.py:306-319). `processed`: True, as it is indexed (averaged with its
+        neighbours when `nlpar` is on, then filtered); False, as it is stored; "averaged", averaged
+        with its neighbours and not filtered; "background", the static background subtracted from
+        every pattern (an error when `static_background` subtracts none)."""
+        stage = {"averaged": 2, "background": 3}.get(processed) if isinstance(processed, str) else int(bool(processed))
+        if stage is None:
+            raise Error(f"pattern: processed={processed!r}")
+        return self._call("pattern", self._e.pattern, int(cell), stage, bool(full))
+
+    def nlpar_view(self):
+        """What averaging with its neighbours did to the pattern `pattern` last returned
+        (__init__.py:321-334): noise (its standard deviation a pixel, as stored), left (the share of
+        it the average keeps), own (the average's share of the pattern itself) and shares (side ×
+        side of the stored patterns around it, NaN outside the map); None when it was not averaged."""
+        v = self._e._nl_view
+        return None if v is None else dict(v, shares=v["shares"].copy())
+
     def fit_patterns(self):
         """The last fit's patterns: (cells, phases, quaternions in the fundamental zone, scores)."""
         f = self._e.fit

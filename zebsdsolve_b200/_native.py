@@ -82,6 +82,9 @@ _SIGS = {
     "zeb_mask_pixels": ([ctypes.POINTER(Frame)], c_int),
     "zeb_pc_splat": ([c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
     "zeb_clahe_scratch_bytes": ([c_int, c_int, c_int], c_size_t),
+    "zeb_nlpar_scratch_bytes": ([c_int, c_int, c_int, c_int], c_size_t),
+    "zeb_nlpar": ([c_void_p, c_int, c_void_p, c_void_p, c_int, c_int, c_float, c_void_p, c_void_p, c_void_p, c_void_p,
+                   c_void_p], c_int),
     "zeb_clahe": ([c_void_p, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p, c_void_p], c_int),
     "zeb_combine": ([c_void_p, c_void_p, c_void_p, c_longlong, c_int, c_void_p], c_int),
     "zeb_master_symmetrize": ([c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p], c_int),
@@ -104,7 +107,7 @@ _lib = None
 ZEB_PEAKS_STATIC_SLABS = 1 << 19  # include/zebsdsolve_b200.h
 
 # kernels each entry point launches (for the launch counts the benchmark reports)
-KERNELS = {"zeb_pc_splat": 0, "zeb_sums6_list": 1, "zeb_clahe": 4, "zeb_combine": 1, "zeb_master_symmetrize": 1, "zeb_prep": 1, "zeb_prep_ex": 1, "zeb_prep_reduced": 1, "zeb_sphere_coefficients": 3, "zeb_sphere_coefficients_spans": 3, "zeb_sphere_spans": 1, "zeb_spectrum_f32": 1,
+KERNELS = {"zeb_nlpar": 5, "zeb_pc_splat": 0, "zeb_sums6_list": 1, "zeb_clahe": 4, "zeb_combine": 1, "zeb_master_symmetrize": 1, "zeb_prep": 1, "zeb_prep_ex": 1, "zeb_prep_reduced": 1, "zeb_sphere_coefficients": 3, "zeb_sphere_coefficients_spans": 3, "zeb_sphere_spans": 1, "zeb_spectrum_f32": 1,
            "zeb_spectrum_bf16": 2, "zeb_tc_pack_master": 0, "zeb_correlate_peaks": 2, "zeb_correlate_peaks_static": 2, "zeb_correlate_volume": 1, "zeb_rden_build": 1,
            "zeb_refine": 1, "zeb_chance": 1, "zeb_project": 1, "zeb_records_fz": 1, "zeb_det6": 1, "zeb_det6_list": 1, "zeb_solve6": 1, "zeb_pack_panel": 1, "zeb_mask_list": 1, "zeb_refine_list": 1, "zeb_dict_sims": 1, "zeb_match_bf16": 1, "zeb_match_f32": 1, "zeb_match_best": 1, "zeb_master_blur_pass": 1, "zeb_master_gradient": 1, "zeb_master_pairs": 1,
            "zeb_master_sample_grid": 1, "zeb_gauss_legendre": 1, "zeb_legendre_table": 1, "zeb_wigner_half_pi": 1,

@@ -168,6 +168,7 @@ class Engine:
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
         self.geo_given = Geometry()  # the geometry as given (set_geometry), where a full fit starts
+        self._nl_view = None  # what averaging with neighbours did to the last pattern looked at
         self.pc_history = []  # the grids of the last pattern-centre vote (pcfit.run)
         self.plane_points = None  # the source points of the last plane fit
         self.fit = None  # the last fit's patterns: cells, orientations, phases, scores
@@ -509,12 +510,164 @@ class Engine:
         sigma = s["dynamic_sigma"] * w if dyn else 0.0
         return dyn, sigma
 
-    def preprocess(self, raw, n):
+    # ── averaging with neighbours (NLPAR) ──
+
+    NLPAR_BYTES = 256 << 20  # one copy of a window's patterns on the device at most (engine.zig:1196)
+
+    def nlpar_window(self, wanted):
+        """engine.zig:1201-1258 — the cells averaging `wanted` needs: the wanted ones, then ring
+        after ring of the map's cells around them (8-neighbourhoods) out to radius · passes + 1;
+        counts[d] cells lie within d rings; nbr[k][slot] the list index of the cell at each offset
+        up to radius · passes each way (rows first), 0xffffffff outside the map or the list."""
+        rows, cols = self.info()[:2]
+        R, P = int(self.set["nlpar_radius"]), int(self.set["nlpar_iterations"])
+        wanted = np.asarray(wanted, np.int64)
+        index = np.full(rows * cols, -1, np.int64)
+        first = np.unique(wanted, return_index=True)[1]
+        lst = [wanted[np.sort(first)]]
+        index[lst[0]] = np.arange(len(lst[0]))
+        counts = [len(lst[0])]
+        grid = np.zeros((rows, cols), bool)
+        grid.reshape(-1)[lst[0]] = True
+        total = counts[0]
+        for _ in range(R * P + 1):
+            d = grid.copy()
+            d[1:] |= grid[:-1]
+            d[:-1] |= grid[1:]
+            e = d.copy()
+            e[:, 1:] |= d[:, :-1]
+            e[:, :-1] |= d[:, 1:]
+            new = np.flatnonzero((e & ~grid).reshape(-1))
+            index[new] = total + np.arange(len(new))
+            total += len(new)
+            lst.append(new)
+            counts.append(total)
+            grid = e
+        cells = np.concatenate(lst)
+        r = R * P
+        off = np.arange(-r, r + 1)
+        y = (cells // cols)[:, None, None] + off[None, :, None]
+        x = (cells % cols)[:, None, None] + off[None, None, :]
+        inside = (y >= 0) & (y < rows) & (x >= 0) & (x < cols)
+        at = np.where(inside, index[np.clip(y, 0, rows - 1) * cols + np.clip(x, 0, cols - 1)], -1)
+        nbr = np.where(at >= 0, at, 0xFFFFFFFF).astype(np.uint32).reshape(len(cells), -1)
+        return cells, counts, nbr
+
+    def nlpar_average(self, cells, account=False):
+        """engine.zig:1504-1553 — the cells' stored patterns averaged with their neighbours on the
+        device (loaded at the reduced size, not yet filtered): [n·h·w] float32. In parts when a
+        window's patterns would pass NLPAR_BYTES. account: keep what the averaging did to the
+        first cell (its noise, the share of it left, its own share, its shares), for nlpar_view."""
+        s = self.set
+        rows, cols, sh, sw = self.info()
+        h, w = self.pattern_shape()
+        px = h * w
+        cells = np.asarray(cells, np.int64)
+        n = len(cells)
+        R, P = int(s["nlpar_radius"]), int(s["nlpar_iterations"])
+        F = (2 * R * P + 1) ** 2
+        out = self.buf("nl_out", max(n, 1) * px)
+        most = max(1, self.NLPAR_BYTES // (px * 4))
+        t0, guess = 0, n
+        mask = (ctypes.c_float * 3)(0.0, 0.0, 0.0)
+        while t0 < n:
+            m = min(n - t0, guess)
+            lst, counts, nbr = self.nlpar_window(cells[t0:t0 + m])
+            while m > 1 and len(lst) > most:
+                m = (m + 1) // 2
+                lst, counts, nbr = self.nlpar_window(cells[t0:t0 + m])
+            guess = 2 * m
+            nw = len(lst)
+            raw = self.buf("nl_raw", nw * sh * sw, self.pinned().dtype)[: nw * sh * sw].view(nw, sh, sw)
+            self.upload_raw(lst, raw, torch.cuda.current_stream())
+            loaded = self.buf("nl_loaded", nw * px)
+            sb = N.load().zeb_prep_scratch_bytes(nw, h, w, 0.0)
+            N.call("zeb_prep_reduced", ptr(raw), self.pixel, nw, sh, sw, float(s["binning"]), None, 0, 0.0, mask, 0,
+                   ptr(loaded), ptr(self.buf("prep_scratch", sb // 4 + 1) if sb else None), stream_ptr())
+            nbr_d = self.to_device("nl_nbr", nbr)
+            cnt = (ctypes.c_int * len(counts))(*counts)
+            scratch = self.buf("nl_scratch", N.load().zeb_nlpar_scratch_bytes(nw, px, R, P) // 4 + 1)
+            sig = shares = None
+            if account and t0 == 0:
+                sig = torch.empty(counts[R * P], dtype=torch.float32, device=self.dev)
+                shares = torch.empty(counts[0] * F, dtype=torch.float32, device=self.dev)
+            N.call("zeb_nlpar", ptr(loaded), px, ptr(nbr_d), cnt, R, P, float(s["nlpar_lambda"]), ptr(out[t0 * px:]),
+                   ptr(sig), ptr(shares), ptr(scratch), stream_ptr())
+            if sig is not None:
+                self._nl_view = self._nlpar_view(sig.cpu().numpy(), shares.cpu().numpy()[:F], nbr[0], R * P)
+            t0 += m
+        return out[: n * px]
+
+    @staticmethod
+    def _nlpar_view(sig, share, nbr0, reach):
+        """engine.zig:1285-1306 for one average: the stored pattern's noise (a pixel's standard
+        deviation), the share of it the average keeps, the average's own share, and its shares of
+        the stored patterns around it (NaN outside the map)."""
+        side = 2 * reach + 1
+        inside = nbr0 != 0xFFFFFFFF
+        before = float(sig[0])
+        after = float((share[inside].astype(np.float64) ** 2 * sig[nbr0[inside].astype(np.int64)]).sum())
+        grid = np.where(inside, share, np.nan).reshape(side, side).astype(np.float32)
+        return {"noise": float(np.sqrt(before)) if before > 0 else 0.0,
+                "left": float(np.sqrt(after / before)) if before > 0 else 0.0,
+                "own": float(share[len(share) // 2]), "shares": grid}
+
+    def pattern(self, cell, stage, full=False):
+        """exports.zig ze_pattern — one cell's pattern (float32 [h, w]) at the reduced size, or
+        (full) the stored one: stage 0 as stored, 1 as indexed (averaged when nlpar is on, then
+        filtered), 2 averaged with its neighbours and not filtered, 3 the static background."""
+        rows, cols, sh, sw = self.info()
+        h, w = self.pattern_shape()
+        if full and (h, w) != (sh, sw) and stage != 0:
+            raise EngineError("pattern: only the stored pattern is kept at the full size (binning is on)")
+        self._nl_view = None
+        if stage == 3:
+            bg = self.static_background()
+            if bg is None:
+                raise EngineError("NoStaticBackground")
+            return bg.reshape(h, w).cpu().numpy()
+        cells = np.array([int(cell)], np.int64)
+        if not 0 <= cells[0] < rows * cols:
+            raise EngineError("CellOutOfRange")
+        if stage == 1:
+            if self.set["nlpar"]:
+                avg = self.nlpar_average(cells, account=True)
+                view = self._nl_view
+                out = self.filter_chain(avg, 2, 1, h, w, 1.0)
+                self._nl_view = view
+            else:
+                out = self.upload(cells)
+            return out[: h * w].reshape(h, w).cpu().numpy()
+        if stage == 2 and self.set["nlpar"]:
+            return self.nlpar_average(cells, account=True)[: h * w].reshape(h, w).cpu().numpy()
+        raw = self.buf("raw_up", sh * sw, self.pinned().dtype)[: sh * sw].view(1, sh, sw)
+        self.upload_raw(cells, raw, torch.cuda.current_stream())
+        oh, ow = (sh, sw) if full else (h, w)
+        out = torch.empty(oh * ow, dtype=torch.float32, device=self.dev)
+        mask = (ctypes.c_float * 3)(0.0, 0.0, 0.0)
+        N.call("zeb_prep_reduced", ptr(raw), self.pixel, 1, sh, sw, 1.0 if full else float(self.set["binning"]), None, 0,
+               0.0, mask, 0, ptr(out), None, stream_ptr())
+        return out.reshape(oh, ow).cpu().numpy()
+
+    def preprocess(self, raw, n, cells=None):
         """engine.zig:1452-1563, prep.zig:143-204 — n stored patterns on the device (raw, the scan's
-        pixel type) through the filter chain into the float32 pattern buffer: static background,
+        pixel type) through the filter chain into the float32 pattern buffer: with nlpar, first
+        averaged with their neighbours (the cells' windows read from the scan); static background,
         dynamic background, CLAHE, band pass, then the mask and the normalization."""
         rows, cols, sh, sw = self.info()
         h, w = self.pattern_shape()  # reduced by binning as the patterns are unpacked
+        s = self.set
+        if s["nlpar"]:
+            if cells is None:
+                raise EngineError("nlpar: the cells of the patterns are needed to average them with their neighbours")
+            raw = self.nlpar_average(cells)
+            return self.filter_chain(raw, 2, n, h, w, 1.0)
+        return self.filter_chain(raw, self.pixel, n, sh, sw, float(s["binning"]))
+
+    def filter_chain(self, raw, pixel, n, sh, sw, factor):
+        """prep.zig:143-204 — n patterns (pixel type, stored size sh × sw reduced by factor) through
+        static background, dynamic background, CLAHE, band pass, mask and normalization."""
+        h, w = self.pattern_shape()
         s = self.set
         out = self.buf("pats", n * h * w)
         static = self.static_background()
@@ -530,10 +683,10 @@ class Engine:
                    ptr(dst), ptr(scratch), stream_ptr())
 
         if not extra:
-            run(raw, self.pixel, sh, sw, float(s["binning"]), static, dyn, sigma, 1, out)
+            run(raw, pixel, sh, sw, factor, static, dyn, sigma, 1, out)
             return out
         cur = self.buf("prep_cur", n * h * w)
-        run(raw, self.pixel, sh, sw, float(s["binning"]), static, dyn, sigma, 0, cur)
+        run(raw, pixel, sh, sw, factor, static, dyn, sigma, 0, cur)
         if s["clahe"]:
             cs = self.buf("clahe_scratch", N.load().zeb_clahe_scratch_bytes(n, s["clahe_grid"], s["clahe_bins"]) // 4 + 1)
             N.call("zeb_clahe", ptr(cur), n, h, w, s["clahe_grid"], s["clahe_bins"], float(s["clahe_clip"]), ptr(cs),
@@ -558,7 +711,7 @@ class Engine:
         n = len(cells)
         raw = self.buf("raw_up", max(n, 1) * h * w, self.pinned().dtype)[: n * h * w].view(n, h, w)
         self.upload_raw(cells, raw, torch.cuda.current_stream())
-        return self.preprocess(raw, n)
+        return self.preprocess(raw, n, cells)
 
     def prepare(self, bandwidth=None, method="spherical", grid=None):
         """Everything a batch needs besides its patterns: tables, chance calibration, denominators
@@ -669,7 +822,7 @@ class Engine:
         fr = self.frame()
         mark = timer.mark if timer is not None else (lambda name: None)
         mark("prep")
-        pats = self.preprocess(raw, n)
+        pats = self.preprocess(raw, n, cells)
         items = self.items_of(cells)
         self.batch_stamp = self.batch_stamp % (1 << 24) + 1
         bt = b["tables"]
@@ -712,7 +865,7 @@ class Engine:
         fr = self.frame()
         mark = timer.mark if timer is not None else (lambda name: None)
         mark("prep")
-        pats = self.preprocess(raw, n)
+        pats = self.preprocess(raw, n, cells)
         items = self.items_of(cells)
         self.batch_stamp = self.batch_stamp % (1 << 24) + 1
         recs = self.buf("recs", n_ph * n * 8)
