@@ -106,8 +106,59 @@ class Solver:
     @property
     def scan(self):
         rows, cols, h, w = self._call("scan", self._e.info)
+        src = getattr(self._e, "scan_source", None) or {}
         return {"rows": rows, "cols": cols, "pattern_shape": (h, w),
-                "dtype": ["uint8", "uint16", "float32"][self._e.pixel], "format": "array"}
+                "dtype": ["uint8", "uint16", "float32"][self._e.pixel], "format": src.get("format", "array"),
+                "voltage_kv": src.get("voltage_kv", float("nan")), "pc_note": src.get("pc_note", "")}
+
+    def open(self, *paths):
+        """Open a scan file, and the side files it needs after it (__init__.py:216-240): EDAX .up1 /
+        .up2 (with its scan's .ang for the map's shape, the steps and the pattern centre), Oxford
+        .ebsp (uncompressed), NORDIF Pattern.dat (its Setting.txt picked up from beside it when not
+        given). The geometry takes what the file says (steps, tilts, pattern centre); the region of
+        interest goes back to the whole map. HDF5 scan files are refused (no HDF5 reader here:
+        pass their patterns as an array)."""
+        import os
+
+        from . import scan as SC
+
+        paths = [str(p) for p in paths]
+        if len(paths) == 1 and paths[0].lower().endswith(".dat"):
+            side = os.path.join(os.path.dirname(paths[0]), "Setting.txt")
+            if os.path.isfile(side):
+                paths.append(side)
+        sc = self._call("open", SC.open_scan, paths)
+        info = sc.info
+        self.set_patterns(np.asarray(sc.map()))
+        self.configure(roi_x=0, roi_y=0, roi_w=0, roi_h=0)
+        geo = {k: info[k] for k in ("step_x_um", "step_y_um", "sample_tilt_deg", "detector_tilt_deg")
+               if np.isfinite(info[k])}
+        if info["pc"] is not None:
+            geo["pc"] = tuple(info["pc"])
+        if geo:
+            self.set_geometry(**geo)
+        self._e.scan_source = {"format": sc.format, "voltage_kv": info["voltage_kv"], "pc_note": info["pc_note"],
+                               "paths": paths}
+        return self
+
+    def export(self, path):
+        """Write the results by the path's extension (__init__.py:879-905): an EDAX .ang or an HKL
+        .ctf, the orientations in the engine's own frame. (The reference's .h5oina export copies an
+        Oxford acquisition's HDF5 file: not part of this engine.)"""
+        from . import output
+
+        ext = str(path).rsplit(".", 1)[-1].lower()
+        if ext not in ("ang", "ctf"):
+            raise Error(f"export: .{ext} is not written by this engine (.ang, .ctf)")
+        e = self._e
+        rows, cols, h, w = e.info()
+        phases = [{"name": p.master.name, "laue": p.master.laue, "lattice": p.master.lattice,
+                   "space_group": p.master.space_group} for p in e.phases]
+        src = getattr(e, "scan_source", None) or {}
+        text = self._call("export", output.export_text, ext, e.res, phases, e.geo, rows, cols, h, w,
+                          src.get("voltage_kv", float("nan")))
+        with open(path, "w") as fh:
+            fh.write(text)
 
     def shape(self, full=False):
         return self._call("pattern_shape", self._e.pattern_shape)

@@ -32,14 +32,13 @@ class Result:
 
 
 def _open(solver, scan, phases, kwargs):
-    from . import Error
-
     geo = {k: kwargs.pop(k) for k in list(kwargs) if k in GEOMETRY_FIELDS}
     roi = {k: kwargs.pop(k) for k in list(kwargs) if k in ("roi_x", "roi_y", "roi_w", "roi_h")}
     solver.configure(**kwargs)
     if isinstance(scan, (str, Path)) or (isinstance(scan, (list, tuple)) and scan and isinstance(scan[0], (str, Path))):
-        raise Error("open: scan files are read by the reference's readers; pass the patterns as an array")
-    solver.set_patterns(scan)
+        solver.open(*([scan] if isinstance(scan, (str, Path)) else scan))
+    else:
+        solver.set_patterns(scan)
     if roi:
         solver.configure(**roi)
     if geo:

@@ -203,6 +203,7 @@ class Engine:
         if a.shape[2] < 4 or a.shape[3] < 4:
             raise EngineError("PatternTooSmall")
         self.patterns = np.ascontiguousarray(a)
+        self.scan_source = None  # the file the patterns came from (Solver.open), if any
         self._pinned = None
         rows, cols = a.shape[:2]
         self.avg = None

@@ -79,6 +79,7 @@ class Master:
         if self.raw.size != 2 * self.side * self.side:
             raise MasterError("master sheets do not match their side")
         self.ops = [np.asarray(o, np.float64).reshape(3, 3) for o in ops]
+        self.lattice = None  # a, b, c (Å), α, β, γ (degrees) when the file says
         self.point_group = int(point_group)
         self.space_group = int(space_group)
         self.voltage_kv = float(voltage_kv)
@@ -267,8 +268,23 @@ def load_npz(path):
     pg = int(meta.get("pg_num") or 0)
     sg = int(meta.get("space_group") or 0)
     m = Master(path.stem, side, normalize(sheets), ops, pg, sg, float(meta.get("voltage_kv") or 0.0))
+    m.lattice = lattice_of(meta)
     m.measure_symmetry()
     return m
+
+
+def lattice_of(meta):
+    """master.zig:255-274 — the cell (a, b, c in Å; α, β, γ in degrees) from the metadata's "cell",
+    or None when it is absent or not a cell."""
+    cell = meta.get("cell") if isinstance(meta, dict) else None
+    if not isinstance(cell, dict):
+        return None
+    try:
+        v = [float(cell[k]) for k in ("a_angstrom", "b_angstrom", "c_angstrom", "alpha_deg", "beta_deg", "gamma_deg")]
+    except (KeyError, TypeError, ValueError):
+        return None
+    ok = all(math.isfinite(x) and x > 0 for x in v) and all(x < 180 for x in v[3:])
+    return v if ok else None
 
 
 def write_npz(path, sheets, side, ops, point_group, meta=None):

@@ -1,0 +1,93 @@
+"""The results as the text files other EBSD software reads (the reference's src/output.zig
+exportText): EDAX/TSL .ang and HKL .ctf, the orientations as Bunge angles of the stored
+quaternions (each in its phase's fundamental zone) in the engine's own frame (sample x on the
+surface toward the detector, z out of it; each master's crystal axes X ∥ a, Z ∥ c*). Cells not
+indexed carry the formats' own markers.
+"""
+import math
+
+import numpy as np
+
+from . import rotations as R
+
+VERSION = "0.2.8"
+FRAME = "X +x Y +y Z +z, passive, X||a Z||c*"
+# output.zig:124-138 — the TSL symmetry code of each Laue class, and the class's number (sym.zig)
+TSL = {"c1": 1, "c2": 2, "d2": 22, "c4": 4, "d4": 42, "c3": 3, "d3": 32, "c6": 6, "d6": 62, "t": 23, "o": 43}
+LAUE_NUMBER = {"c1": 1, "c2": 2, "d2": 3, "c4": 4, "d4": 5, "c3": 6, "d3": 7, "c6": 8, "d6": 9, "t": 10, "o": 11}
+
+
+class ExportError(ValueError):
+    pass
+
+
+def export_text(kind, res, phases, geo, rows, cols, pat_h, pat_w, voltage_kv=float("nan")):
+    """output.zig:148-216 — kind "ang" or "ctf". res: quat [n, 4], ncc, nmi, phase [n] (−1: not
+    indexed); phases: dicts of name, laue (the Laue class's key), lattice (a, b, c, α, β, γ) and
+    space_group; geo: pc (Bruker), step_x_um, step_y_um, sample_tilt_deg."""
+    for p in phases:
+        if p.get("lattice") is None:
+            raise ExportError("MissingPhaseLattice: a phase's master names no cell (a, b, c, α, β, γ)")
+    q = np.asarray(res["quat"], np.float64).reshape(-1, 4)
+    bunge = R.to_bunge(q)
+    phase = np.asarray(res["phase"]).reshape(-1)
+    ncc = np.asarray(res["ncc"], np.float64).reshape(-1)
+    nmi = np.asarray(res["nmi"], np.float64).reshape(-1)
+    n_ph = len(phases)
+    out = []
+    if kind == "ang":
+        ratio = pat_w / pat_h
+        # EDAX measures the pattern centre's y from the bottom, x and y in fractions of the width
+        # and height, z of the smaller of the two
+        out.append(f"# TEM_PIX_PER_UM          1.000000\n# x-star                 {geo.pc[0]:.6f}\n"
+                   f"# y-star                 {1 - geo.pc[1]:.6f}\n# z-star                 {geo.pc[2] / min(ratio, 1):.6f}\n"
+                   "# WorkingDistance        0.000000\n#\n")
+        for pi, p in enumerate(phases):
+            L = p["lattice"]
+            out.append(f"# Phase {pi + 1}\n# MaterialName  \t{p['name']}\n# Formula     \t\n# Info \t\t\n"
+                       f"# Symmetry              {TSL[p['laue']]}\n"
+                       f"# LatticeConstants      {L[0]:.8f} {L[1]:.8f} {L[2]:.8f}  {L[3]:.8f}  {L[4]:.8f}  {L[5]:.8f}\n"
+                       "# NumberFamilies        0\n#\n")
+        out.append(f"# GRID: SqrGrid\n# XSTEP: {geo.step_x_um:.6f}\n# YSTEP: {geo.step_y_um:.6f}\n# NCOLS_ODD: {cols}\n"
+                   f"# NCOLS_EVEN: {cols}\n# NROWS: {rows}\n#\n# SOFTWARE: zebsdsolve {VERSION} (EDAX pattern centre)\n"
+                   f"# FRAME: {FRAME}\n# COLUMNS: phi1 PHI phi2 x y IQ(NMI) CI(NCC) Phase SEM Fit\n")
+        for r in range(rows):
+            for c in range(cols):
+                at = r * cols + c
+                x, y = c * geo.step_x_um, r * geo.step_y_um
+                ph = int(phase[at])
+                if ph < 0:
+                    out.append(f"  12.56637   12.56637   12.56637 {x:12.5f} {y:12.5f}      0.0  -1.000  0      0  0.000\n")
+                    continue
+                b = bunge[at]
+                pid = 0 if n_ph == 1 else ph + 1  # single-phase files number the phase 0
+                out.append(f"{b[0]:10.5f} {b[1]:10.5f} {b[2]:10.5f} {x:12.5f} {y:12.5f} {nmi[at]:8.4f} {ncc[at]:7.4f} "
+                           f"{pid:2d} {0:6d} {0.0:6.3f}\n")
+    elif kind == "ctf":
+        kv = 0.0 if math.isnan(voltage_kv) else voltage_kv
+        out.append(f"Channel Text File\nPrj\tzebsdsolve; frame {FRAME}\nAuthor\t\nJobMode\tGrid\nXCells\t{cols}\n"
+                   f"YCells\t{rows}\nXStep\t{geo.step_x_um:.6f}\nYStep\t{geo.step_y_um:.6f}\nAcqE1\t0\nAcqE2\t0\nAcqE3\t0\n")
+        out.append(f"Euler angles refer to Sample Coordinate system (CS0)!\tMag\t0\tCoverage\t100\tDevice\t0\tKV\t{kv:.1f}"
+                   f"\tTiltAngle\t{geo.sample_tilt_deg:.2f}\tTiltAxis\t0\n")
+        out.append(f"Phases\t{n_ph}\n")
+        for p in phases:
+            L = p["lattice"]
+            out.append(f"{L[0]:.8f};{L[1]:.8f};{L[2]:.8f}\t{L[3]:.8f};{L[4]:.8f};{L[5]:.8f}\t{p['name']}\t"
+                       f"{LAUE_NUMBER[p['laue']]}\t{p['space_group']}\t\t\t\n")
+        out.append("Phase\tX\tY\tBands\tError\tEuler1\tEuler2\tEuler3\tMAD\tBC\tBS\n")
+        deg = 180.0 / math.pi
+        for r in range(rows):
+            for c in range(cols):
+                at = r * cols + c
+                x, y = c * geo.step_x_um, r * geo.step_y_um
+                ph = int(phase[at])
+                if ph < 0:
+                    out.append(f"0\t{x:.4f}\t{y:.4f}\t0\t3\t0.0000\t0.0000\t0.0000\t0.0000\t0\t0\n")
+                    continue
+                b = bunge[at] * deg
+                bc = int(math.floor(255 * min(max(ncc[at], 0.0), 1.0) + 0.5))
+                bs = int(math.floor(255 * min(max(nmi[at], 0.0), 1.0) + 0.5))
+                out.append(f"{ph + 1}\t{x:.4f}\t{y:.4f}\t0\t0\t{b[0]:.4f}\t{b[1]:.4f}\t{b[2]:.4f}\t0.0000\t{bc}\t{bs}\n")
+    else:
+        raise ExportError(f"UnknownKind: {kind!r}")
+    return "".join(out)
