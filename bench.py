@@ -56,11 +56,13 @@ def parse():
     ap.add_argument("--batch", type=int, default=16384, help="patterns per device pass in the value measurement")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit", "plane"),
+    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit", "plane", "large"),
                     help="index: the scan of 60x60 patterns (the headline); adjoint: six-unknown refinement "
                          "of 120x120 patterns with jittered pattern centres; uneven: many scans of uneven "
                          "lengths and detector sizes, two phases; pcfit: the pattern-centre vote at its default "
-                         "settings; plane: the plane of source points (fit_plane, fit_geometry)")
+                         "settings; plane: the plane of source points (fit_plane, fit_geometry); large: 160x160 "
+                         "patterns binned 2x, two sweeps L=64 then L=128, adjoint refinement, and a PCA dictionary")
+    ap.add_argument("--large", type=int, default=250000, help="large: patterns of the scan (config 5 names 1 000 000)")
     ap.add_argument("--scans", type=int, default=64, help="uneven: number of scans")
     ap.add_argument("--max-count", type=int, default=200000, help="uneven: the longest scan (log-uniform from 1000)")
     return ap.parse_args()
@@ -777,6 +779,84 @@ def plane_main(a):
     print(json.dumps(line), flush=True)
 
 
+def large_main(a):
+    """Config 5's path at --large patterns (1 000 000 in the configuration; 250 000 by default, so
+    that the stored scan and its page-locked copy stay within 26 GB of host memory): 160 x 160 u16
+    patterns of the 432 master with grains as in the headline workload, binned 2x to 80 x 80;
+    indexed in two sweeps (L = 64, then L = 128 for the cells not accepted) in the BF16 form and in
+    the plain FP32 form, then every pattern refined over six unknowns with the adjoint gradient;
+    beside it the PCA dictionary of 295 389 orientations (dict_grid 96) reduced to 512 components
+    and matched on the tensor cores (top 8, rescored in FP32). Each path timed from the patterns
+    on the host to its results."""
+    import torch
+
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import synthetic as syn
+    from zebsdsolve_b200.master import write_npz
+
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp()
+    write_npz(f"{tmp}/m432.npz", syn.master_sheets(2, side=401, lmax=96, group="432", device="cuda"), 401,
+              syn.group_matrices("432"), 30)
+    side = int(math.isqrt(a.large))
+    rows = cols = side
+    n = rows * cols
+    s = ze.Solver()
+    s.add_phase(f"{tmp}/m432.npz")
+    s.set_patterns(np.zeros((rows, cols, 160, 160), np.uint16))
+    s.set_geometry(pc=PC, sample_tilt_deg=70.0, detector_tilt_deg=0.0)
+    rng = np.random.default_rng(700)
+    q, _ = syn.grain_map(rng, rows, cols, GRAINS, SPREAD_DEG)
+    pats = np.empty((n, 160, 160), np.uint16)
+    e = s._e
+    for i in range(0, n, 4096):
+        c = np.arange(i, min(n, i + 4096))
+        pats[c] = syn.counted_patterns(e.simulate_device(0, c, q[c]), seed=70 + i // 4096).cpu().numpy()
+    s.set_patterns(pats.reshape(rows, cols, 160, 160))
+    G = e.phases[0].master.rotations()
+
+    def median_deg(quats):
+        return round(float(np.median(np.degrees(s.disorientation(quats.reshape(-1, 4), q)))), 4)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t0
+
+    out = {}
+    cells = np.arange(n)
+    for prec in (a.precision, "f32"):
+        s.configure(binning=2, bandwidth=128, sweeps=2, sweep_bandwidth=64, sweep_method="same", precision=prec,
+                    method="spherical")
+        s.index_cells(cells[:4096], bandwidth=64)  # tables and masters of both bandwidths, untimed
+        s.index_cells(cells[:4096], bandwidth=128)
+        r, t_index = timed(s.index)
+        g, t_ref = timed(lambda: s.refine_patterns(cells, gradient="adjoint"))
+        sw = r["sweep"].reshape(-1)
+        out[prec] = {"value": round(n / (t_index + t_ref), 1), "index_s": round(t_index, 3), "refine_s": round(t_ref, 3),
+                     "accepted_first_sweep": round(float((sw == 0).mean()), 4),
+                     "accepted_second_sweep": round(float((sw == 1).mean()), 4),
+                     "median_deg_indexed": median_deg(r["quaternions"]), "median_deg_refined": median_deg(g["quaternions"]),
+                     "refine_rounds": int(g["rounds"])}
+    s.configure(method="pca", dict_grid=96, pca_components=512, sweeps=1, bandwidth=64, precision=a.precision)
+    _, t_build = timed(lambda: s.index_cells(cells[:4096]))  # the dictionary simulated and learned
+    rp, t_pca = timed(s.index)
+    out["pca"] = {"value": round(n / t_pca, 1), "index_s": round(t_pca, 3), "build_s": round(t_build, 3),
+                  "median_deg": median_deg(rp["quaternions"]), "dictionary": 295389, "components": 512}
+    line = {"metric": "patterns/s, 160x160 binned 2x, sweeps L=64 then L=128 and adjoint refinement, 1 B200",
+            "value": out[a.precision]["value"], "unit": "patterns/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "higher_is_better": True, "dtype": "bf16+f32", "data": "synthetic",
+            "config": {"workload": f"{rows}x{cols} scan of 160x160 uint16 patterns (1 000 000 in the configuration), "
+                                   f"{GRAINS} Voronoi grains (0.5 deg spread), 432 master 401^2 (SH <= 96), binned 2x "
+                                   "to 80x80; PCA dictionary 295 389 orientations, 512 components",
+                       "patterns": n, "precision": a.precision},
+            a.precision: out[a.precision], "fp32_form": out["f32"],
+            "vs_fp32_form": round(out[a.precision]["value"] / out["f32"]["value"], 3), "pca_dictionary": out["pca"]}
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     args = parse()
     if args.impl == "reference":
@@ -789,5 +869,7 @@ if __name__ == "__main__":
         pcfit_main(args)
     elif args.workload == "plane":
         plane_main(args)
+    elif args.workload == "large":
+        large_main(args)
     else:
         device_main(args)
