@@ -1,0 +1,101 @@
+"""The real scan: kikuchipy's nickel scan (55 × 75 patterns of 60 × 60, h5ebsd) opened through this
+package's HDF5 reader and indexed against the nickel master, checked as the reference's own test
+checks it (tests/test_api.py:664-735): the file's geometry is taken, the patterns come as stored
+and filtered, the stored static background is what "file" subtracts, the ballots find the
+scan's centre from a wrong start where the mean vote does not, and the orientations agree with
+the ones kikuchipy refined for the scan (median < 0.6°, more than 97 % within 3°, mean NCC
+> 0.45), nearly every match accepted. Needs the reference's test data (tests/golden/
+copy_testdata.sh); skipped without it."""
+import numpy as np
+import pytest
+
+from conftest import testdata
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _unit(a, mask=None):
+    m = np.ones(a.shape, bool) if mask is None else mask
+    out = np.where(m, a - a[m].mean(), 0).astype(np.float64)
+    return out / np.sqrt((out ** 2).sum())
+
+
+@pytest.fixture(scope="module")
+def nickel():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    scan, ni, qref = (testdata("nickel", f) for f in ("patterns_v2.h5", "Ni_master_20kV.npz", "reference_quaternions.f32"))
+    if scan is None or ni is None or qref is None:
+        pytest.skip("the reference's test data is not here (tests/golden/copy_testdata.sh)")
+    return scan, ni, np.fromfile(qref, "<f4").reshape(-1, 4)
+
+
+def test_nickel_scan_opens_with_its_geometry(nickel):
+    import zebsdsolve_b200 as ze
+
+    scan, _, _ = nickel
+    s = ze.Solver()
+    s.open(scan)
+    info = s.scan
+    assert info["rows"] == 55 and info["cols"] == 75 and info["pattern_shape"] == (60, 60)
+    assert info["format"] == "kikuchipy h5ebsd" and info["has_background"] and info["has_pc"]
+    assert np.allclose(s.geometry["pc"], (0.42326, 0.21363, 0.50207), atol=1e-4) and s.geometry["sample_tilt_deg"] == 70
+    raw = s.pattern(0, processed=False)
+    proc = s.pattern(0, processed=True)
+    assert raw.shape == (60, 60) and 0 <= raw.min() and raw.max() <= 255
+    assert abs(float(proc.sum())) < 1e-2 and abs(float((proc ** 2).sum()) - 1) < 1e-3
+    # the static background: the average of a lattice of patterns, or the one the file stores
+    cells = s.lattice(1024)
+    avg = np.mean([s.pattern(int(c), processed=False) for c in cells], axis=0)
+    s.configure(static_background="average", dynamic_background="none", mask=False)
+    assert len(cells) > 900 and np.abs(s.pattern(7) - _unit(s.pattern(7, processed=False) - avg)).max() < 1e-4
+    from zebsdsolve_b200 import scan as SC
+
+    stored_bg = SC.open_scan([scan]).info["background"].astype(np.float64)
+    s.configure(static_background="file")
+    assert np.abs(s.pattern(7) - _unit(s.pattern(7, processed=False) - stored_bg)).max() < 1e-4
+    assert np.abs(s.pattern(0, "background") - stored_bg).max() < 1e-3 * stored_bg.max()
+    s.close()
+
+
+def test_nickel_scan_indexes_as_kikuchipy_refined_it(nickel):
+    import zebsdsolve_b200 as ze
+
+    scan, ni, q_ref = nickel
+    s = ze.Solver()
+    s.open(scan)
+    pc_file = np.array(s.geometry["pc"])
+    s.add_phase(ni)
+    # the vote from a wrong start, on 5 × 5 fit patterns: the ballots land near the scan's own
+    # centre, the mean of the scores a ridge away from it
+    off = {}
+    s.configure(fit_grid=5)
+    for rule in ("ballots", "mean"):
+        s.configure(pc_vote=rule)
+        s.set_geometry(pc=(0.36, 0.16, 0.46))
+        off[rule] = float(np.abs(np.array(s.fit_pc()["pc"]) - pc_file).max())
+    s.configure(pc_vote="ballots", fit_grid=10)
+    s.set_geometry(pc=tuple(pc_file))
+    assert off["ballots"] < 0.006 and off["mean"] > 2 * off["ballots"], off
+    seen = []
+    r = s.index(lambda st: seen.append((st["done"], st["total"])))
+    dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), q_ref))
+    assert np.median(dis) < 0.6 and (dis < 3).mean() > 0.97 and r["ncc"].mean() > 0.45, \
+        (np.median(dis), (dis < 3).mean(), r["ncc"].mean())
+    assert len(seen) >= 1 and seen[-1] == (4125, 4125)
+    assert (r["sweep"] >= 0).mean() > 0.98 and np.median(r["z"]) > 30
+    s.close()
+
+
+def test_nickel_scan_through_index_by_path(nickel):
+    import zebsdsolve_b200 as ze
+
+    scan, ni, q_ref = nickel
+    res = ze.index(str(scan), [str(ni)], roi_x=0, roi_y=0, roi_w=30, roi_h=10, batch=128)
+    q = np.asarray(res.quaternions).reshape(55, 75, 4)[:10, :30].reshape(-1, 4)
+    s = ze.Solver()
+    s.add_phase(ni)
+    dis = np.degrees(s.disorientation(q, q_ref.reshape(55, 75, 4)[:10, :30].reshape(-1, 4)))
+    assert np.median(dis) < 0.6 and (dis < 3).mean() > 0.95
+    s.close()

@@ -131,7 +131,7 @@ def test_nordif_with_setting(tmp_path):
 
 def test_refusals(tmp_path):
     (tmp_path / "x.h5").write_bytes(b"\x89HDF\r\n\x1a\n" + bytes(100))
-    with pytest.raises(SC.ScanError, match="UnsupportedFormat"):
+    with pytest.raises(SC.ScanError, match="UnsupportedHdf5: offset size"):
         SC.open_scan([tmp_path / "x.h5"])
     with pytest.raises(SC.ScanError, match="UnknownScanFormat"):
         SC.open_scan([tmp_path / "x.xyz"])

@@ -109,15 +109,20 @@ class Solver:
         src = getattr(self._e, "scan_source", None) or {}
         return {"rows": rows, "cols": cols, "pattern_shape": (h, w),
                 "dtype": ["uint8", "uint16", "float32"][self._e.pixel], "format": src.get("format", "array"),
-                "voltage_kv": src.get("voltage_kv", float("nan")), "pc_note": src.get("pc_note", "")}
+                "voltage_kv": src.get("voltage_kv", float("nan")), "pc_note": src.get("pc_note", ""),
+                "has_background": src.get("background") is not None, "has_pc": src.get("pc") is not None,
+                "pattern_kinds": src.get("pattern_kinds", [])}
 
     def open(self, *paths):
         """Open a scan file, and the side files it needs after it (__init__.py:216-240): EDAX .up1 /
         .up2 (with its scan's .ang for the map's shape, the steps and the pattern centre), Oxford
         .ebsp (uncompressed), NORDIF Pattern.dat (its Setting.txt picked up from beside it when not
-        given). The geometry takes what the file says (steps, tilts, pattern centre); the region of
-        interest goes back to the whole map. HDF5 scan files are refused (no HDF5 reader here:
-        pass their patterns as an array)."""
+        given), and HDF5: h5ebsd (kikuchipy, Bruker, EDAX), Oxford .h5oina, EMsoft's EMEBSD output.
+        The geometry takes what the file says (steps, tilts, pattern centre, pixel size, Oxford's
+        detector orientation); the region of interest goes back to the whole map. A file that
+        stores processed and unprocessed patterns side by side (an Oxford acquisition can) is read
+        as the setting `stored_patterns` says; `scan["pattern_kinds"]` names the kinds it stores.
+        A static background the file stores is what `static_background: "file"` subtracts."""
         import os
 
         from . import scan as SC
@@ -127,18 +132,26 @@ class Solver:
             side = os.path.join(os.path.dirname(paths[0]), "Setting.txt")
             if os.path.isfile(side):
                 paths.append(side)
-        sc = self._call("open", SC.open_scan, paths)
+        sc = self._call("open", SC.open_scan, paths,
+                        unprocessed=self._e.set["stored_patterns"] == "unprocessed")
         info = sc.info
         self.set_patterns(np.asarray(sc.map()))
         self.configure(roi_x=0, roi_y=0, roi_w=0, roi_h=0)
         geo = {k: info[k] for k in ("step_x_um", "step_y_um", "sample_tilt_deg", "detector_tilt_deg")
                if np.isfinite(info[k])}
-        if info["pc"] is not None:
+        if info["pc"] is not None:  # (engine.zig:933-946: a file's pattern centre comes unturned)
             geo["pc"] = tuple(info["pc"])
+            geo["rot"] = (0.0, 0.0, 0.0)
+        if info.get("detector_rot") is not None:
+            geo["rot"] = tuple(info["detector_rot"])
+        if np.isfinite(info.get("px_um", float("nan"))) and info["px_um"] > 0:
+            geo["px_um"] = float(info["px_um"])
         if geo:
             self.set_geometry(**geo)
         self._e.scan_source = {"format": sc.format, "voltage_kv": info["voltage_kv"], "pc_note": info["pc_note"],
-                               "paths": paths}
+                               "paths": paths, "pc": info["pc"], "background": info.get("background"),
+                               "pattern_kinds": info.get("pattern_kinds", [])}
+        self._e.avg = None
         return self
 
     def export(self, path):

@@ -204,6 +204,7 @@ class Engine:
             raise EngineError("PatternTooSmall")
         self.patterns = np.ascontiguousarray(a)
         self.scan_source = None  # the file the patterns came from (Solver.open), if any
+        self.told_no_background = False
         self._pinned = None
         rows, cols = a.shape[:2]
         self.avg = None
@@ -293,10 +294,26 @@ class Engine:
         return ((y0 + np.arange(h))[:, None] * cols + x0 + np.arange(w)[None, :]).reshape(-1).astype(np.int64)
 
     def static_background(self):
-        """engine.zig:1344-1424 — the average of `static_patterns` lattice patterns (none/file)."""
-        if self.set["static_background"] != "average":
+        """engine.zig:1344-1424 — the average of `static_patterns` lattice patterns; "file": the
+        background the scan file stores (none where it stores none); "none"."""
+        kind = self.set["static_background"]
+        if kind == "file":
+            src = (getattr(self, "scan_source", None) or {}).get("background")
+            if src is None:
+                if not getattr(self, "told_no_background", False):
+                    self.log('static background: this scan stores none, so none is subtracted '
+                             '(static_background: "average" takes the patterns\' own)')
+                    self.told_no_background = True
+                return None
+            key = ("file", id(src), self.set["binning"])
+            if self.avg is None or self.avg[0] != key:
+                avg = reduce_image(np.asarray(src, np.float64), self.set["binning"]).astype(np.float32)
+                self.avg = (key, torch.as_tensor(avg, device=self.dev))
+            return self.avg[1]
+        if kind != "average":
             return None
-        if self.avg is None or self.avg[0] != self.set["static_patterns"]:
+        key = ("average", self.set["static_patterns"], self.set["binning"])
+        if self.avg is None or self.avg[0] != key:
             cells = self.lattice(self.set["static_patterns"])
             rows, cols, h, w = self.info()
             flat = self.patterns.reshape(rows * cols, h, w)
@@ -304,7 +321,7 @@ class Engine:
             for i in range(0, len(cells), 1024):
                 acc += flat[cells[i:i + 1024]].sum(0, dtype=np.float64)
             avg = reduce_image(acc / len(cells), self.set["binning"]).astype(np.float32)
-            self.avg = (self.set["static_patterns"], torch.as_tensor(avg, device=self.dev))
+            self.avg = (key, torch.as_tensor(avg, device=self.dev))
             self.log(f"static background: the average of {len(cells)} patterns over the map")
         return self.avg[1]
 

@@ -1,14 +1,17 @@
-"""Scan files (the reference's src/scan.zig, src/ang.zig): the pattern files that need no HDF5
-reader — EDAX .up1 / .up2 (with their scan's .ang for the map's shape, the steps and the pattern
-centre), Oxford .ebsp (uncompressed) and NORDIF Pattern.dat (with Setting.txt). The patterns are
-mapped from the file, not read into memory; numbered row-major over the map, top row first, as
-stored. HDF5 scan files (h5ebsd of kikuchipy, Bruker, EDAX; Oxford .h5oina; EMsoft) are refused:
-this engine has no HDF5 reader.
+"""Scan files (the reference's src/scan.zig, src/ang.zig): EDAX .up1 / .up2 (with their scan's
+.ang for the map's shape, the steps and the pattern centre), Oxford .ebsp (uncompressed), NORDIF
+Pattern.dat (with Setting.txt), and the HDF5 layouts — h5ebsd as kikuchipy, Bruker (Esprit) and
+EDAX (OIM) write it, Oxford's .h5oina and EMsoft's EMEBSD output — through this package's own
+HDF5 reader. Patterns are mapped from the file where they lie in it contiguously (read into
+memory otherwise); numbered row-major over the map, top row first, as stored.
 """
 import math
 import os
 
 import numpy as np
+
+from . import hdf5 as H5
+from . import rotations as R
 
 
 class ScanError(ValueError):
@@ -30,7 +33,8 @@ def _same_step(a, b):
 class Scan:
     """An opened scan: `patterns` [n, h, w] (np.memmap of the file, the stored pixel type) and
     `info` (rows, cols, pat_h, pat_w, step_x_um, step_y_um, pc, pc_note, voltage_kv,
-    sample_tilt_deg, detector_tilt_deg; NaN / None where the file says nothing)."""
+    sample_tilt_deg, detector_tilt_deg, px_um, background (float32 [h, w]), detector_rot (a
+    rotation vector); NaN / None where the file says nothing)."""
 
     def __init__(self, fmt, patterns, info):
         self.format, self.patterns, self.info = fmt, patterns, info
@@ -44,12 +48,15 @@ class Scan:
 def _blank_info():
     nan = float("nan")
     return {"rows": 0, "cols": 0, "pat_h": 0, "pat_w": 0, "step_x_um": nan, "step_y_um": nan, "pc": None,
-            "pc_note": "", "voltage_kv": nan, "sample_tilt_deg": nan, "detector_tilt_deg": nan}
+            "pc_note": "", "voltage_kv": nan, "sample_tilt_deg": nan, "detector_tilt_deg": nan, "px_um": nan,
+            "background": None, "detector_rot": None}
 
 
-def open_scan(paths, rows=0, cols=0, pat_h=0, pat_w=0):
+def open_scan(paths, rows=0, cols=0, pat_h=0, pat_w=0, unprocessed=False, scan_name=""):
     """scan.zig Scan.open — by the first path's extension; rows/cols (and for NORDIF pat_h, pat_w)
-    say what the file does not."""
+    say what the file does not. HDF5: `scan_name` picks the scan group (else the first with
+    EBSD/Data and EBSD/Header); `unprocessed` reads an Oxford file's unprocessed patterns where
+    it stores both kinds."""
     paths = [str(p) for p in paths]
     if not paths:
         raise ScanError("NoScanFile")
@@ -61,8 +68,7 @@ def open_scan(paths, rows=0, cols=0, pat_h=0, pat_w=0):
     if ext == "dat":
         return _open_nordif(paths, rows, cols, pat_h, pat_w)
     if ext in ("h5", "hdf5", "h5ebsd", "h5oina"):
-        raise ScanError(f"UnsupportedFormat: {os.path.basename(paths[0])} is an HDF5 file; this engine reads "
-                        ".up1, .up2, .ebsp and NORDIF .dat scans (pass HDF5 patterns as an array)")
+        return _open_h5(paths[0], rows, cols, unprocessed, scan_name)
     raise ScanError(f"UnknownScanFormat: {os.path.basename(paths[0])}")
 
 
@@ -358,3 +364,289 @@ def _open_nordif(paths, rows, cols, pat_h, pat_w):
         raise ScanError("ScanShapeMismatch")
     pats = np.memmap(paths[0], np.uint8, "r", shape=(n, info["pat_h"], info["pat_w"]))
     return Scan("nordif", pats, info)
+
+
+# ── HDF5 ──
+
+# scan.zig:583-586 — what each writer names the same things: format, pattern datasets (Data),
+# header fields (Header), static background; Oxford's unprocessed patterns beside the processed
+_H5_VENDORS = (
+    ("kikuchipy h5ebsd", ("patterns",), "n_rows", "n_columns", "step_x", "step_y", "sample_tilt",
+     "elevation_angle", "static_background", "", ""),
+    ("Bruker h5ebsd", ("RawPatterns",), "NROWS", "NCOLS", "XSTEP", "YSTEP", "SampleTilt", "CameraTilt",
+     "StaticBackground", "", ""),
+    ("EDAX h5ebsd", ("Pattern",), "nRows", "nColumns", "Step X", "Step Y", "Sample Tilt", "Camera Elevation Angle",
+     "", "", ""),
+    ("Oxford h5oina", ("Processed Patterns",), "Y Cells", "X Cells", "X Step", "Y Step", "Tilt Angle", "",
+     "Processed Static Background", "Unprocessed Patterns", "Unprocessed Static Background"),
+)
+
+
+def _h5_get(h, group, name):
+    """A header number, NaN where absent or not a number."""
+    if not name:
+        return float("nan")
+    try:
+        a = h.child(group, name)
+        return float("nan") if a is None else h.number(a)
+    except H5.H5Error:
+        return float("nan")
+
+
+def _h5_values(h, group, name, limit=1 << 24):
+    try:
+        a = h.child(group, name)
+        if a is None:
+            return None
+        v = h.numbers(a)
+        return v[:limit] if v.size else None
+    except H5.H5Error:
+        return None
+
+
+def _h5_mean(h, group, name):
+    """scan.zig:653-668 — the mean of a per-pattern array."""
+    v = _h5_values(h, group, name)
+    return float("nan") if v is None else float(v.sum() / max(v.size, 1))
+
+
+def _h5_drift(h, group, name, rows, cols):
+    """scan.zig:637-651 — how a per-pattern array changes from one column to the next and from one
+    row to the next, on average (the last column less the first over the columns between, and
+    likewise down the rows)."""
+    nan = (float("nan"), float("nan"))
+    if rows < 2 or cols < 2:
+        return nan
+    v = _h5_values(h, group, name)
+    if v is None or v.size != rows * cols:
+        return nan
+    m = v.reshape(rows, cols)
+    return (float((m[:, -1] - m[:, 0]).sum()) / (rows * (cols - 1)),
+            float((m[-1, :] - m[0, :]).sum()) / (cols * (rows - 1)))
+
+
+def _bunge_matrix(e):
+    """The active rotation Rz(φ1) Rx(Φ) Rz(φ2) of Bunge angles, row-major."""
+    c1, s1, c, s, c2, s2 = math.cos(e[0]), math.sin(e[0]), math.cos(e[1]), math.sin(e[1]), math.cos(e[2]), math.sin(e[2])
+    return np.array([[c1 * c2 - s1 * c * s2, -c1 * s2 - s1 * c * c2, s1 * s],
+                     [s1 * c2 + c1 * c * s2, -s1 * s2 + c1 * c * c2, -c1 * s],
+                     [s * s2, s * c2, c]])
+
+
+# Oxford's nominal detector orientation (0, 90°, 0): Bunge angles of the detector's axes (x along
+# the pattern's columns, y up it, z its normal toward the sample) in the sample's (scan.zig:94-97)
+_OXFORD_NOMINAL = (0.0, math.pi / 2, 0.0)
+
+
+def oxford_detector_rot(e):
+    """scan.zig:121-127 — Oxford's stored detector orientation as the geometry's rotation vector
+    (detector axes), None where not finite or more than 15° from the nominal one."""
+    if not all(math.isfinite(float(v)) for v in e):
+        return None
+    b = _bunge_matrix(_OXFORD_NOMINAL).T @ _bunge_matrix(e)
+    v = np.asarray(R.log_map(R.from_matrix(b)), np.float64)
+    if float(np.linalg.norm(v)) > math.radians(15.0):
+        return None
+    return [float(-v[1]), float(v[0]), float(v[2])]
+
+
+def _h5_pixels(ds):
+    """scan.zig:613-624 — u8 and u16 as stored, f32 as stored, signed 16-bit (Oxford's unprocessed
+    patterns) widened to f32."""
+    k, n = ds.dtype.kind, ds.dtype.size
+    if (k == "u" and n in (1, 2)) or (k == "f" and n == 4) or (k == "i" and n == 2):
+        return
+    raise ScanError("UnsupportedPixelType")
+
+
+def _h5_patterns(h, ds):
+    arr = h.read(ds)
+    if ds.dtype.kind == "i":
+        return arr.astype(np.float32)
+    if ds.dtype.big:
+        return arr.astype(arr.dtype.newbyteorder("="))
+    return arr
+
+
+def _open_h5(path, rows, cols, unprocessed, scan_name):
+    """scan.zig:536-791 — an h5ebsd-like file: the scan group (the named one, else the first group
+    holding EBSD/Data and EBSD/Header), the patterns, and the header's geometry as each writer
+    states it; else EMsoft's EMData/EBSD/EBSDPatterns."""
+    try:
+        h = H5.File(path)
+    except H5.H5Unsupported as e:
+        raise ScanError(f"UnsupportedHdf5: {e}") from None
+    except H5.H5Error as e:
+        raise ScanError(f"BadScanFile: {e}") from None
+    try:
+        return _open_h5_in(h, rows, cols, unprocessed, scan_name)
+    except H5.H5Unsupported as e:
+        raise ScanError(f"UnsupportedHdf5: {e}") from None
+    except H5.H5Error as e:
+        raise ScanError(f"BadScanFile: {e}") from None
+
+
+def _open_h5_in(h, rows, cols, unprocessed, scan_name):
+    scan = None
+    for nm in h.list(h.root):
+        if scan_name and nm != scan_name:
+            continue
+        a = h.child(h.root, nm)
+        if a is None or not h.is_group(a):
+            continue
+        e = h.child(a, "EBSD")
+        if e is not None and h.child(e, "Data") is not None and h.child(e, "Header") is not None:
+            scan = a
+            break
+    if scan is None:
+        a = h.find("EMData/EBSD/EBSDPatterns")
+        if a is not None:
+            return _open_emsoft(h, a, rows, cols)
+        raise ScanError("NoScanInFile")
+    ebsd = h.child(scan, "EBSD")
+    data, header = h.child(ebsd, "Data"), h.child(ebsd, "Header")
+    info = _blank_info()
+    vendor = None
+    for v in _H5_VENDORS:
+        if h.child(header, v[2]) is None:
+            continue
+        processed = next((a for a in (h.child(data, pn) for pn in v[1]) if a is not None), None)
+        raw = h.child(data, v[9]) if v[9] else None
+        if processed is None and raw is None:
+            continue
+        vendor = v
+        if v[9]:
+            info["pattern_kinds"] = [k for k, a in (("processed", processed), ("unprocessed", raw)) if a is not None]
+        info["unprocessed"] = raw is not None and (processed is None or unprocessed)
+        pat_addr = raw if info["unprocessed"] else processed
+        break
+    if vendor is None:
+        raise ScanError("NoPatternsInFile")
+    fmt, _, k_rows, k_cols, k_sx, k_sy, k_tilt, k_det, k_bg, _, k_ubg = vendor
+    ds = h.dataset(pat_addr)
+    if ds.shape is None or len(ds.shape) not in (3, 4):
+        raise ScanError("NoPatternsInFile")
+    _h5_pixels(ds)
+    info["pat_h"], info["pat_w"] = int(ds.shape[-2]), int(ds.shape[-1])
+    n_stored = ds.shape[0] * ds.shape[1] if len(ds.shape) == 4 else ds.shape[0]
+    r, c = _h5_get(h, header, k_rows), _h5_get(h, header, k_cols)
+    info["rows"] = int(r) if r > 0 else 0
+    info["cols"] = int(c) if c > 0 else 0
+    if rows and cols:
+        info["rows"], info["cols"] = rows, cols
+    if info["rows"] * info["cols"] != n_stored:
+        if len(ds.shape) == 4:
+            info["rows"], info["cols"] = int(ds.shape[0]), int(ds.shape[1])
+        elif info["rows"] == 0 or info["cols"] == 0:
+            info["rows"], info["cols"] = 1, int(n_stored)
+        else:
+            raise ScanError("ScanIsNotAFullGrid")
+    info["step_x_um"], info["step_y_um"] = _h5_get(h, header, k_sx), _h5_get(h, header, k_sy)
+    info["sample_tilt_deg"] = _h5_get(h, header, k_tilt)
+    if math.isnan(info["sample_tilt_deg"]) and fmt == "Bruker h5ebsd":
+        info["sample_tilt_deg"] = _h5_get(h, header, "Sample Tilt")
+    info["detector_tilt_deg"] = _h5_get(h, header, k_det)
+    ratio = info["pat_w"] / info["pat_h"]
+    pc = None
+    if fmt == "kikuchipy h5ebsd":
+        pc = [_h5_mean(h, header, k) for k in ("pcx", "pcy", "pcz")]
+        px, binning = _h5_get(h, header, "detector_pixel_size"), _h5_get(h, header, "binning")
+        if px > 1:  # kikuchipy writes 1 when the size is unknown
+            info["px_um"] = px * (binning if binning > 0 else 1)
+        sem = h.child(scan, "SEM")
+        sh = h.child(sem, "Header") if sem is not None else None
+        if sh is not None:
+            info["voltage_kv"] = _h5_get(h, sh, "beam_energy")
+    elif fmt == "Bruker h5ebsd":
+        pc = [_h5_mean(h, data, k) for k in ("PCX", "PCY", "DD")]
+        full, unclipped = _h5_get(h, header, "DetectorFullHeightMicrons"), _h5_get(h, header, "UnClippedPatternHeight")
+        if full > 0 and unclipped > 0:
+            info["px_um"] = full / unclipped
+        # a clipped pattern's PCY is a fraction of the height before clipping, from the top; DD
+        # of the stored height (scan.zig:707-716)
+        if unclipped > info["pat_h"] and not math.isnan(pc[1]):
+            pc[1] *= unclipped / info["pat_h"]
+            info["pc_note"] = ("Bruker's PCY read as a fraction of the pattern's height before clipping "
+                               "(UnClippedPatternHeight), DD of its stored height")
+        info["voltage_kv"] = _h5_get(h, header, "KV")
+    elif fmt == "EDAX h5ebsd":
+        dia = _h5_get(h, header, "Camera Diameter")  # the pattern spans the camera (millimetres)
+        if dia > 0 and info["pat_w"] > 0:
+            info["px_um"] = 1000.0 * dia / info["pat_w"]
+        cal = h.child(header, "Pattern Center Calibration")
+        if cal is not None:
+            x, y, z = (_h5_get(h, cal, k) for k in ("x-star", "y-star", "z-star"))
+            # y from the bottom, x and y fractions of the width and height, z of the smaller of
+            # the two; all zero means not calibrated
+            if x != 0 or y != 0 or z != 0:
+                pc = [x, 1 - y, z * min(ratio, 1)]
+    else:  # Oxford: y from the bottom, y and z fractions of the width; the tilt in radians
+        x, y, z = (_h5_mean(h, data, k) for k in ("Pattern Center X", "Pattern Center Y", "Detector Distance"))
+        pc = [x, 1 - y * ratio, z * ratio]
+        dx, dy, dz = (_h5_drift(h, data, k, info["rows"], info["cols"])
+                      for k in ("Pattern Center X", "Pattern Center Y", "Detector Distance"))
+        info["pc_per_col"] = [dx[0], -dy[0] * ratio, dz[0] * ratio]
+        info["pc_per_row"] = [dx[1], -dy[1] * ratio, dz[1] * ratio]
+        turn = _h5_get(h, header, "Scanning Rotation Angle")
+        info["scan_turn"] = 1
+        if math.isfinite(turn):
+            w = turn % (2 * math.pi)
+            if abs(w - math.pi) <= 1e-4:
+                info["turn_note"] = "a half turn: the beam as the scan signs say"
+            elif min(w, 2 * math.pi - w) <= 1e-4:
+                info["scan_turn"] = -1
+                info["turn_note"] = "none: the beam the other way from what the scan signs say"
+            else:
+                info["turn_note"] = "neither none nor a half turn, which is not read: the beam as the scan signs say"
+        info["sample_tilt_deg"] = math.degrees(info["sample_tilt_deg"])
+        info["tilt_axis_deg"] = math.degrees(_h5_get(h, header, "Tilt Axis"))
+        eu = _h5_values(h, header, "Detector Orientation Euler")
+        if eu is not None and eu.size == 3:
+            info["detector_rot"] = oxford_detector_rot(eu)
+        info["voltage_kv"] = _h5_get(h, header, "Beam Voltage")
+    if pc is not None and not any(math.isnan(v) for v in pc):
+        info["pc"] = tuple(float(v) for v in pc)
+    bg_name = k_ubg if info.get("unprocessed") else k_bg
+    a = h.child(header, bg_name) if bg_name else None
+    if a is not None:
+        try:
+            bds = h.dataset(a)
+            whole = bds.elements == info["pat_h"] * info["pat_w"]
+            if k_ubg:  # (an Oxford acquisition's: only this detector's pixels, a row at a time)
+                whole = bds.shape == (info["pat_h"], info["pat_w"])
+            if whole and bds.dtype.kind in "uif":
+                info["background"] = np.asarray(h.read(bds), np.float32).reshape(info["pat_h"], info["pat_w"])
+        except H5.H5Error:
+            pass
+    pats = _h5_patterns(h, ds).reshape(n_stored, info["pat_h"], info["pat_w"])
+    return Scan(fmt, pats, info)
+
+
+def _open_emsoft(h, pat_addr, rows, cols):
+    """scan.zig:793-838 — EMsoft's EMEBSD output: patterns (n, h, w) and the simulation's detector
+    parameters (EBSDNameList: xpc, ypc pixel offsets of the pattern centre from the detector's
+    middle, L and the pixel size delta in micrometres, at the unbinned size numsx × numsy)."""
+    ds = h.dataset(pat_addr)
+    if ds.shape is None or len(ds.shape) != 3:
+        raise ScanError("NoPatternsInFile")
+    k, sz = ds.dtype.kind, ds.dtype.size
+    if not ((k == "u" and sz in (1, 2)) or (k == "f" and sz == 4)):
+        raise ScanError("UnsupportedPixelType")
+    info = _blank_info()
+    n = int(ds.shape[0])
+    info["pat_h"], info["pat_w"] = int(ds.shape[1]), int(ds.shape[2])
+    info["rows"], info["cols"] = 1, n
+    if rows and cols and rows * cols == n:
+        info["rows"], info["cols"] = rows, cols
+    nml = h.find("NMLparameters/EBSDNameList")
+    if nml is not None:
+        xpc, ypc, L, delta, numsx, numsy = (_h5_get(h, nml, k) for k in ("xpc", "ypc", "L", "delta", "numsx", "numsy"))
+        if delta > 0 and numsx > 0 and numsy > 0 and not math.isnan(xpc + ypc + L):
+            info["pc"] = (0.5 - xpc / numsx, 0.5 - ypc / numsy, L / (numsy * delta))
+            info["px_um"] = delta * numsy / info["pat_h"]
+        info["detector_tilt_deg"] = _h5_get(h, nml, "thetac")
+        info["voltage_kv"] = _h5_get(h, nml, "energymax")
+        mc = h.find("NMLparameters/MCCLNameList")
+        if mc is not None:
+            info["sample_tilt_deg"] = _h5_get(h, mc, "sig")
+    return Scan("EMsoft patterns", _h5_patterns(h, ds), info)
