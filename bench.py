@@ -919,7 +919,12 @@ def nickel_main(a):
     one = timed_index()
     s.configure(sweeps=2, sweep_bandwidth=32, bandwidth=64)
     two = timed_index()
-    s.configure(sweeps=1, nlpar=True)  # one pass of 7 x 7, lambda 0.7 (the defaults)
+    # the BF16 form of the spectrum (hi + lo split for l <= 16; the headline's), same settings
+    s.configure(sweeps=1, precision="bf16")
+    one_bf16 = timed_index()
+    s.configure(sweeps=2)
+    two_bf16 = timed_index()
+    s.configure(sweeps=1, precision="f32", nlpar=True)  # one pass of 7 x 7, lambda 0.7 (the defaults)
     averaged = timed_index()
     s.configure(nlpar=False)
     gan = _testdata("gan", "GaN_master_20kV.npz")
@@ -953,9 +958,11 @@ def nickel_main(a):
     line = {"metric": "patterns/s indexed, kikuchipy's nickel scan (55x75 of 60x60), L=64 one pass, 1 B200",
             "value": one["value"], "unit": "patterns/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
             "higher_is_better": True, "dtype": "bf16+f32", "data": "kikuchipy nickel_ebsd_large (real, h5ebsd)",
-            "config": {"workload": "nickel scan 55x75 of 60x60 u8, Ni master 501^2 (m-3m), defaults; timed from the "
-                                   "patterns on the host to the results on the host (Solver.index)", "patterns": n},
-            "one_pass": one, "two_sweeps": two, "nlpar_7x7": averaged, "nickel_and_gan": phases, "fits": fits, "open_s": round(t_open, 3),
+            "config": {"workload": "nickel scan 55x75 of 60x60 u8, Ni master 501^2 (m-3m), defaults (precision f32, "
+                                   "the drop-in form; bf16_* the BF16 form); timed from the patterns on the host to the "
+                                   "results on the host (Solver.index)", "patterns": n},
+            "one_pass": one, "two_sweeps": two, "bf16_one_pass": one_bf16, "bf16_two_sweeps": two_bf16,
+            "nlpar_7x7": averaged, "nickel_and_gan": phases, "fits": fits, "open_s": round(t_open, 3),
             "reference_published": {"one_pass": 22700, "two_sweeps": 67000, "median_deg": 0.32, "within_3deg": 0.99,
                                      "mean_ncc": 0.53, "nlpar_mean_ncc": 0.62, "nickel_of_two_phases": 0.999,
                                      "hardware": "desktop GPU"}}
