@@ -65,6 +65,8 @@ def parse():
                          "nickel: the reference's real scan (kikuchipy's nickel scan, h5ebsd), one pass and two sweeps")
     ap.add_argument("--large", type=int, default=250000, help="large: patterns of the scan (config 5 names 1 000 000)")
     ap.add_argument("--scans", type=int, default=64, help="uneven: number of scans")
+    ap.add_argument("--kernel-split", action="store_true",
+                    help="nickel: also the device time by kernel (torch.profiler), printed to stderr")
     ap.add_argument("--max-count", type=int, default=200000, help="uneven: the longest scan (log-uniform from 1000)")
     return ap.parse_args()
 
@@ -954,6 +956,30 @@ def nickel_main(a):
             if k in out:
                 fits[name][k] = out[k]
         s.set_geometry(pc=tuple(pc_file), plane_kind="none")
+    split = {}
+    if a.kernel_split:  # device time by kernel over 5 calls in each form (CUPTI through torch.profiler)
+        from torch.profiler import ProfilerActivity, profile
+
+        for prec in ("f32", "bf16"):
+            s.configure(precision=prec)
+            s.index()
+            torch.cuda.synchronize()
+            with profile(activities=[ProfilerActivity.CUDA]) as prof:
+                for _ in range(5):
+                    s.index()
+                torch.cuda.synchronize()
+            rows_ = [(ev.key, ev.count, ev.self_device_time_total) for ev in prof.key_averages()
+                     if ev.self_device_time_total > 0]
+            total = sum(r[2] for r in rows_)
+            rows_.sort(key=lambda r: -r[2])
+            split[prec] = [{"kernel": k[:80], "launches": c, "us_per_call": round(t / 5, 1),
+                            "share": round(t / total, 4)} for k, c, t in rows_[:12]]
+            print(f"kernel split, precision {prec}, 5 index() calls, {total / 5:.0f} us of device time a call:",
+                  file=sys.stderr)
+            for r in split[prec]:
+                print(f"  {r['share'] * 100:5.1f} %  {r['us_per_call']:8.1f} us/call  {r['launches']:3d}  {r['kernel']}",
+                      file=sys.stderr)
+        s.configure(precision="f32")
     s.close()
     line = {"metric": "patterns/s indexed, kikuchipy's nickel scan (55x75 of 60x60), L=64 one pass, 1 B200",
             "value": one["value"], "unit": "patterns/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
@@ -963,6 +989,7 @@ def nickel_main(a):
                                    "results on the host (Solver.index)", "patterns": n},
             "one_pass": one, "two_sweeps": two, "bf16_one_pass": one_bf16, "bf16_two_sweeps": two_bf16,
             "nlpar_7x7": averaged, "nickel_and_gan": phases, "fits": fits, "open_s": round(t_open, 3),
+            **({"kernel_split": split} if split else {}),
             "reference_published": {"one_pass": 22700, "two_sweeps": 67000, "median_deg": 0.32, "within_3deg": 0.99,
                                      "mean_ncc": 0.53, "nlpar_mean_ncc": 0.62, "nickel_of_two_phases": 0.999,
                                      "hardware": "desktop GPU"}}
