@@ -165,6 +165,8 @@ class Engine:
         self.tuned = {}  # what tune() chose for the way work is cut up (device_batch)
         self._pinned = None
         self._pin_buf = None  # the page-locked buffer behind _pinned, reused across scans
+        self._index_calls = 0  # index runs and index_cells calls over the scan since set_patterns
+        self._ring, self._ring_i = [], 0  # two page-locked slots a scan not pinned whole streams through
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
         self.geo_given = Geometry()  # the geometry as given (set_geometry), where a full fit starts
@@ -206,6 +208,7 @@ class Engine:
         self.scan_source = None  # the file the patterns came from (Solver.open), if any
         self.told_no_background = False
         self._pinned = None
+        self._index_calls = 0
         rows, cols = a.shape[:2]
         self.avg = None
         self.chance_key = None
@@ -596,7 +599,7 @@ class Engine:
                 lst, counts, nbr = self.nlpar_window(cells[t0:t0 + m])
             guess = 2 * m
             nw = len(lst)
-            raw = self.buf("nl_raw", nw * sh * sw, self.pinned().dtype)[: nw * sh * sw].view(nw, sh, sw)
+            raw = self.buf("nl_raw", nw * sh * sw, self.raw_dtype())[: nw * sh * sw].view(nw, sh, sw)
             self.upload_raw(lst, raw, torch.cuda.current_stream())
             loaded = self.buf("nl_loaded", nw * px)
             sb = N.load().zeb_prep_scratch_bytes(nw, h, w, 0.0)
@@ -658,7 +661,7 @@ class Engine:
             return out[: h * w].reshape(h, w).cpu().numpy()
         if stage == 2 and self.set["nlpar"]:
             return self.nlpar_average(cells, account=True)[: h * w].reshape(h, w).cpu().numpy()
-        raw = self.buf("raw_up", sh * sw, self.pinned().dtype)[: sh * sw].view(1, sh, sw)
+        raw = self.buf("raw_up", sh * sw, self.raw_dtype())[: sh * sw].view(1, sh, sw)
         self.upload_raw(cells, raw, torch.cuda.current_stream())
         oh, ow = (sh, sw) if full else (h, w)
         out = torch.empty(oh * ow, dtype=torch.float32, device=self.dev)
@@ -727,7 +730,7 @@ class Engine:
         """The cells' stored patterns to the device (from the pinned scan), preprocessed."""
         rows, cols, h, w = self.info()
         n = len(cells)
-        raw = self.buf("raw_up", max(n, 1) * h * w, self.pinned().dtype)[: n * h * w].view(n, h, w)
+        raw = self.buf("raw_up", max(n, 1) * h * w, self.raw_dtype())[: n * h * w].view(n, h, w)
         self.upload_raw(cells, raw, torch.cuda.current_stream())
         return self.preprocess(raw, n, cells)
 
@@ -944,20 +947,69 @@ class Engine:
             self._pinned.copy_(src)
         return self._pinned
 
+    STAGE_BYTES = 64 << 20
+
+    def raw_dtype(self):
+        """The stored pixel type as a torch dtype."""
+        return torch.from_numpy(np.zeros(1, self.patterns.dtype)).dtype
+
+    def whole_pinned(self):
+        """Whether uploads come from a page-locked copy of the whole scan: when it is made already,
+        when the buffer kept from earlier scans holds it (no page-locking to pay), or from the
+        scan's second index run on (a scan indexed once streams through the staging slots:
+        page-locking gigabytes for one run costs more than the run)."""
+        if self._pinned is not None:
+            return True
+        nbytes = self.patterns.size * self.patterns.itemsize
+        return (self._pin_buf is not None and self._pin_buf.numel() >= nbytes) or self._index_calls >= 2
+
+    def _slot(self):
+        if not self._ring:
+            self._ring = [[torch.empty(self.STAGE_BYTES, dtype=torch.uint8, pin_memory=True), None] for _ in range(2)]
+        slot = self._ring[self._ring_i]
+        self._ring_i ^= 1
+        if slot[1] is not None:
+            slot[1].synchronize()  # the copy that last read this slot has finished
+        return slot
+
     def upload_raw(self, cells, dst, stream):
         """Enqueue on `stream` the copies of the given cells' stored patterns into dst[0:n], one
-        per run of consecutive cells."""
-        src = self.pinned()
+        per run of consecutive cells: from the page-locked copy of the scan, or (a scan indexed
+        once) through two page-locked slots of 64 MB in turn, each filled on the host while the
+        other's copy runs."""
         cells = np.asarray(cells, np.int64)
         if len(cells) == 0:
             return
         cut = np.flatnonzero(np.diff(cells) != 1) + 1
         starts = np.concatenate([[0], cut])
         ends = np.concatenate([cut, [len(cells)]])
+        if self.whole_pinned():
+            src = self.pinned()
+            with torch.cuda.stream(stream):
+                for a0, a1 in zip(starts, ends):
+                    c0 = int(cells[a0])
+                    dst[a0:a1].copy_(src[c0:c0 + (a1 - a0)], non_blocking=True)
+            return
+        rows, cols, h, w = self.info()
+        flat = self.patterns.reshape(rows * cols, h, w)
+        per = h * w * self.patterns.itemsize
+        most = max(1, self.STAGE_BYTES // per)
+        if per > self.STAGE_BYTES:
+            raise EngineError("PatternTooLarge: one pattern exceeds the staging slot")
+        td = self.raw_dtype()
         with torch.cuda.stream(stream):
             for a0, a1 in zip(starts, ends):
-                c0 = int(cells[a0])
-                dst[a0:a1].copy_(src[c0:c0 + (a1 - a0)], non_blocking=True)
+                c, o, left = int(cells[a0]), int(a0), int(a1 - a0)
+                while left > 0:
+                    k = min(left, most)
+                    slot = self._slot()
+                    host = slot[0].numpy()[: k * per].view(self.patterns.dtype).reshape(k, h, w)
+                    np.copyto(host, flat[c:c + k])
+                    dst[o:o + k].copy_(slot[0][: k * per].view(td).view(k, h, w), non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(stream)
+                    slot[1] = ev
+                    c, o, left = c + k, o + k, left - k
 
     def refine_patterns(self, cells, quaternions, phase, trust, rounds, gradient):
         """planefit.zig:570-622 (settle, k = 6) for the given cells against one phase."""
@@ -1014,9 +1066,10 @@ class Engine:
             raise EngineError("NoPhases")
         if n == 0:
             return np.zeros((n_ph, 0, 8), np.float32)
+        self._index_calls += 1  # (a scan indexed a second time is pinned whole: whole_pinned)
         self.prepare(bandwidth, method, grid)
         rows, cols, h, w = self.info()
-        raw = self.buf("raw_up", n * h * w, self.pinned().dtype).view(-1)[: n * h * w].view(n, h, w)
+        raw = self.buf("raw_up", n * h * w, self.raw_dtype()).view(-1)[: n * h * w].view(n, h, w)
         self.upload_raw(cells, raw, torch.cuda.current_stream())
         recs = self.run_device(raw, cells, bandwidth, method=method, grid=grid)
         self._last_fz = self.fz_of(recs).cpu().numpy()
@@ -1111,12 +1164,11 @@ class Engine:
         self.prepare(bandwidth, method, grid)
         rows, cols, h, w = self.info()
         B = min(self.device_batch(), len(cells))
-        pin = self.pinned()
         comp = torch.cuda.current_stream()
         if getattr(self, "_copy_stream", None) is None:
             self._copy_stream = torch.cuda.Stream(device=self.dev)
         cps = self._copy_stream
-        raw = [self.buf(f"raw_pipe{k}", B * h * w, pin.dtype)[: B * h * w].view(B, h, w) for k in range(2)]
+        raw = [self.buf(f"raw_pipe{k}", B * h * w, self.raw_dtype())[: B * h * w].view(B, h, w) for k in range(2)]
         # the copy stream starts after everything already queued on the compute stream: memory the
         # caching allocator hands out here may have been freed by work still pending there
         cps.wait_stream(comp)
@@ -1328,6 +1380,7 @@ class Engine:
         each through index_pipelined: the same cells, records and landing as repeated
         index_step calls, with uploads, kernels, readbacks and landing overlapped."""
         s = self.set
+        self._index_calls += 1
         while len(self.index_cells_list) - self.index_done > 0 and not self.cancel:
             bw, dg, method = s.sweep(self.index_sweep)
             stop = [False]
