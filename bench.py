@@ -78,108 +78,92 @@ def scan_shape(n):
     return int(math.ceil(n / cols)), cols
 
 
-# ── the reference's algorithm on the host (the oracle restatement) ──
+# ── the reference's algorithm on the host (the oracle: the checker and the CPU baseline) ──
 
-def _oracle_world(seed=2):
-    """Inputs of the CPU legs: the master and a handful of patterns, made on the host."""
-    import oracle.detector as od
+ORACLE_CELLS = 1024  # the lattice of cells the oracle indexes (>= 1000, spread over the map's grains)
+
+
+def oracle_scan(raw_sheets, static_bg, L_=L, refine=True, baked=None):
+    """The oracle's state for the workload (FP64): the master baked for this detector, its tables
+    at L_, the map-centre window's denominators, the static background given."""
     import oracle.geometry as og
-    import oracle.master as om
-    import oracle.prep as op
-    import oracle.spherical as osp
+    import oracle.pipeline as opl
     from zebsdsolve_b200 import synthetic as syn
 
-    sheets = syn.master_sheets(seed, side=401, lmax=96, group="432").reshape(-1)
-    m = om.Master(401, sheets, syn.group_matrices("432"), 30)
     geo = og.Geometry(pc=PC, sample_tilt_deg=70.0)
-    frame = geo.frame()
-    mask = og.mask_of(H, W)
-    return {"sheets": sheets, "m": m, "geo": geo, "frame": frame, "mask": mask}
+    return opl.Scan(np.asarray(raw_sheets, np.float64).reshape(-1), 401, syn.group_matrices("432"), geo, H, W, L_,
+                    static_bg=static_bg, refine=refine, baked=baked)
 
 
-def _oracle_setup(L_):
-    import oracle.master as om
+def _oracle_cell(raw):
+    import oracle.pipeline as opl
+
+    r = opl._one(raw)
+    return r["q"], r["ncc"], r["nmi"]
+
+
+def oracle_run(scan, raws):
+    """The oracle over the stored patterns `raws` on the host cores (oracle.pipeline.index_many):
+    (records [(q in the fundamental zone, NCC, NMI)], patterns/s, cores, seconds)."""
+    import oracle.pipeline as opl
+
+    recs, dt, cores = opl.index_many(scan, raws)
+    return [(r["q"], r["ncc"], r["nmi"]) for r in recs], len(recs) / dt, cores, dt
+
+
+def parity_of(oracle_recs, rotations, q, ncc, nmi):
+    """Each cell's record against the oracle's: the misorientation (degrees, modulo the group) and
+    the NCC and NMI differences."""
+    import oracle.sym as osym
+
+    oq = np.array([r[0] for r in oracle_recs], np.float64)
+    oncc = np.array([r[1] for r in oracle_recs])
+    onmi = np.array([r[2] for r in oracle_recs])
+    dis = np.degrees(osym.disorientation(np.asarray(q, np.float64).reshape(-1, 4), oq, rotations))
+    dn = np.abs(np.asarray(ncc, np.float64) - oncc)
+    dm = np.abs(np.asarray(nmi, np.float64) - onmi)
+    return {"n": int(len(dis)), "within_0.1deg": round(float((dis <= 0.1).mean()), 5),
+            "median_deg": round(float(np.median(dis)), 5), "p99_deg": round(float(np.percentile(dis, 99)), 5),
+            "max_deg": round(float(dis.max()), 5), "ncc_within_1e-3": round(float((dn <= 1e-3).mean()), 5),
+            "ncc_abs_max": float(f"{dn.max():.3g}"), "ncc_abs_p99": float(f"{np.percentile(dn, 99):.3g}"),
+            "nmi_abs_max": float(f"{dm.max():.3g}")}
+
+
+def host_workload(rank=0):
+    """The workload's lattice cells made on the host, for a run without a GPU (the reference arm):
+    the same master and grain map (same seeds), each cell's pattern simulated by the oracle's
+    projection of the baked master and given the same noise model (Poisson counts of
+    1000·(0.6 + 0.4·m)·B, NumPy's generator). Returns (raws [cells][H][W] u16, scan, cells)."""
     import oracle.detector as od
-    import oracle.spherical as osp
+    import oracle.geometry as og
+    import oracle.pipeline as opl
+    from zebsdsolve_b200 import synthetic as syn
 
-    w = _oracle_world()
-    tb = osp.Tables(L_)
-    hm = om.Harmonics(w["m"], w["sheets"], L_)
-    pt = osp.PhaseTables(tb, hm, om.fold_of(hm.rules))
-    t0 = w["geo"].translation(H, W)
-    walm, wst = osp.coefficients(tb, None, t0, w["frame"], w["mask"], flags=osp.FLAG_WINDOW, shape=(H, W))
-    rden = osp.window_denominators(tb, pt, walm, wst[0])
-    grad = od.gradient_table(w["sheets"], 401)
-    return w, tb, hm, pt, rden, grad
-
-
-_ORACLE = {}
-
-
-def _oracle_pattern(args):
-    """One pattern through the oracle's path: filters, sphere, correlation, peak, refinement, NMI."""
-    import oracle.detector as od
-    import oracle.prep as op
-    import oracle.spherical as osp
-
-    raw, q0 = args
-    if "state" not in _ORACLE:
-        _ORACLE["state"] = _oracle_setup(L)
-    w, tb, hm, pt, rden, grad = _ORACLE["state"]
-    t = w["geo"].translation(H, W)
-    pat = op.run(raw, static=None, dynamic="subtract", dynamic_sigma=0.15 * W, mask=w["mask"])
-    g, _ = osp.coefficients(tb, pat, t, w["frame"], w["mask"])
-    vol = osp.correlation_volume(tb, pt, hm.f, g) * rden
-    q, v0, _, _ = osp.peak(tb, pt, vol)
-    qb, best, step = od.refine(grad, 401, w["frame"], t, q, pat, w["mask"])
-    v = od.nmi(w["sheets"], 401, w["frame"], t, qb, pat, w["mask"])
-    return float(best), float(v)
-
-
-def cpu_leg(seconds, seed=4, warmup=1, steps=0):
-    """The oracle over bounded samples of the workload in a spawn pool over the host cores: after
-    one set-up round and `warmup` rounds, timed rounds of one pattern per core until at least
-    `steps` rounds and `seconds` have passed. Returns (patterns/s, cores, sample description)."""
-    import multiprocessing as mp
-
-    import oracle.detector as od
-
-    w = _oracle_world()
-    rng = np.random.default_rng(seed)
-    cores = min(len(os.sched_getaffinity(0)), 64)
-    n = 2 * cores
-    q = rng.normal(size=(n, 4))
-    q /= np.linalg.norm(q, axis=1, keepdims=True)
-    t = w["geo"].translation(H, W)
+    rows, cols = ROWS, COLS
+    sheets = syn.master_sheets(2, side=401, lmax=96, group="432")
+    rng = np.random.default_rng(100 + rank)
+    q, _ = syn.grain_map(rng, rows, cols, GRAINS, SPREAD_DEG)
+    cells = opl.lattice(rows, cols, ORACLE_CELLS)
+    geo = og.Geometry(pc=PC, sample_tilt_deg=70.0)
+    baked = opl.bake(sheets, 401, opl.pixel_angle(geo, H))
+    frame, t0 = geo.frame(), geo.translation(H, W)
     yy, xx = np.meshgrid(np.arange(H) + 0.5 - H / 2, np.arange(W) + 0.5 - W / 2, indexing="ij")
     B = np.exp(-(xx ** 2 + yy ** 2) / (2 * (0.4 * W) ** 2))
     B *= B.size / B.sum()
-    pats = []
-    for i in range(n):
-        sim = od.project(w["sheets"], 401, w["frame"], t, q[i], H, W)
-        pats.append(np.clip(rng.poisson(np.maximum(1000 * (0.6 + 0.4 * sim) * B, 0)), 0, 65535).astype(np.uint16))
-    # one thread per worker: the workers' BLAS and FFT pools would otherwise each take every core
-    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS"):
-        os.environ[k] = "1"
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        # every round is bounded: a round that does not finish in `limit` seconds raises
-        limit = 600.0
-        pool.map_async(_oracle_pattern, [(pats[i], q[i]) for i in range(cores)]).get(limit)  # set-up in every worker
-        for _ in range(warmup):
-            pool.map_async(_oracle_pattern, [(pats[i % n], q[i % n]) for i in range(cores)]).get(limit)
-        done = rounds = 0
-        t0 = time.perf_counter()
-        while True:
-            pool.map_async(_oracle_pattern, [(pats[(i + rounds) % n], q[(i + rounds) % n])
-                                             for i in range(cores)]).get(limit)
-            done += cores
-            rounds += 1
-            if rounds >= steps and time.perf_counter() - t0 > seconds:
-                break
-        dt = time.perf_counter() - t0
-    return done / dt, cores, (f"{done} patterns of the workload (60x60 u16, L=64, filtered, correlated, refined, NMI) "
-                              f"through the FP64 NumPy restatement, {rounds} rounds of {cores} in {dt:.1f} s")
+    noise = np.random.default_rng(7 + rank)
+    raws = np.empty((len(cells), H, W), np.uint16)
+    for k, c in enumerate(cells):
+        sim = od.project(baked, 401, frame, t0, q[c], H, W)
+        raws[k] = np.clip(noise.poisson(np.maximum(1000 * (0.6 + 0.4 * sim) * B, 0)), 0, 65535)
+    # the lattice is the static background's lattice: its mean is the scan's static background
+    scan = oracle_scan(sheets, raws.astype(np.float64).mean(0), baked=baked)
+    return raws, scan, cells
+
+
+def config_of(a, n):
+    """The workload as the bench line names it (both arms)."""
+    return {"workload": WORKLOAD, "patterns_per_gpu": n, "bandwidth": L, "precision": a.precision,
+            "device_batch": min(a.batch, n), "l2": "inputs (720 MB) larger than L2, no flush"}
 
 
 # ── the device ──
@@ -398,8 +382,7 @@ def device_main(a):
         "value": round(value, 1), "unit": "patterns/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if a.precision == "f32" else "bf16+f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "patterns_per_gpu": n, "bandwidth": L, "precision": a.precision,
-                   "device_batch": batch, "l2": "inputs (720 MB) larger than L2, no flush"},
+        "config": config_of(a, n),
         "e2e": {"value": round(e2e, 1), "unit": "patterns/s", "h2d_bytes_per_step": int(n * H * W * 2),
                 "d2h_bytes_per_step": int(n * (8 + 4) * 4 * len(e.phases))},
         "gpu_launches": int(launches),
@@ -413,8 +396,27 @@ def device_main(a):
         line["fp32_form"] = fp32
         line["vs_fp32_form"] = {"value": round(value / fp32["value"], 3), "e2e": round(e2e / fp32["e2e"], 3)}
     if not a.no_cpu:
-        v, cores, sample = cpu_leg(a.cpu_seconds)
-        line["cpu_baseline"] = {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port", "sample": sample}
+        # the oracle (FP64) on a lattice of the workload's own stored patterns, with the GPU path's
+        # settings (static background of the same lattice average, dynamic background, mask, the
+        # master baked for this detector, 8 refinement iterations): the CPU baseline's timing and
+        # each form's parity, cell by cell
+        import oracle.pipeline as opl
+
+        ocells = opl.lattice(rows, cols, ORACLE_CELLS)
+        scan = oracle_scan(sheets, opl.static_average(pats, rows, cols, 1024))
+        orecs, v, cores, dt = oracle_run(scan, pats[ocells])
+        line["cpu_baseline"] = {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port",
+                                "sample": f"{len(ocells)} cells on a lattice over the map (their own stored patterns: "
+                                          f"filtered, correlated at L={L}, refined, NMI) through the FP64 oracle in "
+                                          f"{dt:.1f} s"}
+        forms = {a.precision: r}
+        if fp32 is not None:
+            forms["f32"] = r32
+        line["oracle_parity"] = {"cells": f"{len(ocells)} on a lattice over the {rows}x{cols} map",
+                                 "bar": "within 0.1 deg for >= 99.9 % and |dNCC| <= 1e-3"}
+        for k, rr in forms.items():
+            line["oracle_parity"][k] = parity_of(orecs, scan.rotations, rr["quaternions"].reshape(-1, 4)[ocells],
+                                                 rr["ncc"].reshape(-1)[ocells], rr["nmi"].reshape(-1)[ocells])
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -585,18 +587,53 @@ def uneven_main(a):
 
 
 def reference_main(a):
+    """The reference's algorithm on the host cores (the oracle, FP64 NumPy; the reference engine
+    itself, Zig + WGSL on wgpu-native, cannot run on this box): a step indexes one pattern per
+    core from the workload's lattice of cells, made on the host (host_workload); W untimed steps,
+    then K timed ones. Under torchrun only rank 0 runs."""
+    import multiprocessing as mp
+
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    v, cores, sample = cpu_leg(0.0, warmup=a.warmup, steps=a.steps)
+    raws, scan, cells = host_workload()
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS"):
+        os.environ[k] = "1"
+    cores = max(1, min(len(os.sched_getaffinity(0)), 64))
+    ctx = mp.get_context("spawn")
+    limit = 600.0
+    nxt = [0]
+
+    def step(pool):
+        sel = [raws[(nxt[0] + i) % len(raws)] for i in range(cores)]
+        nxt[0] += cores
+        return pool.map_async(_oracle_cell, sel, chunksize=1).get(limit)
+
+    import oracle.pipeline as opl
+    import oracle.spherical as osp
+
+    osp._wigner_blocks(scan.tb)  # built once here and shipped to the workers with the scan
+    with ctx.Pool(cores, initializer=opl._init, initargs=(scan,)) as pool:
+        for _ in range(max(a.warmup, 1)):
+            step(pool)
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            step(pool)
+        dt = time.perf_counter() - t0
+    done = a.steps * cores
+    v = done / dt
+    n = ROWS * COLS if a.patterns == ROWS * COLS else a.patterns
     line = {"impl": "reference", "metric": "patterns/s indexed+refined on 1 B200, BF16 form vs plain FP32 at <=0.1 deg error",
             "value": round(v, 3), "unit": "patterns/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "bandwidth": L},
-            "cpu_baseline": {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port", "sample": sample},
+            "ms_per_step": round(1e3 * dt / a.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(a, n),
+            "cpu_baseline": {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port",
+                             "sample": f"{done} patterns of the workload's lattice of {len(cells)} cells (made on the "
+                                       f"host: the same master and grain map), one per core a step, filtered, "
+                                       f"correlated at L={L}, refined and scored through the FP64 oracle"},
             "e2e": {"value": round(v, 3), "unit": "patterns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference engine (Zig + WGSL on wgpu-native) cannot be built or run here; its algorithm is timed "
-                    "as the FP64 NumPy restatement on the host cores"}
+            "note": "the reference engine (Zig + WGSL on wgpu-native) cannot be built or run here; its algorithm is "
+                    "timed as the FP64 oracle on the host cores"}
     print(json.dumps(line), flush=True)
 
 

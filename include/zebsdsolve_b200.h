@@ -237,9 +237,11 @@ int zeb_correlate_peaks(const float* U, int n_items, const zeb_so3_dims_t* d, co
  * The candidates' scratch is a file-scope __device__ array of ZEB_PEAKS_STATIC_SLABS (item, j)
  * slabs (4 MiB; every GPU that loads the library holds it until the process exits), so one call
  * takes at most ZEB_PEAKS_STATIC_SLABS / nb items (8065 at L = 64); larger calls fail with
- * ZEB_ESIZE and a message. The first call on a device looks the array's device address up
- * (cudaGetSymbolAddress, once per device, with that device current); make that first call
- * before any stream capture. Every call shares the one array and leaves its candidates in it:
+ * ZEB_ESIZE and a message. The first call in a CUDA context looks the array's device address up
+ * (cudaGetSymbolAddress, with that context current) and keeps it for that context, keyed by the
+ * context's unique ID: after a cudaDeviceReset, or with another driver-API context current on the
+ * device, the next call is again a first call. Make each context's first call before any stream
+ * capture in it. Every call shares the one array and leaves its candidates in it:
  * calls that overlap on the GPU (other streams, other threads) race and must be serialized by
  * the caller. Nothing in it needs to start at zero: each call writes every candidate it reads.
  * Allocates nothing (no cudaMalloc, cudaFree or allocating library routine). */

@@ -111,6 +111,20 @@ class PhaseTables:
         self.nb = tables.n // 2 + 1
 
 
+def _wigner_blocks(tables):
+    """d^l_{k,x}(π/2) for signed k, x in [−l, l], one (2l+1)² block per degree l, kept on the tables
+    (sh.zig:296-302 element by element, as correlation_volume reads them)."""
+    blocks = getattr(tables, "_blocks", None)
+    if blocks is None:
+        tab = tables.wigner
+        blocks = []
+        for l in range(tables.L):
+            ks = range(-l, l + 1)
+            blocks.append(np.array([[sh.d_half_pi(tab, l, k, x) for x in ks] for k in ks]))
+        tables._blocks = blocks
+    return blocks
+
+
 def correlation_volume(tables, ph, f, g):
     """so3.wgsl:1-43 — C[j, iq, ia] = Σ T[k,m',m] e^{−i(k b_j + m' a + m c)} on the Euler grid
     (b_j = 2πj/n for j ≤ n/2, a = 2π ia/n, c = 2π iq/n), from
@@ -120,10 +134,11 @@ def correlation_volume(tables, ph, f, g):
     fold, nc, mu_max = ph.fold, ph.nc, ph.mu_max
     tab = tables.wigner
     A = np.zeros((n, n, nc), np.complex128)
+    blocks = _wigner_blocks(tables)
     for l in range(L):
         ks = np.arange(-l, l + 1)
-        # d^l_{k, x} for signed k, x in [−l, l]
-        D = np.array([[sh.d_half_pi(tab, l, int(k), int(x)) for x in ks] for k in ks])
+        # d^l_{k, x} for signed k, x in [−l, l] (the same values for every pattern: built once)
+        D = blocks[l]
         gl = np.array([sh.signed_coef(L, g, l, int(x)) for x in ks])
         mus = [mu for mu in range(-mu_max, mu_max + 1) if abs(mu * fold) <= l]
         for mu in mus:

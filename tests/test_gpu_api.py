@@ -94,3 +94,22 @@ def test_tune_changes_no_result(scan):
     r2 = s.index()
     for k in ("quaternions", "ncc", "nmi", "phase", "z", "sweep"):
         assert np.array_equal(r1[k], r2[k]), k
+
+
+def test_a_scan_stepped_through_once_is_not_page_locked_whole(scan):
+    """index_step calls index_cells once per ~4096 cells; the scan then counts as indexed once, so
+    its uploads stream through the two staging slots and the whole scan is never page-locked.
+    A second pass over it (here a Solver.index after the step loop) is what page-locks it."""
+    s, _ = _solver(scan)
+    e = s._e
+    calls = []
+    real = e.pinned
+    e.pinned = lambda: calls.append(1) or real()
+    s.configure(batch=4)  # two steps over the 96 cells: 4 × 16 cells, then the 32 left
+    s.index_begin()
+    steps = 0
+    while s.index_step() > 0:
+        steps += 1
+    assert steps >= 1 and not calls and e._pinned is None
+    s.index()
+    assert calls and e._pinned is not None

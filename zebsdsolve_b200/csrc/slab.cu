@@ -9,6 +9,8 @@
 // (j·nc + c)·n + ia; each slab keeps its best (first index of equal values).
 // k_peak_finish then takes each item's best slab, re-evaluates the six neighbours of the peak by
 // direct sums over m' and fits the parabolic vertex along a, c and b (so3.wgsl:665-796).
+#include <cuda.h>
+
 #include <mutex>
 
 #include "abi_util.cuh"
@@ -536,14 +538,49 @@ extern "C" int zeb_rden_build(const float* vol_f, const float* vol_f2, const flo
 // The candidates of zeb_correlate_peaks (one (value, index) per (item, j) slab) live here instead
 // of in caller memory: ZEB_PEAKS_STATIC_SLABS of them, 4 MiB, held by every device that loads the
 // library until the process exits. Host code may not hand g_peaks_scratch to a kernel (in host
-// code the name stands for a host-side shadow, not a device address): each device's address is
-// looked up once with cudaGetSymbolAddress, with that device current, and passed to the kernels.
+// code the name stands for a host-side shadow, not a device address): the address is looked up
+// with cudaGetSymbolAddress, with the device current, and passed to the kernels.
+//
+// Each CUDA context has its own copy of the array (a context loads the module for itself), so the
+// address is cached per context, keyed by the context's unique ID (cuCtxGetId: an ID is never
+// reused, unlike a context handle or a device ordinal). After a cudaDeviceReset, or under another
+// context made current on the same device, the next call meets a new ID and looks the address up
+// again with that context current.
 static __device__ __align__(256) float2 g_peaks_scratch[ZEB_PEAKS_STATIC_SLABS];
 
 namespace {
 std::mutex g_static_mu;
-float2* g_static_addr[256];
+struct StaticAddr {
+  unsigned long long ctx_id;
+  float2* addr;
+};
+StaticAddr g_static_addr[64];  // the most recent contexts, oldest replaced first
+int g_static_next = 0;
+
+typedef CUresult (*ctx_current_fn)(CUcontext*);
+typedef CUresult (*ctx_id_fn)(CUcontext, unsigned long long*);
+
+// the current context's unique ID through the runtime's driver entry points (no link against libcuda)
+bool current_ctx_id(unsigned long long* id) {
+  static ctx_current_fn get_current = nullptr;
+  static ctx_id_fn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return false;
+    get_current = (ctx_current_fn)p;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return false;
+    get_id = (ctx_id_fn)p;
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  return get_id(ctx, id) == CUDA_SUCCESS;
 }
+}  // namespace
 
 extern "C" int zeb_correlate_peaks_static(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw,
                                           const float* rden, int rden_div, float* peaks, void* stream) {
@@ -555,21 +592,30 @@ extern "C" int zeb_correlate_peaks_static(const float* U, int n_items, const zeb
               "correlate_peaks_static: %d items need %lld slabs of scratch; the static scratch holds %d "
               "(at most %d items at this bandwidth)",
               n_items, (long long)n_items * d->nb, ZEB_PEAKS_STATIC_SLABS, ZEB_PEAKS_STATIC_SLABS / d->nb);
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  ZEB_REQUIRE(e == cudaSuccess && dev >= 0 && dev < 256, ZEB_ECUDA, "correlate_peaks_static: cudaGetDevice: %s",
-              cudaGetErrorString(e));
+  unsigned long long id = 0;
+  cudaError_t e = cudaSuccess;
+  if (!current_ctx_id(&id)) {
+    // no context is current on this thread yet: cudaSetDevice makes the device's primary one so
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaSetDevice(dev);
+    ZEB_REQUIRE(e == cudaSuccess && current_ctx_id(&id), ZEB_ECUDA, "correlate_peaks_static: no CUDA context: %s",
+                cudaGetErrorString(e));
+  }
   float2* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[dev]) {
+    for (const StaticAddr& a : g_static_addr)
+      if (a.addr && a.ctx_id == id) scratch = a.addr;
+    if (!scratch) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_peaks_scratch);
       ZEB_REQUIRE(e == cudaSuccess && p, ZEB_ECUDA, "correlate_peaks_static: cudaGetSymbolAddress: %s",
                   cudaGetErrorString(e));
-      g_static_addr[dev] = (float2*)p;
+      scratch = (float2*)p;
+      g_static_addr[g_static_next] = StaticAddr{id, scratch};
+      g_static_next = (g_static_next + 1) % 64;
     }
-    scratch = g_static_addr[dev];
   }
   // every slab writes its candidate before k_peak_finish reads it: nothing needs clearing
   SlabArgs a{};

@@ -165,7 +165,7 @@ class Engine:
         self.tuned = {}  # what tune() chose for the way work is cut up (device_batch)
         self._pinned = None
         self._pin_buf = None  # the page-locked buffer behind _pinned, reused across scans
-        self._index_calls = 0  # index runs and index_cells calls over the scan since set_patterns
+        self._index_calls = 0  # whole passes over the scan since set_patterns (whole_pinned)
         self._ring, self._ring_i = [], 0  # two page-locked slots a scan not pinned whole streams through
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
@@ -1056,9 +1056,10 @@ class Engine:
             N.call("zeb_records_fz", ptr(recs[pi]), n, ptr(ops), ops.shape[0], ptr(fz[pi]), stream_ptr())
         return fz
 
-    def index_cells(self, cells, bandwidth=None, method="spherical", grid=None):
+    def index_cells(self, cells, bandwidth=None, method="spherical", grid=None, whole_pass=True):
         """engine.zig:1990-2137 — index the given cells against every phase: records
-        [phase][cell][8] = (q, NCC, NMI, last improving step, z)."""
+        [phase][cell][8] = (q, NCC, NMI, last improving step, z). whole_pass: the call counts as
+        one pass over the scan (whole_pinned); index_step counts only its sweep's first step."""
         cells = np.asarray(cells, np.int64)
         n = len(cells)
         n_ph = len(self.phases)
@@ -1066,7 +1067,8 @@ class Engine:
             raise EngineError("NoPhases")
         if n == 0:
             return np.zeros((n_ph, 0, 8), np.float32)
-        self._index_calls += 1  # (a scan indexed a second time is pinned whole: whole_pinned)
+        if whole_pass:
+            self._index_calls += 1  # (a scan indexed a second time is pinned whole: whole_pinned)
         self.prepare(bandwidth, method, grid)
         rows, cols, h, w = self.info()
         raw = self.buf("raw_up", n * h * w, self.raw_dtype()).view(-1)[: n * h * w].view(n, h, w)
@@ -1354,7 +1356,9 @@ class Engine:
         n = min(left, batch * min(max(4096 // batch, 2), 16))
         cells = cells_all[self.index_done:self.index_done + n]
         bw, dg, method = s.sweep(self.index_sweep)
-        recs = self.index_cells(cells, bw, method, dg)
+        # a scan stepped through once is one pass: only the first step of the first sweep counts
+        first = self.index_done == 0 and self.index_sweep == 0
+        recs = self.index_cells(cells, bw, method, dg, whole_pass=first)
         self.land(cells, recs, self._last_fz)
         self.next_sweep(bw)
         return len(self.index_cells_list) - self.index_done
