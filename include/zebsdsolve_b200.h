@@ -221,6 +221,30 @@ int zeb_tc_pack_master(const zeb_so3_dims_t* d, int split, const double* Y, void
 size_t zeb_tc_master_bytes(const zeb_so3_dims_t* d, int split);
 size_t zeb_tc_patterns_bytes(const zeb_so3_dims_t* d, int split, int n_items);
 
+/* The BF16 form's spectrum kept in FP16 (half the bytes of U): zeb_spectrum_bf16's GEMM, its
+ * accumulators scaled by `scale` and rounded to FP16 as they drain, stored as
+ * U16[m'][ν = 2(j·nc + c) + (re|im)][item] with the items padded to a multiple of 128
+ * (zeb_spectrum_h_bytes bytes; U16 128-byte aligned). `scale` is a power of two with
+ * scale·max|U| well inside FP16's range: the host takes it from the table, as 2^floor(log2(16384 /
+ * y)) with y the largest column norm over l of any order's table (|U| <= y since the coefficients
+ * have unit norm). Same A, B, split and status as zeb_spectrum_bf16; needs 2·nb·nc >= 128.
+ * Replaces Spherical.spectrum (src/spherical.zig:369-382; shaders/so3.wgsl spectrum). */
+size_t zeb_spectrum_h_bytes(const zeb_so3_dims_t* d, int n_items);
+int zeb_spectrum_bf16_h(const float* alm, int n_items, const zeb_so3_dims_t* d, int split, const void* A, void* B,
+                        void* U16, float scale, int* status, void* stream);
+
+/* zeb_correlate_peaks over U16 (zeb_spectrum_bf16_h, the same `scale`), the transform along a on
+ * the tcgen05 tensor cores: per (j, c) one GEMM of 128 items × n values of a × 2L (m', re|im),
+ * FP16 operands (the transform matrix f_m'·cos / f_m'·sin of 2π m'a/n built on the device), FP32
+ * accumulation in tensor memory, each value times rden (one volume shared by every item) and
+ * each (item, j) slab's largest kept as the drain runs; then the vertex from direct sums over m'
+ * at the peak and its six neighbours (the peak's score from the same sum). Supports 16 <= L <= 64
+ * with n = 2L. scratch: zeb_peaks_scratch_bytes; status as zeb_spectrum_bf16 (a timed-out wait).
+ * Replaces Spherical.correlate's a_peak_m, peak_reduce and peak_finish_m (src/spherical.zig:
+ * 401-432; shaders/so3.wgsl :489-593, 631-663, 716-796). */
+int zeb_correlate_peaks_h(const void* U16, int n_items, const zeb_so3_dims_t* d, float scale, const float* rden,
+                          float* peaks, void* scratch, int* status, void* stream);
+
 /* The correlation volume's transform along a (U comes transformed along b and c), times rden
  * (volume b / rden_div for item b), each (item, j, c) line's largest value, each item's largest, and its sub-grid vertex and
  * orientation: peaks[b] = (q.w, q.x, q.y, q.z, score, a, b, c). Replaces Spherical.correlate's

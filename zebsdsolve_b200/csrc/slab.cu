@@ -10,6 +10,7 @@
 // k_peak_finish then takes each item's best slab, re-evaluates the six neighbours of the peak by
 // direct sums over m' and fits the parabolic vertex along a, c and b (so3.wgsl:665-796).
 #include <cuda.h>
+#include <cuda_fp16.h>
 
 #include <mutex>
 
@@ -309,10 +310,21 @@ __global__ void __launch_bounds__(WARPS * 32, PER_SM) k_slab_cols(SlabArgs a) {
 }
 
 // V[j; m', c] of item b: U is already transformed along c (so3.wgsl:667-674)
-__device__ __forceinline__ float2 v_at(const float2* __restrict__ U, int b, int j, int mp, int c,
-                                       const zeb_so3_dims_t& d) {
-  return __ldg(U + (((size_t)b * d.nb + j) * d.L + mp) * d.nc + c);
-}
+struct UReader32 {  // FP32, [item][j][m'][c]
+  const float2* U;
+  __device__ __forceinline__ float2 operator()(int b, int j, int mp, int c, const zeb_so3_dims_t& d) const {
+    return __ldg(U + (((size_t)b * d.nb + j) * d.L + mp) * d.nc + c);
+  }
+};
+struct UReader16 {  // s·U in FP16, [m'][2(j·nc + c) + (re|im)][item], items padded to ppad
+  const __half* U;
+  size_t ppad, rows;
+  float inv;  // 1/s
+  __device__ __forceinline__ float2 operator()(int b, int j, int mp, int c, const zeb_so3_dims_t& d) const {
+    const size_t o = ((size_t)mp * rows + 2 * (size_t)(j * d.nc + c)) * ppad + b;
+    return make_float2(__half2float(U[o]) * inv, __half2float(U[o + ppad]) * inv);
+  }
+};
 
 // Re(V e^{−i m a}) at grid point ia (so3.wgsl:766-769)
 __device__ __forceinline__ float a_term(float2 v, int m, int ia, int n) {
@@ -328,8 +340,12 @@ __device__ __forceinline__ float vertex(float lo, float mid, float hi) {
   return fminf(fmaxf(0.5f * (lo - hi) / den, -0.5f), 0.5f);
 }
 
-__global__ void __launch_bounds__(64) k_peak_finish(SlabArgs a, float* __restrict__ peaks) {
-  __shared__ float pf[6][64];
+// CENTER: the peak's own value comes again from the direct sum (with exact twiddles) rather than
+// from the candidate, so that the vertex fit sees seven values of the same arithmetic (the FP16
+// spectrum's transform along a runs with FP16 twiddles)
+template <class R, bool CENTER>
+__global__ void __launch_bounds__(64) k_peak_finish(SlabArgs a, R v_at, float* __restrict__ peaks) {
+  __shared__ float pf[7][64];
   __shared__ float2 best;
   const zeb_so3_dims_t& d = a.d;
   const int b = blockIdx.x;
@@ -351,7 +367,7 @@ __global__ void __launch_bounds__(64) k_peak_finish(SlabArgs a, float* __restric
     if (threadIdx.x == 0) best = make_float2(bv, __uint_as_float(bi));
   }
   __syncthreads();
-  const float v0 = best.x;
+  const float vbest = best.x;
   uint32_t idx = __float_as_uint(best.y);
   if (idx == 0xffffffffu) idx = 0;
   const int ia = idx & (n - 1);
@@ -360,33 +376,35 @@ __global__ void __launch_bounds__(64) k_peak_finish(SlabArgs a, float* __restric
   const bool inner = j > 0 && j < n / 2;
   const int iqm = (iq + nc - 1) & (nc - 1), iqp = (iq + 1) & (nc - 1);
   const int iam = (ia + n - 1) & (n - 1), iap = (ia + 1) & (n - 1);
-  float s[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float s[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   for (int m = threadIdx.x; m < L; m += 64) {
     float f = m == 0 ? 1.f : 2.f;
-    float2 vc = v_at(a.U, b, j, m, iq, d);
-    float2 vm = v_at(a.U, b, j, m, iqm, d);
-    float2 vp = v_at(a.U, b, j, m, iqp, d);
+    float2 vc = v_at(b, j, m, iq, d);
+    float2 vm = v_at(b, j, m, iqm, d);
+    float2 vp = v_at(b, j, m, iqp, d);
     s[0] += f * a_term(vc, m, iam, n);
     s[1] += f * a_term(vc, m, iap, n);
     s[2] += f * a_term(vm, m, ia, n);
     s[3] += f * a_term(vp, m, ia, n);
     if (inner) {
-      s[4] += f * a_term(v_at(a.U, b, j - 1, m, iq, d), m, ia, n);
-      s[5] += f * a_term(v_at(a.U, b, j + 1, m, iq, d), m, ia, n);
+      s[4] += f * a_term(v_at(b, j - 1, m, iq, d), m, ia, n);
+      s[5] += f * a_term(v_at(b, j + 1, m, iq, d), m, ia, n);
     }
+    if (CENTER) s[6] += f * a_term(vc, m, ia, n);
   }
 #pragma unroll
-  for (int k = 0; k < 6; ++k) pf[k][threadIdx.x] = s[k];
+  for (int k = 0; k < 7; ++k) pf[k][threadIdx.x] = s[k];
   __syncthreads();
   for (int off = 32; off > 0; off >>= 1) {
     if ((int)threadIdx.x < off)
 #pragma unroll
-      for (int k = 0; k < 6; ++k) pf[k][threadIdx.x] += pf[k][threadIdx.x + off];
+      for (int k = 0; k < 7; ++k) pf[k][threadIdx.x] += pf[k][threadIdx.x + off];
     __syncthreads();
   }
   if (threadIdx.x != 0) return;
   const float* rd = a.rden + (size_t)(b / a.rden_div) * nb * nc * n;
   auto rat = [&](int jj, int qq, int aa) { return __ldg(rd + ((size_t)jj * nc + qq) * n + aa); };
+  const float v0 = CENTER ? pf[6][0] * rat(j, iq, ia) : vbest;
   float da = vertex(pf[0][0] * rat(j, iq, iam), v0, pf[1][0] * rat(j, iq, iap));
   float dc = vertex(pf[2][0] * rat(j, iqm, ia), v0, pf[3][0] * rat(j, iqp, ia));
   float dj = 0.f;
@@ -509,8 +527,24 @@ extern "C" int zeb_correlate_peaks(const float* U, int n_items, const zeb_so3_di
   cudaStream_t st = (cudaStream_t)stream;
   int rc = slab_launch(U, n_items, d, tw, a, false, st);
   if (rc) return rc;
-  k_peak_finish<<<n_items, 64, 0, st>>>(a, peaks);
+  k_peak_finish<UReader32, false><<<n_items, 64, 0, st>>>(a, UReader32{(const float2*)U}, peaks);
   return zeb_launch_check("peak_finish");
+}
+
+// the candidates of the tensor-core transform (slab_tc.cu) reduced, and the vertex fitted from
+// the FP16 spectrum: zeb_correlate_peaks_h's last step
+extern "C" int zeb_peak_finish_h(const void* U16, int n_items, const zeb_so3_dims_t* d, float scale, const float* rden,
+                                 const float2* cand, float* peaks, void* stream) {
+  SlabArgs a{};
+  a.n_items = n_items;
+  a.d = *d;
+  a.rden = rden;
+  a.rden_div = 1 << 30;
+  a.cand = const_cast<float2*>(cand);
+  const size_t ppad = (size_t)((n_items + 127) / 128) * 128;
+  UReader16 r{(const __half*)U16, ppad, 2 * (size_t)d->nb * d->nc, 1.f / scale};
+  k_peak_finish<UReader16, true><<<n_items, 64, 0, (cudaStream_t)stream>>>(a, r, peaks);
+  return zeb_launch_check("peak_finish (FP16 spectrum)");
 }
 
 extern "C" int zeb_correlate_volume(const float* U, int n_items, const zeb_so3_dims_t* d, const float* tw, float* vol,
@@ -625,6 +659,6 @@ extern "C" int zeb_correlate_peaks_static(const float* U, int n_items, const zeb
   cudaStream_t st = (cudaStream_t)stream;
   int rc = slab_launch(U, n_items, d, tw, a, false, st);
   if (rc) return rc;
-  k_peak_finish<<<n_items, 64, 0, st>>>(a, peaks);
+  k_peak_finish<UReader32, false><<<n_items, 64, 0, st>>>(a, UReader32{(const float2*)U}, peaks);
   return zeb_launch_check("peak_finish");
 }

@@ -30,6 +30,7 @@
 // issued, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -175,6 +176,7 @@ struct TcArgs {
   int* status;      // nonzero after a timed-out wait (what the CTA was waiting on)
   long long limit;  // nanoseconds before a wait gives up
   int per;          // row tiles per CTA (blockIdx.z picks the group)
+  float scale;      // HALF: U is stored as scale·U in FP16
 };
 
 struct TcShared {
@@ -187,6 +189,10 @@ struct TcShared {
   int failed;
 };
 
+// HALF = false: U in FP32 as [item][j][m'][c] (re, im); true: scale·U in FP16 as
+// [m'][ν = 2(j·nc + c) + (re|im)][item] (items padded to whole tiles of 128), the layout the
+// tensor-core transform along a (slab_tc.cu) loads its operand tiles from.
+template <bool HALF>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const __grid_constant__ CUtensorMap umap) {
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   TcShared& s = *reinterpret_cast<TcShared*>((void*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023));
@@ -293,6 +299,62 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
     const int two_nc = 2 * t.nc;
     int chunk = 0;
     for (int mt = 0; mt < mtiles; ++mt) {
+      if constexpr (HALF) {
+        const int acc = mt & 1;
+        if (!bar_and(1, 128, leader ? mbar_wait_sleep(&s.acc_full[acc], (mt >> 1) & 1, lim) : true)) {
+          if (leader) {
+            atomicOr(a.status, 4);
+            s.failed = 1;
+          }
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int r0 = (mt0 + mt) * TC_BM;  // first row ν of the tile
+        // two 64-pattern chunks: TMEM → registers → ×scale → FP16 → a staging buffer of 128-byte
+        // rows [ν][64 items], 16-byte chunks XOR-swizzled by ν mod 8 (the tensor map's 128-byte
+        // swizzle) → one 16 KB tensor store
+#pragma unroll 1
+        for (int c0 = 0; c0 < TC_BN; c0 += 64, ++chunk) {
+          uint32_t v[32], w[32];
+          TMEM_LD32(tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(acc * TC_BN + c0), v);
+          TMEM_LD32(tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(acc * TC_BN + c0 + 32), w);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (c0 + 64 == TC_BN) {  // the accumulator is read out: the next tile's MMAs may start
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&s.acc_empty[acc]);
+          }
+          uint8_t* stg = reinterpret_cast<uint8_t*>(s.stage[chunk & 1]);
+          if (leader) bulk_wait_read1();  // the store that last used this buffer has read it
+          bar_sync(1, 128);
+          const float sc = a.scale;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            uint4 o;
+            o.x = pack_half2(__uint_as_float(v[8 * q + 0]) * sc, __uint_as_float(v[8 * q + 1]) * sc);
+            o.y = pack_half2(__uint_as_float(v[8 * q + 2]) * sc, __uint_as_float(v[8 * q + 3]) * sc);
+            o.z = pack_half2(__uint_as_float(v[8 * q + 4]) * sc, __uint_as_float(v[8 * q + 5]) * sc);
+            o.w = pack_half2(__uint_as_float(v[8 * q + 6]) * sc, __uint_as_float(v[8 * q + 7]) * sc);
+            *(uint4*)(stg + sw128(row, 8 * q)) = o;
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            uint4 o;
+            o.x = pack_half2(__uint_as_float(w[8 * q + 0]) * sc, __uint_as_float(w[8 * q + 1]) * sc);
+            o.y = pack_half2(__uint_as_float(w[8 * q + 2]) * sc, __uint_as_float(w[8 * q + 3]) * sc);
+            o.z = pack_half2(__uint_as_float(w[8 * q + 4]) * sc, __uint_as_float(w[8 * q + 5]) * sc);
+            o.w = pack_half2(__uint_as_float(w[8 * q + 6]) * sc, __uint_as_float(w[8 * q + 7]) * sc);
+            *(uint4*)(stg + sw128(row, 32 + 8 * q)) = o;
+          }
+          fence_proxy_async();
+          bar_sync(1, 128);
+          if (leader) {
+            if (ptile * TC_BN + c0 < a.n_items) tma_store_3d(&umap, stg, ptile * TC_BN + c0, r0, mp);
+            bulk_commit();
+          }
+        }
+        continue;
+      }
       const int acc = mt & 1;
       // the four warps agree on the outcome (a barrier that ANDs their results)
       // one thread waits for the accumulator (sleeping between polls); the barrier hands the
@@ -432,7 +494,7 @@ extern "C" int zeb_spectrum_bf16(const float* alm, int n_items, const zeb_so3_di
   a.status = status;
   a.limit = 1000000000LL;  // 1 s: far above any legitimate wait inside one CTA
   size_t smem = sizeof(TcShared) + 1024;
-  cudaFuncSetAttribute(k_spectrum_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_spectrum_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   // enough CTAs for several waves: row tiles split into groups when the pattern tiles are few
   int sms = 148;
   {
@@ -446,6 +508,69 @@ extern "C" int zeb_spectrum_bf16(const float* alm, int n_items, const zeb_so3_di
   a.per = (t.mtiles + groups - 1) / groups;
   groups = (t.mtiles + a.per - 1) / a.per;  // no empty group: every CTA has at least one row tile
   dim3 g(t.ptiles, d->L, groups);
-  k_spectrum_tc<<<g, TC_THREADS, smem, st>>>(a, umap);
+  k_spectrum_tc<false><<<g, TC_THREADS, smem, st>>>(a, umap);
   return zeb_launch_check("spectrum_bf16");
+}
+
+// scale·U in FP16 as [m'][ν][item]: a 3-D tensor [L][rows][items rounded up to tiles], boxes of 64
+// items × 128 rows × 1 order with the 128-byte swizzle of the staging buffer
+static bool tc_u16_map(CUtensorMap* m, void* U16, const zeb_so3_dims_t* d, int n_items) {
+  auto fn = tc_encode_fn();
+  if (!fn) return false;
+  const cuuint64_t ppad = (cuuint64_t)((n_items + TC_BN - 1) / TC_BN) * TC_BN;
+  const cuuint64_t rows = 2 * (cuuint64_t)d->nb * d->nc;
+  cuuint64_t dims[3] = {ppad, rows, (cuuint64_t)d->L};
+  cuuint64_t strides[2] = {ppad * 2, ppad * 2 * rows};
+  cuuint32_t box[3] = {64, (cuuint32_t)TC_BM, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, U16, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+extern "C" size_t zeb_spectrum_h_bytes(const zeb_so3_dims_t* d, int n_items) {
+  if (!tc_dims_ok(d, -1) || n_items <= 0) return 0;
+  const size_t ppad = (size_t)((n_items + TC_BN - 1) / TC_BN) * TC_BN;
+  return (size_t)d->L * 2 * d->nb * d->nc * ppad * 2;
+}
+
+extern "C" int zeb_spectrum_bf16_h(const float* alm, int n_items, const zeb_so3_dims_t* d, int split, const void* A,
+                                   void* B, void* U16, float scale, int* status, void* stream) {
+  ZEB_REQUIRE(alm && A && B && U16 && status, ZEB_EARG, "spectrum_bf16_h: null argument");
+  ZEB_REQUIRE(tc_dims_ok(d, split), ZEB_EARG, "spectrum_bf16_h: unsupported dims (L=%d, split=%d)", d ? d->L : -1,
+              split);
+  ZEB_REQUIRE(2 * d->nb * d->nc >= TC_BM, ZEB_EARG, "spectrum_bf16_h: bandwidth %d too small", d->L);
+  ZEB_REQUIRE(scale > 0.f && scale < 1e30f, ZEB_EARG, "spectrum_bf16_h: scale %g", (double)scale);
+  if (n_items <= 0) return ZEB_OK;
+  TcLayout t = tc_layout(d, split, n_items);
+  cudaStream_t st = (cudaStream_t)stream;
+  long long chunks = (long long)t.ptiles * tc_kblocks(d->L, 0, split) * TC_BN * 8;
+  dim3 gp((unsigned)((chunks + 255) / 256), d->L);
+  k_pack_patterns<<<gp, 256, 0, st>>>((const float2*)alm, n_items, d->n_pairs, t, (uint8_t*)B);
+  int rc = zeb_launch_check("pack_patterns");
+  if (rc) return rc;
+  CUtensorMap umap;
+  ZEB_REQUIRE(((uintptr_t)U16 & 127) == 0, ZEB_EARG, "spectrum_bf16_h: U16 must be 128-byte aligned");
+  ZEB_REQUIRE(tc_u16_map(&umap, U16, d, n_items), ZEB_ECUDA, "spectrum_bf16_h: tensor map for U16 refused");
+  TcArgs a{};
+  a.t = t; a.A = (const uint8_t*)A; a.B = (const uint8_t*)B; a.n_items = n_items; a.U = nullptr;
+  a.status = status;
+  a.limit = 1000000000LL;
+  a.scale = scale;
+  size_t smem = sizeof(TcShared) + 1024;
+  cudaFuncSetAttribute(k_spectrum_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int sms = 148;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const long long base = (long long)t.ptiles * d->L;
+  int groups = (int)std::min<long long>(t.mtiles, (8LL * sms + base - 1) / base);
+  groups = std::max(1, std::min(groups, 65535));
+  a.per = (t.mtiles + groups - 1) / groups;
+  groups = (t.mtiles + a.per - 1) / a.per;
+  dim3 g(t.ptiles, d->L, groups);
+  k_spectrum_tc<true><<<g, TC_THREADS, smem, st>>>(a, umap);
+  return zeb_launch_check("spectrum_bf16_h");
 }

@@ -124,6 +124,19 @@ def synthesize(coef, plm, L, n_phi):
     return torch.fft.irfft(G, n=n_phi, dim=1) * n_phi
 
 
+def spectrum_scale(Y, L):
+    """The power of two s with s·|U| <= 16384 for every spectrum of this table: |U[j][m'][c]| =
+    |Σ_l conj(g_lm') Y[pair(m',l)][j·nc+c]| <= ||g|| · y (Cauchy–Schwarz; the coefficients have unit
+    norm), y the largest column norm over l of any order m' (Y: complex [pair][column], pairs
+    m-major). FP16 then keeps 11 significant bits of every value far from its range's ends."""
+    ms, _ = pair_orders(L)
+    rows = torch.as_tensor(ms, device=Y.device)
+    sq = torch.zeros(L, Y.shape[1], dtype=torch.float64, device=Y.device)
+    sq.index_add_(0, rows, (Y.real * Y.real + Y.imag * Y.imag))
+    y = float(torch.sqrt(sq.max()))
+    return float(2.0 ** math.floor(math.log2(16384.0 / max(y, 1e-30))))
+
+
 class PhaseBand:
     """A phase at one bandwidth: harmonics, rules, fold, weight tables → correlation tables."""
 
@@ -166,6 +179,12 @@ class PhaseBand:
             self.A = torch.empty(nbytes, dtype=torch.uint8, device=dev)
             N.call("zeb_tc_pack_master", ctypes.byref(self.dims), self.split, ptr(torch.view_as_real(Y64)),
                    ptr(self.A), stream_ptr())
+        # the BF16 form keeps the spectrum in FP16 (zeb_spectrum_bf16_h, zeb_correlate_peaks_h) where
+        # the tensor-core transform along a takes the bandwidth; bf16x3 keeps FP32 (its point is
+        # FP32-quality U)
+        self.u_scale = None
+        if precision == "bf16" and 16 <= L <= 64 and n == 2 * L and 2 * self.dims.nb * self.dims.nc >= 128:
+            self.u_scale = spectrum_scale(Y64, L)
         del Y64
         self.rden = None
         self.rden_key = None

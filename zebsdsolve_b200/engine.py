@@ -863,11 +863,22 @@ class Engine:
             tile = self.tile_items(ph, n)
             for t0 in range(0, n, tile):
                 nt = min(tile, n - t0)
-                U = self.buf("spec", N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), nt) // 4 + 1)
                 a0 = alm[t0 * bt.n_pairs * 2:]
+                cand = self.buf("cand", N.load().zeb_peaks_scratch_bytes(ctypes.byref(ph.dims), nt) // 4 + 1)
+                if ph.u_scale is not None:
+                    # the BF16 form: the spectrum in FP16, the transform along a on the tensor cores
+                    U16 = self.buf("spec16", N.load().zeb_spectrum_h_bytes(ctypes.byref(ph.dims), nt), torch.uint8)
+                    B = self.buf("tc_b", N.load().zeb_tc_patterns_bytes(ctypes.byref(ph.dims), ph.split, nt), torch.uint8)
+                    mark("spectrum")
+                    N.call("zeb_spectrum_bf16_h", ptr(a0), nt, ctypes.byref(ph.dims), ph.split, ptr(ph.A), ptr(B),
+                           ptr(U16), ph.u_scale, ptr(self.tc_status()), stream_ptr())
+                    mark("peaks")
+                    N.call("zeb_correlate_peaks_h", ptr(U16), nt, ctypes.byref(ph.dims), ph.u_scale, ptr(ph.rden),
+                           ptr(peaks[t0 * 8:]), ptr(cand), ptr(self.tc_status()), stream_ptr())
+                    continue
+                U = self.buf("spec", N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), nt) // 4 + 1)
                 mark("spectrum")
                 self.spectrum(a0, nt, ph, ph.Y_f, U)
-                cand = self.buf("cand", N.load().zeb_peaks_scratch_bytes(ctypes.byref(ph.dims), nt) // 4 + 1)
                 mark("peaks")
                 N.call("zeb_correlate_peaks", ptr(U), nt, ctypes.byref(ph.dims), ptr(bt.tw), ptr(ph.rden), 1 << 30,
                        ptr(peaks[t0 * 8:]), ptr(cand), stream_ptr())
@@ -1247,7 +1258,10 @@ class Engine:
     def tile_items(self, ph, n):
         """Items whose spectra one pass holds: tile_mb of them, at least 512 (spherical.zig:311-315),
         spread evenly over the passes a batch needs (no short last tile)."""
-        per = N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), 1)
+        if ph.u_scale is not None:  # the FP16 spectrum: half the bytes per item
+            per = N.load().zeb_spectrum_h_bytes(ctypes.byref(ph.dims), 128) // 128
+        else:
+            per = N.load().zeb_spectrum_bytes(ctypes.byref(ph.dims), 1)
         most = int(max(1, min(n, max(512, (self.set["tile_mb"] << 20) // per))))
         tiles = -(-n // most)
         return -(-n // tiles)
