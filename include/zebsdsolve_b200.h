@@ -223,7 +223,7 @@ size_t zeb_tc_patterns_bytes(const zeb_so3_dims_t* d, int split, int n_items);
 
 /* The BF16 form's spectrum kept in FP16 (half the bytes of U): zeb_spectrum_bf16's GEMM, its
  * accumulators scaled by `scale` and rounded to FP16 as they drain, stored as
- * U16[m'][ν = 2(j·nc + c) + (re|im)][item] with the items padded to a multiple of 128
+ * U16[j·nc + c][item / 128][m'][re|im][item % 128] with the items padded to a multiple of 128
  * (zeb_spectrum_h_bytes bytes; U16 128-byte aligned). `scale` is a power of two with
  * scale·max|U| well inside FP16's range: the host takes it from the table, as 2^floor(log2(16384 /
  * y)) with y the largest column norm over l of any order's table (|U| <= y since the coefficients

@@ -52,7 +52,7 @@ def test_fp16_spectrum_and_tensor_core_peaks(L, group, side, lmax, n):
     b = e.prepare(L)
     bt = b["tables"]
     ph = b["phases"][0][1]
-    assert ph.u_scale is not None and ph.split == 16
+    assert ph.u_scale is not None and ph.split == min(16, L - 1)
     dims = ph.dims
     pats = e.preprocess(torch.as_tensor(pats16, device="cuda"), n, np.arange(n))
     items = e.items_of(np.arange(n))
@@ -73,11 +73,12 @@ def test_fp16_spectrum_and_tensor_core_peaks(L, group, side, lmax, n):
     torch.cuda.synchronize()
     assert int(status.item()) == 0
 
-    # U16[m'][2(j·nc+c) + re|im][item] / s against U[item][j][m'][c] (re, im)
+    # U16[j][c][item tile][m'][re|im][item % 128] / s against U[item][j][m'][c] (re, im)
     Ln, nb, nc = dims.L, dims.nb, dims.nc
-    ppad = (n + 127) // 128 * 128
-    h = U16.view(torch.float16)[: Ln * 2 * nb * nc * ppad].view(Ln, nb, nc, 2, ppad)[..., :n].float() / ph.u_scale
-    u = U[: n * nb * Ln * nc * 2].view(n, nb, Ln, nc, 2).permute(2, 1, 3, 4, 0)  # → [m'][j][c][ri][item]
+    pt = (n + 127) // 128
+    h = U16.view(torch.float16)[: nb * nc * pt * Ln * 2 * 128].view(nb, nc, pt, Ln, 2, 128)
+    h = h.permute(0, 1, 3, 4, 2, 5).reshape(nb, nc, Ln, 2, pt * 128)[..., :n].float() / ph.u_scale
+    u = U[: n * nb * Ln * nc * 2].view(n, nb, Ln, nc, 2).permute(1, 3, 2, 4, 0)  # → [j][c][m'][ri][item]
     top = float(u.abs().max())
     assert top * ph.u_scale <= 16384 * 1.001  # the scale's bound holds
     err = float((h - u).abs().max())
@@ -97,8 +98,9 @@ def test_fp16_spectrum_and_tensor_core_peaks(L, group, side, lmax, n):
     assert np.isfinite(g).all()
     ds = np.abs(g[:, 4] - w[:, 4])
     assert ds.max() <= 5e-4, np.sort(ds)[-4:]
-    dot = np.abs((g[:, :4] * w[:, :4]).sum(1)).clip(0, 1)
-    ang = np.degrees(2 * np.arccos(dot))
+    # modulo the master's rotations: its symmetric copies in the volume are exact ties, which the
+    # two forms' rounding may break either way
+    ang = np.degrees(s.disorientation(g[:, :4], w[:, :4]))
     assert (ang <= 0.1).mean() >= 0.9, np.sort(ang)[-8:]
 
 

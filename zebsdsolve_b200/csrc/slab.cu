@@ -316,13 +316,13 @@ struct UReader32 {  // FP32, [item][j][m'][c]
     return __ldg(U + (((size_t)b * d.nb + j) * d.L + mp) * d.nc + c);
   }
 };
-struct UReader16 {  // s·U in FP16, [m'][2(j·nc + c) + (re|im)][item], items padded to ppad
+struct UReader16 {  // s·U in FP16, [(j, c)][item tile][m'][re|im][128 items]
   const __half* U;
-  size_t ppad, rows;
+  size_t ptiles;
   float inv;  // 1/s
   __device__ __forceinline__ float2 operator()(int b, int j, int mp, int c, const zeb_so3_dims_t& d) const {
-    const size_t o = ((size_t)mp * rows + 2 * (size_t)(j * d.nc + c)) * ppad + b;
-    return make_float2(__half2float(U[o]) * inv, __half2float(U[o + ppad]) * inv);
+    const size_t o = ((((size_t)(j * d.nc + c) * ptiles + (b >> 7)) * d.L + mp) * 2) * 128 + (b & 127);
+    return make_float2(__half2float(U[o]) * inv, __half2float(U[o + 128]) * inv);
   }
 };
 
@@ -541,8 +541,7 @@ extern "C" int zeb_peak_finish_h(const void* U16, int n_items, const zeb_so3_dim
   a.rden = rden;
   a.rden_div = 1 << 30;
   a.cand = const_cast<float2*>(cand);
-  const size_t ppad = (size_t)((n_items + 127) / 128) * 128;
-  UReader16 r{(const __half*)U16, ppad, 2 * (size_t)d->nb * d->nc, 1.f / scale};
+  UReader16 r{(const __half*)U16, (size_t)((n_items + 127) / 128), 1.f / scale};
   k_peak_finish<UReader16, true><<<n_items, 64, 0, (cudaStream_t)stream>>>(a, r, peaks);
   return zeb_launch_check("peak_finish (FP16 spectrum)");
 }

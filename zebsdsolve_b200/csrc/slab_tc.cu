@@ -2,7 +2,7 @@
 // tensor cores, over the spectrum kept in FP16.
 //
 // U (transformed along b and c by the spectrum GEMM) arrives as s·U in FP16, laid out
-// [m'][ν = 2(j·nc + c) + (re|im)][item] (k_spectrum_tc<true>).  For one (j, c) the real transform
+// [(j, c)][item tile][m'][re|im][128 items] (k_spectrum_tc<true>).  For one (j, c) the real transform
 // along a (so3.wgsl:279-315, 396-593),
 //
 //   C(a) = Re V[0] + 2 Re Σ_{m'>0} V[m'] e^{−2πi m' a/n} = Σ_κ V_κ F[a][κ],  κ = 2m' + (re|im),
@@ -10,7 +10,7 @@
 //
 // is then one GEMM per (j, c) over a tile of 128 items: D[item][a] = Σ_κ A[item][κ] F[a][κ] with
 // M = 128 items, N = n, K = 2L, FP16 operands and FP32 accumulation in tensor memory.  A is the
-// tile of U as it lies in memory (items contiguous: an MN-major operand, brought in by two 3-D
+// tile of U as it lies in memory (items contiguous: an MN-major operand, brought in by two 5-D
 // tensor loads with the 128-byte swizzle); F, the same for every tile, is built once per CTA in
 // shared memory (K-major, 128-byte swizzle).  The epilogue scales each value by the shared
 // denominator volume, rden[j][c][a]/s, and keeps each item's largest with its volume index
@@ -20,9 +20,10 @@
 // k_peak_finish (slab.cu's, with an FP16 reader) then reduces the candidates and fits the vertex
 // from direct sums over m' at the peak and its six neighbours.
 //
-// One persistent CTA per SM: warp 0 issues the tensor loads (a ring of ST_STAGES tiles), warp 1
-// the MMAs into two accumulators of n columns, warps 2-9 drain them (two warps per TMEM lane
-// quadrant, each half of the n columns).  Every wait is bounded: on a timeout the CTA records the
+// One persistent CTA per SM: warp 0 issues the tensor loads (a ring of ST_STAGES tiles) and the
+// bulk copies of each tile's row of rden (a ring of ST_RSLOTS), warp 1 the MMAs into ST_ACC
+// accumulators of n columns, warps 2-9 drain them (two warps per TMEM lane quadrant, each half of
+// the n columns).  Every wait is bounded: on a timeout the CTA records the
 // failure, waits (bounded) for what it issued, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_fp16.h>
@@ -50,12 +51,17 @@ struct SlabTcArgs {
   long long limit;
 };
 
+constexpr int ST_ACC = 4;    // accumulators in tensor memory (4 × 128 columns)
+constexpr int ST_RSLOTS = 8;  // rows of rden staged ahead of the epilogue
+
 struct SlabTcShared {
   uint8_t f[2][16384];                        // F: n rows × 2L FP16, K-major, in 64-wide K blocks
   uint8_t a[ST_STAGES][2][ST_HALF_BYTES];     // tiles of U: [half][κ][64 items]
+  float rden[ST_RSLOTS][128];                 // each tile's row rden[j][c][0 … n)
   float bestv[2][ST_BM];                      // the second half's best, handed to the first
   uint32_t besti[2][ST_BM];
-  uint64_t full[ST_STAGES], empty[ST_STAGES], acc_full[2], acc_empty[2], mma_done;
+  uint64_t full[ST_STAGES], empty[ST_STAGES], acc_full[ST_ACC], acc_empty[ST_ACC], rfull[ST_RSLOTS],
+      rempty[ST_RSLOTS], mma_done;
   uint32_t tmem;
 };
 
@@ -89,9 +95,13 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
       mbar_init(&s.full[i], 1);
       mbar_init(&s.empty[i], 1);
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < ST_ACC; ++i) {
       mbar_init(&s.acc_full[i], 1);
       mbar_init(&s.acc_empty[i], ST_EPI);
+    }
+    for (int i = 0; i < ST_RSLOTS; ++i) {
+      mbar_init(&s.rfull[i], 1);
+      mbar_init(&s.rempty[i], ST_EPI);
     }
     mbar_init(&s.mma_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -100,7 +110,7 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
   fence_proxy_async();  // F, written by these threads, is read by the tensor cores (async proxy)
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s.tmem)),
-                 "r"(256));
+                 "r"(128 * ST_ACC));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -124,9 +134,18 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
             break;
           }
           mbar_expect_tx(&s.full[st], tile_bytes);
-          const int nu = 2 * (j * nc + c);
-          tma_load_3d(&umap, s.a[st][0], &s.full[st], pt * ST_BM, nu, 0);
-          tma_load_3d(&umap, s.a[st][1], &s.full[st], pt * ST_BM + 64, nu, 0);
+          // the 2L × 256 contiguous bytes of (j, c) and this tile, as two halves of 64 items
+          tma_load_5d(&umap, s.a[st][0], &s.full[st], 0, 0, 0, pt, j * nc + c);
+          tma_load_5d(&umap, s.a[st][1], &s.full[st], 64, 0, 0, pt, j * nc + c);
+          // and the tile's row of rden, for the epilogue
+          const int rs = (int)(it % ST_RSLOTS);
+          if (!mbar_wait(&s.rempty[rs], (uint32_t)((it / ST_RSLOTS) & 1) ^ 1u, lim)) {
+            ok = false;
+            ++it;
+            break;
+          }
+          mbar_expect_tx(&s.rfull[rs], (uint32_t)n * 4u);
+          bulk_g2s(s.rden[rs], a.rden + (size_t)(j * nc + c) * n, (uint32_t)n * 4u, &s.rfull[rs]);
         }
       }
       if (!ok) atomicOr(a.status, 1);
@@ -134,6 +153,8 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
       // phase already consumed reads as complete)
       for (long long i = (it > ST_STAGES ? it - ST_STAGES : 0); i < it; ++i)
         mbar_wait(&s.full[i % ST_STAGES], (uint32_t)((i / ST_STAGES) & 1), lim);
+      for (long long i = (it > ST_RSLOTS ? it - ST_RSLOTS : 0); i < it; ++i)
+        mbar_wait(&s.rfull[i % ST_RSLOTS], (uint32_t)((i / ST_RSLOTS) & 1), lim);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -145,9 +166,9 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
       bool ok = true;
       long long t = 0;
       for (; t < total && ok; ++t) {
-        const int acc = (int)(t & 1);
+        const int acc = (int)(t % ST_ACC);
         const int st = (int)(t % ST_STAGES);
-        ok = mbar_wait(&s.acc_empty[acc], (uint32_t)((t >> 1) & 1) ^ 1u, lim);
+        ok = mbar_wait(&s.acc_empty[acc], (uint32_t)((t / ST_ACC) & 1) ^ 1u, lim);
         if (ok) ok = mbar_wait(&s.full[st], (uint32_t)((t / ST_STAGES) & 1), lim);
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -168,24 +189,33 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
     }
   } else {
     // epilogue: warp w reads TMEM lanes 32·(w mod 4) …; warps w and w + 4 take the two halves of
-    // the n columns. Thread = one item (row of the tile) × half the a values of each tile.
+    // the n columns. Thread = one item (row of the tile) × half the a values of each tile. Each
+    // warp follows the accumulators on its own (the MMAs run up to ST_ACC tiles ahead); the eight
+    // meet once per item, where the halves' bests merge.
     const int ew = warp & 3;
     const int row = ew * 32 + lane;
     const int half = (warp - 2) >> 2;
     const int hn = n >> 1;  // columns per half: 16, 32 or 64
     const uint32_t lanes = (uint32_t)(ew * 32) << 16;
-    const bool lead = warp == 2 && lane == 0;
+    const float rsc = a.rscale;
     float bv = -3.4e38f;
     uint32_t bi = 0xffffffffu;
     long long t = 0;
     bool ok = true;
-    for (long long mi = 0; mi < my_items && ok; ++mi) {
+    for (long long mi = 0; mi < my_items; ++mi) {
       const long long item = blockIdx.x + mi * gridDim.x;
       const int j = (int)(item / a.ptiles), pt = (int)(item - (long long)j * a.ptiles);
-      for (int c = 0; c < nc; ++c, ++t) {
-        const int acc = (int)(t & 1);
-        if (!bar_and(1, 32 * ST_EPI, lead ? mbar_wait_sleep(&s.acc_full[acc], (uint32_t)((t >> 1) & 1), lim) : true)) {
-          if (lead) atomicOr(a.status, 4);
+      for (int c = 0; c < nc && ok; ++c, ++t) {
+        const int acc = (int)(t % ST_ACC);
+        const int rs = (int)(t % ST_RSLOTS);
+        // lane 0 waits (try_wait suspends it in hardware until the phase completes); the warp follows
+        int got = 1;
+        if (lane == 0)
+          got = mbar_wait(&s.acc_full[acc], (uint32_t)((t / ST_ACC) & 1), lim) &&
+                mbar_wait(&s.rfull[rs], (uint32_t)((t / ST_RSLOTS) & 1), lim);
+        got = __shfl_sync(0xffffffffu, got, 0);
+        if (!got) {
+          if (lane == 0) atomicOr(a.status, 4);
           ok = false;
           break;
         }
@@ -195,42 +225,60 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
         TMEM_LD32(c0, v);
         if (hn > 32) TMEM_LD32(c0 + 32, (v + 32));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        // the accumulator is read out: the MMAs of tile t + 2 may start
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncwarp();
-        if (lane == 0) mbar_arrive(&s.acc_empty[acc]);
-        const uint32_t base = (uint32_t)(j * nc + c) * (uint32_t)n + (uint32_t)(half * hn);
-        const float4* rd = reinterpret_cast<const float4*>(a.rden + base);
-        const float rs = a.rscale;
+        if (lane == 0) mbar_arrive(&s.acc_empty[acc]);  // the MMAs of tile t + ST_ACC may start
+        // the values s·C·rden (s a power of two: the order, and every product's rounding, are those
+        // of C·rden; the candidate is scaled by 1/s once, exactly); their largest by a tree
+        const float* rrow = s.rden[rs] + half * hn;
+        float x[64];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           if (4 * q < hn) {
-            const float4 r = __ldg(rd + q);
-            const float x0 = __uint_as_float(v[4 * q + 0]) * (r.x * rs);
-            const float x1 = __uint_as_float(v[4 * q + 1]) * (r.y * rs);
-            const float x2 = __uint_as_float(v[4 * q + 2]) * (r.z * rs);
-            const float x3 = __uint_as_float(v[4 * q + 3]) * (r.w * rs);
-            if (x0 > bv) { bv = x0; bi = base + 4 * q; }
-            if (x1 > bv) { bv = x1; bi = base + 4 * q + 1; }
-            if (x2 > bv) { bv = x2; bi = base + 4 * q + 2; }
-            if (x3 > bv) { bv = x3; bi = base + 4 * q + 3; }
+            const float4 r = *reinterpret_cast<const float4*>(rrow + 4 * q);
+            x[4 * q + 0] = __uint_as_float(v[4 * q + 0]) * r.x;
+            x[4 * q + 1] = __uint_as_float(v[4 * q + 1]) * r.y;
+            x[4 * q + 2] = __uint_as_float(v[4 * q + 2]) * r.z;
+            x[4 * q + 3] = __uint_as_float(v[4 * q + 3]) * r.w;
+          } else {
+            x[4 * q + 0] = x[4 * q + 1] = x[4 * q + 2] = x[4 * q + 3] = -3.4e38f;
           }
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s.rempty[rs]);  // this warp is done with the staged row
+        float m4[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          float m = x[k];
+#pragma unroll
+          for (int q = 1; q < 16; ++q) m = fmaxf(m, x[4 * q + k]);
+          m4[k] = m;
+        }
+        const float m = fmaxf(fmaxf(m4[0], m4[1]), fmaxf(m4[2], m4[3]));
+        if (m > bv) {  // a new best: its first position in the tile (indices grow along the tile)
+          int kk = 0;
+#pragma unroll
+          for (int k = 63; k >= 0; --k)
+            if (x[k] == m) kk = k;
+          bv = m;
+          bi = (uint32_t)(j * nc + c) * (uint32_t)n + (uint32_t)(half * hn + kk);
+        }
       }
-      if (!ok) break;
-      // the item's end: the second half's best joins the first's (lower index on equal values)
+      // the item's end: the eight warps agree on the outcome, and the second half's best joins the
+      // first's (lower index on equal values)
       const int par = (int)(mi & 1);
       if (half == 1) {
         s.bestv[par][row] = bv;
         s.besti[par][row] = bi;
       }
-      bar_sync(2, 32 * ST_EPI);
+      ok = bar_and(2, 32 * ST_EPI, ok);
+      if (!ok) break;
       if (half == 0) {
         const float ov = s.bestv[par][row];
         const uint32_t oi = s.besti[par][row];
         if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
         const int p = pt * ST_BM + row;
-        if (p < a.n_items) a.cand[(size_t)p * nb + j] = make_float2(bv, __uint_as_float(bi));
+        if (p < a.n_items) a.cand[(size_t)p * nb + j] = make_float2(bv * rsc, __uint_as_float(bi));
       }
       bv = -3.4e38f;
       bi = 0xffffffffu;
@@ -239,15 +287,16 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128 * ST_ACC));
 }
 
 }  // namespace zeb
 
 using namespace zeb;
 
-// U16 as the 3-D tensor [L][rows][items rounded up to 128]; boxes of 64 items × the two rows of one
-// (j, c) × every order, landing as [order][re|im][64 items] with the 128-byte swizzle
+// U16 as the 5-D tensor (items within the tile, re|im, order, tile, (j, c)); boxes of 64 items × re|im
+// × every order of one (j, c) and one tile, landing as [order][re|im][64 items] with the 128-byte
+// swizzle
 static bool st_u16_map(CUtensorMap* m, const void* U16, const zeb_so3_dims_t* d, int n_items) {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -258,13 +307,13 @@ static bool st_u16_map(CUtensorMap* m, const void* U16, const zeb_so3_dims_t* d,
       fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
   }
   if (!fn) return false;
-  const cuuint64_t ppad = (cuuint64_t)((n_items + ST_BM - 1) / ST_BM) * ST_BM;
-  const cuuint64_t rows = 2 * (cuuint64_t)d->nb * d->nc;
-  cuuint64_t dims[3] = {ppad, rows, (cuuint64_t)d->L};
-  cuuint64_t strides[2] = {ppad * 2, ppad * 2 * rows};
-  cuuint32_t box[3] = {64, 2, (cuuint32_t)d->L};
-  cuuint32_t es[3] = {1, 1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void*>(U16), dims, strides, box, es,
+  const cuuint64_t ptiles = (cuuint64_t)((n_items + ST_BM - 1) / ST_BM);
+  const cuuint64_t L = (cuuint64_t)d->L;
+  cuuint64_t dims[5] = {ST_BM, 2, L, ptiles, (cuuint64_t)d->nb * d->nc};
+  cuuint64_t strides[4] = {ST_BM * 2, ST_BM * 4, ST_BM * 4 * L, ST_BM * 4 * L * ptiles};
+  cuuint32_t box[5] = {64, 2, (cuuint32_t)d->L, 1, 1};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 5, const_cast<void*>(U16), dims, strides, box, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }

@@ -190,7 +190,7 @@ struct TcShared {
 };
 
 // HALF = false: U in FP32 as [item][j][m'][c] (re, im); true: scale·U in FP16 as
-// [m'][ν = 2(j·nc + c) + (re|im)][item] (items padded to whole tiles of 128), the layout the
+// [(j, c)][item tile][m'][re|im][128 items] (items padded to whole tiles of 128), the layout the
 // tensor-core transform along a (slab_tc.cu) loads its operand tiles from.
 template <bool HALF>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const __grid_constant__ CUtensorMap umap) {
@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
           fence_proxy_async();
           bar_sync(1, 128);
           if (leader) {
-            if (ptile * TC_BN + c0 < a.n_items) tma_store_3d(&umap, stg, ptile * TC_BN + c0, r0, mp);
+            if (ptile * TC_BN + c0 < a.n_items) tma_store_5d(&umap, stg, c0, 0, mp, ptile, r0 >> 1);
             bulk_commit();
           }
         }
@@ -512,18 +512,21 @@ extern "C" int zeb_spectrum_bf16(const float* alm, int n_items, const zeb_so3_di
   return zeb_launch_check("spectrum_bf16");
 }
 
-// scale·U in FP16 as [m'][ν][item]: a 3-D tensor [L][rows][items rounded up to tiles], boxes of 64
-// items × 128 rows × 1 order with the 128-byte swizzle of the staging buffer
+// scale·U in FP16 as [(j, c)][item tile][m'][re|im][128 items]: a 5-D tensor (items within the tile,
+// re|im, order, tile, (j, c)); a store box is 64 items × the 128 rows ν = 2(j·nc + c) + (re|im) of
+// a row tile (64 (j, c) × re|im) of one order and one tile, with the staging buffer's 128-byte
+// swizzle. One (j, c) of one tile of items is then 2L × 256 contiguous bytes: what the transform
+// along a loads as one operand tile.
 static bool tc_u16_map(CUtensorMap* m, void* U16, const zeb_so3_dims_t* d, int n_items) {
   auto fn = tc_encode_fn();
   if (!fn) return false;
-  const cuuint64_t ppad = (cuuint64_t)((n_items + TC_BN - 1) / TC_BN) * TC_BN;
-  const cuuint64_t rows = 2 * (cuuint64_t)d->nb * d->nc;
-  cuuint64_t dims[3] = {ppad, rows, (cuuint64_t)d->L};
-  cuuint64_t strides[2] = {ppad * 2, ppad * 2 * rows};
-  cuuint32_t box[3] = {64, (cuuint32_t)TC_BM, 1};
-  cuuint32_t es[3] = {1, 1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, U16, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+  const cuuint64_t ptiles = (cuuint64_t)((n_items + TC_BN - 1) / TC_BN);
+  const cuuint64_t L = (cuuint64_t)d->L;
+  cuuint64_t dims[5] = {TC_BN, 2, L, ptiles, (cuuint64_t)d->nb * d->nc};
+  cuuint64_t strides[4] = {TC_BN * 2, TC_BN * 4, TC_BN * 4 * L, TC_BN * 4 * L * ptiles};
+  cuuint32_t box[5] = {64, 2, 1, 1, (cuuint32_t)TC_BM / 2};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 5, U16, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
          CUDA_SUCCESS;
 }
