@@ -14,8 +14,11 @@ scan.  Inputs (720 MB) exceed L2 (126 MB), so no flush is needed between steps.
 
 `value` times the device path with the stored patterns already resident in HBM; `e2e` times the
 public API (Solver.index) from host memory: uploads, device path, the records' readback and the
-host's landing of results.  Under torchrun each rank indexes its own scan (weak scaling, no
-collective on the data path; the max of the ranks' times is reported).
+host's landing of results.  With --gpus N (N > 1; run directly, the command re-executes itself
+under torch.distributed.run, one process per GPU) every rank holds the same scan: `value` has each
+rank index all of it (weak scaling, no collective on the data path), `e2e` shards the one scan
+over the ranks (shard.index_sharded: contiguous shares, the records gathered to rank 0); both
+report the max of the ranks' CUDA-event times.
 """
 import argparse
 import json
@@ -249,6 +252,8 @@ def device_main(a):
     from zebsdsolve_b200 import synthetic as syn
     from zebsdsolve_b200.master import write_npz
 
+    from zebsdsolve_b200 import shard
+
     rows, cols = scan_shape(a.patterns)
     n = rows * cols
     sheets = syn.master_sheets(2, side=401, lmax=96, group="432", device="cuda")
@@ -260,12 +265,14 @@ def device_main(a):
     s.set_patterns(np.zeros((rows, cols, H, W), np.uint16))
     s.set_geometry(pc=PC, sample_tilt_deg=70.0, detector_tilt_deg=0.0)
     e = s._e
-    rng = np.random.default_rng(100 + rank)
+    # the same scan on every rank: each indexes all of it for the device-resident value (weak
+    # scaling) and its share of it for the end-to-end value (one scan sharded over the ranks)
+    rng = np.random.default_rng(100)
     q, grain = syn.grain_map(rng, rows, cols, GRAINS, SPREAD_DEG)
     pats = np.empty((n, H, W), np.uint16)
     for i in range(0, n, 16384):
         sims = e.simulate_device(0, np.arange(i, min(n, i + 16384)), q[i:i + 16384])
-        pats[i:i + len(sims)] = syn.counted_patterns(sims, seed=1000 * rank + i // 16384).cpu().numpy()
+        pats[i:i + len(sims)] = syn.counted_patterns(sims, seed=i // 16384).cpu().numpy()
     s.set_patterns(pats.reshape(rows, cols, H, W))
     e.prepare(L)
     torch.cuda.synchronize()
@@ -318,9 +325,14 @@ def device_main(a):
         stages = timer.totals()
         # e2e: the public API from pinned host memory, every step (uploads, passes, readbacks, landing);
         # two untimed runs: a scan's first run streams through the staging slots, its second makes
-        # the page-locked copy of the whole scan that every later run uploads from
+        # the page-locked copy of the whole scan that every later run uploads from. With several
+        # ranks the one scan is sharded (shard.index_sharded: each rank its contiguous share of the
+        # cells, the records gathered to rank 0, which holds the whole map's results)
+        def api_run():
+            return shard.index_sharded(s, dist) if dist else s.index()
+
         for _ in range(max(2, a.warmup - 2)):
-            s.index()
+            api_run()
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -328,7 +340,7 @@ def device_main(a):
         torch.cuda.synchronize()
         e0.record()
         for _ in range(a.steps):
-            r = s.index()
+            r = api_run()
         e1.record()
         torch.cuda.synchronize()
         ems = max_over_ranks(e0.elapsed_time(e1) / a.steps)
@@ -337,28 +349,31 @@ def device_main(a):
     clk = Clocks(local)
     ms, ems, launches, stages, r = time_form(a.precision, clk, nvtx=True)
     value = n * world / (ms / 1e3)
-    e2e = n * world / (ems / 1e3)
-    dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), q))
+    e2e = n / (ems / 1e3)  # one scan's patterns over the job's time (all of it on one rank, or sharded)
     fp32 = None
     if not a.no_fp32_form and a.precision != "f32":
         ms32, ems32, _, stages32, r32 = time_form("f32")
-        dis32 = np.degrees(s.disorientation(r32["quaternions"].reshape(-1, 4), q))
-        agree = np.degrees(s.disorientation(r32["quaternions"].reshape(-1, 4), r["quaternions"].reshape(-1, 4)))
-        fp32 = {"value": round(n * world / (ms32 / 1e3), 1), "e2e": round(n * world / (ems32 / 1e3), 1),
-                "ms_per_step": round(ms32, 3), "stage_ms_per_step": {k: round(v, 3) for k, v in stages32.items()},
-                "median_deg": round(float(np.median(dis32)), 4),
-                "forms_within_0.1deg": round(float((agree < 0.1).mean()), 5)}
 
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
+    dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), q))
+    if not a.no_fp32_form and a.precision != "f32":
+        dis32 = np.degrees(s.disorientation(r32["quaternions"].reshape(-1, 4), q))
+        agree = np.degrees(s.disorientation(r32["quaternions"].reshape(-1, 4), r["quaternions"].reshape(-1, 4)))
+        fp32 = {"value": round(n * world / (ms32 / 1e3), 1), "e2e": round(n / (ems32 / 1e3), 1),
+                "ms_per_step": round(ms32, 3), "stage_ms_per_step": {k: round(v, 3) for k, v in stages32.items()},
+                "median_deg": round(float(np.median(dis32)), 4),
+                "forms_within_0.1deg": round(float((agree < 0.1).mean()), 5)}
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     ph = e.bands[L]["phases"][0][1]
     d = ph.dims
-    # algorithmic HBM bytes of each stage per pattern (its kernels' compulsory reads and writes)
-    u_bytes = d.nb * d.L * d.nc * 8
+    # algorithmic HBM bytes of each stage per pattern (its kernels' compulsory reads and writes):
+    # U, the spectrum, is complex FP32 (8 bytes a value) in the FP32 form and complex FP16 (4) in
+    # the BF16 form
+    u_bytes = d.nb * d.L * d.nc * (4 if ph.u_scale is not None else 8)
     algo = {"prep": H * W * (2 + 4),                       # u16 in, f32 out
             "sphere": H * W * 4 + d.n_pairs * 8,           # pattern in, coefficients out
             "spectrum": d.n_pairs * 8 + u_bytes,           # coefficients in, U out
@@ -384,7 +399,10 @@ def device_main(a):
         "dtype": "f32" if a.precision == "f32" else "bf16+f32", "data": "synthetic",
         "config": config_of(a, n),
         "e2e": {"value": round(e2e, 1), "unit": "patterns/s", "h2d_bytes_per_step": int(n * H * W * 2),
-                "d2h_bytes_per_step": int(n * (8 + 4) * 4 * len(e.phases))},
+                "d2h_bytes_per_step": int(n * (8 + 4) * 4 * len(e.phases)),
+                **({"scaling": "strong", "note": f"one {rows}x{cols} scan sharded over {world} ranks "
+                                                  "(shard.index_sharded), records gathered to rank 0"}
+                   if world > 1 else {})},
         "gpu_launches": int(launches),
         "roofline": dict(roof[dom], kernel=dom, per_launch_patterns=batch),
         "rooflines": roof,
@@ -624,7 +642,8 @@ def reference_main(a):
     v = done / dt
     n = ROWS * COLS if a.patterns == ROWS * COLS else a.patterns
     line = {"impl": "reference", "metric": "patterns/s indexed+refined on 1 B200, BF16 form vs plain FP32 at <=0.1 deg error",
-            "value": round(v, 3), "unit": "patterns/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "value": round(v, 3), "unit": "patterns/s", "n_gpus": int(os.environ.get("WORLD_SIZE", a.gpus)),
+            "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": round(1e3 * dt / a.steps, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(a, n),
             "cpu_baseline": {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port",
@@ -1035,8 +1054,23 @@ def nickel_main(a):
     print(json.dumps(line), flush=True)
 
 
+def relaunch(a):
+    """`--gpus N` (N > 1) run directly: the same command under torch.distributed.run, one process
+    per GPU of this node (rendezvous on 127.0.0.1); returns its exit status."""
+    import socket
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={a.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 if __name__ == "__main__":
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args))
     if args.impl == "reference":
         reference_main(args)
     elif args.workload == "adjoint":

@@ -282,6 +282,14 @@ int zeb_correlate_volume(const float* U, int n_items, const zeb_so3_dims_t* d, c
 int zeb_rden_build(const float* vol_f, const float* vol_f2, const float* stats, int n, long long cells,
                    float* rden, void* stream);
 
+/* The failure test of the tensor-core kernels (zeb_spectrum_bf16, zeb_spectrum_bf16_h,
+ * zeb_correlate_peaks_h, zeb_match_bf16): while ns > 0, each of them launched makes its MMA thread
+ * wait first on an mbarrier that nothing arrives at and gives every wait ns nanoseconds, so that the
+ * kernel gives up as it would on a real timeout: it sets its status word, waits (up to 1 s) for its
+ * own copies and MMAs in flight, frees its tensor memory and returns. 0 (the default) turns it off.
+ * No counterpart in the reference (its waits are the WebGPU queue's). */
+int zeb_set_test_stall(long long ns);
+
 /* ── (c) refinement and scores on the detector ──────────────────────────────────────────── */
 
 typedef struct {

@@ -98,3 +98,80 @@ def test_two_gloo_ranks_assemble_the_map(tmp_path):
     assert ok == 1.0
     assert slowest == 11.0  # the max over the ranks
     assert mine == 25  # 7 × 7 region cells split 25 / 24: rank 0 takes 25
+
+
+# ── the real engine on two ranks (one GPU: each rank's kernels are its own; the ranks meet only
+# on the host, in gloo collectives) ──
+
+def _engine_worker(rank, world, port, out, path):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        s = _scan_solver(path)
+        r = shard.index_sharded(s, dist)  # the default run(): the engine's sweeps over this rank's cells
+        if rank == 0:
+            single = _scan_solver(path).index()  # the same scan on one rank
+            np.savez(out, **{f"s_{k}": v for k, v in r.items()}, **{f"o_{k}": v for k, v in single.items()})
+        else:
+            assert r is None
+    finally:
+        dist.destroy_process_group()
+
+
+def _scan_solver(path):
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import synthetic as syn
+
+    s = ze.Solver()
+    s.configure(bandwidth=32, precision="bf16")
+    s.add_phase(path)
+    rows, cols = 9, 13
+    s.set_patterns(np.zeros((rows, cols, 60, 60), np.uint16))
+    s.set_geometry(pc=(0.5, 0.3, 0.6), sample_tilt_deg=70, detector_tilt_deg=0)
+    q, _ = syn.grain_map(np.random.default_rng(8), rows, cols, 7, 0.5)
+    sims = s._e.simulate_device(0, np.arange(rows * cols), q)
+    s.set_patterns(syn.counted_patterns(sims, seed=3).cpu().numpy().reshape(rows, cols, 60, 60))
+    return s
+
+
+@pytest.mark.gpu
+def test_index_sharded_on_two_ranks_equals_one_rank(tmp_path):
+    """shard.index_sharded with its default run() on two ranks: each rank's own chance calibration
+    (from the same region lattice), sweeps, acceptance and landing over its contiguous share; rank 0
+    assembles the map. Every result field equals a one-rank Solver.index of the same scan."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import tempfile
+
+    import torch.multiprocessing as mp
+    from zebsdsolve_b200 import synthetic as syn
+    from zebsdsolve_b200.master import write_npz
+
+    d = tempfile.mkdtemp()
+    sheets = syn.master_sheets(4, side=201, lmax=48, group="432")
+    write_npz(f"{d}/m.npz", sheets, 201, syn.group_matrices("432"), 30)
+    out = str(tmp_path / "rank0.npz")
+    mp.spawn(_engine_worker, args=(2, _free_port(), out, f"{d}/m.npz"), nprocs=2, join=True)
+    z = np.load(out)
+    for k in ("quaternions", "euler", "ncc", "nmi", "phase", "z", "sweep"):
+        assert np.array_equal(z[f"s_{k}"], z[f"o_{k}"]), k
+    assert (z["s_phase"] >= 0).all()
+
+
+def test_bench_gpus_n_runs_n_ranks():
+    """`bench.py --gpus 2` run directly re-executes itself under torch.distributed.run; rank 0 alone
+    prints the line (the reference arm: no GPU needed) with n_gpus 2, and the job exits 0."""
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    p = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "1"], capture_output=True, text=True, timeout=900, env=env)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [json.loads(l) for l in p.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1 and lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"

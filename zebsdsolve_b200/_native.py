@@ -71,6 +71,7 @@ _SIGS = {
     "zeb_peaks_scratch_bytes": ([ctypes.POINTER(So3Dims), c_int], c_size_t),
     "zeb_correlate_peaks": ([P, c_int, ctypes.POINTER(So3Dims), P, P, c_int, P, P, P], c_int),
     "zeb_spectrum_h_bytes": ([ctypes.POINTER(So3Dims), c_int], c_size_t),
+    "zeb_set_test_stall": ([c_longlong], c_int),
     "zeb_spectrum_bf16_h": ([P, c_int, ctypes.POINTER(So3Dims), c_int, P, P, P, c_float, P, P], c_int),
     "zeb_correlate_peaks_h": ([P, c_int, ctypes.POINTER(So3Dims), c_float, P, P, P, P, P], c_int),
     "zeb_correlate_peaks_static": ([P, c_int, ctypes.POINTER(So3Dims), P, P, c_int, P, P], c_int),

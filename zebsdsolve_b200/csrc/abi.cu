@@ -6,6 +6,9 @@
 
 namespace zeb {
 static thread_local char g_error[1024];
+static long long g_test_stall_ns = 0;  // zeb_set_test_stall: 0 off
+
+long long test_stall_ns() { return __atomic_load_n(&g_test_stall_ns, __ATOMIC_RELAXED); }
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -27,3 +30,12 @@ extern "C" size_t zeb_error(char* buf, size_t cap) {
 }
 
 extern "C" const char* zeb_version(void) { return "0.2.8"; }
+
+// The wait limit of the tensor-core kernels' failure test: while ns > 0, every tcgen05 kernel
+// launched makes its MMA thread wait first on an mbarrier that nothing arrives at, and gives each
+// of its waits ns nanoseconds (the waits for its own copies in flight keep 1 s).
+extern "C" int zeb_set_test_stall(long long ns) {
+  ZEB_REQUIRE(ns >= 0 && ns <= 10000000000LL, ZEB_EARG, "set_test_stall: %lld ns", ns);
+  __atomic_store_n(&zeb::g_test_stall_ns, ns, __ATOMIC_RELAXED);
+  return ZEB_OK;
+}

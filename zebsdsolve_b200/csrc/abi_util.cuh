@@ -9,6 +9,11 @@
 
 namespace zeb {
 void set_error(const char* fmt, ...);
+long long test_stall_ns();  // zeb_set_test_stall's value (0: off)
+// how long a wait of the tensor-core kernels may take (1 s, far above any legitimate wait inside
+// one CTA), and the waits for a CTA's own copies and MMAs in flight once it has given up
+constexpr long long kWaitNs = 1000000000LL;
+constexpr long long kDrainNs = 1000000000LL;
 }
 
 #define ZEB_REQUIRE(cond, code, ...) \

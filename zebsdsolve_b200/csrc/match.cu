@@ -133,13 +133,14 @@ struct MatchArgs {
   int* cand_i;
   int* status;
   long long limit;
+  long long stall;  // > 0: the failure test (the MMA thread first waits on `never`)
 };
 
 struct MatchShared {
   uint8_t a[MT_STAGES][MT_A_BLOCK];
   uint8_t b[MT_STAGES][MT_B_BLOCK];
   float stash[32][32 * MT_EPI];  // a chunk of each epilogue thread's scores, [column][thread]
-  uint64_t full[MT_STAGES], empty[MT_STAGES], acc_full[2], acc_empty[2], mma_done;
+  uint64_t full[MT_STAGES], empty[MT_STAGES], acc_full[2], acc_empty[2], mma_done, never;
   uint32_t tmem;
 };
 
@@ -194,6 +195,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
       mbar_init(&s.acc_empty[i], MT_EPI);
     }
     mbar_init(&s.mma_done, 1);
+    mbar_init(&s.never, 1);  // nothing arrives: the failure test's wait
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
       // the copies still in flight land before the CTA may leave (bounded waits on their phases;
       // a phase already consumed reads as complete)
       for (int i = (it > MT_STAGES ? it - MT_STAGES : 0); i < it; ++i)
-        mbar_wait(&s.full[i % MT_STAGES], (i / MT_STAGES) & 1, lim);
+        mbar_wait(&s.full[i % MT_STAGES], (i / MT_STAGES) & 1, kDrainNs);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -232,6 +234,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
       const uint32_t idesc =
           (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(MT_BN >> 3) << 17) | ((uint32_t)(MT_BM >> 4) << 24);
       bool ok = true;
+      if (a.stall > 0 && !mbar_wait(&s.never, 0, a.stall)) ok = false;  // the failure test
       int it = 0;
       for (int t = 0; t < my_tiles && ok; ++t) {
         const int acc = t & 1;
@@ -255,7 +258,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
       }
       if (!ok) atomicOr(a.status, 2);
       umma_commit(&s.mma_done);
-      if (!mbar_wait(&s.mma_done, 0, lim)) atomicOr(a.status, 8);
+      if (!mbar_wait(&s.mma_done, 0, kDrainNs)) atomicOr(a.status, 8);
     }
   } else {
     // epilogue: warp w may read only TMEM lanes 32·(w mod 4) …, so warps w and w + 4 share a
@@ -559,7 +562,8 @@ extern "C" int zeb_match_bf16(const void* x_panel, int n_exp, const void* d_pane
   a.cand_v = cand_v;
   a.cand_i = cand_i;
   a.status = status;
-  a.limit = 1000000000LL;  // 1 s: far above any legitimate wait inside one CTA
+  a.stall = test_stall_ns();
+  a.limit = a.stall > 0 ? a.stall : kWaitNs;
   // every candidate reads as "none" until the kernel writes it (a CTA that gave up writes nothing)
   cudaMemsetAsync(cand_i, 0xFF, (size_t)n_exp * slices * MT_TOP * sizeof(int), (cudaStream_t)stream);
   const size_t smem = sizeof(MatchShared) + 1024;

@@ -369,7 +369,9 @@ __global__ void __launch_bounds__(64) k_peak_finish(SlabArgs a, R v_at, float* _
   __syncthreads();
   const float vbest = best.x;
   uint32_t idx = __float_as_uint(best.y);
-  if (idx == 0xffffffffu) idx = 0;
+  // no candidate, or one a transform that gave up on a wait never wrote (its status word reports
+  // it): the volume's first cell, so that every read below stays inside U and rden
+  if (idx >= (uint32_t)nb * (uint32_t)nc * (uint32_t)n) idx = 0;
   const int ia = idx & (n - 1);
   const int iq = (idx / n) & (nc - 1);
   const int j = idx / (n * nc);

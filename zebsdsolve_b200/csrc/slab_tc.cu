@@ -49,6 +49,7 @@ struct SlabTcArgs {
   float2* cand;       // [item][nb]: (value, bits of the volume index)
   int* status;
   long long limit;
+  long long stall;  // > 0: the failure test (the MMA thread first waits on `never`)
 };
 
 constexpr int ST_ACC = 4;    // accumulators in tensor memory (4 × 128 columns)
@@ -61,7 +62,7 @@ struct SlabTcShared {
   float bestv[2][ST_BM];                      // the second half's best, handed to the first
   uint32_t besti[2][ST_BM];
   uint64_t full[ST_STAGES], empty[ST_STAGES], acc_full[ST_ACC], acc_empty[ST_ACC], rfull[ST_RSLOTS],
-      rempty[ST_RSLOTS], mma_done;
+      rempty[ST_RSLOTS], mma_done, never;
   uint32_t tmem;
 };
 
@@ -104,6 +105,7 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
       mbar_init(&s.rempty[i], ST_EPI);
     }
     mbar_init(&s.mma_done, 1);
+    mbar_init(&s.never, 1);  // nothing arrives: the failure test's wait
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   build_dft(s.f, n, a.L);
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
 
   if (warp == 0) {
     if (lane == 0) {
-      long long it = 0;
+      long long it = 0, rit = 0;  // tiles of U and rows of rden issued
       bool ok = true;
       for (long long mi = 0; mi < my_items && ok; ++mi) {
         const long long item = blockIdx.x + mi * gridDim.x;
@@ -141,20 +143,21 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
           const int rs = (int)(it % ST_RSLOTS);
           if (!mbar_wait(&s.rempty[rs], (uint32_t)((it / ST_RSLOTS) & 1) ^ 1u, lim)) {
             ok = false;
-            ++it;
+            ++it;  // its tile of U is in flight
             break;
           }
           mbar_expect_tx(&s.rfull[rs], (uint32_t)n * 4u);
           bulk_g2s(s.rden[rs], a.rden + (size_t)(j * nc + c) * n, (uint32_t)n * 4u, &s.rfull[rs]);
+          rit = it + 1;
         }
       }
       if (!ok) atomicOr(a.status, 1);
       // the loads still in flight land before the CTA may leave (bounded waits on their phases; a
       // phase already consumed reads as complete)
       for (long long i = (it > ST_STAGES ? it - ST_STAGES : 0); i < it; ++i)
-        mbar_wait(&s.full[i % ST_STAGES], (uint32_t)((i / ST_STAGES) & 1), lim);
-      for (long long i = (it > ST_RSLOTS ? it - ST_RSLOTS : 0); i < it; ++i)
-        mbar_wait(&s.rfull[i % ST_RSLOTS], (uint32_t)((i / ST_RSLOTS) & 1), lim);
+        mbar_wait(&s.full[i % ST_STAGES], (uint32_t)((i / ST_STAGES) & 1), kDrainNs);
+      for (long long i = (rit > ST_RSLOTS ? rit - ST_RSLOTS : 0); i < rit; ++i)
+        mbar_wait(&s.rfull[i % ST_RSLOTS], (uint32_t)((i / ST_RSLOTS) & 1), kDrainNs);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -164,6 +167,7 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
       const int ksteps = (2 * a.L) / 16;
       const uint32_t fbase = smem_addr(s.f[0]);
       bool ok = true;
+      if (a.stall > 0 && !mbar_wait(&s.never, 0, a.stall)) ok = false;  // the failure test
       long long t = 0;
       for (; t < total && ok; ++t) {
         const int acc = (int)(t % ST_ACC);
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
       }
       if (!ok) atomicOr(a.status, 2);
       umma_commit(&s.mma_done);  // every MMA issued has finished before TMEM may be freed
-      if (!mbar_wait(&s.mma_done, 0, lim)) atomicOr(a.status, 8);
+      if (!mbar_wait(&s.mma_done, 0, kDrainNs)) atomicOr(a.status, 8);
     }
   } else {
     // epilogue: warp w reads TMEM lanes 32·(w mod 4) …; warps w and w + 4 take the two halves of
@@ -347,7 +351,8 @@ extern "C" int zeb_correlate_peaks_h(const void* U16, int n_items, const zeb_so3
   a.rden = rden;
   a.cand = (float2*)scratch;
   a.status = status;
-  a.limit = 1000000000LL;  // 1 s: far above any legitimate wait inside one CTA
+  a.stall = test_stall_ns();
+  a.limit = a.stall > 0 ? a.stall : kWaitNs;
   cudaStream_t st = (cudaStream_t)stream;
   const size_t smem = sizeof(SlabTcShared) + 1024;
   cudaFuncSetAttribute(k_slab_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -175,6 +175,7 @@ struct TcArgs {
   float2* U;
   int* status;      // nonzero after a timed-out wait (what the CTA was waiting on)
   long long limit;  // nanoseconds before a wait gives up
+  long long stall;  // > 0: the failure test (the MMA thread first waits on `never`)
   int per;          // row tiles per CTA (blockIdx.z picks the group)
   float scale;      // HALF: U is stored as scale·U in FP16
 };
@@ -183,7 +184,7 @@ struct TcShared {
   uint8_t b[TC_MAX_KB][TC_B_BLOCK];   // 96 KB, 1024-aligned
   uint8_t a[TC_STAGES][TC_A_BLOCK];   // 80 KB
   float stage[2][32 * TC_BM];          // 2 × 16 KB: a 32-pattern chunk of the tile, [pattern][row]
-  uint64_t b_full, a_full[TC_STAGES], a_empty[TC_STAGES], acc_full[2], acc_empty[2], mma_done;
+  uint64_t b_full, a_full[TC_STAGES], a_empty[TC_STAGES], acc_full[2], acc_empty[2], mma_done, never;
   long long a_off, b_off;
   uint32_t tmem;
   int failed;
@@ -206,6 +207,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
   if (threadIdx.x == 0) {
     mbar_init(&s.b_full, 1);
     mbar_init(&s.mma_done, 1);
+    mbar_init(&s.never, 1);  // nothing arrives: the failure test's wait
     s.a_off = tc_offset(t.L, t.split, mp, t.mtiles, TC_A_BLOCK);
     s.b_off = tc_offset(t.L, t.split, mp, t.ptiles, TC_B_BLOCK);
     for (int i = 0; i < TC_STAGES; ++i) {
@@ -248,17 +250,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
       if (it < total) {
         atomicOr(a.status, 1);
         s.failed = 1;
-        // the copies still in flight land before the CTA may leave (bounded waits on their phases)
-        mbar_wait(&s.b_full, 0, lim);
-        for (int i = (it > TC_STAGES ? it - TC_STAGES : 0); i < it; ++i)
-          mbar_wait(&s.a_full[i % TC_STAGES], (i / TC_STAGES) & 1, lim);
       }
+      // the copies still in flight land before the CTA may leave, whether or not the MMAs took
+      // them (bounded waits on their phases; a phase already consumed reads as complete)
+      mbar_wait(&s.b_full, 0, kDrainNs);
+      for (int i = (it > TC_STAGES ? it - TC_STAGES : 0); i < it; ++i)
+        mbar_wait(&s.a_full[i % TC_STAGES], (i / TC_STAGES) & 1, kDrainNs);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       // kind::f16: F32 accumulate, BF16 A and B, both K-major, N = 128, M = 128
       const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
       bool ok = mbar_wait(&s.b_full, 0, lim);
+      if (a.stall > 0 && !mbar_wait(&s.never, 0, a.stall)) ok = false;  // the failure test
       int it = 0;
       for (int mt = 0; mt < mtiles && ok; ++mt) {
         const int acc = mt & 1;
@@ -286,7 +290,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
       }
       // every MMA issued has finished before TMEM may be freed
       umma_commit(&s.mma_done);
-      if (!mbar_wait(&s.mma_done, 0, lim)) atomicOr(a.status, 8);
+      if (!mbar_wait(&s.mma_done, 0, kDrainNs)) atomicOr(a.status, 8);
     }
   } else {
     // epilogue (warps 2-5): a warp may reach only its TMEM lane quadrant, so warp w drains tile
@@ -492,7 +496,8 @@ extern "C" int zeb_spectrum_bf16(const float* alm, int n_items, const zeb_so3_di
   TcArgs a{};
   a.t = t; a.A = (const uint8_t*)A; a.B = (const uint8_t*)B; a.n_items = n_items; a.U = (float2*)U;
   a.status = status;
-  a.limit = 1000000000LL;  // 1 s: far above any legitimate wait inside one CTA
+  a.stall = test_stall_ns();
+  a.limit = a.stall > 0 ? a.stall : kWaitNs;
   size_t smem = sizeof(TcShared) + 1024;
   cudaFuncSetAttribute(k_spectrum_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   // enough CTAs for several waves: row tiles split into groups when the pattern tiles are few
@@ -558,7 +563,8 @@ extern "C" int zeb_spectrum_bf16_h(const float* alm, int n_items, const zeb_so3_
   TcArgs a{};
   a.t = t; a.A = (const uint8_t*)A; a.B = (const uint8_t*)B; a.n_items = n_items; a.U = nullptr;
   a.status = status;
-  a.limit = 1000000000LL;
+  a.stall = test_stall_ns();
+  a.limit = a.stall > 0 ? a.stall : kWaitNs;
   a.scale = scale;
   size_t smem = sizeof(TcShared) + 1024;
   cudaFuncSetAttribute(k_spectrum_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
