@@ -98,19 +98,29 @@ def oracle_scan(raw_sheets, static_bg, L_=L, refine=True, baked=None):
                     static_bg=static_bg, refine=refine, baked=baked)
 
 
-def _oracle_cell(raw):
+def _oracle_cell(job):
     import oracle.pipeline as opl
 
-    r = opl._one(raw)
+    r = opl._one(job)
     return r["q"], r["ncc"], r["nmi"]
 
 
-def oracle_run(scan, raws):
-    """The oracle over the stored patterns `raws` on the host cores (oracle.pipeline.index_many):
-    (records [(q in the fundamental zone, NCC, NMI)], patterns/s, cores, seconds)."""
+def oracle_geometry(px_um=0.0, step_um=1.0):
+    """The workload's geometry in the oracle's terms (the pixel size the engine takes by default:
+    the detector's 24 mm over 60 pixels; steps of 1 µm)."""
+    import oracle.geometry as og
+
+    return og.Geometry(pc=PC, sample_tilt_deg=70.0, px_um=px_um or 1000.0 * 24.0 / W, step_x_um=step_um,
+                       step_y_um=step_um)
+
+
+def oracle_run(scan, raws, ts=None):
+    """The oracle over the stored patterns `raws` (at positions `ts`) on the host cores
+    (oracle.pipeline.index_many): (records [(q in the fundamental zone, NCC, NMI)], patterns/s,
+    cores, seconds)."""
     import oracle.pipeline as opl
 
-    recs, dt, cores = opl.index_many(scan, raws)
+    recs, dt, cores = opl.index_many(scan, raws, ts)
     return [(r["q"], r["ncc"], r["nmi"]) for r in recs], len(recs) / dt, cores, dt
 
 
@@ -136,7 +146,9 @@ def host_workload(rank=0):
     """The workload's lattice cells made on the host, for a run without a GPU (the reference arm):
     the same master and grain map (same seeds), each cell's pattern simulated by the oracle's
     projection of the baked master and given the same noise model (Poisson counts of
-    1000·(0.6 + 0.4·m)·B, NumPy's generator). Returns (raws [cells][H][W] u16, scan, cells)."""
+    1000·(0.6 + 0.4·m)·B, NumPy's generator), at its own detector position (the engine's default
+    pixel size and steps, its default scan signs −1). Returns (raws [cells][H][W] u16, scan, cells,
+    positions)."""
     import oracle.detector as od
     import oracle.geometry as og
     import oracle.pipeline as opl
@@ -147,20 +159,21 @@ def host_workload(rank=0):
     rng = np.random.default_rng(100 + rank)
     q, _ = syn.grain_map(rng, rows, cols, GRAINS, SPREAD_DEG)
     cells = opl.lattice(rows, cols, ORACLE_CELLS)
-    geo = og.Geometry(pc=PC, sample_tilt_deg=70.0)
+    geo = oracle_geometry()
     baked = opl.bake(sheets, 401, opl.pixel_angle(geo, H))
-    frame, t0 = geo.frame(), geo.translation(H, W)
+    frame = geo.frame()
+    ts = opl.cell_positions(geo, rows, cols, cells, H, W, -1.0, -1.0)
     yy, xx = np.meshgrid(np.arange(H) + 0.5 - H / 2, np.arange(W) + 0.5 - W / 2, indexing="ij")
     B = np.exp(-(xx ** 2 + yy ** 2) / (2 * (0.4 * W) ** 2))
     B *= B.size / B.sum()
     noise = np.random.default_rng(7 + rank)
     raws = np.empty((len(cells), H, W), np.uint16)
     for k, c in enumerate(cells):
-        sim = od.project(baked, 401, frame, t0, q[c], H, W)
+        sim = od.project(baked, 401, frame, ts[k], q[c], H, W)
         raws[k] = np.clip(noise.poisson(np.maximum(1000 * (0.6 + 0.4 * sim) * B, 0)), 0, 65535)
     # the lattice is the static background's lattice: its mean is the scan's static background
     scan = oracle_scan(sheets, raws.astype(np.float64).mean(0), baked=baked)
-    return raws, scan, cells
+    return raws, scan, cells, ts
 
 
 def config_of(a, n):
@@ -422,7 +435,10 @@ def device_main(a):
 
         ocells = opl.lattice(rows, cols, ORACLE_CELLS)
         scan = oracle_scan(sheets, opl.static_average(pats, rows, cols, 1024))
-        orecs, v, cores, dt = oracle_run(scan, pats[ocells])
+        g = e.geo
+        og_ = oracle_geometry(g.px_um, g.step_x_um)
+        ts = opl.cell_positions(og_, rows, cols, ocells, H, W, s.settings["scan_x_sign"], s.settings["scan_y_sign"])
+        orecs, v, cores, dt = oracle_run(scan, pats[ocells], ts)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port",
                                 "sample": f"{len(ocells)} cells on a lattice over the map (their own stored patterns: "
                                           f"filtered, correlated at L={L}, refined, NMI) through the FP64 oracle in "
@@ -614,7 +630,7 @@ def reference_main(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    raws, scan, cells = host_workload()
+    raws, scan, cells, ts = host_workload()
     for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS"):
         os.environ[k] = "1"
     cores = max(1, min(len(os.sched_getaffinity(0)), 64))
@@ -623,7 +639,7 @@ def reference_main(a):
     nxt = [0]
 
     def step(pool):
-        sel = [raws[(nxt[0] + i) % len(raws)] for i in range(cores)]
+        sel = [(raws[(nxt[0] + i) % len(raws)], ts[(nxt[0] + i) % len(raws)]) for i in range(cores)]
         nxt[0] += cores
         return pool.map_async(_oracle_cell, sel, chunksize=1).get(limit)
 

@@ -46,6 +46,14 @@ def static_average(patterns, rows, cols, want=1024):
     return np.asarray(patterns)[cells].astype(np.float64).mean(0)
 
 
+def cell_positions(geo, rows, cols, cells, h, w, x_sign=1.0, y_sign=1.0, binning=1.0):
+    """engine.zig:1601-1613 with geometry.zig:165-192 — each map cell's detector position
+    (pixels): the map-centre cell's less the beam's travel from it (none without a pixel size)."""
+    cells = np.asarray(cells, np.int64)
+    return np.stack([geo.position_for(c // cols, c % cols, 0.5 * (rows - 1), 0.5 * (cols - 1), x_sign, y_sign, binning,
+                                      h / binning, w / binning) for c in cells])
+
+
 def pixel_angle(geo, h, binning=1.0, pixel_angle_deg=0.0):
     """engine.zig:1028-1035 — a detector pixel's angular width, radians."""
     if pixel_angle_deg > 0:
@@ -121,15 +129,17 @@ def _init(scan):
     _STATE["scan"] = scan
 
 
-def _one(raw):
-    return _STATE["scan"].index(raw)
+def _one(job):
+    raw, t = job
+    return _STATE["scan"].index(raw, t)
 
 
-def index_many(scan, raws, workers=None, limit=1800.0):
-    """Scan.index over the stored patterns `raws` in a spawn pool of `workers` processes (default:
-    every core this process may use, at most 64), one thread each. One pattern per worker goes first,
-    untimed (imports, caches). Returns (records, seconds of the timed map, workers); a map that
-    takes more than `limit` seconds raises."""
+def index_many(scan, raws, ts=None, workers=None, limit=1800.0):
+    """Scan.index over the stored patterns `raws` (at detector positions `ts`, default the map
+    centre's) in a spawn pool of `workers` processes (default: every core this process may use,
+    at most 64), one thread each. One pattern per worker goes first, untimed (imports, caches).
+    Returns (records, seconds of the timed map, workers); a map that takes more than `limit`
+    seconds raises."""
     import multiprocessing as mp
     import os
     import time
@@ -137,7 +147,7 @@ def index_many(scan, raws, workers=None, limit=1800.0):
     # one thread per worker: the workers' BLAS and FFT pools would otherwise each take every core
     for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS"):
         os.environ[k] = "1"
-    raws = list(raws)
+    raws = list(zip(raws, [None] * len(raws) if ts is None else list(ts)))
     workers = max(1, min(workers or len(os.sched_getaffinity(0)), 64, len(raws)))
     osp._wigner_blocks(scan.tb)  # built once here and shipped to the workers with the rest
     with mp.get_context("spawn").Pool(workers, initializer=_init, initargs=(scan,)) as pool:

@@ -113,3 +113,77 @@ def test_a_scan_stepped_through_once_is_not_page_locked_whole(scan):
     assert steps >= 1 and not calls and e._pinned is None
     s.index()
     assert calls and e._pinned is not None
+
+
+def test_cell_under_another_centre_leaves_the_geometry(scan):
+    """cell_under (__init__.py:198-212): one cell indexed and simulated under another pattern
+    centre; the geometry in use is untouched, and under the geometry in use it is index_cells."""
+    s, q = _solver(scan)
+    before = s.geometry
+    u = s.cell_under(7, pc=(0.51, 0.31, 0.61))
+    assert s.geometry == before
+    assert set(u) == {"phase", "quaternion", "ncc", "nmi", "simulation"}
+    assert u["simulation"].shape == (60, 60) and u["phase"] == 0
+    same = s.cell_under(7)
+    ref = s.index_cells([7], bandwidth=s.settings["fit_bandwidth"])
+    assert np.array_equal(same["quaternion"], ref["quaternions"][0, 0])
+    assert np.allclose(same["simulation"], s.simulate(same["quaternion"][None], cells=[7])[0])
+    # the same cell under the other centre scores differently (its own projection)
+    assert abs(u["ncc"] - same["ncc"]) > 1e-6
+
+
+def test_pattern_stats_profile_and_counts(scan):
+    s, _ = _solver(scan)
+    mean, std = s.pattern_stats()
+    pats = s._e.patterns.reshape(96, -1).astype(np.float64)
+    assert mean.shape == (8, 12)
+    assert np.allclose(mean.reshape(-1), pats.mean(1), rtol=1e-6) and np.allclose(std.reshape(-1), pats.std(1), rtol=1e-5)
+    m2, s2 = s.pattern_stats([3, 50])
+    assert np.allclose(m2, mean.reshape(-1)[[3, 50]])
+    s.gpu_counts()
+    assert s.profile(True) is True
+    s.index()
+    rep = s.profile_report()
+    s.profile(False)
+    names = [ln.split()[0] for ln in rep.splitlines()[1:-1]]
+    assert "zeb_refine_list" in names and "zeb_sphere_coefficients_spans" in names, rep
+    c = s.gpu_counts()
+    assert c["dispatches"] > 0 and c["submits"] >= 1 and c["reads"] >= 2 and c["waits"] >= 1, c
+    assert s.gpu_counts()["dispatches"] == 0  # since the last call
+    # the plain function reads a scan file's patterns (here the test data's h5ebsd, when present)
+    from conftest import testdata
+    import zebsdsolve_b200 as ze
+
+    path = testdata("nickel", "patterns_v2.h5")
+    if path is not None:
+        p3 = ze.load_patterns(str(path), cells=[0, 1, 2])
+        assert p3.shape == (3, 60, 60) and p3.dtype == np.float32
+
+
+def test_binned_search_refined_or_scored_at_the_stored_size(scan):
+    """settings.full_resolution (engine.zig:996-1003, 2101-2119): the search on patterns binned 2×,
+    then the refinement ("refine") or only the scores ("scores") at the stored size: scores change
+    (they are the stored size's), orientations are those of the binned run when only the scores
+    move, and a refinement at the stored size is at least as good as the binned one."""
+    s, q = _solver(scan)
+    s.configure(binning=2)
+    assert s.pattern_shape == (30, 30) and s.shape(full=True) == (60, 60)
+    assert s.pattern(5).shape == (30, 30) and s.pattern(5, full=True).shape == (60, 60)
+    full = s.pattern(5, full=True)
+    assert abs(float(full.sum())) < 1e-3 and abs(float((full ** 2).sum()) - 1) < 1e-3  # filtered at 60 × 60
+    rb = {}
+    for mode in ("none", "scores", "refine"):
+        s.configure(full_resolution=mode)
+        rb[mode] = s.index()
+        rb[mode]["dis"] = np.degrees(s.disorientation(rb[mode]["quaternions"].reshape(-1, 4), q))
+    assert np.allclose(rb["scores"]["dis"], rb["none"]["dis"], atol=0.05)
+    assert abs(float(rb["scores"]["ncc"].mean() - rb["none"]["ncc"].mean())) > 1e-3
+    assert rb["refine"]["ncc"].mean() > rb["scores"]["ncc"].mean() - 1e-3
+    assert np.median(rb["refine"]["dis"]) <= np.median(rb["none"]["dis"]) + 0.02
+    assert (rb["refine"]["phase"] == 0).all()
+    # refined at the stored size, the binned search's peaks settle where the unbinned run's do
+    s.configure(binning=1, full_resolution="none")
+    r1 = s.index()
+    apart = np.degrees(s.disorientation(rb["refine"]["quaternions"].reshape(-1, 4), r1["quaternions"].reshape(-1, 4)))
+    assert np.median(apart) < 0.02 and (apart < 0.1).mean() > 0.95, np.sort(apart)[-4:]
+    assert abs(float(rb["refine"]["ncc"].mean() - r1["ncc"].mean())) < 2e-3

@@ -48,10 +48,13 @@ def world():
     pats = syn.counted_patterns(sims, seed=31).cpu().numpy()
     s.set_patterns(pats.reshape(rows, cols, 60, 60))
 
-    geo = og.Geometry(pc=PC, sample_tilt_deg=70.0)
+    g = s.geometry
+    geo = og.Geometry(pc=PC, sample_tilt_deg=70.0, px_um=g["px_um"], step_x_um=g["step_x_um"], step_y_um=g["step_y_um"])
     scan = opl.Scan(sheets, 401, syn.group_matrices("432"), geo, 60, 60, 64,
                     static_bg=opl.static_average(pats, rows, cols, 1024))
-    recs, _, _ = opl.index_many(scan, pats)
+    st = s.settings
+    ts = opl.cell_positions(geo, rows, cols, np.arange(N_CELLS), 60, 60, st["scan_x_sign"], st["scan_y_sign"])
+    recs, _, _ = opl.index_many(scan, pats, ts)
     return {"s": s, "pats": pats, "q": q, "scan": scan, "oracle": recs}
 
 

@@ -94,6 +94,8 @@ class Solver:
         step_x_um, step_y_um, plane_kind, plane). A pattern centre set by hand is one for the whole
         map again (the plane of source points goes unless one comes with it)."""
         self._call("set_geometry", self._e.geo.given, fields, self._e.geo_given)
+        if not self._e.geo.px_um > 0:  # (no pixel size: the scan's own, or its detector's width's)
+            self._e.geo.px_um = self._e.default_px()
         return self
 
     # ── scan ──
@@ -111,6 +113,7 @@ class Solver:
                 "dtype": ["uint8", "uint16", "float32"][self._e.pixel], "format": src.get("format", "array"),
                 "voltage_kv": src.get("voltage_kv", float("nan")), "pc_note": src.get("pc_note", ""),
                 "has_background": src.get("background") is not None, "has_pc": src.get("pc") is not None,
+                "has_px": bool(src.get("px_um")),
                 "pattern_kinds": src.get("pattern_kinds", [])}
 
     def open(self, *paths):
@@ -148,7 +151,9 @@ class Solver:
             geo["px_um"] = float(info["px_um"])
         if geo:
             self.set_geometry(**geo)
-        self._e.scan_source = {"format": sc.format, "voltage_kv": info["voltage_kv"], "pc_note": info["pc_note"],
+        px = info.get("px_um", float("nan"))
+        self._e.scan_source = {"px_um": float(px) if np.isfinite(px) and px > 0 else None,
+                               "format": sc.format, "voltage_kv": info["voltage_kv"], "pc_note": info["pc_note"],
                                "paths": paths, "pc": info["pc"], "background": info.get("background"),
                                "pattern_kinds": info.get("pattern_kinds", [])}
         self._e.avg = None
@@ -174,7 +179,29 @@ class Solver:
             fh.write(text)
 
     def shape(self, full=False):
+        """(h, w) of a pattern as the search sees it (reduced by `binning`), or (full) as stored."""
+        if full:
+            return tuple(self._call("scan", self._e.info)[2:])
         return self._call("pattern_shape", self._e.pattern_shape)
+
+    def pattern_stats(self, cells=None):
+        """(mean, standard deviation) of the stored patterns of the given map cells (all of them by
+        default, shaped (rows, cols)), over every stored pixel in FP64 (engine.zig:2696-2728): maps
+        of either show the microstructure before indexing."""
+        rows, cols, h, w = self._call("scan", self._e.info)
+        whole = cells is None
+        c = np.arange(rows * cols) if whole else np.asarray(cells, np.int64).reshape(-1)
+        if len(c) and (c.min() < 0 or c.max() >= rows * cols):
+            raise Error("pattern_stats: OutOfRange")
+        flat = self._e.patterns.reshape(rows * cols, h * w)
+        mean = np.empty(len(c), np.float32)
+        std = np.empty(len(c), np.float32)
+        for i in range(0, len(c), 4096):
+            x = flat[c[i:i + 4096]].astype(np.float64)
+            m = x.mean(1)
+            mean[i:i + 4096] = m
+            std[i:i + 4096] = np.sqrt(np.maximum((x * x).mean(1) - m * m, 0.0))
+        return (mean.reshape(rows, cols), std.reshape(rows, cols)) if whole else (mean, std)
 
     @property
     def pattern_shape(self):
@@ -419,6 +446,75 @@ class Solver:
                 "phase": r["phase"].reshape(rows, cols).copy(), "z": r["z"].reshape(rows, cols).copy(),
                 "sweep": r["sweep"].reshape(rows, cols).copy()}
 
+    def cell_under(self, cell, bandwidth=None, full=False, **fields):
+        """Index one map cell and simulate it under another geometry than the one in use, which
+        stays as it is (__init__.py:198-212): the fields given change it as for `set_geometry`
+        (e.g. cell_under(c, pc=file_pc) to set two pattern centres side by side). The spherical
+        correlation at `bandwidth` (default fit_bandwidth), then the refinement. Returns the best
+        phase's {phase, quaternion, ncc, nmi, simulation} (the simulation at the stored size with
+        `full`)."""
+        e = self._e
+        keep = e.geo
+        tmp = keep.copy()
+        self._call("cell_under", tmp.given, fields, type(keep)())
+        if not tmp.px_um > 0:
+            tmp.px_um = e.default_px()
+        bw = int(bandwidth or e.set["fit_bandwidth"])
+        try:
+            e.geo = tmp
+            recs = self._call("cell_under", e.index_cells, np.array([int(cell)], np.int64), bw, "spherical", None,
+                              False)
+            p = int(e.choose_phase(recs)[0])
+            r = recs[p, 0]
+            binning = e.set["binning"]
+            if full and binning != 1:
+                e.set.apply({"binning": 1.0})
+            try:
+                sim = self._call("cell_under", e.simulate, p, np.array([int(cell)]), r[None, :4])[0]
+            finally:
+                if full and binning != 1:
+                    e.set.apply({"binning": binning})
+        finally:
+            e.geo = keep
+        return {"phase": p, "quaternion": r[:4].copy(), "ncc": float(r[4]), "nmi": float(r[5]), "simulation": sim}
+
+    # ── the device's own accounts ──
+
+    def gpu_counts(self):
+        """GPU traffic since the last call (__init__.py:938-942): kernel launches (dispatches),
+        device passes (submits), readbacks to the host (reads) and host waits on the device (waits)."""
+        from . import _native as N
+
+        c = self._e.counts
+        now = {"dispatches": N.launches["count"], "submits": c["submits"], "reads": c["reads"], "waits": c["waits"]}
+        last, self._counts_seen = getattr(self, "_counts_seen", None) or dict.fromkeys(now, 0), now
+        return {k: int(now[k] - last[k]) for k in now}
+
+    def profile(self, on=True):
+        """Time every kernel entry point on the GPU from now on (CUDA events on the stream it runs
+        on; __init__.py:944-946); profile_report() gives the totals. Returns True (timing is
+        always available here)."""
+        from . import _native as N
+
+        if on and not N.profiling["on"]:
+            N.profiling["pairs"], N.profiling["totals"] = [], {}
+        N.profiling["on"] = bool(on)
+        return True
+
+    def profile_report(self):
+        """The profile's totals per entry point since profile(True): calls, device milliseconds,
+        microseconds a call and share of the whole, largest first (__init__.py:948-951)."""
+        from . import _native as N
+
+        N.profile_flush(wait=True)
+        rows = sorted(N.profiling["totals"].items(), key=lambda kv: -kv[1][1])
+        total = sum(v[1] for _, v in rows) or 1.0
+        lines = [f"{'entry point':<34} {'calls':>7} {'ms':>10} {'us/call':>10} {'share':>7}"]
+        for name, (n, ms) in rows:
+            lines.append(f"{name:<34} {n:>7d} {ms:>10.3f} {1000 * ms / max(n, 1):>10.1f} {100 * ms / total:>6.1f}%")
+        lines.append(f"{'total':<34} {sum(v[0] for _, v in rows):>7d} {total if rows else 0.0:>10.3f}")
+        return "\n".join(lines) + "\n"
+
     def reduce(self, quaternions, phase=0):
         from .rotations import to_bunge, to_fz
 
@@ -433,4 +529,4 @@ class Solver:
         return disorientation(qa, qb, self._e.phases[phase].master.rotations())
 
 
-from .api import Result, fit_pattern_center, fit_plane, index  # noqa: E402,F401
+from .api import Result, fit_pattern_center, fit_plane, index, load_patterns  # noqa: E402,F401

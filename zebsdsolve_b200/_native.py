@@ -151,10 +151,45 @@ def last_error(lib=None):
     return buf.value.decode(errors="replace") if n else ""
 
 
+# Solver.profile: while on, every entry point that launches kernels is bracketed by two CUDA events
+# on the current stream (the one the entry points are given); profile_report sums them by name
+profiling = {"on": False, "pairs": [], "totals": {}}
+
+
+def profile_flush(wait=True):
+    """Fold the recorded event pairs into the per-entry-point totals (name → [calls, ms]); with
+    wait, after the device has finished them, else only the pairs already complete."""
+    import torch
+
+    if wait and profiling["pairs"]:
+        torch.cuda.synchronize()
+    keep = []
+    for name, e0, e1 in profiling["pairs"]:
+        if wait or e1.query():
+            t = profiling["totals"].setdefault(name, [0, 0.0])
+            t[0] += 1
+            t[1] += e0.elapsed_time(e1)
+        else:
+            keep.append((name, e0, e1))
+    profiling["pairs"] = keep
+
+
 def call(name, *args):
     """Call an entry point; a negative return raises NativeError with the library's message."""
     lib = load()
+    timed = profiling["on"] and KERNELS.get(name, 0) > 0
+    if timed:
+        import torch
+
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record()
     rc = getattr(lib, name)(*args)
+    if timed:
+        e1 = torch.cuda.Event(enable_timing=True)
+        e1.record()
+        profiling["pairs"].append((name, e0, e1))
+        if len(profiling["pairs"]) > 4096:
+            profile_flush(wait=False)
     launches["count"] += KERNELS.get(name, 0)
     if isinstance(rc, int) and rc < 0:
         raise NativeError(f"{name}: {last_error(lib) or rc}")

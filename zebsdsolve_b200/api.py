@@ -47,6 +47,20 @@ def _open(solver, scan, phases, kwargs):
         solver.add_phase(p)
 
 
+def load_patterns(scan, cells=None, processed=False, **settings):
+    """Patterns of a scan file as float32 (n, h, w) (api.py:70-80): the given map cells
+    (row-major indices; all of them by default), as stored or after the filters, at the size the
+    `binning` setting reduces them to."""
+    from . import Solver
+
+    with Solver() as s:
+        s.configure(**settings)
+        s.open(*([scan] if isinstance(scan, (str, Path)) else scan))
+        info = s.scan
+        cells = range(info["rows"] * info["cols"]) if cells is None else cells
+        return np.stack([s.pattern(int(c), processed) for c in cells])
+
+
 def fit_pattern_center(scan, phases, **kwargs):
     """Fit the pattern centre by the voting search (api.py:83-93). Returns the fit's report (pc,
     score, start, …) with the last grid's votes under "scores", its axes under "axes" and the

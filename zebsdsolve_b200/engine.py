@@ -169,8 +169,11 @@ class Engine:
         self._ring, self._ring_i = [], 0  # two page-locked slots a scan not pinned whole streams through
         self._last_fz = None  # the last index_cells' records in the fundamental zones
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
+        self.counts = {"submits": 0, "reads": 0, "waits": 0}  # device passes, readbacks, host waits
+        self._full = False  # at_full: the stored size is the level being worked at
         self.geo_given = Geometry()  # the geometry as given (set_geometry), where a full fit starts
         self._nl_view = None  # what averaging with neighbours did to the last pattern looked at
+        self._nl_report = False  # log what the averaging did to the next batch (an indexing run's first)
         self.pc_history = []  # the grids of the last pattern-centre vote (pcfit.run)
         self.plane_points = None  # the source points of the last plane fit
         self.fit = None  # the last fit's patterns: cells, orientations, phases, scores
@@ -225,10 +228,42 @@ class Engine:
         rows, cols, h, w = self.patterns.shape
         return rows, cols, h, w
 
+    # ── levels (engine.zig:990-1035): the patterns reduced by settings.binning, and as stored ──
+
+    def factor(self):
+        """The reduction of the level being worked at: settings.binning, or 1 inside at_full."""
+        return 1.0 if self._full else float(self.set["binning"])
+
+    def at_full(self):
+        """A context in which everything that depends on the level (the pattern's size, the frame,
+        the detector positions, the static background, the filters' widths, the master's bake,
+        the chance calibration) is the stored size's (engine.zig Level.full)."""
+        import contextlib
+
+        @contextlib.contextmanager
+        def ctx():
+            was = self._full
+            self._full = True
+            try:
+                yield
+            finally:
+                self._full = was
+
+        return ctx()
+
+    def stage_full(self, stage):
+        """engine.zig:996-1003 — whether a stage ("search", "refine", "score") works at the stored
+        size: never when nothing is reduced; settings.full_resolution "scores" puts the scores
+        there, "refine" the refinement and the scores."""
+        if self.set["binning"] == 1:
+            return False
+        mode = self.set["full_resolution"]
+        return (mode == "scores" and stage == "score") or (mode == "refine" and stage != "search")
+
     def pattern_shape(self):
-        """engine.zig:1011-1017 — the reduced size floor(size / binning) (no other level here)."""
+        """engine.zig:1011-1017 — the level's size floor(size / factor)."""
         rows, cols, h, w = self.info()
-        b = self.set["binning"]
+        b = self.factor()
         return int(math.floor(h / b)), int(math.floor(w / b))
 
     def mask_of(self, h, w):
@@ -257,7 +292,7 @@ class Engine:
         """The detector position for each cell (FP64; geometry.zig:80-83): the plane of source
         points' where the geometry has one, else the reference cell's less the beam's travel."""
         rows, cols, h, w = self.info()
-        b = self.set["binning"]
+        b = self.factor()
         g = self.geo if geo is None else geo
         cells = np.asarray(cells, np.int64)
         if g.plane_kind:
@@ -308,14 +343,14 @@ class Engine:
                              '(static_background: "average" takes the patterns\' own)')
                     self.told_no_background = True
                 return None
-            key = ("file", id(src), self.set["binning"])
+            key = ("file", id(src), self.factor())
             if self.avg is None or self.avg[0] != key:
-                avg = reduce_image(np.asarray(src, np.float64), self.set["binning"]).astype(np.float32)
+                avg = reduce_image(np.asarray(src, np.float64), self.factor()).astype(np.float32)
                 self.avg = (key, torch.as_tensor(avg, device=self.dev))
             return self.avg[1]
         if kind != "average":
             return None
-        key = ("average", self.set["static_patterns"], self.set["binning"])
+        key = ("average", self.set["static_patterns"], self.factor())
         if self.avg is None or self.avg[0] != key:
             cells = self.lattice(self.set["static_patterns"])
             rows, cols, h, w = self.info()
@@ -323,7 +358,7 @@ class Engine:
             acc = np.zeros((h, w))
             for i in range(0, len(cells), 1024):
                 acc += flat[cells[i:i + 1024]].sum(0, dtype=np.float64)
-            avg = reduce_image(acc / len(cells), self.set["binning"]).astype(np.float32)
+            avg = reduce_image(acc / len(cells), self.factor()).astype(np.float32)
             self.avg = (key, torch.as_tensor(avg, device=self.dev))
             self.log(f"static background: the average of {len(cells)} patterns over the map")
         return self.avg[1]
@@ -345,11 +380,25 @@ class Engine:
         self.dicts = {}
         self.chance_key = None
 
+    def default_px(self):
+        """engine.zig:948-956 — the detector's pixel size (µm) when none is set by hand: the scan
+        file's, else the detector's width (settings.detector_width_mm) over the pattern's stored
+        pixels across; 0 with no scan."""
+        if self.patterns is None:
+            return 0.0
+        px = ((getattr(self, "scan_source", None) or {}).get("px_um")) or 0.0
+        if px > 0:
+            return float(px)
+        return 1000.0 * float(self.set["detector_width_mm"]) / max(self.info()[3], 1)
+
     def pixel_angle(self):
-        """engine.zig:1028-1035 — angular width of one reduced pixel, radians."""
-        rows, cols, h, w = self.info()
-        stored = math.radians(self.set["pixel_angle_deg"]) if self.set["pixel_angle_deg"] > 0 else 1.0 / max(self.geo.pc[2] * h, 1e-9)
-        return stored * self.set["binning"]
+        """engine.zig:1028-1035 — angular width of one reduced pixel, radians (0 before any scan is
+        set, unless pixel_angle_deg gives it: the master is then baked unsmoothed)."""
+        if self.patterns is None and not self.set["pixel_angle_deg"] > 0:
+            return 0.0
+        stored = (math.radians(self.set["pixel_angle_deg"]) if self.set["pixel_angle_deg"] > 0
+                  else 1.0 / max(self.geo.pc[2] * self.info()[2], 1e-9))
+        return stored * self.factor()
 
     def bake_key(self, p):
         """engine.zig:1674-1697 — what a phase's master must be filtered for: the smoothing (its
@@ -362,7 +411,7 @@ class Engine:
         if not px > 0:
             return (None, s["master_smooth"], False, 0.0, 0.0, False, 0, 0, 0.0)
         q = int(math.floor(math.log(px) / math.log(1.05) + 0.5))
-        f = s["binning"]
+        f = self.factor()
         fine, coarse = (s["bp_fine"] / f, s["bp_coarse"] / f) if s["bandpass"] else (0.0, 0.0)
         tiles = bins = 0
         clip = 0.0
@@ -384,9 +433,8 @@ class Engine:
             key = self.bake_key(p)
             if p.baked is not None and p.baked[0] == key:
                 continue
-            if key in p.bakes:  # a detector size met before (scans of several sizes): its master as baked then
-                p.baked = p.bakes[key]
-                self.chance_key = None
+            if key in p.bakes:  # a detector size or level met before: its master as baked then (the
+                p.baked = p.bakes[key]  # chance calibration's key names each phase's bake)
                 continue
             sheets = self.bake(p, key)
             grad = torch.empty(sheets.numel() * 4, dtype=torch.float32, device=self.dev)
@@ -469,7 +517,7 @@ class Engine:
         """engine.zig:1839-1849, spherical.zig:448-464 — each phase's reciprocal denominator
         volume for the map-centre geometry (cached per geometry)."""
         rows, cols, h, w = self.info()
-        bn = self.set["binning"]
+        bn = self.factor()
         t = self.geo.translation(h / bn, w / bn).astype(np.float32)
         key = (tuple(fr.c0), tuple(fr.c1), tuple(fr.c2), fr.h, fr.w, tuple(fr.mask), tuple(t))
         bt = b["tables"]
@@ -603,21 +651,51 @@ class Engine:
             self.upload_raw(lst, raw, torch.cuda.current_stream())
             loaded = self.buf("nl_loaded", nw * px)
             sb = N.load().zeb_prep_scratch_bytes(nw, h, w, 0.0)
-            N.call("zeb_prep_reduced", ptr(raw), self.pixel, nw, sh, sw, float(s["binning"]), None, 0, 0.0, mask, 0,
+            N.call("zeb_prep_reduced", ptr(raw), self.pixel, nw, sh, sw, self.factor(), None, 0, 0.0, mask, 0,
                    ptr(loaded), ptr(self.buf("prep_scratch", sb // 4 + 1) if sb else None), stream_ptr())
             nbr_d = self.to_device("nl_nbr", nbr)
             cnt = (ctypes.c_int * len(counts))(*counts)
             scratch = self.buf("nl_scratch", N.load().zeb_nlpar_scratch_bytes(nw, px, R, P) // 4 + 1)
             sig = shares = None
-            if account and t0 == 0:
+            report = self._nl_report and t0 == 0
+            if (account or report) and t0 == 0:
                 sig = torch.empty(counts[R * P], dtype=torch.float32, device=self.dev)
                 shares = torch.empty(counts[0] * F, dtype=torch.float32, device=self.dev)
             N.call("zeb_nlpar", ptr(loaded), px, ptr(nbr_d), cnt, R, P, float(s["nlpar_lambda"]), ptr(out[t0 * px:]),
                    ptr(sig), ptr(shares), ptr(scratch), stream_ptr())
             if sig is not None:
-                self._nl_view = self._nlpar_view(sig.cpu().numpy(), shares.cpu().numpy()[:F], nbr[0], R * P)
+                sg, sh_ = sig.cpu().numpy(), shares.cpu().numpy()
+                if account:
+                    self._nl_view = self._nlpar_view(sg, sh_[:F], nbr[0], R * P)
+                if report:
+                    self._nl_report = False
+                    self._log_nlpar(sg, sh_, nbr, counts[0], F)
             t0 += m
         return out[: n * px]
+
+    def _log_nlpar(self, sig, shares, nbr, n, F):
+        """engine.zig:1285-1321 — what the averaging did to a batch's n cells, logged: the stored
+        patterns' noise (a pixel's standard deviation), the share of it an average keeps and the
+        share of an average that is the pattern itself, each a mean over the cells."""
+        s = self.set
+        noise = kept = own = counted = 0.0
+        for c in range(n):
+            sh_ = shares[c * F:(c + 1) * F].astype(np.float64)
+            nb = nbr[c]
+            inside = nb != 0xFFFFFFFF
+            before = float(sig[c])
+            after = float((sh_[inside] ** 2 * sig[nb[inside].astype(np.int64)]).sum())
+            own += sh_[F // 2]
+            if not before > 0:
+                continue
+            noise += math.sqrt(before)
+            kept += math.sqrt(after / before)
+            counted += 1
+        P, R = int(s["nlpar_iterations"]), int(s["nlpar_radius"])
+        self.log(f"neighbour averaging: {P} pass{'' if P == 1 else 'es'} over {2 * R + 1} × {2 * R + 1} cells "
+                 f"(λ {s['nlpar_lambda']:.2f}); noise about {noise / max(counted, 1):.2f} a pixel, "
+                 f"{100 * kept / max(counted, 1):.0f} % of it left; an average is {100 * own / max(n, 1):.0f} % the "
+                 f"pattern itself")
 
     @staticmethod
     def _nlpar_view(sig, share, nbr0, reach):
@@ -640,7 +718,8 @@ class Engine:
         rows, cols, sh, sw = self.info()
         h, w = self.pattern_shape()
         if full and (h, w) != (sh, sw) and stage != 0:
-            raise EngineError("pattern: only the stored pattern is kept at the full size (binning is on)")
+            with self.at_full():  # the filters (and the background) at the stored size's level
+                return self.pattern(cell, stage, False)
         self._nl_view = None
         if stage == 3:
             bg = self.static_background()
@@ -683,14 +762,14 @@ class Engine:
                 raise EngineError("nlpar: the cells of the patterns are needed to average them with their neighbours")
             raw = self.nlpar_average(cells)
             return self.filter_chain(raw, 2, n, h, w, 1.0)
-        return self.filter_chain(raw, self.pixel, n, sh, sw, float(s["binning"]))
+        return self.filter_chain(raw, self.pixel, n, sh, sw, self.factor())
 
-    def filter_chain(self, raw, pixel, n, sh, sw, factor):
+    def filter_chain(self, raw, pixel, n, sh, sw, factor, out_name="pats"):
         """prep.zig:143-204 — n patterns (pixel type, stored size sh × sw reduced by factor) through
         static background, dynamic background, CLAHE, band pass, mask and normalization."""
         h, w = self.pattern_shape()
         s = self.set
-        out = self.buf("pats", n * h * w)
+        out = self.buf(out_name, n * h * w)
         static = self.static_background()
         dyn, sigma = self.prep_options()
         mask = (ctypes.c_float * 3)(*self.mask_of(h, w))
@@ -713,7 +792,7 @@ class Engine:
             N.call("zeb_clahe", ptr(cur), n, h, w, s["clahe_grid"], s["clahe_bins"], float(s["clahe_clip"]), ptr(cs),
                    stream_ptr())
         if bandpass:
-            f = float(s["binning"])
+            f = self.factor()
             fine, coarse = s["bp_fine"] / f, s["bp_coarse"] / f
             low = self.buf("prep_low", n * h * w)
             run(cur, 2, h, w, 1.0, None, 3, coarse, 0, low)
@@ -741,13 +820,23 @@ class Engine:
             self.prepare_masters()
             for pi in range(len(self.phases)):
                 self.dictionary(pi, int(grid or self.set["dict_grid"]), method)
-            self.calibrate()
+            self.calibrate_at_score_level()
+            self.prepare_masters()
             return None
         L = int(bandwidth or self.set["bandwidth"])
         b = self.band(L)
-        self.calibrate()
+        self.calibrate_at_score_level()
+        self.prepare_masters()  # (the search level's bake)
         self.denominators(b, self.frame())
         return b
+
+    def calibrate_at_score_level(self):
+        """What chance gives, measured where the scores are taken (engine.zig:2250)."""
+        if self.stage_full("score"):
+            with self.at_full():
+                self.calibrate()
+        else:
+            self.calibrate()
 
     def dictionary(self, pi, grid, method):
         """engine.zig:1851-1955 — phase pi's dictionary of this grid, simulated at the map's
@@ -761,7 +850,7 @@ class Engine:
             self.dicts[(pi, grid)] = d
             self.log(f"dictionary: {d.n} orientations for the rotations {p.master.setting.rotation} (grid {grid})")
         rows, cols, h, w = self.info()
-        bn = self.set["binning"]
+        bn = self.factor()
         t = self.geo.translation(h / bn, w / bn).astype(np.float32)
         fr = self.frame()
         s = self.set
@@ -834,6 +923,7 @@ class Engine:
     def run_device(self, raw, cells, bandwidth=None, timer=None, method="spherical", grid=None):
         """One pass of the device path over n = len(cells) stored patterns already on the device:
         records [phase][cell][8] as a device tensor (engine.zig:2005-2122, no readback)."""
+        self.counts["submits"] += 1
         if method != "spherical":
             return self.run_device_dictionary(raw, cells, method, int(grid or self.set["dict_grid"]), timer)
         n = len(cells)
@@ -857,9 +947,11 @@ class Engine:
                ptr(spans), FLAG_CENTER | FLAG_NORM, ptr(alm), ptr(stats), ptr(sphere_scratch), stream_ptr())
         opts = N.RefineOpts(s["refine_iters"] if s["refine"] else 0, math.radians(s["refine_step"]), 1.0, 0.02, 1e4,
                             s["nmi_bins"], float(self.batch_stamp))
+        self._seeds = []
         for pi, p in enumerate(self.phases):
             ph = b["phases"][pi][1]
-            peaks = self.buf("peaks", n * 8)
+            peaks = self.buf(f"peaks{pi}" if self.stage_full("refine") else "peaks", n * 8)
+            self._seeds.append(peaks)
             tile = self.tile_items(ph, n)
             for t0 in range(0, n, tile):
                 nt = min(tile, n - t0)
@@ -883,9 +975,40 @@ class Engine:
                 N.call("zeb_correlate_peaks", ptr(U), nt, ctypes.byref(ph.dims), ptr(bt.tw), ptr(ph.rden), 1 << 30,
                        ptr(peaks[t0 * 8:]), ptr(cand), stream_ptr())
             mark("refine")
-            self.refine(pats, items, peaks, n, fr, p, opts, recs[pi * n * 8:])
+            if not self.stage_full("refine"):
+                self.refine(pats, items, peaks, n, fr, p, opts, recs[pi * n * 8:])
+        self.finish_levels(raw, cells, pats, items, fr, recs, opts)
         mark("end")
         return recs[: n_ph * n * 8].view(n_ph, n, 8)
+
+    def finish_levels(self, raw, cells, pats, items, fr, recs, opts):
+        """engine.zig:2101-2119 — with settings.full_resolution "refine", each phase's refinement
+        from its search seeds (self._seeds), with "scores", the refined records scored again (no
+        step), at the stored size: the patterns filtered at that size, the detector positions and
+        frame in its pixels, each phase's master baked for it. The records are written into recs."""
+        lr, lc = self.stage_full("refine"), self.stage_full("score")
+        if not (lr or lc):
+            return
+        n = len(cells)
+        rows, cols, sh, sw = self.info()
+        with self.at_full():
+            self.prepare_masters()
+            fp = self.filter_chain(raw, self.pixel, n, sh, sw, 1.0, out_name="pats_full") if not self.set["nlpar"] \
+                else self.preprocess(raw, n, cells)
+            t = self.positions(cells)
+            fi = self.to_device("items_full", np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1))
+            ff = self.frame()
+            for pi, p in enumerate(self.phases):
+                out = recs[pi * n * 8:]
+                if lr:
+                    self.refine(fp, fi, self._seeds[pi], n, ff, p, opts, out)
+                else:  # the refined orientations scored again at the stored size (no step)
+                    seeds = self.buf("rescore_seeds", n * 8)
+                    seeds[: n * 8].copy_(out[: n * 8])
+                    sc = N.RefineOpts(0, opts.max_step, opts.scale0, opts.scale_min, opts.scale_max, opts.nmi_bins,
+                                      opts.stamp)
+                    self.refine(fp, fi, seeds, n, ff, p, sc, out)
+        self.prepare_masters()  # (back to the search level's bake)
 
     def run_device_dictionary(self, raw, cells, method, grid, timer=None):
         """run_device with a dictionary search (engine.zig:2094-2112): each pattern's best entry
@@ -905,13 +1028,18 @@ class Engine:
                             s["nmi_bins"], float(self.batch_stamp))
         x = pats[: n * fr.h * fr.w].view(n, fr.h * fr.w)
         tc = s["precision"] != "f32"
+        self._seeds = []
         for pi, p in enumerate(self.phases):
             d = self.dictionary(pi, grid, method)
             mark("match")
             xs = x @ d.W.T if method == "pca" else x  # the patterns' coefficients (pca.zig:159-162)
-            peaks = d.seeds(xs.contiguous(), tc, self.tc_status(), self.buf("peaks", n * 8))
+            peaks = d.seeds(xs.contiguous(), tc, self.tc_status(),
+                            self.buf(f"peaks{pi}" if self.stage_full("refine") else "peaks", n * 8))
+            self._seeds.append(peaks)
             mark("refine")
-            self.refine(pats, items, peaks, n, fr, p, opts, recs[pi * n * 8:])
+            if not self.stage_full("refine"):
+                self.refine(pats, items, peaks, n, fr, p, opts, recs[pi * n * 8:])
+        self.finish_levels(raw, cells, pats, items, fr, recs, opts)
         mark("end")
         return recs[: n_ph * n * 8].view(n_ph, n, 8)
 
@@ -1087,6 +1215,8 @@ class Engine:
         recs = self.run_device(raw, cells, bandwidth, method=method, grid=grid)
         self._last_fz = self.fz_of(recs).cpu().numpy()
         out = recs.cpu().numpy()
+        self.counts["reads"] += 2
+        self.counts["waits"] += 2
         self.check_device()
         return self.finish(out)
 
@@ -1206,6 +1336,8 @@ class Engine:
         def drain(k):
             ev, cb, stamp = back[k]
             ev.synchronize()
+            self.counts["reads"] += 2  # the records and their fundamental-zone orientations
+            self.counts["waits"] += 1
             back[k] = None
             out = host[k][:, : len(cb)].numpy().copy()
             fz = hfz[k][:, : len(cb)].numpy().copy()
@@ -1272,7 +1404,7 @@ class Engine:
         n_ph = len(self.phases)
         s = self.set
         key = (s["static_background"], s["static_patterns"], s["dynamic_background"], s["dynamic_sigma"], s["mask"],
-               s["mask_radius"], s["nmi_bins"], s["binning"], s["master_smooth"], s["pixel_angle_deg"], self.geo.key(),
+               s["mask_radius"], s["nmi_bins"], self.factor(), s["master_smooth"], s["pixel_angle_deg"], self.geo.key(),
                tuple(id(p.baked[1]) if p.baked else None for p in self.phases), s["roi_x"], s["roi_y"], s["roi_w"],
                s["roi_h"], id(self.patterns))
         if key == self.chance_key and len(self.chance_med) == n_ph:
@@ -1323,6 +1455,7 @@ class Engine:
         self.res["phase"][cells] = -1
         self.res["sweep"][cells] = -1
         self.res["z"][cells] = 0
+        self._nl_report = bool(self.set["nlpar"])  # the run's first batch says what the averaging did
 
     def land(self, cells, recs, fz=None):
         """engine.zig:2392-2419 — each cell keeps the better match; accepted ones their sweep.
