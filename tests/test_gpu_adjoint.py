@@ -42,7 +42,7 @@ def setup():
     rng = np.random.default_rng(31)
     pc0 = np.array([0.5, 0.3, 0.6])
     s.set_patterns(np.zeros((1, n, h, w), np.float32))
-    s.set_geometry(pc=tuple(pc0), sample_tilt_deg=70, detector_tilt_deg=0)
+    s.set_geometry(pc=tuple(pc0), sample_tilt_deg=70, detector_tilt_deg=0, step_x_um=0, step_y_um=0)  # one source for every cell
     e = s._e
     e.prepare_masters()
     baked = e.phases[0].baked[1].cpu().numpy().astype(np.float64)

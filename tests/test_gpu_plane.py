@@ -39,7 +39,7 @@ def small():
     n = 5
     rng = np.random.default_rng(41)
     s.set_patterns(np.zeros((1, n, h, w), np.float32))
-    s.set_geometry(pc=(0.5, 0.3, 0.6), sample_tilt_deg=70, detector_tilt_deg=0)
+    s.set_geometry(pc=(0.5, 0.3, 0.6), sample_tilt_deg=70, detector_tilt_deg=0, step_x_um=0, step_y_um=0)  # one source
     e = s._e
     e.prepare_masters()
     baked = e.phases[0].baked[1].cpu().numpy().astype(np.float64)
