@@ -223,7 +223,7 @@ size_t zeb_tc_patterns_bytes(const zeb_so3_dims_t* d, int split, int n_items);
 
 /* The BF16 form's spectrum kept in FP16 (half the bytes of U): zeb_spectrum_bf16's GEMM, its
  * accumulators scaled by `scale` and rounded to FP16 as they drain, stored as
- * U16[j·nc + c][item / 128][m'][re|im][item % 128] with the items padded to a multiple of 128
+ * U16[item / 128][j·nc + c][m'][re|im][item % 128] with the items padded to a multiple of 128
  * (zeb_spectrum_h_bytes bytes; U16 128-byte aligned). `scale` is a power of two with
  * scale·max|U| well inside FP16's range: the host takes it from the table, as 2^floor(log2(16384 /
  * y)) with y the largest column norm over l of any order's table (|U| <= y since the coefficients
@@ -384,6 +384,18 @@ int zeb_match_bf16(const void* x_panel, int n_exp, const void* d_panel, int n_di
 int zeb_match_f32(const float* x, int n_exp, const float* d, int n_dict, int cols, int slices, float* cand_v,
                   int* cand_i, void* stream);
 
+/* The patterns' coefficients on a PCA's components: out[p][c] = Σ_k x[p][k]·w[c][k] (the batch's
+ * projection of Pca.project, src/pca.zig:159-162; shaders/pca.wgsl project). The BF16 form on the
+ * tcgen05 tensor cores from split panels (zeb_pack_panel_split: each operand x = hi + lo in BF16,
+ * the product hi·hi + hi·lo + lo·hi, near FP32), role 0 for the patterns and 1 for the components
+ * (zeb_panel_split_bytes bytes each); status as zeb_match_bf16. The plain FP32 form from row-major
+ * x [n_exp][cols] and w [k][cols] on the CUDA cores. out is n_exp × k FP32, 16-byte aligned. */
+size_t zeb_panel_split_bytes(int rows, int cols);
+int zeb_pack_panel_split(const float* src, int rows, int cols, int ld, int role, void* panel, void* stream);
+int zeb_project_bf16(const void* x_split, int n_exp, const void* w_split, int k, int cols, float* out, int* status,
+                     void* stream);
+int zeb_project_f32(const float* x, int n_exp, const float* w, int k, int cols, float* out, void* stream);
+
 /* Each pattern's n_cand candidate entries scored again in FP32 (x·d over cols; indices outside
  * [0, n_dict) skipped), the best (ties to the lower index) written as a seed: seeds[p] = (dict_q[best] (w, x, y, z), score, best, 0, 0).
  * Replaces Detector.seedDict (src/detector.zig:231-235; shaders/detector.wgsl seed_dict 311-317). */
@@ -402,6 +414,21 @@ int zeb_mask_list(const zeb_frame_t* fr, uint32_t* list, void* stream);
 int zeb_refine_list(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
                     const zeb_frame_t* fr, const uint32_t* list, int npix, const float* vpair, const float* gpair,
                     int side, const zeb_refine_opts_t* o, float* records, void* stream);
+
+/* The BF16 form's refinement table: for every texel of the [2][side][side] sheets its 2 × 2
+ * neighbourhood (the texel, the one right of it, the one below, the one below right) in one
+ * 32-byte record of FP16 values — the four masters, then the four tangent gradients (xyz) —
+ * from the gradient table grad4 of zeb_master_gradient (quads: 32 × 2·side² bytes, 32-byte
+ * aligned). No counterpart in the reference (its lookups read the four texels in FP32). */
+int zeb_master_quads(const float* grad4, int side, void* quads, void* stream);
+
+/* zeb_refine_list with every lookup of the Gauss–Newton passes from the FP16 records of
+ * zeb_master_quads (one 32-byte record a pixel instead of two; the weights and every sum in
+ * FP32; the NMI from vpair in FP32 as before). The same records as zeb_refine_list to FP16's
+ * rounding of the master's values and gradients. */
+int zeb_refine_list_h(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
+                      const zeb_frame_t* fr, const uint32_t* list, int npix, const float* vpair, const void* quads,
+                      int side, const zeb_refine_opts_t* o, float* records, void* stream);
 
 /* Simulated patterns: the master at q·ray for every pixel of item b (poses[b] = t.xyz, pattern
  * index, q.wxyz): sims[b][h][w]. Replaces Detector.project (src/detector.zig:138-142;

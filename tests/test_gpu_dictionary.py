@@ -227,3 +227,37 @@ def test_sweeps_mix_methods(world):
     sw = r["sweep"].ravel()
     dis = np.degrees(s.disorientation(r["quaternions"].reshape(-1, 4), world["q"]))
     assert (sw >= 0).all() and np.median(dis) < 0.15 and dis.max() < 1.0, (sw, np.median(dis), dis.max())
+
+
+@pytest.mark.parametrize("n,k,cols", [(300, 256, 3600), (130, 200, 3500), (1, 512, 6400)])
+def test_pca_projection_kernels_match_fp64(n, k, cols):
+    """The batch's projection onto the components (pca.zig:159-162): the tcgen05 form from split
+    BF16 panels (hi·hi + hi·lo + lo·hi) and the plain FP32 form against FP64, ragged in patterns,
+    components and pixels; unit-norm rows, so every coefficient is at most 1 in size."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import ctypes
+
+    from zebsdsolve_b200 import _native as N
+
+    g = torch.Generator(device="cuda").manual_seed(n + k)
+    x = torch.randn(n, cols, generator=g, device="cuda")
+    x /= x.norm(dim=1, keepdim=True)
+    w = torch.randn(k, cols, generator=g, device="cuda")
+    w /= w.norm(dim=1, keepdim=True)
+    want = (x.double() @ w.double().T).cpu().numpy()
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    xs = torch.empty(N.load().zeb_panel_split_bytes(n, cols), dtype=torch.uint8, device="cuda")
+    ws = torch.empty(N.load().zeb_panel_split_bytes(k, cols), dtype=torch.uint8, device="cuda")
+    N.call("zeb_pack_panel_split", P(x), n, cols, cols, 0, P(xs), sp)
+    N.call("zeb_pack_panel_split", P(w), k, cols, cols, 1, P(ws), sp)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    got = torch.full((n, k), float("nan"), device="cuda")
+    N.call("zeb_project_bf16", P(xs), n, P(ws), k, cols, P(got), P(status), sp)
+    got32 = torch.full((n, k), float("nan"), device="cuda")
+    N.call("zeb_project_f32", P(x), n, P(w), k, cols, P(got32), sp)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    assert np.abs(got.cpu().numpy() - want).max() < 2e-5
+    assert np.abs(got32.cpu().numpy() - want).max() < 2e-6

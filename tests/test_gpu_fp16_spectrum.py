@@ -73,11 +73,11 @@ def test_fp16_spectrum_and_tensor_core_peaks(L, group, side, lmax, n):
     torch.cuda.synchronize()
     assert int(status.item()) == 0
 
-    # U16[j][c][item tile][m'][re|im][item % 128] / s against U[item][j][m'][c] (re, im)
+    # U16[item tile][j][c][m'][re|im][item % 128] / s against U[item][j][m'][c] (re, im)
     Ln, nb, nc = dims.L, dims.nb, dims.nc
     pt = (n + 127) // 128
-    h = U16.view(torch.float16)[: nb * nc * pt * Ln * 2 * 128].view(nb, nc, pt, Ln, 2, 128)
-    h = h.permute(0, 1, 3, 4, 2, 5).reshape(nb, nc, Ln, 2, pt * 128)[..., :n].float() / ph.u_scale
+    h = U16.view(torch.float16)[: pt * nb * nc * Ln * 2 * 128].view(pt, nb, nc, Ln, 2, 128)
+    h = h.permute(1, 2, 3, 4, 0, 5).reshape(nb, nc, Ln, 2, pt * 128)[..., :n].float() / ph.u_scale
     u = U[: n * nb * Ln * nc * 2].view(n, nb, Ln, nc, 2).permute(1, 3, 2, 4, 0)  # → [j][c][m'][ri][item]
     top = float(u.abs().max())
     assert top * ph.u_scale <= 16384 * 1.001  # the scale's bound holds

@@ -426,10 +426,11 @@ def test_records_fz_equals_the_host_reduction(lib, kind):
     assert np.array_equal(fz.cpu().numpy().reshape(-1, 4), want)
 
 
-@pytest.mark.parametrize("entry", ["zeb_refine", "zeb_refine_list"])
+@pytest.mark.parametrize("entry", ["zeb_refine", "zeb_refine_list", "zeb_refine_list_h"])
 def test_refine_and_nmi_match_oracle(world, lib, entry):
-    """Both refinement kernels (pixels compacted per block; the frame's shared pixel list, 128
-    threads an item) against the oracle's refinement and NMI."""
+    """The refinement kernels (pixels compacted per block; the frame's shared pixel list, 128
+    threads an item; the same with the BF16 form's FP16 neighbourhood records) against the
+    oracle's refinement and NMI, at the same bounds."""
     s = world["s"]
     e = s._e
     e.prepare_masters()
@@ -459,8 +460,9 @@ def test_refine_and_nmi_match_oracle(world, lib, entry):
         lib.call("zeb_mask_list", ctypes.byref(fr), P(lst), sp())
         rr, cc = np.nonzero(od.in_mask(fr.h, fr.w, mask))  # raster order
         assert np.array_equal(lst.cpu().numpy(), (rr << 16) | cc)
-        lib.call("zeb_refine_list", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(lst), npix, P(p.baked[3]),
-                 P(p.baked[4]), p.master.side, ctypes.byref(opts), P(recs), sp())
+        table = p.baked[4] if entry == "zeb_refine_list" else p.quads[p.baked[0]]
+        lib.call(entry, P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(lst), npix, P(p.baked[3]), P(table),
+                 p.master.side, ctypes.byref(opts), P(recs), sp())
     got = recs.cpu().numpy().reshape(n, 8)
     grad = od.gradient_table(world["baked"], 151)
     frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))

@@ -5,6 +5,7 @@
 // sample directions to crystal directions.  A master pattern is two side × side equal-area
 // Lambert sheets [north | south].
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -184,6 +185,32 @@ __device__ __forceinline__ float4 grad_at_pair(const float* __restrict__ gp, flo
   ldg_v8(gp + 8 * (size_t)p.o, a, b);
   ldg_v8(gp + 8 * ((size_t)p.o + side), c, d);
   return lerp4(lerp4(a, b, p.tj), lerp4(c, d, p.tj), p.ti);
+}
+
+// two floats rounded to FP16 in one word (the first in the low half), and back
+__device__ __forceinline__ uint32_t zeb_half2(float lo, float hi) {
+  const __half2 h = __floats2half2_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ float2 zeb_unhalf2(uint32_t w) {
+  return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+
+// The same lookup from the FP16 neighbourhood records (zeb_master_quads): one 32-byte record a
+// pixel; the bilinear weights and every sum in FP32.
+__device__ __forceinline__ float4 grad_at_quad(const float* __restrict__ gq, float3 v, int side) {
+  SheetPos p = sheet_pos(v, side);
+  uint32_t h[8];
+  asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(h[0]), "=r"(h[1]), "=r"(h[2]), "=r"(h[3]), "=r"(h[4]), "=r"(h[5]), "=r"(h[6]), "=r"(h[7])
+      : "l"(gq + 8 * (size_t)p.o));
+  const float2 m01 = zeb_unhalf2(h[0]), m23 = zeb_unhalf2(h[1]);
+  const float2 a = zeb_unhalf2(h[2]), b = zeb_unhalf2(h[3]), c = zeb_unhalf2(h[4]);
+  const float2 d = zeb_unhalf2(h[5]), e = zeb_unhalf2(h[6]), f = zeb_unhalf2(h[7]);
+  // texels 0 (a.x a.y b.x), 1 (b.y c.x c.y), 2 (d.x d.y e.x), 3 (e.y f.x f.y)
+  const float4 t0 = make_float4(a.x, a.y, b.x, m01.x), t1 = make_float4(b.y, c.x, c.y, m01.y);
+  const float4 t2 = make_float4(d.x, d.y, e.x, m23.x), t3 = make_float4(e.y, f.x, f.y, m23.y);
+  return lerp4(lerp4(t0, t1, p.tj), lerp4(t2, t3, p.tj), p.ti);
 }
 
 __device__ __forceinline__ float master_at_pair(const float2* __restrict__ vp, float3 v, int side) {

@@ -608,6 +608,8 @@ __device__ float nmi_list(const DetArgs& a, const uint32_t* __restrict__ list, c
   return h_marg > 1e-12f ? 2.f * (h_marg - h_joint) / h_marg : 0.f;
 }
 
+// QUAD: the lookups from the FP16 neighbourhood records (a.gpair holds zeb_master_quads' table)
+template <bool QUAD>
 __global__ void __launch_bounds__(RL_THREADS, 6) k_refine_list(DetArgs a, const uint32_t* __restrict__ list,
                                                                  int npix) {
   extern __shared__ float pv[];  // [npix] pattern values, then [npix] simulated values (NMI)
@@ -640,7 +642,7 @@ __global__ void __launch_bounds__(RL_THREADS, 6) k_refine_list(DetArgs a, const 
 #pragma unroll 4
     for (int k = threadIdx.x; k < npix; k += RL_THREADS) {
       const float3 c = qrot(q, list_ray(a, t, __ldg(list + k)));
-      const float4 m = grad_at_pair(a.gpair, c, a.side);
+      const float4 m = QUAD ? grad_at_quad(a.gpair, c, a.side) : grad_at_pair(a.gpair, c, a.side);
       const float3 d = cross3(c, make_float3(m.x, m.y, m.z));
       const float e = pv[k];
       s[1] += m.w; s[2] += m.w * m.w; s[3] += m.w * e;
@@ -771,9 +773,37 @@ extern "C" int zeb_refine_list(const float* pats, const float* items, const floa
   ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine_list: bad frame");
   a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
   a.vpair = (const float2*)vpair; a.gpair = gpair; a.side = side; a.o = *o; a.records = records;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_refine_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_refine_list<<<n, RL_THREADS, smem, (cudaStream_t)stream>>>(a, list, npix);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_refine_list<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_refine_list<false><<<n, RL_THREADS, smem, (cudaStream_t)stream>>>(a, list, npix);
   return zeb_launch_check("refine_list");
+}
+
+extern "C" int zeb_refine_list_h(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
+                                 const zeb_frame_t* fr, const uint32_t* list, int npix, const float* vpair,
+                                 const void* quads, int side, const zeb_refine_opts_t* o, float* records,
+                                 void* stream) {
+  ZEB_REQUIRE(pats && items && seeds && list && vpair && quads && o && records, ZEB_EARG,
+              "refine_list_h: null argument");
+  ZEB_REQUIRE(((uintptr_t)quads & 31) == 0 && ((uintptr_t)vpair & 7) == 0, ZEB_EARG,
+              "refine_list_h: tables misaligned");
+  ZEB_REQUIRE(seed_stride >= 4 && side >= 3 && o->iters >= 0 && o->iters <= 1000 && o->nmi_bins >= 2 &&
+                  o->nmi_bins <= 32,
+              ZEB_EARG, "refine_list_h: bad arguments");
+  ZEB_REQUIRE(fr && npix == zeb_mask_count(fr), ZEB_EARG, "refine_list_h: %d pixels listed, the frame masks %d", npix,
+              fr ? zeb_mask_count(fr) : -1);
+  const size_t smem = (size_t)npix * 2 * sizeof(float);
+  ZEB_REQUIRE(npix >= 1 && smem <= DET_LIST_SMEM, ZEB_ESIZE, "refine_list_h: %d pixels (at most %zu)", npix,
+              DET_LIST_SMEM / 8);
+  if (n <= 0) return ZEB_OK;
+  DetArgs a{};
+  ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine_list_h: bad frame");
+  a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
+  a.vpair = (const float2*)vpair; a.gpair = (const float*)quads; a.side = side; a.o = *o; a.records = records;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_refine_list<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_refine_list<true><<<n, RL_THREADS, smem, (cudaStream_t)stream>>>(a, list, npix);
+  return zeb_launch_check("refine_list_h");
 }
 
 extern "C" int zeb_chance(const float* pats, const float* items, int n, int draws, const zeb_frame_t* fr,

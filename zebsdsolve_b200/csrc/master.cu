@@ -140,6 +140,39 @@ extern "C" int zeb_master_pairs(const float* sheets, const float* grad4, int sid
   return zeb_launch_check("master_pairs");
 }
 
+// The 2 × 2 neighbourhood of every texel in one 32-byte record of FP16 values: the master at the
+// texel, its right-hand neighbour, the one below and the one below right, then their tangent
+// gradients (xyz each) in the same order. A texel on the last row or column repeats itself where a
+// neighbour would fall off the sheet (the lookups never start there).
+__global__ void k_master_quads(const float4* __restrict__ grad4, int side, uint4* __restrict__ quads) {
+  const long long total = 2LL * side * side;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int c = (int)(i % side), r = (int)((i / side) % side);
+  const long long right = c + 1 < side ? 1 : 0, down = r + 1 < side ? side : 0;
+  const float4 g[4] = {grad4[i], grad4[i + right], grad4[i + down], grad4[i + down + right]};
+  uint32_t h[8];
+  h[0] = zeb_half2(g[0].w, g[1].w);
+  h[1] = zeb_half2(g[2].w, g[3].w);
+  h[2] = zeb_half2(g[0].x, g[0].y);
+  h[3] = zeb_half2(g[0].z, g[1].x);
+  h[4] = zeb_half2(g[1].y, g[1].z);
+  h[5] = zeb_half2(g[2].x, g[2].y);
+  h[6] = zeb_half2(g[2].z, g[3].x);
+  h[7] = zeb_half2(g[3].y, g[3].z);
+  quads[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
+  quads[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+extern "C" int zeb_master_quads(const float* grad4, int side, void* quads, void* stream) {
+  ZEB_REQUIRE(grad4 && quads && side >= 3, ZEB_EARG, "master_quads: bad arguments side=%d", side);
+  ZEB_REQUIRE(((uintptr_t)quads & 31) == 0, ZEB_EARG, "master_quads: quads must be 32-byte aligned");
+  const long long total = 2LL * side * side;
+  k_master_quads<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>((const float4*)grad4, side,
+                                                                                  (uint4*)quads);
+  return zeb_launch_check("master_quads");
+}
+
 extern "C" int zeb_master_sample_grid(const float* sheets, int side, const double* x, int n_theta, int n_phi,
                                       double* out, void* stream) {
   ZEB_REQUIRE(sheets && x && out && side >= 2 && n_theta >= 1 && n_phi >= 1, ZEB_EARG,

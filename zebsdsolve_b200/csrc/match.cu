@@ -120,6 +120,37 @@ __global__ void k_pack_panel(const float* __restrict__ src, int rows, int cols, 
   *(uint4*)(dst + (size_t)kb * rows_pad * 128 + sw128(row, c16 * 8)) = wv;
 }
 
+// The panel of FP32 rows as three K segments of BF16 for a near-FP32 product on the tensor cores:
+// x = hi + lo with hi = bf16(x), lo = bf16(x − hi); segment order (hi, hi, lo) for the left
+// operand (role 0) and (hi, lo, hi) for the right one (role 1), so that the one GEMM over the
+// three segments sums hi·hi + hi·lo + lo·hi.
+__global__ void k_pack_panel_split(const float* __restrict__ src, int rows, int cols, int ld, int rows_pad,
+                                   int kblocks, int role, uint8_t* __restrict__ dst) {
+  const long long chunks = 3LL * kblocks * rows_pad * 8;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= chunks) return;
+  const int c16 = (int)(e & 7);
+  const int row = (int)((e >> 3) % rows_pad);
+  const int kbs = (int)((e >> 3) / rows_pad);  // K-block of the whole panel
+  const int seg = kbs / kblocks, kb = kbs - seg * kblocks;
+  const bool lo = role == 0 ? seg == 2 : seg == 1;
+  const int k0 = kb * 64 + c16 * 8;
+  uint16_t v[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int k = k0 + i;
+    const float x = row < rows && k < cols ? __ldg(src + (size_t)row * ld + k) : 0.f;
+    const float hi = bf16_value(bf16_bits(x));
+    v[i] = bf16_bits(lo ? x - hi : x);
+  }
+  uint4 wv;
+  wv.x = v[0] | ((uint32_t)v[1] << 16);
+  wv.y = v[2] | ((uint32_t)v[3] << 16);
+  wv.z = v[4] | ((uint32_t)v[5] << 16);
+  wv.w = v[6] | ((uint32_t)v[7] << 16);
+  *(uint4*)(dst + (size_t)kbs * rows_pad * 128 + sw128(row, c16 * 8)) = wv;
+}
+
 // ── top eight on the tensor cores ──
 
 struct MatchArgs {
@@ -134,6 +165,7 @@ struct MatchArgs {
   int* status;
   long long limit;
   long long stall;  // > 0: the failure test (the MMA thread first waits on `never`)
+  float* out;       // PROJECT: the products themselves, out[p][entry] (n_exp × n_dict)
 };
 
 struct MatchShared {
@@ -177,6 +209,9 @@ __device__ __forceinline__ void top8_push(float (&v)[MT_TOP], int (&id)[MT_TOP],
   id[0] = gt[0] ? i : id[0];
 }
 
+// PROJECT: the epilogue writes every product (the patterns' coefficients on the components of a
+// PCA, zeb_project_bf16) instead of keeping each pattern's eight best
+template <bool PROJECT>
 __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
   extern __shared__ __align__(1024) uint8_t mt_smem_raw[];
   MatchShared& s = *reinterpret_cast<MatchShared*>((void*)(((uintptr_t)mt_smem_raw + 1023) & ~(uintptr_t)1023));
@@ -307,6 +342,37 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int e0 = (nt0 + t) * MT_BN + half * 128;
       const uint32_t c0 = tmem + lanes + (uint32_t)(acc * MT_BN + half * 128);
+      if constexpr (PROJECT) {
+        // four chunks of 32 columns, each stored as it is read (the row's entries past n_dict and
+        // the rows past n_exp not at all)
+        const int p = mt * MT_BM + row;
+        float* orow = a.out + (size_t)p * a.n_dict;
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+          uint32_t v[32];
+          TMEM_LD32(c0 + 32 * q, v);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (q == 3) {  // the accumulator is read out: the MMAs of tile t + 2 may start
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&s.acc_empty[acc]);
+          }
+          const int eq = e0 + 32 * q;
+          if (p < a.n_exp) {
+            if (eq + 32 <= a.n_dict && (a.n_dict & 3) == 0) {
+#pragma unroll
+              for (int c = 0; c < 32; c += 4)
+                *(float4*)(orow + eq + c) = make_float4(__uint_as_float(v[c]), __uint_as_float(v[c + 1]),
+                                                        __uint_as_float(v[c + 2]), __uint_as_float(v[c + 3]));
+            } else {
+#pragma unroll
+              for (int c = 0; c < 32; ++c)
+                if (eq + c < a.n_dict) orow[eq + c] = __uint_as_float(v[c]);
+            }
+          }
+        }
+        continue;
+      }
       // four chunks of 32 columns, the next one's load in flight while one is taken
       uint32_t va[32], vb[32];
       TMEM_LD32(c0, va);
@@ -327,25 +393,28 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
       take(vb, e0 + 96);
     }
     // the second half's list joins the first's (through the stash, once every thread is done)
-    bar_sync(1, 32 * MT_EPI);
-    if (half == 1) {
-#pragma unroll
-      for (int k = 0; k < MT_TOP; ++k) {
-        s.stash[k][row] = tv[k];
-        s.stash[MT_TOP + k][row] = __int_as_float(ti[k]);
-      }
-    }
-    bar_sync(1, 32 * MT_EPI);
-    const int p = mt * MT_BM + row;
-    if (half == 0) {
-#pragma unroll 1
-      for (int k = 0; k < MT_TOP; ++k) top8_insert(tv, ti, s.stash[k][row], __float_as_int(s.stash[MT_TOP + k][row]));
-      if (ok && p < a.n_exp) {
-        const size_t o = ((size_t)p * a.slices + slice) * MT_TOP;
+    if constexpr (!PROJECT) {
+      bar_sync(1, 32 * MT_EPI);
+      if (half == 1) {
 #pragma unroll
         for (int k = 0; k < MT_TOP; ++k) {
-          a.cand_v[o + k] = tv[k];
-          a.cand_i[o + k] = ti[k];
+          s.stash[k][row] = tv[k];
+          s.stash[MT_TOP + k][row] = __int_as_float(ti[k]);
+        }
+      }
+      bar_sync(1, 32 * MT_EPI);
+      const int p = mt * MT_BM + row;
+      if (half == 0) {
+#pragma unroll 1
+        for (int k = 0; k < MT_TOP; ++k)
+          top8_insert(tv, ti, s.stash[k][row], __float_as_int(s.stash[MT_TOP + k][row]));
+        if (ok && p < a.n_exp) {
+          const size_t o = ((size_t)p * a.slices + slice) * MT_TOP;
+#pragma unroll
+          for (int k = 0; k < MT_TOP; ++k) {
+            a.cand_v[o + k] = tv[k];
+            a.cand_i[o + k] = ti[k];
+          }
         }
       }
     }
@@ -362,9 +431,12 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_match_tc(MatchArgs a) {
 // thread; after each tile every pattern's best of its 128 entries joins its running best.
 constexpr int MF_BM = 64, MF_BN = 128, MF_BK = 16;
 
+// PROJECT: every product is written to out[p][entry] (the coefficients of a PCA projection,
+// zeb_project_f32) instead of each pattern's best
+template <bool PROJECT>
 __global__ void __launch_bounds__(256) k_match_f32(const float* __restrict__ x, int n_exp, const float* __restrict__ d,
                                                    int n_dict, int cols, int per, int slices, float* cand_v,
-                                                   int* cand_i) {
+                                                   int* cand_i, float* out = nullptr) {
   __shared__ float xs[MF_BK][MF_BM + 4];
   __shared__ float ds[MF_BK][MF_BN + 4];
   const int tid = threadIdx.x;
@@ -411,6 +483,18 @@ __global__ void __launch_bounds__(256) k_match_f32(const float* __restrict__ x, 
       }
       __syncthreads();
     }
+    if constexpr (PROJECT) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int p = p0 + ty * 4 + i;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int e = e0 + tx * 8 + j;
+          if (p < n_exp && e < n_dict) out[(size_t)p * n_dict + e] = acc[i][j];
+        }
+      }
+      continue;
+    }
     // each pattern's best of this tile: over the thread's 8 entries, then across the 16 threads
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -430,6 +514,7 @@ __global__ void __launch_bounds__(256) k_match_f32(const float* __restrict__ x, 
       if (id >= 0 && v > bv[i]) { bv[i] = v; bi[i] = id; }
     }
   }
+  if (PROJECT) return;
   if (tx == 0) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -567,10 +652,54 @@ extern "C" int zeb_match_bf16(const void* x_panel, int n_exp, const void* d_pane
   // every candidate reads as "none" until the kernel writes it (a CTA that gave up writes nothing)
   cudaMemsetAsync(cand_i, 0xFF, (size_t)n_exp * slices * MT_TOP * sizeof(int), (cudaStream_t)stream);
   const size_t smem = sizeof(MatchShared) + 1024;
-  cudaFuncSetAttribute(k_match_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_match_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 g((n_exp + MT_BM - 1) / MT_BM, slices);
-  k_match_tc<<<g, MT_THREADS, smem, (cudaStream_t)stream>>>(a);
+  k_match_tc<false><<<g, MT_THREADS, smem, (cudaStream_t)stream>>>(a);
   return zeb_launch_check("match_bf16");
+}
+
+extern "C" size_t zeb_panel_split_bytes(int rows, int cols) {
+  if (rows <= 0 || cols <= 0) return 0;
+  return 3 * (size_t)panel_kblocks(cols) * panel_rows(rows) * 128;
+}
+
+extern "C" int zeb_pack_panel_split(const float* src, int rows, int cols, int ld, int role, void* panel, void* stream) {
+  ZEB_REQUIRE(src && panel && rows > 0 && cols > 0 && ld >= cols && (role == 0 || role == 1), ZEB_EARG,
+              "pack_panel_split: bad arguments");
+  ZEB_REQUIRE(((uintptr_t)panel & 127) == 0, ZEB_EARG, "pack_panel_split: panel must be 128-byte aligned");
+  const int rp = panel_rows(rows), kb = panel_kblocks(cols);
+  const long long chunks = 3LL * kb * rp * 8;
+  k_pack_panel_split<<<(unsigned)((chunks + 255) / 256), 256, 0, (cudaStream_t)stream>>>(src, rows, cols, ld, rp, kb,
+                                                                                        role, (uint8_t*)panel);
+  return zeb_launch_check("pack_panel_split");
+}
+
+extern "C" int zeb_project_bf16(const void* x_split, int n_exp, const void* w_split, int k, int cols, float* out,
+                                int* status, void* stream) {
+  ZEB_REQUIRE(x_split && w_split && out && status && cols > 0 && k > 0, ZEB_EARG, "project_bf16: bad arguments");
+  ZEB_REQUIRE(((uintptr_t)x_split & 127) == 0 && ((uintptr_t)w_split & 127) == 0 && ((uintptr_t)out & 15) == 0,
+              ZEB_EARG, "project_bf16: panels must be 128-byte and out 16-byte aligned");
+  if (n_exp <= 0) return ZEB_OK;
+  const int ntiles = (k + MT_BN - 1) / MT_BN;
+  MatchArgs a{};
+  a.A = (const uint8_t*)x_split;
+  a.B = (const uint8_t*)w_split;
+  a.rows_a = panel_rows(n_exp);
+  a.rows_b = panel_rows(k);
+  a.kb = 3 * panel_kblocks(cols);  // the three segments: hi·hi + hi·lo + lo·hi
+  a.n_exp = n_exp;
+  a.n_dict = k;
+  a.per = 1;  // a CTA per (pattern tile, tile of components)
+  a.slices = ntiles;
+  a.out = out;
+  a.status = status;
+  a.stall = test_stall_ns();
+  a.limit = a.stall > 0 ? a.stall : kWaitNs;
+  const size_t smem = sizeof(MatchShared) + 1024;
+  cudaFuncSetAttribute(k_match_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 g((n_exp + MT_BM - 1) / MT_BM, ntiles);
+  k_match_tc<true><<<g, MT_THREADS, smem, (cudaStream_t)stream>>>(a);
+  return zeb_launch_check("project_bf16");
 }
 
 extern "C" int zeb_match_f32(const float* x, int n_exp, const float* d, int n_dict, int cols, int slices,
@@ -581,8 +710,17 @@ extern "C" int zeb_match_f32(const float* x, int n_exp, const float* d, int n_di
   ZEB_REQUIRE(slices >= 1 && slices <= ntiles, ZEB_EARG, "match_f32: %d slices of %d dictionary tiles", slices, ntiles);
   const int per = (ntiles + slices - 1) / slices;
   dim3 g((n_exp + MF_BM - 1) / MF_BM, slices);
-  k_match_f32<<<g, 256, 0, (cudaStream_t)stream>>>(x, n_exp, d, n_dict, cols, per, slices, cand_v, cand_i);
+  k_match_f32<false><<<g, 256, 0, (cudaStream_t)stream>>>(x, n_exp, d, n_dict, cols, per, slices, cand_v, cand_i);
   return zeb_launch_check("match_f32");
+}
+
+extern "C" int zeb_project_f32(const float* x, int n_exp, const float* w, int k, int cols, float* out, void* stream) {
+  ZEB_REQUIRE(x && w && out && cols > 0 && k > 0, ZEB_EARG, "project_f32: bad arguments");
+  if (n_exp <= 0) return ZEB_OK;
+  const int ntiles = (k + MF_BN - 1) / MF_BN;
+  dim3 g((n_exp + MF_BM - 1) / MF_BM, ntiles);
+  k_match_f32<true><<<g, 256, 0, (cudaStream_t)stream>>>(x, n_exp, w, k, cols, 1, ntiles, nullptr, nullptr, out);
+  return zeb_launch_check("project_f32");
 }
 
 extern "C" int zeb_match_best(const float* x, int n_exp, const float* d, int n_dict, int cols, const int* cand,

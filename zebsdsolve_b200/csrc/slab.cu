@@ -316,12 +316,12 @@ struct UReader32 {  // FP32, [item][j][m'][c]
     return __ldg(U + (((size_t)b * d.nb + j) * d.L + mp) * d.nc + c);
   }
 };
-struct UReader16 {  // s·U in FP16, [(j, c)][item tile][m'][re|im][128 items]
+struct UReader16 {  // s·U in FP16, [item tile][(j, c)][m'][re|im][128 items]
   const __half* U;
   size_t ptiles;
   float inv;  // 1/s
   __device__ __forceinline__ float2 operator()(int b, int j, int mp, int c, const zeb_so3_dims_t& d) const {
-    const size_t o = ((((size_t)(j * d.nc + c) * ptiles + (b >> 7)) * d.L + mp) * 2) * 128 + (b & 127);
+    const size_t o = (((((size_t)(b >> 7) * d.nb + j) * d.nc + c) * d.L + mp) * 2) * 128 + (b & 127);
     return make_float2(__half2float(U[o]) * inv, __half2float(U[o + 128]) * inv);
   }
 };

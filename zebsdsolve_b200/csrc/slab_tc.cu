@@ -2,7 +2,7 @@
 // tensor cores, over the spectrum kept in FP16.
 //
 // U (transformed along b and c by the spectrum GEMM) arrives as s·U in FP16, laid out
-// [(j, c)][item tile][m'][re|im][128 items] (k_spectrum_tc<true>).  For one (j, c) the real transform
+// [item tile][(j, c)][m'][re|im][128 items] (k_spectrum_tc<true>).  For one (j, c) the real transform
 // along a (so3.wgsl:279-315, 396-593),
 //
 //   C(a) = Re V[0] + 2 Re Σ_{m'>0} V[m'] e^{−2πi m' a/n} = Σ_κ V_κ F[a][κ],  κ = 2m' + (re|im),
@@ -137,8 +137,8 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
           }
           mbar_expect_tx(&s.full[st], tile_bytes);
           // the 2L × 256 contiguous bytes of (j, c) and this tile, as two halves of 64 items
-          tma_load_5d(&umap, s.a[st][0], &s.full[st], 0, 0, 0, pt, j * nc + c);
-          tma_load_5d(&umap, s.a[st][1], &s.full[st], 64, 0, 0, pt, j * nc + c);
+          tma_load_5d(&umap, s.a[st][0], &s.full[st], 0, 0, 0, j * nc + c, pt);
+          tma_load_5d(&umap, s.a[st][1], &s.full[st], 64, 0, 0, j * nc + c, pt);
           // and the tile's row of rden, for the epilogue
           const int rs = (int)(it % ST_RSLOTS);
           if (!mbar_wait(&s.rempty[rs], (uint32_t)((it / ST_RSLOTS) & 1) ^ 1u, lim)) {
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(ST_THREADS, 1) k_slab_tc(SlabTcArgs a, const _
 
 using namespace zeb;
 
-// U16 as the 5-D tensor (items within the tile, re|im, order, tile, (j, c)); boxes of 64 items × re|im
+// U16 as the 5-D tensor (items within the tile, re|im, order, (j, c), tile); boxes of 64 items × re|im
 // × every order of one (j, c) and one tile, landing as [order][re|im][64 items] with the 128-byte
 // swizzle
 static bool st_u16_map(CUtensorMap* m, const void* U16, const zeb_so3_dims_t* d, int n_items) {
@@ -312,9 +312,9 @@ static bool st_u16_map(CUtensorMap* m, const void* U16, const zeb_so3_dims_t* d,
   }
   if (!fn) return false;
   const cuuint64_t ptiles = (cuuint64_t)((n_items + ST_BM - 1) / ST_BM);
-  const cuuint64_t L = (cuuint64_t)d->L;
-  cuuint64_t dims[5] = {ST_BM, 2, L, ptiles, (cuuint64_t)d->nb * d->nc};
-  cuuint64_t strides[4] = {ST_BM * 2, ST_BM * 4, ST_BM * 4 * L, ST_BM * 4 * L * ptiles};
+  const cuuint64_t L = (cuuint64_t)d->L, jc = (cuuint64_t)d->nb * d->nc;
+  cuuint64_t dims[5] = {ST_BM, 2, L, jc, ptiles};
+  cuuint64_t strides[4] = {ST_BM * 2, ST_BM * 4, ST_BM * 4 * L, ST_BM * 4 * L * jc};
   cuuint32_t box[5] = {64, 2, (cuuint32_t)d->L, 1, 1};
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 5, const_cast<void*>(U16), dims, strides, box, es,

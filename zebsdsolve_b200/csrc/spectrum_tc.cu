@@ -191,7 +191,7 @@ struct TcShared {
 };
 
 // HALF = false: U in FP32 as [item][j][m'][c] (re, im); true: scale·U in FP16 as
-// [(j, c)][item tile][m'][re|im][128 items] (items padded to whole tiles of 128), the layout the
+// [item tile][(j, c)][m'][re|im][128 items] (items padded to whole tiles of 128), the layout the
 // tensor-core transform along a (slab_tc.cu) loads its operand tiles from.
 template <bool HALF>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const __grid_constant__ CUtensorMap umap) {
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
           fence_proxy_async();
           bar_sync(1, 128);
           if (leader) {
-            if (ptile * TC_BN + c0 < a.n_items) tma_store_5d(&umap, stg, c0, 0, mp, ptile, r0 >> 1);
+            if (ptile * TC_BN + c0 < a.n_items) tma_store_5d(&umap, stg, c0, 0, mp, r0 >> 1, ptile);
             bulk_commit();
           }
         }
@@ -517,19 +517,20 @@ extern "C" int zeb_spectrum_bf16(const float* alm, int n_items, const zeb_so3_di
   return zeb_launch_check("spectrum_bf16");
 }
 
-// scale·U in FP16 as [(j, c)][item tile][m'][re|im][128 items]: a 5-D tensor (items within the tile,
-// re|im, order, tile, (j, c)); a store box is 64 items × the 128 rows ν = 2(j·nc + c) + (re|im) of
-// a row tile (64 (j, c) × re|im) of one order and one tile, with the staging buffer's 128-byte
+// scale·U in FP16 as [item tile][(j, c)][m'][re|im][128 items]: a 5-D tensor (items within the tile,
+// re|im, order, (j, c), tile); a store box is 64 items × the 128 rows ν = 2(j·nc + c) + (re|im) of a
+// row tile (64 (j, c) × re|im) of one order and one tile, with the staging buffer's 128-byte
 // swizzle. One (j, c) of one tile of items is then 2L × 256 contiguous bytes: what the transform
-// along a loads as one operand tile.
+// along a loads as one operand tile; and a CTA's stores (one tile, one order) stay within the
+// tile's region of 2L × 256 bytes × (j, c).
 static bool tc_u16_map(CUtensorMap* m, void* U16, const zeb_so3_dims_t* d, int n_items) {
   auto fn = tc_encode_fn();
   if (!fn) return false;
   const cuuint64_t ptiles = (cuuint64_t)((n_items + TC_BN - 1) / TC_BN);
-  const cuuint64_t L = (cuuint64_t)d->L;
-  cuuint64_t dims[5] = {TC_BN, 2, L, ptiles, (cuuint64_t)d->nb * d->nc};
-  cuuint64_t strides[4] = {TC_BN * 2, TC_BN * 4, TC_BN * 4 * L, TC_BN * 4 * L * ptiles};
-  cuuint32_t box[5] = {64, 2, 1, 1, (cuuint32_t)TC_BM / 2};
+  const cuuint64_t L = (cuuint64_t)d->L, jc = (cuuint64_t)d->nb * d->nc;
+  cuuint64_t dims[5] = {TC_BN, 2, L, jc, ptiles};
+  cuuint64_t strides[4] = {TC_BN * 2, TC_BN * 4, TC_BN * 4 * L, TC_BN * 4 * L * jc};
+  cuuint32_t box[5] = {64, 2, 1, (cuuint32_t)TC_BM / 2, 1};
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 5, U16, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==

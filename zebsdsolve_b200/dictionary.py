@@ -214,6 +214,7 @@ class Dictionary:
         self.rows = None     # FP32 rows the patterns are scored against: sims [n][h·w] or coefficients [n][k]
         self.panel = None    # their BF16 panel (tensor-core forms)
         self.W = None        # PCA components [k][h·w]
+        self.w_split = None  # the components as a split BF16 panel (the BF16 form's projection)
         self.kept = None
 
     def chunk(self, px):
@@ -226,7 +227,7 @@ class Dictionary:
         step = max(1, (1 << 30) // (px * 4))
         for d0 in range(0, self.n, step):
             simulate(fr, vpair, side, t0, self.q[d0:d0 + step], rows[d0:d0 + step])
-        self.rows, self.W = rows, None
+        self.rows, self.W, self.w_split = rows, None, None
 
     def prepare_pca(self, fr, vpair, side, t0, k, epochs, log=None):
         """engine.zig:1905-1955 — components by Oja's rule over `epochs` passes (steps of chunk()
@@ -256,10 +257,29 @@ class Dictionary:
             torch.mm(x, W.T, out=coef[d0:d0 + nb])
         head = coef[: min(self.n, 2048)]
         self.kept = float((head.double() ** 2).sum() / head.shape[0])
-        self.rows, self.W = coef, W
+        self.rows, self.W, self.w_split = coef, W, None
         if log:
             log(f"dictionary components: {k} of {px} pixels hold {100 * self.kept:.1f} % of {self.n} patterns' "
                 f"variance ({taken} steps of Oja's rule)")
+
+    def project(self, x, tensor_cores, status):
+        """pca.zig:159-162 — the batch's coefficients on the components, x [n, h·w] → [n, k]: on the
+        tcgen05 tensor cores from split BF16 panels (near FP32; zeb_project_bf16) or in plain FP32
+        (zeb_project_f32)."""
+        n, px = x.shape
+        x, w = x.contiguous(), self.W.contiguous()
+        k = w.shape[0]
+        out = torch.empty(n, k, dtype=torch.float32, device=x.device)
+        if tensor_cores:
+            if self.w_split is None:
+                self.w_split = torch.empty(N.load().zeb_panel_split_bytes(k, px), dtype=torch.uint8, device=x.device)
+                N.call("zeb_pack_panel_split", ptr(w), k, px, px, 1, ptr(self.w_split), stream_ptr())
+            xs = torch.empty(N.load().zeb_panel_split_bytes(n, px), dtype=torch.uint8, device=x.device)
+            N.call("zeb_pack_panel_split", ptr(x), n, px, px, 0, ptr(xs), stream_ptr())
+            N.call("zeb_project_bf16", ptr(xs), n, ptr(self.w_split), k, px, ptr(out), ptr(status), stream_ptr())
+        else:
+            N.call("zeb_project_f32", ptr(x), n, ptr(w), k, px, ptr(out), stream_ptr())
+        return out
 
     def seeds(self, x, tensor_cores, status, out):
         """The best entry for each row of x [n, K] (patterns or their coefficients) as seeds

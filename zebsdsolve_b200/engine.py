@@ -123,6 +123,7 @@ class Phase:
         self.master = master
         self.baked = None  # (key, sheets, grad4, value pairs, gradient pairs), all on the device
         self.bakes = {}    # the last few of them by smoothing key (detector sizes met before)
+        self.quads = {}    # each bake's FP16 neighbourhood records (zeb_master_quads), by the same key
 
     def info(self, bands):
         m = self.master
@@ -442,9 +443,13 @@ class Engine:
             vpair = torch.empty(sheets.numel() * 2, dtype=torch.float32, device=self.dev)
             gpair = torch.empty(sheets.numel() * 8, dtype=torch.float32, device=self.dev)
             N.call("zeb_master_pairs", ptr(sheets), ptr(grad), m.side, ptr(vpair), ptr(gpair), stream_ptr())
+            # the BF16 form's refinement table: each texel's 2 × 2 neighbourhood in FP16, one record
+            quads = torch.empty(sheets.numel() * 32, dtype=torch.uint8, device=self.dev)
+            N.call("zeb_master_quads", ptr(grad), m.side, ptr(quads), stream_ptr())
+            p.quads[key] = quads
             p.baked = (key, sheets, grad, vpair, gpair)
             if len(p.bakes) >= 8:
-                p.bakes.pop(next(iter(p.bakes)))
+                p.quads.pop(p.bakes.pop(next(iter(p.bakes)))[0], None)
             p.bakes[key] = p.baked
             self.chance_key = None
 
@@ -1032,7 +1037,7 @@ class Engine:
         for pi, p in enumerate(self.phases):
             d = self.dictionary(pi, grid, method)
             mark("match")
-            xs = x @ d.W.T if method == "pca" else x  # the patterns' coefficients (pca.zig:159-162)
+            xs = d.project(x, tc, self.tc_status()) if method == "pca" else x  # their coefficients (pca.zig:159-162)
             peaks = d.seeds(xs.contiguous(), tc, self.tc_status(),
                             self.buf(f"peaks{pi}" if self.stage_full("refine") else "peaks", n * 8))
             self._seeds.append(peaks)
@@ -1059,10 +1064,15 @@ class Engine:
         return lst
 
     def refine(self, pats, items, peaks, n, fr, p, opts, out):
-        """detector.zig:178-202 — every item refined from its seed (peaks, stride 8) and scored."""
-        _, sheets, grad, vpair, gpair = p.baked
+        """detector.zig:178-202 — every item refined from its seed (peaks, stride 8) and scored;
+        in the BF16 form from the FP16 neighbourhood records (zeb_refine_list_h)."""
+        key, sheets, grad, vpair, gpair = p.baked
         lst = self.mask_list(fr)
-        if lst is not None:
+        quads = p.quads.get(key) if self.set["precision"] == "bf16" else None
+        if lst is not None and quads is not None:
+            N.call("zeb_refine_list_h", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(lst),
+                   lst.numel(), ptr(vpair), ptr(quads), p.master.side, ctypes.byref(opts), ptr(out), stream_ptr())
+        elif lst is not None:
             N.call("zeb_refine_list", ptr(pats), ptr(items), ptr(peaks), 8, n, ctypes.byref(fr), ptr(lst), lst.numel(),
                    ptr(vpair), ptr(gpair), p.master.side, ctypes.byref(opts), ptr(out), stream_ptr())
         else:
