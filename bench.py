@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=16384, help="patterns per device pass in the value measurement")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit", "plane", "large", "nickel"),
+    ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit", "plane", "large", "nickel",
+                                                              "match"),
                     help="index: the scan of 60x60 patterns (the headline); adjoint: six-unknown refinement "
                          "of 120x120 patterns with jittered pattern centres; uneven: many scans of uneven "
                          "lengths and detector sizes, two phases; pcfit: the pattern-centre vote at its default "
@@ -68,6 +69,8 @@ def parse():
                          "nickel: the reference's real scan (kikuchipy's nickel scan, h5ebsd), one pass and two sweeps")
     ap.add_argument("--large", type=int, default=250000, help="large: patterns of the scan (config 5 names 1 000 000)")
     ap.add_argument("--scans", type=int, default=64, help="uneven: number of scans")
+    ap.add_argument("--entries", type=int, default=65536, help="match: dictionary entries")
+    ap.add_argument("--components", type=int, default=512, help="match: values per row (PCA components)")
     ap.add_argument("--kernel-split", action="store_true",
                     help="nickel: also the device time by kernel (torch.profiler), printed to stderr")
     ap.add_argument("--max-count", type=int, default=200000, help="uneven: the longest scan (log-uniform from 1000)")
@@ -1070,6 +1073,54 @@ def nickel_main(a):
     print(json.dumps(line), flush=True)
 
 
+def match_main(a):
+    """The dictionary match alone (zeb_match_bf16: BF16 tcgen05 GEMM with each pattern's eight best
+    kept by the epilogue) on random unit rows: --patterns patterns × --entries entries ×
+    --components values (the PCA configuration's shape by default: 16 384 × 65 536 × 512). Prints
+    the kernel's TFLOP/s (CUDA events over --steps launches after --warmup)."""
+    import ctypes
+
+    import torch
+
+    from zebsdsolve_b200 import _native as N
+    from zebsdsolve_b200.dictionary import panel
+
+    n, m, k = min(a.patterns, 16384), a.entries, a.components
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x = torch.randn(n, k, generator=g, device="cuda")
+    x /= x.norm(dim=1, keepdim=True)
+    d = torch.randn(m, k, generator=g, device="cuda")
+    d /= d.norm(dim=1, keepdim=True)
+    xp, dp = panel(x), panel(d)
+    sl = N.load().zeb_match_slices(n, m, k, 1)
+    cv = torch.empty(n * sl * 8, device="cuda")
+    ci = torch.empty(n * sl * 8, dtype=torch.int32, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def run():
+        N.call("zeb_match_bf16", P(xp), n, P(dp), m, k, sl, P(cv), P(ci), P(st), sp)
+
+    for _ in range(max(a.warmup, 1)):
+        run()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(a.steps):
+        run()
+    t1.record()
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    ms = t0.elapsed_time(t1) / a.steps
+    tf = 2.0 * n * m * k / (ms / 1e3) / 1e12
+    print(json.dumps({"metric": "dictionary match TFLOP/s (BF16 tcgen05, top 8 kept in the epilogue), 1 B200",
+                      "value": round(tf, 1), "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+                      "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "bf16", "data": "synthetic",
+                      "config": {"workload": f"{n} patterns x {m} entries x {k} values, random unit rows",
+                                 "slices": sl}}), flush=True)
+
+
 def relaunch(a):
     """`--gpus N` (N > 1) run directly: the same command under torch.distributed.run, one process
     per GPU of this node (rendezvous on 127.0.0.1); returns its exit status."""
@@ -1101,5 +1152,7 @@ if __name__ == "__main__":
         large_main(args)
     elif args.workload == "nickel":
         nickel_main(args)
+    elif args.workload == "match":
+        match_main(args)
     else:
         device_main(args)
