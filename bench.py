@@ -67,7 +67,7 @@ def parse():
                          "settings; plane: the plane of source points (fit_plane, fit_geometry); large: 160x160 "
                          "patterns binned 2x, two sweeps L=64 then L=128, adjoint refinement, and a PCA dictionary; "
                          "nickel: the reference's real scan (kikuchipy's nickel scan, h5ebsd), one pass and two sweeps")
-    ap.add_argument("--large", type=int, default=250000, help="large: patterns of the scan (config 5 names 1 000 000)")
+    ap.add_argument("--large", type=int, default=1000000, help="large: patterns of the scan (1 000 000: 51 GB of u16 on the host)")
     ap.add_argument("--scans", type=int, default=64, help="uneven: number of scans")
     ap.add_argument("--entries", type=int, default=65536, help="match: dictionary entries")
     ap.add_argument("--components", type=int, default=512, help="match: values per row (PCA components)")
@@ -860,8 +860,8 @@ def plane_main(a):
 
 
 def large_main(a):
-    """Config 5's path at --large patterns (1 000 000 in the configuration; 250 000 by default, so
-    that the stored scan and its page-locked copy stay within 26 GB of host memory): 160 x 160 u16
+    """Config 5's path at --large patterns (1 000 000 by default: 51 GB of stored patterns on the
+    host, streamed to the device through two page-locked slots, never locked whole): 160 x 160 u16
     patterns of the 432 master with grains as in the headline workload, binned 2x to 80 x 80;
     indexed in two sweeps (L = 64, then L = 128 for the cells not accepted) in the BF16 form and in
     the plain FP32 form, then every pattern refined over six unknowns with the adjoint gradient;

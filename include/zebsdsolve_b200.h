@@ -331,8 +331,11 @@ int zeb_records_fz(const float* records, int n, const double* ops, int n_ops, fl
  * rotation and the ray's normalization), out[b][6] = NCC: the adjoint, which recomputes the
  * projection. mode 2: out[b][0..42] = the 43 sums of detector.wgsl:435-499 (sums), with the
  * directions from the gradient table gpair (the reference's Gauss–Newton Jacobian), from which
- * planefit.zig:176-200 (localOf) forms NCC, gradient and GN matrix. vpair/gpair:
- * zeb_master_pairs. Replaces Detector's `sums` schedule (src/planefit.zig:523-558 eval). */
+ * planefit.zig:176-200 (localOf) forms NCC, gradient and GN matrix. mode 3: out[b][0..60] =
+ * mode 2's 43 sums, then from the same pass mode 1's exact derivatives D' summed as ΣD' (43-48),
+ * ΣM·D' (49-54) and Σe·D' (55-60): one pass a round for the adjoint settle (GN matrix from the
+ * table, gradient from the adjoint). vpair/gpair: zeb_master_pairs. Replaces Detector's `sums`
+ * schedule (src/planefit.zig:523-558 eval). */
 int zeb_det6(int mode, const float* pats, const float* items, int n, const zeb_frame_t* fr, const float* vpair,
              const float* gpair, int side, const float* x, const float* q0, float* out, void* stream);
 

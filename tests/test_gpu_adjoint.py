@@ -189,6 +189,34 @@ def test_adjoint_and_reference_jacobian_agree(setup):
     assert float(((ga - gr).norm(dim=1) / gr.norm(dim=1)).max()) < 0.1
 
 
+@pytest.mark.parametrize("use_list", [False, True])
+def test_one_pass_mode_gives_both_passes(setup, use_list):
+    """zeb_det6 mode 3 (the adjoint settle's one pass a round) gives mode 2's 43 sums and, through
+    adjoint.adjoint_gradient, mode 1's exact gradient (FP32 summation-order noise: 1e-5 of each
+    output's scale; the gradient 1e-4 of its norm)."""
+    from zebsdsolve_b200 import adjoint
+
+    st = setup
+    e = st["e"]
+    plan, _ = _plan(st)
+    if use_list:
+        plan = adjoint.Plan(plan.pats, plan.items, plan.frame, plan.vpair, plan.gpair, plan.side,
+                            e.mask_list(e.frame()))
+    rng = np.random.default_rng(3)
+    x = torch.as_tensor(np.concatenate([rng.normal(0, 0.5, (st["n"], 3)), rng.normal(0, 0.01, (st["n"], 3))], 1),
+                        dtype=torch.float32, device="cuda").contiguous()
+    q0 = torch.as_tensor(st["q_start"], dtype=torch.float32, device="cuda").contiguous()
+    s3 = plan.run(3, x, q0)
+    s2 = plan.run(2, x, q0)
+    a, b = s3[:, :43].cpu().numpy(), s2.cpu().numpy()
+    scale = np.maximum(np.abs(b).max(0), 1e-6)
+    assert np.all(np.abs(a - b) <= 1e-5 * scale + 1e-7), np.abs(a - b).max()
+    g1 = plan.run(1, x, q0)[:, :6].double()
+    g3 = adjoint.adjoint_gradient(s3)
+    err = (g3 - g1).norm(dim=1) / g1.norm(dim=1)
+    assert float(err.max()) < 1e-4, err
+
+
 @pytest.mark.parametrize("gradient", ["reference", "adjoint"])
 def test_refine_patterns_settles_like_the_oracle(setup, gradient):
     """The six-unknown Levenberg–Marquardt from orientations 1–2° off and the nominal pattern
@@ -221,7 +249,7 @@ def test_refine_patterns_settles_like_the_oracle(setup, gradient):
             assert r["ncc"][i] > ncc - 1e-4, (r["ncc"][i], ncc)
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_pixel_list_kernel_equals_the_block_list_kernel(setup, mode):
     """zeb_det6_list (the frame's shared pixel list, 128 threads a pattern) gives zeb_det6's
     outputs in every mode, to FP32 summation-order noise (1e-5 of each output's scale)."""

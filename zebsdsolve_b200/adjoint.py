@@ -32,7 +32,7 @@ class Plan:
         self.n = items.shape[0]
 
     def run(self, mode, x, q0):
-        width = (1, 7, 43)[mode]
+        width = (1, 7, 43, 61)[mode]
         out = torch.empty(self.n * width, dtype=torch.float32, device=x.device)
         if self.pixels is not None:
             N.call("zeb_det6_list", mode, ptr(self.pats), ptr(self.items), self.n, ctypes.byref(self.frame),
@@ -118,14 +118,29 @@ def local_of(s):
     return ok, ncc, g, H
 
 
+def adjoint_gradient(s):
+    """∂NCC/∂x from the one-pass sums of zeb_det6 mode 3 [n, 61] (FP64): the NCC's statistics
+    (sums 0-3) with the exact derivatives' ΣD', ΣM·D', Σe·D' (sums 43-60), by the formula of
+    planefit.zig:176-200 (au = (ΣM·D' − mean·ΣD')/σ, g = (Σe·D' − NCC·au)/σ)."""
+    s = s.to(torch.float64)
+    n = torch.clamp(s[:, 0], min=1.0)
+    mean = s[:, 1] / n
+    var_n = s[:, 2] - n * mean * mean
+    ok = var_n > 1e-12
+    inv = torch.where(ok, torch.rsqrt(torch.where(ok, var_n, torch.ones_like(var_n))), torch.zeros_like(var_n))
+    ncc = s[:, 3] * inv
+    au = (s[:, 49:55] - mean[:, None] * s[:, 43:49]) * inv[:, None]
+    return (s[:, 55:61] - ncc[:, None] * au) * inv[:, None]
+
+
 def refine6(plan, q0, trust, most=60, gradient="reference"):
     """planefit.zig:570-622 (settle, k = 6) over every pattern of `plan` at once: λ from 1e-3;
     each round every pattern's damped step (its shift clamped to ±trust pixels, its rotation
     exp(d)·q) is kept where its own NCC rose (λ ← max(λ/3, 1e-4)), else λ ← min(5λ, 1e8); until
     a round gains the patterns' mean NCC less than 1e-7 (a round in which every step overshot
     goes again while some λ < 1e8) or after `most` rounds. gradient: "reference" (the gradient
-    table's, as the reference) or "adjoint" (the exact derivative of the forward: the adjoint
-    kernel that ProjectedNCC's backward runs, called once per round for gradient and NCC).
+    table's, as the reference) or "adjoint" (the exact derivative of the forward, ProjectedNCC's
+    backward: the derivatives of its adjoint kernel summed in the same pass as the GN sums, mode 3).
     Returns (q [n,4] f64, shift [n,3] f64 pixels, NCC [n], rounds)."""
     dev = q0.device
     n = plan.n
@@ -135,14 +150,13 @@ def refine6(plan, q0, trust, most=60, gradient="reference"):
     def local(qq, ss):
         x = torch.cat([ss, torch.zeros(n, 3, dtype=torch.float64, device=dev)], 1).to(torch.float32).contiguous()
         qf = qq.to(torch.float32).contiguous()
-        ok, ncc, g, H = local_of(plan.run(2, x, qf))
         if gradient == "adjoint":
-            # the exact gradient and the NCC from one pass of the adjoint kernel (what
-            # ProjectedNCC's backward runs; its forward pass would only repeat the NCC)
-            res = plan.run(1, x, qf).to(torch.float64)
-            g = res[:, :6]
-            ncc = torch.where(ok, res[:, 6], ncc)
-        return ok, ncc, g, H
+            # one pass: the GN sums and the adjoint's derivatives of the same projection
+            sums = plan.run(3, x, qf)
+            ok, ncc, _, H = local_of(sums[:, :43])
+            g = torch.where(ok[:, None], adjoint_gradient(sums), torch.zeros_like(H[:, 0]))
+            return ok, ncc, g, H
+        return local_of(plan.run(2, x, qf))
 
     keep = local(q, shift)
     lam = torch.full((n,), 1e-3, dtype=torch.float64, device=dev)

@@ -636,12 +636,18 @@ __global__ void __launch_bounds__(RL_THREADS, 6) k_refine_list(DetArgs a, const 
 
   for (int iter = 0; iter <= a.o.iters; ++iter) {
     const float4 q = sh_q;
+    // the frame turned by q once a pass: q·(u/|u|) = (R u)/|R u| with R u = row·R c0 + col·R c1 + R t
+    const float3 rc0 = qrot(q, a.c0), rc1 = qrot(q, a.c1), rt = qrot(q, t);
     float s[19];
 #pragma unroll
     for (int k = 0; k < 19; ++k) s[k] = 0.f;
 #pragma unroll 4
     for (int k = threadIdx.x; k < npix; k += RL_THREADS) {
-      const float3 c = qrot(q, list_ray(a, t, __ldg(list + k)));
+      const uint32_t v = __ldg(list + k);
+      const float row = (float)(int)(v >> 16), col = (float)(int)(v & 0xffffu);
+      const float3 c = normalize3(make_float3(fmaf(rc0.x, row, fmaf(rc1.x, col, rt.x)),
+                                              fmaf(rc0.y, row, fmaf(rc1.y, col, rt.y)),
+                                              fmaf(rc0.z, row, fmaf(rc1.z, col, rt.z))));
       const float4 m = QUAD ? grad_at_quad(a.gpair, c, a.side) : grad_at_pair(a.gpair, c, a.side);
       const float3 d = cross3(c, make_float3(m.x, m.y, m.z));
       const float e = pv[k];

@@ -13,6 +13,9 @@
 //   MODE 2 (the reference's Gauss–Newton sums, detector.wgsl:435-499): with D from the master's
 //     gradient table instead (q⁻¹·∇M/|v|, c × ∇M), all 43 sums (n, ΣM, ΣM², ΣM·e, ΣD, ΣM·D, Σe·D,
 //     ΣDᵢDⱼ) from which planefit.zig:176-200 forms the NCC, its gradient and its GN matrix.
+//   MODE 3 (the adjoint settle's one pass a round): MODE 2's 43 sums and, from the same ray and
+//     rotation, MODE 1's exact derivatives D' with their ΣD', ΣM·D', Σe·D' (61 sums): the GN
+//     matrix from the table and the gradient from the adjoint, as two passes would give them.
 // k_solve6: a damped 6 × 6 system per pattern in FP64 by elimination with partial pivoting
 // (planefit.zig:203-248).
 #include "abi_util.cuh"
@@ -30,7 +33,7 @@ struct Det6Args {
   int side;
   const float* x;   // [n][6]: δt (3, pixels), φ (3, radians)
   const float* q0;  // [n][4] (w, x, y, z)
-  float* out;       // MODE 0: [n]; MODE 1: [n][7] (∂NCC/∂x, NCC); MODE 2: [n][43]
+  float* out;       // MODE 0: [n]; MODE 1: [n][7] (∂NCC/∂x, NCC); MODE 2: [n][43]; MODE 3: [n][61]
   const float* sheets;  // MODE 2 with interp 1 or 2: the master's two sheets [2][side][side]
   int interp;           // MODE 2: 0 the gradient table (bilinear), 1 bicubic, 2 Keys' six-point
 };
@@ -159,22 +162,25 @@ __device__ __forceinline__ void sheet_jacobian(float3 c, int side, float3& dfj, 
   dfj = make_float3(0.f, 0.f, 0.f);
   dfi = make_float3(0.f, 0.f, 0.f);
   if (rho2 < 1e-20f) return;
-  const float den = 1.f + az;
-  const float qv = 0.5f * ZEB_PI * rho2 / den;
+  const float rden = __frcp_rn(1.f + az), rrho2 = __frcp_rn(rho2);
+  const float qv = 0.5f * ZEB_PI * rho2 * rden;
   const float xn = sqrtf(qv);
   // ∂xn = ∂q / (2 xn); ∂q = (π x/den, π y/den, −(π/2) ρ² sgn(z)/den²)
   const float k = 0.5f / xn;
-  const float3 dxn = make_float3(k * ZEB_PI * c.x / den, k * ZEB_PI * c.y / den, -k * 0.5f * ZEB_PI * rho2 * sz / (den * den));
+  const float3 dxn = make_float3(k * ZEB_PI * c.x * rden, k * ZEB_PI * c.y * rden, -k * 0.5f * ZEB_PI * rho2 * sz * rden * rden);
   const float four_pi = 4.f / ZEB_PI;
+  // the angle as the lookup's map takes it (sphere_to_square_fast: the fitted arctangent of the
+  // smaller over the larger coordinate)
+  const float ang = atan01(__fdividef(fminf(ax, ay), fmaxf(ax, ay)));
   float3 du, dw;
   if (ax >= ay) {
-    const float al = atan2f(ay, ax);
-    const float3 dal = make_float3(-ay * sx / rho2, ax * sy / rho2, 0.f);
+    const float al = ang;
+    const float3 dal = make_float3(-ay * sx * rrho2, ax * sy * rrho2, 0.f);
     du = dxn;
     dw = make_float3(four_pi * (dxn.x * al + xn * dal.x), four_pi * (dxn.y * al + xn * dal.y), four_pi * dxn.z * al);
   } else {
-    const float be = atan2f(ax, ay);
-    const float3 dbe = make_float3(ay * sx / rho2, -ax * sy / rho2, 0.f);
+    const float be = ang;
+    const float3 dbe = make_float3(ay * sx * rrho2, -ax * sy * rrho2, 0.f);
     du = make_float3(four_pi * (dxn.x * be + xn * dbe.x), four_pi * (dxn.y * be + xn * dbe.y), four_pi * dxn.z * be);
     dw = dxn;
   }
@@ -218,19 +224,30 @@ __device__ __forceinline__ void det6_pixel(const Det6Args& a, float4 q, float4 q
   const float inv = 1.f / dist;
   const float3 c = qrot(q, make_float3(v.x * inv, v.y * inv, v.z * inv));
   float m;
-  float d[6];
+  float d[6], dx[6];
   if (MODE == 0) {
     m = master_at_pair(a.vpair, c, a.side);
   } else {
     float3 g;
     if (MODE == 1) {
       m = master_and_slope(a.vpair, c, a.side, g);
-    } else {
+    } else if (MODE == 2) {
       const float4 gm = a.interp == 0   ? grad_at_pair(a.gpair, c, a.side)
                         : a.interp == 1 ? grad_smooth<1>(a.sheets, c, a.side)
                                         : grad_smooth<2>(a.sheets, c, a.side);
       m = gm.w;
       g = make_float3(gm.x, gm.y, gm.z);
+    } else {
+      // the table's value is the sheet's bilinear value at the same place (the same arithmetic)
+      const float4 gm = grad_at_pair(a.gpair, c, a.side);
+      m = gm.w;
+      g = make_float3(gm.x, gm.y, gm.z);
+      float3 ge;
+      master_and_slope(a.vpair, c, a.side, ge);
+      const float3 we = qrot(qi, ge);
+      const float3 re = cross3(c, ge);
+      dx[0] = we.x * inv; dx[1] = we.y * inv; dx[2] = we.z * inv;
+      dx[3] = re.x; dx[4] = re.y; dx[5] = re.z;
     }
     const float3 w = qrot(qi, g);
     const float3 r = cross3(c, g);
@@ -249,12 +266,20 @@ __device__ __forceinline__ void det6_pixel(const Det6Args& a, float4 q, float4 q
       s[16 + i] += e * d[i];
     }
   }
-  if (MODE == 2) {
+  if (MODE >= 2) {
     int o = 22;
 #pragma unroll
     for (int i = 0; i < 6; ++i)
 #pragma unroll
       for (int j = i; j < 6; ++j) s[o++] += d[i] * d[j];
+  }
+  if (MODE == 3) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      s[43 + i] += dx[i];
+      s[49 + i] += m * dx[i];
+      s[55 + i] += e * dx[i];
+    }
   }
 }
 
@@ -262,8 +287,8 @@ __device__ __forceinline__ void det6_pixel(const Det6Args& a, float4 q, float4 q
 // MODE 1 the NCC and its gradient (planefit.zig:176-200)
 template <int MODE, int NS>
 __device__ __forceinline__ void det6_finish(const Det6Args& a, int b, const float (&s)[NS]) {
-  if (MODE == 2) {
-    for (int k = 0; k < 43; ++k) a.out[(size_t)b * 43 + k] = s[k];
+  if (MODE >= 2) {
+    for (int k = 0; k < NS; ++k) a.out[(size_t)b * NS + k] = s[k];
     return;
   }
   // planefit.zig:176-200: NCC and (MODE 1) its gradient
@@ -291,7 +316,7 @@ __device__ __forceinline__ void det6_finish(const Det6Args& a, int b, const floa
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
-  constexpr int NS = MODE == 0 ? 4 : (MODE == 1 ? 22 : 43);
+  constexpr int NS = MODE == 0 ? 4 : (MODE == 1 ? 22 : (MODE == 2 ? 43 : 61));
   extern __shared__ float4 px6[];
   __shared__ float red[NS * 8];
   __shared__ int wcnt[8];
@@ -357,7 +382,7 @@ __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
 // block fills an SM's shared memory for one 120 × 120 pattern).
 template <int MODE>
 __global__ void __launch_bounds__(128, 4) k_det6_list(Det6Args a, const uint32_t* __restrict__ list, int npix) {
-  constexpr int NS = MODE == 0 ? 4 : (MODE == 1 ? 22 : 43);
+  constexpr int NS = MODE == 0 ? 4 : (MODE == 1 ? 22 : (MODE == 2 ? 43 : 61));
   extern __shared__ float pv6[];
   __shared__ float red[NS * 4];
   __shared__ float4 sh_q;
@@ -451,8 +476,8 @@ using namespace zeb;
 extern "C" int zeb_det6(int mode, const float* pats, const float* items, int n, const zeb_frame_t* fr,
                         const float* vpair, const float* gpair, int side, const float* x, const float* q0, float* out,
                         void* stream) {
-  ZEB_REQUIRE(mode >= 0 && mode <= 2, ZEB_EARG, "det6: mode %d", mode);
-  ZEB_REQUIRE(pats && items && vpair && x && q0 && out && fr && side >= 3 && (mode != 2 || gpair), ZEB_EARG,
+  ZEB_REQUIRE(mode >= 0 && mode <= 3, ZEB_EARG, "det6: mode %d", mode);
+  ZEB_REQUIRE(pats && items && vpair && x && q0 && out && fr && side >= 3 && (mode < 2 || gpair), ZEB_EARG,
               "det6: bad arguments");
   ZEB_REQUIRE(((uintptr_t)gpair & 31) == 0 && ((uintptr_t)vpair & 7) == 0, ZEB_EARG, "det6: pair tables misaligned");
   if (n <= 0) return ZEB_OK;
@@ -475,9 +500,12 @@ extern "C" int zeb_det6(int mode, const float* pats, const float* items, int n, 
   } else if (mode == 1) {
     cudaFuncSetAttribute(k_det6<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
     k_det6<1><<<n, 256, list, st>>>(a);
-  } else {
+  } else if (mode == 2) {
     cudaFuncSetAttribute(k_det6<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
     k_det6<2><<<n, 256, list, st>>>(a);
+  } else {
+    cudaFuncSetAttribute(k_det6<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)list);
+    k_det6<3><<<n, 256, list, st>>>(a);
   }
   return zeb_launch_check("det6");
 }
@@ -485,8 +513,8 @@ extern "C" int zeb_det6(int mode, const float* pats, const float* items, int n, 
 extern "C" int zeb_det6_list(int mode, const float* pats, const float* items, int n, const zeb_frame_t* fr,
                              const uint32_t* list, int npix, const float* vpair, const float* gpair, int side,
                              const float* x, const float* q0, float* out, void* stream) {
-  ZEB_REQUIRE(mode >= 0 && mode <= 2, ZEB_EARG, "det6_list: mode %d", mode);
-  ZEB_REQUIRE(pats && items && list && vpair && x && q0 && out && fr && side >= 3 && (mode != 2 || gpair), ZEB_EARG,
+  ZEB_REQUIRE(mode >= 0 && mode <= 3, ZEB_EARG, "det6_list: mode %d", mode);
+  ZEB_REQUIRE(pats && items && list && vpair && x && q0 && out && fr && side >= 3 && (mode < 2 || gpair), ZEB_EARG,
               "det6_list: bad arguments");
   ZEB_REQUIRE(((uintptr_t)gpair & 31) == 0 && ((uintptr_t)vpair & 7) == 0, ZEB_EARG,
               "det6_list: pair tables misaligned");
@@ -511,9 +539,12 @@ extern "C" int zeb_det6_list(int mode, const float* pats, const float* items, in
   } else if (mode == 1) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_det6_list<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_det6_list<1><<<n, 128, smem, st>>>(a, list, npix);
-  } else {
+  } else if (mode == 2) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_det6_list<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_det6_list<2><<<n, 128, smem, st>>>(a, list, npix);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_det6_list<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_det6_list<3><<<n, 128, smem, st>>>(a, list, npix);
   }
   return zeb_launch_check("det6_list");
 }

@@ -34,6 +34,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "abi_util.cuh"
 #include "tc_util.cuh"
@@ -190,13 +191,54 @@ struct TcShared {
   int failed;
 };
 
+// The FP16 form: K' <= 256 (split <= 16 at L <= 64), so 4 B blocks and 4 A stages; the drain
+// stages a whole tile (128 rows × 128 items in FP16: two 16 KB store boxes) at once, two tiles deep.
+constexpr int TCH_MAX_KB = 4;
+constexpr int TCH_STAGES = 4;
+constexpr int TCH_BOX = 64 * TC_BM * 2;  // bytes of one store box: 64 items × 128 rows
+struct TcSharedH {
+  uint8_t b[TCH_MAX_KB][TC_B_BLOCK];   // 64 KB, 1024-aligned
+  uint8_t a[TCH_STAGES][TC_A_BLOCK];   // 64 KB
+  uint8_t stage[2][2 * TCH_BOX];       // 2 × 32 KB: a tile, items 0-63 then 64-127, [ν][64 items]
+  uint64_t b_full, a_full[TCH_STAGES], a_empty[TCH_STAGES], acc_full[2], acc_empty[2], mma_done, never;
+  long long a_off, b_off;
+  uint32_t tmem;
+  int failed;
+};
+
+// 64 accumulator columns of one row ν (two TMEM loads of 32) × scale → FP16 → the row's 128 bytes
+// of a store box, 16-byte chunks XOR-swizzled by ν mod 8 (the tensor map's 128-byte swizzle)
+__device__ __forceinline__ void tch_row(uint8_t* box, int row, const uint32_t (&v)[32], const uint32_t (&w)[32],
+                                        float sc) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint4 o;
+    o.x = pack_half2(__uint_as_float(v[8 * q + 0]) * sc, __uint_as_float(v[8 * q + 1]) * sc);
+    o.y = pack_half2(__uint_as_float(v[8 * q + 2]) * sc, __uint_as_float(v[8 * q + 3]) * sc);
+    o.z = pack_half2(__uint_as_float(v[8 * q + 4]) * sc, __uint_as_float(v[8 * q + 5]) * sc);
+    o.w = pack_half2(__uint_as_float(v[8 * q + 6]) * sc, __uint_as_float(v[8 * q + 7]) * sc);
+    *(uint4*)(box + sw128(row, 8 * q)) = o;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint4 o;
+    o.x = pack_half2(__uint_as_float(w[8 * q + 0]) * sc, __uint_as_float(w[8 * q + 1]) * sc);
+    o.y = pack_half2(__uint_as_float(w[8 * q + 2]) * sc, __uint_as_float(w[8 * q + 3]) * sc);
+    o.z = pack_half2(__uint_as_float(w[8 * q + 4]) * sc, __uint_as_float(w[8 * q + 5]) * sc);
+    o.w = pack_half2(__uint_as_float(w[8 * q + 6]) * sc, __uint_as_float(w[8 * q + 7]) * sc);
+    *(uint4*)(box + sw128(row, 32 + 8 * q)) = o;
+  }
+}
+
 // HALF = false: U in FP32 as [item][j][m'][c] (re, im); true: scale·U in FP16 as
 // [item tile][(j, c)][m'][re|im][128 items] (items padded to whole tiles of 128), the layout the
 // tensor-core transform along a (slab_tc.cu) loads its operand tiles from.
 template <bool HALF>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const __grid_constant__ CUtensorMap umap) {
+  using Sh = std::conditional_t<HALF, TcSharedH, TcShared>;
+  constexpr int NST = HALF ? TCH_STAGES : TC_STAGES;
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
-  TcShared& s = *reinterpret_cast<TcShared*>((void*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023));
+  Sh& s = *reinterpret_cast<Sh*>((void*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ptile = blockIdx.x, mp = blockIdx.y;
   const TcLayout& t = a.t;
@@ -210,7 +252,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
     mbar_init(&s.never, 1);  // nothing arrives: the failure test's wait
     s.a_off = tc_offset(t.L, t.split, mp, t.mtiles, TC_A_BLOCK);
     s.b_off = tc_offset(t.L, t.split, mp, t.ptiles, TC_B_BLOCK);
-    for (int i = 0; i < TC_STAGES; ++i) {
+    for (int i = 0; i < NST; ++i) {
       mbar_init(&s.a_full[i], 1);
       mbar_init(&s.a_empty[i], 1);
     }
@@ -242,8 +284,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
       const int total = mtiles * kb;  // this CTA's blocks of the order's A, [mtile][kblock]
       int it = 0;
       for (; it < total; ++it) {
-        const int st = it % TC_STAGES;
-        if (!mbar_wait(&s.a_empty[st], ((it / TC_STAGES) & 1) ^ 1, lim)) break;
+        const int st = it % NST;
+        if (!mbar_wait(&s.a_empty[st], ((it / NST) & 1) ^ 1, lim)) break;
         mbar_expect_tx(&s.a_full[st], TC_A_BLOCK);
         bulk_g2s(s.a[st], asrc + (size_t)it * TC_A_BLOCK, TC_A_BLOCK, &s.a_full[st]);
       }
@@ -254,8 +296,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
       // the copies still in flight land before the CTA may leave, whether or not the MMAs took
       // them (bounded waits on their phases; a phase already consumed reads as complete)
       mbar_wait(&s.b_full, 0, kDrainNs);
-      for (int i = (it > TC_STAGES ? it - TC_STAGES : 0); i < it; ++i)
-        mbar_wait(&s.a_full[i % TC_STAGES], (i / TC_STAGES) & 1, kDrainNs);
+      for (int i = (it > NST ? it - NST : 0); i < it; ++i)
+        mbar_wait(&s.a_full[i % NST], (i / NST) & 1, kDrainNs);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -271,8 +313,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + (uint32_t)(acc * TC_BN);
         for (int k = 0; k < kb; ++k, ++it) {
-          const int st = it % TC_STAGES;
-          ok = mbar_wait(&s.a_full[st], (it / TC_STAGES) & 1, lim);
+          const int st = it % NST;
+          ok = mbar_wait(&s.a_full[st], (it / NST) & 1, lim);
           if (!ok) break;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t abase = smem_addr(s.a[st]), bbase = smem_addr(s.b[k]);
@@ -304,6 +346,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
     int chunk = 0;
     for (int mt = 0; mt < mtiles; ++mt) {
       if constexpr (HALF) {
+        // the whole tile at once: four TMEM loads (128 items of row ν), the accumulator handed back
+        // to the MMAs, FP16 rows into the tile's staging buffer, two 16 KB tensor stores; the
+        // buffer of two tiles back has been read by its stores (the last group may still read)
         const int acc = mt & 1;
         if (!bar_and(1, 128, leader ? mbar_wait_sleep(&s.acc_full[acc], (mt >> 1) & 1, lim) : true)) {
           if (leader) {
@@ -314,85 +359,65 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int r0 = (mt0 + mt) * TC_BM;  // first row ν of the tile
-        // two 64-pattern chunks: TMEM → registers → ×scale → FP16 → a staging buffer of 128-byte
-        // rows [ν][64 items], 16-byte chunks XOR-swizzled by ν mod 8 (the tensor map's 128-byte
-        // swizzle) → one 16 KB tensor store
+        const uint32_t ta = tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(acc * TC_BN);
+        uint32_t v0[32], v1[32], v2[32], v3[32];
+        TMEM_LD32(ta, v0);
+        TMEM_LD32(ta + 32, v1);
+        TMEM_LD32(ta + 64, v2);
+        TMEM_LD32(ta + 96, v3);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s.acc_empty[acc]);
+        uint8_t* stg = s.stage[mt & 1];
+        if (leader) bulk_wait_read1();
+        bar_sync(1, 128);
+        const float sc = a.scale;
+        tch_row(stg, row, v0, v1, sc);
+        tch_row(stg + TCH_BOX, row, v2, v3, sc);
+        fence_proxy_async();
+        bar_sync(1, 128);
+        if (leader) {
+          if (ptile * TC_BN < a.n_items) tma_store_5d(&umap, stg, 0, 0, mp, r0 >> 1, ptile);
+          if (ptile * TC_BN + 64 < a.n_items) tma_store_5d(&umap, stg + TCH_BOX, 64, 0, mp, r0 >> 1, ptile);
+          bulk_commit();
+        }
+      } else {
+        const int acc = mt & 1;
+        // the four warps agree on the outcome (a barrier that ANDs their results)
+        // one thread waits for the accumulator (sleeping between polls); the barrier hands the
+        // outcome to the others, which wait there without taking issue slots
+        if (!bar_and(1, 128, leader ? mbar_wait_sleep(&s.acc_full[acc], (mt >> 1) & 1, lim) : true)) {
+          if (leader) {
+            atomicOr(a.status, 4);
+            s.failed = 1;
+          }
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int r0 = (mt0 + mt) * TC_BM;  // first row ν of the tile
+        const int j0 = r0 / two_nc, x0 = two_nc <= TC_BM ? 0 : r0 % two_nc;
 #pragma unroll 1
-        for (int c0 = 0; c0 < TC_BN; c0 += 64, ++chunk) {
-          uint32_t v[32], w[32];
+        for (int c0 = 0; c0 < TC_BN; c0 += 32, ++chunk) {
+          uint32_t v[32];
           TMEM_LD32(tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(acc * TC_BN + c0), v);
-          TMEM_LD32(tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(acc * TC_BN + c0 + 32), w);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          if (c0 + 64 == TC_BN) {  // the accumulator is read out: the next tile's MMAs may start
+          if (c0 + 32 == TC_BN) {  // the accumulator is read out: the next tile's MMAs may start
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&s.acc_empty[acc]);
           }
-          uint8_t* stg = reinterpret_cast<uint8_t*>(s.stage[chunk & 1]);
+          float* stg = s.stage[chunk & 1];
           if (leader) bulk_wait_read1();  // the store that last used this buffer has read it
           bar_sync(1, 128);
-          const float sc = a.scale;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            uint4 o;
-            o.x = pack_half2(__uint_as_float(v[8 * q + 0]) * sc, __uint_as_float(v[8 * q + 1]) * sc);
-            o.y = pack_half2(__uint_as_float(v[8 * q + 2]) * sc, __uint_as_float(v[8 * q + 3]) * sc);
-            o.z = pack_half2(__uint_as_float(v[8 * q + 4]) * sc, __uint_as_float(v[8 * q + 5]) * sc);
-            o.w = pack_half2(__uint_as_float(v[8 * q + 6]) * sc, __uint_as_float(v[8 * q + 7]) * sc);
-            *(uint4*)(stg + sw128(row, 8 * q)) = o;
-          }
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            uint4 o;
-            o.x = pack_half2(__uint_as_float(w[8 * q + 0]) * sc, __uint_as_float(w[8 * q + 1]) * sc);
-            o.y = pack_half2(__uint_as_float(w[8 * q + 2]) * sc, __uint_as_float(w[8 * q + 3]) * sc);
-            o.z = pack_half2(__uint_as_float(w[8 * q + 4]) * sc, __uint_as_float(w[8 * q + 5]) * sc);
-            o.w = pack_half2(__uint_as_float(w[8 * q + 6]) * sc, __uint_as_float(w[8 * q + 7]) * sc);
-            *(uint4*)(stg + sw128(row, 32 + 8 * q)) = o;
-          }
+          for (int c = 0; c < 32; ++c) stg[c * TC_BM + row] = __uint_as_float(v[c]);
           fence_proxy_async();
           bar_sync(1, 128);
           if (leader) {
-            if (ptile * TC_BN + c0 < a.n_items) tma_store_5d(&umap, stg, c0, 0, mp, r0 >> 1, ptile);
+            if (ptile * TC_BN + c0 < a.n_items) tma_store_4d(&umap, stg, x0, mp, j0, ptile * TC_BN + c0);
             bulk_commit();
           }
-        }
-        continue;
-      }
-      const int acc = mt & 1;
-      // the four warps agree on the outcome (a barrier that ANDs their results)
-      // one thread waits for the accumulator (sleeping between polls); the barrier hands the
-      // outcome to the others, which wait there without taking issue slots
-      if (!bar_and(1, 128, leader ? mbar_wait_sleep(&s.acc_full[acc], (mt >> 1) & 1, lim) : true)) {
-        if (leader) {
-          atomicOr(a.status, 4);
-          s.failed = 1;
-        }
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int r0 = (mt0 + mt) * TC_BM;  // first row ν of the tile
-      const int j0 = r0 / two_nc, x0 = two_nc <= TC_BM ? 0 : r0 % two_nc;
-#pragma unroll 1
-      for (int c0 = 0; c0 < TC_BN; c0 += 32, ++chunk) {
-        uint32_t v[32];
-        TMEM_LD32(tmem + ((uint32_t)(ew * 32) << 16) + (uint32_t)(acc * TC_BN + c0), v);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (c0 + 32 == TC_BN) {  // the accumulator is read out: the next tile's MMAs may start
-          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&s.acc_empty[acc]);
-        }
-        float* stg = s.stage[chunk & 1];
-        if (leader) bulk_wait_read1();  // the store that last used this buffer has read it
-        bar_sync(1, 128);
-#pragma unroll
-        for (int c = 0; c < 32; ++c) stg[c * TC_BM + row] = __uint_as_float(v[c]);
-        fence_proxy_async();
-        bar_sync(1, 128);
-        if (leader) {
-          if (ptile * TC_BN + c0 < a.n_items) tma_store_4d(&umap, stg, x0, mp, j0, ptile * TC_BN + c0);
-          bulk_commit();
         }
       }
     }
@@ -549,6 +574,9 @@ extern "C" int zeb_spectrum_bf16_h(const float* alm, int n_items, const zeb_so3_
   ZEB_REQUIRE(tc_dims_ok(d, split), ZEB_EARG, "spectrum_bf16_h: unsupported dims (L=%d, split=%d)", d ? d->L : -1,
               split);
   ZEB_REQUIRE(2 * d->nb * d->nc >= TC_BM, ZEB_EARG, "spectrum_bf16_h: bandwidth %d too small", d->L);
+  ZEB_REQUIRE(tc_kblocks(d->L, 0, split) <= TCH_MAX_KB, ZEB_EARG,
+              "spectrum_bf16_h: K' of %d blocks (L=%d, split=%d) exceeds the FP16 form's %d", tc_kblocks(d->L, 0, split),
+              d->L, split, TCH_MAX_KB);
   ZEB_REQUIRE(scale > 0.f && scale < 1e30f, ZEB_EARG, "spectrum_bf16_h: scale %g", (double)scale);
   if (n_items <= 0) return ZEB_OK;
   TcLayout t = tc_layout(d, split, n_items);
@@ -567,7 +595,7 @@ extern "C" int zeb_spectrum_bf16_h(const float* alm, int n_items, const zeb_so3_
   a.stall = test_stall_ns();
   a.limit = a.stall > 0 ? a.stall : kWaitNs;
   a.scale = scale;
-  size_t smem = sizeof(TcShared) + 1024;
+  size_t smem = sizeof(TcSharedH) + 1024;
   cudaFuncSetAttribute(k_spectrum_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int sms = 148;
   {

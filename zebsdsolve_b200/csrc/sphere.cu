@@ -14,6 +14,8 @@
 // k_legendre: contracts the ring spectra with the weighted Legendre table, a block per
 // (order m, tile of items) with the table's rows for m staged in shared memory (sphere.wgsl:
 // 271-288). k_sh_norm: unit harmonic norm and the item's stats (sphere.wgsl:290-324).
+#include <algorithm>
+
 #include "abi_util.cuh"
 
 namespace zeb {
@@ -37,6 +39,7 @@ struct SphereArgs {
   const int2* spans;  // [n_theta] (first φ sample, count), cyclic; null: every sample
   int ring_major;     // spectra laid out [item][m][ring pair] (else [item][ring pair][m])
   int leg_items;      // items per k_legendre block (a multiple of 4)
+  int cache_cap;      // k_sphere_rings_w: samples its shared cache holds (0: none)
 };
 
 struct Sampler {
@@ -263,8 +266,13 @@ __device__ __forceinline__ void fft_reg8(float2 (&x)[8]) {
 
 // ── the rings of one item, a warp per ring pair, for n_φ = 256 ──
 //
-// The block holds the item's pattern and the φ cosines; after the window sums (over the spans),
-// each warp takes one ring pair with samples at a time: it zeroes its 256-point line, samples the
+// The block holds the item's pattern and the φ cosines; the window sums (over the spans) sample
+// every direction once and keep each sample in a shared cache (span order: ring y's samples from
+// the prefix sum of the spans before it), the value where the window holds it and a marker where
+// it does not; the transforms then read the cache, and their lines take the pattern's shared
+// memory.  Where an item's spans hold more samples than the cache (a span that fell short makes
+// its ring whole), the transforms sample again, from the pattern in global memory.
+// Each warp takes one ring pair with samples at a time: it zeroes its 256-point line, fills the
 // northern ring (real part) and its mirror (imaginary part) over their spans, and transforms the
 // line with no block barrier: lane l holds points l + 32k (k < 8), takes the 8-point DFT over k in
 // registers, multiplies by e^{−2πi l k₁/256}, then the 32-point DFT over the lanes by five radix-2
@@ -273,6 +281,9 @@ __device__ __forceinline__ void fft_reg8(float2 (&x)[8]) {
 // for m < L.  Spectra are written [item][m][ring pair].
 constexpr int RW_WARPS = 8;
 constexpr int RW_PAD = 256 + 32;  // line slots per warp: F + F/8
+constexpr int RW_CACHE = 7168;    // cached samples (28 KB): the spans of a 60 × 60 or 80 × 80 frame
+constexpr uint32_t RW_OUT = 0x7fc0dea1u;  // cache marker of a sample outside the window: a NaN no
+                                          // arithmetic produces (computed NaNs are canonical)
 
 __device__ __forceinline__ int rw_slot(int f) { return f + (f >> 3); }
 
@@ -287,14 +298,17 @@ __global__ void __launch_bounds__(RW_WARPS * 32) k_sphere_rings_w(SphereArgs a) 
   const int b = blockIdx.x;
   const int hw = a.h * a.w;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* lines = (float2*)smem4;                 // [RW_WARPS][RW_PAD]
-  float* spat = (float*)(lines + RW_WARPS * RW_PAD);
+  // dynamic shared memory: [the pattern (sampling), then the lines (transforms)] [the cache]
+  float2* lines = (float2*)smem4;  // [RW_WARPS][RW_PAD]
+  float* spat = (float*)smem4;
+  const int region = max(RW_WARPS * RW_PAD * 2, a.pat_in_smem ? hw : 0);  // floats
+  float* cache = (float*)smem4 + region;
   const float4 it = a.items[b];
   const bool window = (a.flags & ZEB_FLAG_WINDOW) != 0;
+  const float* src = window ? nullptr : a.pats + (size_t)(int)it.w * hw;
   Sampler s;
   s.pat = nullptr;
   if (!window) {
-    const float* src = a.pats + (size_t)(int)it.w * hw;
     if (a.pat_in_smem) {
       for (int i = threadIdx.x; i < hw; i += blockDim.x) spat[i] = src[i];
       s.pat = spat;
@@ -341,7 +355,8 @@ __global__ void __launch_bounds__(RW_WARPS * 32) k_sphere_rings_w(SphereArgs a) 
   __syncthreads();
 
   // the window's sums over the spans, a warp per ring pair as below (no search for a flat
-  // index's ring)
+  // index's ring); each sample into the cache when the item's spans fit it
+  const bool cached = pre[nt] <= a.cache_cap;
   float acc[2] = {0.f, 0.f};
   for (int ai = warp; ai < n_act; ai += RW_WARPS) {
     const int y2[2] = {act[ai], nt - 1 - act[ai]};
@@ -349,15 +364,18 @@ __global__ void __launch_bounds__(RW_WARPS * 32) k_sphere_rings_w(SphereArgs a) 
     for (int h = 0; h < 2; ++h) {
       const float4 rg = __ldg(a.ring + y2[h]);
       const int2 v = sp[y2[h]];
+      float* cy = cache + pre[y2[h]];
       for (int e = lane; e < v.y; e += 32) {
         const float2 cs = pcs[(v.x + e) & pmask];
         const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
         acc[0] += g.x * g.y * rg.z;
         acc[1] += g.y * rg.z;
+        if (cached) cy[e] = g.y > 0.f ? g.x : __uint_as_float(RW_OUT);
       }
     }
   }
-  block_sums<2>(acc, red);
+  block_sums<2>(acc, red);  // (its barriers also end every read of the pattern in shared memory)
+  if (!cached && a.pat_in_smem) s.pat = src;  // the lines take the pattern's shared memory
   const float mean = (a.flags & ZEB_FLAG_CENTER) ? acc[0] / fmaxf(acc[1], 1e-20f) : 0.f;
   if (threadIdx.x == 0) {
     a.stats[b * 4 + 0] = acc[1] * ZEB_TAU / (float)nphi;
@@ -386,24 +404,38 @@ __global__ void __launch_bounds__(RW_WARPS * 32) k_sphere_rings_w(SphereArgs a) 
 #pragma unroll
     for (int k = 0; k < 8; ++k) buf[lane + 32 * k] = make_float2(0.f, 0.f);
     __syncwarp();
-    {
-      const float4 rg = __ldg(a.ring + y);
-      const int2 v = sp[y];
-      for (int e = lane; e < v.y; e += 32) {
-        const int j = (v.x + e) & pmask;
-        const float2 cs = pcs[j];
-        const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
-        buf[j].x = (g.x - mean) * g.y;
+    if (cached) {
+      const int2 vn = sp[y], vs = sp[ys];
+      const float* cn = cache + pre[y];
+      const float* cq = cache + pre[ys];
+      for (int e = lane; e < vn.y; e += 32) {
+        const float c = cn[e];
+        buf[(vn.x + e) & pmask].x = __float_as_uint(c) == RW_OUT ? 0.f : c - mean;
       }
-    }
-    {
-      const float4 rg = __ldg(a.ring + ys);
-      const int2 v = sp[ys];
-      for (int e = lane; e < v.y; e += 32) {
-        const int j = (v.x + e) & pmask;
-        const float2 cs = pcs[j];
-        const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
-        buf[j].y = (g.x - mean) * g.y;
+      for (int e = lane; e < vs.y; e += 32) {
+        const float c = cq[e];
+        buf[(vs.x + e) & pmask].y = __float_as_uint(c) == RW_OUT ? 0.f : c - mean;
+      }
+    } else {
+      {
+        const float4 rg = __ldg(a.ring + y);
+        const int2 v = sp[y];
+        for (int e = lane; e < v.y; e += 32) {
+          const int j = (v.x + e) & pmask;
+          const float2 cs = pcs[j];
+          const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
+          buf[j].x = (g.x - mean) * g.y;
+        }
+      }
+      {
+        const float4 rg = __ldg(a.ring + ys);
+        const int2 v = sp[ys];
+        for (int e = lane; e < v.y; e += 32) {
+          const int j = (v.x + e) & pmask;
+          const float2 cs = pcs[j];
+          const float2 g = s.sample(make_float3(rg.y * cs.x, rg.y * cs.y, rg.x));
+          buf[j].y = (g.x - mean) * g.y;
+        }
       }
     }
     __syncwarp();
@@ -690,7 +722,9 @@ extern "C" int zeb_sphere_coefficients_spans(const float* pats, const float* ite
   if (nphi == 256) {
     // the warp-per-ring-pair kernel
     a.ring_major = 1;
-    const size_t wsm = (size_t)RW_WARPS * RW_PAD * sizeof(float2) + (a.pat_in_smem ? hw * 4 : 0);
+    a.cache_cap = RW_CACHE;
+    const size_t wsm = std::max((size_t)RW_WARPS * RW_PAD * sizeof(float2), a.pat_in_smem ? hw * 4 : (size_t)0) +
+                       (size_t)RW_CACHE * sizeof(float);
     cudaFuncSetAttribute(k_sphere_rings_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
     k_sphere_rings_w<<<n_items, RW_WARPS * 32, wsm, st>>>(a);
     rc = zeb_launch_check("sphere_rings (warps)");

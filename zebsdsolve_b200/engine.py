@@ -1097,6 +1097,7 @@ class Engine:
         return self._pinned
 
     STAGE_BYTES = 64 << 20
+    PIN_MAX_BYTES = 16 << 30
 
     def raw_dtype(self):
         """The stored pixel type as a torch dtype."""
@@ -1106,10 +1107,14 @@ class Engine:
         """Whether uploads come from a page-locked copy of the whole scan: when it is made already,
         when the buffer kept from earlier scans holds it (no page-locking to pay), or from the
         scan's second index run on (a scan indexed once streams through the staging slots:
-        page-locking gigabytes for one run costs more than the run)."""
+        page-locking gigabytes for one run costs more than the run). A scan above PIN_MAX_BYTES
+        always streams: locking tens of gigabytes takes longer than a pass and holds that much of
+        the host's memory twice."""
         if self._pinned is not None:
             return True
         nbytes = self.patterns.size * self.patterns.itemsize
+        if nbytes > self.PIN_MAX_BYTES:
+            return False
         return (self._pin_buf is not None and self._pin_buf.numel() >= nbytes) or self._index_calls >= 2
 
     def _slot(self):
@@ -1120,6 +1125,31 @@ class Engine:
         if slot[1] is not None:
             slot[1].synchronize()  # the copy that last read this slot has finished
         return slot
+
+    FILL_PART = 8 << 20
+
+    def _fill(self, host, src):
+        """host[:] = src (a staging slot from the stored scan) in parts of FILL_PART bytes on a
+        pool of host threads: numpy copies without the interpreter lock, and one thread's copy
+        bandwidth, not the link's, bounds a streamed scan."""
+        nb = src.nbytes
+        parts = min(self._fill_threads(), max(1, nb // self.FILL_PART))
+        if parts <= 1:
+            np.copyto(host, src)
+            return
+        step = -(-len(src) // parts)
+        futs = [self._pool.submit(np.copyto, host[i:i + step], src[i:i + step]) for i in range(0, len(src), step)]
+        for f in futs:
+            f.result()
+
+    def _fill_threads(self):
+        if getattr(self, "_pool", None) is None:
+            import concurrent.futures as cf
+            import os
+
+            self._pool_n = max(1, min(8, (os.cpu_count() or 2) // 2))
+            self._pool = cf.ThreadPoolExecutor(self._pool_n, thread_name_prefix="zeb-fill")
+        return self._pool_n
 
     def upload_raw(self, cells, dst, stream):
         """Enqueue on `stream` the copies of the given cells' stored patterns into dst[0:n], one
@@ -1153,7 +1183,7 @@ class Engine:
                     k = min(left, most)
                     slot = self._slot()
                     host = slot[0].numpy()[: k * per].view(self.patterns.dtype).reshape(k, h, w)
-                    np.copyto(host, flat[c:c + k])
+                    self._fill(host, flat[c:c + k])
                     dst[o:o + k].copy_(slot[0][: k * per].view(td).view(k, h, w), non_blocking=True)
                     ev = torch.cuda.Event()
                     ev.record(stream)
