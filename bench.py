@@ -60,14 +60,17 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit", "plane", "large", "nickel",
-                                                              "match"),
+                                                              "match", "target"),
                     help="index: the scan of 60x60 patterns (the headline); adjoint: six-unknown refinement "
                          "of 120x120 patterns with jittered pattern centres; uneven: many scans of uneven "
                          "lengths and detector sizes, two phases; pcfit: the pattern-centre vote at its default "
                          "settings; plane: the plane of source points (fit_plane, fit_geometry); large: 160x160 "
                          "patterns binned 2x, two sweeps L=64 then L=128, adjoint refinement, and a PCA dictionary; "
-                         "nickel: the reference's real scan (kikuchipy's nickel scan, h5ebsd), one pass and two sweeps")
-    ap.add_argument("--large", type=int, default=1000000, help="large: patterns of the scan (1 000 000: 51 GB of u16 on the host)")
+                         "nickel: the reference's real scan (kikuchipy's nickel scan, h5ebsd), one pass and two sweeps; "
+                         "target: 1M patterns of 60x60 indexed and refined over six unknowns (adjoint), BF16 form "
+                         "against the FP32 form")
+    ap.add_argument("--large", type=int, default=1000000, help="large and target: patterns of the scan (1 000 000; "
+                                                                "large: 51 GB of u16 on the host, target: 7.2 GB)")
     ap.add_argument("--scans", type=int, default=64, help="uneven: number of scans")
     ap.add_argument("--entries", type=int, default=65536, help="match: dictionary entries")
     ap.add_argument("--components", type=int, default=512, help="match: values per row (PCA components)")
@@ -937,6 +940,84 @@ def large_main(a):
     print(json.dumps(line), flush=True)
 
 
+def target_main(a):
+    """Indexing and six-unknown refinement of a --large-pattern scan (1 000 000 by default) of
+    60 x 60 u16 patterns (the headline's master and grain map, 7.2 GB on the host): each form
+    (BF16 and plain FP32) timed from the patterns on the host to the refined records, Solver.index
+    (one pass at L = 64 with its 8-iteration refinement) then Solver.refine_patterns over every
+    cell with the adjoint gradient (orientation and pattern centre, Levenberg-Marquardt). Two
+    untimed index passes and one refinement first: the second pass makes the page-locked copy of
+    the scan that the timed runs of both forms upload from. Accuracy: the median misorientation against the simulated
+    orientations after each step, and the two forms against each other."""
+    import torch
+
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import synthetic as syn
+    from zebsdsolve_b200.master import write_npz
+
+    torch.cuda.set_device(0)
+    tmp = tempfile.mkdtemp()
+    sheets = syn.master_sheets(2, side=401, lmax=96, group="432", device="cuda")
+    write_npz(f"{tmp}/m432.npz", sheets, 401, syn.group_matrices("432"), 30)
+    side = int(math.isqrt(a.large))
+    rows = cols = side
+    n = rows * cols
+    s = ze.Solver()
+    s.add_phase(f"{tmp}/m432.npz")
+    s.set_patterns(np.zeros((rows, cols, H, W), np.uint16))
+    s.set_geometry(pc=PC, sample_tilt_deg=70.0, detector_tilt_deg=0.0)
+    e = s._e
+    rng = np.random.default_rng(100)
+    q, _ = syn.grain_map(rng, rows, cols, GRAINS, SPREAD_DEG)
+    pats = np.empty((n, H, W), np.uint16)
+    for i in range(0, n, 16384):
+        c = np.arange(i, min(n, i + 16384))
+        pats[c] = syn.counted_patterns(e.simulate_device(0, c, q[c]), seed=i // 16384).cpu().numpy()
+    s.set_patterns(pats.reshape(rows, cols, H, W))
+    cells = np.arange(n)
+
+    def med(quats):
+        return round(float(np.median(np.degrees(s.disorientation(quats.reshape(-1, 4), q)))), 4)
+
+    out, res = {}, {}
+    for prec in (a.precision, "f32"):
+        s.configure(precision=prec, bandwidth=L, sweeps=1)
+        for _ in range(2):
+            s.index()
+        s.refine_patterns(cells, gradient="adjoint")  # (its buffers and plan made once, untimed)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = s.index()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        g = s.refine_patterns(cells, gradient="adjoint")
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        res[prec] = (r, g)
+        out[prec] = {"value": round(n / (t2 - t0), 1), "index_s": round(t1 - t0, 3), "refine_s": round(t2 - t1, 3),
+                     "index_value": round(n / (t1 - t0), 1), "median_deg_indexed": med(r["quaternions"]),
+                     "median_deg_refined": med(g["quaternions"]), "refine_rounds": int(g["rounds"]),
+                     "mean_ncc_refined": round(float(g["ncc"].mean()), 5)}
+
+    def agree(x, y):
+        d = np.degrees(s.disorientation(x.reshape(-1, 4), y.reshape(-1, 4)))
+        return {"median_deg": round(float(np.median(d)), 5), "within_0.1deg": round(float((d < 0.1).mean()), 5)}
+
+    rb, rf = res[a.precision], res["f32"]
+    line = {"metric": "patterns/s indexed + refined over six unknowns (adjoint), 1M 60x60, 1 B200",
+            "value": out[a.precision]["value"], "unit": "patterns/s", "n_gpus": 1, "steps": 1, "warmup": 2,
+            "higher_is_better": True, "dtype": "bf16+f32", "data": "synthetic",
+            "config": {"workload": f"{rows}x{cols} scan of 60x60 uint16 patterns, {GRAINS} Voronoi grains (0.5 deg "
+                                   "spread), 432 master 401^2 (SH <= 96), L = 64, then Levenberg-Marquardt over "
+                                   "orientation and pattern centre with the adjoint gradient",
+                       "patterns": n, "precision": a.precision},
+            a.precision: out[a.precision], "fp32_form": out["f32"],
+            "vs_fp32_form": round(out[a.precision]["value"] / out["f32"]["value"], 3),
+            "forms_agree": {"indexed": agree(rb[0]["quaternions"], rf[0]["quaternions"]),
+                            "refined": agree(rb[1]["quaternions"], rf[1]["quaternions"])}}
+    print(json.dumps(line), flush=True)
+
+
 def _testdata(*parts):
     """The reference's test data: under $ZEBSDSOLVE_TESTDATA, else tests/data/ (filled by
     tests/golden/copy_testdata.sh); None where absent."""
@@ -1154,5 +1235,7 @@ if __name__ == "__main__":
         nickel_main(args)
     elif args.workload == "match":
         match_main(args)
+    elif args.workload == "target":
+        target_main(args)
     else:
         device_main(args)

@@ -344,7 +344,7 @@ int zeb_det6(int mode, const float* pats, const float* items, int n, const zeb_f
  * solve of planefit.zig:203-233 (the damped Levenberg–Marquardt step of settle). */
 /* zeb_det6 over the frame's masked-pixel list (zeb_mask_list, npix = zeb_mask_pixels entries, at
  * most 51200): 128 threads per pattern keep only the pattern's values in shared memory and
- * recompute each pixel's ray, so that four patterns share an SM; the same outputs. */
+ * recompute each pixel's ray, so that four or five patterns share an SM; the same outputs. */
 int zeb_det6_list(int mode, const float* pats, const float* items, int n, const zeb_frame_t* fr, const uint32_t* list,
                   int npix, const float* vpair, const float* gpair, int side, const float* x, const float* q0,
                   float* out, void* stream);

@@ -55,6 +55,35 @@ def test_pipelined_index_equals_the_step_loop(scan):
     assert np.median(dis) < 0.5
 
 
+def test_refinement_after_an_indexing_run_starts_from_the_kept_patterns(scan):
+    """A whole indexing run keeps its filtered patterns on the device (Engine.keep_prepared); a
+    following refine_patterns starts from them without uploading and filtering again, with the
+    results of a solver that has no kept patterns, bit for bit; a settings change or a new scan
+    drops them."""
+    s, q = _solver(scan)
+    e = s._e
+    e.device_batch = lambda: 40  # three passes, the last one ragged
+    cells = np.arange(96)
+    fresh, _ = _solver(scan)
+    want = fresh.refine_patterns(cells, quaternions=q, gradient="adjoint", rounds=4)
+    assert fresh._e._resident is None
+    s.index()
+    assert e._resident is not None and e._resident["valid"].all()
+    got = s.refine_patterns(cells, quaternions=q, gradient="adjoint", rounds=4)
+    for k in ("quaternions", "shift", "ncc"):
+        assert np.array_equal(got[k], want[k]), k
+    # the kept rows are the filtered patterns: a run of cells as a view, scattered cells gathered
+    for c in (np.arange(10, 50), np.array([90, 3, 41, 7])):
+        kept = e.prepared(c).clone()
+        e._resident["key"] = None
+        assert torch.equal(kept, e.upload(c)[: kept.numel()])
+        e._resident["key"] = e._prep_key()
+    s.configure(dynamic_sigma=0.2)
+    assert e._resident["key"] != e._prep_key()  # (prepared uploads and filters again)
+    s.set_patterns(e.patterns.copy())
+    assert e._resident["key"] is None
+
+
 def test_progress_returning_false_stops_after_a_pass(scan):
     s, _ = _solver(scan)
     s._e.device_batch = lambda: 40

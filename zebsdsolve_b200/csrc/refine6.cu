@@ -2,9 +2,10 @@
 // sample's axes) and the crystal's rotation, and the score they give: the normalized cross-
 // correlation of the pattern with the master projected through them.
 //
-// k_det6<MODE>: one block per pattern. The masked pixels are listed once per block as (c0·row +
-// c1·col + t, pattern value) in shared memory; with the pattern's parameters x = (δt, φ) the block
-// projects every listed pixel, v = u + δt, c = (exp(φ)·q0)·v/|v|, and sums over the pixels:
+// k_det6<MODE>: one block per pattern. The masked pixels are listed once per block as (row, col,
+// pattern value) in shared memory; with the pattern's parameters x = (δt, φ) the block projects
+// every listed pixel, v = c0·row + c1·col + t + δt, c = (exp(φ)·q0)·v/|v| (the frame turned by the
+// rotation once a block), and sums over the pixels:
 //   MODE 0 (forward): n, ΣM, ΣM², ΣM·e → the NCC;
 //   MODE 1 (adjoint): with the exact derivatives D = ∂M/∂x of the forward — the bilinear
 //     lookup's slopes in the sheet, through the square-Lambert map's Jacobian, the rotation and
@@ -215,14 +216,42 @@ __device__ __forceinline__ float master_and_slope(const float2* __restrict__ vp,
   return m;
 }
 
-// one pixel's share of the sums: its ray u (pixels, before the shift), pattern value e
+// Both lookups of MODE 3 from the gradient table alone: its 2 × 2 records' value slots are the
+// sheet's texels, so the bilinear value and its exact slopes (master_and_slope's) come with the
+// table's interpolated gradient (grad_at_pair's), from one map to the square and one pair of loads.
+__device__ __forceinline__ float4 grad_and_slope(const float* __restrict__ gp, float3 c, int side, float3& grad) {
+  const float2 uv = sphere_to_square_fast(c);
+  const float last = (float)(side - 1);
+  const float fj0 = (uv.x + 1.f) * 0.5f * last, fi0 = (uv.y + 1.f) * 0.5f * last;
+  const float fj = fminf(fmaxf(fj0, 0.f), last), fi = fminf(fmaxf(fi0, 0.f), last);
+  const uint32_t cj = min((uint32_t)fj, (uint32_t)(side - 2)), ri = min((uint32_t)fi, (uint32_t)(side - 2));
+  uint32_t o = ri * side + cj;
+  if (c.z < 0.f) o += side * side;
+  const float tj = fj - (float)cj, ti = fi - (float)ri;
+  float4 ta, tb, tc, td;
+  ldg_v8(gp + 8 * (size_t)o, ta, tb);
+  ldg_v8(gp + 8 * ((size_t)o + side), tc, td);
+  const float4 top = lerp4(ta, tb, tj), bot = lerp4(tc, td, tj);
+  const float4 gm = lerp4(top, bot, ti);
+  const float dmj = (fj0 > 0.f && fj0 < last) ? (1.f - ti) * (tb.w - ta.w) + ti * (td.w - tc.w) : 0.f;
+  const float dmi = (fi0 > 0.f && fi0 < last) ? bot.w - top.w : 0.f;
+  float3 dfj, dfi;
+  sheet_jacobian(c, side, dfj, dfi);
+  const float3 g = make_float3(dmj * dfj.x + dmi * dfi.x, dmj * dfj.y + dmi * dfi.y, dmj * dfj.z + dmi * dfi.z);
+  const float r = dot3(g, c);
+  grad = make_float3(g.x - r * c.x, g.y - r * c.y, g.z - r * c.z);
+  return gm;
+}
+
+// One pixel's share of the sums, from its ray already turned by the pattern's rotation R:
+// rv = R·v, v = u + δt (pixels), and its pattern value e. The derivatives along the shift,
+// R⁻¹·∇M/|v|, are summed in the turned frame as ∇M/|v| (det6_unturn takes the sums back once a
+// pattern: R⁻¹ on the vectors, R⁻¹·(·)·R and R⁻¹·(·) on the blocks of products); those along the
+// rotation, c × ∇M, need no turning.
 template <int MODE, int NS>
-__device__ __forceinline__ void det6_pixel(const Det6Args& a, float4 q, float4 qi, float3 dt, float3 u, float e,
-                                           float (&s)[NS]) {
-  const float3 v = make_float3(u.x + dt.x, u.y + dt.y, u.z + dt.z);
-  const float dist = sqrtf(dot3(v, v));
-  const float inv = 1.f / dist;
-  const float3 c = qrot(q, make_float3(v.x * inv, v.y * inv, v.z * inv));
+__device__ __forceinline__ void det6_pixel(const Det6Args& a, float3 rv, float e, float (&s)[NS]) {
+  const float inv = rsqrtf(dot3(rv, rv));  // 1/|v|
+  const float3 c = make_float3(rv.x * inv, rv.y * inv, rv.z * inv);
   float m;
   float d[6], dx[6];
   if (MODE == 0) {
@@ -238,20 +267,16 @@ __device__ __forceinline__ void det6_pixel(const Det6Args& a, float4 q, float4 q
       m = gm.w;
       g = make_float3(gm.x, gm.y, gm.z);
     } else {
-      // the table's value is the sheet's bilinear value at the same place (the same arithmetic)
-      const float4 gm = grad_at_pair(a.gpair, c, a.side);
+      float3 ge;
+      const float4 gm = grad_and_slope(a.gpair, c, a.side, ge);
       m = gm.w;
       g = make_float3(gm.x, gm.y, gm.z);
-      float3 ge;
-      master_and_slope(a.vpair, c, a.side, ge);
-      const float3 we = qrot(qi, ge);
       const float3 re = cross3(c, ge);
-      dx[0] = we.x * inv; dx[1] = we.y * inv; dx[2] = we.z * inv;
+      dx[0] = ge.x * inv; dx[1] = ge.y * inv; dx[2] = ge.z * inv;
       dx[3] = re.x; dx[4] = re.y; dx[5] = re.z;
     }
-    const float3 w = qrot(qi, g);
     const float3 r = cross3(c, g);
-    d[0] = w.x * inv; d[1] = w.y * inv; d[2] = w.z * inv;
+    d[0] = g.x * inv; d[1] = g.y * inv; d[2] = g.z * inv;
     d[3] = r.x; d[4] = r.y; d[5] = r.z;
   }
   s[0] += 1.f;
@@ -280,6 +305,41 @@ __device__ __forceinline__ void det6_pixel(const Det6Args& a, float4 q, float4 q
       s[49 + i] += m * dx[i];
       s[55 + i] += e * dx[i];
     }
+  }
+}
+
+// offset of the product (i, j), i <= j, among the 21 of the GN sums
+__host__ __device__ constexpr int det6_pair(int i, int j) { return 22 + i * 6 - (i * (i - 1)) / 2 + (j - i); }
+
+// the summed shift derivatives back from the turned frame (thread 0, once a pattern): with R's
+// columns r_k = R·e_k, a vector w becomes (r_k · w)_k, the shift × shift block M becomes
+// r_kᵀ·M·r_l, the shift × rotation block N becomes r_kᵀ·N
+template <int MODE, int NS>
+__device__ __forceinline__ void det6_unturn(float4 q, float (&s)[NS]) {
+  if (MODE == 0) return;
+  const float3 r[3] = {qrot(q, make_float3(1.f, 0.f, 0.f)), qrot(q, make_float3(0.f, 1.f, 0.f)),
+                       qrot(q, make_float3(0.f, 0.f, 1.f))};
+  auto vec = [&](int o) {
+    const float3 w = make_float3(s[o], s[o + 1], s[o + 2]);
+    s[o] = dot3(r[0], w); s[o + 1] = dot3(r[1], w); s[o + 2] = dot3(r[2], w);
+  };
+  vec(4); vec(10); vec(16);
+  if (MODE == 3) { vec(43); vec(49); vec(55); }
+  if (MODE >= 2) {
+    float M[3][3], N[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        M[i][j] = s[det6_pair(i < j ? i : j, i < j ? j : i)];
+        N[i][j] = s[det6_pair(i, 3 + j)];
+      }
+    float MR[3][3];  // M·r_l
+    for (int i = 0; i < 3; ++i)
+      for (int l = 0; l < 3; ++l) MR[i][l] = M[i][0] * r[l].x + M[i][1] * r[l].y + M[i][2] * r[l].z;
+    for (int k = 0; k < 3; ++k)
+      for (int l = k; l < 3; ++l)
+        s[det6_pair(k, l)] = r[k].x * MR[0][l] + r[k].y * MR[1][l] + r[k].z * MR[2][l];
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l < 3; ++l) s[det6_pair(k, 3 + l)] = r[k].x * N[0][l] + r[k].y * N[1][l] + r[k].z * N[2][l];
   }
 }
 
@@ -342,11 +402,7 @@ __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
       if (w2 < wid) off += wcnt[w2];
       tot += wcnt[w2];
     }
-    if (m) {
-      const float3 u = make_float3(a.c0.x * row + a.c1.x * col + it.x, a.c0.y * row + a.c1.y * col + it.y,
-                                   a.c0.z * row + a.c1.z * col + it.z);
-      px6[off + __popc(bal & ((1u << lane) - 1u))] = make_float4(u.x, u.y, u.z, __ldg(gpat + i));
-    }
+    if (m) px6[off + __popc(bal & ((1u << lane) - 1u))] = make_float4((float)row, (float)col, 0.f, __ldg(gpat + i));
     npix += tot;
     __syncthreads();
   }
@@ -360,8 +416,10 @@ __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
   }
   __syncthreads();
   const float4 q = sh_q;
-  const float4 qi = make_float4(q.x, -q.y, -q.z, -q.w);
   const float3 dt = sh_t;
+  // the frame turned once: R·v = row·R c0 + col·R c1 + R (t + δt)
+  const float3 rc0 = qrot(q, a.c0), rc1 = qrot(q, a.c1);
+  const float3 rt = qrot(q, make_float3(it.x + dt.x, it.y + dt.y, it.z + dt.z));
   float s[NS];
 #pragma unroll
   for (int k = 0; k < NS; ++k) s[k] = 0.f;
@@ -369,10 +427,13 @@ __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
 #pragma unroll 2
   for (int k = threadIdx.x; k < npix; k += blockDim.x) {
     const float4 p = px6[k];
-    det6_pixel<MODE, NS>(a, q, qi, dt, make_float3(p.x, p.y, p.z), p.w, s);
+    const float3 rv = make_float3(fmaf(rc0.x, p.x, fmaf(rc1.x, p.y, rt.x)), fmaf(rc0.y, p.x, fmaf(rc1.y, p.y, rt.y)),
+                                  fmaf(rc0.z, p.x, fmaf(rc1.z, p.y, rt.z)));
+    det6_pixel<MODE, NS>(a, rv, p.w, s);
   }
   block_sums<NS>(s, red);
   if (threadIdx.x != 0) return;
+  det6_unturn<MODE, NS>(q, s);
   det6_finish<MODE, NS>(a, b, s);
 }
 
@@ -380,8 +441,13 @@ __global__ void __launch_bounds__(256) k_det6(Det6Args a) {
 // threads per pattern keep only the pattern's values along the list in shared memory and
 // recompute each pixel's ray, so that several patterns share an SM (a list of (ray, value) per
 // block fills an SM's shared memory for one 120 × 120 pattern).
+// (the one-pass mode: five blocks an SM at 96 registers, one pixel a thread at a time, measured
+// 11 % faster than four blocks with two pixels in flight: the table loads' latency is hidden by
+// the warps rather than by unrolling; the other modes keep four blocks, which mode 2's smooth
+// kernels need to run without spilling)
 template <int MODE>
-__global__ void __launch_bounds__(128, 4) k_det6_list(Det6Args a, const uint32_t* __restrict__ list, int npix) {
+__global__ void __launch_bounds__(128, MODE == 3 ? 5 : 4) k_det6_list(Det6Args a, const uint32_t* __restrict__ list,
+                                                                     int npix) {
   constexpr int NS = MODE == 0 ? 4 : (MODE == 1 ? 22 : (MODE == 2 ? 43 : 61));
   extern __shared__ float pv6[];
   __shared__ float red[NS * 4];
@@ -404,21 +470,30 @@ __global__ void __launch_bounds__(128, 4) k_det6_list(Det6Args a, const uint32_t
   }
   __syncthreads();
   const float4 q = sh_q;
-  const float4 qi = make_float4(q.x, -q.y, -q.z, -q.w);
   const float3 dt = sh_t;
+  // the frame turned once: R·v = row·R c0 + col·R c1 + R (t + δt)
+  const float3 rc0 = qrot(q, a.c0), rc1 = qrot(q, a.c1);
+  const float3 rt = qrot(q, make_float3(it.x + dt.x, it.y + dt.y, it.z + dt.z));
   float s[NS];
 #pragma unroll
   for (int k = 0; k < NS; ++k) s[k] = 0.f;
-#pragma unroll 2
-  for (int k = threadIdx.x; k < npix; k += blockDim.x) {
+  auto pixel = [&](int k) {
     const uint32_t v = __ldg(list + k);
     const float row = (float)(int)(v >> 16), col = (float)(int)(v & 0xffffu);
-    const float3 u = make_float3(a.c0.x * row + a.c1.x * col + it.x, a.c0.y * row + a.c1.y * col + it.y,
-                                 a.c0.z * row + a.c1.z * col + it.z);
-    det6_pixel<MODE, NS>(a, q, qi, dt, u, pv6[k], s);
+    const float3 rv = make_float3(fmaf(rc0.x, row, fmaf(rc1.x, col, rt.x)), fmaf(rc0.y, row, fmaf(rc1.y, col, rt.y)),
+                                  fmaf(rc0.z, row, fmaf(rc1.z, col, rt.z)));
+    det6_pixel<MODE, NS>(a, rv, pv6[k], s);
+  };
+  if constexpr (MODE == 3) {
+#pragma unroll 1
+    for (int k = threadIdx.x; k < npix; k += blockDim.x) pixel(k);
+  } else {
+#pragma unroll 2
+    for (int k = threadIdx.x; k < npix; k += blockDim.x) pixel(k);
   }
   block_sums<NS>(s, red);
   if (threadIdx.x != 0) return;
+  det6_unturn<MODE, NS>(q, s);
   det6_finish<MODE, NS>(a, b, s);
 }
 

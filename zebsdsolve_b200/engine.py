@@ -172,6 +172,8 @@ class Engine:
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
         self.counts = {"submits": 0, "reads": 0, "waits": 0}  # device passes, readbacks, host waits
         self._full = False  # at_full: the stored size is the level being worked at
+        self._resident = None  # the scan's filtered patterns a whole pass kept on the device (prepared)
+        self._whole_pass = False  # an indexing run over the scan is under way (its batches are kept)
         self.geo_given = Geometry()  # the geometry as given (set_geometry), where a full fit starts
         self._nl_view = None  # what averaging with neighbours did to the last pattern looked at
         self._nl_report = False  # log what the averaging did to the next batch (an indexing run's first)
@@ -213,6 +215,8 @@ class Engine:
         self.told_no_background = False
         self._pinned = None
         self._index_calls = 0
+        if self._resident is not None:
+            self._resident["key"] = None  # (its buffer is kept for the next scan, as the page-locked one)
         rows, cols = a.shape[:2]
         self.avg = None
         self.chance_key = None
@@ -810,6 +814,58 @@ class Engine:
         run(cur, 2, h, w, 1.0, None, 0, 0.0, 1, out)
         return out
 
+    RESIDENT_FRAC = 0.25  # of the device's memory: the most the kept filtered scan may take
+
+    def _prep_key(self):
+        """What the filter chain's output depends on: the scan, every setting, the level."""
+        return (self.patterns.shape, self.set.to_json(), self._full, self.pattern_shape(), self.factor())
+
+    def keep_prepared(self, pats, cells):
+        """A whole pass's filtered patterns kept on the device, the scan's rows [cell][h·w] in FP32,
+        where the scan fits RESIDENT_FRAC of the device's memory: what refine_patterns then starts
+        from without uploading and filtering the patterns again (prepared)."""
+        rows, cols = self.info()[:2]
+        h, w = self.pattern_shape()
+        total = rows * cols * h * w
+        key = self._prep_key()
+        r = self._resident
+        if r is None or r["key"] != key:
+            if total * 4 > self.RESIDENT_FRAC * torch.cuda.get_device_properties(self.dev).total_memory:
+                self._resident = None
+                return
+            old = r["pats"] if r is not None and r["pats"].numel() >= total else None
+            self._resident = None
+            r = {"key": key, "pats": old if old is not None else torch.empty(total, dtype=torch.float32, device=self.dev),
+                 "valid": np.zeros(rows * cols, bool)}
+            self._resident = r
+        n = len(cells)
+        view = r["pats"][:total].view(rows * cols, h * w)
+        src = pats[: n * h * w].view(n, h * w)
+        c = np.asarray(cells, np.int64)
+        if n and c[-1] - c[0] == n - 1 and (n == 1 or (np.diff(c) == 1).all()):
+            view[int(c[0]):int(c[0]) + n].copy_(src)
+        else:
+            view.index_copy_(0, torch.as_tensor(c, device=self.dev), src)
+        r["valid"][c] = True
+
+    def prepared(self, cells):
+        """The cells' patterns as the filter chain leaves them: the rows a whole pass kept on the
+        device (keep_prepared) where they hold every cell under the current settings, a view for a
+        run of consecutive cells; else uploaded and filtered (upload)."""
+        r = self._resident
+        c = np.asarray(cells, np.int64)
+        n = len(c)
+        if r is not None and n and r["key"] == self._prep_key() and r["valid"][c].all():
+            rows, cols = self.info()[:2]
+            h, w = self.pattern_shape()
+            view = r["pats"][: rows * cols * h * w].view(rows * cols, h * w)
+            if c[-1] - c[0] == n - 1 and (n == 1 or (np.diff(c) == 1).all()):
+                return view[int(c[0]):int(c[0]) + n].reshape(-1)
+            out = self.buf("pats_kept", n * h * w)[: n * h * w].view(n, h * w)
+            torch.index_select(view, 0, torch.as_tensor(c, device=self.dev), out=out)
+            return out.reshape(-1)
+        return self.upload(cells)
+
     def upload(self, cells):
         """The cells' stored patterns to the device (from the pinned scan), preprocessed."""
         rows, cols, h, w = self.info()
@@ -900,7 +956,11 @@ class Engine:
     def items_of(self, cells):
         cells = np.asarray(cells, np.int64)
         t = self.positions(cells)
-        self._batch_t = (t.min(0), t.max(0)) if len(t) else None
+        if len(t):
+            tt = np.ascontiguousarray(t.T)  # (a reduction along the long axis of a contiguous array)
+            self._batch_t = (tt.min(1), tt.max(1))
+        else:
+            self._batch_t = None
         return self.to_device("items", np.concatenate([t, np.arange(len(cells), dtype=np.float32)[:, None]], 1))
 
     def spans(self, bt, fr):
@@ -939,6 +999,8 @@ class Engine:
         mark = timer.mark if timer is not None else (lambda name: None)
         mark("prep")
         pats = self.preprocess(raw, n, cells)
+        if self._whole_pass:
+            self.keep_prepared(pats, cells)
         items = self.items_of(cells)
         self.batch_stamp = self.batch_stamp % (1 << 24) + 1
         bt = b["tables"]
@@ -1026,6 +1088,8 @@ class Engine:
         mark = timer.mark if timer is not None else (lambda name: None)
         mark("prep")
         pats = self.preprocess(raw, n, cells)
+        if self._whole_pass:
+            self.keep_prepared(pats, cells)
         items = self.items_of(cells)
         self.batch_stamp = self.batch_stamp % (1 << 24) + 1
         recs = self.buf("recs", n_ph * n * 8)
@@ -1126,7 +1190,7 @@ class Engine:
             slot[1].synchronize()  # the copy that last read this slot has finished
         return slot
 
-    FILL_PART = 8 << 20
+    FILL_PART = 4 << 20
 
     def _fill(self, host, src):
         """host[:] = src (a staging slot from the stored scan) in parts of FILL_PART bytes on a
@@ -1147,7 +1211,7 @@ class Engine:
             import concurrent.futures as cf
             import os
 
-            self._pool_n = max(1, min(8, (os.cpu_count() or 2) // 2))
+            self._pool_n = max(1, min(16, (os.cpu_count() or 2) - 2))
             self._pool = cf.ThreadPoolExecutor(self._pool_n, thread_name_prefix="zeb-fill")
         return self._pool_n
 
@@ -1205,7 +1269,7 @@ class Engine:
             q0 = self.res["quat"][cells].astype(np.float64)
         else:
             q0 = np.asarray(quaternions, np.float64).reshape(n, 4)
-        pats = self.upload(cells)
+        pats = self.prepared(cells)
         items = self.items_of(cells)
         fr = self.frame()
         _, sheets, grad, vpair, gpair = self.phases[phase].baked
@@ -1218,9 +1282,10 @@ class Engine:
         most = int(s["plane_iters"] if rounds is None else rounds)
         q, shift, ncc, it = adjoint.refine6(plan, torch.as_tensor(q0, device=self.dev), trust_px, most, gradient)
         J = adjoint.pc_jacobian(self.geo, h, w)
-        sh = shift.cpu().numpy()
-        dpc = np.linalg.solve(J, sh.T).T
-        return {"quaternions": q.cpu().numpy(), "shift": sh, "pc": self.geo.pc[None, :] + dpc,
+        # the pattern centres on the device: pc = pc0 + J⁻¹·shift for every pattern
+        Ji = torch.as_tensor(np.linalg.inv(J).T, dtype=torch.float64, device=self.dev)
+        pc = torch.as_tensor(self.geo.pc[None, :], dtype=torch.float64, device=self.dev) + shift @ Ji
+        return {"quaternions": q.cpu().numpy(), "shift": shift.cpu().numpy(), "pc": pc.cpu().numpy(),
                 "ncc": ncc.cpu().numpy(), "rounds": int(it)}
 
     def fz_of(self, recs):
@@ -1545,7 +1610,11 @@ class Engine:
         bw, dg, method = s.sweep(self.index_sweep)
         # a scan stepped through once is one pass: only the first step of the first sweep counts
         first = self.index_done == 0 and self.index_sweep == 0
-        recs = self.index_cells(cells, bw, method, dg, whole_pass=first)
+        self._whole_pass = True
+        try:
+            recs = self.index_cells(cells, bw, method, dg, whole_pass=first)
+        finally:
+            self._whole_pass = False
         self.land(cells, recs, self._last_fz)
         self.next_sweep(bw)
         return len(self.index_cells_list) - self.index_done
@@ -1572,6 +1641,14 @@ class Engine:
         index_step calls, with uploads, kernels, readbacks and landing overlapped."""
         s = self.set
         self._index_calls += 1
+        self._whole_pass = True
+        try:
+            self._index_sweeps(progress)
+        finally:
+            self._whole_pass = False
+
+    def _index_sweeps(self, progress):
+        s = self.set
         while len(self.index_cells_list) - self.index_done > 0 and not self.cancel:
             bw, dg, method = s.sweep(self.index_sweep)
             stop = [False]
