@@ -191,10 +191,11 @@ struct TcShared {
   int failed;
 };
 
-// The FP16 form: K' <= 256 (split <= 16 at L <= 64), so 4 B blocks and 4 A stages; the drain
+// The FP16 form: K' <= 256 (split <= 16 at L <= 64), so 4 B blocks; 6 A stages (a tile of the
+// low orders takes 4, so the next tile's loads start while its MMAs run; 225 KB in all); the drain
 // stages a whole tile (128 rows × 128 items in FP16: two 16 KB store boxes) at once, two tiles deep.
 constexpr int TCH_MAX_KB = 4;
-constexpr int TCH_STAGES = 4;
+constexpr int TCH_STAGES = 6;
 constexpr int TCH_BOX = 64 * TC_BM * 2;  // bytes of one store box: 64 items × 128 rows
 struct TcSharedH {
   uint8_t b[TCH_MAX_KB][TC_B_BLOCK];   // 64 KB, 1024-aligned
@@ -350,7 +351,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_spectrum_tc(TcArgs a, const _
         // to the MMAs, FP16 rows into the tile's staging buffer, two 16 KB tensor stores; the
         // buffer of two tiles back has been read by its stores (the last group may still read)
         const int acc = mt & 1;
-        if (!bar_and(1, 128, leader ? mbar_wait_sleep(&s.acc_full[acc], (mt >> 1) & 1, lim) : true)) {
+        // the leader polls (no backoff: a sleep would outlast the MMAs of a tile), the others wait at
+        // the barrier
+        if (!bar_and(1, 128, leader ? mbar_wait(&s.acc_full[acc], (mt >> 1) & 1, lim) : true)) {
           if (leader) {
             atomicOr(a.status, 4);
             s.failed = 1;

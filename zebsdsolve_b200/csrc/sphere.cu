@@ -274,11 +274,9 @@ __device__ __forceinline__ void fft_reg8(float2 (&x)[8]) {
 // its ring whole), the transforms sample again, from the pattern in global memory.
 // Each warp takes one ring pair with samples at a time: it zeroes its 256-point line, fills the
 // northern ring (real part) and its mirror (imaginary part) over their spans, and transforms the
-// line with no block barrier: lane l holds points l + 32k (k < 8), takes the 8-point DFT over k in
-// registers, multiplies by e^{−2πi l k₁/256}, then the 32-point DFT over the lanes by five radix-2
-// stages of shuffles (decimation in frequency, so lane l ends with output bit-reverse(l)); the
-// outputs go back to the line (a padded order without bank conflicts) and the lanes split N and S
-// for m < L.  Spectra are written [item][m][ring pair].
+// line with no block barrier, in three register steps with the line between them (8-point DFTs
+// over the stride-32 points, 8-point DFTs of the 32-point transforms' quarters, their 4-point sums,
+// only for the orders kept), and the lanes split N and S for m < L.  Spectra are written [item][m][ring pair].
 constexpr int RW_WARPS = 8;
 constexpr int RW_PAD = 256 + 32;  // line slots per warp: F + F/8
 constexpr int RW_CACHE = 7168;    // cached samples (28 KB): the spans of a 60 × 60 or 80 × 80 frame
@@ -388,14 +386,14 @@ __global__ void __launch_bounds__(RW_WARPS * 32) k_sphere_rings_w(SphereArgs a) 
     if (sp[y].y == 0 && sp[nt - 1 - y].y == 0) outb[e] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
 
-  // this lane's twiddles: e^{−2πi l k₁/256} (k₁ < 8) and, per shuffle stage h, e^{−2πi (l mod h)/(2h)}
-  float2 tw8[8], tws[5];
+  // this lane's twiddles: e^{−2πi l k/256} (the 256-point step, l = lane) and e^{−2πi a c/32}
+  // (the 32-point step, a = lane mod 4), k, c < 8
+  float2 tw8[8], tw32[8];
+  const int grp = lane >> 2, qa = lane & 3;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) tw8[k] = __ldg(a.tw + ((lane * k * 4) & (ZEB_TW_LEN - 1)));
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    const int h = 16 >> q;
-    tws[q] = __ldg(a.tw + (lane & (h - 1)) * (ZEB_TW_LEN / (2 * h)));
+  for (int k = 0; k < 8; ++k) {
+    tw8[k] = __ldg(a.tw + ((lane * k * 4) & (ZEB_TW_LEN - 1)));
+    tw32[k] = __ldg(a.tw + ((qa * k * (ZEB_TW_LEN / 32)) & (ZEB_TW_LEN - 1)));
   }
   float2* buf = lines + warp * RW_PAD;
   const int na = n_act;
@@ -439,29 +437,49 @@ __global__ void __launch_bounds__(RW_WARPS * 32) k_sphere_rings_w(SphereArgs a) 
       }
     }
     __syncwarp();
+    // X[m] = Σ_j x[j] W^{jm} (W = e^{−2πi/256}) with j = j1 + 32 j2, m = m2 + 8 m1:
+    // (1) lane j1: the 8-point DFTs over j2, × W^{j1 m2} → Z[j1][m2] (to the line, 9 a row);
+    // (2) lane (m2, a) of the 8 groups of 4: with j1 = a + 4b and m1 = c + 8d, the 8-point DFT over
+    //     b of Z[a + 4b][m2], × e^{−2πi a c/32} → V[m2][a][c] (to the line);
+    // (3) lane (m2, a) finishes c = 2a, 2a + 1: the 4-point sums over a for d = 0 and d = 3 only,
+    //     m = m2 + 8c + 64d: the orders m < 64 and 256 − m the split below reads (n_φ = 256 means
+    //     L ≤ 64), written at rw_slot(m)
     float2 x[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) x[k] = buf[lane + 32 * k];
     fft_reg8(x);
 #pragma unroll
     for (int k = 1; k < 8; ++k) x[k] = cmulf(x[k], tw8[k]);
-    // the 32-point transforms over the lanes, decimation in frequency
+    __syncwarp();
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      const int h = 16 >> q;
-      const bool upper = (lane & h) != 0;
+    for (int k = 0; k < 8; ++k) buf[lane * 9 + k] = x[k];
+    __syncwarp();
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const float2 u = make_float2(__shfl_xor_sync(0xffffffffu, x[k].x, h), __shfl_xor_sync(0xffffffffu, x[k].y, h));
-        const float2 sum = make_float2(x[k].x + u.x, x[k].y + u.y);
-        const float2 dif = cmulf(make_float2(u.x - x[k].x, u.y - x[k].y), tws[q]);
-        x[k] = upper ? dif : sum;
-      }
+    for (int b = 0; b < 8; ++b) x[b] = buf[(qa + 4 * b) * 9 + grp];
+    fft_reg8(x);
+#pragma unroll
+    for (int c = 1; c < 8; ++c) x[c] = cmulf(x[c], tw32[c]);
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 8; ++c) buf[(grp * 4 + qa) * 9 + c] = x[c];
+    __syncwarp();
+    float2 o0[2], o3[2];
+#pragma unroll
+    for (int hh = 0; hh < 2; ++hh) {
+      const int c = 2 * qa + hh;
+      const float2 v0 = buf[(grp * 4 + 0) * 9 + c], v1 = buf[(grp * 4 + 1) * 9 + c];
+      const float2 v2 = buf[(grp * 4 + 2) * 9 + c], v3 = buf[(grp * 4 + 3) * 9 + c];
+      o0[hh] = make_float2(v0.x + v1.x + v2.x + v3.x, v0.y + v1.y + v2.y + v3.y);
+      // d = 3: the weights e^{−2πi 3a/4} = 1, i, −1, −i
+      o3[hh] = make_float2(v0.x - v1.y - v2.x + v3.y, v0.y + v1.x - v2.y - v3.x);
     }
     __syncwarp();
-    const int r = (int)(__brev((unsigned)lane) >> 27);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) buf[rw_slot(k + 8 * r)] = x[k];
+    for (int hh = 0; hh < 2; ++hh) {
+      const int m = grp + 8 * (2 * qa + hh);
+      buf[rw_slot(m)] = o0[hh];
+      buf[rw_slot(m + 192)] = o3[hh];
+    }
     __syncwarp();
     // the two apart: Z = N + iS for real N, S gives N_m = (Z_m + conj Z_{n−m})/2 and
     // S_m = (Z_m − conj Z_{n−m})/2i; keep (N+S, N−S) for m < L
