@@ -367,6 +367,7 @@ def device_main(a):
 
     clk = Clocks(local)
     ms, ems, launches, stages, r = time_form(a.precision, clk, nvtx=True)
+    u_half = e.bands[L]["phases"][0][1].u_scale is not None  # the timed form keeps U in FP16
     value = n * world / (ms / 1e3)
     e2e = n / (ems / 1e3)  # one scan's patterns over the job's time (all of it on one rank, or sharded)
     fp32 = None
@@ -392,7 +393,7 @@ def device_main(a):
     # algorithmic HBM bytes of each stage per pattern (its kernels' compulsory reads and writes):
     # U, the spectrum, is complex FP32 (8 bytes a value) in the FP32 form and complex FP16 (4) in
     # the BF16 form
-    u_bytes = d.nb * d.L * d.nc * (4 if ph.u_scale is not None else 8)
+    u_bytes = d.nb * d.L * d.nc * (4 if u_half else 8)
     algo = {"prep": H * W * (2 + 4),                       # u16 in, f32 out
             "sphere": H * W * 4 + d.n_pairs * 8,           # pattern in, coefficients out
             "spectrum": d.n_pairs * 8 + u_bytes,           # coefficients in, U out
