@@ -658,11 +658,34 @@ __global__ void __launch_bounds__(RL_THREADS, 6) k_refine_list(DetArgs a, const 
       s[13] += d.x * d.x; s[14] += d.y * d.y; s[15] += d.z * d.z;
       s[16] += d.x * d.y; s[17] += d.x * d.z; s[18] += d.y * d.z;
     }
-    // each warp's sums, then warp 0 alone adds the warps' (lane k: sum k) and takes the step
+    // each warp's sums (16 of them by a transposing reduction: each exchange halves the values a
+    // lane holds, so lane pair i ends with sum 1 + i's total in 16 shuffles instead of 80), then
+    // warp 0 alone adds the warps' (lane k: sum k) and takes the step
+    {
+      float v[8];
 #pragma unroll
-    for (int k = 1; k < 19; ++k) {
-      const float w = warp_sum(s[k]);
-      if (lane == 0) red[k * NW + wid] = w;
+      for (int i = 0; i < 8; ++i) {
+        const bool up = (lane & 16) != 0;
+        const float send = up ? s[1 + i] : s[9 + i];
+        v[i] = (up ? s[9 + i] : s[1 + i]) + __shfl_xor_sync(0xffffffffu, send, 16);
+      }
+#pragma unroll
+      for (int o = 8, n = 4; o >= 2; o >>= 1, n >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int i = 0; i < n; ++i) {
+          const float send = up ? v[i] : v[i + n];
+          v[i] = (up ? v[i + n] : v[i]) + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+      }
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+      const int idx = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+      if ((lane & 1) == 0) red[(1 + idx) * NW + wid] = v[0];
+      const float w17 = warp_sum(s[17]), w18 = warp_sum(s[18]);
+      if (lane == 0) {
+        red[17 * NW + wid] = w17;
+        red[18 * NW + wid] = w18;
+      }
     }
     __syncthreads();
     if (wid == 0) {
