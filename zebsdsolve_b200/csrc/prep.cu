@@ -284,11 +284,12 @@ __global__ void __launch_bounds__(256) k_prep(PrepArgs a) {
 // the left, at least R + 14 on the right, pw odd so that rows at stride pw fall in different
 // banks) and the zero-padded row-blurred image Q[R + h + R + 16][w].  A thread takes eight
 // consecutive outputs along the blur's direction and walks the taps eight at a time: eight taps
-// and the fifteen inputs they reach go into registers, then 64 FMAs, so a shared load serves
-// several FMAs (the taps beyond 2R are zeros, adding exact zeros).  Each output sums its taps in
-// increasing order with fmaf, the order of k_prep, so the results are the same bits; the taps
-// inside the image are summed once per column and per row for the edge renormalization.
-constexpr int PD_OUT = 8;
+// (two 16-byte loads) and the 23 inputs they reach go into registers, then 128 FMAs, so a shared
+// load serves several FMAs (the taps beyond 2R are zeros, adding exact zeros).  Each output sums
+// its taps in increasing order with fmaf, the order of k_prep, so the results are the same bits;
+// the taps inside the image are summed once per column and per row for the edge renormalization.
+constexpr int PD_OUT = 16;  // outputs a thread takes along the blur
+constexpr int PD_TB = 8;    // taps a step
 
 __host__ __device__ inline int pd_pw(int w, int R) { return ((w + 2 * R + 2 * PD_OUT) | 1); }
 __host__ __device__ inline int pd_qrows(int h, int R) { return h + 2 * R + 2 * PD_OUT; }
@@ -298,17 +299,17 @@ __host__ __device__ inline size_t pd_smem(int h, int w, int R) {
 
 __global__ void __launch_bounds__(256) k_prep_direct(PrepArgs a) {
   extern __shared__ float sm[];
-  __shared__ float taps[128 + PD_OUT];
+  __shared__ __align__(16) float taps[128 + PD_TB];
   __shared__ float gsum[2][512];  // Σ taps inside the image, per column and per row
   __shared__ float red[2 * 8];
   const int b = blockIdx.x;
   const int h = a.h, w = a.w, hw = h * w, R = a.radius;
   const int pw = pd_pw(w, R), qr = pd_qrows(h, R);
-  const int ntap = 2 * R + 1, nblk = (ntap + PD_OUT - 1) / PD_OUT;
+  const int ntap = 2 * R + 1, nblk = (ntap + PD_TB - 1) / PD_TB;
   float* P = sm;           // [h][pw], the image at columns R … R + w − 1
   float* Q = P + h * pw;   // [qr][w], the row-blurred image at rows R … R + h − 1
   const size_t base = (size_t)b * hw;
-  for (int d = threadIdx.x; d < nblk * PD_OUT; d += blockDim.x) {
+  for (int d = threadIdx.x; d < nblk * PD_TB; d += blockDim.x) {
     const int dd = abs(d - R);
     taps[d] = d < ntap ? expf(-(float)(dd * dd) * a.k0) : 0.f;
   }
@@ -336,14 +337,15 @@ __global__ void __launch_bounds__(256) k_prep_direct(PrepArgs a) {
     float acc[PD_OUT];
 #pragma unroll
     for (int k = 0; k < PD_OUT; ++k) acc[k] = 0.f;
-    for (int d0 = 0; d0 < nblk * PD_OUT; d0 += PD_OUT) {
-      float tv[PD_OUT], x[2 * PD_OUT - 1];
+    for (int d0 = 0; d0 < nblk * PD_TB; d0 += PD_TB) {
+      float x[PD_OUT + PD_TB - 1];
+      const float4 ta = *reinterpret_cast<const float4*>(taps + d0);
+      const float4 tb = *reinterpret_cast<const float4*>(taps + d0 + 4);
+      const float tv[PD_TB] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
 #pragma unroll
-      for (int k = 0; k < PD_OUT; ++k) tv[k] = taps[d0 + k];
+      for (int k = 0; k < PD_OUT + PD_TB - 1; ++k) x[k] = src[d0 + k];
 #pragma unroll
-      for (int k = 0; k < 2 * PD_OUT - 1; ++k) x[k] = src[d0 + k];
-#pragma unroll
-      for (int dd = 0; dd < PD_OUT; ++dd)
+      for (int dd = 0; dd < PD_TB; ++dd)
 #pragma unroll
         for (int k = 0; k < PD_OUT; ++k) acc[k] = fmaf(tv[dd], x[k + dd], acc[k]);
     }
@@ -361,14 +363,15 @@ __global__ void __launch_bounds__(256) k_prep_direct(PrepArgs a) {
     float acc[PD_OUT];
 #pragma unroll
     for (int k = 0; k < PD_OUT; ++k) acc[k] = 0.f;
-    for (int d0 = 0; d0 < nblk * PD_OUT; d0 += PD_OUT) {
-      float tv[PD_OUT], x[2 * PD_OUT - 1];
+    for (int d0 = 0; d0 < nblk * PD_TB; d0 += PD_TB) {
+      float x[PD_OUT + PD_TB - 1];
+      const float4 ta = *reinterpret_cast<const float4*>(taps + d0);
+      const float4 tb = *reinterpret_cast<const float4*>(taps + d0 + 4);
+      const float tv[PD_TB] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
 #pragma unroll
-      for (int k = 0; k < PD_OUT; ++k) tv[k] = taps[d0 + k];
+      for (int k = 0; k < PD_OUT + PD_TB - 1; ++k) x[k] = src[(d0 + k) * w];
 #pragma unroll
-      for (int k = 0; k < 2 * PD_OUT - 1; ++k) x[k] = src[(d0 + k) * w];
-#pragma unroll
-      for (int dd = 0; dd < PD_OUT; ++dd)
+      for (int dd = 0; dd < PD_TB; ++dd)
 #pragma unroll
         for (int k = 0; k < PD_OUT; ++k) acc[k] = fmaf(tv[dd], x[k + dd], acc[k]);
     }
