@@ -321,6 +321,11 @@ int zeb_chance(const float* pats, const float* items, int n, int draws, const ze
  * w >= 0, ties within 1e-12 keeping the first, in FP64 rounded once to FP32. The landing's
  * reduction (engine.zig:2392-2419 with sym.zig:120-131), moved from the host to the device. */
 int zeb_records_fz(const float* records, int n, const double* ops, int n_ops, float* fz, void* stream);
+/* zeb_records_fz with each reduced orientation's Bunge angles too: bunge[b] = (φ1, Φ, φ2) in radians
+ * ([0, 2π), [0, π], [0, 2π)) of the FP32 quaternion fz[b], by the formulas of rot.zig:151-173 in
+ * FP64 rounded once to FP32 — the landing's conversion (engine.zig:2392-2419), moved to the device. */
+int zeb_records_fz_bunge(const float* records, int n, const double* ops, int n_ops, float* fz, float* bunge,
+                         void* stream);
 
 /* Six unknowns per item: x[b] = (δt: the rays' origin moved, 3 floats in pixels, sample axes;
  * φ: a rotation vector applied on the left of q0[b], radians), the detector projection

@@ -426,6 +426,38 @@ def test_records_fz_equals_the_host_reduction(lib, kind):
     assert np.array_equal(fz.cpu().numpy().reshape(-1, 4), want)
 
 
+@pytest.mark.parametrize("kind", ["o", "d6"])
+def test_records_bunge_equal_the_host_conversion(lib, kind):
+    """zeb_records_fz_bunge: the same zone orientations as zeb_records_fz, and their Bunge angles as
+    the host's landing converts them (rotations.to_bunge in FP64, rounded to FP32): equal bits but
+    where the device's atan2 (within 2 ulp of FP64) and the host's round across an FP32 boundary,
+    never more than one FP32 ulp; the poles of the Bunge chart (Φ = 0 or π) included."""
+    from zebsdsolve_b200 import rotations as R
+
+    rng = np.random.default_rng(13)
+    ops = R.group(kind)
+    q = rng.normal(size=(6000, 4))
+    q[:100, 1:3] = 0.0  # Φ = 0: x = y = 0
+    q[100:200, [0, 3]] = 0.0  # Φ = π: w = z = 0
+    q[200:300, 1:3] *= 1e-9  # near the pole
+    recs = np.zeros((len(q), 8), np.float32)
+    recs[:, :4] = q.astype(np.float32)
+    rd = torch.as_tensor(recs, device="cuda")
+    od_ = torch.as_tensor(ops, device="cuda")
+    fz = torch.empty(len(q) * 4, device="cuda")
+    fz2 = torch.empty(len(q) * 4, device="cuda")
+    bg = torch.empty(len(q) * 3, device="cuda")
+    lib.call("zeb_records_fz", P(rd), len(q), P(od_), len(ops), P(fz), sp())
+    lib.call("zeb_records_fz_bunge", P(rd), len(q), P(od_), len(ops), P(fz2), P(bg), sp())
+    f = fz.cpu().numpy().reshape(-1, 4)
+    assert np.array_equal(f, fz2.cpu().numpy().reshape(-1, 4))
+    got = bg.cpu().numpy().reshape(-1, 3)
+    want = R.to_bunge(f.astype(np.float64)).astype(np.float32)
+    ulp = np.spacing(np.abs(want).astype(np.float32))
+    assert np.all(np.abs(got - want) <= ulp), np.abs(got - want).max()
+    assert (got == want).mean() >= 0.999
+
+
 @pytest.mark.parametrize("entry", ["zeb_refine", "zeb_refine_list", "zeb_refine_list_h"])
 def test_refine_and_nmi_match_oracle(world, lib, entry):
     """The refinement kernels (pixels compacted per block; the frame's shared pixel list, 128

@@ -87,6 +87,7 @@ _SIGS = {
     "zeb_refine": ([P, P, P, c_int, c_int, ctypes.POINTER(Frame), P, P, c_int, ctypes.POINTER(RefineOpts), P, P], c_int),
     "zeb_chance": ([P, P, c_int, c_int, ctypes.POINTER(Frame), P, c_int, c_int, P, P], c_int),
     "zeb_records_fz": ([P, c_int, P, c_int, P, P], c_int),
+    "zeb_records_fz_bunge": ([P, c_int, P, c_int, P, P, P], c_int),
     "zeb_det6": ([c_int, P, P, c_int, ctypes.POINTER(Frame), P, P, c_int, P, P, P, P], c_int),
     "zeb_det6_list": ([c_int, P, P, c_int, ctypes.POINTER(Frame), P, c_int, P, P, c_int, P, P, P, P], c_int),
     "zeb_solve6": ([P, P, c_int, P, P, P], c_int),
@@ -120,7 +121,7 @@ ZEB_PEAKS_STATIC_SLABS = 1 << 19  # include/zebsdsolve_b200.h
 # kernels each entry point launches (for the launch counts the benchmark reports)
 KERNELS = {"zeb_nlpar": 5, "zeb_pc_splat": 0, "zeb_sums6_list": 1, "zeb_clahe": 4, "zeb_combine": 1, "zeb_master_symmetrize": 1, "zeb_prep": 1, "zeb_prep_ex": 1, "zeb_prep_reduced": 1, "zeb_sphere_coefficients": 3, "zeb_sphere_coefficients_spans": 3, "zeb_sphere_spans": 1, "zeb_spectrum_f32": 1,
            "zeb_spectrum_bf16": 2, "zeb_tc_pack_master": 0, "zeb_correlate_peaks": 2, "zeb_correlate_peaks_static": 2, "zeb_spectrum_bf16_h": 2, "zeb_correlate_peaks_h": 2, "zeb_master_quads": 1, "zeb_refine_list_h": 1, "zeb_pack_panel_split": 1, "zeb_project_bf16": 1, "zeb_project_f32": 1, "zeb_correlate_volume": 1, "zeb_rden_build": 1,
-           "zeb_refine": 1, "zeb_chance": 1, "zeb_project": 1, "zeb_records_fz": 1, "zeb_det6": 1, "zeb_det6_list": 1, "zeb_solve6": 1, "zeb_pack_panel": 1, "zeb_mask_list": 1, "zeb_refine_list": 1, "zeb_dict_sims": 1, "zeb_match_bf16": 1, "zeb_match_f32": 1, "zeb_match_best": 1, "zeb_master_blur_pass": 1, "zeb_master_gradient": 1, "zeb_master_pairs": 1,
+           "zeb_refine": 1, "zeb_chance": 1, "zeb_project": 1, "zeb_records_fz": 1, "zeb_records_fz_bunge": 1, "zeb_det6": 1, "zeb_det6_list": 1, "zeb_solve6": 1, "zeb_pack_panel": 1, "zeb_mask_list": 1, "zeb_refine_list": 1, "zeb_dict_sims": 1, "zeb_match_bf16": 1, "zeb_match_f32": 1, "zeb_match_best": 1, "zeb_master_blur_pass": 1, "zeb_master_gradient": 1, "zeb_master_pairs": 1,
            "zeb_master_sample_grid": 1, "zeb_gauss_legendre": 1, "zeb_legendre_table": 1, "zeb_wigner_half_pi": 1,
            "zeb_correlation_table": 1}
 launches = {"count": 0}

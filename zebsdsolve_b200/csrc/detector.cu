@@ -491,8 +491,40 @@ __device__ __forceinline__ double4 qmul_d(double4 a, double4 b) {
   return make_double4(w, x, y, z);
 }
 
+// Bunge angles (φ1, Φ, φ2), radians in [0, 2π) × [0, π] × [0, 2π), of a quaternion (rot.zig:151-173):
+// standardized, then the host's formulas in FP64 with every product, sum and quotient rounded
+// on its own in the host's order; atan2 is CUDA's (within 2 ulp of FP64), so after rounding to
+// FP32 the angles are the host's but where an FP64 value lies within those ulps of an FP32
+// rounding boundary.
+__device__ void bunge_d(double4 q, float* e) {
+  q = qstd_d(q);
+  const double w = q.x, x = q.y, y = q.z, z = q.w;
+  const double two_pi = 6.283185307179586;
+  const double q03 = __dadd_rn(__dmul_rn(w, w), __dmul_rn(z, z));
+  const double q12 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+  const double chi = sqrt(__dmul_rn(q03, q12));
+  double e1, e2, e3;
+  if (chi < 1e-14) {
+    e1 = q12 <= q03 ? atan2(__dmul_rn(__dmul_rn(-2.0, w), z), __dsub_rn(__dmul_rn(w, w), __dmul_rn(z, z)))
+                    : atan2(__dmul_rn(__dmul_rn(2.0, x), y), __dsub_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
+    e2 = q12 <= q03 ? 0.0 : 3.141592653589793;
+    e3 = 0.0;
+  } else {
+    e1 = atan2(__ddiv_rn(__dsub_rn(__dmul_rn(x, z), __dmul_rn(w, y)), chi),
+               __ddiv_rn(__dsub_rn(__dmul_rn(-w, x), __dmul_rn(y, z)), chi));
+    e2 = atan2(__dmul_rn(2.0, chi), __dsub_rn(q03, q12));
+    e3 = atan2(__ddiv_rn(__dadd_rn(__dmul_rn(w, y), __dmul_rn(x, z)), chi),
+               __ddiv_rn(__dsub_rn(__dmul_rn(y, z), __dmul_rn(w, x)), chi));
+  }
+  if (e1 < 0.0) e1 = __dadd_rn(e1, two_pi);
+  if (e3 < 0.0) e3 = __dadd_rn(e3, two_pi);
+  e[0] = __double2float_rn(e1); e[1] = __double2float_rn(e2); e[2] = __double2float_rn(e3);
+}
+
+// bunge (optional): each reduced orientation's Bunge angles, from its FP32-rounded quaternion as
+// the host's landing would take it
 __global__ void k_records_fz(const float* __restrict__ recs, int n, const double4* __restrict__ ops, int n_ops,
-                             float* __restrict__ fz) {
+                             float* __restrict__ fz, float* __restrict__ bunge) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float* r = recs + (size_t)i * 8;
@@ -509,6 +541,7 @@ __global__ void k_records_fz(const float* __restrict__ recs, int n, const double
   float* o = fz + (size_t)i * 4;
   o[0] = __double2float_rn(best.x); o[1] = __double2float_rn(best.y);
   o[2] = __double2float_rn(best.z); o[3] = __double2float_rn(best.w);
+  if (bunge) bunge_d(make_double4((double)o[0], (double)o[1], (double)o[2], (double)o[3]), bunge + (size_t)i * 3);
 }
 
 static bool fill_frame(DetArgs& a, const zeb_frame_t* fr) {
@@ -871,8 +904,13 @@ extern "C" int zeb_project(const float* master, int side, const float* poses, in
 }
 
 extern "C" int zeb_records_fz(const float* records, int n, const double* ops, int n_ops, float* fz, void* stream) {
+  return zeb_records_fz_bunge(records, n, ops, n_ops, fz, nullptr, stream);
+}
+
+extern "C" int zeb_records_fz_bunge(const float* records, int n, const double* ops, int n_ops, float* fz, float* bunge,
+                                    void* stream) {
   ZEB_REQUIRE(records && ops && fz && n_ops >= 1 && n_ops <= 48, ZEB_EARG, "records_fz: bad arguments");
   if (n <= 0) return ZEB_OK;
-  k_records_fz<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(records, n, (const double4*)ops, n_ops, fz);
+  k_records_fz<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(records, n, (const double4*)ops, n_ops, fz, bunge);
   return zeb_launch_check("records_fz");
 }

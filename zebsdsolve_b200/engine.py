@@ -168,7 +168,7 @@ class Engine:
         self._pin_buf = None  # the page-locked buffer behind _pinned, reused across scans
         self._index_calls = 0  # whole passes over the scan since set_patterns (whole_pinned)
         self._ring, self._ring_i = [], 0  # two page-locked slots a scan not pinned whole streams through
-        self._last_fz = None  # the last index_cells' records in the fundamental zones
+        self._last_fz = None  # the last index_cells' records in the fundamental zones, their Bunge angles
         self.pending_skip = 0  # batches whose readback is dropped (host-side fault injection)
         self.counts = {"submits": 0, "reads": 0, "waits": 0}  # device passes, readbacks, host waits
         self._full = False  # at_full: the stored size is the level being worked at
@@ -1289,16 +1289,19 @@ class Engine:
                 "ncc": ncc.cpu().numpy(), "rounds": int(it)}
 
     def fz_of(self, recs):
-        """Each phase's records reduced to its fundamental zone on the device: [phase][n][4]."""
+        """Each phase's records reduced to its fundamental zone on the device, with their Bunge
+        angles (the landing's conversion): ([phase][n][4], [phase][n][3]) device tensors."""
         n_ph, n = recs.shape[0], recs.shape[1]
         fz = self.buf("fz", max(n_ph * n * 4, 1))[: n_ph * n * 4].view(n_ph, n, 4)
+        bg = self.buf("fz_bunge", max(n_ph * n * 3, 1))[: n_ph * n * 3].view(n_ph, n, 3)
         for pi, p in enumerate(self.phases):
             ops = getattr(p, "ops_dev", None)
             if ops is None:
                 ops = torch.as_tensor(np.ascontiguousarray(p.master.rotations(), np.float64), device=self.dev)
                 p.ops_dev = ops
-            N.call("zeb_records_fz", ptr(recs[pi]), n, ptr(ops), ops.shape[0], ptr(fz[pi]), stream_ptr())
-        return fz
+            N.call("zeb_records_fz_bunge", ptr(recs[pi]), n, ptr(ops), ops.shape[0], ptr(fz[pi]), ptr(bg[pi]),
+                   stream_ptr())
+        return fz, bg
 
     def index_cells(self, cells, bandwidth=None, method="spherical", grid=None, whole_pass=True):
         """engine.zig:1990-2137 — index the given cells against every phase: records
@@ -1318,7 +1321,8 @@ class Engine:
         raw = self.buf("raw_up", n * h * w, self.raw_dtype()).view(-1)[: n * h * w].view(n, h, w)
         self.upload_raw(cells, raw, torch.cuda.current_stream())
         recs = self.run_device(raw, cells, bandwidth, method=method, grid=grid)
-        self._last_fz = self.fz_of(recs).cpu().numpy()
+        fzd, bgd = self.fz_of(recs)
+        self._last_fz = (fzd.cpu().numpy(), bgd.cpu().numpy())
         out = recs.cpu().numpy()
         self.counts["reads"] += 2
         self.counts["waits"] += 2
@@ -1401,7 +1405,8 @@ class Engine:
     def index_pipelined(self, cells, bandwidth, on_batch, keep_going=lambda: True, method="spherical", grid=None):
         """engine.zig:1990-2137 over many cells at once: device passes of device_batch() cells,
         each pass's upload (a copy stream, from the pinned scan) overlapping the previous pass's
-        kernels, its records read back asynchronously and handed to on_batch(cells, records, fz) on
+        kernels, its records read back asynchronously and handed to on_batch(cells, records, fz,
+        bunge) on
         the host while the next pass runs.  keep_going() is asked before each new pass."""
         cells = np.asarray(cells, np.int64)
         n_ph = len(self.phases)
@@ -1422,6 +1427,7 @@ class Engine:
         cps.wait_stream(comp)
         host = [torch.empty((n_ph, B, 8), dtype=torch.float32, pin_memory=True) for _ in range(2)]
         hfz = [torch.empty((n_ph, B, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+        hbg = [torch.empty((n_ph, B, 3), dtype=torch.float32, pin_memory=True) for _ in range(2)]
         # a small first pass (its upload is the one nothing hides), then passes of B
         first = min(len(cells), max(1, B // 4))
         parts = [cells[:first]] + [cells[i:i + B] for i in range(first, len(cells), B)]
@@ -1446,7 +1452,8 @@ class Engine:
             back[k] = None
             out = host[k][:, : len(cb)].numpy().copy()
             fz = hfz[k][:, : len(cb)].numpy().copy()
-            on_batch(cb, self.finish(out, stamp), fz)
+            bg = hbg[k][:, : len(cb)].numpy().copy()
+            on_batch(cb, self.finish(out, stamp), fz, bg)
 
         issue_upload(0)
         for i in range(len(parts)):
@@ -1461,9 +1468,10 @@ class Engine:
             comp_done[k] = ev
             if back[k] is not None:
                 drain(k)
-            fzd = self.fz_of(recs)
+            fzd, bgd = self.fz_of(recs)
             host[k][:, : len(cb)].copy_(recs, non_blocking=True)
             hfz[k][:, : len(cb)].copy_(fzd, non_blocking=True)
+            hbg[k][:, : len(cb)].copy_(bgd, non_blocking=True)
             evb = torch.cuda.Event()
             evb.record(comp)
             back[k] = (evb, cb, self.batch_stamp)
@@ -1562,10 +1570,11 @@ class Engine:
         self.res["z"][cells] = 0
         self._nl_report = bool(self.set["nlpar"])  # the run's first batch says what the averaging did
 
-    def land(self, cells, recs, fz=None):
+    def land(self, cells, recs, fz=None, bunge=None):
         """engine.zig:2392-2419 — each cell keeps the better match; accepted ones their sweep.
         fz: the records' orientations already in each phase's fundamental zone ([phase][cell][4],
-        zeb_records_fz); computed here on the host when absent."""
+        zeb_records_fz), bunge their Bunge angles ([phase][cell][3], zeb_records_fz_bunge); computed
+        here on the host when absent."""
         s = self.set
         res = self.res
         cells = np.asarray(cells, np.int64)
@@ -1583,7 +1592,10 @@ class Engine:
                 q[sel] = R.to_fz(r[sel, :4].astype(np.float64), self.phases[int(p)].master.rotations())
         idx = cells[replace]
         res["quat"][idx] = q[replace]
-        res["euler"][idx] = R.to_bunge(q[replace].astype(np.float64)).astype(np.float32)
+        if bunge is not None and fz is not None:
+            res["euler"][idx] = bunge[best, np.arange(len(cells))][replace]
+        else:
+            res["euler"][idx] = R.to_bunge(q[replace].astype(np.float64)).astype(np.float32)
         res["ncc"][idx] = r[replace, 4]
         res["nmi"][idx] = r[replace, 5]
         res["z"][idx] = r[replace, 7]
@@ -1615,7 +1627,7 @@ class Engine:
             recs = self.index_cells(cells, bw, method, dg, whole_pass=first)
         finally:
             self._whole_pass = False
-        self.land(cells, recs, self._last_fz)
+        self.land(cells, recs, *self._last_fz)
         self.next_sweep(bw)
         return len(self.index_cells_list) - self.index_done
 
@@ -1653,8 +1665,8 @@ class Engine:
             bw, dg, method = s.sweep(self.index_sweep)
             stop = [False]
 
-            def on_batch(cb, recs, fz):
-                self.land(cb, recs, fz)  # a pass already in flight when the stop came still lands
+            def on_batch(cb, recs, fz, bg):
+                self.land(cb, recs, fz, bg)  # a pass already in flight when the stop came still lands
                 if progress is not None and not stop[0] and progress(self.status()) is False:
                     stop[0] = True
 
