@@ -425,15 +425,16 @@ int zeb_refine_list(const float* pats, const float* items, const float* seeds, i
 
 /* The BF16 form's refinement table: for every texel of the [2][side][side] sheets its 2 × 2
  * neighbourhood (the texel, the one right of it, the one below, the one below right) in one
- * 32-byte record of FP16 values — the four masters, then the four tangent gradients (xyz) —
- * from the gradient table grad4 of zeb_master_gradient (quads: 32 × 2·side² bytes, 32-byte
- * aligned). No counterpart in the reference (its lookups read the four texels in FP32). */
+ * 32-byte record of FP16 values — per texel (gx, gy) and (gz, master) as two half2 — from the
+ * gradient table grad4 of zeb_master_gradient (quads: 32 × 2·side² bytes, 32-byte aligned). No
+ * counterpart in the reference (its lookups read the four texels in FP32). */
 int zeb_master_quads(const float* grad4, int side, void* quads, void* stream);
 
 /* zeb_refine_list with every lookup of the Gauss–Newton passes from the FP16 records of
- * zeb_master_quads (one 32-byte record a pixel instead of two; the weights and every sum in
- * FP32; the NMI from vpair in FP32 as before). The same records as zeb_refine_list to FP16's
- * rounding of the master's values and gradients. */
+ * zeb_master_quads (one 32-byte record a pixel instead of two; the bilinear interpolation in
+ * packed FP16, every sum in FP32; the NMI from vpair in FP32 as before). The same records as
+ * zeb_refine_list to FP16's rounding of the master's values and gradients and of the
+ * interpolation. */
 int zeb_refine_list_h(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
                       const zeb_frame_t* fr, const uint32_t* list, int npix, const float* vpair, const void* quads,
                       int side, const zeb_refine_opts_t* o, float* records, void* stream);

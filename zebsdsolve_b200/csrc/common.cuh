@@ -197,20 +197,25 @@ __device__ __forceinline__ float2 zeb_unhalf2(uint32_t w) {
 }
 
 // The same lookup from the FP16 neighbourhood records (zeb_master_quads): one 32-byte record a
-// pixel; the bilinear weights and every sum in FP32.
+// pixel, each texel's (gx, gy) and (gz, value) as two half2; the bilinear interpolation in packed
+// FP16 arithmetic (two channels an instruction, the weights rounded to FP16), its result widened
+// to FP32 for the sums.
 __device__ __forceinline__ float4 grad_at_quad(const float* __restrict__ gq, float3 v, int side) {
   SheetPos p = sheet_pos(v, side);
   uint32_t h[8];
   asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
       : "=r"(h[0]), "=r"(h[1]), "=r"(h[2]), "=r"(h[3]), "=r"(h[4]), "=r"(h[5]), "=r"(h[6]), "=r"(h[7])
       : "l"(gq + 8 * (size_t)p.o));
-  const float2 m01 = zeb_unhalf2(h[0]), m23 = zeb_unhalf2(h[1]);
-  const float2 a = zeb_unhalf2(h[2]), b = zeb_unhalf2(h[3]), c = zeb_unhalf2(h[4]);
-  const float2 d = zeb_unhalf2(h[5]), e = zeb_unhalf2(h[6]), f = zeb_unhalf2(h[7]);
-  // texels 0 (a.x a.y b.x), 1 (b.y c.x c.y), 2 (d.x d.y e.x), 3 (e.y f.x f.y)
-  const float4 t0 = make_float4(a.x, a.y, b.x, m01.x), t1 = make_float4(b.y, c.x, c.y, m01.y);
-  const float4 t2 = make_float4(d.x, d.y, e.x, m23.x), t3 = make_float4(e.y, f.x, f.y, m23.y);
-  return lerp4(lerp4(t0, t1, p.tj), lerp4(t2, t3, p.tj), p.ti);
+  const __half2 tj = __float2half2_rn(p.tj), ti = __float2half2_rn(p.ti);
+  const __half2* t = reinterpret_cast<const __half2*>(h);
+  // texels 0 (right 1) above, 2 (right 3) below: top = t0 + (t1 − t0)·tj, bot likewise, then ti
+  const __half2 top_xy = __hfma2(__hsub2(t[2], t[0]), tj, t[0]);
+  const __half2 top_zm = __hfma2(__hsub2(t[3], t[1]), tj, t[1]);
+  const __half2 bot_xy = __hfma2(__hsub2(t[6], t[4]), tj, t[4]);
+  const __half2 bot_zm = __hfma2(__hsub2(t[7], t[5]), tj, t[5]);
+  const float2 xy = __half22float2(__hfma2(__hsub2(bot_xy, top_xy), ti, top_xy));
+  const float2 zm = __half22float2(__hfma2(__hsub2(bot_zm, top_zm), ti, top_zm));
+  return make_float4(xy.x, xy.y, zm.x, zm.y);
 }
 
 __device__ __forceinline__ float master_at_pair(const float2* __restrict__ vp, float3 v, int side) {

@@ -151,15 +151,12 @@ __global__ void k_master_quads(const float4* __restrict__ grad4, int side, uint4
   const int c = (int)(i % side), r = (int)((i / side) % side);
   const long long right = c + 1 < side ? 1 : 0, down = r + 1 < side ? side : 0;
   const float4 g[4] = {grad4[i], grad4[i + right], grad4[i + down], grad4[i + down + right]};
-  uint32_t h[8];
-  h[0] = zeb_half2(g[0].w, g[1].w);
-  h[1] = zeb_half2(g[2].w, g[3].w);
-  h[2] = zeb_half2(g[0].x, g[0].y);
-  h[3] = zeb_half2(g[0].z, g[1].x);
-  h[4] = zeb_half2(g[1].y, g[1].z);
-  h[5] = zeb_half2(g[2].x, g[2].y);
-  h[6] = zeb_half2(g[2].z, g[3].x);
-  h[7] = zeb_half2(g[3].y, g[3].z);
+  uint32_t h[8];  // per texel (gx, gy) then (gz, value): the pairs the packed bilinear takes
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    h[2 * k] = zeb_half2(g[k].x, g[k].y);
+    h[2 * k + 1] = zeb_half2(g[k].z, g[k].w);
+  }
   quads[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
   quads[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
