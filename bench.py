@@ -104,13 +104,6 @@ def oracle_scan(raw_sheets, static_bg, L_=L, refine=True, baked=None):
                     static_bg=static_bg, refine=refine, baked=baked)
 
 
-def _oracle_cell(job):
-    import oracle.pipeline as opl
-
-    r = opl._one(job)
-    return r["q"], r["ncc"], r["nmi"]
-
-
 def oracle_geometry(px_um=0.0, step_um=1.0):
     """The workload's geometry in the oracle's terms (the pixel size the engine takes by default:
     the detector's 24 mm over 60 pixels; steps of 1 µm)."""
@@ -128,6 +121,23 @@ def oracle_run(scan, raws, ts=None):
 
     recs, dt, cores = opl.index_many(scan, raws, ts)
     return [(r["q"], r["ncc"], r["nmi"]) for r in recs], len(recs) / dt, cores, dt
+
+
+def cpu_ref_run(scan, raws, ts=None, threads=None):
+    """The C++ FP32 restatement (oracle/cpu_ref) over the stored patterns `raws` (at positions
+    `ts`) on `threads` host threads (default: every core this process may use), after a few
+    untimed patterns: (records [(q in the fundamental zone, NCC, NMI)], patterns/s, threads,
+    seconds)."""
+    import oracle.cpu_ref as ocr
+
+    threads = threads or max(1, len(os.sched_getaffinity(0)))
+    cr = ocr.CpuRef(scan)
+    k = min(len(raws), threads)
+    cr.index(raws[:k], None if ts is None else ts[:k], threads)
+    t0 = time.perf_counter()
+    recs = cr.index(raws, ts, threads)
+    dt = time.perf_counter() - t0
+    return [(r["q"], r["ncc"], r["nmi"]) for r in recs], len(recs) / dt, threads, dt
 
 
 def parity_of(oracle_recs, rotations, q, ncc, nmi):
@@ -445,11 +455,15 @@ def device_main(a):
         g = e.geo
         og_ = oracle_geometry(g.px_um, g.step_x_um)
         ts = opl.cell_positions(og_, rows, cols, ocells, H, W, s.settings["scan_x_sign"], s.settings["scan_y_sign"])
-        orecs, v, cores, dt = oracle_run(scan, pats[ocells], ts)
-        line["cpu_baseline"] = {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port",
+        orecs, v64, cores64, dt64 = oracle_run(scan, pats[ocells], ts)
+        # the CPU baseline: the same cells through the C++ FP32 restatement on every host thread
+        crecs, vc, cores, dtc = cpu_ref_run(scan, pats[ocells], ts)
+        line["cpu_baseline"] = {"value": round(vc, 3), "unit": "patterns/s", "cores": cores, "kind": "port",
                                 "sample": f"{len(ocells)} cells on a lattice over the map (their own stored patterns: "
-                                          f"filtered, correlated at L={L}, refined, NMI) through the FP64 oracle in "
-                                          f"{dt:.1f} s"}
+                                          f"filtered, correlated at L={L}, refined, NMI) through the C++ FP32 "
+                                          f"restatement of the path (oracle/cpu_ref) on {cores} threads in {dtc:.2f} s"}
+        line["oracle_fp64"] = {"value": round(v64, 3), "unit": "patterns/s", "cores": cores64,
+                               "sample": f"the same {len(ocells)} cells through the FP64 NumPy oracle in {dt64:.1f} s"}
         forms = {a.precision: r}
         if fp32 is not None:
             forms["f32"] = r32
@@ -458,6 +472,8 @@ def device_main(a):
         for k, rr in forms.items():
             line["oracle_parity"][k] = parity_of(orecs, scan.rotations, rr["quaternions"].reshape(-1, 4)[ocells],
                                                  rr["ncc"].reshape(-1)[ocells], rr["nmi"].reshape(-1)[ocells])
+        line["oracle_parity"]["cpu_ref"] = parity_of(orecs, scan.rotations, np.array([c[0] for c in crecs]),
+                                                     np.array([c[1] for c in crecs]), np.array([c[2] for c in crecs]))
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -628,54 +644,41 @@ def uneven_main(a):
 
 
 def reference_main(a):
-    """The reference's algorithm on the host cores (the oracle, FP64 NumPy; the reference engine
-    itself, Zig + WGSL on wgpu-native, cannot run on this box): a step indexes one pattern per
-    core from the workload's lattice of cells, made on the host (host_workload); W untimed steps,
-    then K timed ones. Under torchrun only rank 0 runs."""
-    import multiprocessing as mp
+    """The reference's algorithm on the host cores: its C++ FP32 restatement (oracle/cpu_ref,
+    checked against the FP64 oracle; the reference engine itself, Zig + WGSL on wgpu-native, cannot
+    run on this box), every host thread taking the next pattern; a step indexes the workload's
+    lattice of cells, made on the host (host_workload); W untimed steps, then K timed ones. Under
+    torchrun only rank 0 runs."""
+    import oracle.cpu_ref as ocr
 
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     raws, scan, cells, ts = host_workload()
-    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS"):
-        os.environ[k] = "1"
-    cores = max(1, min(len(os.sched_getaffinity(0)), 64))
-    ctx = mp.get_context("spawn")
-    limit = 600.0
-    nxt = [0]
-
-    def step(pool):
-        sel = [(raws[(nxt[0] + i) % len(raws)], ts[(nxt[0] + i) % len(raws)]) for i in range(cores)]
-        nxt[0] += cores
-        return pool.map_async(_oracle_cell, sel, chunksize=1).get(limit)
-
-    import oracle.pipeline as opl
-    import oracle.spherical as osp
-
-    osp._wigner_blocks(scan.tb)  # built once here and shipped to the workers with the scan
-    with ctx.Pool(cores, initializer=opl._init, initargs=(scan,)) as pool:
-        for _ in range(max(a.warmup, 1)):
-            step(pool)
-        t0 = time.perf_counter()
-        for _ in range(a.steps):
-            step(pool)
-        dt = time.perf_counter() - t0
-    done = a.steps * cores
+    cores = max(1, len(os.sched_getaffinity(0)))
+    cr = ocr.CpuRef(scan)
+    for _ in range(max(a.warmup, 1)):
+        cr.index(raws, ts, cores)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        cr.index(raws, ts, cores)
+    dt = time.perf_counter() - t0
+    done = a.steps * len(raws)
     v = done / dt
     n = ROWS * COLS if a.patterns == ROWS * COLS else a.patterns
     line = {"impl": "reference", "metric": "patterns/s indexed+refined on 1 B200, BF16 form vs plain FP32 at <=0.1 deg error",
             "value": round(v, 3), "unit": "patterns/s", "n_gpus": int(os.environ.get("WORLD_SIZE", a.gpus)),
             "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": round(1e3 * dt / a.steps, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(a, n),
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(a, n),
             "cpu_baseline": {"value": round(v, 3), "unit": "patterns/s", "cores": cores, "kind": "port",
-                             "sample": f"{done} patterns of the workload's lattice of {len(cells)} cells (made on the "
-                                       f"host: the same master and grain map), one per core a step, filtered, "
-                                       f"correlated at L={L}, refined and scored through the FP64 oracle"},
+                             "sample": f"a step: the workload's lattice of {len(cells)} cells (made on the host: the "
+                                       f"same master and grain map), filtered, correlated at L={L}, refined and "
+                                       f"scored through the C++ FP32 restatement of the path (oracle/cpu_ref) on "
+                                       f"{cores} threads"},
             "e2e": {"value": round(v, 3), "unit": "patterns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference engine (Zig + WGSL on wgpu-native) cannot be built or run here; its algorithm is "
-                    "timed as the FP64 oracle on the host cores"}
+                    "timed as a C++ FP32 restatement of the path on the host cores"}
     print(json.dumps(line), flush=True)
 
 
