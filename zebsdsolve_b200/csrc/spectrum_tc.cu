@@ -22,12 +22,14 @@
 // (k_pack_master, FP64 → BF16 hi/lo); the patterns' B per batch (k_pack_patterns).
 //
 // k_spectrum_tc: one CTA per (pattern tile of 128, order m'), 6 warps: warp 0 issues the bulk
-// copies (B once, then A block by block through a ring of TC_STAGES), warp 1 allocates TMEM and one of
-// its threads issues the MMAs (M = 128 rows of ν, N = 128 patterns, K = 16 a step) into two
-// accumulators of 128 columns, warps 2-5 drain an accumulator (tcgen05.ld) while the next one
-// fills, staging 32 patterns at a time in shared memory for a tensor store into U (scattered
-// 128-byte stores from four warps cap an SM near 13 GB/s; the tensor store does not). Every wait is bounded: on a timeout the CTA records the failure, drains what it
-// issued, frees its TMEM and returns.
+// copies (B once, then A block by block through a ring of stages: TC_STAGES for the FP32 U,
+// TCH_STAGES for the FP16 one), warp 1 allocates TMEM and one of its threads issues the MMAs
+// (M = 128 rows of ν, N = 128 patterns, K = 16 a step) into two accumulators of 128 columns, warps
+// 2-5 drain an accumulator (tcgen05.ld) while the next one fills: the FP32 U 32 patterns at a time
+// through shared memory into a tensor store, the FP16 U a whole tile at once (scattered 128-byte
+// stores from four warps cap an SM near 13 GB/s; the tensor store does not). Every wait is
+// bounded: on a timeout the CTA records the failure, drains what it issued, frees its TMEM and
+// returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
