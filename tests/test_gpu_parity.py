@@ -586,6 +586,78 @@ def test_refine_and_chance_on_a_large_detector_match_oracle(world, lib):
             assert abs(dec[d, i] - vd) < 2e-3
 
 
+@pytest.mark.parametrize("side", [100, 120])
+def test_larger_detectors_take_their_own_launch_shapes(world, lib, side):
+    """Detectors whose masked-pixel lists leave fewer refinement blocks an SM (100²: 256 threads a
+    pattern; 120²: 512) and, at 120², whose pattern exceeds the ring kernel's 48 KB of shared
+    memory (sampled from global memory): coefficients at L = 64 and the refinement over the shared
+    pixel list against the oracle, with the 60 × 60 bounds."""
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import rotations as R
+    from zebsdsolve_b200.device import BandTables
+
+    s = ze.Solver()
+    s.configure(static_background="none", dynamic_background="none", bandwidth=16)
+    s.add_phase(world["path"])
+    n = 3
+    s.set_patterns(np.zeros((1, n, side, side), np.float32))
+    s.set_geometry(pc=(0.5, 0.3, 0.6), sample_tilt_deg=70, detector_tilt_deg=0)
+    q = world["q"][:n]
+    rng = np.random.default_rng(side)
+    sims = s.simulate(q, cells=np.arange(n))
+    pats = sims + 0.3 * sims.std() * rng.normal(size=sims.shape)
+    s.set_patterns(pats.astype(np.float32).reshape(1, n, side, side))
+    e = s._e
+    e.prepare_masters()
+    fr = _frame(s)
+    mask = np.array(fr.mask)
+    normed = np.stack([op.normalize(p.astype(np.float64), mask) for p in pats]).astype(np.float32)
+    t = e.positions(np.arange(n))
+    items = torch.as_tensor(np.concatenate([t, np.arange(n, dtype=np.float32)[:, None]], 1), device="cuda")
+    pd = torch.as_tensor(normed, device="cuda").reshape(-1)
+    frame = (np.array(fr.c0), np.array(fr.c1), np.array(fr.c2))
+    # the coefficients at L = 64 (the warp-per-ring-pair kernel)
+    bt = BandTables(64, e.dev)
+    alm = torch.empty(n * bt.n_pairs * 2, device="cuda")
+    stats = torch.empty(n * 4, device="cuda")
+    scr = torch.empty(lib.load().zeb_sphere_scratch_bytes(ctypes.byref(bt.st), n) // 4 + 1, device="cuda")
+    lib.call("zeb_sphere_coefficients", P(pd), P(items), n, ctypes.byref(fr), ctypes.byref(bt.st), 3, P(alm), P(stats),
+             P(scr), sp())
+    got = alm.cpu().numpy().reshape(n, -1, 2)
+    got = got[..., 0] + 1j * got[..., 1]
+    tb = osp.Tables(64)
+    for i in range(n):
+        ref, _ = osp.coefficients(tb, normed[i].astype(np.float64), t[i].astype(np.float64), frame, mask)
+        assert np.abs(got[i] - ref).max() < 2e-5, np.abs(got[i] - ref).max()
+    # over the ring spans (each direction sampled once into the shared cache): the same coefficients
+    ts = torch.as_tensor(np.concatenate([t[:1], np.zeros((1, 1), np.float32)], 1).astype(np.float32), device="cuda")
+    spans = torch.empty(bt.n_theta * 2, dtype=torch.int32, device="cuda")
+    lib.call("zeb_sphere_spans", ctypes.byref(fr), ctypes.byref(bt.st), P(ts), 1, 2, P(spans), sp())
+    alm2 = torch.empty_like(alm)
+    lib.call("zeb_sphere_coefficients_spans", P(pd), P(items), n, ctypes.byref(fr), ctypes.byref(bt.st), P(spans), 3,
+             P(alm2), P(stats), P(scr), sp())
+    assert float((alm2 - alm).abs().max()) < 2e-6
+    # the refinement over the shared pixel list
+    lst = e.mask_list(fr)
+    assert lst is not None
+    start = R.qstd(R.qmul(R.exp_map(rng.normal(0, math.radians(0.8), (n, 3))), q))
+    seeds = torch.as_tensor(np.concatenate([start, np.zeros((n, 4))], 1).astype(np.float32), device="cuda")
+    recs = torch.empty(n * 8, device="cuda")
+    p = e.phases[0]
+    opts = lib.RefineOpts(8, math.radians(2.0), 1.0, 0.02, 1e4, 16, 3.0)
+    lib.call("zeb_refine_list", P(pd), P(items), P(seeds), 8, n, ctypes.byref(fr), P(lst), lst.numel(), P(p.baked[3]),
+             P(p.baked[4]), p.master.side, ctypes.byref(opts), P(recs), sp())
+    got = recs.cpu().numpy().reshape(n, 8)
+    grad = od.gradient_table(world["baked"], 151)
+    ops = world["m_or"].rotations()
+    for i in range(n):
+        qb, best, step = od.refine(grad, 151, frame, t[i], start[i], normed[i].astype(np.float64), mask)
+        assert abs(got[i, 4] - best) < 2e-4, (got[i, 4], best)
+        assert math.degrees(float(osym.disorientation(got[i, :4].astype(np.float64), qb, ops))) < 0.02
+        v = od.nmi(world["baked"], 151, frame, t[i], got[i, :4].astype(np.float64), normed[i].astype(np.float64), mask)
+        assert abs(got[i, 5] - v) < 2e-3, (got[i, 5], v)
+
+
 @pytest.mark.parametrize("precision", ["f32", "bf16", "bf16x3"])
 def test_index_end_to_end_recovers_orientations(lib, precision):
     """The reference's own bar (tests/test_api.py:206-214): 8 × 12 simulated patterns with noise of

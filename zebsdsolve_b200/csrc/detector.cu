@@ -576,6 +576,9 @@ static size_t det_smem(DetArgs& a) {
 // k_refine.
 constexpr int RL_THREADS = 128;
 
+// the block size for a list whose pattern values and simulated values take `smem` bytes
+inline int rl_threads(size_t smem) { return smem <= 36 * 1024 ? 128 : (smem <= 72 * 1024 ? 256 : 512); }
+
 __device__ __forceinline__ float3 list_ray(const DetArgs& a, float3 t, uint32_t v) {
   return ray_dir(a, t, (int)(v >> 16), (int)(v & 0xffffu));
 }
@@ -642,20 +645,22 @@ __device__ float nmi_list(const DetArgs& a, const uint32_t* __restrict__ list, c
 }
 
 // QUAD: the lookups from the FP16 neighbourhood records (a.gpair holds zeb_master_quads' table)
-template <bool QUAD>
-__global__ void __launch_bounds__(RL_THREADS, 6) k_refine_list(DetArgs a, const uint32_t* __restrict__ list,
+// TH threads a pattern: 128 (six patterns an SM) while the list is small; a list whose shared
+// memory leaves fewer blocks an SM takes 256 or 512, so that an SM keeps its warps
+template <bool QUAD, int TH>
+__global__ void __launch_bounds__(TH, TH == 128 ? 6 : (TH == 256 ? 3 : 1)) k_refine_list(DetArgs a, const uint32_t* __restrict__ list,
                                                                  int npix) {
   extern __shared__ float pv[];  // [npix] pattern values, then [npix] simulated values (NMI)
-  __shared__ float red[20 * (RL_THREADS / 32)];
+  __shared__ float red[20 * (TH / 32)];
   __shared__ uint32_t hist[32 * 32];
   __shared__ float4 sh_q;
   const int b = blockIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  constexpr int NW = RL_THREADS / 32;
+  constexpr int NW = TH / 32;
   const float4 it = a.items[b];
   const float3 t = make_float3(it.x, it.y, it.z);
   const float* gpat = a.pats + (size_t)(int)it.w * a.h * a.w;
-  for (int k = threadIdx.x; k < npix; k += RL_THREADS) {
+  for (int k = threadIdx.x; k < npix; k += TH) {
     const uint32_t v = __ldg(list + k);
     pv[k] = __ldg(gpat + (int)(v >> 16) * a.w + (int)(v & 0xffffu));
   }
@@ -675,7 +680,7 @@ __global__ void __launch_bounds__(RL_THREADS, 6) k_refine_list(DetArgs a, const 
 #pragma unroll
     for (int k = 0; k < 19; ++k) s[k] = 0.f;
 #pragma unroll 4
-    for (int k = threadIdx.x; k < npix; k += RL_THREADS) {
+    for (int k = threadIdx.x; k < npix; k += TH) {
       const uint32_t v = __ldg(list + k);
       const float row = (float)(int)(v >> 16), col = (float)(int)(v & 0xffffu);
       const float3 c = normalize3(make_float3(fmaf(rc0.x, row, fmaf(rc1.x, col, rt.x)),
@@ -771,6 +776,20 @@ __global__ void k_mask_list(DetArgs a, uint32_t* __restrict__ list) {
   }
 }
 
+template <bool QUAD, int TH>
+void rl_launch_th(const DetArgs& a, const uint32_t* list, int npix, size_t smem, cudaStream_t st) {
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_refine_list<QUAD, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_refine_list<QUAD, TH><<<a.n, TH, smem, st>>>(a, list, npix);
+}
+
+template <bool QUAD>
+void rl_launch(const DetArgs& a, const uint32_t* list, int npix, size_t smem, cudaStream_t st) {
+  const int th = rl_threads(smem);
+  if (th == 128) rl_launch_th<QUAD, 128>(a, list, npix, smem, st);
+  else if (th == 256) rl_launch_th<QUAD, 256>(a, list, npix, smem, st);
+  else rl_launch_th<QUAD, 512>(a, list, npix, smem, st);
+}
+
 }  // namespace zeb
 
 using namespace zeb;
@@ -835,9 +854,7 @@ extern "C" int zeb_refine_list(const float* pats, const float* items, const floa
   ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine_list: bad frame");
   a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
   a.vpair = (const float2*)vpair; a.gpair = gpair; a.side = side; a.o = *o; a.records = records;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_refine_list<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_refine_list<false><<<n, RL_THREADS, smem, (cudaStream_t)stream>>>(a, list, npix);
+  rl_launch<false>(a, list, npix, smem, (cudaStream_t)stream);
   return zeb_launch_check("refine_list");
 }
 
@@ -862,9 +879,7 @@ extern "C" int zeb_refine_list_h(const float* pats, const float* items, const fl
   ZEB_REQUIRE(fill_frame(a, fr), ZEB_EARG, "refine_list_h: bad frame");
   a.pats = pats; a.items = (const float4*)items; a.seeds = seeds; a.seed_stride = seed_stride; a.n = n;
   a.vpair = (const float2*)vpair; a.gpair = (const float*)quads; a.side = side; a.o = *o; a.records = records;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_refine_list<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_refine_list<true><<<n, RL_THREADS, smem, (cudaStream_t)stream>>>(a, list, npix);
+  rl_launch<true>(a, list, npix, smem, (cudaStream_t)stream);
   return zeb_launch_check("refine_list_h");
 }
 

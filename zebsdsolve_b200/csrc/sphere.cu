@@ -738,8 +738,10 @@ extern "C" int zeb_sphere_coefficients_spans(const float* pats, const float* ite
   cudaStream_t st = (cudaStream_t)stream;
   int rc;
   if (nphi == 256) {
-    // the warp-per-ring-pair kernel
+    // the warp-per-ring-pair kernel; a pattern above 48 KB is read from global memory (through
+    // L1) rather than held in shared memory, which would leave one block an SM
     a.ring_major = 1;
+    if (hw * 4 > 48 * 1024) a.pat_in_smem = 0;
     a.cache_cap = RW_CACHE;
     const size_t wsm = std::max((size_t)RW_WARPS * RW_PAD * sizeof(float2), a.pat_in_smem ? hw * 4 : (size_t)0) +
                        (size_t)RW_CACHE * sizeof(float);
