@@ -1162,6 +1162,9 @@ class Engine:
 
     STAGE_BYTES = 64 << 20
     PIN_MAX_BYTES = 16 << 30
+    # more runs of consecutive cells than this are gathered into a staging slot on the host (one
+    # copy) rather than copied run by run (one copy each)
+    PINNED_RUNS = 32
 
     def raw_dtype(self):
         """The stored pixel type as a torch dtype."""
@@ -1206,6 +1209,18 @@ class Engine:
         for f in futs:
             f.result()
 
+    def _gather(self, host, flat, part):
+        """host[:] = flat[part] (scattered cells into a staging slot) on the same pool of host
+        threads; the cells are checked against the scan first, so that none is read out of it."""
+        if len(part) and (part.min() < 0 or part.max() >= len(flat)):
+            raise EngineError(f"cells outside the scan of {len(flat)} patterns")
+        parts = min(self._fill_threads(), max(1, host.nbytes // self.FILL_PART))
+        step = -(-len(part) // parts)
+        futs = [self._pool.submit(np.take, flat, part[i:i + step], 0, host[i:i + step], "clip")
+                for i in range(0, len(part), step)]
+        for f in futs:
+            f.result()
+
     def _fill_threads(self):
         if getattr(self, "_pool", None) is None:
             import concurrent.futures as cf
@@ -1216,17 +1231,17 @@ class Engine:
         return self._pool_n
 
     def upload_raw(self, cells, dst, stream):
-        """Enqueue on `stream` the copies of the given cells' stored patterns into dst[0:n], one
-        per run of consecutive cells: from the page-locked copy of the scan, or (a scan indexed
-        once) through two page-locked slots of 64 MB in turn, each filled on the host while the
-        other's copy runs."""
+        """Enqueue on `stream` the copies of the given cells' stored patterns into dst[0:n]: one
+        per run of consecutive cells from the page-locked copy of the scan, where it is held and
+        the cells make few runs; otherwise through two page-locked slots of 64 MB in turn, each
+        filled on the host (a run copied, scattered cells gathered) while the other's copy runs."""
         cells = np.asarray(cells, np.int64)
         if len(cells) == 0:
             return
         cut = np.flatnonzero(np.diff(cells) != 1) + 1
-        starts = np.concatenate([[0], cut])
-        ends = np.concatenate([cut, [len(cells)]])
-        if self.whole_pinned():
+        if self.whole_pinned() and len(cut) < self.PINNED_RUNS:
+            starts = np.concatenate([[0], cut])
+            ends = np.concatenate([cut, [len(cells)]])
             src = self.pinned()
             with torch.cuda.stream(stream):
                 for a0, a1 in zip(starts, ends):
@@ -1241,18 +1256,19 @@ class Engine:
             raise EngineError("PatternTooLarge: one pattern exceeds the staging slot")
         td = self.raw_dtype()
         with torch.cuda.stream(stream):
-            for a0, a1 in zip(starts, ends):
-                c, o, left = int(cells[a0]), int(a0), int(a1 - a0)
-                while left > 0:
-                    k = min(left, most)
-                    slot = self._slot()
-                    host = slot[0].numpy()[: k * per].view(self.patterns.dtype).reshape(k, h, w)
-                    self._fill(host, flat[c:c + k])
-                    dst[o:o + k].copy_(slot[0][: k * per].view(td).view(k, h, w), non_blocking=True)
-                    ev = torch.cuda.Event()
-                    ev.record(stream)
-                    slot[1] = ev
-                    c, o, left = c + k, o + k, left - k
+            for o in range(0, len(cells), most):
+                part = cells[o:o + most]
+                k = len(part)
+                slot = self._slot()
+                host = slot[0].numpy()[: k * per].view(self.patterns.dtype).reshape(k, h, w)
+                if k == 1 or bool((np.diff(part) == 1).all()):
+                    self._fill(host, flat[int(part[0]):int(part[0]) + k])
+                else:
+                    self._gather(host, flat, part)
+                dst[o:o + k].copy_(slot[0][: k * per].view(td).view(k, h, w), non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                slot[1] = ev
 
     def refine_patterns(self, cells, quaternions, phase, trust, rounds, gradient):
         """planefit.zig:570-622 (settle, k = 6) for the given cells against one phase."""
