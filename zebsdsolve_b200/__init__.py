@@ -168,15 +168,21 @@ class Solver:
         ext = str(path).rsplit(".", 1)[-1].lower()
         if ext not in ("ang", "ctf"):
             raise Error(f"export: .{ext} is not written by this engine (.ang, .ctf)")
+        text = self.export_text(ext)
+        with open(path, "w") as fh:
+            fh.write(text)
+
+    def export_text(self, kind):
+        """The results as the text of an EDAX .ang (`kind` "ang") or an HKL .ctf ("ctf")."""
+        from . import output
+
         e = self._e
-        rows, cols, h, w = e.info()
+        rows, cols, h, w = self._call("export", e.info)
         phases = [{"name": p.master.name, "laue": p.master.laue, "lattice": p.master.lattice,
                    "space_group": p.master.space_group} for p in e.phases]
         src = getattr(e, "scan_source", None) or {}
-        text = self._call("export", output.export_text, ext, e.res, phases, e.geo, rows, cols, h, w,
+        return self._call("export", output.export_text, kind, e.res, phases, e.geo, rows, cols, h, w,
                           src.get("voltage_kv", float("nan")))
-        with open(path, "w") as fh:
-            fh.write(text)
 
     def shape(self, full=False):
         """(h, w) of a pattern as the search sees it (reduced by `binning`), or (full) as stored."""
@@ -453,13 +459,19 @@ class Solver:
         correlation at `bandwidth` (default fit_bandwidth), then the refinement. Returns the best
         phase's {phase, quaternion, ncc, nmi, simulation} (the simulation at the stored size with
         `full`)."""
+        bw = int(bandwidth or self._e.set["fit_bandwidth"])
+        p, recs, sim = self._cell_under(cell, bw, full, fields)
+        r = recs[p, 0]
+        return {"phase": p, "quaternion": r[:4].copy(), "ncc": float(r[4]), "nmi": float(r[5]), "simulation": sim}
+
+    def _cell_under(self, cell, bw, full, fields):
+        """cell_under's work: (the best phase, every phase's record [phases][1][8], its simulation)."""
         e = self._e
         keep = e.geo
         tmp = keep.copy()
         self._call("cell_under", tmp.given, fields, type(keep)())
         if not tmp.px_um > 0:
             tmp.px_um = e.default_px()
-        bw = int(bandwidth or e.set["fit_bandwidth"])
         try:
             e.geo = tmp
             recs = self._call("cell_under", e.index_cells, np.array([int(cell)], np.int64), bw, "spherical", None,
@@ -476,7 +488,7 @@ class Solver:
                     e.set.apply({"binning": binning})
         finally:
             e.geo = keep
-        return {"phase": p, "quaternion": r[:4].copy(), "ncc": float(r[4]), "nmi": float(r[5]), "simulation": sim}
+        return p, recs, sim
 
     # ── the device's own accounts ──
 

@@ -1,5 +1,6 @@
 """Build the CUDA library in place: every csrc/*.cu compiled for sm_100a and linked into
-zebsdsolve_b200/libzebsdsolve_b200.so (the file the package loads).
+zebsdsolve_b200/libzebsdsolve_b200.so (the file the package loads); and, with gcc,
+zebsdsolve_b200/libzebsdsolve.so, the reference's own C ABI over the package (csrc/ze_abi.c).
 
     python -m zebsdsolve_b200.build [--force] [--verbose]
 
@@ -77,7 +78,29 @@ def build(force=False, verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_abi(force)
     return LIB
+
+
+ABI_SRC = CSRC / "ze_abi.c"
+ABI_LIB = HERE / "libzebsdsolve.so"
+
+
+def build_abi(force=False):
+    """libzebsdsolve.so: the reference's own C ABI (csrc/ze_abi.c, include/zebsdsolve.h) with gcc.
+    The Python C API is left to be resolved where the library is loaded (a Python process, or a
+    native host that links libpython)."""
+    import sysconfig
+
+    deps = [ABI_SRC, INCLUDE / "zebsdsolve.h"]
+    if force or not ABI_LIB.exists() or ABI_LIB.stat().st_mtime < max(d.stat().st_mtime for d in deps):
+        cmd = [os.environ.get("CC", "gcc"), "-O2", "-std=c11", "-Wall", "-Wextra", "-Wno-unused-parameter", "-fPIC",
+               "-shared", "-fvisibility=hidden", "-I", sysconfig.get_paths()["include"], str(ABI_SRC), "-o",
+               str(ABI_LIB), "-ldl", "-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"gcc failed on {ABI_SRC.name}:\n{r.stderr}")
+    return ABI_LIB
 
 
 if __name__ == "__main__":
