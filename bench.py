@@ -13,8 +13,10 @@ circular mask, 8 refinement iterations).  A step is one pass of the whole path o
 scan.  Inputs (720 MB) exceed L2 (126 MB), so no flush is needed between steps.
 
 `value` times the device path with the stored patterns already resident in HBM; `e2e` times the
-public API (Solver.index) from host memory: uploads, device path, the records' readback and the
-host's landing of results.  With --gpus N (N > 1; run directly, the command re-executes itself
+reference's own C ABI (libzebsdsolve.so: ze_index_begin, the ze_index_step loop, ze_results of
+every kind, as the reference's Solver.index issues them) from host memory: uploads, device path,
+the records' readback and the host's landing of results; `e2e_python_api` the same through this
+package's Python API (Solver.index), whose results the C ABI's must equal.  With --gpus N (N > 1; run directly, the command re-executes itself
 under torch.distributed.run, one process per GPU) every rank holds the same scan: `value` has each
 rank index all of it (weak scaling, no collective on the data path), `e2e` shards the one scan
 over the ranks (shard.index_sharded: contiguous shares, the records gathered to rank 0); both
@@ -59,6 +61,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=16384, help="patterns per device pass in the value measurement")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-abi", action="store_true", help="skip the end-to-end leg through the reference's C ABI")
     ap.add_argument("--workload", default="index", choices=("index", "adjoint", "uneven", "pcfit", "plane", "large", "nickel",
                                                               "match", "target"),
                     help="index: the scan of 60x60 patterns (the headline); adjoint: six-unknown refinement "
@@ -190,6 +193,73 @@ def host_workload(rank=0):
     # the lattice is the static background's lattice: its mean is the scan's static background
     scan = oracle_scan(sheets, raws.astype(np.float64).mean(0), baked=baked)
     return raws, scan, cells, ts
+
+
+def abi_e2e(settings, master, pats, steps, warmup):
+    """One scan end to end through the reference's own C ABI (zebsdsolve_b200/libzebsdsolve.so, the
+    ze_* calls its Python package binds): ze_set_patterns from a host buffer once, then every step
+    what the reference's Solver.index issues: ze_index_begin, ze_index_step until no cell is left,
+    and ze_results of every kind into host arrays. Returns (ms per step, {kind: array})."""
+    import ctypes
+
+    import torch
+    from zebsdsolve_b200 import build, ze_abi as Z
+
+    lib = ctypes.CDLL(str(build.ABI_LIB))
+    P, SZ, U32, I32, I64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int64
+    G = ctypes.POINTER(Z.Geometry)
+    for name, args, res in (("ze_create", [ctypes.c_char_p], P), ("ze_destroy", [P], None),
+                            ("ze_error", [P, ctypes.c_char_p, SZ], SZ), ("ze_configure", [P, ctypes.c_char_p, SZ], I32),
+                            ("ze_add_phase", [P, ctypes.c_char_p, SZ], I32),
+                            ("ze_set_patterns", [P, P, SZ, U32, U32, U32, U32, U32], I32),
+                            ("ze_get_geometry", [P, G], None), ("ze_set_geometry", [P, G], None),
+                            ("ze_index_begin", [P], I32), ("ze_index_step", [P], I64),
+                            ("ze_results", [P, U32, P, SZ], I64)):
+        fn = getattr(lib, name)
+        fn.argtypes, fn.restype = args, res
+    h = lib.ze_create(b"")
+    if not h:
+        raise RuntimeError("ze_create failed")
+
+    def ok(rc, what):
+        if rc < 0:
+            buf = ctypes.create_string_buffer(1024)
+            k = lib.ze_error(h, buf, 1024)
+            raise RuntimeError(f"{what}: {buf.raw[:k].decode()}")
+        return rc
+
+    rows, cols, hh, ww = pats.shape
+    j = json.dumps(settings).encode()
+    ok(lib.ze_configure(h, j, len(j)), "configure")
+    ok(lib.ze_add_phase(h, master.encode(), len(master)), "add_phase")
+    ok(lib.ze_set_patterns(h, pats.ctypes.data, pats.nbytes, 1, rows, cols, hh, ww), "set_patterns")
+    g = Z.Geometry()
+    lib.ze_get_geometry(h, ctypes.byref(g))
+    g.pc[:], g.sample_tilt_deg, g.detector_tilt_deg = PC, 70.0, 0.0
+    lib.ze_set_geometry(h, ctypes.byref(g))
+    n = rows * cols
+    outs = {kind: np.empty(n * k, dt) for kind, dt, k in ((0, np.float32, 4), (1, np.float32, 1), (2, np.float32, 1),
+                                                          (3, np.int32, 1), (4, np.float32, 3), (5, np.float32, 1),
+                                                          (6, np.int32, 1))}
+
+    def run():
+        ok(lib.ze_index_begin(h), "index_begin")
+        while ok(lib.ze_index_step(h), "index_step") > 0:
+            pass
+        for kind, o in outs.items():
+            ok(lib.ze_results(h, kind, o.ctypes.data, o.nbytes), "results")
+
+    for _ in range(max(2, warmup - 2)):  # as the API leg: the second run makes the page-locked copy
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    lib.ze_destroy(h)
+    return e0.elapsed_time(e1) / steps, outs
 
 
 def config_of(a, n):
@@ -377,6 +447,19 @@ def device_main(a):
 
     clk = Clocks(local)
     ms, ems, launches, stages, r = time_form(a.precision, clk, nvtx=True)
+    abi = None
+    if world == 1 and not a.no_abi:
+        # the same scan through the reference's own C ABI (libzebsdsolve.so), its own engine
+        ams, aouts = abi_e2e({"bandwidth": L, "precision": a.precision}, f"{tmp}/m432.npz",
+                             pats.reshape(rows, cols, H, W), a.steps, a.warmup)
+        same = all(np.array_equal(aouts[k].reshape(r[key].shape), r[key])
+                   for k, key in ((0, "quaternions"), (1, "ncc"), (2, "nmi"), (3, "phase"), (4, "euler"), (5, "z"),
+                                  (6, "sweep")))
+        abi = {"value": round(n / (ams / 1e3), 1), "unit": "patterns/s", "ms_per_step": round(ams, 3),
+               "results_equal_python_api": bool(same),
+               "note": "the reference's own C ABI (libzebsdsolve.so): ze_set_patterns from host memory once, then "
+                       "each step ze_index_begin, the ze_index_step loop and ze_results of all 7 kinds, as the "
+                       "reference's Solver.index issues them"}
     u_half = e.bands[L]["phases"][0][1].u_scale is not None  # the timed form keeps U in FP16
     value = n * world / (ms / 1e3)
     e2e = n / (ems / 1e3)  # one scan's patterns over the job's time (all of it on one rank, or sharded)
@@ -440,6 +523,13 @@ def device_main(a):
                      "within_0.1deg": round(float((dis < 0.1).mean()), 4)},
         "clocks": clk.summary(),
     }
+    if abi is not None:
+        # the headline end-to-end figure is the one through the reference's own C ABI; the same
+        # scan through this package's Python API (Solver.index) beside it
+        line["e2e_python_api"] = {"value": line["e2e"]["value"], "unit": "patterns/s",
+                                  "ms_per_step": round(ems, 3)}
+        line["e2e"].update(value=abi["value"], ms_per_step=abi["ms_per_step"],
+                           results_equal_python_api=abi["results_equal_python_api"], via=abi["note"])
     if fp32 is not None:
         line["fp32_form"] = fp32
         line["vs_fp32_form"] = {"value": round(value / fp32["value"], 3), "e2e": round(e2e / fp32["e2e"], 3)}

@@ -55,9 +55,12 @@ def world():
 
     d = tempfile.mkdtemp()
     paths = []
+    keys = ("a_angstrom", "b_angstrom", "c_angstrom", "alpha_deg", "beta_deg", "gamma_deg")
+    cells = {"432": ([3.52] * 3 + [90.0] * 3, 225), "622": ([3.19, 3.19, 5.19, 90.0, 90.0, 120.0], 186)}
     for g, seed in (("432", 3), ("622", 4)):
         sheets = syn.master_sheets(seed, side=201, lmax=48, group=g, device="cuda")
-        write_npz(f"{d}/m{g}.npz", sheets, 201, syn.group_matrices(g), syn.POINT_GROUP[g])
+        write_npz(f"{d}/m{g}.npz", sheets, 201, syn.group_matrices(g), syn.POINT_GROUP[g],
+                  meta={"cell": dict(zip(keys, cells[g][0])), "space_group": cells[g][1]})
         paths.append(f"{d}/m{g}.npz")
     rows, cols = 8, 12
     s = ze.Solver()
@@ -157,6 +160,7 @@ def test_a_scan_through_the_c_abi_matches_the_python_api(world):
     assert lib.ze_pattern(e, 17, 1, 0, pt.ctypes.data, pt.size) == 0
     assert np.array_equal(pt.reshape(h, w), s.pattern(17))
     size = lib.ze_export(e, 0, None, 0)
+    assert size > 0, _err(lib, e)
     text = ctypes.create_string_buffer(size)
     assert lib.ze_export(e, 0, text, size) == size
     assert text.raw[:size].decode() == s.export_text("ang")
@@ -169,7 +173,8 @@ def test_a_scan_through_the_c_abi_matches_the_python_api(world):
     lib.ze_scan_info(e, ctypes.byref(si))
     assert (si.rows, si.cols, si.pat_h, si.pat_w, si.pixel, si.format) == (rows, cols, h, w, 1, 100)
     fb = ctypes.create_string_buffer(64)
-    assert fb.raw[:lib.ze_scan_format(e, fb, 64)] == b"memory"
+    k = lib.ze_scan_format(e, fb, 64)
+    assert fb.raw[:k] == b"memory"
     qz = want["quaternions"].reshape(-1, 4)[3].copy()
     eu = np.empty(3, np.float64)
     lib.ze_reduce(e, 0, qz.ctypes.data, eu.ctypes.data)
@@ -185,6 +190,7 @@ def test_a_scan_through_the_c_abi_matches_the_python_api(world):
     assert _err(lib, e).startswith("configure") and _err(lib, e) == ""
     assert lib.ze_sim_run(e, None) < 0 and "not part of this engine" in _err(lib, e)
     eb = ctypes.create_string_buffer(1 << 16)
-    kinds = {json.loads(x)["kind"] for x in eb.raw[:lib.ze_events(e, eb, len(eb))].decode().splitlines() if x}
+    k = lib.ze_events(e, eb, len(eb))
+    kinds = {json.loads(x)["kind"] for x in eb.raw[:k].decode().splitlines() if x}
     assert "log" in kinds
     lib.ze_destroy(e)

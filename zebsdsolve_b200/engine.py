@@ -1647,6 +1647,31 @@ class Engine:
         self.next_sweep(bw)
         return len(self.index_cells_list) - self.index_done
 
+    STEP_RUN_CELLS = 1 << 18
+
+    def index_step_run(self, most=None):
+        """index_step over up to `most` cells (STEP_RUN_CELLS by default) of the sweep in progress
+        as one pipelined run (index_pipelined: the cells, records and landing of index_step, with
+        uploads, kernels, readbacks and landing overlapped; none in flight when it returns);
+        returns the cells left. What the C ABI's ze_index_step runs."""
+        s = self.set
+        left = len(self.index_cells_list) - self.index_done
+        if left == 0 or self.cancel:
+            return 0
+        most = self.STEP_RUN_CELLS if most is None else max(1, int(most))
+        bw, dg, method = s.sweep(self.index_sweep)
+        part = self.index_cells_list[self.index_done:self.index_done + most]
+        if self.index_done == 0 and self.index_sweep == 0:
+            self._index_calls += 1  # (a scan indexed a second time is pinned whole: whole_pinned)
+        self._whole_pass = True
+        try:
+            self.index_pipelined(part, bw, lambda cb, recs, fz, bg: self.land(cb, recs, fz, bg),
+                                 keep_going=lambda: not self.cancel, method=method, grid=dg)
+        finally:
+            self._whole_pass = False
+        self.next_sweep(bw)
+        return len(self.index_cells_list) - self.index_done
+
     def next_sweep(self, bw):
         """engine.zig:2452-2463 — at the end of a sweep, the cells not yet accepted go on to the next."""
         s = self.set

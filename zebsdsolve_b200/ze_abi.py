@@ -704,7 +704,9 @@ def ze_index_begin(x):
 
 @_api("index_step")
 def ze_index_step(x):
-    return int(x.s.index_step())
+    """The next part of the sweep (up to Engine.STEP_RUN_CELLS cells) as one pipelined run on the
+    device: the cells and records of the reference's steps of a few batches, with fewer waits."""
+    return int(x.s._call("index", x.s._e.index_step_run))
 
 
 @_api("tune")
