@@ -699,7 +699,7 @@ def uneven_main(a):
     s.index()
     # each scan made, then timed from its patterns on the host to its results (set-up included);
     # one scan is held at a time
-    wall, total, right, dis_all, shapes = 0.0, 0, [], [], []
+    wall, total, right, dis_all, shapes, scan_ms = 0.0, 0, [], [], [], []
     for k in range(a.scans):
         pats, q, phase_of = make(k)
         shapes.append((int(pats.shape[0] * pats.shape[1]), int(pats.shape[2])))
@@ -708,7 +708,9 @@ def uneven_main(a):
         s.set_patterns(pats)
         r = s.index()
         torch.cuda.synchronize()
-        wall += time.perf_counter() - t0
+        dt = time.perf_counter() - t0
+        wall += dt
+        scan_ms.append(round(dt * 1e3, 2))
         total += pats.shape[0] * pats.shape[1]
         ph = r["phase"].reshape(-1)
         right.append(ph == phase_of)
@@ -726,7 +728,7 @@ def uneven_main(a):
             "config": {"workload": f"{a.scans} scans, 1000-{a.max_count} patterns (log-uniform), detector sizes "
                                    "40/60/96/160 u16, masters 432 and 622 (401^2, SH <= 96), L = 64",
                        "patterns": total, "scan_patterns": [c for c, _ in shapes],
-                       "scan_sizes": [z for _, z in shapes], "precision": a.precision},
+                       "scan_sizes": [z for _, z in shapes], "scan_ms": scan_ms, "precision": a.precision},
             "wall_s": round(wall, 3),
             "accuracy": {"phase_right": round(float(right.mean()), 4), "median_deg": round(float(np.median(dis)), 4),
                          "within_0.1deg": round(float((dis < 0.1).mean()), 4)}}

@@ -1474,14 +1474,16 @@ class Engine:
         issue_upload(0)
         for i in range(len(parts)):
             k = i % 2
-            if i + 1 < len(parts):
-                issue_upload(i + 1)
             comp.wait_event(up_done[k])
             cb = parts[i]
             recs = self.run_device(raw[k][: len(cb)], cb, bandwidth, method=method, grid=grid)
             ev = torch.cuda.Event()
             ev.record(comp)
             comp_done[k] = ev
+            if i + 1 < len(parts):
+                # the next pass's upload, its host fill (a scan streamed through the staging
+                # slots) done while this pass runs
+                issue_upload(i + 1)
             if back[k] is not None:
                 drain(k)
             fzd, bgd = self.fz_of(recs)
