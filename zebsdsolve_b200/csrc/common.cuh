@@ -95,18 +95,33 @@ __device__ __forceinline__ float atan01(float t) {
   return t * p;
 }
 
-// sphere_to_square with approximate arithmetic (fast reciprocal and square root, atan01): within
-// a few ulp of the exact map, for the per-pixel loops of the detector kernels.
-__device__ __forceinline__ float2 sphere_to_square_fast(float3 v) {
+// sphere_to_square with approximate arithmetic (the fast square root, atan01): within a few ulp
+// of the exact map, for the per-pixel loops of the detector kernels. square_map keeps the
+// intermediates the derivative of the lookup reuses (sheet_jacobian_of): ρ² = x² + y²,
+// 1/(1 + |z|), q = (π/2) ρ²/(1 + |z|), 1/√q, xn = √q and the fitted arctangent.
+struct SquareMap {
+  float2 uv;
+  float rho2, rden, rq, xn, at;
+};
+
+__device__ __forceinline__ SquareMap square_map(float3 v) {
+  SquareMap m;
   const float ax = fabsf(v.x), ay = fabsf(v.y);
-  const float q = ZEB_PI * 0.5f * (ax * ax + ay * ay) * __frcp_rn(1.f + fabsf(v.z));
-  const float xn = q > 0.f ? q * rsqrtf(q) : 0.f;
+  m.rho2 = ax * ax + ay * ay;
+  m.rden = __frcp_rn(1.f + fabsf(v.z));
+  const float q = ZEB_PI * 0.5f * m.rho2 * m.rden;
+  m.rq = rsqrtf(q);
+  m.xn = q > 0.f ? q * m.rq : 0.f;
   const float lo = fminf(ax, ay), hi = fmaxf(fmaxf(ax, ay), 1e-30f);
-  const float ang = (4.f / ZEB_PI) * xn * atan01(__fdividef(lo, hi));
-  const float u = ax >= ay ? xn : ang, w = ax >= ay ? ang : xn;
+  m.at = atan01(__fdividef(lo, hi));
+  const float ang = (4.f / ZEB_PI) * m.xn * m.at;
+  const float u = ax >= ay ? m.xn : ang, w = ax >= ay ? ang : m.xn;
   const float sc = 0.79788456080286536f;  // 1 / sqrt(π / 2)
-  return make_float2(copysignf(u * sc, v.x < 0.f ? -1.f : 1.f), copysignf(w * sc, v.y < 0.f ? -1.f : 1.f));
+  m.uv = make_float2(copysignf(u * sc, v.x < 0.f ? -1.f : 1.f), copysignf(w * sc, v.y < 0.f ? -1.f : 1.f));
+  return m;
 }
+
+__device__ __forceinline__ float2 sphere_to_square_fast(float3 v) { return square_map(v).uv; }
 
 // Square coordinates → unit vector on the northern or southern hemisphere (mastersph.wgsl:40-62).
 __device__ __forceinline__ float3 square_to_sphere(float px, float py, bool south) {

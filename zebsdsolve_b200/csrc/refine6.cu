@@ -154,25 +154,25 @@ __device__ float4 grad_smooth(const float* __restrict__ sheets, float3 v, int si
 }
 
 // ∂(fj, fi)/∂c of the sheet coordinates fj = (U + 1)/2·last, fi = (W + 1)/2·last of direction c
-// (sphere_to_square, common.wgsl:44-57), from the map's own formula; zero where clamped or at
-// the poles of the map (x = y = 0).
-__device__ __forceinline__ void sheet_jacobian(float3 c, int side, float3& dfj, float3& dfi) {
-  const float ax = fabsf(c.x), ay = fabsf(c.y), az = fabsf(c.z);
+// (sphere_to_square, common.wgsl:44-57), from the map's own formula and the intermediates its
+// evaluation left (square_map: ρ², 1/(1 + |z|), 1/√q, xn = √q, the fitted arctangent); zero where
+// clamped or at the poles of the map (x = y = 0).
+__device__ __forceinline__ void sheet_jacobian_of(const SquareMap& m, float3 c, int side, float3& dfj, float3& dfi) {
+  const float ax = fabsf(c.x), ay = fabsf(c.y);
   const float sx = c.x < 0.f ? -1.f : 1.f, sy = c.y < 0.f ? -1.f : 1.f, sz = c.z < 0.f ? -1.f : 1.f;
-  const float rho2 = ax * ax + ay * ay;
+  const float rho2 = m.rho2;
   dfj = make_float3(0.f, 0.f, 0.f);
   dfi = make_float3(0.f, 0.f, 0.f);
   if (rho2 < 1e-20f) return;
-  const float rden = __frcp_rn(1.f + az), rrho2 = __frcp_rn(rho2);
-  const float qv = 0.5f * ZEB_PI * rho2 * rden;
-  const float xn = sqrtf(qv);
+  const float rden = m.rden, rrho2 = __fdividef(1.f, rho2);
+  const float xn = m.xn;
   // ∂xn = ∂q / (2 xn); ∂q = (π x/den, π y/den, −(π/2) ρ² sgn(z)/den²)
-  const float k = 0.5f / xn;
+  const float k = 0.5f * m.rq;
   const float3 dxn = make_float3(k * ZEB_PI * c.x * rden, k * ZEB_PI * c.y * rden, -k * 0.5f * ZEB_PI * rho2 * sz * rden * rden);
   const float four_pi = 4.f / ZEB_PI;
-  // the angle as the lookup's map takes it (sphere_to_square_fast: the fitted arctangent of the
-  // smaller over the larger coordinate)
-  const float ang = atan01(__fdividef(fminf(ax, ay), fmaxf(ax, ay)));
+  // the angle as the lookup's map takes it (the fitted arctangent of the smaller over the larger
+  // coordinate)
+  const float ang = m.at;
   float3 du, dw;
   if (ax >= ay) {
     const float al = ang;
@@ -195,7 +195,8 @@ __device__ __forceinline__ void sheet_jacobian(float3 c, int side, float3& dfj, 
 // The bilinear master value at c and its gradient along the sphere (the exact derivative of the
 // lookup, projected on the tangent plane at c).
 __device__ __forceinline__ float master_and_slope(const float2* __restrict__ vp, float3 c, int side, float3& grad) {
-  const float2 uv = sphere_to_square_fast(c);
+  const SquareMap sm = square_map(c);
+  const float2 uv = sm.uv;
   const float last = (float)(side - 1);
   const float fj0 = (uv.x + 1.f) * 0.5f * last, fi0 = (uv.y + 1.f) * 0.5f * last;
   const float fj = fminf(fmaxf(fj0, 0.f), last), fi = fminf(fmaxf(fi0, 0.f), last);
@@ -209,7 +210,7 @@ __device__ __forceinline__ float master_and_slope(const float2* __restrict__ vp,
   const float dmj = (fj0 > 0.f && fj0 < last) ? (1.f - ti) * (t.y - t.x) + ti * (u.y - u.x) : 0.f;
   const float dmi = (fi0 > 0.f && fi0 < last) ? bot - top : 0.f;
   float3 dfj, dfi;
-  sheet_jacobian(c, side, dfj, dfi);
+  sheet_jacobian_of(sm, c, side, dfj, dfi);
   float3 g = make_float3(dmj * dfj.x + dmi * dfi.x, dmj * dfj.y + dmi * dfi.y, dmj * dfj.z + dmi * dfi.z);
   const float r = dot3(g, c);
   grad = make_float3(g.x - r * c.x, g.y - r * c.y, g.z - r * c.z);
@@ -220,7 +221,8 @@ __device__ __forceinline__ float master_and_slope(const float2* __restrict__ vp,
 // sheet's texels, so the bilinear value and its exact slopes (master_and_slope's) come with the
 // table's interpolated gradient (grad_at_pair's), from one map to the square and one pair of loads.
 __device__ __forceinline__ float4 grad_and_slope(const float* __restrict__ gp, float3 c, int side, float3& grad) {
-  const float2 uv = sphere_to_square_fast(c);
+  const SquareMap sm = square_map(c);
+  const float2 uv = sm.uv;
   const float last = (float)(side - 1);
   const float fj0 = (uv.x + 1.f) * 0.5f * last, fi0 = (uv.y + 1.f) * 0.5f * last;
   const float fj = fminf(fmaxf(fj0, 0.f), last), fi = fminf(fmaxf(fi0, 0.f), last);
@@ -236,7 +238,7 @@ __device__ __forceinline__ float4 grad_and_slope(const float* __restrict__ gp, f
   const float dmj = (fj0 > 0.f && fj0 < last) ? (1.f - ti) * (tb.w - ta.w) + ti * (td.w - tc.w) : 0.f;
   const float dmi = (fi0 > 0.f && fi0 < last) ? bot.w - top.w : 0.f;
   float3 dfj, dfi;
-  sheet_jacobian(c, side, dfj, dfi);
+  sheet_jacobian_of(sm, c, side, dfj, dfi);
   const float3 g = make_float3(dmj * dfj.x + dmi * dfi.x, dmj * dfj.y + dmi * dfi.y, dmj * dfj.z + dmi * dfi.z);
   const float r = dot3(g, c);
   grad = make_float3(g.x - r * c.x, g.y - r * c.y, g.z - r * c.z);
