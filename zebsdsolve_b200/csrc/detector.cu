@@ -191,7 +191,6 @@ __global__ void __launch_bounds__(256) k_refine_direct(DetArgs a) {
   __shared__ float red[24 * 8];
   __shared__ uint32_t hist[32 * 32];
   __shared__ float4 sh_q;
-  __shared__ int sh_done;
   const int b = blockIdx.x;
   const int hw = a.h * a.w;
   const float4 it = a.items[b];
@@ -246,7 +245,6 @@ __global__ void __launch_bounds__(256) k_refine_direct(DetArgs a) {
     r[0] = qf.x; r[1] = qf.y; r[2] = qf.z; r[3] = qf.w;
     r[4] = best; r[5] = v; r[6] = last_good; r[7] = a.o.stamp;
   }
-  (void)sh_done;
 }
 
 __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
@@ -571,10 +569,10 @@ static size_t det_smem(DetArgs& a) {
 // (row << 16) | col, zeb_mask_list); a block of 128 threads per item keeps only the pattern's
 // values along the list in shared memory (4 bytes a pixel, 8 with NMI's simulated values), so
 // that six items share an SM and one item's serial phase (the reduction and thread 0's step)
-// overlaps the others' pixel passes.  Each pass recomputes the detector ray of every pixel (nine
+// overlaps the others' pixel passes (256 or 512 threads where those values pass 36 or 72 KB, so
+// that the warps an SM holds stay about as many for a large detector's list).  Each pass recomputes the detector ray of every pixel (nine
 // FMAs and a reciprocal square root) instead of keeping it; the sums per pixel are those of
 // k_refine.
-constexpr int RL_THREADS = 128;
 
 // the block size for a list whose pattern values and simulated values take `smem` bytes
 inline int rl_threads(size_t smem) { return smem <= 36 * 1024 ? 128 : (smem <= 72 * 1024 ? 256 : 512); }
