@@ -2,7 +2,6 @@
 zebsdsolve `src/master.zig`)."""
 import json
 import math
-import zipfile
 
 import numpy as np
 

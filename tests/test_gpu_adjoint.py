@@ -6,8 +6,6 @@ device's own forward; the reference's Gauss–Newton sums (mode 2) against the o
 restatement of detector.wgsl `sums`; and the Levenberg–Marquardt settle against the oracle's,
 on patterns simulated with jittered pattern centres and perturbed orientations.
 """
-import ctypes
-import math
 import tempfile
 
 import numpy as np
@@ -19,7 +17,6 @@ pytestmark = pytest.mark.gpu
 import oracle.detector as od  # noqa: E402
 import oracle.geometry as og  # noqa: E402
 import oracle.rot as orot  # noqa: E402
-import oracle.sym as osym  # noqa: E402
 
 
 @pytest.fixture(scope="module")

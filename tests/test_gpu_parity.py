@@ -13,7 +13,6 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 import oracle.detector as od  # noqa: E402
-import oracle.geometry as og  # noqa: E402
 import oracle.master as om  # noqa: E402
 import oracle.prep as op  # noqa: E402
 import oracle.sh as osh  # noqa: E402

@@ -4,7 +4,6 @@ master), and the sphere/correlation path checked against the quadrature integral
 import math
 
 import numpy as np
-import pytest
 
 from oracle import geometry, lambert, rot, sh, spherical
 

@@ -13,9 +13,10 @@ reference's: quaternions (w, x, y, z) map sample directions to crystal direction
 in radians, map cells row-major, the pattern centre in the Bruker convention.
 
 Every computation on the path runs in the CUDA library libzebsdsolve_b200.so (hand-written
-sm_100a kernels behind the C ABI of include/zebsdsolve_b200.h); there is no CPU fallback.
+sm_100a kernels behind the C ABI of include/zebsdsolve_b200.h); there is no CPU fallback. The
+reference's own C ABI, its ze_* calls, is libzebsdsolve.so (include/zebsdsolve.h, ze_abi.py),
+which carries each call onto this package's Solver.
 """
-import json
 
 import numpy as np
 
@@ -30,7 +31,7 @@ class Error(RuntimeError):
 
 
 def _engine():
-    from .engine import Engine, EngineError
+    from .engine import Engine
 
     try:
         return Engine()
@@ -163,8 +164,6 @@ class Solver:
         """Write the results by the path's extension (__init__.py:879-905): an EDAX .ang or an HKL
         .ctf, the orientations in the engine's own frame. (The reference's .h5oina export copies an
         Oxford acquisition's HDF5 file: not part of this engine.)"""
-        from . import output
-
         ext = str(path).rsplit(".", 1)[-1].lower()
         if ext not in ("ang", "ctf"):
             raise Error(f"export: .{ext} is not written by this engine (.ang, .ctf)")

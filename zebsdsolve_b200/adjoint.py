@@ -12,7 +12,6 @@ from the reference's 43 sums (`zeb_det6` mode 2); the gradient is the reference'
 table's) or the exact adjoint's (the kernel behind ProjectedNCC's backward).
 """
 import ctypes
-import math
 
 import numpy as np
 import torch

@@ -15,7 +15,6 @@ fixed-array, extensible-array and version 2 B-tree chunk indexes of files writte
 libver="latest", external links, virtual datasets and other filters.
 """
 import os
-import struct
 import zlib
 
 import numpy as np
