@@ -227,16 +227,15 @@ def ze_settings(x, buf, cap):
 @_api("events", 0)
 def ze_events(x, buf, cap):
     x.pending += b"".join(json.dumps(e).encode() + b"\n" for e in x.s.events())
-    if not x.pending:
-        return 0
-    # whole lines only; a line longer than the buffer is dropped
-    cut = x.pending.rfind(b"\n", 0, int(cap)) + 1
-    if cut == 0:
+    # whole lines only; a line longer than the whole buffer is dropped (0 means no lines are left)
+    while x.pending:
+        cut = x.pending.rfind(b"\n", 0, int(cap)) + 1
+        if cut:
+            n = _put(buf, cap, x.pending[:cut])
+            x.pending = x.pending[cut:]
+            return n
         x.pending = x.pending[x.pending.find(b"\n") + 1:]
-        return 0
-    n = _put(buf, cap, x.pending[:cut])
-    x.pending = x.pending[cut:]
-    return n
+    return 0
 
 
 def ze_cancel(h):
