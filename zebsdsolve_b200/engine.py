@@ -758,11 +758,11 @@ class Engine:
                0.0, mask, 0, ptr(out), None, stream_ptr())
         return out.reshape(oh, ow).cpu().numpy()
 
-    def preprocess(self, raw, n, cells=None):
+    def preprocess(self, raw, n, cells=None, out=None):
         """engine.zig:1452-1563, prep.zig:143-204 — n stored patterns on the device (raw, the scan's
-        pixel type) through the filter chain into the float32 pattern buffer: with nlpar, first
-        averaged with their neighbours (the cells' windows read from the scan); static background,
-        dynamic background, CLAHE, band pass, then the mask and the normalization."""
+        pixel type) through the filter chain into the float32 pattern buffer (or `out`): with nlpar,
+        first averaged with their neighbours (the cells' windows read from the scan); static
+        background, dynamic background, CLAHE, band pass, then the mask and the normalization."""
         rows, cols, sh, sw = self.info()
         h, w = self.pattern_shape()  # reduced by binning as the patterns are unpacked
         s = self.set
@@ -770,15 +770,16 @@ class Engine:
             if cells is None:
                 raise EngineError("nlpar: the cells of the patterns are needed to average them with their neighbours")
             raw = self.nlpar_average(cells)
-            return self.filter_chain(raw, 2, n, h, w, 1.0)
-        return self.filter_chain(raw, self.pixel, n, sh, sw, self.factor())
+            return self.filter_chain(raw, 2, n, h, w, 1.0, out=out)
+        return self.filter_chain(raw, self.pixel, n, sh, sw, self.factor(), out=out)
 
-    def filter_chain(self, raw, pixel, n, sh, sw, factor, out_name="pats"):
+    def filter_chain(self, raw, pixel, n, sh, sw, factor, out_name="pats", out=None):
         """prep.zig:143-204 — n patterns (pixel type, stored size sh × sw reduced by factor) through
-        static background, dynamic background, CLAHE, band pass, mask and normalization."""
+        static background, dynamic background, CLAHE, band pass, mask and normalization, into the
+        buffer `out_name` (or `out`, n·h·w float32 on the device)."""
         h, w = self.pattern_shape()
         s = self.set
-        out = self.buf(out_name, n * h * w)
+        out = self.buf(out_name, n * h * w) if out is None else out
         static = self.static_background()
         dyn, sigma = self.prep_options()
         mask = (ctypes.c_float * 3)(*self.mask_of(h, w))
@@ -820,10 +821,10 @@ class Engine:
         """What the filter chain's output depends on: the scan, every setting, the level."""
         return (self.patterns.shape, self.set.to_json(), self._full, self.pattern_shape(), self.factor())
 
-    def keep_prepared(self, pats, cells):
-        """A whole pass's filtered patterns kept on the device, the scan's rows [cell][h·w] in FP32,
-        where the scan fits RESIDENT_FRAC of the device's memory: what refine_patterns then starts
-        from without uploading and filtering the patterns again (prepared)."""
+    def _resident_buffer(self):
+        """The kept filtered scan's buffer for the current scan and settings (made, or re-keyed with
+        no row valid, when they changed), or None where the scan does not fit RESIDENT_FRAC of the
+        device's memory."""
         rows, cols = self.info()[:2]
         h, w = self.pattern_shape()
         total = rows * cols * h * w
@@ -832,12 +833,51 @@ class Engine:
         if r is None or r["key"] != key:
             if total * 4 > self.RESIDENT_FRAC * torch.cuda.get_device_properties(self.dev).total_memory:
                 self._resident = None
-                return
+                return None
             old = r["pats"] if r is not None and r["pats"].numel() >= total else None
             self._resident = None
             r = {"key": key, "pats": old if old is not None else torch.empty(total, dtype=torch.float32, device=self.dev),
                  "valid": np.zeros(rows * cols, bool)}
             self._resident = r
+        return r
+
+    def resident_rows(self, cells):
+        """Where a whole pass over a run of consecutive cells filters its patterns in place: those
+        cells' rows of the kept filtered scan (a flat view), or None (scattered cells, or a scan too
+        large to keep), for which keep_prepared copies the filtered batch instead."""
+        c = np.asarray(cells, np.int64)
+        n = len(c)
+        if n == 0 or c[-1] - c[0] != n - 1 or (n > 1 and not (np.diff(c) == 1).all()):
+            return None
+        r = self._resident_buffer()
+        if r is None:
+            return None
+        rows, cols = self.info()[:2]
+        h, w = self.pattern_shape()
+        view = r["pats"][: rows * cols * h * w].view(rows * cols, h * w)
+        return view[int(c[0]):int(c[0]) + n].reshape(-1)
+
+    def filter_pass(self, raw, n, cells):
+        """preprocess for a device pass; a whole pass keeps its filtered patterns (in place for a
+        run of consecutive cells, else copied by keep_prepared)."""
+        direct = self.resident_rows(cells) if self._whole_pass else None
+        pats = self.preprocess(raw, n, cells, out=direct)
+        if direct is not None:
+            self._resident["valid"][np.asarray(cells, np.int64)] = True
+        elif self._whole_pass:
+            self.keep_prepared(pats, cells)
+        return pats
+
+    def keep_prepared(self, pats, cells):
+        """A whole pass's filtered patterns kept on the device, the scan's rows [cell][h·w] in FP32,
+        where the scan fits RESIDENT_FRAC of the device's memory: what refine_patterns then starts
+        from without uploading and filtering the patterns again (prepared)."""
+        r = self._resident_buffer()
+        if r is None:
+            return
+        rows, cols = self.info()[:2]
+        h, w = self.pattern_shape()
+        total = rows * cols * h * w
         n = len(cells)
         view = r["pats"][:total].view(rows * cols, h * w)
         src = pats[: n * h * w].view(n, h * w)
@@ -985,9 +1025,11 @@ class Engine:
         self._spans[key] = sp
         return sp
 
-    def run_device(self, raw, cells, bandwidth=None, timer=None, method="spherical", grid=None):
+    def run_device(self, raw, cells, bandwidth=None, timer=None, method="spherical", grid=None, pre=None):
         """One pass of the device path over n = len(cells) stored patterns already on the device:
-        records [phase][cell][8] as a device tensor (engine.zig:2005-2122, no readback)."""
+        records [phase][cell][8] as a device tensor (engine.zig:2005-2122, no readback). pre: the
+        cells' items already on the device with their bounding box (items_of's two results), as
+        index_pipelined copies them ahead of the pass's patterns."""
         self.counts["submits"] += 1
         if method != "spherical":
             return self.run_device_dictionary(raw, cells, method, int(grid or self.set["dict_grid"]), timer)
@@ -998,10 +1040,11 @@ class Engine:
         fr = self.frame()
         mark = timer.mark if timer is not None else (lambda name: None)
         mark("prep")
-        pats = self.preprocess(raw, n, cells)
-        if self._whole_pass:
-            self.keep_prepared(pats, cells)
-        items = self.items_of(cells)
+        pats = self.filter_pass(raw, n, cells)
+        if pre is not None:
+            items, self._batch_t = pre
+        else:
+            items = self.items_of(cells)
         self.batch_stamp = self.batch_stamp % (1 << 24) + 1
         bt = b["tables"]
         recs = self.buf("recs", n_ph * n * 8)
@@ -1087,9 +1130,7 @@ class Engine:
         fr = self.frame()
         mark = timer.mark if timer is not None else (lambda name: None)
         mark("prep")
-        pats = self.preprocess(raw, n, cells)
-        if self._whole_pass:
-            self.keep_prepared(pats, cells)
+        pats = self.filter_pass(raw, n, cells)
         items = self.items_of(cells)
         self.batch_stamp = self.batch_stamp % (1 << 24) + 1
         recs = self.buf("recs", n_ph * n * 8)
@@ -1451,10 +1492,19 @@ class Engine:
         comp_done = [None, None]
         back = [None, None]  # (event, cells, stamp)
 
+        pre = [None, None]
+
         def issue_upload(i):
             k = i % 2
             if comp_done[k] is not None:
                 cps.wait_event(comp_done[k])  # the pass that last read this buffer has finished
+            if method == "spherical":
+                # the cells' detector positions, copied on this stream ahead of their patterns: a
+                # small copy on the compute stream would wait behind the next pass's upload
+                with torch.cuda.stream(cps):
+                    items = self.items_of(parts[i])
+                items.record_stream(comp)
+                pre[k] = (items, self._batch_t)
             self.upload_raw(parts[i], raw[k], cps)
             ev = torch.cuda.Event()
             ev.record(cps)
@@ -1476,7 +1526,7 @@ class Engine:
             k = i % 2
             comp.wait_event(up_done[k])
             cb = parts[i]
-            recs = self.run_device(raw[k][: len(cb)], cb, bandwidth, method=method, grid=grid)
+            recs = self.run_device(raw[k][: len(cb)], cb, bandwidth, method=method, grid=grid, pre=pre[k])
             ev = torch.cuda.Event()
             ev.record(comp)
             comp_done[k] = ev
