@@ -29,6 +29,7 @@ import os
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -270,17 +271,59 @@ def config_of(a, n):
 # ── the device ──
 
 class Clocks:
-    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+    """Samples of the SM clock and the throttle reasons during the timed region: read through NVML
+    (read-only queries) every 10 ms on a thread, or from nvidia-smi at 200 ms where NVML is not
+    available."""
+
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index, off=False):
         self.index = index
         self.off = off
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []  # (sm MHz, max sm MHz, reasons)
+
+    def _nvml_handle(self, nv):
+        """The NVML handle of this process's CUDA device: by its UUID (CUDA_VISIBLE_DEVICES may
+        renumber the devices), else by index."""
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(int(self.index)).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(int(self.index))
+
+    def _nvml_loop(self, h, nv, stop):
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while True:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                why = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), tuple(n for n, b in zip(self.REASONS, bits) if why & b)))
+            except Exception:
+                pass
+            if stop.wait(0.01):
+                return
 
     def __enter__(self):
         if self.off:
             return self
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            self._stop = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(h, nv, self._stop), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         self.path = tempfile.mktemp(suffix=".csv")
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -293,21 +336,29 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join()
         if self.proc is not None:
             self.proc.terminate()
             self.proc.wait()
+            try:
+                for l in open(self.path).read().strip().splitlines():
+                    r = [x.strip() for x in l.split(",")]
+                    if len(r) >= 7 and r[0].replace(".", "").isdigit():
+                        why = tuple(n for k, n in enumerate(self.REASONS) if "Active" in r[3 + k] and "Not" not in r[3 + k])
+                        self.rows.append((float(r[0]), float(r[1]) if r[1].replace(".", "").isdigit() else None, why))
+            except Exception:
+                pass
 
     def summary(self):
-        try:
-            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
-        except Exception:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 3 + k and "Active" in r[3 + k] and "Not" not in r[3 + k]})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows if r[1] is not None]
+        reasons = sorted({n for r in self.rows for n in r[2]})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows), "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
 class StageTimer:
