@@ -803,17 +803,17 @@ def ze_results(x, kind, out, cap):
             raise ValueError("BufferTooSmall")
         b = np.asarray(res["euler"], np.float32).reshape(n, 3).copy()
         b[res["phase"] < 0] = 0
-        ctypes.memmove(out, b.tobytes(), 12 * n)
+        ctypes.memmove(out, b.ctypes.data, 12 * n)
         return 3 * n
     src = {0: ("quat", np.float32), 1: ("ncc", np.float32), 2: ("nmi", np.float32), 3: ("phase", np.int32),
            5: ("z", np.float32), 6: ("sweep", np.int32)}.get(int(kind))
     if src is None:
         raise ValueError("UnknownKind")
-    data = np.ascontiguousarray(res[src[0]], src[1]).tobytes()
-    if cap < len(data):
+    data = np.ascontiguousarray(res[src[0]], src[1])
+    if cap < data.nbytes:
         raise ValueError("BufferTooSmall")
-    ctypes.memmove(out, data, len(data))
-    return len(data) // 4
+    ctypes.memmove(out, data.ctypes.data, data.nbytes)
+    return data.nbytes // 4
 
 
 ze_map = _not_built("map", "colour maps (IPF, scores) are not part of this engine; ze_results gives the values")
