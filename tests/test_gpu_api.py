@@ -216,3 +216,25 @@ def test_binned_search_refined_or_scored_at_the_stored_size(scan):
     apart = np.degrees(s.disorientation(rb["refine"]["quaternions"].reshape(-1, 4), r1["quaternions"].reshape(-1, 4)))
     assert np.median(apart) < 0.02 and (apart < 0.1).mean() > 0.95, np.sort(apart)[-4:]
     assert abs(float(rb["refine"]["ncc"].mean() - r1["ncc"].mean())) < 2e-3
+
+
+def test_static_background_summed_on_the_device_equals_the_host_sum(scan):
+    """The average of the lattice's stored patterns (engine.zig:1344-1424), summed on the device for
+    integer pixels: the same float32 image as the host's float64 sum, bit for bit (the sum of
+    integers is exact in any order)."""
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200.reduce import reduce_image
+
+    rng = np.random.default_rng(4)
+    for dt, top in ((np.uint16, 60000), (np.uint8, 250)):
+        pats = rng.integers(0, top, (23, 31, 40, 44)).astype(dt)
+        s = ze.Solver()
+        s.configure(static_background="average", static_patterns=500)
+        s.add_phase(scan["path"])
+        s.set_patterns(pats)
+        e = s._e
+        got = e.static_background().cpu().numpy()
+        cells = e.lattice(500)
+        acc = pats.reshape(-1, 40, 44)[cells].sum(0, dtype=np.float64)
+        want = reduce_image(acc / len(cells), e.factor()).astype(np.float32)
+        assert np.array_equal(got, want), dt

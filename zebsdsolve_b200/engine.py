@@ -359,11 +359,21 @@ class Engine:
         if self.avg is None or self.avg[0] != key:
             cells = self.lattice(self.set["static_patterns"])
             rows, cols, h, w = self.info()
-            flat = self.patterns.reshape(rows * cols, h, w)
-            acc = np.zeros((h, w))
-            for i in range(0, len(cells), 1024):
-                acc += flat[cells[i:i + 1024]].sum(0, dtype=np.float64)
-            avg = reduce_image(acc / len(cells), self.factor()).astype(np.float32)
+            n = len(cells)
+            if self.pixel in (0, 1):
+                # integer pixels: the sum is an exact integer in any order, so the device sums the
+                # lattice's patterns (one copy of them, gathered on the host threads)
+                raw = self.buf("static_raw", n * h * w, self.raw_dtype())[: n * h * w].view(n, h, w)
+                self.upload_raw(cells, raw, torch.cuda.current_stream())
+                x = raw.view(n, h * w)
+                x = (x.view(torch.int16).to(torch.int32) & 0xFFFF) if self.pixel == 1 else x.to(torch.int32)
+                acc = x.sum(0, dtype=torch.int64).view(h, w).cpu().numpy().astype(np.float64)
+            else:
+                flat = self.patterns.reshape(rows * cols, h, w)
+                acc = np.zeros((h, w))
+                for i in range(0, n, 1024):
+                    acc += flat[cells[i:i + 1024]].sum(0, dtype=np.float64)
+            avg = reduce_image(acc / n, self.factor()).astype(np.float32)
             self.avg = (key, torch.as_tensor(avg, device=self.dev))
             self.log(f"static background: the average of {len(cells)} patterns over the map")
         return self.avg[1]
