@@ -1492,9 +1492,15 @@ class Engine:
         # the copy stream starts after everything already queued on the compute stream: memory the
         # caching allocator hands out here may have been freed by work still pending there
         cps.wait_stream(comp)
-        host = [torch.empty((n_ph, B, 8), dtype=torch.float32, pin_memory=True) for _ in range(2)]
-        hfz = [torch.empty((n_ph, B, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
-        hbg = [torch.empty((n_ph, B, 3), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+        host = [torch.empty(n_ph * B * 8, dtype=torch.float32, pin_memory=True) for _ in range(2)]
+        hfz = [torch.empty(n_ph * B * 4, dtype=torch.float32, pin_memory=True) for _ in range(2)]
+        hbg = [torch.empty(n_ph * B * 3, dtype=torch.float32, pin_memory=True) for _ in range(2)]
+
+        def hv(buf, m, width):
+            """A pass of m cells' readback, [phase][m][width], at the start of a page-locked buffer:
+            contiguous, so that the copy into it stays asynchronous (a strided destination would be
+            staged through pageable memory, the host waiting for the pass)."""
+            return buf[: n_ph * m * width].view(n_ph, m, width)
         # a small first pass (its upload is the one nothing hides), then passes of B
         first = min(len(cells), max(1, B // 4))
         parts = [cells[:first]] + [cells[i:i + B] for i in range(first, len(cells), B)]
@@ -1526,9 +1532,9 @@ class Engine:
             self.counts["reads"] += 2  # the records and their fundamental-zone orientations
             self.counts["waits"] += 1
             back[k] = None
-            out = host[k][:, : len(cb)].numpy().copy()
-            fz = hfz[k][:, : len(cb)].numpy().copy()
-            bg = hbg[k][:, : len(cb)].numpy().copy()
+            out = hv(host[k], len(cb), 8).numpy().copy()
+            fz = hv(hfz[k], len(cb), 4).numpy().copy()
+            bg = hv(hbg[k], len(cb), 3).numpy().copy()
             on_batch(cb, self.finish(out, stamp), fz, bg)
 
         issue_upload(0)
@@ -1547,9 +1553,9 @@ class Engine:
             if back[k] is not None:
                 drain(k)
             fzd, bgd = self.fz_of(recs)
-            host[k][:, : len(cb)].copy_(recs, non_blocking=True)
-            hfz[k][:, : len(cb)].copy_(fzd, non_blocking=True)
-            hbg[k][:, : len(cb)].copy_(bgd, non_blocking=True)
+            hv(host[k], len(cb), 8).copy_(recs, non_blocking=True)
+            hv(hfz[k], len(cb), 4).copy_(fzd, non_blocking=True)
+            hv(hbg[k], len(cb), 3).copy_(bgd, non_blocking=True)
             evb = torch.cuda.Event()
             evb.record(comp)
             back[k] = (evb, cb, self.batch_stamp)
