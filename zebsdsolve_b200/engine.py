@@ -1674,19 +1674,36 @@ class Engine:
             for p in np.unique(best):
                 sel = best == p
                 q[sel] = R.to_fz(r[sel, :4].astype(np.float64), self.phases[int(p)].master.rotations())
-        idx = cells[replace]
-        res["quat"][idx] = q[replace]
-        if bunge is not None and fz is not None:
-            res["euler"][idx] = bunge[best, np.arange(len(cells))][replace]
+        n = len(cells)
+        if n and replace.all() and cells[-1] - cells[0] == n - 1 and (n == 1 or (np.diff(cells) == 1).all()):
+            # every cell of a run of consecutive cells takes its record (a first sweep's pass): the
+            # same writes as slices
+            sel = slice(int(cells[0]), int(cells[0]) + n)
+            res["quat"][sel] = q
+            if bunge is not None and fz is not None:
+                res["euler"][sel] = bunge[best, np.arange(n)]
+            else:
+                res["euler"][sel] = R.to_bunge(q.astype(np.float64)).astype(np.float32)
+            res["ncc"][sel] = r[:, 4]
+            res["nmi"][sel] = r[:, 5]
+            res["z"][sel] = r[:, 7]
+            res["phase"][sel] = best
+            res["settled"][sel] = r[:, 6] <= settle
         else:
-            res["euler"][idx] = R.to_bunge(q[replace].astype(np.float64)).astype(np.float32)
-        res["ncc"][idx] = r[replace, 4]
-        res["nmi"][idx] = r[replace, 5]
-        res["z"][idx] = r[replace, 7]
-        res["phase"][idx] = best[replace]
-        res["settled"][idx] = r[replace, 6] <= settle
-        kept = res["nmi"][cells] >= s["accept_nmi"] if s["accept_nmi"] > 0 else res["z"][cells] >= s["accept_z"]
-        newly = (res["sweep"][cells] < 0) & kept & res["settled"][cells]
+            sel = cells
+            idx = cells[replace]
+            res["quat"][idx] = q[replace]
+            if bunge is not None and fz is not None:
+                res["euler"][idx] = bunge[best, np.arange(n)][replace]
+            else:
+                res["euler"][idx] = R.to_bunge(q[replace].astype(np.float64)).astype(np.float32)
+            res["ncc"][idx] = r[replace, 4]
+            res["nmi"][idx] = r[replace, 5]
+            res["z"][idx] = r[replace, 7]
+            res["phase"][idx] = best[replace]
+            res["settled"][idx] = r[replace, 6] <= settle
+        kept = res["nmi"][sel] >= s["accept_nmi"] if s["accept_nmi"] > 0 else res["z"][sel] >= s["accept_z"]
+        newly = (res["sweep"][sel] < 0) & kept & res["settled"][sel]
         res["sweep"][cells[newly]] = self.index_sweep
         self.index_accepted += int(newly.sum())
         self.index_done += len(cells)
