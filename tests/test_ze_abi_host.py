@@ -281,3 +281,122 @@ def test_phases_indexing_and_fits(lib, eng):
     b = np.array([0, 0, 0, 1], np.float32)
     assert lib.ze_disorientation(h, 0, a.ctypes.data, b.ctypes.data) == pytest.approx(0.0, abs=1e-6)
     assert lib.ze_disorientation(h, 7, a.ctypes.data, b.ctypes.data) == pytest.approx(np.pi, abs=1e-6)
+
+
+class _FitSolver(_Solver):
+    """The stand-in with a pattern-centre search, a plane fit, an NLPAR view and an export."""
+
+    def __init__(self):
+        super().__init__()
+        ax = (np.array([0.4, 0.5, 0.6]), np.array([0.2, 0.3]), np.array([0.55]))
+        self._e.pc_history = [{"axes": ax, "scores": np.arange(6, dtype=np.float32), "best": 4, "walked": True,
+                               "pat_best": np.array([1, 4, 5], np.uint32), "pat_ncc": np.array([0.3, 0.4, 0.5], np.float32),
+                               "pat_scores": np.arange(18, dtype=np.float32), "density": np.ones(6, np.float32),
+                               "peak": (1.5, 0.5, 0.0), "ballots": 3, "inliers": 2}]
+        self._e.plane_points = {"cells": np.array([3, 9], np.uint64), "pc": np.array([[0.5, 0.3, 0.6], [0.51, 0.31, 0.61]]),
+                                "fit": np.array([[0.5, 0.3, 0.6], [0.5, 0.3, 0.6]]), "ncc": np.array([0.7, 0.8]),
+                                "used": np.array([True, False])}
+
+    def fit_pc(self):
+        return {"pc": [0.5, 0.3, 0.6], "start": [0.5, 0.5, 0.5], "score": 0.8, "start_score": 0.6, "n_patterns": 25,
+                "n_candidates": 125, "levels": 3, "at_border": False}
+
+    def fit_plane(self):
+        return {"plane": np.arange(12, dtype=np.float64).reshape(4, 3), "kind": "affine", "frame": "follow",
+                "model": "line", "method": "points", "models": {"centre": {"cv": 0.2, "cv_se": 0.01}},
+                "pc": [0.5, 0.3, 0.6], "pc_se": [1e-3, 2e-3, 3e-3], "start_pc": [0.5, 0.5, 0.5], "rot": [0.0, 0.01, 0.0],
+                "n_patterns": 40, "n_used": 38, "rmsd": [1e-3, 1e-3, 2e-3], "ncc": 0.8, "start_ncc": 0.7, "iterations": 6,
+                "said": {"rot": [0.0, 0.02, 0.0], "rot_se": [1e-3] * 3, "step": [1.0, 1.01], "step_se": [1e-3, 1e-3],
+                         "skew": 0.001, "skew_se": 1e-4, "blocks": 5}}
+
+    def nlpar_view(self):
+        return {"noise": 2.0, "left": 0.4, "own": 0.3, "shares": np.arange(9, dtype=np.float32).reshape(3, 3)}
+
+    def pattern_stats(self, cells):
+        c = np.asarray(cells, np.float32)
+        return c + 0.5, c * 2
+
+    def master(self, phase):
+        return np.arange(2 * 201 * 201, dtype=np.float32).reshape(2, 201, 201)
+
+    def export_text(self, kind):
+        return f"# {kind} header\n1 2 3\n"
+
+
+@pytest.fixture()
+def fit_eng():
+    h = 0x7F10
+    Z._handles[h] = Z._Handle(_FitSolver())
+    yield h, Z._handles[h].s
+    Z._handles.pop(h, None)
+
+
+def _fn(lib, name, args, res):
+    fn = getattr(lib, name)
+    fn.argtypes, fn.restype = args, res
+    return fn
+
+
+def test_fits_grids_and_exports(lib, fit_eng):
+    h, s = fit_eng
+    pr = Z.PcResult()
+    assert _fn(lib, "ze_fit_pc", [P, ctypes.POINTER(Z.PcResult)], I32)(h, ctypes.byref(pr)) == 0
+    assert list(pr.pc) == [0.5, 0.3, 0.6] and (pr.n_patterns, pr.n_candidates, pr.levels, pr.at_border) == (25, 125, 3, 0)
+    # the last grid: its shape and size first, then its values
+    shape = np.empty(3, np.uint32)
+    scores_fn = _fn(lib, "ze_pc_scores", [P, P, P, SZ, P, SZ], I32)
+    assert scores_fn(h, shape.ctypes.data, None, 0, None, 0) == 6 and list(shape) == [1, 2, 3]
+    axes, sc = np.empty(6), np.empty(6, np.float32)
+    assert scores_fn(h, shape.ctypes.data, axes.ctypes.data, 6, sc.ctypes.data, 6) == 6
+    assert np.allclose(axes, [0.4, 0.5, 0.6, 0.2, 0.3, 0.55]) and np.array_equal(sc, np.arange(6))
+    assert _fn(lib, "ze_pc_level_count", [P], U32)(h) == 1
+    info = np.empty(2, np.uint32)
+    best, ncc = np.empty(3, np.uint32), np.empty(3, np.float32)
+    level = _fn(lib, "ze_pc_level", [P, U32, P, P, P, SZ, P, SZ, P, P, SZ], I32)
+    assert level(h, 0, shape.ctypes.data, info.ctypes.data, axes.ctypes.data, 6, sc.ctypes.data, 6, best.ctypes.data,
+                 ncc.ctypes.data, 3) == 6
+    assert list(info) == [4, 1] and list(best) == [1, 4, 5] and np.allclose(ncc, [0.3, 0.4, 0.5])
+    assert level(h, 1, shape.ctypes.data, info.ctypes.data, None, 0, None, 0, None, None, 0) == -1
+    per = np.empty(18, np.float32)
+    assert _fn(lib, "ze_pc_level_scores", [P, U32, P, SZ], I32)(h, 0, per.ctypes.data, 18) == 18
+    dinfo, den = np.empty(5), np.empty(6, np.float32)
+    assert _fn(lib, "ze_pc_level_ballots", [P, U32, P, SZ, P], I32)(h, 0, den.ctypes.data, 6, dinfo.ctypes.data) == 6
+    assert list(dinfo) == [1.5, 0.5, 0.0, 3.0, 2.0] and np.array_equal(den, np.ones(6))
+    # the plane fit into planefit.zig's struct; its points
+    r = Z.PlaneResult()
+    assert _fn(lib, "ze_fit_plane", [P, ctypes.POINTER(Z.PlaneResult)], I32)(h, ctypes.byref(r)) == 0
+    assert list(r.plane) == list(range(12)) and (r.kind, r.frame, r.model, r.method, r.compared) == (1, 1, 1, 1, 1)
+    assert (r.n_patterns, r.n_used, r.iterations, r.blocks) == (40, 38, 6, 5) and r.cv[0] == 0.2 and r.cv[1] == 0.0
+    assert list(r.step) == [1.0, 1.01] and r.skew == 0.001 and list(r.pc_se) == [1e-3, 2e-3, 3e-3]
+    pts_fn = _fn(lib, "ze_plane_points", [P, P, SZ], SZ)
+    n = pts_fn(h, None, 0)
+    pts = (Z.PlanePoint * n)()
+    assert n == 2 and pts_fn(h, ctypes.cast(pts, P), n) == 2
+    assert (pts[0].cell, pts[1].cell, pts[0].used, pts[1].used) == (3, 9, 1, 0) and list(pts[1].pc) == [0.51, 0.31, 0.61]
+    # NLPAR's view: its side first, then the shares
+    out3 = np.empty(3, np.float32)
+    view = _fn(lib, "ze_nlpar_view", [P, P, P, SZ], U32)
+    assert view(h, out3.ctypes.data, None, 0) == 3 and np.allclose(out3, [2.0, 0.4, 0.3])
+    shares = np.empty(9, np.float32)
+    assert view(h, out3.ctypes.data, shares.ctypes.data, 9) == 3 and np.array_equal(shares, np.arange(9))
+    # statistics of given cells, two values a cell; a buffer too small is refused
+    cells = np.array([2, 5], np.uint64)
+    st = np.empty(4, np.float32)
+    stats = _fn(lib, "ze_pattern_stats", [P, P, SZ, P, SZ], I32)
+    assert stats(h, cells.ctypes.data, 2, st.ctypes.data, 4) == 0 and list(st) == [2.5, 4.0, 5.5, 10.0]
+    assert stats(h, cells.ctypes.data, 2, st.ctypes.data, 3) < 0 and "BufferTooSmall" in _err(lib, h)
+    # the master image; the export's size, then its text
+    img = np.empty(2 * 201 * 201, np.float32)
+    mi = _fn(lib, "ze_master_image", [P, U32, P, SZ], I32)
+    assert mi(h, 0, img.ctypes.data, img.size) == 0 and img[-1] == img.size - 1
+    assert mi(h, 0, img.ctypes.data, 10) < 0 and "BufferTooSmall" in _err(lib, h)
+    ex = _fn(lib, "ze_export", [P, U32, P, SZ], I64)
+    size = ex(h, 1, None, 0)
+    text = ctypes.create_string_buffer(size)
+    assert ex(h, 1, text, size) == size and text.raw[:size] == b"# ctf header\n1 2 3\n"
+    assert ex(h, 5, None, 0) < 0 and "UnknownKind" in _err(lib, h)
+    # the search given by the caller is checked before it runs
+    rec = np.empty(16, np.float32)
+    by = _fn(lib, "ze_index_cells_by", [P, P, SZ, U32, U32, U32, P, SZ], I32)
+    assert by(h, cells.ctypes.data, 2, 0, 4, 30, rec.ctypes.data, 16) < 0 and "BadSetting" in _err(lib, h)
+    assert by(h, cells.ctypes.data, 2, 0, 32, 30, rec.ctypes.data, 16) == 0
