@@ -585,12 +585,13 @@ def test_refine_and_chance_on_a_large_detector_match_oracle(world, lib):
             assert abs(dec[d, i] - vd) < 2e-3
 
 
-@pytest.mark.parametrize("side", [100, 120])
+@pytest.mark.parametrize("side", [100, 120, 160])
 def test_larger_detectors_take_their_own_launch_shapes(world, lib, side):
     """Detectors whose masked-pixel lists leave fewer refinement blocks an SM (100²: 256 threads a
-    pattern; 120²: 512) and, at 120², whose pattern exceeds the ring kernel's 48 KB of shared
-    memory (sampled from global memory): coefficients at L = 64 and the refinement over the shared
-    pixel list against the oracle, with the 60 × 60 bounds."""
+    pattern; 120² and 160²: 512, at 160² with about 160 KB of shared memory, one block an SM) and,
+    from 120², whose pattern exceeds the ring kernel's 48 KB of shared memory (sampled from global
+    memory): coefficients at L = 64 and the refinement over the shared pixel list against the
+    oracle, with the 60 × 60 bounds."""
     import zebsdsolve_b200 as ze
     from zebsdsolve_b200 import rotations as R
     from zebsdsolve_b200.device import BandTables
