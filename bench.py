@@ -90,7 +90,7 @@ def scan_shape(n):
     return int(math.ceil(n / cols)), cols
 
 
-# ── the reference's algorithm on the host (the oracle: the checker and the CPU baseline) ──
+# ── the reference's algorithm on the host (the oracle: parity and the CPU baseline) ──
 
 ORACLE_CELLS = 1024  # the lattice of cells the oracle indexes (>= 1000, spread over the map's grains)
 

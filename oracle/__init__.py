@@ -7,7 +7,7 @@ and its WGSL compute kernels (`shaders/common.wgsl`, `sphere.wgsl`, `so3.wgsl`,
 `detector.wgsl`, `mastersph.wgsl`, `prep.wgsl`).  Every function cites the reference
 file:line it follows.
 
-It is the checker, never the product: only `tests/`, `__graft_entry__.smoke()` and the
+It is the oracle, never the product: only `tests/`, `__graft_entry__.smoke()` and the
 `cpu_baseline` / `--impl reference` legs of `bench.py` may import it.  The product path
 (`zebsdsolve_b200`) never imports it and fails loudly when its CUDA library is missing.
 

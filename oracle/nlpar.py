@@ -1,6 +1,6 @@
 """Non-local pattern averaging: oracle restatement of zebsdsolve `shaders/nlpar.wgsl` and
-`src/nlpar.zig` over a whole map at once (test infrastructure — the checker of zeb_nlpar and
-the engine's windows, never part of the product path).
+`src/nlpar.zig` over a whole map at once (test infrastructure — what zeb_nlpar and the engine's
+windows are tested against, never part of the product path).
 
 For a map of stored patterns P[r, c] (FP64): σ²(i) = ½ min over the eight nearest neighbours of
 the mean squared difference (0 without neighbours); then `passes` passes, each over the

@@ -1,5 +1,5 @@
 """Pattern-centre vote: oracle restatement of zebsdsolve `src/pcfit.zig` (test infrastructure —
-the checker of zebsdsolve_b200.pcfit, never part of the product path).
+what zebsdsolve_b200.pcfit is tested against, never part of the product path).
 
 Scalar Python loops over the vote's host arithmetic, in the reference's order, so that the
 product's vectorized version can be held to the same numbers:

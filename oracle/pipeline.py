@@ -1,5 +1,5 @@
 """The reference's per-scan indexing schedule in FP64, from the oracle's pieces (test
-infrastructure: the checker that the parity tests and the bench's CPU leg run on a workload's own
+infrastructure: the oracle that the parity tests and the bench's CPU leg run on a workload's own
 patterns; nothing here is part of the product).
 
 For one phase and one sweep without CLAHE, band pass or NLPAR (the configurations' settings):

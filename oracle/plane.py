@@ -1,5 +1,5 @@
 """The plane of source points: oracle restatement of zebsdsolve `src/plane.zig` (test
-infrastructure — the checker of zebsdsolve_b200.plane, never part of the product path).
+infrastructure — what zebsdsolve_b200.plane is tested against, never part of the product path).
 
 Scalar loops in the reference's order: Frame.of (plane.zig:106-118), model_at / model (123-142),
 fit_theta (168-233), bounded (236-240), slope_weight (245-248), to_plane (252-273), misfit
