@@ -554,6 +554,19 @@ def device_main(a):
         t = traffic.get(k)
         roof[k] = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
                    "traffic": int(t * batch) if t else None, "ms_per_step": round(ms_k, 3)}
+    if "refine" in roof:
+        # the refinement is bound by its record gathers from the L2-resident table, not by HBM: one
+        # 32-byte FP16 neighbourhood record a masked pixel a pass (refine_iters passes and the
+        # last, with the pattern's values from shared memory)
+        import ctypes
+
+        fr = e.frame()
+        npix = int(_native.load().zeb_mask_pixels(ctypes.byref(fr)))
+        passes = int(s.settings["refine_iters"]) + 1
+        roof["refine"]["l2_gather"] = {
+            "achieved": round(n * passes * npix * 32 / (stages["refine"] / 1e3) / 1e9, 1), "unit": "GB/s",
+            "bytes_per_pattern": passes * npix * 32,
+            "note": f"{passes} passes x {npix} masked pixels x 32 B records from the L2-resident table"}
     dom = max((k for k in roof), key=lambda k: stages[k])
     line = {
         "metric": "patterns/s indexed+refined on 1 B200, BF16 form vs plain FP32 at <=0.1 deg error",
