@@ -1004,7 +1004,14 @@ class Engine:
         return dev
 
     def items_of(self, cells):
+        """The cells' items (detector position in pixels, index in the batch) on the device, and
+        their positions' bounding box in _batch_t."""
         cells = np.asarray(cells, np.int64)
+        n = len(cells)
+        fast = self._items_separable(cells) if n and not self.geo.plane_kind else None
+        if fast is not None:
+            items, self._batch_t = fast
+            return self.to_device("items", items)
         t = self.positions(cells)
         if len(t):
             tt = np.ascontiguousarray(t.T)  # (a reduction along the long axis of a contiguous array)
@@ -1012,6 +1019,40 @@ class Engine:
         else:
             self._batch_t = None
         return self.to_device("items", np.concatenate([t, np.arange(len(cells), dtype=np.float32)[:, None]], 1))
+
+    def _items_separable(self, cells):
+        """items_of without a plane of source points, for a run of consecutive cells: the beam's
+        travel is a row's plus a column's (geometry.zig:184-192), so each row's and each column's
+        position is computed once, by positions64's arithmetic, and gathered (the same float32
+        values); the box from the rows and columns the run reaches. None for scattered cells."""
+        n = len(cells)
+        if cells[-1] - cells[0] != n - 1 or (n > 1 and not (np.diff(cells) == 1).all()):
+            return None
+        rows, cols, h, w = self.info()
+        b = self.factor()
+        g = self.geo
+        t = g.translation(h / b, w / b)
+        ref_r, ref_c = 0.5 * (rows - 1), 0.5 * (cols - 1)
+        sx, sy = self.set["scan_x_sign"], self.set["scan_y_sign"]
+        prow = (t[0] - g.scan_offsets(np.arange(rows), np.zeros(rows), ref_r, ref_c, sx, sy, b)[:, 0]).astype(np.float32)
+        pcol = (t[1] - g.scan_offsets(np.zeros(cols), np.arange(cols), ref_r, ref_c, sx, sy, b)[:, 1]).astype(np.float32)
+        pz = np.float32(t[2] - 0.0)
+        r, c = np.divmod(cells, cols)
+        items = np.empty((n, 4), np.float32)
+        items[:, 0] = prow[r]
+        items[:, 1] = pcol[c]
+        items[:, 2] = pz
+        items[:, 3] = np.arange(n, dtype=np.float32)
+        r0, r1, c0, c1 = int(r[0]), int(r[-1]), int(c[0]), int(c[-1])
+        rr = prow[r0:r1 + 1]
+        if r1 == r0:
+            cc = pcol[c0:c1 + 1]
+        elif r1 == r0 + 1 and c1 + 1 < c0:
+            cc = np.concatenate([pcol[c0:], pcol[:c1 + 1]])
+        else:
+            cc = pcol
+        box = (np.array([rr.min(), cc.min(), pz], np.float32), np.array([rr.max(), cc.max(), pz], np.float32))
+        return items, box
 
     def spans(self, bt, fr):
         """The sphere's ring spans for the detector positions of the last items_of batch: the
