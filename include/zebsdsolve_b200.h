@@ -418,7 +418,9 @@ int zeb_mask_list(const zeb_frame_t* fr, uint32_t* list, void* stream);
 
 /* zeb_refine over the frame's pixel list (zeb_mask_list, npix = zeb_mask_pixels entries, at most
  * 25600): a block of 128 threads per item keeps only the pattern's values along the list in shared
- * memory, so that six items share an SM. The same records as zeb_refine. */
+ * memory, so that six items share an SM (256 or 512 threads where those values pass 36 or 72 KB, so
+ * that an SM keeps about as many warps for a large detector's list). The same records as
+ * zeb_refine. */
 int zeb_refine_list(const float* pats, const float* items, const float* seeds, int seed_stride, int n,
                     const zeb_frame_t* fr, const uint32_t* list, int npix, const float* vpair, const float* gpair,
                     int side, const zeb_refine_opts_t* o, float* records, void* stream);
