@@ -125,3 +125,46 @@ def test_calls_without_a_gpu():
         lib.ze_create_error.restype = ctypes.c_size_t
         n = lib.ze_create_error(buf, 512)
         assert b"no CUDA device" in buf.raw[:n]
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
+def test_a_native_host_starts_the_interpreter(tmp_path):
+    """A C program (no Python process around it) linked against libzebsdsolve.so and libpython:
+    the first call starts an interpreter, which finds the package beside the library; the calls
+    answer as in a Python process (without a GPU, ze_create fails with ze_create_error's reason)."""
+    import os
+    import sys
+    import sysconfig
+
+    libdir, ldlib = sysconfig.get_config_var("LIBDIR"), sysconfig.get_config_var("LDLIBRARY")
+    if not libdir or not ldlib or not os.path.exists(os.path.join(libdir, ldlib)):
+        pytest.skip("no shared libpython to link")
+    lib = _lib_path()
+    src = tmp_path / "host.c"
+    src.write_text("""#include <stdio.h>
+#include "zebsdsolve.h"
+int main(void) {
+  char buf[512];
+  void* e = ze_create("");
+  size_t n = ze_create_error(buf, sizeof buf - 1);
+  buf[n] = 0;
+  printf("%s|%d|%s\\n", ze_version(), e != NULL, buf);
+  if (e) ze_destroy(e);
+  return 0;
+}
+""")
+    exe = tmp_path / "host"
+    py = ldlib[3:].split(".so")[0]  # libpython3.12.so -> python3.12
+    subprocess.run(["gcc", str(src), "-I", str(HEADER.parent), "-L", str(lib.parent), "-lzebsdsolve", "-L", libdir,
+                    f"-l{py}", f"-Wl,-rpath,{lib.parent}", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    env = dict(os.environ, PYTHONPATH=os.pathsep.join(p for p in sys.path if p))
+    out = subprocess.run([str(exe)], capture_output=True, text=True, env=env, timeout=300)
+    assert out.returncode == 0, out.stderr
+    version, made, why = out.stdout.strip().splitlines()[-1].split("|", 2)
+    import torch
+
+    assert version == "0.2.8"
+    if torch.cuda.is_available():
+        assert made == "1"
+    else:
+        assert made == "0" and "no CUDA device" in why
