@@ -39,11 +39,14 @@ def test_up2_with_ang_indexes_as_the_array_does():
         fh.write(pats.astype("<u2").tobytes())
     lines = [f"# x-star {pc[0]}", f"# y-star {1 - pc[1]}", f"# z-star {pc[2]}", "# GRID: SqrGrid", "# XSTEP: 1.5",
              "# YSTEP: 1.5", f"# NCOLS_ODD: {cols}", f"# NCOLS_EVEN: {cols}", f"# NROWS: {rows}", "# SOFTWARE: OIM"]
-    lines += ["0 0 0 0 0 0 0 0 0 0"] * (rows * cols)
+    lines += [f"0 0 0 {k % cols * 1.5:.5f} {k // cols * 1.5:.5f} 0 0 0 0 0" for k in range(rows * cols)]
     with open(f"{d}/s.ang", "w") as fh:
         fh.write("\n".join(lines) + "\n")
     s.open(f"{d}/s.up2", f"{d}/s.ang")
     assert s.scan["format"] == "edax_up" and (s.scan["rows"], s.scan["cols"]) == (rows, cols)
+    ov, st = s.stored_overview(), s.stored_orientations()  # the .ang's image quality and orientations
+    assert ov["kind"] == 2 and ov["label"] == "Image quality" and ov["values"].shape == (rows, cols)
+    assert (ov["values"] == 0).all() and st["euler"].shape == (rows, cols, 3) and (st["phase"] == 0).all()
     assert np.allclose(s.geometry["pc"], pc) and s.geometry["step_x_um"] == 1.5
     r_file = s.index()
     r_arr = ze.index(pats.reshape(rows, cols, 60, 60), [f"{d}/m.npz"], pc=pc, sample_tilt_deg=70,

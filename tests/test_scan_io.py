@@ -40,7 +40,7 @@ def _ang_header(path, rows, cols, dx, dy, pc=None, software="EDAX OIM"):
               f"# NROWS: {rows}"]
     if software:
         lines.append(f"# SOFTWARE: {software}")
-    lines += ["  0.1 0.2 0.3 0.0 0.0 1.0 0.5 0 0 0.0"] * (rows * cols)
+    lines += [f"  0.1 0.2 0.3 {k % cols * dx:.5f} {k // cols * dy:.5f} 1.0 0.5 0 0 0.0" for k in range(rows * cols)]
     with open(path, "w") as fh:
         fh.write("\n".join(lines) + "\n")
 

@@ -156,9 +156,40 @@ class Solver:
         self._e.scan_source = {"px_um": float(px) if np.isfinite(px) and px > 0 else None,
                                "format": sc.format, "voltage_kv": info["voltage_kv"], "pc_note": info["pc_note"],
                                "paths": paths, "pc": info["pc"], "background": info.get("background"),
-                               "pattern_kinds": info.get("pattern_kinds", [])}
+                               "pattern_kinds": info.get("pattern_kinds", []),
+                               "overview": info.get("overview", (0, None)), "stored": info.get("stored")}
         self._e.avg = None
         return self
+
+    def stored_overview(self):
+        """The scan file's stored acquisition quality map, or None; never computes pattern statistics
+        (__init__.py:365-375): {"kind": 1 band contrast, 2 image quality, 3 Radon quality, 4 pattern
+        quality; "label"; "values": float32 (rows, cols), NaN where the file's value is not finite}.
+        HDF5 files store it beside the patterns under one of the makers' names (scan.zig:294-332); an
+        EDAX .up takes the image quality column of its .ang."""
+        from . import scan as SC
+
+        src = getattr(self._e, "scan_source", None)
+        kind, read = (src or {}).get("overview") or (0, None)
+        if not kind:
+            return None
+        values = self._call("stored_overview", read)
+        info = self.scan
+        return {"kind": kind, "label": SC.OVERVIEW_LABELS[kind], "values": values.reshape(info["rows"], info["cols"])}
+
+    def stored_orientations(self):
+        """The orientations the scan file stores from its maker's indexing, as it stores them
+        (__init__.py:814-824, scan.zig:220-291): {"euler": (rows, cols, 3) Bunge angles in radians,
+        "phase": (rows, cols) labels, −1 where not indexed}, or None when it stores none (Oxford's
+        Euler, Bruker's phi1/PHI/phi2 in degrees, EDAX's phi1/Phi/phi2, an .up's .ang records)."""
+        src = getattr(self._e, "scan_source", None)
+        read = (src or {}).get("stored")
+        got = self._call("stored_orientations", read) if read is not None else None
+        if got is None:
+            return None
+        info = self.scan
+        return {"euler": got["euler"].reshape(info["rows"], info["cols"], 3),
+                "phase": got["phase"].reshape(info["rows"], info["cols"])}
 
     def export(self, path):
         """Write the results by the path's extension (__init__.py:879-905): an EDAX .ang or an HKL

@@ -34,7 +34,10 @@ class Scan:
     """An opened scan: `patterns` [n, h, w] (np.memmap of the file, the stored pixel type) and
     `info` (rows, cols, pat_h, pat_w, step_x_um, step_y_um, pc, pc_note, voltage_kv,
     sample_tilt_deg, detector_tilt_deg, px_um, background (float32 [h, w]), detector_rot (a
-    rotation vector); NaN / None where the file says nothing)."""
+    rotation vector); NaN / None where the file says nothing). `info["overview"]` is the file's
+    stored quality map, (kind, a function giving its rows × cols values as float32) or (0, None);
+    `info["stored"]` a function giving the maker's own orientations ({"euler": (n, 3) float64
+    radians, "phase": (n,) int32, −1 where not indexed} or None), or None."""
 
     def __init__(self, fmt, patterns, info):
         self.format, self.patterns, self.info = fmt, patterns, info
@@ -49,7 +52,7 @@ def _blank_info():
     nan = float("nan")
     return {"rows": 0, "cols": 0, "pat_h": 0, "pat_w": 0, "step_x_um": nan, "step_y_um": nan, "pc": None,
             "pc_note": "", "voltage_kv": nan, "sample_tilt_deg": nan, "detector_tilt_deg": nan, "px_um": nan,
-            "background": None, "detector_rot": None}
+            "background": None, "detector_rot": None, "overview": (0, None), "stored": None}
 
 
 def open_scan(paths, rows=0, cols=0, pat_h=0, pat_w=0, unprocessed=False, scan_name=""):
@@ -84,7 +87,8 @@ def _shape(info, n, rows, cols):
 def _open_up(paths, is16, rows, cols):
     """scan.zig:842-923 — EDAX .up1 (8-bit) / .up2 (16-bit): a 16-byte header (version, width,
     height, data offset), from version 3 the map's shape, hex flag and steps; an .ang beside it
-    gives the shape, the steps and the pattern centre."""
+    gives the shape, the steps, the pattern centre, and from its records the image-quality map and
+    the maker's orientations."""
     side = [p for p in paths[1:] if _ext(p) == "ang"]
     if len(side) > 1:
         raise ScanError("DuplicateANGSidecar")
@@ -126,6 +130,8 @@ def _open_up(paths, is16, rows, cols):
         ang = read_ang_header(side[0], w, h)
         if ang["rows"] * ang["cols"] != n:
             raise ScanError("ANGPatternCountMismatch")
+        rec = read_ang_records(side[0], ang["rows"], ang["cols"], (ang["step_x_um"], ang["step_y_um"]),
+                               (dx, dy) if version >= 3 else None)
         if version >= 3 and (nx != ang["cols"] or ny != ang["rows"]):
             raise ScanError("ScanShapeMismatch")
         if version >= 3 and not (_same_step(dx, ang["step_x_um"]) and _same_step(dy, ang["step_y_um"])):
@@ -133,7 +139,8 @@ def _open_up(paths, is16, rows, cols):
         if (rows and rows != ang["rows"]) or (cols and cols != ang["cols"]):
             raise ScanError("ScanShapeMismatch")
         info.update(rows=ang["rows"], cols=ang["cols"], step_x_um=ang["step_x_um"], step_y_um=ang["step_y_um"],
-                    pc=ang["pc"], pc_note=ang["pc_note"])
+                    pc=ang["pc"], pc_note=ang["pc_note"], overview=(2, lambda: rec["iq"]),
+                    stored=lambda: {"euler": rec["euler"], "phase": rec["phase"]})
     else:
         _shape(info, n, rows, cols)
     pats = np.memmap(paths[0], dt, "r", offset=off, shape=(n, h, w))
@@ -233,6 +240,85 @@ def read_ang_header(path, width, height):
         raise ScanError("InvalidANGPatternCentre")
     out["pc"], out["pc_note"] = pc, note
     return out
+
+
+def _coordinates_not_row_major(actual, origin, travel, step):
+    """ang.zig:74-85 per record, over all records at once: 0 where a record's coordinate is at its
+    place in row-major order (origin + travel), within the looser of 1e-6 of the step and
+    min(5e-6, 1 % of the step) — else within min(1e-5, 1 % of the step) plus 2^-24 of the
+    magnitudes involved (positions a maker computed in float32 and printed to five decimals);
+    1 where it is not; 2 where that allowance reaches an eighth of the step (the file's
+    precision cannot tell the cells apart)."""
+    expected = origin + travel
+    with np.errstate(invalid="ignore", over="ignore"):
+        residual = np.abs((actual - origin) - travel)
+        strict = max(step * 1e-6, min(5e-6, step * 0.01))
+        budget = min(1e-5, step * 0.01) + 2.0 ** -24 * (abs(origin) + np.abs(expected) + 2 * np.abs(travel))
+        code = np.where(residual <= strict, 0,
+                        np.where(~np.isfinite(budget) | (budget >= step / 8), 2, np.where(residual > budget, 1, 0)))
+    code[~(np.isfinite(actual) & np.isfinite(expected))] = 1
+    return code
+
+
+def read_ang_records(path, rows, cols, steps, up_steps=None):
+    """ang.zig:216-268 (the records): per map cell, in row-major order, the legacy columns phi1 Phi
+    phi2 x y IQ CI phase. Returns {"iq": float32 (n,) (NaN where not finite), "euler": float64
+    (n, 3) Bunge angles as written, "phase": int32 (n,) — the label, −1 where it is negative, not an
+    integer, or the angles are not finite or past 2π (ANG's not-indexed 4π)}. The x and y columns
+    must step through the grid row-major by the header's `steps` (x, y), and by the .up file's own
+    (`up_steps`) where it states them."""
+    n = rows * cols
+    vals = np.full((n, 6), np.nan)
+    label = np.full(n, -1, np.int64)
+    count = 0
+    with open(path, "r", errors="replace") as fh:
+        for line in fh:
+            line = line.strip(" \t\r\n")
+            if not line:
+                continue
+            if line[0] == "#":
+                if count:
+                    raise ScanError("InvalidANGRecord")
+                continue
+            if count >= n:
+                raise ScanError("ANGPatternCountMismatch")
+            words = line.split()
+            if len(words) < 8:
+                raise ScanError("InvalidANGRecord")
+            try:
+                vals[count] = [float(w) for w in words[:6]]
+            except ValueError:
+                raise ScanError("InvalidANGRecord") from None
+            try:
+                v = int(words[7])
+                label[count] = v if -(1 << 31) <= v < 1 << 31 else -1
+            except ValueError:
+                pass
+            count += 1
+    if count != n or count == 0:
+        raise ScanError("ANGPatternCountMismatch")
+    k = np.arange(n)
+    col, row = (k % cols).astype(np.float64), (k // cols).astype(np.float64)
+    checks = []
+    for st, err in ((steps, None), (up_steps, "UPANGStepMismatch")):
+        if st is None:
+            continue
+        cx = _coordinates_not_row_major(vals[:, 3], vals[0, 3], col * st[0], st[0])
+        cy = _coordinates_not_row_major(vals[:, 4], vals[0, 4], row * st[1], st[1])
+        checks.append((cx, err))
+        checks.append((cy, err))
+    # the first record that fails a check, and its first failing check, give the error
+    bad = np.zeros(n, bool)
+    for c, _ in checks:
+        bad |= c != 0
+    if bad.any():
+        i = int(np.argmax(bad))
+        for c, err in checks:
+            if c[i]:
+                raise ScanError(err or ("ANGCoordinatePrecisionInsufficient" if c[i] == 2 else "ANGCoordinatesNotRowMajor"))
+    euler = vals[:, :3].copy()
+    phase = np.where(label >= 0, label, -1).astype(np.int32)
+    return {"iq": _f32_or_nan(vals[:, 5]), "euler": euler, "phase": _marked_unindexed(euler, phase)}
 
 
 def _open_ebsp(path, rows, cols):
@@ -404,6 +490,117 @@ def _h5_values(h, group, name, limit=1 << 24):
         return None
 
 
+# scan.zig:294-332: the makers' names for a stored quality map, in the order they are tried, each
+# with its kind (1 band contrast, 2 image quality, 3 Radon quality, 4 pattern quality)
+OVERVIEW_NAMES = (("Band Contrast", 1), ("band_contrast", 1), ("BandContrast", 1), ("Image Quality", 2),
+                  ("IQ", 2), ("image_quality", 2), ("iq", 2), ("ImageQuality", 2), ("RadonQuality", 3),
+                  ("Radon Quality", 3), ("Pattern Quality", 4), ("PatternQuality", 4))
+OVERVIEW_LABELS = {1: "Band contrast", 2: "Image quality", 3: "Radon quality", 4: "Pattern quality"}
+
+
+def _f32_or_nan(v):
+    """Values as float32, NaN where not finite or past float32's range (scan.zig:217, ang.zig:259)."""
+    v = np.asarray(v, np.float64)
+    with np.errstate(invalid="ignore"):
+        ok = np.isfinite(v) & (np.abs(v) <= float(np.finfo(np.float32).max))
+    return np.where(ok, v, np.nan).astype(np.float32)
+
+
+def _h5_first(h, group, name, count):
+    """The first `count` values of a numeric dataset as float64, or None where it is absent, not
+    numeric or shorter (hdf5.zig:1043-1055 reads min(stored, asked) values)."""
+    try:
+        a = h.child(group, name)
+        v = h.numbers(a) if a is not None else None
+    except H5.H5Error:
+        return None
+    return v[:count] if v is not None and v.size >= count and count else None
+
+
+def _h5_overview(h, group, rows, cols):
+    """scan.zig:294-332 — the stored quality map: the first of OVERVIEW_NAMES under the data group
+    whose dataset holds one number per map cell, as a vector (n, (n, 1) or (1, n)) or as the raster
+    (rows, cols), in an integer of 1, 2, 4 or 8 bytes or a float of 4 or 8. Returns (kind, a reader
+    of its n values as float32, scan.zig:205-217), or (0, None). The values are read when asked."""
+    n = rows * cols
+    for name, kind in OVERVIEW_NAMES:
+        try:
+            a = h.child(group, name)
+            ds = h.dataset(a) if a is not None else None
+        except H5.H5Error:
+            continue
+        if ds is None or ds.shape is None or n == 0:
+            continue
+        if tuple(int(d) for d in ds.shape) not in ((n,), (n, 1), (1, n), (rows, cols)):
+            continue
+        k, size = ds.dtype.kind, ds.dtype.size
+        if not ((k in "ui" and size in (1, 2, 4, 8)) or (k == "f" and size in (4, 8))):
+            continue
+
+        def read(a=a):
+            try:
+                v = h.numbers(a)
+            except H5.H5Error:
+                v = None
+            if v is None or v.size != n:
+                raise ScanError("InvalidStoredOverview")
+            return _f32_or_nan(v)
+        return kind, read
+    return 0, None
+
+
+# scan.zig:236-243: where each maker keeps its own orientations — one (n, 3) dataset or a column per
+# angle (the names each may go by) —, whether in degrees, and whether its phase 0 marks a cell not
+# indexed
+_STORED_ORIENTATIONS = {
+    "Oxford h5oina": ("Euler", None, False, True),
+    "Bruker h5ebsd": ("", (("phi1",), ("PHI",), ("phi2",)), True, True),
+    "EDAX h5ebsd": ("", (("phi1", "Phi1"), ("Phi", "PHI"), ("phi2", "Phi2")), False, False),
+}
+
+
+def _marked_unindexed(euler, phase):
+    """Cells whose angles are not finite or past 2π (+0.01; 4π is the makers' not-indexed marker)
+    get phase −1 (scan.zig:283-289, ang.zig:261-264)."""
+    with np.errstate(invalid="ignore"):
+        ok = np.all(np.isfinite(euler) & (np.abs(euler) <= 2 * np.pi + 0.01), axis=1)
+    phase[~ok] = -1
+    return phase
+
+
+def _h5_stored(h, data, fmt, n):
+    """scan.zig:224-291 — the orientations an HDF5 file stores from its maker's indexing: Bunge
+    angles in radians (Bruker's degrees converted) and the "Phase" label per cell (0 where absent;
+    Oxford's and Bruker's 0, and any cell whose angles are past 2π, as −1), or None."""
+    if fmt not in _STORED_ORIENTATIONS or n == 0:
+        return None
+    one, three, degrees, zero_unindexed = _STORED_ORIENTATIONS[fmt]
+    if one:
+        e = _h5_first(h, data, one, 3 * n)
+        if e is None:
+            return None
+        euler = e.reshape(n, 3).copy()
+    else:
+        angles = []
+        for names in three:
+            col = next((v for v in (_h5_first(h, data, nm, n) for nm in names) if v is not None), None)
+            if col is None:
+                return None
+            angles.append(col)
+        euler = np.stack(angles, 1)
+    if degrees:
+        euler = np.radians(euler)
+    phase = np.zeros(n, np.int32)
+    p = _h5_first(h, data, "Phase", n)
+    if p is not None:
+        with np.errstate(invalid="ignore"):
+            ok = np.isfinite(p) & (np.abs(p) < 1 << 30)
+        phase = np.where(ok, np.trunc(np.where(ok, p, 0)), -1).astype(np.int32)
+    if zero_unindexed:
+        phase[phase == 0] = -1
+    return {"euler": np.ascontiguousarray(euler, np.float64), "phase": _marked_unindexed(euler, phase)}
+
+
 def _h5_mean(h, group, name):
     """scan.zig:653-668 — the mean of a per-pattern array."""
     v = _h5_values(h, group, name)
@@ -541,6 +738,8 @@ def _open_h5_in(h, rows, cols, unprocessed, scan_name):
             info["rows"], info["cols"] = 1, int(n_stored)
         else:
             raise ScanError("ScanIsNotAFullGrid")
+    info["overview"] = _h5_overview(h, data, info["rows"], info["cols"])
+    info["stored"] = lambda: _h5_stored(h, data, fmt, info["rows"] * info["cols"])
     info["step_x_um"], info["step_y_um"] = _h5_get(h, header, k_sx), _h5_get(h, header, k_sy)
     info["sample_tilt_deg"] = _h5_get(h, header, k_tilt)
     if math.isnan(info["sample_tilt_deg"]) and fmt == "Bruker h5ebsd":
@@ -638,6 +837,8 @@ def _open_emsoft(h, pat_addr, rows, cols):
     info["rows"], info["cols"] = 1, n
     if rows and cols and rows * cols == n:
         info["rows"], info["cols"] = rows, cols
+    # EMsoft's per-pattern scalars sit beside EBSDPatterns
+    info["overview"] = _h5_overview(h, h.find("EMData/EBSD"), info["rows"], info["cols"])
     nml = h.find("NMLparameters/EBSDNameList")
     if nml is not None:
         xpc, ypc, L, delta, numsx, numsy = (_h5_get(h, nml, k) for k in ("xpc", "ypc", "L", "delta", "numsx", "numsy"))

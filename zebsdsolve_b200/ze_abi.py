@@ -332,20 +332,48 @@ def ze_scan_format(h, buf, cap):
     return _put(buf, cap, name.encode())
 
 
+def _stored_overview_of(x):
+    src = getattr(x.s._e, "scan_source", None) if x.s._e.patterns is not None else None
+    return (src or {}).get("overview") or (0, None)
+
+
 def ze_scan_overview_kind(h):
-    """No reader here takes a file's stored quality map (band contrast, image quality): 0."""
-    return 0
+    """exports.zig:451-454 — the stored quality map's kind: 0 none, 1 band contrast, 2 image
+    quality, 3 Radon quality, 4 pattern quality."""
+    x = _handles.get(int(h))
+    return int(_stored_overview_of(x)[0]) if x is not None else 0
 
 
 @_api("scan_overview")
 def ze_scan_overview(x, out, cap):
-    return 0
+    """exports.zig:456-465 — the stored quality map's size (rows × cols; 0 for none), and with a
+    buffer its values as float32; BufferTooSmall when cap is short."""
+    kind, read = _stored_overview_of(x)
+    if not kind:
+        return 0
+    sc = x.s.scan
+    n = sc["rows"] * sc["cols"]
+    if out:
+        if cap < n:
+            raise RuntimeError("BufferTooSmall")
+        _view(out, n, np.float32)[:] = read()
+    return n
 
 
 @_api("stored_orientations")
 def ze_stored_orientations(x, euler, phase, n):
-    """The readers here do not take a maker's stored orientations: 0, none stored."""
-    return 0
+    """exports.zig:819-834 — the maker's stored orientations: Bunge angles (3 f64 a cell) and a
+    phase label a cell (−1: not indexed), n cells; 1, or 0 when the file stores none."""
+    src = getattr(x.s._e, "scan_source", None) if x.s._e.patterns is not None else None
+    read = (src or {}).get("stored")
+    got = read() if read is not None else None
+    if got is None:
+        return 0
+    if got["phase"].size != n:
+        raise RuntimeError("BadLength")
+    _view(euler, 3 * n, np.float64)[:] = got["euler"].reshape(-1)
+    _view(phase, n, np.int32)[:] = got["phase"]
+    return 1
 
 
 # ── geometry (exports.zig:124-158) ──
