@@ -196,3 +196,25 @@ def test_the_c_abi_hands_out_both(tmp_path):
         assert lib.ze_stored_orientations(h, eu.ctypes.data, ph.ctypes.data, n - 1) < 0
     finally:
         Z._handles.pop(h, None)
+
+
+def test_the_solver_hands_out_both(tmp_path):
+    """Solver.open keeps the readers' stored maps; Solver.stored_overview/stored_orientations give
+    them shaped as the map (an engine without a device: the host side of open alone)."""
+    import zebsdsolve_b200 as ze
+    from zebsdsolve_b200 import engine as E
+    from zebsdsolve_b200.settings import Settings
+
+    s = ze.Solver.__new__(ze.Solver)
+    e = E.Engine.__new__(E.Engine)
+    e.set, e.geo, e._resident, e.patterns = Settings(), E.Geometry(), None, None
+    s._e = e
+    ph = np.array([1, 0, 2, 1, 1, 2], np.int32)
+    s.open(_h5ebsd(tmp_path / "o.h5", "oxford", {"Band Contrast": D(Q.reshape(2, 3)), "Phase": D(ph),
+                                                  "Euler": D(np.full((6, 3), 0.5, np.float32))}))
+    ov, st = s.stored_overview(), s.stored_orientations()
+    assert ov["kind"] == 1 and ov["label"] == "Band contrast" and np.array_equal(ov["values"], Q.reshape(2, 3))
+    assert st["euler"].shape == (2, 3, 3) and np.allclose(st["euler"], 0.5)
+    assert np.array_equal(st["phase"], np.where(ph == 0, -1, ph).reshape(2, 3))
+    s.set_patterns(np.zeros((2, 3, H, W), np.uint8))  # patterns from memory: none stored
+    assert s.stored_overview() is None and s.stored_orientations() is None
