@@ -482,6 +482,18 @@ class Solver:
                 "phase": r["phase"].reshape(rows, cols).copy(), "z": r["z"].reshape(rows, cols).copy(),
                 "sweep": r["sweep"].reshape(rows, cols).copy()}
 
+    def map(self, kind="ipf_z"):
+        """A result map as RGBA uint8 (rows, cols, 4) (__init__.py:790-795, output.zig:15-84): "ncc",
+        "nmi" and "z" as gray between the indexed cells' extremes, "phase" and "sweep" in the
+        reference's palette (dark gray: no sweep accepted the cell); cells not indexed transparent
+        black. The IPF maps ("ipf_x", "ipf_y", "ipf_z") are not built: they raise."""
+        from . import output as O
+
+        rows, cols, h, w = self._call("map", self._e.info)
+        if kind not in O.MAPS:
+            raise Error(f"map: UnknownKind {kind!r}")
+        return self._call("map", O.result_map, O.MAPS[kind], self._e.res).reshape(rows, cols, 4)
+
     def cell_under(self, cell, bandwidth=None, full=False, **fields):
         """Index one map cell and simulate it under another geometry than the one in use, which
         stays as it is (__init__.py:198-212): the fields given change it as for `set_geometry`

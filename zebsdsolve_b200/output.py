@@ -91,3 +91,47 @@ def export_text(kind, res, phases, geo, rows, cols, pat_h, pat_w, voltage_kv=flo
     else:
         raise ExportError(f"UnknownKind: {kind!r}")
     return "".join(out)
+
+
+# output.zig:10-13: the colours of phases and sweeps (the label modulo eight), as the reference's maps
+# draw them, so that a map made here matches one made there pixel for pixel
+PALETTE = np.array([[0x3b, 0x82, 0xf6], [0xf5, 0x9e, 0x0b], [0x10, 0xb9, 0x81], [0xef, 0x44, 0x44],
+                    [0x8b, 0x5c, 0xf6], [0x14, 0xb8, 0xa6], [0xec, 0x48, 0x99], [0x84, 0xcc, 0x16]], np.uint8)
+NO_SWEEP = np.array([0x3a, 0x3a, 0x3e], np.uint8)
+MAPS = {"ipf_x": 0, "ipf_y": 1, "ipf_z": 2, "ncc": 3, "nmi": 4, "phase": 5, "z": 6, "sweep": 7}
+
+
+def result_map(kind, res):
+    """output.zig:15-84 — a result map as RGBA8 (n, 4), cells in map order: kind 3 NCC, 4 NMI and 6
+    the NMI's distance above chance as gray between the indexed cells' extremes (one level where
+    they are equal; values past them clamped), 5 the phase's colour, 7 the colour of the sweep that
+    accepted the cell (dark gray: none did). Cells not indexed are transparent black. Kinds 0-2,
+    the inverse pole figure colours, take the colour keys of the crystal classes, which this
+    package does not build: they raise."""
+    if kind not in range(8):
+        raise ValueError("UnknownKind")
+    if kind <= 2:
+        raise NotImplementedError("NotImplemented: IPF colours (their keys are not part of this engine)")
+    phase = np.asarray(res["phase"])
+    ok = phase >= 0
+    out = np.zeros((phase.size, 4), np.uint8)
+    if kind in (3, 4, 6):
+        v = np.asarray(res[{3: "ncc", 4: "nmi", 6: "z"}[kind]], np.float32)
+        # extremes over the indexed cells, NaN passed over (the minimum and maximum of IEEE 754-2008)
+        lo = np.fmin.reduce(v[ok], initial=np.float32(np.inf)).astype(np.float32)
+        hi = np.fmax.reduce(v[ok], initial=np.float32(-np.inf)).astype(np.float32)
+        if not hi > lo:
+            hi = np.float32(lo + np.float32(1))
+        with np.errstate(invalid="ignore", divide="ignore", over="ignore"):
+            t = np.fmax(np.float32(0), np.fmin((v - lo) / (hi - lo), np.float32(1)))
+            gray = np.floor(np.float32(255) * t + np.float32(0.5))  # (t ≥ 0: half away from zero)
+        out[:, :3] = np.nan_to_num(gray, nan=0.0).astype(np.uint8)[:, None]
+    elif kind == 5:
+        out[:, :3] = PALETTE[np.where(ok, phase, 0) % len(PALETTE)]
+    else:
+        sw = np.asarray(res["sweep"])
+        out[:, :3] = np.where((sw < 0)[:, None], NO_SWEEP, PALETTE[np.where(sw < 0, 0, sw) % len(PALETTE)])
+    out[:, 3] = 255
+    out[~ok] = 0
+    return out
+

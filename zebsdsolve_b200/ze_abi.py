@@ -844,7 +844,19 @@ def ze_results(x, kind, out, cap):
     return data.nbytes // 4
 
 
-ze_map = _not_built("map", "colour maps (IPF, scores) are not part of this engine; ze_results gives the values")
+@_api("map")
+def ze_map(x, kind, out, n):
+    """exports.zig:726-729 — a result map as RGBA8 (4 bytes a cell): the score, phase and sweep maps
+    (kinds 3-7); the IPF kinds 0-2 fail with NotImplemented. BadLength unless n is 4 × the cells."""
+    from .output import result_map
+
+    res = x.s._e.res
+    if res is None:
+        raise RuntimeError("NoScan")
+    if n != 4 * len(res["ncc"]):
+        raise RuntimeError("BadLength")
+    _view(out, n, np.uint8)[:] = result_map(int(kind), res).reshape(-1)
+    return 0
 ze_ipf_key = _not_built("ipf_key", "IPF colour keys are not part of this engine")
 
 
