@@ -218,3 +218,31 @@ def test_the_solver_hands_out_both(tmp_path):
     assert np.array_equal(st["phase"], np.where(ph == 0, -1, ph).reshape(2, 3))
     s.set_patterns(np.zeros((2, 3, H, W), np.uint8))  # patterns from memory: none stored
     assert s.stored_overview() is None and s.stored_orientations() is None
+
+
+@pytest.mark.parametrize("line,why", [
+    ("# GRID: SqrGrid", "DuplicateANGMetadata"), ("# NROWS: 2", "DuplicateANGMetadata"),
+    ("# XSTEP: 0.5", "DuplicateANGMetadata"), ("# COLUMN_HEADERS: phi1, PHI, phi2", "UnsupportedANGColumns"),
+    ("# XUNITS: nm", "UnsupportedANGUnits"), ("# Indexed by ACOM", "UnsupportedANGConvention"),
+    ("# TEM data", "UnsupportedANGConvention"), ("# x-star: abc", "InvalidANGPatternCentre")])
+def test_ang_header_refusals(tmp_path, line, why):
+    """ang.zig:170-214: the header lines the reference refuses."""
+    n = ROWS * COLS
+    paths = _up_and_ang(tmp_path, [line] + _records(np.zeros((n, 3)), ["1"] * n, ["0"] * n))
+    with pytest.raises(SC.ScanError, match=why):
+        SC.open_scan(paths)
+
+
+def test_ang_header_dimensions_steps_and_units(tmp_path):
+    n = ROWS * COLS
+    recs = _records(np.zeros((n, 3)), ["1"] * n, ["0"] * n)
+    for unit in ("# SCAN_UNIT: um", "# XUNITS: [microns]", "# YUNITS: µm"):
+        SC.open_scan(_up_and_ang(tmp_path, [unit] + recs))  # micrometres, however written
+    text = open(_up_and_ang(tmp_path, recs)[1]).read()
+    for a, b, why in (("# NROWS: 2", "# NROWS: two", "InvalidANGDimensions"),
+                      ("# NROWS: 2", "# NROWS: 0", "InvalidANGDimensions"),
+                      ("# XSTEP: 0.5", "# XSTEP: -0.5", "InvalidANGStep"),
+                      ("# YSTEP: 0.5", "# YSTEP: inf", "InvalidANGStep")):
+        open(tmp_path / "s.ang", "w").write(text.replace(a, b))
+        with pytest.raises(SC.ScanError, match=why):
+            SC.open_scan([tmp_path / "s.up2", tmp_path / "s.ang"])

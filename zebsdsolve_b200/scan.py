@@ -7,6 +7,7 @@ memory otherwise); numbered row-major over the map, top row first, as stored.
 """
 import math
 import os
+import re
 
 import numpy as np
 
@@ -147,6 +148,9 @@ def _open_up(paths, is16, rows, cols):
     return Scan("edax_up", pats, info)
 
 
+_MICRO = ("um", "µm", "μm", "micron", "microns", "micrometer", "micrometers", "micrometre", "micrometres")
+
+
 def read_ang_header(path, width, height):
     """ang.zig:87-270 (the header): the map's shape and steps and the pattern centre in the
     Bruker convention — EDAX's (x and y in fractions of width and height, y from the bottom, z of
@@ -158,24 +162,30 @@ def read_ang_header(path, width, height):
     square = False
     with open(path, "r", errors="replace") as fh:
         for line in fh:
-            line = line.strip()
+            line = line.strip(" \t\r\n")
             if not line:
                 continue
             if not line.startswith("#"):
                 break
-            content = line[1:].strip()
-            parts = content.replace(":", " ").split(None, 1)
-            if not parts:
+            content = line[1:].strip(" \t")
+            # ang.zig:177-187: an ACOM (TEM) file's angles follow another convention
+            words = re.findall(r"[A-Za-z0-9_]+", content)
+            if "ACOM" in words or any(a == "TEM" and b == "data" for a, b in zip(words, words[1:])):
+                raise ScanError("UnsupportedANGConvention")
+            m = re.match(r"[: \t]*([^: \t]+)(.*)", content)
+            if m is None:
                 continue
-            key, value = parts[0], (parts[1].strip(": \t") if len(parts) > 1 else "")
+            key, value = m.group(1), m.group(2).strip(": \t")
             k = {"x-star": 0, "y-star": 1, "z-star": 2}.get(key)
             if k is not None:
                 if raw[k] is not None:
                     raise ScanError("DuplicateANGPatternCentre")
                 try:
-                    raw[k] = float(value.split()[0])
-                except (ValueError, IndexError):
+                    raw[k] = float(value)
+                except ValueError:
                     raise ScanError("InvalidANGPatternCentre") from None
+                if not math.isfinite(raw[k]):
+                    raise ScanError("InvalidANGPatternCentre")
             elif key == "SOFTWARE":
                 software_seen = True
                 words = value.split()
@@ -192,21 +202,40 @@ def read_ang_header(path, width, height):
             elif key == "HEADER" and value == "Start":
                 header_start = True
             elif key == "VERSION":
-                numeric_version = value.isdigit()
-            elif key == "GRID":
+                numeric_version = value.isdigit() and int(value) < 1 << 32
+            # ang.zig:190-214: each grid line once, whole numbers and positive steps, micrometres
+            if key == "GRID":
+                if square:
+                    raise ScanError("DuplicateANGMetadata")
                 if value != "SqrGrid":
                     raise ScanError("UnsupportedANGGrid")
                 square = True
-            elif key == "NROWS":
-                rows = int(value)
-            elif key == "NCOLS_ODD":
-                odd = int(value)
-            elif key == "NCOLS_EVEN":
-                even = int(value)
-            elif key == "XSTEP":
-                dx = float(value)
-            elif key == "YSTEP":
-                dy = float(value)
+            elif key in ("NROWS", "NCOLS_ODD", "NCOLS_EVEN"):
+                if {"NROWS": rows, "NCOLS_ODD": odd, "NCOLS_EVEN": even}[key]:
+                    raise ScanError("DuplicateANGMetadata")
+                if not (value.isdigit() and 0 < int(value) < 1 << 32):
+                    raise ScanError("InvalidANGDimensions")
+                if key == "NROWS":
+                    rows = int(value)
+                elif key == "NCOLS_ODD":
+                    odd = int(value)
+                else:
+                    even = int(value)
+            elif key in ("XSTEP", "YSTEP"):
+                if (dx if key == "XSTEP" else dy) != 0:
+                    raise ScanError("DuplicateANGMetadata")
+                try:
+                    v = float(value)
+                except ValueError:
+                    raise ScanError("InvalidANGStep") from None
+                if not (math.isfinite(v) and v > 0):
+                    raise ScanError("InvalidANGStep")
+                dx, dy = (v, dy) if key == "XSTEP" else (dx, v)
+            elif key in ("COLUMN_HEADERS", "COLUMN_UNITS"):
+                raise ScanError("UnsupportedANGColumns")
+            elif key in ("SCAN_UNIT", "SCANUNIT", "XUNITS", "YUNITS"):
+                if value.strip(" \t[]()") not in _MICRO:
+                    raise ScanError("UnsupportedANGUnits")
     if not square or rows == 0 or odd == 0 or even == 0:
         raise ScanError("ANGGridMetadataRequired")
     if odd != even:
