@@ -184,8 +184,10 @@ def test_settings_events_and_the_error_channel(lib, eng):
     assert msg.startswith("configure") and _err(lib, h) == ""
     # a part this engine does not build
     assert lib.ze_sim_run(h, None) < 0 and "not part of this engine" in _err(lib, h)
+    j = b'{"axes": [2, 1, 3], "active": false, "crystal": "x_a_z_cstar"}'  # left-handed: no convention
+    assert lib.ze_set_frame(h, j, len(j)) < 0 and "InvalidFrame" in _err(lib, h)
     j = b'{"axes": [2, 1, -3], "active": false, "crystal": "x_a_z_cstar"}'
-    assert lib.ze_set_frame(h, j, len(j)) < 0 and "engine's own" in _err(lib, h)
+    assert lib.ze_set_frame(h, j, len(j)) == 0 and s._e.convention.axes == (2, 1, -3)
     own = b'{"axes": [1, 2, 3], "active": false, "crystal": "x_a_z_cstar"}'
     assert lib.ze_set_frame(h, own, len(own)) == 0
     msg = ctypes.create_string_buffer(256)

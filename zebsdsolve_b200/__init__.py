@@ -18,6 +18,8 @@ reference's own C ABI, its ze_* calls, is libzebsdsolve.so (include/zebsdsolve.h
 which carries each call onto this package's Solver.
 """
 
+import math
+
 import numpy as np
 
 __version__ = "0.2.8"
@@ -212,7 +214,75 @@ class Solver:
                    "space_group": p.master.space_group} for p in e.phases]
         src = getattr(e, "scan_source", None) or {}
         return self._call("export", output.export_text, kind, e.res, phases, e.geo, rows, cols, h, w,
-                          src.get("voltage_kv", float("nan")))
+                          src.get("voltage_kv", float("nan")), getattr(e, "convention", None))
+
+    @property
+    def frame(self):
+        """The reference frame convention the exports write orientations in (__init__.py:858-867):
+        `axes` (the convention's sample X, Y, Z as the engine's axes, 1 x on the surface toward the
+        detector, 2 y the tilt axis, 3 z out of the surface, negative reversed), `active`,
+        `crystal` (x_a_z_cstar, the masters' own; x_astar_z_c; y_b_z_cstar; y_bstar_z_c) and
+        `text`, a line naming it. The engine's own until identified (`identify_frame`) or set; a
+        new scan resets it."""
+        from .convention import Frame
+
+        return (getattr(self._e, "convention", None) or Frame()).as_dict()
+
+    @frame.setter
+    def frame(self, value):
+        from .convention import Frame
+
+        self._e.convention = None if value is None else self._call("set_frame", Frame.from_dict, dict(value))
+
+    def identify_frame(self, euler=None, phase=None):
+        """The reference frame convention a maker's orientations are in, found against the results
+        (__init__.py:826-856, engine.zig:784-812, convention.zig:254-404): from `euler` (Bunge
+        angles, radians, (rows, cols, 3) or (n, 3), one per map cell) and `phase` (a label per cell,
+        negative where not indexed), or with neither the scan file's own. Every convention of the
+        sample's axes, the rotation's sense and the crystal's axes on the lattice is tried, cell by
+        cell under each phase's own symmetry.
+
+        Returns a dict: `frame` (as `frame` has it), `cells` compared, `within` (the fraction within
+        2°), `median_deg`, `runner_up_deg` (the best other convention's median), `matched` (the
+        reference's label for each phase), `installed` (the exports take the convention when it was
+        told clearly: median under 5°, and the best other's at least twice that and 5° more), and
+        the misorientation left, which no convention removes and nothing applies:
+        `misorientation` (rotation vector, radians, about the engine's x, y, z, at the map's
+        middle), `misorientation_rows` and `misorientation_cols` (its change from the first row to
+        the last and from the first column to the last) and `misorientation_cells`."""
+        from . import convention as C
+
+        e = self._e
+        if not e.phases:
+            raise Error("identify_frame: NoPhases")
+        if euler is None:
+            got = self.stored_orientations()
+            if got is None:
+                raise Error("identify_frame: NoStoredOrientations")
+            euler, phase = got["euler"], got["phase"]
+        euler = np.asarray(euler, np.float64).reshape(-1, 3)
+        phase = np.asarray(phase, np.int32).reshape(-1)
+        if len(phase) != len(euler):
+            raise Error("identify_frame: euler and phase differ in length")
+        rows, cols, h, w = self._call("identify_frame", e.info)
+        views = [(p.master.rotations(), p.master.lattice) for p in e.phases[:C.MAX_PHASES]]
+        frame, out = self._call("identify_frame", C.identify, e.res["quat"], e.res["phase"], cols, euler, phase,
+                                views)
+        holds = out["median_deg"] < 5 and out["runner_up_deg"] >= 2 * out["median_deg"] + 5
+        if holds:
+            e.convention = frame
+        m = np.array(out["misorientation"])
+        th = float(np.linalg.norm(m))
+        u = m / th if th > 0 else np.zeros(3)
+        e.log((
+            f"frame of the stored orientations: {frame.describe()}; {out['cells']} cells, median "
+            f"{out['median_deg']:.2f}°, {100 * out['within']:.0f} % within 2°, {out['runner_up_deg']:.1f}° under the "
+            f"next convention{'; the exports take it' if holds else '; not told clearly, the exports keep theirs'}; "
+            f"misorientation left {math.degrees(th):.2f}° about ({u[0]:.3f}, {u[1]:.3f}, {u[2]:.3f}) (x, y, z: toward "
+            f"the detector, the tilt axis, out of the surface), changing "
+            f"{math.degrees(np.linalg.norm(out['misorientation_rows'])):.2f}° from the first row to the last and "
+            f"{math.degrees(np.linalg.norm(out['misorientation_cols'])):.2f}° from the first column to the last"))
+        return {"frame": frame.as_dict(), **out, "installed": holds}
 
     def shape(self, full=False):
         """(h, w) of a pattern as the search sees it (reduced by `binning`), or (full) as stored."""

@@ -212,6 +212,7 @@ class Engine:
             raise EngineError("PatternTooSmall")
         self.patterns = np.ascontiguousarray(a)
         self.scan_source = None  # the file the patterns came from (Solver.open), if any
+        self.convention = None  # the orientation convention the exports write in (None: the engine's own)
         self.told_no_background = False
         self._pinned = None
         self._index_calls = 0

@@ -11,7 +11,6 @@ import numpy as np
 from . import rotations as R
 
 VERSION = "0.2.8"
-FRAME = "X +x Y +y Z +z, passive, X||a Z||c*"
 # output.zig:124-138 — the TSL symmetry code of each Laue class, and the class's number (sym.zig)
 TSL = {"c1": 1, "c2": 2, "d2": 22, "c4": 4, "d4": 42, "c3": 3, "d3": 32, "c6": 6, "d6": 62, "t": 23, "o": 43}
 LAUE_NUMBER = {"c1": 1, "c2": 2, "d2": 3, "c4": 4, "d4": 5, "c3": 6, "d3": 7, "c6": 8, "d6": 9, "t": 10, "o": 11}
@@ -21,16 +20,29 @@ class ExportError(ValueError):
     pass
 
 
-def export_text(kind, res, phases, geo, rows, cols, pat_h, pat_w, voltage_kv=float("nan")):
+def export_text(kind, res, phases, geo, rows, cols, pat_h, pat_w, voltage_kv=float("nan"), frame=None):
     """output.zig:148-216 — kind "ang" or "ctf". res: quat [n, 4], ncc, nmi, phase [n] (−1: not
     indexed); phases: dicts of name, laue (the Laue class's key), lattice (a, b, c, α, β, γ) and
-    space_group; geo: pc (Bruker), step_x_um, step_y_um, sample_tilt_deg."""
+    space_group; geo: pc (Bruker), step_x_um, step_y_um, sample_tilt_deg; frame: the convention
+    the orientations are written in (convention.Frame; None: the engine's own), named in the
+    header."""
+    from .convention import Frame
+
+    frame = frame or Frame()
+    crystal = []
     for p in phases:
-        if p.get("lattice") is None:
+        c = frame.crystal_of(p.get("lattice")) if p.get("lattice") is not None else None
+        if c is None:
             raise ExportError("MissingPhaseLattice: a phase's master names no cell (a, b, c, α, β, γ)")
+        crystal.append(c)
     q = np.asarray(res["quat"], np.float64).reshape(-1, 4)
-    bunge = R.to_bunge(q)
     phase = np.asarray(res["phase"]).reshape(-1)
+    if frame.is_engine():
+        bunge = R.to_bunge(q)
+    else:
+        c = np.array(crystal + [[1.0, 0.0, 0.0, 0.0]])[np.where((phase >= 0) & (phase < len(crystal)), phase, -1)]
+        bunge = R.to_bunge(frame.to_frame(q, c))
+    frame_text = frame.describe()
     ncc = np.asarray(res["ncc"], np.float64).reshape(-1)
     nmi = np.asarray(res["nmi"], np.float64).reshape(-1)
     n_ph = len(phases)
@@ -50,7 +62,7 @@ def export_text(kind, res, phases, geo, rows, cols, pat_h, pat_w, voltage_kv=flo
                        "# NumberFamilies        0\n#\n")
         out.append(f"# GRID: SqrGrid\n# XSTEP: {geo.step_x_um:.6f}\n# YSTEP: {geo.step_y_um:.6f}\n# NCOLS_ODD: {cols}\n"
                    f"# NCOLS_EVEN: {cols}\n# NROWS: {rows}\n#\n# SOFTWARE: zebsdsolve {VERSION} (EDAX pattern centre)\n"
-                   f"# FRAME: {FRAME}\n# COLUMNS: phi1 PHI phi2 x y IQ(NMI) CI(NCC) Phase SEM Fit\n")
+                   f"# FRAME: {frame_text}\n# COLUMNS: phi1 PHI phi2 x y IQ(NMI) CI(NCC) Phase SEM Fit\n")
         for r in range(rows):
             for c in range(cols):
                 at = r * cols + c
@@ -65,7 +77,7 @@ def export_text(kind, res, phases, geo, rows, cols, pat_h, pat_w, voltage_kv=flo
                            f"{pid:2d} {0:6d} {0.0:6.3f}\n")
     elif kind == "ctf":
         kv = 0.0 if math.isnan(voltage_kv) else voltage_kv
-        out.append(f"Channel Text File\nPrj\tzebsdsolve; frame {FRAME}\nAuthor\t\nJobMode\tGrid\nXCells\t{cols}\n"
+        out.append(f"Channel Text File\nPrj\tzebsdsolve; frame {frame_text}\nAuthor\t\nJobMode\tGrid\nXCells\t{cols}\n"
                    f"YCells\t{rows}\nXStep\t{geo.step_x_um:.6f}\nYStep\t{geo.step_y_um:.6f}\nAcqE1\t0\nAcqE2\t0\nAcqE3\t0\n")
         out.append(f"Euler angles refer to Sample Coordinate system (CS0)!\tMag\t0\tCoverage\t100\tDevice\t0\tKV\t{kv:.1f}"
                    f"\tTiltAngle\t{geo.sample_tilt_deg:.2f}\tTiltAxis\t0\n")

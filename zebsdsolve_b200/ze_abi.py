@@ -28,8 +28,6 @@ FORMATS = ("kikuchipy h5ebsd", "Bruker h5ebsd", "EDAX h5ebsd", "Oxford h5oina", 
            "NORDIF", "EMsoft patterns")
 FORMAT_ALIASES = {"edax_up": "EDAX up1/up2", "oxford_ebsp": "Oxford ebsp", "nordif": "NORDIF"}
 # convention.zig:54-59, 102-109: the engine's own frame (kikuchipy's), the only one here
-ENGINE_FRAME = {"axes": [1, 2, 3], "active": False, "crystal": "x_a_z_cstar"}
-ENGINE_FRAME_TEXT = "X +x Y +y Z +z, passive, X||a Z||c*"
 
 U32, I32, U64, F64 = ctypes.c_uint32, ctypes.c_int32, ctypes.c_uint64, ctypes.c_double
 
@@ -871,24 +869,50 @@ def ze_export(x, kind, buf, cap):
 
 
 ze_export_h5oina = _not_built("export_h5oina", "the .h5oina export is not part of this engine")
-ze_identify_frame = _not_built("identify_frame", "finding a maker's orientation convention is not part of this "
-                                                 "engine; its exports use the engine's own frame")
+@_api("identify_frame")
+def ze_identify_frame(x, euler, phase, n, buf, cap):
+    """exports.zig:785-817 — the convention of a maker's orientations (Bunge radians, 3 f64 a cell,
+    and a label a cell, negative: not indexed; with a null `euler` the scan file's own), found
+    against the results, as JSON: the frame, how well it holds, the misorientation left, the
+    labels matched and whether the exports took it. BufferTooSmall when cap is short."""
+    if euler:
+        if not phase:
+            raise RuntimeError("MissingPhases")
+        got = x.s.identify_frame(_view(euler, 3 * n, np.float64).copy(), _view(phase, n, np.int32).copy())
+    else:
+        got = x.s.identify_frame()
+    keys = ("frame", "cells", "within", "median_deg", "runner_up_deg", "installed", "misorientation_cells",
+            "misorientation", "misorientation_rows", "misorientation_cols", "matched")
+    b = json.dumps({k: got[k] for k in keys}, separators=(",", ":")).encode()
+    if cap < len(b):
+        raise RuntimeError("BufferTooSmall")
+    _put(buf, cap, b)
+    return len(b)
+
+
+def _frame_of(x):
+    from .convention import Frame
+
+    return (getattr(x.s._e, "convention", None) if x is not None else None) or Frame()
 
 
 def ze_frame(h, buf, cap):
-    b = json.dumps({**ENGINE_FRAME, "text": ENGINE_FRAME_TEXT}, separators=(",", ":")).encode()
+    """exports.zig:836-845 — the convention the exports write in, as JSON (axes, active, crystal
+    and a line naming it); its length, copied as far as cap allows."""
+    b = json.dumps(_frame_of(_handles.get(int(h))).as_dict(), separators=(",", ":")).encode()
     _put(buf, cap, b)
     return len(b)
 
 
 @_api("set_frame")
 def ze_set_frame(x, js, n):
-    if n == 0:
-        return 0
-    f = json.loads(_text(js, n))
-    if all(f.get(k, v) == v for k, v in ENGINE_FRAME.items()):
-        return 0
-    raise NotBuilt("orientation conventions other than the engine's own are not part of this engine")
+    """exports.zig:847-859 — set the exports' convention from JSON as ze_frame gives it (axes,
+    active, crystal; other keys ignored), or the engine's own when empty; InvalidFrame unless it
+    is one of the conventions."""
+    from .convention import Frame
+
+    x.s._e.convention = None if n == 0 else Frame.from_dict(json.loads(_text(js, n)))
+    return 0
 
 
 def _ops(x, phase):
