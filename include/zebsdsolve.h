@@ -17,9 +17,8 @@
  * Not part of this engine (the call fails, ze_error says so): master simulation and crystals
  * (ze_sim_*, ze_cell_info, ze_cell_view, ze_sphere_view), toy scans (ze_synthesize), the IPF
  * colours (ze_map's kinds 0-2, ze_ipf_key; its score, phase and sweep maps, kinds 3-7, are built),
- * the .h5oina export, orientation conventions other than the engine's own (ze_identify_frame;
- * ze_set_frame takes only the engine's own), WGSL (ze_compile_wgsl reports that none is compiled;
- * ze_shader lists no modules).
+ * the .h5oina export, WGSL (ze_compile_wgsl reports that none is compiled; ze_shader lists no
+ * modules).
  *
  * A native host (not a Python process) links libpython3.12 as well; the first call then starts an
  * interpreter, which finds the package beside the library.
