@@ -15,7 +15,7 @@
  * path it takes is not used (the engine runs on the current CUDA device).
  *
  * Not part of this engine (the call fails, ze_error says so): master simulation and crystals
- * (ze_sim_*, ze_cell_info, ze_cell_view, ze_sphere_view), toy scans (ze_synthesize), the IPF
+ * (ze_sim_*, ze_cell_info, ze_cell_view, ze_sphere_view), the IPF
  * colours (ze_map's kinds 0-2, ze_ipf_key; its score, phase and sweep maps, kinds 3-7, are built),
  * the .h5oina export, WGSL (ze_compile_wgsl reports that none is compiled; ze_shader lists no
  * modules).

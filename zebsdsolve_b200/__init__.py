@@ -347,6 +347,89 @@ class Solver:
 
     # ── simulation ──
 
+    def synthesize(self, **settings):
+        """A toy scan from the phases loaded, in place of any scan open, and its answer
+        (__init__.py:233-258, engine.zig:2778-2896): a dict with quaternions (rows, cols, 4), phase
+        (rows, cols; −1 a blank cell), grain (rows, cols) and geometry (the one it was simulated
+        under, its true one).
+
+        Keywords are settings. The microstructure, from `toy_seed`: `toy_rows` × `toy_cols` cells,
+        each in the grain of the nearest of `toy_grains` points scattered over the map, each grain
+        with a uniformly random orientation and phase; `toy_spread_deg` turns every cell a little
+        within its grain; `toy_blank` is the share of cells holding no crystal. The detector:
+        patterns of `toy_height` × `toy_width`, the simulation (darkest pixel 0, mean 1 over the
+        crystals) weighted `toy_contrast` on a background of mean 1 (flat, or a Gaussian hump of
+        `toy_background_sigma` × the width). The counting: a Poisson draw per pixel at a mean of
+        `toy_counts` electrons (0: none), from `toy_noise_seed` (0: from `toy_seed`). The draws
+        are numpy's (PCG64), so a seed gives the reference's distributions, not its numbers."""
+        from . import rotations as R
+
+        if settings:
+            self.configure(**settings)
+        e = self._e
+        if not e.phases:
+            raise Error("synthesize: NoPhases")
+        st = e.set
+        rows, cols, h, w = st["toy_rows"], st["toy_cols"], st["toy_height"], st["toy_width"]
+        n, px = rows * cols, h * w
+        geometry = self.geometry
+        # an empty scan of the shape first: a cell's place in it is part of its geometry
+        self.set_patterns(np.zeros((rows, cols, h, w), np.float32))
+        rng = np.random.default_rng(int(st["toy_seed"]))
+        k = min(int(st["toy_grains"]), n)
+        gx, gy = rng.random(k) * cols, rng.random(k) * rows
+        gq = R.qstd(rng.normal(size=(k, 4)))  # four normal numbers, normalized: uniform over the rotations
+        gp = rng.integers(0, len(e.phases), k)
+        grain = np.empty(n, np.int64)
+        x = np.arange(cols) + 0.5
+        for r in range(rows):  # the nearest point, a row at a time (the first of equals)
+            d = (gx[None, :] - x[:, None]) ** 2 + (gy[None, :] - (r + 0.5)) ** 2
+            grain[r * cols:(r + 1) * cols] = np.argmin(d, 1)
+        q = gq[grain]
+        spread = math.radians(st["toy_spread_deg"]) / math.sqrt(3.0)
+        if spread > 0:
+            q = R.qstd(R.qmul(R.exp_map(spread * rng.normal(size=(n, 3))), q))
+        phase = gp[grain].astype(np.int32)
+        if st["toy_blank"] > 0:
+            phase[rng.random(n) < st["toy_blank"]] = -1
+        data = np.zeros((n, px), np.float32)
+        chunk = max(1, (4 << 20) // px)
+        made = 0
+        with e.at_full():  # simulated at the stored size (engine.zig:2828)
+            for p in range(len(e.phases)):
+                cells = np.flatnonzero(phase == p)
+                for i in range(0, len(cells), chunk):
+                    c = cells[i:i + chunk]
+                    sims = self._call("synthesize", e.simulate, p, c, q[c].astype(np.float32))
+                    data[c] = np.asarray(sims).reshape(len(c), px)
+                    made += len(c)
+                    e.events.append({"kind": "progress", "stage": "synthesize", "done": made, "total": n})
+        # the detector: the simulation (its darkest pixel 0, its mean 1) on a background (mean 1)
+        crystal = phase >= 0
+        mean = float(data[crystal].mean(dtype=np.float64)) if crystal.any() else 0.0
+        low = float(data[crystal].min()) if crystal.any() else 0.0
+        gain = 1.0 / (mean - low) if crystal.any() and mean > low else 0.0
+        back = np.ones(px)
+        if st["toy_background_sigma"] > 0:
+            sg = st["toy_background_sigma"] * w
+            yy, xx = np.mgrid[0:h, 0:w]
+            back = np.exp(-((xx + 0.5 - 0.5 * w) ** 2 + (yy + 0.5 - 0.5 * h) ** 2) / (2 * sg * sg)).reshape(-1)
+            back *= px / back.sum()
+        blank = (~crystal) | (gain == 0)
+        signal = np.where(blank[:, None], 1.0, (data - low) * gain)
+        intensity = (1 - st["toy_contrast"]) * back[None, :] + st["toy_contrast"] * signal
+        if st["toy_counts"] > 0:
+            noise = np.random.default_rng(int(st["toy_noise_seed"]) or (int(st["toy_seed"]) ^ 0x9E3779B97F4A7C15))
+            data = noise.poisson(st["toy_counts"] * intensity).astype(np.float32)
+        else:
+            data = intensity.astype(np.float32)
+        self.set_patterns(data.reshape(rows, cols, h, w))
+        e.log(f"toy scan: {rows} × {cols} patterns of {h} × {w}, {k} grains of {len(e.phases)} phase(s), "
+              f"{int((~crystal).sum())} blank cells, contrast {st['toy_contrast']:.2f}, {st['toy_counts']:.4f} "
+              f"electrons a pixel, seed {st['toy_seed']}")
+        return {"quaternions": q.astype(np.float32).reshape(rows, cols, 4), "phase": phase.reshape(rows, cols),
+                "grain": grain.astype(np.int32).reshape(rows, cols), "geometry": geometry}
+
     def simulate(self, quaternions, cells=None, phase=0):
         q = np.asarray(quaternions, np.float32).reshape(-1, 4)
         cells = np.arange(len(q)) if cells is None else np.asarray(cells).reshape(-1)

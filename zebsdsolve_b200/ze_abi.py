@@ -265,7 +265,19 @@ def ze_set_patterns(x, data, n, pixel, rows, cols, h, w):
     return 0
 
 
-ze_synthesize = _not_built("synthesize", "toy scans (Solver.synthesize) are not part of this engine")
+@_api("synthesize")
+def ze_synthesize(x, quats, phase, grain, n):
+    """exports.zig:97-102 — a toy scan from the phases loaded, in place of any scan open
+    (Solver.synthesize): its orientations (4 f32 a cell), phases and grains (i32) into the
+    caller's buffers, n = toy_rows × toy_cols cells (BadLength otherwise)."""
+    st = x.s._e.set
+    if n != st["toy_rows"] * st["toy_cols"]:
+        raise RuntimeError("BadLength")
+    got = x.s.synthesize()
+    _view(quats, 4 * n, np.float32)[:] = got["quaternions"].reshape(-1)
+    _view(phase, n, np.int32)[:] = got["phase"].reshape(-1)
+    _view(grain, n, np.int32)[:] = got["grain"].reshape(-1)
+    return 0
 
 
 def ze_close_scan(h):
